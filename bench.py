@@ -1,0 +1,322 @@
+"""Benchmark: GTEPS of the fused decode kernels on the compressed temporal graph.
+
+A step is one pass of the seven reference workloads (RA/neighbour access, BFS, CC, PageRank x30,
+HITS x30, degree centrality, JP colouring) over the configuration "2M vertices, 40M temporal
+edges" -- seeded synthetic data with that shape, compressed in the reference's format and held
+in HBM.  value = temporal edges decoded by all workloads / device time (GTEPS, whole job over
+all ranks); e2e = the same through the public C-ABI calls with host result buffers (device-to-
+host copies inside the timed region); roofline = the PageRank iteration kernel's compressed bytes
+per launch / its average launch time against the measured HBM copy bandwidth.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+
+Multi-GPU runs are independent replicas (the north star is one GPU; nothing is exchanged).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+CONFIG_NAME = "all7"
+WORKLOAD = ("all7: 2,000,000 vertices, 40,000,000 temporal edges, power-law out-degree alpha 2.0 with "
+            "preferential in-degree, 70% of successors within +-64, 20% of each list copied from a vertex "
+            "in the window of 7, Poisson timestamps over a 1e8 span; RA, BFS, CC, PR x30, HITS x30, DC, GC")
+METRIC = "GTEPS on compressed graph (all seven workloads)"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+def dataset_dir() -> Path:
+    return Path(os.environ.get("TGA_BENCH_DATA", Path(tempfile.gettempdir()) / "tga_bench_all7"))
+
+
+def ensure_dataset(tga, rank: int, world: int, barrier):
+    d = dataset_dir()
+    marker = d / "summary.json"
+    if rank == 0 and not marker.exists():
+        t = time.time()
+        s = tga.generate(tga.CONFIGS[CONFIG_NAME], d, CONFIG_NAME)
+        s["gen_seconds"] = time.time() - t
+        marker.write_text(json.dumps(s))
+        log(f"generated {CONFIG_NAME} in {s['gen_seconds']:.1f}s: {s}")
+    if world > 1:
+        barrier()
+    return d, json.loads(marker.read_text())
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.path = Path(tempfile.gettempdir()) / f"tga_clocks_{os.getpid()}.csv"
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.gpu)], stdout=open(self.path, "w"),
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path.exists():
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        self.path.unlink(missing_ok=True)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def suite(g, outputs: bool):
+    """One step: the seven workloads; returns (edges decoded, launches, per-workload timing)."""
+    cfg = g.cfg
+    per = {}
+    edges = launches = 0
+
+    def rec(name):
+        nonlocal edges, launches
+        t = g.timing()
+        per[name] = t
+        edges += t["edges_decoded"]
+        launches += t["launches"]
+
+    g.neighbor_access(outputs=outputs); rec("RA")
+    g.bfs(cfg.bfs_start_vertex, outputs=outputs); rec("BFS")
+    g.connected_components(outputs=outputs); rec("CC")
+    g.pagerank(30, outputs=outputs); rec("PR")
+    g.hits(30, outputs=outputs); rec("HITS")
+    g.degree_centrality(0, 0, outputs=outputs); rec("DC")
+    g.color(0, outputs=outputs); rec("GC")
+    return edges, launches, per
+
+
+def d2h_bytes_per_step(nv: int) -> int:
+    # RA: uint8 + uint64 + int32; BFS: 2x int32; CC: int32; PR: f32; HITS: 2x f32; DC: int32 + int64; GC: 2x u32
+    return nv * ((1 + 8 + 4) + 8 + 4 + 4 + 8 + 12 + 8)
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        j = json.loads(p.read_text())
+        return float(j["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def kernel_traffic():
+    """DRAM bytes per launch of the PageRank kernel from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / "traffic.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text()).get("k_pr_iter_all7_bytes_per_launch")
+        except Exception:
+            return None
+    return None
+
+
+def cpu_baseline(ddir: Path, summary: dict, threads: int):
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle
+
+    n = int(summary["n"])
+    o = pyoracle.Oracle(ddir, CONFIG_NAME, n, materialize=False)
+    iters = 1
+    t = time.time()
+    _, edges = o.stream_pagerank(n - 1, n, 0, iters, threads=threads)
+    dt = time.time() - t
+    o.close()
+    return {"value": edges / dt / 1e9, "unit": "GTEPS", "cores": threads or pyoracle.max_threads(), "kind": "port",
+            "sample": f"{iters} temporal-PageRank iteration over the full {CONFIG_NAME} graph, every list decoded "
+                      f"from the compressed streams by the C oracle port ({edges} edges, {dt:.2f}s)"}
+
+
+def run_reference(args):
+    rank, local, world = dist_env()
+    if rank != 0:
+        return 0
+    import compresstemporalgraph_b200 as tga
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle
+
+    ddir, summary = ensure_dataset(tga, 0, 1, None)
+    n = int(summary["n"])
+    threads = pyoracle.max_threads()
+    o = pyoracle.Oracle(ddir, CONFIG_NAME, n, materialize=False)
+    for _ in range(args.warmup):
+        o.stream_decode(0, n - 1, threads=threads)
+    t = time.time()
+    edges = 0
+    for _ in range(args.steps):
+        _, e = o.stream_decode(0, n - 1, threads=threads)
+        edges += e
+    dt = time.time() - t
+    v = edges / dt / 1e9
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "GTEPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dt * 1000 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "sample": "one full neighbour-access decode sweep per step"},
+            "cpu_baseline": {"value": v, "unit": "GTEPS", "cores": threads, "kind": "port",
+                             "sample": "full decode sweep of every list (successors + timestamps) of the 2M/40M "
+                                       "graph per step, C oracle port, all host threads"},
+            "e2e": {"value": v, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+
+    rank, local, world = dist_env()
+    torch.cuda.set_device(local)
+    barrier = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        barrier = lambda: dist.barrier(device_ids=[local])
+    import compresstemporalgraph_b200 as tga
+
+    ddir, summary = ensure_dataset(tga, rank, world, barrier)
+    n = int(summary["n"])
+    cfg = tga.DatasetConfig(name=CONFIG_NAME, max_label=n - 1, max_vertex=n, bfs_start_vertex=1)
+    g = tga.Graph.open_dir(ddir, CONFIG_NAME, cfg)
+    stream = torch.cuda.ExternalStream(g.stream)
+
+    for _ in range(args.warmup):
+        suite(g, outputs=False)
+
+    def timed(outputs: bool):
+        if barrier:
+            barrier()
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        edges = launches = 0
+        per_all = []
+        for _ in range(args.steps):
+            e, l, per = suite(g, outputs)
+            edges += e
+            launches += l
+            per_all.append(per)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        if barrier:
+            barrier()
+        ms = ev0.elapsed_time(ev1)
+        if world > 1:
+            t = torch.tensor([ms], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, edges, launches, per_all
+
+    with Clocks(local) as clk:
+        ms, edges, launches, per_all = timed(outputs=False)
+    clocks = clk.summary()
+    e2e_ms, e2e_edges, _, _ = timed(outputs=True)
+
+    total_edges = edges * world
+    value = total_edges / (ms / 1e3) / 1e9
+    e2e_value = e2e_edges * world / (e2e_ms / 1e3) / 1e9
+
+    # Roofline of the PageRank iteration kernel (30 launches per step, one full decode pass each).
+    pr = [p["PR"] for p in per_all]
+    pr_launch_ms = sum(p["decode_ms"] for p in pr) / max(1, sum(p["decode_launches"] for p in pr))
+    info = g.info
+    active_bytes = info["graph_bytes"] + info["timestamp_bytes"] + info["index_bytes"]
+    achieved = active_bytes / (pr_launch_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peak()
+    traffic = kernel_traffic()
+    breakdown = {}
+    for name in per_all[0]:
+        ms_w = sum(p[name]["total_ms"] for p in per_all) / len(per_all)
+        ed = sum(p[name]["edges_decoded"] for p in per_all) / len(per_all)
+        breakdown[name] = {"ms": round(ms_w, 3), "edges": int(ed), "gteps": round(ed / (ms_w / 1e3) / 1e9, 3) if ms_w else None,
+                           "iterations": per_all[0][name]["iterations"]}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "vertices": n, "temporal_edges": int(summary["m"]),
+                   "compressed_bytes": active_bytes, "l2": "inputs larger than L2 (compressed graph "
+                   f"{active_bytes / 1e6:.0f} MB > 126 MB L2), no flush", "parallelism": f"replicas x{world}"},
+        "e2e": {"value": e2e_value, "unit": "GTEPS", "h2d_bytes_per_step": 64,
+                "d2h_bytes_per_step": d2h_bytes_per_step(n)},
+        "roofline": {"bound": "hbm", "kernel": "k_pr_iter", "achieved": achieved, "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                     "bytes_per_launch": active_bytes, "launch_ms": pr_launch_ms},
+        "clocks": clocks,
+        "gpu_launches": launches,
+        "workloads": breakdown,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline(ddir, summary, 0)
+        except Exception as e:  # reported, not fatal
+            line["cpu_baseline"] = {"value": None, "error": str(e)}
+    g.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,154 @@
+// Host-side MSB-first bit streams and the instantaneous codes of the compressed
+// temporal-graph format (unary, Elias gamma, zeta_k, minimal binary, int2nat).
+//
+// The on-disk streams are written exactly like dsiutils' OutputBitStream, which the
+// reference encoder uses (BVMultiGraph.java:485-563 write/readResidual, writeBlock;
+// EvolvingMultiGraph.java:131-144 writeLongZeta of int2nat(delta)):
+//   * bits are packed MSB-first inside each byte, the last byte is zero-padded;
+//   * unary(x)   = x zeros followed by a one                      (x+1 bits);
+//   * gamma(x)   = unary(msb(x+1)) then the low msb(x+1) bits of x+1;
+//   * zeta_k(x)  = unary(h), h = msb(x+1)/k, then x+1-2^(hk) in minimal binary
+//                  over [0, 2^(hk)(2^k-1)): hk+k-1 bits if the value is < 2^(hk),
+//                  else (value + 2^(hk)) in hk+k bits;
+//   * int2nat(x) = 2x for x >= 0, -2x-1 for x < 0 (nat2int is its inverse).
+// The decode tables shipped with the reference (gpu_cuda/decode_tables/gammaInA.txt,
+// zetaInA.txt) are regenerated from these definitions by table16() and match entry
+// for entry.
+#pragma once
+#include <cstdint>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace tga {
+
+inline int msb64(uint64_t v) { return v ? 63 - __builtin_clzll(v) : -1; }
+
+inline uint64_t int2nat(int64_t x) { return x >= 0 ? (uint64_t)x << 1 : ((uint64_t)(-(x + 1)) << 1) | 1u; }
+inline int64_t nat2int(uint64_t n) { return (n & 1) ? -(int64_t)(n >> 1) - 1 : (int64_t)(n >> 1); }
+
+class BitWriter {
+ public:
+  std::vector<uint8_t> bytes;
+  uint64_t nbits = 0;
+
+  void reserve_bits(uint64_t b) { bytes.reserve((b + 7) / 8); }
+
+  // Appends the low `len` bits of `v`, most significant first (len <= 64).
+  void write_bits(uint64_t v, int len) {
+    while (len > 0) {
+      const int used = (int)(nbits & 7);
+      if (used == 0) bytes.push_back(0);
+      const int room = 8 - used;
+      const int take = len < room ? len : room;
+      const uint64_t chunk = (len == 64 && take == 64) ? v : (v >> (len - take)) & ((1ull << take) - 1);
+      bytes.back() |= (uint8_t)(chunk << (room - take));
+      nbits += take;
+      len -= take;
+    }
+  }
+  int write_unary(uint64_t x) {
+    uint64_t z = x;
+    while (z >= 32) { write_bits(0, 32); z -= 32; }
+    write_bits(1, (int)z + 1);
+    return (int)x + 1;
+  }
+  int write_gamma(uint64_t x) {
+    const uint64_t v = x + 1;
+    const int m = msb64(v);
+    write_unary((uint64_t)m);
+    if (m) write_bits(v, m);
+    return 2 * m + 1;
+  }
+  int write_minimal_binary(uint64_t x, uint64_t b) {
+    const int lb = msb64(b);
+    const uint64_t m = (lb + 1 >= 64 ? 0ull : (1ull << (lb + 1))) - b;
+    if (x < m) { if (lb) write_bits(x, lb); return lb; }
+    write_bits(x + m, lb + 1);
+    return lb + 1;
+  }
+  int write_zeta(uint64_t x, int k) {
+    const uint64_t v = x + 1;
+    const int h = msb64(v) / k;
+    const int u = write_unary((uint64_t)h);
+    const uint64_t left = 1ull << (h * k);
+    return u + write_minimal_binary(v - left, (left << k) - left);
+  }
+  int write_long(uint64_t x, int len) { write_bits(x, len); return len; }
+};
+
+// Counts bits without storing them (the "NullOutputStream" bit counter of diffComp).
+struct BitCounter {
+  uint64_t nbits = 0;
+  int write_unary(uint64_t x) { nbits += x + 1; return (int)x + 1; }
+  int write_gamma(uint64_t x) { const int m = msb64(x + 1); nbits += 2 * m + 1; return 2 * m + 1; }
+  int write_zeta(uint64_t x, int k) {
+    const uint64_t v = x + 1;
+    const int h = msb64(v) / k;
+    const uint64_t left = 1ull << (h * k);
+    const int len = (v - left < left) ? h * k + k - 1 : h * k + k;
+    nbits += h + 1 + len;
+    return h + 1 + len;
+  }
+};
+
+// Sequential MSB-first reader over a byte buffer (host side; used by the loader,
+// the EF producer and the index builders, never on the device).
+class BitReader {
+ public:
+  BitReader(const uint8_t* d, uint64_t nbytes, uint64_t pos = 0) : d_(d), nbits_(nbytes * 8), pos_(pos) {}
+  uint64_t pos() const { return pos_; }
+  void seek(uint64_t p) { pos_ = p; }
+  int bit() {
+    if (pos_ >= nbits_) throw std::runtime_error("bit stream overrun at bit " + std::to_string(pos_));
+    const int b = (d_[pos_ >> 3] >> (7 - (pos_ & 7))) & 1;
+    ++pos_;
+    return b;
+  }
+  uint64_t bits(int len) {
+    uint64_t v = 0;
+    for (int i = 0; i < len; ++i) v = (v << 1) | (uint64_t)bit();
+    return v;
+  }
+  uint64_t unary() {
+    uint64_t n = 0;
+    while (bit() == 0) ++n;
+    return n;
+  }
+  uint64_t gamma() {
+    const uint64_t m = unary();
+    if (m > 63) throw std::runtime_error("gamma code too long");
+    return ((1ull << m) | bits((int)m)) - 1;
+  }
+  uint64_t zeta(int k) {
+    const uint64_t h = unary();
+    if (h * k + k > 64) throw std::runtime_error("zeta code too long");
+    const uint64_t left = 1ull << (h * k);
+    const uint64_t val = bits((int)(h * k + k - 1));
+    if (val < left) return val + left - 1;
+    return ((val << 1) | (uint64_t)bit()) - 1;
+  }
+
+ private:
+  const uint8_t* d_;
+  uint64_t nbits_;
+  uint64_t pos_;
+};
+
+// 16-bit look-ahead table in the reference's layout: entry w = (code length << 16) |
+// value for the code that starts at the top of the 16-bit window w, 0 when the code
+// does not fit in 16 bits.  kind 0 = gamma, kind 3 = zeta_3.
+inline std::vector<int32_t> table16(int kind) {
+  std::vector<int32_t> t(65536, 0);
+  for (uint32_t w = 0; w < 65536; ++w) {
+    uint8_t buf[4] = {(uint8_t)(w >> 8), (uint8_t)w, 0, 0};
+    BitReader r(buf, 4);
+    uint64_t v;
+    try { v = kind == 0 ? r.gamma() : r.zeta(kind); } catch (...) { continue; }
+    if (r.pos() <= 16 && v < 65536) t[w] = (int32_t)((r.pos() << 16) | v);
+  }
+  return t;
+}
+
+}  // namespace tga

@@ -1,0 +1,391 @@
+// Loader and handle management: reads the reference's on-disk files, builds the EF select
+// samples, uploads everything into HBM in the layout documented in dview.cuh, and computes the
+// per-vertex outdegrees once.
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "decoder.cuh"
+#include "engine.hpp"
+#include "format.hpp"
+
+namespace tga {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+int DevBuf::ensure(size_t n) {
+  if (n <= bytes && p) return TGA_OK;
+  release();
+  if (n == 0) n = 8;
+  cudaError_t e = cudaMalloc(&p, n);
+  if (e != cudaSuccess) {
+    p = nullptr;
+    bytes = 0;
+    cudaGetLastError();
+    return fail(TGA_E_OOM, "device allocation of " + std::to_string(n) + " bytes failed: " + cudaGetErrorString(e));
+  }
+  bytes = n;
+  return TGA_OK;
+}
+
+void DevBuf::release() {
+  if (p) cudaFree(p);
+  p = nullptr;
+  bytes = 0;
+}
+
+GraphHandle::~GraphHandle() {
+  if (stream) cudaStreamSynchronize(stream);
+  for (DevBuf* b : {&d_graph, &d_ts, &d_gl, &d_gu, &d_gs, &d_tl, &d_tu, &d_ts_samples, &d_err, &d_deg, &s_a, &s_b,
+                    &s_c, &s_d, &s_e, &s_f, &s_g, &s_q0, &s_q1, &s_cnt, &s_sum})
+    b->release();
+  for (auto& k : ktimers) {
+    if (k.a) cudaEventDestroy(k.a);
+    if (k.b) cudaEventDestroy(k.b);
+  }
+  if (ev_begin) cudaEventDestroy(ev_begin);
+  if (ev_end) cudaEventDestroy(ev_end);
+  if (h_pinned) cudaFreeHost(h_pinned);
+  if (stream) cudaStreamDestroy(stream);
+}
+
+int GraphHandle::begin_call() {
+  timing = tga_timing{};
+  ktimer_used = 0;
+  TGA_CUDA_TRY(cudaMemsetAsync(d_err.p, 0, sizeof(uint32_t), stream));
+  TGA_CUDA_TRY(cudaEventRecord(ev_begin, stream));
+  return TGA_OK;
+}
+
+cudaEvent_t* GraphHandle::kernel_begin() {
+  if (!time_kernels) return nullptr;
+  if (ktimer_used == ktimers.size()) {
+    KernelTimer k;
+    if (cudaEventCreate(&k.a) != cudaSuccess || cudaEventCreate(&k.b) != cudaSuccess) return nullptr;
+    ktimers.push_back(k);
+  }
+  KernelTimer& k = ktimers[ktimer_used++];
+  cudaEventRecord(k.a, stream);
+  return &k.a;
+}
+
+void GraphHandle::kernel_end(cudaEvent_t* pair) {
+  if (!pair) return;
+  KernelTimer* k = reinterpret_cast<KernelTimer*>(pair);
+  cudaEventRecord(k->b, stream);
+  timing.decode_launches++;
+}
+
+int GraphHandle::check_device_error() {
+  uint32_t err = 0;
+  TGA_CUDA_TRY(cudaMemcpyAsync(h_pinned, d_err.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+  TGA_CUDA_TRY(cudaStreamSynchronize(stream));
+  err = h_pinned[0];
+  if (err) {
+    std::string what;
+    if (err & kErrCursor) what += " cursor-past-stream";
+    if (err & kErrCode) what += " code-too-long";
+    if (err & kErrChain) what += " reference-chain-too-deep";
+    if (err & kErrId) what += " vertex-id-out-of-range";
+    if (err & kErrCount) what += " list-shorter-than-outdegree";
+    if (err & kErrIndex) what += " index-lookup-out-of-range";
+    if (err & kErrTimeout) return fail(TGA_E_TIMEOUT, "iteration cap reached on the device");
+    return fail(TGA_E_DECODE, "device decode error:" + what);
+  }
+  return TGA_OK;
+}
+
+int GraphHandle::end_call() {
+  TGA_CUDA_TRY(cudaEventRecord(ev_end, stream));
+  TGA_CUDA_TRY(cudaGetLastError());
+  int rc = check_device_error();
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ev_begin, ev_end);
+  timing.total_ms = ms;
+  double dk = 0;
+  for (size_t i = 0; i < ktimer_used; ++i) {
+    float t = 0;
+    if (cudaEventElapsedTime(&t, ktimers[i].a, ktimers[i].b) == cudaSuccess) dk += t;
+  }
+  timing.decode_ms = dk;
+  return rc;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Loading
+
+static void to_be_words(const std::vector<uint8_t>& bytes, std::vector<uint64_t>& words, size_t pad_words) {
+  const size_t nw = (bytes.size() + 7) / 8;
+  words.assign(nw + pad_words, 0);
+  for (size_t i = 0; i < bytes.size(); ++i) words[i >> 3] |= (uint64_t)bytes[i] << (56 - 8 * (i & 7));
+}
+
+static void to_le_words(const std::vector<uint8_t>& bytes, std::vector<uint64_t>& words, size_t pad_words) {
+  const size_t nw = (bytes.size() + 7) / 8;
+  words.assign(nw + pad_words, 0);
+  std::memcpy(words.data(), bytes.data(), bytes.size());
+}
+
+// samples[k] = position of the (64k)-th one; returns the number of ones.
+static uint64_t build_select_samples(const std::vector<uint64_t>& upper, std::vector<uint64_t>& samples) {
+  samples.clear();
+  uint64_t ones = 0;
+  for (size_t wi = 0; wi < upper.size(); ++wi) {
+    uint64_t w = upper[wi];
+    while (w) {
+      const int b = __builtin_ctzll(w);
+      if ((ones & 63) == 0) samples.push_back(wi * 64 + (uint64_t)b);
+      ++ones;
+      w &= w - 1;
+    }
+  }
+  samples.push_back(upper.size() * 64);  // guard
+  return ones;
+}
+
+static std::map<std::string, std::string> read_properties(const std::string& path) {
+  std::map<std::string, std::string> m;
+  std::vector<uint8_t> raw;
+  if (!read_file(path, raw)) return m;
+  std::string s(raw.begin(), raw.end());
+  size_t p = 0;
+  while (p < s.size()) {
+    size_t e = s.find('\n', p);
+    if (e == std::string::npos) e = s.size();
+    std::string line = s.substr(p, e - p);
+    p = e + 1;
+    if (line.empty() || line[0] == '#') continue;
+    const size_t eq = line.find('=');
+    if (eq == std::string::npos) continue;
+    m[line.substr(0, eq)] = line.substr(eq + 1);
+  }
+  return m;
+}
+
+template <class T>
+static int upload(GraphHandle& h, DevBuf& b, const std::vector<T>& v) {
+  int rc = b.ensure(v.size() * sizeof(T));
+  if (rc) return rc;
+  TGA_CUDA_TRY(cudaMemcpy(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  h.info.device_bytes += v.size() * sizeof(T);
+  return TGA_OK;
+}
+
+__global__ void k_outdegrees(GraphView g, int32_t* deg, int32_t count) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= count) return;
+  uint64_t pos = ef_get(g, g.gef, (uint64_t)x);
+  deg[x] = (int32_t)read_gamma(g, g.g, pos);
+}
+
+int load_graph(GraphHandle& h, const std::string& dir, const std::string& base, const tga_dataset_cfg& cfg) {
+  h.cfg = cfg;
+  if (cfg.max_label < 0 || cfg.max_vertex <= cfg.max_label)
+    return fail(TGA_E_ARG, "max_vertex must exceed max_label >= 0");
+  const std::string bp = dir + "/" + base;
+  std::vector<uint8_t> graph, ts, gl, gu, tl, tu;
+  const std::pair<const char*, std::vector<uint8_t>*> files[] = {
+      {".graph", &graph}, {".timestamps", &ts}};
+  for (const auto& f : files)
+    if (!read_file(bp + f.first, *f.second))
+      return fail(TGA_E_IO, "Cannot open required file: " + bp + f.first + " (set TGA_COMPRESS_ROOT if needed)");
+  const std::pair<const char*, std::vector<uint8_t>*> idx[] = {
+      {"/graph_lower_bits.bin", &gl}, {"/graph_upper_bits.bin", &gu},
+      {"/timestamp_lower_bits.bin", &tl}, {"/timestamp_upper_bits.bin", &tu}};
+  for (const auto& f : idx)
+    if (!read_file(dir + f.first, *f.second))
+      return fail(TGA_E_IO, "Cannot open required file: " + dir + f.first + " (set TGA_COMPRESS_ROOT if needed)");
+  if (ts.size() < 8) return fail(TGA_E_FORMAT, "timestamps file shorter than its 64-bit header");
+  int64_t header = 0;
+  for (int i = 0; i < 8; ++i) header = (int64_t)(((uint64_t)header << 8) | ts[(size_t)i]);
+  if (cfg.min_timestamp != TGA_UNSET_TS && cfg.min_timestamp != header)
+    return fail(TGA_E_FORMAT, "minTimestamp " + std::to_string(cfg.min_timestamp) +
+                                  " of the configuration differs from the .timestamps header " +
+                                  std::to_string(header));
+
+  const auto props = read_properties(bp + ".properties");
+  auto prop_int = [&](const char* k, long long dflt) -> long long {
+    auto it = props.find(k);
+    return it == props.end() ? dflt : std::atoll(it->second.c_str());
+  };
+  if (prop_int("windowsize", 7) <= 0) return fail(TGA_E_FORMAT, "graphs stored without references (windowsize 0) are not supported");
+  if (prop_int("zetak", 3) != 3) return fail(TGA_E_FORMAT, "only zeta_3 residual coding is supported");
+  const int min_interval = (int)prop_int("minintervallength", 4);
+  if (min_interval < 1) return fail(TGA_E_FORMAT, "minimum interval length must be positive");
+  if (prop_int("maxrefcount", 3) > kMaxLevels - 1)
+    return fail(TGA_E_FORMAT, "reference chains deeper than " + std::to_string(kMaxLevels - 1) + " are not supported");
+
+  std::vector<uint64_t> wg, wt, wgl, wgu, wtl, wtu, sg, st;
+  to_be_words(graph, wg, 2);
+  to_be_words(ts, wt, 2);
+  to_be_words(gl, wgl, 2);
+  to_be_words(tl, wtl, 2);
+  to_le_words(gu, wgu, 1);
+  to_le_words(tu, wtu, 1);
+  const uint64_t gcount = build_select_samples(wgu, sg);
+  const uint64_t tcount = build_select_samples(wtu, st);
+  const int lg = ef_low_bits(graph.size(), cfg.max_label);
+  const int lt = ef_low_bits(ts.size(), cfg.max_label);
+  if (gcount < (uint64_t)cfg.max_label + 1 || tcount < (uint64_t)cfg.max_label + 1)
+    return fail(TGA_E_FORMAT, "EF index holds " + std::to_string(gcount) + "/" + std::to_string(tcount) +
+                                  " entries, fewer than max_label+1 = " + std::to_string(cfg.max_label + 1));
+  if (gl.size() * 8 < gcount * (uint64_t)lg || tl.size() * 8 < tcount * (uint64_t)lt)
+    return fail(TGA_E_FORMAT, "EF lower-bits file too short for its entry count");
+  int64_t n = prop_int("nodes", -1);
+  if (n <= 0) n = (int64_t)std::min<uint64_t>(gcount, tcount);
+  if (n > INT32_MAX) return fail(TGA_E_FORMAT, "more than 2^31-1 vertices");
+
+  h.info.n = (int32_t)n;
+  h.info.max_label = cfg.max_label;
+  h.info.max_vertex = cfg.max_vertex;
+  h.info.active_vertex_begin = cfg.active_vertex_begin;
+  h.info.min_timestamp = header;
+  h.info.graph_bytes = graph.size();
+  h.info.timestamp_bytes = ts.size();
+  h.info.index_bytes = gl.size() + gu.size() + tl.size() + tu.size();
+  h.info.graph_ef_low_bits = lg;
+  h.info.timestamp_ef_low_bits = lt;
+
+  TGA_CUDA_TRY(cudaGetDevice(&h.device));
+  TGA_CUDA_TRY(cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking));
+  TGA_CUDA_TRY(cudaEventCreate(&h.ev_begin));
+  TGA_CUDA_TRY(cudaEventCreate(&h.ev_end));
+  TGA_CUDA_TRY(cudaMallocHost((void**)&h.h_pinned, 4096));
+  int rc;
+  if ((rc = upload(h, h.d_graph, wg)) || (rc = upload(h, h.d_ts, wt)) || (rc = upload(h, h.d_gl, wgl)) ||
+      (rc = upload(h, h.d_gu, wgu)) || (rc = upload(h, h.d_gs, sg)) || (rc = upload(h, h.d_tl, wtl)) ||
+      (rc = upload(h, h.d_tu, wtu)) || (rc = upload(h, h.d_ts_samples, st)))
+    return rc;
+  if ((rc = h.d_err.ensure(256))) return rc;
+  TGA_CUDA_TRY(cudaMemset(h.d_err.p, 0, 256));
+
+  GraphView& v = h.view;
+  v.g = Stream{h.d_graph.as<uint64_t>(), graph.size() * 8, wg.size()};
+  v.t = Stream{h.d_ts.as<uint64_t>(), ts.size() * 8, wt.size()};
+  v.gef = EFView{h.d_gl.as<uint64_t>(), h.d_gu.as<uint64_t>(), h.d_gs.as<uint64_t>(), wgu.size(), gcount, lg};
+  v.tef = EFView{h.d_tl.as<uint64_t>(), h.d_tu.as<uint64_t>(), h.d_ts_samples.as<uint64_t>(), wtu.size(), tcount, lt};
+  v.n = (int32_t)n;
+  v.max_label = cfg.max_label;
+  v.max_vertex = cfg.max_vertex;
+  v.active_begin = cfg.active_vertex_begin;
+  v.min_interval = min_interval;
+  v.min_ts = header;
+  v.err = h.d_err.as<uint32_t>();
+
+  const int32_t ndeg = (int32_t)std::min<int64_t>(n, (int64_t)cfg.max_vertex);
+  if ((rc = h.d_deg.ensure((size_t)cfg.max_vertex * sizeof(int32_t)))) return rc;
+  h.info.device_bytes += (size_t)cfg.max_vertex * sizeof(int32_t);
+  TGA_CUDA_TRY(cudaMemsetAsync(h.d_deg.p, 0, (size_t)cfg.max_vertex * sizeof(int32_t), h.stream));
+  k_outdegrees<<<grid_for(ndeg, 256), 256, 0, h.stream>>>(v, h.d_deg.as<int32_t>(), ndeg);
+  TGA_CUDA_TRY(cudaGetLastError());
+  std::vector<int32_t> deg((size_t)ndeg);
+  TGA_CUDA_TRY(cudaMemcpyAsync(deg.data(), h.d_deg.p, (size_t)ndeg * 4, cudaMemcpyDeviceToHost, h.stream));
+  if ((rc = h.check_device_error())) return rc;
+  int64_t maxd = 0, m = 0;
+  for (int32_t d : deg) {
+    if (d < 0) return fail(TGA_E_FORMAT, "negative outdegree");
+    maxd = std::max<int64_t>(maxd, d);
+    m += d;
+  }
+  // Every temporal edge owns a zeta_2 timestamp code of at least 2 bits.
+  if ((uint64_t)m > (uint64_t)(ts.size() - 8) * 4)
+    return fail(TGA_E_FORMAT, "outdegrees sum to " + std::to_string(m) + " edges, more than the .timestamps stream can hold");
+  // The largest outdegree caps every header-driven loop of the decoder on damaged streams.
+  v.max_list = (int32_t)std::min<int64_t>(INT32_MAX / 4, std::max<int64_t>(maxd, 1));
+  h.info_edges = m;
+  h.degrees = std::move(deg);
+  return TGA_OK;
+}
+
+}  // namespace tga
+
+using namespace tga;
+
+extern "C" {
+
+void tga_cfg_default(tga_dataset_cfg* c) {
+  if (!c) return;
+  std::memset(c, 0, sizeof *c);
+  c->name = "";
+  c->storage_name = nullptr;
+  c->max_label = 0;
+  c->max_vertex = 0;
+  c->min_timestamp = TGA_UNSET_TS;
+  c->min_graph_vertex = 0;
+  c->active_vertex_begin = 0;
+  c->bfs_start_vertex = 1;
+  c->cc_vertex_begin = 1;
+  c->multiple_initial_value = -1;
+  c->pr_iters = 10;
+  c->hits_iters = 10;
+}
+
+const char* tga_last_error(void) { return g_last_error.c_str(); }
+
+static int open_common(const std::string& dir, const std::string& base, const tga_dataset_cfg* cfg, tga_graph** out) {
+  if (!cfg || !out) return fail(TGA_E_ARG, "null argument");
+  *out = nullptr;
+  tga_graph* g = new (std::nothrow) tga_graph();
+  if (!g) return fail(TGA_E_OOM, "host allocation failed");
+  g->name = cfg->name ? cfg->name : "";
+  g->storage = cfg->storage_name ? cfg->storage_name : g->name;
+  const int rc = load_graph(*g, dir, base, *cfg);
+  if (rc) {
+    const std::string msg = tga_last_error();
+    delete g;
+    set_error(msg);
+    return rc;
+  }
+  *out = g;
+  return TGA_OK;
+}
+
+int tga_open(const char* root, const tga_dataset_cfg* cfg, tga_graph** out) {
+  if (!cfg) return fail(TGA_E_ARG, "null configuration");
+  std::string r = root ? root : "";
+  if (r.empty()) {
+    const char* env = std::getenv("TGA_COMPRESS_ROOT");
+    r = (env && env[0]) ? env : "../..";
+  }
+  while (!r.empty() && (r.back() == '/' || r.back() == '\\')) r.pop_back();
+  const std::string name = cfg->name ? cfg->name : "";
+  const std::string storage = cfg->storage_name ? cfg->storage_name : name;
+  if (storage.empty()) return fail(TGA_E_ARG, "dataset name is empty");
+  return open_common(r + "/data/compressed/" + storage, storage, cfg, out);
+}
+
+int tga_open_dir(const char* dir, const char* basename, const tga_dataset_cfg* cfg, tga_graph** out) {
+  if (!dir || !basename) return fail(TGA_E_ARG, "null path");
+  return open_common(dir, basename, cfg, out);
+}
+
+int tga_close(tga_graph* g) {
+  delete g;
+  return TGA_OK;
+}
+
+int tga_get_info(tga_graph* g, tga_info* out) {
+  if (!g || !out) return fail(TGA_E_ARG, "null argument");
+  *out = g->info;
+  return TGA_OK;
+}
+
+int tga_get_timing(tga_graph* g, tga_timing* out) {
+  if (!g || !out) return fail(TGA_E_ARG, "null argument");
+  *out = g->timing;
+  return TGA_OK;
+}
+
+void* tga_stream(tga_graph* g) { return g ? (void*)g->stream : nullptr; }
+
+}  // extern "C"

@@ -1,0 +1,76 @@
+// Host-side state of one resident compressed graph (the object behind tga_graph*).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/tga.h"
+#include "dview.cuh"
+
+namespace tga {
+
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+
+#define TGA_CUDA_TRY(expr)                                                                    \
+  do {                                                                                        \
+    cudaError_t e_ = (expr);                                                                  \
+    if (e_ != cudaSuccess)                                                                    \
+      return ::tga::fail(e_ == cudaErrorMemoryAllocation ? TGA_E_OOM : TGA_E_CUDA,           \
+                         std::string(#expr " failed: ") + cudaGetErrorString(e_));            \
+  } while (0)
+
+// Growable device buffer owned by a handle.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  int ensure(size_t n);  // keeps contents only when no growth is needed
+  void release();
+  template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+struct KernelTimer {
+  cudaEvent_t a = nullptr, b = nullptr;
+};
+
+struct GraphHandle {
+  tga_dataset_cfg cfg{};
+  std::string name, storage;
+  tga_info info{};
+  GraphView view{};
+  cudaStream_t stream = nullptr;
+  int device = 0;
+  // resident format data
+  DevBuf d_graph, d_ts, d_gl, d_gu, d_gs, d_tl, d_tu, d_ts_samples, d_err;
+  // per-vertex outdegrees (int32, filled once at load by a decode kernel)
+  DevBuf d_deg;
+  // scratch used by the algorithms
+  DevBuf s_a, s_b, s_c, s_d, s_e, s_f, s_g, s_q0, s_q1, s_cnt, s_sum;
+  uint32_t* h_pinned = nullptr;  // small pinned readback area
+  // timing of the last call
+  cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
+  std::vector<KernelTimer> ktimers;
+  size_t ktimer_used = 0;
+  tga_timing timing{};
+  bool time_kernels = true;
+  int64_t info_edges = 0;            // total temporal edges (sum of outdegrees)
+  std::vector<int32_t> degrees;      // host copy of the outdegrees
+
+  int begin_call();                 // resets timing, records the start event
+  int end_call();                   // records the end event, syncs, checks the device error word
+  cudaEvent_t* kernel_begin();      // event pair around one decode launch (nullptr if disabled)
+  void kernel_end(cudaEvent_t* pair);
+  int check_device_error();
+  ~GraphHandle();
+};
+
+int load_graph(GraphHandle& h, const std::string& dir, const std::string& base, const tga_dataset_cfg& cfg);
+
+// Launch helpers shared by the algorithm files.
+inline unsigned grid_for(int64_t items, int block) { return (unsigned)((items + block - 1) / block); }
+
+}  // namespace tga
+
+struct tga_graph : tga::GraphHandle {};

@@ -1,0 +1,126 @@
+// Host-only C entry points of the format layer (no GPU needed).
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/tga.h"
+#include "format.hpp"
+#include "gen.hpp"
+
+namespace tga {
+int fail(int code, const std::string& msg);
+}
+
+using namespace tga;
+
+static void fill_summary(tga_gen_summary* out, int64_t n, int64_t m, int64_t maxdeg, uint64_t gb, uint64_t tb,
+                         uint64_t ib, const EncoderStats& s) {
+  if (!out) return;
+  std::memset(out, 0, sizeof *out);
+  out->n = n;
+  out->m = m;
+  out->max_degree = maxdeg;
+  out->graph_bytes = gb;
+  out->timestamp_bytes = tb;
+  out->index_bytes = ib;
+  out->copied_arcs = s.copied_arcs;
+  out->intervalised_arcs = s.intervalised_arcs;
+  out->residual_arcs = s.residual_arcs;
+  out->multiples_arcs = s.multiples_arcs;
+  out->max_chain = s.max_chain;
+}
+
+extern "C" {
+
+int tga_generate(const tga_gen_params* p, const char* dir, const char* base, const char* raw_path, tga_gen_summary* out) {
+  if (!p || !dir || !base) return fail(TGA_E_ARG, "null argument");
+  GenParams g;
+  g.n = p->n;
+  g.m = p->m;
+  g.deg_exponent = p->deg_exponent;
+  g.max_degree = p->max_degree;
+  g.repeat_frac = p->repeat_frac;
+  g.local_frac = p->local_frac;
+  g.local_radius = p->local_radius;
+  g.pref_frac = p->pref_frac;
+  g.copy_frac = p->copy_frac;
+  g.ts_kind = p->ts_kind;
+  g.ts_span = p->ts_span;
+  g.min_timestamp = p->min_timestamp;
+  g.seed = p->seed;
+  g.ref_safe = p->ref_safe != 0;
+  if (g.n > INT32_MAX || g.ts_span <= 0 || g.min_timestamp < 0 || g.min_timestamp + g.ts_span > INT32_MAX)
+    return fail(TGA_E_ARG, "vertex ids and timestamps must fit in [0, 2^31)");
+  try {
+    const GenSummary s = generate_dataset(g, dir, base, raw_path ? raw_path : "");
+    fill_summary(out, s.n, s.m, s.max_degree, s.graph_bytes, s.ts_bytes, s.index_bytes, s.stats);
+  } catch (const std::exception& e) {
+    return fail(TGA_E_IO, e.what());
+  }
+  return TGA_OK;
+}
+
+int tga_encode_raw(const char* raw_path, const char* dir, const char* base, int64_t max_label, tga_gen_summary* out) {
+  if (!raw_path || !dir || !base) return fail(TGA_E_ARG, "null argument");
+  std::vector<uint8_t> raw;
+  if (!read_file(raw_path, raw)) return fail(TGA_E_IO, std::string("Cannot open required file: ") + raw_path);
+  try {
+    const RawGraph g = parse_raw_text(std::string(raw.begin(), raw.end()));
+    const WrittenDataset w = encode_and_write(g, dir, base, max_label, EncoderParams{});
+    int64_t maxdeg = 0;
+    for (int64_t v = 0; v < g.n; ++v) maxdeg = std::max<int64_t>(maxdeg, g.src_begin[v + 1] - g.src_begin[v]);
+    fill_summary(out, w.n, w.m, maxdeg, w.graph_bytes, w.ts_bytes, w.index_bytes, w.stats);
+  } catch (const std::exception& e) {
+    return fail(TGA_E_FORMAT, e.what());
+  }
+  return TGA_OK;
+}
+
+int tga_decode_table(int32_t kind, int32_t* out) {
+  if (!out || (kind != 0 && kind != 3)) return fail(TGA_E_ARG, "kind must be 0 (gamma) or 3 (zeta_3)");
+  const std::vector<int32_t> t = table16(kind);
+  std::memcpy(out, t.data(), t.size() * sizeof(int32_t));
+  return TGA_OK;
+}
+
+int tga_encode_codes(int32_t kind, int32_t k, const uint64_t* values, int64_t n, uint8_t* out, int64_t cap,
+                     int64_t* nbits) {
+  if ((!values && n) || !nbits || n < 0) return fail(TGA_E_ARG, "null argument");
+  if (kind == 1 && k < 1) return fail(TGA_E_ARG, "zeta needs k >= 1");
+  BitWriter w;
+  for (int64_t i = 0; i < n; ++i) {
+    switch (kind) {
+      case 0: w.write_gamma(values[i]); break;
+      case 1: w.write_zeta(values[i], k); break;
+      case 2: w.write_unary(values[i]); break;
+      case 3: w.write_long(values[i], 64); break;
+      default: return fail(TGA_E_ARG, "unknown code kind");
+    }
+  }
+  *nbits = (int64_t)w.nbits;
+  if (!out) return TGA_OK;
+  if (cap < (int64_t)w.bytes.size()) return fail(TGA_E_ARG, "output buffer too small");
+  std::memcpy(out, w.bytes.data(), w.bytes.size());
+  return TGA_OK;
+}
+
+int tga_ef_encode(const uint64_t* values, int64_t n, int32_t l, uint8_t* lower, int64_t lower_cap, uint8_t* upper,
+                  int64_t upper_cap, int64_t* lower_bytes, int64_t* upper_bytes) {
+  if ((!values && n) || !lower_bytes || !upper_bytes || n < 0 || l < 0 || l > 62) return fail(TGA_E_ARG, "bad argument");
+  EFIndex ef;
+  try {
+    ef = ef_build(std::vector<uint64_t>(values, values + n), l);
+  } catch (const std::exception& e) {
+    return fail(TGA_E_ARG, e.what());
+  }
+  *lower_bytes = (int64_t)ef.lower.size();
+  *upper_bytes = (int64_t)ef.upper.size();
+  if (!lower || !upper) return TGA_OK;
+  if (lower_cap < *lower_bytes || upper_cap < *upper_bytes) return fail(TGA_E_ARG, "output buffer too small");
+  std::memcpy(lower, ef.lower.data(), ef.lower.size());
+  std::memcpy(upper, ef.upper.data(), ef.upper.size());
+  return TGA_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,226 @@
+/*
+ * tga.h - C ABI of the B200 engine for temporal-graph analytics on the compressed
+ * WebGraph/ChronoGraph-style format of Yukun-Cui/CompressTemporalGraph.
+ *
+ * The reference has no library: every workload is a standalone CUDA executable per dataset
+ * (gpu_cuda/<DS>/<alg>.cu -> gpu_cuda/shared/<alg>.cu main()) configured by compile-time
+ * macros (gpu_cuda/shared/dataset_config_base.cuh:1-67).  Each entry point below replaces one
+ * of those main() bodies, or the host loader they share; the comment on each one names the
+ * reference lines it stands in for.  All pointers are host pointers unless stated otherwise,
+ * every result buffer is owned by the caller, the graph handle owns all device memory, and a
+ * handle must not be used from two threads at once.  Every function returns a tga_status and
+ * leaves a message in tga_last_error() (per thread) when it fails; nothing calls exit().
+ */
+#ifndef TGA_H
+#define TGA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  TGA_OK = 0,
+  TGA_E_IO = 1,        /* missing / unreadable file (reference: tgaOpenFile -> exit, shared/path_config.cuh:26-36) */
+  TGA_E_FORMAT = 2,    /* malformed or inconsistent files, unsupported format parameters */
+  TGA_E_OOM = 3,       /* device allocation failed or the admission budget is exceeded */
+  TGA_E_DECODE = 4,    /* device decode error (cursor past a stream, id out of range, chain too deep) */
+  TGA_E_TIMEOUT = 5,   /* an iteration cap or a bounded wait ran out */
+  TGA_E_ARG = 6,       /* invalid argument */
+  TGA_E_CUDA = 7,      /* CUDA runtime error (reference: CHECK -> exit(1), shared/bfs.cu:23-32) */
+  TGA_E_AGAIN = 8      /* served form: request not finished yet */
+} tga_status;
+
+/* Runtime form of the per-dataset macros of shared/dataset_config_base.cuh:11-45 and
+ * gpu_cuda/<DS>/dataset_config.cuh (same names, same defaults). */
+typedef struct {
+  const char* name;               /* DATASET_NAME */
+  const char* storage_name;       /* DATASET_STORAGE_NAME (NULL -> name) */
+  int32_t max_label;              /* MAX_LABEL: largest vertex id processed */
+  int32_t max_vertex;             /* MAX_Vertex: length of per-vertex result arrays */
+  int64_t min_timestamp;          /* minTimestamp; TGA_UNSET_TS -> taken from the .timestamps header */
+  int32_t min_graph_vertex;       /* MIN_GRAPH_VERTEX (diagnostics only) */
+  int32_t active_vertex_begin;    /* ACTIVE_VERTEX_BEGIN */
+  int32_t bfs_start_vertex;       /* BFS_START_VERTEX (default 1) */
+  int32_t cc_vertex_begin;        /* CONNECTED_COMPONENTS_VERTEX_BEGIN (default 1) */
+  int32_t multiple_initial_value; /* MULTIPLE_INITIAL_VALUE; accepted for compatibility, the
+                                     decoder needs no multiples sentinel */
+  int32_t pr_iters;               /* PAGERANK_ITERATIONS (default 10) */
+  int32_t hits_iters;             /* HITS_ITERATIONS (default 10) */
+} tga_dataset_cfg;
+
+#define TGA_UNSET_TS ((int64_t)INT64_MIN)
+#define TGA_T_MIN ((int64_t)0)
+#define TGA_T_MAX ((int64_t)INT64_MAX)
+
+typedef struct tga_graph tga_graph;
+
+typedef struct {
+  int32_t n;                      /* vertices in the files */
+  int32_t max_label, max_vertex, active_vertex_begin;
+  int64_t min_timestamp;          /* from the .timestamps header */
+  uint64_t graph_bytes, timestamp_bytes, index_bytes;   /* bytes of .graph, .timestamps, 4 EF files */
+  uint64_t device_bytes;          /* device memory held by the handle */
+  int32_t graph_ef_low_bits, timestamp_ef_low_bits;
+} tga_info;
+
+/* Device-timed figures of the last algorithm call on a handle (CUDA events on its stream). */
+typedef struct {
+  double total_ms;                /* whole call, device side */
+  double decode_ms;               /* sum over the launches of the fused decode kernels */
+  int64_t decode_launches;
+  int64_t edges_decoded;          /* temporal edges decoded (multi-edges included, all passes) */
+  uint64_t compressed_bytes;      /* algorithmic bytes: stream + index bytes of the lists decoded */
+  int32_t iterations;             /* levels / rounds / iterations executed */
+  int64_t launches;               /* kernels of this library launched by the call */
+} tga_timing;
+
+/* Fills *cfg with the defaults of shared/dataset_config_base.cuh. */
+void tga_cfg_default(tga_dataset_cfg* cfg);
+
+/* Last error message of the calling thread ("" if none). */
+const char* tga_last_error(void);
+
+/* Replaces the loader part of every gpu_cuda/shared/<alg>.cu main() (bfs.cu:1694-1935): reads
+ * <root>/data/compressed/<STORAGE>/<STORAGE>.{graph,timestamps}, graph_{lower,upper}_bits.bin
+ * and timestamp_{lower,upper}_bits.bin (dataset_config_base.cuh:46-67).  root NULL or "" ->
+ * $TGA_COMPRESS_ROOT, else "../.." (path_config.cuh:10-24, dataset_config_base.cuh:39-41).
+ * The select structure of the EF index is built here (bfs.cu:1643-1654 builds it with one
+ * device thread); the decode tables are not needed. */
+int tga_open(const char* root, const tga_dataset_cfg* cfg, tga_graph** out);
+
+/* Same as tga_open for files <dir>/<basename>.* and the four EF files in <dir>. */
+int tga_open_dir(const char* dir, const char* basename, const tga_dataset_cfg* cfg, tga_graph** out);
+
+int tga_close(tga_graph* g);
+int tga_get_info(tga_graph* g, tga_info* out);
+int tga_get_timing(tga_graph* g, tga_timing* out);
+/* cudaStream_t of the handle, as an opaque pointer (all work of the handle runs on it). */
+void* tga_stream(tga_graph* g);
+
+/* Neighbour access / "RA" (neighbor_access.cu:1438-1642, main 1909-1930): decodes every list of
+ * [active_vertex_begin, max_label) with its timestamps.  small_out[v] = outdegree(v) < 4 (the
+ * reference's dv2), checksum_out[v] = order-sensitive hash of v's (successor, timestamp)
+ * sequence, degree_out[v] = outdegree.  Any output may be NULL (then it stays on the device). */
+int tga_neighbor_access(tga_graph* g, uint8_t* small_out, uint64_t* checksum_out, int32_t* degree_out);
+
+/* Successors and timestamps of one vertex in list order (EvolvingMultiGraph.successors,
+ * EvolvingMultiGraph.java:391-443).  Writes min(count, cap) entries; *count = outdegree. */
+int tga_neighbors(tga_graph* g, int32_t v, int32_t* dst, int64_t* ts, int32_t cap, int32_t* count);
+
+/* Whole graph as CSR: offsets[n+1], dst[m], ts[m] (cap = capacity of dst/ts). */
+int tga_decode_all(tga_graph* g, int64_t* offsets, int32_t* dst, int64_t* ts, int64_t cap);
+
+/* Temporal BFS (bfs.cu:1218-1692, host loop 1999-2038).  Edge (x->y,t) with t in [t_lo, t_hi)
+ * relaxes y when arrival(x) <= t; only the first in-window occurrence of consecutive equal
+ * successors counts.  arrival_out[v] = earliest arrival (INT32_MAX unreached, source = max(t_lo,0));
+ * hops_out[v] = least hop count among the earliest arrivals (the deterministic form of the
+ * reference's racy d_Ca level).  src < 0 -> bfs_start_vertex. */
+int tga_bfs(tga_graph* g, int32_t src, int64_t t_lo, int64_t t_hi, int32_t* arrival_out, int32_t* hops_out);
+
+/* Connected components by temporal reach (connected_components.cu:1210-1233,1679-1776, seed loop
+ * 2091-2149): seeds ascend from cc_vertex_begin below max_label, need outdegree > 9 and must be
+ * unreached; every vertex a seed reaches gets that seed's component number (last seed wins).
+ * flags & 1: apply the reference's early exits (stop once > 0.8*max_label vertices were reached,
+ * or after more than 50 consecutive components smaller than 5) on exact reach counts.
+ * label_out[v] = -1 when never reached. */
+#define TGA_CC_EARLY_EXIT 1
+int tga_cc(tga_graph* g, int64_t t_lo, int64_t t_hi, int32_t flags, int32_t* label_out, int32_t* components_out);
+
+/* Temporal PageRank (pagerank.cu:1221-1660, loop 1956-2007) in FP32: rank starts at 1/max_vertex;
+ * each iteration new[u] = (1-d)/max_label, then every source x in [active, max_label) adds
+ * d*R[x]*(1-exp(-alpha*t))/deg(x) to each deduplicated in-window successor, then new is divided
+ * by its sum.  deg(x) = in-window outdegree (= outdegree without a window).  iters <= 0 ->
+ * pr_iters of the configuration; alpha is TEMPORAL_ALPHA (0.1 in the reference). */
+int tga_pagerank(tga_graph* g, int32_t iters, float damping, float alpha, int64_t t_lo, int64_t t_hi, float* rank_out);
+
+/* HITS (hits.cu:1428-1987, loop 2284-2349) in FP32.  mode 0 = reference GPU semantics (hub and
+ * authority accumulate without reset, L2-normalised each half step); mode 1 = Java semantics
+ * (reset before each half step, BaselineRunner.java:493-549). */
+#define TGA_HITS_GPU 0
+#define TGA_HITS_JAVA 1
+int tga_hits(tga_graph* g, int32_t iters, int32_t mode, int64_t t_lo, int64_t t_hi, float* hub_out, float* auth_out);
+
+/* Windowed degree centrality with Java semantics (BaselineRunner.java:316-346; the GPU version
+ * is degree_centrality.cu:1211-1680): for x in [active, max_label] count out-edges to active
+ * successors with t_start <= t <= t_end ((0,0) = all edges), keep the running integer mean
+ * time, and when t_start != t_end replace the count by (int)(0.85*c + 0.15*c*(avg-start)/(end-start) + 1). */
+int tga_degree(tga_graph* g, int64_t t_start, int64_t t_end, int32_t* degree_out, int64_t* avg_out);
+
+/* Jones-Plassmann greedy colouring (graph_coloring.cu:1475-1734): round c colours every worklist
+ * vertex that has no deduplicated out-neighbour with higher (priority, lower id) still
+ * uncoloured at the start of the round; at most 512 rounds.
+ * prio_mode 0 = cuRAND XORWOW curand_init(123, v, 0), curand() % 256 (the reference's
+ *               initialize_randlist, graph_coloring.cu:1624-1632, generated by cuRAND on device);
+ *           1 = java.util.Random(123).nextInt(256) per vertex (BaselineRunner.java:392-396);
+ *           2 = caller-provided prio_in[max_vertex].
+ * flags & 1 = Java semantics for vertices without out-edges (coloured in round 0; the reference
+ * GPU never colours them).  color_out[v] = round, UINT32_MAX if uncoloured.  prio_out optional. */
+#define TGA_GC_JAVA_ISOLATED 1
+int tga_color(tga_graph* g, int32_t prio_mode, const uint32_t* prio_in, int32_t flags, uint32_t* color_out,
+              uint32_t* prio_out, int32_t* rounds_out);
+
+/* ---- batched form ---------------------------------------------------------------------------
+ * Many temporal BFS queries in one traversal: sources are packed 64 per 64-bit word of a
+ * bitmask frontier, each with its own window [t_lo[i], t_hi[i]).  arrival_out is nsrc x max_vertex
+ * (row i = query i), same semantics as tga_bfs; hops are not produced. */
+int tga_bfs_batch(tga_graph* g, int32_t nsrc, const int32_t* src, const int64_t* t_lo, const int64_t* t_hi,
+                  int32_t* arrival_out);
+
+/* Many windowed PageRanks as one strided vector (rank_out is nq x max_vertex, row i = query i). */
+int tga_pagerank_batch(tga_graph* g, int32_t nq, int32_t iters, float damping, float alpha, const int64_t* t_lo,
+                       const int64_t* t_hi, float* rank_out);
+
+/* ---- format layer (host only, no GPU needed) ----------------------------------------------- */
+
+typedef struct {
+  int64_t n, m;
+  double deg_exponent;
+  int64_t max_degree;
+  double repeat_frac, local_frac;
+  int32_t local_radius;
+  double pref_frac, copy_frac;
+  int32_t ts_kind;                /* 0 uniform, 1 Poisson process, 2 bursty */
+  int64_t ts_span, min_timestamp;
+  uint64_t seed;
+  int32_t ref_safe;               /* no in-edges to vertex 0 and n-1 */
+} tga_gen_params;
+
+typedef struct {
+  int64_t n, m, max_degree;
+  uint64_t graph_bytes, timestamp_bytes, index_bytes;
+  int64_t copied_arcs, intervalised_arcs, residual_arcs, multiples_arcs, max_chain;
+} tga_gen_summary;
+
+/* Seeded synthetic dataset written in the reference layout under dir (base.* plus the 4 EF
+ * files); raw_path (optional) receives the 4-column text edge list. */
+int tga_generate(const tga_gen_params* p, const char* dir, const char* base, const char* raw_path,
+                 tga_gen_summary* out);
+
+/* Compresses a 4-column raw text edge list ("src dst w ts", sources sorted) the way
+ * EvolvingMultiGraph.store does (EvolvingMultiGraph.java:147-275), plus the 4 EF index files.
+ * max_label < 0 -> n-1. */
+int tga_encode_raw(const char* raw_path, const char* dir, const char* base, int64_t max_label, tga_gen_summary* out);
+
+/* 65536-entry 16-bit look-ahead decode table, (length << 16) | value, 0 if the code does not fit;
+ * kind 0 = gamma (gpu_cuda/decode_tables/gammaInA.txt), 3 = zeta_3 (zetaInA.txt). */
+int tga_decode_table(int32_t kind, int32_t* out);
+
+/* Writes n values with one code into out (MSB-first, zero-padded), as dsiutils' OutputBitStream
+ * does for the reference encoder: kind 0 = gamma, 1 = zeta_k, 2 = unary, 3 = 64-bit fixed width
+ * (writeLong(x, 64), the .timestamps header).  *nbits = bits written; TGA_E_ARG if cap is short. */
+int tga_encode_codes(int32_t kind, int32_t k, const uint64_t* values, int64_t n, uint8_t* out, int64_t cap,
+                     int64_t* nbits);
+
+/* Elias-Fano index of a non-decreasing sequence in the GPU layout of the four *_bits.bin files
+ * (read by gpu_cuda/shared/bfs.cu:543-565).  l < 0 -> l = (int)log2(stream_bytes*8/max_label) is
+ * the caller's job; here l must be given.  Sizes are returned in *lower_bytes / *upper_bytes; a
+ * NULL buffer is a size query. */
+int tga_ef_encode(const uint64_t* values, int64_t n, int32_t l, uint8_t* lower, int64_t lower_cap, uint8_t* upper,
+                  int64_t upper_cap, int64_t* lower_bytes, int64_t* upper_bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TGA_H */

@@ -1,0 +1,209 @@
+"""GPU parity: every fused decode kernel against the CPU oracle on the same seeded datasets.
+
+Integer results (decoded lists, timestamps, checksums, arrivals, hop counts, components, degrees,
+colours) must be bit-exact.  PageRank and HITS run in FP32 on the GPU and in FP64 in the oracle;
+their tolerances are stated next to each assertion.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import compresstemporalgraph_b200 as tga
+import pyoracle
+from conftest import SHAPES
+
+pytestmark = pytest.mark.gpu
+
+T_MAX = tga.T_MAX
+
+
+class Pair:
+    def __init__(self, d, **cfg_kw):
+        n = d["summary"]["n"]
+        kw = dict(name=d["base"], max_label=n - 1, max_vertex=n)
+        kw.update(cfg_kw)
+        self.cfg = tga.DatasetConfig(**kw)
+        self.g = tga.Graph.open_dir(d["dir"], d["base"], self.cfg)
+        self.o = pyoracle.Oracle(d["dir"], d["base"], n)
+        self.d = d
+        self.n = n
+        self.ml, self.mv, self.act = self.cfg.max_label, self.cfg.max_vertex, self.cfg.active_vertex_begin
+
+
+@pytest.fixture(scope="module")
+def pairs(datasets):
+    out = {name: Pair(d) for name, d in datasets.items()}
+    # Non-default configuration: inactive low ids and result arrays longer than the id space.
+    out["small_view"] = Pair(datasets["chains"], active_vertex_begin=100, max_vertex=datasets["chains"]["summary"]["n"] + 37)
+    yield out
+    for p in out.values():
+        p.g.close()
+
+
+ALL = list(SHAPES) + ["small_view"]
+
+
+@pytest.mark.parametrize("shape", list(SHAPES))
+def test_decode_all_bit_exact(pairs, shape):
+    p = pairs[shape]
+    off, dst, ts = p.g.decode_all()
+    ooff, odst, ots = p.o.csr()
+    assert np.array_equal(off, ooff)
+    assert np.array_equal(dst, odst)
+    assert np.array_equal(ts, ots)
+
+
+@pytest.mark.parametrize("shape", ALL)
+def test_neighbor_access_checksums(pairs, shape):
+    p = pairs[shape]
+    small, csum, deg = p.g.neighbor_access()
+    end = min(p.ml, p.n)
+    osmall, ocs = p.o.checksums(p.act, end, p.mv)
+    assert np.array_equal(csum[p.act:end], ocs[p.act:end])
+    assert np.array_equal(small[p.act:end], osmall[p.act:end])
+    t = p.g.timing()
+    assert t["edges_decoded"] == int(deg[p.act:end].sum())
+
+
+@pytest.mark.parametrize("shape", ["chains", "hubs", "small"])
+def test_neighbors_single_vertex(pairs, shape):
+    p = pairs[shape]
+    off, _, _ = p.o.csr()
+    degs = np.diff(off)
+    picks = [0, int(np.argmax(degs)), p.n - 1] + list(np.random.default_rng(1).integers(0, p.n, 20))
+    for v in picks:
+        dst, ts = p.g.neighbors(int(v))
+        odst, ots = p.o.neighbors(int(v))
+        assert np.array_equal(dst, odst) and np.array_equal(ts, ots), v
+
+
+def _windows(p):
+    lo = p.d["params"].min_timestamp
+    span = p.d["params"].ts_span
+    return [(0, T_MAX), (lo + span // 4, lo + 3 * span // 4), (lo + span // 2, lo + span // 2 + span // 20)]
+
+
+@pytest.mark.parametrize("shape", ALL)
+def test_bfs_arrival_and_hops(pairs, shape):
+    p = pairs[shape]
+    off, _, _ = p.o.csr()
+    degs = np.diff(off)
+    srcs = [int(np.argmax(degs)), max(p.act, 1), p.act + 7]
+    for src in srcs:
+        for lo, hi in _windows(p):
+            arr, hops = p.g.bfs(src, lo, hi)
+            oarr, ohops = p.o.bfs(p.ml, p.mv, p.act, src, lo, hi)
+            assert np.array_equal(arr, oarr), (src, lo, hi)
+            assert np.array_equal(hops, ohops), (src, lo, hi)
+
+
+@pytest.mark.parametrize("shape", ALL)
+@pytest.mark.parametrize("early", [True, False])
+def test_connected_components(pairs, shape, early):
+    p = pairs[shape]
+    for lo, hi in _windows(p)[:2]:
+        lab, k = p.g.connected_components(lo, hi, early_exit=early)
+        olab, ok = p.o.cc(p.ml, p.mv, p.act, p.cfg.connected_components_vertex_begin, lo, hi, early)
+        assert k == ok
+        assert np.array_equal(lab, olab)
+
+
+@pytest.mark.parametrize("shape", ALL)
+@pytest.mark.parametrize("iters", [1, 20])
+def test_pagerank_fp32_vs_fp64(pairs, shape, iters):
+    p = pairs[shape]
+    for lo, hi in _windows(p)[:2]:
+        r = p.g.pagerank(iters, 0.85, 0.1, lo, hi)
+        o = p.o.pagerank(p.ml, p.mv, p.act, iters, 0.85, 0.1, lo, hi)
+        # Stated tolerance: L1 distance to the FP64 oracle <= 1e-5 of the total rank mass (1.0),
+        # and every entry within 1e-4 relative + 1e-9 absolute.
+        l1 = float(np.abs(r.astype(np.float64) - o).sum())
+        assert l1 <= 1e-5, l1
+        assert np.allclose(r, o, rtol=1e-4, atol=1e-9)
+
+
+@pytest.mark.parametrize("shape", ALL)
+@pytest.mark.parametrize("mode", [tga.HITS_GPU, tga.HITS_JAVA])
+def test_hits_fp32_vs_fp64(pairs, shape, mode):
+    p = pairs[shape]
+    iters = 10
+    for lo, hi in _windows(p)[:2]:
+        hub, auth = p.g.hits(iters, mode, lo, hi)
+        ohub, oauth = p.o.hits(p.ml, p.mv, p.act, iters, mode == tga.HITS_JAVA, lo, hi)
+        # Stated tolerance: unit-L2 vectors; L1 distance to FP64 <= 1e-4 and max error <= 1e-5.
+        for a, b in ((hub, ohub), (auth, oauth)):
+            assert float(np.abs(a.astype(np.float64) - b).sum()) <= 1e-4
+            assert float(np.abs(a.astype(np.float64) - b).max()) <= 1e-5
+
+
+@pytest.mark.parametrize("shape", ALL)
+def test_degree_centrality(pairs, shape):
+    p = pairs[shape]
+    lo = p.d["params"].min_timestamp
+    span = p.d["params"].ts_span
+    for s, e in [(0, 0), (lo + span // 3, lo + 2 * span // 3), (lo, lo)]:
+        deg, avg = p.g.degree_centrality(s, e)
+        odeg, oavg = p.o.degree(p.ml, p.mv, p.act, s, e)
+        assert np.array_equal(deg, odeg), (s, e)
+        assert np.array_equal(avg, oavg), (s, e)
+
+
+@pytest.mark.parametrize("shape", ALL)
+@pytest.mark.parametrize("java_isolated", [False, True])
+def test_coloring_curand_priorities(pairs, shape, java_isolated):
+    p = pairs[shape]
+    col, prio, rounds = p.g.color(0, java_isolated=java_isolated)
+    assert prio.max() < 256
+    ocol, orounds = p.o.color(p.ml, p.mv, p.act, prio, java_isolated)
+    assert rounds == orounds
+    assert np.array_equal(col, ocol)
+
+
+def test_coloring_java_priorities(pairs):
+    p = pairs["small"]
+    col, prio, rounds = p.g.color(1)
+    assert np.array_equal(prio, pyoracle.java_random256(123, p.mv))
+    ocol, _ = p.o.color(p.ml, p.mv, p.act, prio)
+    assert np.array_equal(col, ocol)
+
+
+def test_coloring_given_priorities(pairs):
+    p = pairs["hubs"]
+    prio = np.random.default_rng(5).integers(0, 4, p.mv).astype(np.uint32)  # many ties
+    col, pout, _ = p.g.color(2, prio)
+    assert np.array_equal(pout, prio)
+    ocol, _ = p.o.color(p.ml, p.mv, p.act, prio)
+    assert np.array_equal(col, ocol)
+
+
+def test_batched_bfs_equals_single(pairs):
+    p = pairs["chains"]
+    rng = np.random.default_rng(2)
+    srcs = rng.integers(0, p.n, 70).astype(np.int32)
+    span = p.d["params"].ts_span
+    lo = rng.integers(0, span // 2, 70)
+    hi = lo + rng.integers(span // 20, span // 2, 70)
+    out = p.g.bfs_batch(srcs, lo, hi)
+    for i in range(0, 70, 9):
+        arr, _ = p.g.bfs(int(srcs[i]), int(lo[i]), int(hi[i]))
+        assert np.array_equal(out[i], arr)
+
+
+def test_batched_pagerank_equals_single(pairs):
+    p = pairs["small"]
+    span = p.d["params"].ts_span
+    lo = np.array([0, span // 4, span // 2], np.int64)
+    hi = np.array([T_MAX, span // 2, span], np.int64)
+    out = p.g.pagerank_batch(lo, hi, iters=5)
+    for i in range(3):
+        r = p.g.pagerank(5, 0.85, 0.1, int(lo[i]), int(hi[i]))
+        assert np.allclose(out[i], r, rtol=1e-4, atol=1e-9)
+
+
+def test_timing_reports_device_time(pairs):
+    p = pairs["small"]
+    p.g.pagerank(3)
+    t = p.g.timing()
+    assert t["total_ms"] > 0 and t["decode_ms"] > 0 and t["decode_launches"] == 3
+    assert t["edges_decoded"] == 3 * p.o.m - 3 * int(np.diff(p.o.csr()[0])[p.ml:].sum())
