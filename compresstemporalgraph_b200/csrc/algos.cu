@@ -1,6 +1,10 @@
 // Fused decode + algorithm kernels and their C ABI entry points.  Every kernel decodes the
 // successor lists and timestamps it needs straight from the compressed streams; decoded edges
 // live only in registers.
+//
+// Work decomposition (slices.cuh): sweeps over all lists run one thread per work item (a run of
+// short lists or one slice of a long list); frontier kernels expand a long list into its slices
+// when they enqueue it.  Queue entries are vertex ids (>= 0) or -(slice + 1).
 #include <curand_kernel.h>
 
 #include <algorithm>
@@ -8,23 +12,29 @@
 #include <cstring>
 #include <vector>
 
-#include "decoder.cuh"
 #include "engine.hpp"
 
 namespace tga {
 
 constexpr int kBlock = 256;
-// Launches a kernel of kBlock threads on the handle's stream and counts it in the call's timing.
-#define KL(kernel, grid) ++h.timing.launches, kernel<<<(grid), kBlock, 0, h.stream>>>
 constexpr uint64_t kTpInf = ~0ull;
 constexpr uint32_t kColorInf = 0xFFFFFFFFu;
 
-// Order-sensitive hash of a successor list, also computed by the oracle.
-__host__ __device__ __forceinline__ uint64_t mix_edge(uint64_t h, int32_t y, int64_t t) {
-  const uint64_t k = ((uint64_t)(uint32_t)y * 0x9E3779B97F4A7C15ull) ^ ((uint64_t)t * 0xC2B2AE3D27D4EB4Full);
-  h ^= k;
-  h = (h << 23) | (h >> 41);
-  return h * 0x165667B19E3779F9ull;
+// Launches a kernel of kBlock threads on the handle's stream and counts it in the call's timing.
+#define KL(kernel, grid) ++h.timing.launches, kernel<<<(grid), kBlock, 0, h.stream>>>
+
+// Per-edge term of the neighbour-access checksum: the checksum of a list is the sum (mod 2^64)
+// of edge_hash over its edges, so slices can add their parts; the edge index keeps it
+// order-sensitive.  The oracle computes the same sum.
+__host__ __device__ __forceinline__ uint64_t edge_hash(uint32_t v, uint32_t i, int32_t y, int64_t t) {
+  uint64_t z = (((uint64_t)v << 32) | i) * 0x9E3779B97F4A7C15ull;
+  z ^= (uint64_t)(uint32_t)y * 0xC2B2AE3D27D4EB4Full;
+  z ^= (uint64_t)t * 0x165667B19E3779F9ull;
+  z ^= z >> 31;
+  z *= 0xBF58476D1CE4E5B9ull;
+  z ^= z >> 29;
+  z *= 0x94D049BB133111EBull;
+  return z ^ (z >> 32);
 }
 
 __device__ __forceinline__ void add_edges(unsigned long long* ctr, unsigned long long mine) {
@@ -45,39 +55,102 @@ __device__ __forceinline__ double block_sum(double v) {
   return s;  // valid in thread 0
 }
 
+struct Work {
+  const WorkItem* items;
+  const SliceState* slices;
+  const int32_t* slice_first;
+  int32_t nitems;
+};
+
+// Opens queue entry e: a whole list (e >= 0) or one slice.  Returns the vertex.
+__device__ __forceinline__ int open_entry(const GraphView& g, const Work& w, int e, EdgeCursor& c, int& count) {
+  if (e >= 0) {
+    count = c.open(g, e);
+    return e;
+  }
+  const SliceState& s = w.slices[-e - 1];
+  cursor_restore(g, c, s);
+  count = s.count;
+  return s.v;
+}
+
+// Appends y (or all slices of y) to a queue.
+__device__ __forceinline__ void enqueue(const Work& w, int y, int32_t* q, int32_t* cnt) {
+  const int a = w.slice_first[y], b = w.slice_first[y + 1];
+  if (a == b) {
+    q[atomicAdd(cnt, 1)] = y;
+  } else {
+    const int base = atomicAdd(cnt, b - a);
+    for (int j = a; j < b; ++j) q[base + j - a] = -(j + 1);
+  }
+}
+
+// Runs `body(c, v, first, count)` for work item i: every vertex of a run of short lists that
+// `want(v)`, or one slice.  Returns the edges handed to the body.
+template <class Want, class Body>
+__device__ __forceinline__ unsigned long long sweep_item(const GraphView& g, const Work& w, int i, Want want, Body body) {
+  const WorkItem it = w.items[i];
+  unsigned long long edges = 0;
+  if (it.slice >= 0) {
+    if (!want(it.v0)) return 0;
+    EdgeCursor c;
+    const SliceState& s = w.slices[it.slice];
+    cursor_restore(g, c, s);
+    edges = (unsigned long long)s.count;
+    body(c, it.v0, s.first, s.count);
+  } else {
+    for (int v = it.v0; v < it.v1; ++v) {
+      if (!want(v)) continue;
+      EdgeCursor c;
+      const int d = c.open(g, v);
+      edges += (unsigned long long)d;
+      body(c, v, 0, d);
+    }
+  }
+  return edges;
+}
+
 // ---------------------------------------------------------------------------------------------
 // Neighbour access and raw decode
 
-__global__ void __launch_bounds__(kBlock) k_neighbor_access(GraphView g, int32_t begin, int32_t end, uint8_t* small,
-                                                            uint64_t* csum, unsigned long long* edges) {
-  const int x = begin + blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(kBlock) k_neighbor_access(GraphView g, Work w, int32_t begin, int32_t end,
+                                                            unsigned long long* csum, unsigned long long* edges) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long mine = 0;
-  if (x < end) {
-    EdgeCursor c;
-    const int d = c.open(g, x);
-    small[x] = d < 4;
-    uint64_t h = 0x27D4EB2F165667C5ull ^ (uint64_t)(uint32_t)x;
-    int y;
-    int64_t t;
-    while (c.next(g, y, t)) h = mix_edge(h, y, t);
-    csum[x] = h;
-    mine = (unsigned long long)d;
+  if (i < w.nitems) {
+    mine = sweep_item(
+        g, w, i, [&](int v) { return v >= begin && v < end; },
+        [&](EdgeCursor& c, int v, int first, int) {
+          uint64_t h = 0;
+          uint32_t k = (uint32_t)first;
+          int y;
+          int64_t t;
+          while (c.next(g, y, t)) h += edge_hash((uint32_t)v, k++, y, t);
+          atomicAdd(&csum[v], (unsigned long long)h);
+        });
   }
   add_edges(edges, mine);
 }
 
-__global__ void k_decode_csr(GraphView g, int32_t count, const int64_t* off, int32_t* dst, int64_t* ts, int64_t cap) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  if (x >= count) return;
-  EdgeCursor c;
-  c.open(g, x);
-  int64_t o = off[x];
-  int y;
-  int64_t t;
-  while (c.next(g, y, t)) {
-    if (o < cap) { dst[o] = y; ts[o] = t; }
-    ++o;
-  }
+__global__ void k_small_flags(const int32_t* deg, uint8_t* small, int32_t begin, int32_t end) {
+  const int v = begin + blockIdx.x * blockDim.x + threadIdx.x;
+  if (v < end) small[v] = deg[v] < 4;
+}
+
+__global__ void k_decode_csr(GraphView g, Work w, const int64_t* off, int32_t* dst, int64_t* ts, int64_t cap) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= w.nitems) return;
+  sweep_item(
+      g, w, i, [&](int) { return true; },
+      [&](EdgeCursor& c, int v, int first, int) {
+        int64_t o = off[v] + first;
+        int y;
+        int64_t t;
+        while (c.next(g, y, t)) {
+          if (o < cap) { dst[o] = y; ts[o] = t; }
+          ++o;
+        }
+      });
 }
 
 __global__ void k_neighbors(GraphView g, int32_t v, int32_t* dst, int64_t* ts, int32_t cap, int32_t* count) {
@@ -93,45 +166,78 @@ __global__ void k_neighbors(GraphView g, int32_t v, int32_t* dst, int64_t* ts, i
 }
 
 // ---------------------------------------------------------------------------------------------
-// Temporal BFS (label-correcting, packed (arrival << 32 | hops) relaxation)
+// Temporal BFS: phase 1 earliest arrival (label-correcting minimum), phase 2 hop levels.
 
 struct BfsArgs {
   const int32_t* q;
   int32_t* nq;
   int32_t* ncnt;
-  uint64_t* tp;
-  uint32_t* stamp;
+  uint64_t* tp;          // arrival << 32 per vertex (all ones = unreached)
+  uint32_t* stamp;       // last wave in which the vertex was enqueued
   uint32_t wave;
   int64_t lo, hi;
-  int32_t* touched;     // optional: vertices whose arrival became finite (CC)
+  int32_t* touched;      // optional: vertices whose arrival became finite (CC)
   int32_t* tcnt;
   unsigned long long* edges;
 };
 
-__global__ void __launch_bounds__(kBlock) k_bfs_level(GraphView g, BfsArgs a, int32_t qn) {
+// Edge filter shared by every traversal: in-window, first of equal consecutive successors,
+// successor inside [active_begin, max_vertex).
+#define TGA_EDGE_FILTER(g, lo, hi, y, t, prev_y)                          \
+  if ((t) < (lo) || (t) >= (hi)) continue;                                \
+  if ((y) == (prev_y)) continue;                                          \
+  (prev_y) = (y);                                                         \
+  if ((y) < (g).active_begin || (y) >= (g).max_vertex) continue;
+
+// Phase 1: tp[v] holds arrival << 32, so the 64-bit atomicMin is an arrival minimum; a vertex
+// whose arrival drops is enqueued once per level (stamp) and relaxes its successors again.
+__global__ void __launch_bounds__(kBlock) k_bfs_level(GraphView g, Work w, BfsArgs a, int32_t qn) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long mine = 0;
   if (i < qn) {
-    const int x = a.q[i];
+    EdgeCursor c;
+    int cnt;
+    const int x = open_entry(g, w, a.q[i], c, cnt);
     if (x >= g.active_begin && x <= g.max_label) {
-      const uint64_t wx = a.tp[x];
-      const uint32_t ax = (uint32_t)(wx >> 32), hx = (uint32_t)wx;
-      EdgeCursor c;
-      mine = (unsigned long long)c.open(g, x);
+      const uint32_t ax = (uint32_t)(a.tp[x] >> 32);
+      mine = (unsigned long long)cnt;
       int y, prev_y = -1;
       int64_t t;
       while (c.next(g, y, t)) {
-        if (t < a.lo || t >= a.hi) continue;
-        if (y == prev_y) continue;
-        prev_y = y;
-        if (y < g.active_begin || y >= g.max_vertex) continue;
+        TGA_EDGE_FILTER(g, a.lo, a.hi, y, t, prev_y)
         if ((int64_t)ax > t || t >= 0xFFFFFFFFll) continue;
-        const uint64_t nv = ((uint64_t)t << 32) | (uint64_t)(hx + 1);
+        const uint64_t nv = (uint64_t)t << 32;
         const uint64_t old = atomicMin((unsigned long long*)&a.tp[y], (unsigned long long)nv);
         if (nv < old) {
           if (a.touched && (old >> 32) == 0xFFFFFFFFull) a.touched[atomicAdd(a.tcnt, 1)] = y;
-          if (atomicMax(&a.stamp[y], a.wave) < a.wave) a.nq[atomicAdd(a.ncnt, 1)] = y;
+          if (atomicMax(&a.stamp[y], a.wave) < a.wave) enqueue(w, y, a.nq, a.ncnt);
         }
+      }
+    }
+  }
+  add_edges(a.edges, mine);
+}
+
+// Phase 2: with the final arrivals fixed, an edge passing the same filters is tight when
+// arrival(x) <= t == arrival(y); hops = BFS level over tight edges, each vertex claimed once.
+__global__ void __launch_bounds__(kBlock) k_bfs_hops(GraphView g, Work w, BfsArgs a, int32_t qn, uint32_t* hops,
+                                                     uint32_t level) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long mine = 0;
+  if (i < qn) {
+    EdgeCursor c;
+    int cnt;
+    const int x = open_entry(g, w, a.q[i], c, cnt);
+    if (x >= g.active_begin && x <= g.max_label) {
+      const uint32_t ax = (uint32_t)(a.tp[x] >> 32);
+      mine = (unsigned long long)cnt;
+      int y, prev_y = -1;
+      int64_t t;
+      while (c.next(g, y, t)) {
+        TGA_EDGE_FILTER(g, a.lo, a.hi, y, t, prev_y)
+        if ((int64_t)ax > t || t >= 0xFFFFFFFFll) continue;
+        if ((int64_t)(a.tp[y] >> 32) != t) continue;
+        if (atomicCAS(&hops[y], 0xFFFFFFFFu, level + 1) == 0xFFFFFFFFu) enqueue(w, y, a.nq, a.ncnt);
       }
     }
   }
@@ -151,29 +257,45 @@ __global__ void k_fill_i32(int32_t* p, int32_t v, int64_t n) {
   if (i < n) p[i] = v;
 }
 
-__global__ void k_unpack_tp(const uint64_t* tp, int32_t* arr, int32_t* hops, int32_t n) {
+__global__ void k_unpack_bfs(const uint64_t* tp, const uint32_t* hops_in, int32_t* arr, int32_t* hops, int32_t n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const uint64_t w = tp[i];
-  const bool inf = (w >> 32) == 0xFFFFFFFFull;
-  arr[i] = inf ? INT32_MAX : (int32_t)(w >> 32);
-  hops[i] = inf ? INT32_MAX : (int32_t)(uint32_t)w;
+  const uint64_t wd = tp[i];
+  const bool inf = (wd >> 32) == 0xFFFFFFFFull;
+  arr[i] = inf ? INT32_MAX : (int32_t)(wd >> 32);
+  const uint32_t hv = hops_in[i];
+  hops[i] = (inf || hv == 0xFFFFFFFFu) ? INT32_MAX : (int32_t)hv;
 }
 
-// Runs the level loop from an initialised frontier; returns levels executed or <0 on error.
+// Host side: the queue entries of one vertex (itself or its slices).
+static int32_t seed_entries(const GraphHandle& h, int32_t v, std::vector<int32_t>& out) {
+  out.clear();
+  const int32_t a = h.slice_first_host[(size_t)v], b = h.slice_first_host[(size_t)v + 1];
+  if (a == b) out.push_back(v);
+  else
+    for (int32_t j = a; j < b; ++j) out.push_back(-(j + 1));
+  return (int32_t)out.size();
+}
+
+static Work work_of(const GraphHandle& h) {
+  return Work{h.d_items.as<WorkItem>(), h.d_slices.as<SliceState>(), h.d_slice_first.as<int32_t>(), h.nitems};
+}
+
+// Level loop of phase 1 from an initialised queue of qn entries; returns the levels executed.
 static int run_bfs_levels(GraphHandle& h, BfsArgs a, DevBuf& q0, DevBuf& q1, int32_t qn, uint32_t& wave, int& rc) {
   int levels = 0;
   DevBuf* cur = &q0;
   DevBuf* nxt = &q1;
+  const Work w = work_of(h);
   rc = TGA_OK;
   while (qn > 0) {
-    if (levels > 1 << 22) { rc = fail(TGA_E_TIMEOUT, "BFS level cap reached"); return levels; }
+    if (levels > (1 << 22)) { rc = fail(TGA_E_TIMEOUT, "BFS level cap reached"); return levels; }
     a.q = cur->as<int32_t>();
     a.nq = nxt->as<int32_t>();
     a.wave = ++wave;
     cudaMemsetAsync(a.ncnt, 0, sizeof(int32_t), h.stream);
     cudaEvent_t* ev = h.kernel_begin();
-    KL(k_bfs_level, grid_for(qn, kBlock))(h.view, a, qn);
+    KL(k_bfs_level, grid_for(qn, kBlock))(h.view, w, a, qn);
     h.kernel_end(ev);
     cudaMemcpyAsync(h.h_pinned, a.ncnt, sizeof(int32_t), cudaMemcpyDeviceToHost, h.stream);
     if (cudaStreamSynchronize(h.stream) != cudaSuccess) { rc = fail(TGA_E_CUDA, "BFS level failed"); return levels; }
@@ -186,9 +308,10 @@ static int run_bfs_levels(GraphHandle& h, BfsArgs a, DevBuf& q0, DevBuf& q1, int
 
 static int bfs_buffers(GraphHandle& h) {
   const size_t nv = (size_t)h.view.max_vertex;
+  const size_t qcap = nv + (size_t)h.nslices + 1;
   int rc;
-  if ((rc = h.s_a.ensure(nv * 8)) || (rc = h.s_b.ensure(nv * 4)) || (rc = h.s_q0.ensure(nv * 4)) ||
-      (rc = h.s_q1.ensure(nv * 4)) || (rc = h.s_cnt.ensure(64)) || (rc = h.s_c.ensure(nv * 4)))
+  if ((rc = h.s_a.ensure(nv * 8)) || (rc = h.s_b.ensure(nv * 4)) || (rc = h.s_q0.ensure(qcap * 4)) ||
+      (rc = h.s_q1.ensure(qcap * 4)) || (rc = h.s_cnt.ensure(64)) || (rc = h.s_c.ensure(nv * 4)))
     return rc;
   return TGA_OK;
 }
@@ -219,13 +342,16 @@ __global__ void k_cc_find_seed(const uint8_t* reached, const int32_t* deg, int32
 }
 
 // ---------------------------------------------------------------------------------------------
-// PageRank
+// PageRank: one launch per iteration.  Three rank buffers rotate: iteration k reads IN (the
+// unnormalised result of k-1, scaled by 1/sum[k-1]), scatters into OUT (already set to the base
+// value) and resets RESET (read by iteration k-1, written by k+1) to the base value.
 
 struct PrArgs {
   const float* invdeg;   // per-vertex 1/deg for a window, or nullptr (use outdegree)
   const int32_t* deg;
-  float* in;
+  const float* in;
   float* out;
+  float* reset;
   double* sums;
   int32_t k;
   float damping, alpha, base;
@@ -233,34 +359,37 @@ struct PrArgs {
   unsigned long long* edges;
 };
 
-__global__ void __launch_bounds__(kBlock) k_pr_iter(GraphView g, PrArgs a) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+// 1 - exp(-alpha t): for alpha*t > 18 expf is below 2^-25 and the difference rounds to 1.0f.
+__device__ __forceinline__ float temporal_weight(float alpha, int64_t t) {
+  const float a = alpha * (float)t;
+  return a > 18.0f ? 1.0f : 1.0f - expf(-a);
+}
+
+__global__ void __launch_bounds__(kBlock) k_pr_iter(GraphView g, Work w, PrArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  for (int x = i; x < g.max_vertex; x += gridDim.x * blockDim.x) a.reset[x] = a.base;
   double local = 0;
   unsigned long long mine = 0;
-  if (x < g.max_vertex) {
+  if (i < w.nitems) {
     const double s = a.k == 0 ? 1.0 : 1.0 / a.sums[a.k - 1];
-    const float r = (float)((double)a.in[x] * s);
-    a.in[x] = a.base;
-    if (x >= g.active_begin && x < g.max_label) {
-      const int d = a.deg[x];
-      const float inv = a.invdeg ? a.invdeg[x] : (d > 0 ? 1.0f / (float)d : 0.0f);
-      if (d > 0 && inv > 0.0f) {
-        const float c0 = a.damping * r * inv;
-        EdgeCursor c;
-        mine = (unsigned long long)c.open(g, x);
-        int y, prev_y = -1;
-        int64_t t;
-        while (c.next(g, y, t)) {
-          if (t < a.lo || t >= a.hi) continue;
-          if (y == prev_y) continue;
-          prev_y = y;
-          if (y < g.active_begin || y >= g.max_vertex) continue;
-          const float contrib = c0 * (1.0f - expf(-a.alpha * (float)t));
-          atomicAdd(&a.out[y], contrib);
-          local += contrib;
-        }
-      }
-    }
+    mine = sweep_item(
+        g, w, i,
+        [&](int v) {
+          if (v < g.active_begin || v >= g.max_label) return false;
+          return a.invdeg ? a.invdeg[v] > 0.0f : a.deg[v] > 0;
+        },
+        [&](EdgeCursor& c, int v, int, int) {
+          const float inv = a.invdeg ? a.invdeg[v] : 1.0f / (float)a.deg[v];
+          const float c0 = a.damping * (float)((double)a.in[v] * s) * inv;
+          int y, prev_y = -1;
+          int64_t t;
+          while (c.next(g, y, t)) {
+            TGA_EDGE_FILTER(g, a.lo, a.hi, y, t, prev_y)
+            const float contrib = c0 * temporal_weight(a.alpha, t);
+            atomicAdd(&a.out[y], contrib);
+            local += contrib;
+          }
+        });
   }
   add_edges(a.edges, mine);
   const double bs = block_sum(local);
@@ -277,93 +406,83 @@ __global__ void k_pr_final(const float* buf, const double* sums, int k, float* o
   if (i < n) out[i] = (float)((double)buf[i] / sums[k]);
 }
 
-// In-window outdegree of each source (timestamps only need decoding, ids come along).
-__global__ void __launch_bounds__(kBlock) k_window_invdeg(GraphView g, int64_t lo, int64_t hi, float* invdeg,
-                                                          unsigned long long* edges) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+// In-window outdegree of each source, counted over items, then inverted.
+__global__ void __launch_bounds__(kBlock) k_window_count(GraphView g, Work w, int64_t lo, int64_t hi, int32_t* cnt,
+                                                         unsigned long long* edges) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long mine = 0;
-  if (x < g.max_vertex) {
-    int cnt = 0;
-    if (x >= g.active_begin && x < g.max_label) {
-      EdgeCursor c;
-      mine = (unsigned long long)c.open(g, x);
-      int y;
-      int64_t t;
-      while (c.next(g, y, t)) cnt += (t >= lo && t < hi);
-    }
-    invdeg[x] = cnt ? 1.0f / (float)cnt : 0.0f;
+  if (i < w.nitems) {
+    mine = sweep_item(
+        g, w, i, [&](int v) { return v >= g.active_begin && v < g.max_label; },
+        [&](EdgeCursor& c, int v, int, int) {
+          int k = 0, y;
+          int64_t t;
+          while (c.next(g, y, t)) k += (t >= lo && t < hi);
+          if (k) atomicAdd(&cnt[v], k);
+        });
   }
   add_edges(edges, mine);
 }
 
-// ---------------------------------------------------------------------------------------------
-// HITS
-
-struct HitsArgs {
-  float* hub;
-  const float* auth_in;   // current authority, not yet normalised
-  float* auth_next;       // receives the base of the next authority, then the scatter
-  double* hsum;           // sum of hub^2 of this iteration (accumulated by the hub kernel)
-  const double* aprev;    // sum of auth^2 of the previous iteration (nullptr: scale 1)
-  int java;
-  int64_t lo, hi;
-  unsigned long long* edges;
-};
-
-__global__ void __launch_bounds__(kBlock) k_hits_hub(GraphView g, HitsArgs a) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  double local = 0;
-  unsigned long long mine = 0;
-  if (x < g.max_vertex) {
-    const double sa = (a.aprev && *a.aprev > 0) ? 1.0 / sqrt(*a.aprev) : 1.0;
-    const float sf = (float)sa;
-    float h = a.java ? 0.0f : a.hub[x];
-    if (x >= g.active_begin && x < g.max_label) {
-      EdgeCursor c;
-      mine = (unsigned long long)c.open(g, x);
-      int y, prev_y = -1;
-      int64_t t;
-      float acc = 0.0f;
-      while (c.next(g, y, t)) {
-        if (t < a.lo || t >= a.hi) continue;
-        if (y == prev_y) continue;
-        prev_y = y;
-        if (y < g.active_begin || y >= g.max_vertex) continue;
-        acc += a.auth_in[y];
-      }
-      h += acc * sf;
-    }
-    a.hub[x] = h;
-    a.auth_next[x] = a.java ? 0.0f : a.auth_in[x] * sf;
-    local = (double)h * (double)h;
-  }
-  add_edges(a.edges, mine);
-  const double bs = block_sum(local);
-  if (threadIdx.x == 0 && bs != 0.0) atomicAdd(a.hsum, bs);
+__global__ void k_invert(const int32_t* cnt, float* inv, int32_t n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) inv[i] = cnt[i] ? 1.0f / (float)cnt[i] : 0.0f;
 }
 
-__global__ void __launch_bounds__(kBlock) k_hits_auth(GraphView g, HitsArgs a) {
+// ---------------------------------------------------------------------------------------------
+// HITS.  Per iteration: hub base (vector), hub gather (items), sum hub^2, authority scatter
+// (items), normalise hub, sum auth^2.  Authorities are kept unnormalised between iterations
+// and scaled by 1/||auth|| when read.
+
+__global__ void k_hits_base(float* hub, const float* auth_in, float* auth_next, const double* aprev, int java, int32_t n) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= n) return;
+  const float sa = (aprev && *aprev > 0) ? (float)(1.0 / sqrt(*aprev)) : 1.0f;
+  if (java) hub[x] = 0.0f;
+  auth_next[x] = java ? 0.0f : auth_in[x] * sa;
+}
+
+__global__ void __launch_bounds__(kBlock) k_hits_hub(GraphView g, Work w, float* hub, const float* auth_in,
+                                                     const double* aprev, int64_t lo, int64_t hi, unsigned long long* edges) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long mine = 0;
-  if (x < g.max_vertex) {
-    const double sh = *a.hsum > 0 ? 1.0 / sqrt(*a.hsum) : 1.0;
-    const float hn = (float)((double)a.hub[x] * sh);
-    a.hub[x] = hn;
-    if (x >= g.active_begin && x < g.max_label && hn != 0.0f) {
-      EdgeCursor c;
-      mine = (unsigned long long)c.open(g, x);
-      int y, prev_y = -1;
-      int64_t t;
-      while (c.next(g, y, t)) {
-        if (t < a.lo || t >= a.hi) continue;
-        if (y == prev_y) continue;
-        prev_y = y;
-        if (y < g.active_begin || y >= g.max_vertex) continue;
-        atomicAdd(&a.auth_next[y], hn);
-      }
-    }
+  if (i < w.nitems) {
+    const float sa = (aprev && *aprev > 0) ? (float)(1.0 / sqrt(*aprev)) : 1.0f;
+    mine = sweep_item(
+        g, w, i, [&](int v) { return v >= g.active_begin && v < g.max_label; },
+        [&](EdgeCursor& c, int v, int, int) {
+          float acc = 0.0f;
+          int y, prev_y = -1;
+          int64_t t;
+          while (c.next(g, y, t)) {
+            TGA_EDGE_FILTER(g, lo, hi, y, t, prev_y)
+            acc += auth_in[y];
+          }
+          if (acc != 0.0f) atomicAdd(&hub[v], acc * sa);
+        });
   }
-  add_edges(a.edges, mine);
+  add_edges(edges, mine);
+}
+
+__global__ void __launch_bounds__(kBlock) k_hits_auth(GraphView g, Work w, const float* hub, const double* hsum,
+                                                      float* auth_next, int64_t lo, int64_t hi, unsigned long long* edges) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long mine = 0;
+  if (i < w.nitems) {
+    const float sh = *hsum > 0 ? (float)(1.0 / sqrt(*hsum)) : 1.0f;
+    mine = sweep_item(
+        g, w, i, [&](int v) { return v >= g.active_begin && v < g.max_label && hub[v] != 0.0f; },
+        [&](EdgeCursor& c, int v, int, int) {
+          const float hn = hub[v] * sh;
+          int y, prev_y = -1;
+          int64_t t;
+          while (c.next(g, y, t)) {
+            TGA_EDGE_FILTER(g, lo, hi, y, t, prev_y)
+            atomicAdd(&auth_next[y], hn);
+          }
+        });
+  }
+  add_edges(edges, mine);
 }
 
 __global__ void k_sumsq(const float* v, int32_t n, double* out) {
@@ -381,20 +500,25 @@ __global__ void k_scale(const float* v, const double* sumsq, float* out, int32_t
 }
 
 // ---------------------------------------------------------------------------------------------
-// Degree centrality (Java semantics)
+// Degree centrality (Java semantics).  The running integer mean is sequential per list, so a
+// long list is processed whole by the thread that owns its first slice.
 
-__global__ void __launch_bounds__(kBlock) k_degree(GraphView g, int64_t s, int64_t e, int32_t* deg, int64_t* avg,
-                                                   unsigned long long* edges) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(kBlock) k_degree(GraphView g, Work w, int64_t s, int64_t e, int32_t* deg,
+                                                   int64_t* avg, unsigned long long* edges) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long mine = 0;
-  if (x < g.max_vertex) {
-    int32_t d = 0;
-    int64_t mean = 0;
-    if (x >= g.active_begin && x <= g.max_label) {
-      const bool all = (s == 0 && e == 0);
-      const int lim = min(g.max_label + 1, g.max_vertex);
+  if (i < w.nitems) {
+    const WorkItem it = w.items[i];
+    int v0 = it.v0, v1 = it.v1;
+    if (it.slice >= 0 && w.slices[it.slice].first != 0) v1 = v0;  // later slices: owned by slice 0
+    const bool all = (s == 0 && e == 0);
+    const int lim = min(g.max_label + 1, g.max_vertex);
+    for (int x = v0; x < v1; ++x) {
+      if (x < g.active_begin || x > g.max_label) continue;
+      int32_t d = 0;
+      int64_t mean = 0;
       EdgeCursor c;
-      mine = (unsigned long long)c.open(g, x);
+      mine += (unsigned long long)c.open(g, x);
       int y;
       int64_t t;
       while (c.next(g, y, t)) {
@@ -405,15 +529,17 @@ __global__ void __launch_bounds__(kBlock) k_degree(GraphView g, int64_t s, int64
         }
       }
       if (s != e) d = (int32_t)(0.85 * d + 0.15 * d * (double)(mean - s) / (double)(e - s) + 1);
+      deg[x] = d;
+      avg[x] = mean;
     }
-    deg[x] = d;
-    avg[x] = mean;
   }
   add_edges(edges, mine);
 }
 
 // ---------------------------------------------------------------------------------------------
-// Jones-Plassmann colouring
+// Jones-Plassmann colouring: per round a check over queue entries (vertices or slices) marks
+// vertices that have a higher-priority uncoloured neighbour, then a decision pass colours the
+// others and builds the next worklist.
 
 __global__ void k_gc_prio_curand(uint32_t* prio, int32_t n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -423,47 +549,58 @@ __global__ void k_gc_prio_curand(uint32_t* prio, int32_t n) {
   prio[i] = curand(&st) % 256u;
 }
 
-__global__ void __launch_bounds__(kBlock) k_gc_round(GraphView g, const int32_t* wl, int32_t wn, int32_t* out_wl,
-                                                     int32_t* out_n, uint32_t* color, const uint32_t* prio, uint32_t round,
-                                                     int java_isolated, unsigned long long* edges) {
+__global__ void __launch_bounds__(kBlock) k_gc_check(GraphView g, Work w, const int32_t* entries, int32_t en,
+                                                     const uint32_t* color, const uint32_t* prio, uint32_t round,
+                                                     uint32_t* found, unsigned long long* edges) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long mine = 0;
-  if (i < wn) {
-    const int x = wl[i];
-    if (x >= g.active_begin && color[x] == kColorInf && x <= g.max_label) {
-      EdgeCursor c;
-      const int d = c.open(g, x);
-      if (d == 0) {
-        if (java_isolated) color[x] = round;
-      } else {
-        const uint32_t px = prio[x];
-        bool larger = false;
-        int y, prev_y = -1;
-        int64_t t;
-        int seen = 0;
-        while (c.next(g, y, t)) {
-          ++seen;
-          if (y == prev_y) continue;
-          prev_y = y;
-          if (y < g.active_begin || y >= g.max_vertex) continue;
-          const uint32_t py = prio[y];
-          if ((py > px || (py == px && y < x)) && color[y] >= round) {
-            larger = true;
-            break;
-          }
-        }
-        mine = (unsigned long long)seen;
-        if (larger) out_wl[atomicAdd(out_n, 1)] = x;
-        else color[x] = round;
+  if (i < en) {
+    EdgeCursor c;
+    int cnt;
+    const int x = open_entry(g, w, entries[i], c, cnt);
+    const uint32_t px = prio[x];
+    int y, prev_y = -1;
+    int64_t t;
+    while (c.next(g, y, t)) {
+      ++mine;
+      if (y == prev_y) continue;
+      prev_y = y;
+      if (y < g.active_begin || y >= g.max_vertex) continue;
+      const uint32_t py = prio[y];
+      if ((py > px || (py == px && y < x)) && color[y] >= round) {
+        found[x] = round + 1;
+        break;
       }
     }
   }
   add_edges(edges, mine);
 }
 
-__global__ void k_iota(int32_t* p, int32_t n) {
+__global__ void k_gc_decide(GraphView g, Work w, const int32_t* wl, int32_t wn, const int32_t* deg, uint32_t* color,
+                            const uint32_t* found, uint32_t round, int java_isolated, int32_t* out_wl, int32_t* out_n,
+                            int32_t* out_entries, int32_t* out_en) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) p[i] = i;
+  if (i >= wn) return;
+  const int x = wl[i];
+  if (x < g.active_begin || x > g.max_label || color[x] != kColorInf) return;
+  if (x >= g.n || deg[x] == 0) {
+    if (java_isolated) color[x] = round;
+    return;
+  }
+  if (found[x] == round + 1) {
+    out_wl[atomicAdd(out_n, 1)] = x;
+    enqueue(w, x, out_entries, out_en);
+  } else {
+    color[x] = round;
+  }
+}
+
+__global__ void k_gc_first(GraphView g, Work w, const int32_t* deg, int32_t n, int32_t* wl, int32_t* wn,
+                           int32_t* entries, int32_t* en) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= n) return;
+  wl[atomicAdd(wn, 1)] = x;
+  if (x >= g.active_begin && x <= g.max_label && x < g.n && deg[x] > 0) enqueue(w, x, entries, en);
 }
 
 }  // namespace tga
@@ -498,6 +635,10 @@ static unsigned long long* edge_counter(GraphHandle& h) {
   return p;
 }
 
+static uint64_t pass_bytes(const GraphHandle& h) {
+  return h.info.graph_bytes + h.info.timestamp_bytes + h.info.index_bytes;
+}
+
 extern "C" {
 
 int tga_neighbor_access(tga_graph* gp, uint8_t* small_out, uint64_t* checksum_out, int32_t* degree_out) {
@@ -513,17 +654,18 @@ int tga_neighbor_access(tga_graph* gp, uint8_t* small_out, uint64_t* checksum_ou
   cudaMemsetAsync(h.s_b.p, 0, (size_t)nv * 8, h.stream);
   const int32_t b = h.view.active_begin, e = std::min(h.view.max_label, h.view.n);
   if (e > b) {
+    const Work w = work_of(h);
     cudaEvent_t* ev = h.kernel_begin();
-    KL(k_neighbor_access, grid_for(e - b, kBlock))(h.view, b, e, h.s_a.as<uint8_t>(),
-                                                                        h.s_b.as<uint64_t>(), edges);
+    KL(k_neighbor_access, grid_for(w.nitems, kBlock))(h.view, w, b, e, h.s_b.as<unsigned long long>(), edges);
     h.kernel_end(ev);
+    KL(k_small_flags, grid_for(e - b, kBlock))(h.d_deg.as<int32_t>(), h.s_a.as<uint8_t>(), b, e);
   }
   if (small_out) cudaMemcpyAsync(small_out, h.s_a.p, (size_t)nv, cudaMemcpyDeviceToHost, h.stream);
   if (checksum_out) cudaMemcpyAsync(checksum_out, h.s_b.p, (size_t)nv * 8, cudaMemcpyDeviceToHost, h.stream);
   if (degree_out) cudaMemcpyAsync(degree_out, h.d_deg.p, (size_t)nv * 4, cudaMemcpyDeviceToHost, h.stream);
   h.timing.iterations = 1;
   const int rc = finish(h, edges);
-  h.timing.compressed_bytes = h.info.graph_bytes + h.info.timestamp_bytes + h.info.index_bytes;
+  h.timing.compressed_bytes = pass_bytes(h);
   return rc;
 }
 
@@ -536,7 +678,8 @@ int tga_neighbors(tga_graph* gp, int32_t v, int32_t* dst, int64_t* ts, int32_t c
   TGA_TRY(h.s_d.ensure((size_t)cap * 8 + 64));
   TGA_TRY(h.s_cnt.ensure(64));
   TGA_TRY(h.begin_call());
-  ++h.timing.launches, k_neighbors<<<1, 1, 0, h.stream>>>(h.view, v, h.s_c.as<int32_t>(), h.s_d.as<int64_t>(), cap, h.s_cnt.as<int32_t>());
+  ++h.timing.launches;
+  k_neighbors<<<1, 1, 0, h.stream>>>(h.view, v, h.s_c.as<int32_t>(), h.s_d.as<int64_t>(), cap, h.s_cnt.as<int32_t>());
   cudaMemcpyAsync(&h.h_pinned[16], h.s_cnt.p, 4, cudaMemcpyDeviceToHost, h.stream);
   TGA_TRY(h.end_call());
   *count = (int32_t)h.h_pinned[16];
@@ -552,11 +695,9 @@ int tga_decode_all(tga_graph* gp, int64_t* offsets, int32_t* dst, int64_t* ts, i
   if (!gp || !offsets) return fail(TGA_E_ARG, "null argument");
   GraphHandle& h = *gp;
   const int32_t n = h.view.n;
-  const int32_t nd = std::min(n, h.view.max_vertex);
-  std::vector<int32_t> deg((size_t)nd);
-  TGA_CUDA_TRY(cudaMemcpy(deg.data(), h.d_deg.p, (size_t)nd * 4, cudaMemcpyDeviceToHost));
+  const int32_t nd = (int32_t)h.degrees.size();
   offsets[0] = 0;
-  for (int32_t v = 0; v < n; ++v) offsets[v + 1] = offsets[v] + (v < nd ? deg[(size_t)v] : 0);
+  for (int32_t v = 0; v < n; ++v) offsets[v + 1] = offsets[v] + (v < nd ? h.degrees[(size_t)v] : 0);
   const int64_t m = offsets[n];
   if (!dst || !ts) return TGA_OK;  // size query
   if (cap < m) return fail(TGA_E_ARG, "capacity below the number of edges");
@@ -565,8 +706,9 @@ int tga_decode_all(tga_graph* gp, int64_t* offsets, int32_t* dst, int64_t* ts, i
   TGA_TRY(h.s_g.ensure((size_t)std::max<int64_t>(m, 1) * 8));
   TGA_CUDA_TRY(cudaMemcpy(h.s_e.p, offsets, (size_t)(n + 1) * 8, cudaMemcpyHostToDevice));
   TGA_TRY(h.begin_call());
-  KL(k_decode_csr, grid_for(nd, kBlock))(h.view, nd, h.s_e.as<int64_t>(), h.s_f.as<int32_t>(),
-                                                               h.s_g.as<int64_t>(), m);
+  const Work w = work_of(h);
+  KL(k_decode_csr, grid_for(w.nitems, kBlock))(h.view, w, h.s_e.as<int64_t>(), h.s_f.as<int32_t>(),
+                                                h.s_g.as<int64_t>(), m);
   cudaMemcpyAsync(dst, h.s_f.p, (size_t)m * 4, cudaMemcpyDeviceToHost, h.stream);
   cudaMemcpyAsync(ts, h.s_g.p, (size_t)m * 8, cudaMemcpyDeviceToHost, h.stream);
   return h.end_call();
@@ -593,14 +735,40 @@ int tga_bfs(tga_graph* gp, int32_t src, int64_t t_lo, int64_t t_hi, int32_t* arr
   cudaMemsetAsync(a.stamp, 0, (size_t)nv * 4, h.stream);
   const uint64_t start = (uint64_t)std::max<int64_t>(t_lo, 0) << 32;
   cudaMemcpyAsync(a.tp + src, &start, 8, cudaMemcpyHostToDevice, h.stream);
-  cudaMemcpyAsync(h.s_q0.p, &src, 4, cudaMemcpyHostToDevice, h.stream);
+  std::vector<int32_t> seed;
+  const int32_t sq = src < h.view.n ? seed_entries(h, src, seed) : 0;
+  if (sq) cudaMemcpyAsync(h.s_q0.p, seed.data(), (size_t)sq * 4, cudaMemcpyHostToDevice, h.stream);
   uint32_t wave = 0;
   int rc = TGA_OK;
-  const int levels = run_bfs_levels(h, a, h.s_q0, h.s_q1, 1, wave, rc);
+  int levels = run_bfs_levels(h, a, h.s_q0, h.s_q1, sq, wave, rc);
   if (rc) return rc;
+  // Phase 2: hop levels over tight edges.
+  uint32_t* hops_u = h.s_c.as<uint32_t>();
+  cudaMemsetAsync(hops_u, 0xFF, (size_t)nv * 4, h.stream);
+  cudaMemsetAsync(hops_u + src, 0, 4, h.stream);
+  if (sq) cudaMemcpyAsync(h.s_q0.p, seed.data(), (size_t)sq * 4, cudaMemcpyHostToDevice, h.stream);
+  {
+    const Work w = work_of(h);
+    DevBuf* cur = &h.s_q0;
+    DevBuf* nxt = &h.s_q1;
+    int32_t qn = sq;
+    for (uint32_t level = 0; qn > 0; ++level) {
+      a.q = cur->as<int32_t>();
+      a.nq = nxt->as<int32_t>();
+      cudaMemsetAsync(a.ncnt, 0, sizeof(int32_t), h.stream);
+      cudaEvent_t* ev = h.kernel_begin();
+      KL(k_bfs_hops, grid_for(qn, kBlock))(h.view, w, a, qn, hops_u, level);
+      h.kernel_end(ev);
+      cudaMemcpyAsync(h.h_pinned, a.ncnt, sizeof(int32_t), cudaMemcpyDeviceToHost, h.stream);
+      TGA_CUDA_TRY(cudaStreamSynchronize(h.stream));
+      qn = (int32_t)h.h_pinned[0];
+      std::swap(cur, nxt);
+      ++levels;
+    }
+  }
   int32_t* arr = h.s_q0.as<int32_t>();
   int32_t* hops = h.s_q1.as<int32_t>();
-  KL(k_unpack_tp, grid_for(nv, kBlock))(a.tp, arr, hops, nv);
+  KL(k_unpack_bfs, grid_for(nv, kBlock))(a.tp, hops_u, arr, hops, nv);
   if (arrival_out) cudaMemcpyAsync(arrival_out, arr, (size_t)nv * 4, cudaMemcpyDeviceToHost, h.stream);
   if (hops_out) cudaMemcpyAsync(hops_out, hops, (size_t)nv * 4, cudaMemcpyDeviceToHost, h.stream);
   h.timing.iterations = levels;
@@ -635,12 +803,13 @@ int tga_cc(tga_graph* gp, int64_t t_lo, int64_t t_hi, int32_t flags, int32_t* la
   cudaMemsetAsync(a.stamp, 0, (size_t)nv * 4, h.stream);
   cudaMemsetAsync(reached, 0, (size_t)nv, h.stream);
   const int32_t limit = (int32_t)(0.8 * h.view.max_label);
-  const int32_t end = std::min(h.view.max_label, nv);
+  const int32_t end = std::min(std::min(h.view.max_label, nv), h.view.n);
   int64_t total = 0;
   int small_run = 0, comp = 0, levels = 0;
   uint32_t wave = 0;
   int32_t v = std::max(h.cfg.cc_vertex_begin, 0);
   const uint64_t start = (uint64_t)std::max<int64_t>(t_lo, 0) << 32;
+  std::vector<int32_t> seedq;
   while (v < end) {
     if ((flags & TGA_CC_EARLY_EXIT) && total > limit) break;
     // Next seed: smallest unreached vertex >= v with outdegree > 9, searched in growing chunks.
@@ -658,15 +827,15 @@ int tga_cc(tga_graph* gp, int64_t t_lo, int64_t t_hi, int32_t flags, int32_t* la
     h.h_pinned[22] = 0;
     cudaMemcpyAsync(a.tcnt, &h.h_pinned[22], 4, cudaMemcpyHostToDevice, h.stream);
     cudaMemcpyAsync(a.tp + seed, &start, 8, cudaMemcpyHostToDevice, h.stream);
-    cudaMemcpyAsync(h.s_q0.p, &seed, 4, cudaMemcpyHostToDevice, h.stream);
+    const int32_t sq = seed_entries(h, seed, seedq);
+    cudaMemcpyAsync(h.s_q0.p, seedq.data(), (size_t)sq * 4, cudaMemcpyHostToDevice, h.stream);
     int rc = TGA_OK;
-    levels += run_bfs_levels(h, a, h.s_q0, h.s_q1, 1, wave, rc);
+    levels += run_bfs_levels(h, a, h.s_q0, h.s_q1, sq, wave, rc);
     if (rc) return rc;
     cudaMemcpyAsync(&h.h_pinned[23], a.tcnt, 4, cudaMemcpyDeviceToHost, h.stream);
     TGA_CUDA_TRY(cudaStreamSynchronize(h.stream));
     const int32_t reach = (int32_t)h.h_pinned[23];
-    KL(k_cc_label, grid_for(std::max(reach, 1), kBlock))(a.touched, a.tcnt, seed, comp, a.tp,
-                                                                             label, reached);
+    KL(k_cc_label, grid_for(std::max(reach, 1), kBlock))(a.touched, a.tcnt, seed, comp, a.tp, label, reached);
     ++comp;
     total += reach + 1;
     if (reach + 1 < 5) ++small_run;
@@ -690,35 +859,43 @@ int tga_pagerank(tga_graph* gp, int32_t iters, float damping, float alpha, int64
   TGA_TRY(h.s_a.ensure((size_t)nv * 4));
   TGA_TRY(h.s_b.ensure((size_t)nv * 4));
   TGA_TRY(h.s_c.ensure((size_t)nv * 4));
+  TGA_TRY(h.s_d.ensure((size_t)nv * 4));
+  TGA_TRY(h.s_e.ensure((size_t)nv * 4));
   TGA_TRY(h.s_g.ensure((size_t)(iters + 1) * 8));
   TGA_TRY(h.begin_call());
   unsigned long long* edges = edge_counter(h);
   const float base = (1.0f - damping) / (float)h.view.max_label;
-  float* bufs[2] = {h.s_a.as<float>(), h.s_b.as<float>()};
+  float* bufs[3] = {h.s_a.as<float>(), h.s_b.as<float>(), h.s_c.as<float>()};
   double* sums = h.s_g.as<double>();
+  const Work w = work_of(h);
   KL(k_fill_f32, grid_for(nv, kBlock))(bufs[0], 1.0f / (float)nv, nv);
   KL(k_fill_f32, grid_for(nv, kBlock))(bufs[1], base, nv);
   KL(k_pr_init_sums, grid_for(iters, kBlock))(sums, iters, (double)base * (double)nv);
   float* invdeg = nullptr;
   if (windowed) {
-    invdeg = h.s_c.as<float>();
+    int32_t* cnt = h.s_e.as<int32_t>();
+    invdeg = h.s_d.as<float>();
+    cudaMemsetAsync(cnt, 0, (size_t)nv * 4, h.stream);
     cudaEvent_t* ev = h.kernel_begin();
-    KL(k_window_invdeg, grid_for(nv, kBlock))(h.view, t_lo, t_hi, invdeg, edges);
+    KL(k_window_count, grid_for(w.nitems, kBlock))(h.view, w, t_lo, t_hi, cnt, edges);
     h.kernel_end(ev);
+    KL(k_invert, grid_for(nv, kBlock))(cnt, invdeg, nv);
   }
+  const unsigned grid = std::max(grid_for(w.nitems, kBlock), 1u);
   for (int k = 0; k < iters; ++k) {
-    PrArgs a{invdeg, h.d_deg.as<int32_t>(), bufs[k & 1], bufs[(k + 1) & 1], sums, k, damping, alpha, base, t_lo, t_hi, edges};
+    PrArgs a{invdeg, h.d_deg.as<int32_t>(), bufs[k % 3], bufs[(k + 1) % 3], bufs[(k + 2) % 3], sums, k,
+             damping, alpha, base, t_lo, t_hi, edges};
     cudaEvent_t* ev = h.kernel_begin();
-    KL(k_pr_iter, grid_for(nv, kBlock))(h.view, a);
+    KL(k_pr_iter, grid)(h.view, w, a);
     h.kernel_end(ev);
   }
-  float* out = bufs[iters & 1];
-  float* fin = h.s_c.as<float>();
+  float* out = bufs[iters % 3];
+  float* fin = h.s_d.as<float>();
   KL(k_pr_final, grid_for(nv, kBlock))(out, sums, iters - 1, fin, nv);
   if (rank_out) cudaMemcpyAsync(rank_out, fin, (size_t)nv * 4, cudaMemcpyDeviceToHost, h.stream);
   h.timing.iterations = iters;
   const int rc = finish(h, edges);
-  h.timing.compressed_bytes = (uint64_t)(iters + (windowed ? 1 : 0)) * (h.info.graph_bytes + h.info.timestamp_bytes + h.info.index_bytes);
+  h.timing.compressed_bytes = (uint64_t)(iters + (windowed ? 1 : 0)) * pass_bytes(h);
   return rc;
 }
 
@@ -738,38 +915,35 @@ int tga_hits(tga_graph* gp, int32_t iters, int32_t mode, int64_t t_lo, int64_t t
   float* hub = h.s_a.as<float>();
   float* auth[2] = {h.s_b.as<float>(), h.s_c.as<float>()};
   double* sums = h.s_g.as<double>();
+  const Work w = work_of(h);
+  const int java = mode == TGA_HITS_JAVA;
   KL(k_fill_f32, grid_for(nv, kBlock))(hub, 1.0f, nv);
   KL(k_fill_f32, grid_for(nv, kBlock))(auth[0], 1.0f, nv);
   cudaMemsetAsync(sums, 0, (size_t)(2 * iters + 2) * 8, h.stream);
   // sums[2k] = sum hub^2 of iteration k, sums[2k+1] = sum auth^2 of iteration k.
   for (int k = 0; k < iters; ++k) {
-    HitsArgs a{};
-    a.hub = hub;
-    a.auth_in = auth[k & 1];
-    a.auth_next = auth[(k + 1) & 1];
-    a.hsum = sums + 2 * k;
-    a.aprev = k == 0 ? nullptr : sums + 2 * k - 1;
-    a.java = mode == TGA_HITS_JAVA;
-    a.lo = t_lo;
-    a.hi = t_hi;
-    a.edges = edges;
+    const double* aprev = k == 0 ? nullptr : sums + 2 * k - 1;
+    float* ain = auth[k & 1];
+    float* anext = auth[(k + 1) & 1];
+    KL(k_hits_base, grid_for(nv, kBlock))(hub, ain, anext, aprev, java, nv);
     cudaEvent_t* ev = h.kernel_begin();
-    KL(k_hits_hub, grid_for(nv, kBlock))(h.view, a);
+    KL(k_hits_hub, grid_for(w.nitems, kBlock))(h.view, w, hub, ain, aprev, t_lo, t_hi, edges);
     h.kernel_end(ev);
+    KL(k_sumsq, grid_for(nv, kBlock))(hub, nv, sums + 2 * k);
     ev = h.kernel_begin();
-    KL(k_hits_auth, grid_for(nv, kBlock))(h.view, a);
+    KL(k_hits_auth, grid_for(w.nitems, kBlock))(h.view, w, hub, sums + 2 * k, anext, t_lo, t_hi, edges);
     h.kernel_end(ev);
-    KL(k_sumsq, grid_for(nv, kBlock))(a.auth_next, nv, sums + 2 * k + 1);
+    KL(k_scale, grid_for(nv, kBlock))(hub, sums + 2 * k, hub, nv);
+    KL(k_sumsq, grid_for(nv, kBlock))(anext, nv, sums + 2 * k + 1);
   }
-  float* hub_fin = hub;
   float* auth_fin = auth[iters & 1];
   float* out_auth = auth[(iters + 1) & 1];
   KL(k_scale, grid_for(nv, kBlock))(auth_fin, sums + 2 * iters - 1, out_auth, nv);
-  if (hub_out) cudaMemcpyAsync(hub_out, hub_fin, (size_t)nv * 4, cudaMemcpyDeviceToHost, h.stream);
+  if (hub_out) cudaMemcpyAsync(hub_out, hub, (size_t)nv * 4, cudaMemcpyDeviceToHost, h.stream);
   if (auth_out) cudaMemcpyAsync(auth_out, out_auth, (size_t)nv * 4, cudaMemcpyDeviceToHost, h.stream);
   h.timing.iterations = iters;
   const int rc = finish(h, edges);
-  h.timing.compressed_bytes = (uint64_t)(2 * iters) * (h.info.graph_bytes + h.info.timestamp_bytes + h.info.index_bytes);
+  h.timing.compressed_bytes = (uint64_t)(2 * iters) * pass_bytes(h);
   return rc;
 }
 
@@ -781,15 +955,17 @@ int tga_degree(tga_graph* gp, int64_t t_start, int64_t t_end, int32_t* degree_ou
   TGA_TRY(h.s_b.ensure((size_t)nv * 8));
   TGA_TRY(h.begin_call());
   unsigned long long* edges = edge_counter(h);
+  cudaMemsetAsync(h.s_a.p, 0, (size_t)nv * 4, h.stream);
+  cudaMemsetAsync(h.s_b.p, 0, (size_t)nv * 8, h.stream);
+  const Work w = work_of(h);
   cudaEvent_t* ev = h.kernel_begin();
-  KL(k_degree, grid_for(nv, kBlock))(h.view, t_start, t_end, h.s_a.as<int32_t>(),
-                                                          h.s_b.as<int64_t>(), edges);
+  KL(k_degree, grid_for(w.nitems, kBlock))(h.view, w, t_start, t_end, h.s_a.as<int32_t>(), h.s_b.as<int64_t>(), edges);
   h.kernel_end(ev);
   if (degree_out) cudaMemcpyAsync(degree_out, h.s_a.p, (size_t)nv * 4, cudaMemcpyDeviceToHost, h.stream);
   if (avg_out) cudaMemcpyAsync(avg_out, h.s_b.p, (size_t)nv * 8, cudaMemcpyDeviceToHost, h.stream);
   h.timing.iterations = 1;
   const int rc = finish(h, edges);
-  h.timing.compressed_bytes = h.info.graph_bytes + h.info.timestamp_bytes + h.info.index_bytes;
+  h.timing.compressed_bytes = pass_bytes(h);
   return rc;
 }
 
@@ -810,10 +986,14 @@ int tga_color(tga_graph* gp, int32_t prio_mode, const uint32_t* prio_in, int32_t
   const int32_t nv = h.view.max_vertex;
   if (prio_mode == 2 && !prio_in) return fail(TGA_E_ARG, "priorities required for mode 2");
   if (prio_mode < 0 || prio_mode > 2) return fail(TGA_E_ARG, "unknown priority mode");
+  const size_t qcap = (size_t)nv + (size_t)h.nslices + 1;
   TGA_TRY(h.s_a.ensure((size_t)nv * 4));  // colours
   TGA_TRY(h.s_b.ensure((size_t)nv * 4));  // priorities
+  TGA_TRY(h.s_c.ensure((size_t)nv * 4));  // found stamps
   TGA_TRY(h.s_q0.ensure((size_t)nv * 4));
   TGA_TRY(h.s_q1.ensure((size_t)nv * 4));
+  TGA_TRY(h.s_d.ensure(qcap * 4));
+  TGA_TRY(h.s_e.ensure(qcap * 4));
   TGA_TRY(h.s_cnt.ensure(64));
   std::vector<uint32_t> host_prio;
   if (prio_mode == 1) {
@@ -825,26 +1005,38 @@ int tga_color(tga_graph* gp, int32_t prio_mode, const uint32_t* prio_in, int32_t
   unsigned long long* edges = edge_counter(h);
   uint32_t* color = h.s_a.as<uint32_t>();
   uint32_t* prio = h.s_b.as<uint32_t>();
+  uint32_t* found = h.s_c.as<uint32_t>();
+  const Work w = work_of(h);
   if (prio_mode == 0) KL(k_gc_prio_curand, grid_for(nv, kBlock))(prio, nv);
   else cudaMemcpyAsync(prio, prio_in, (size_t)nv * 4, cudaMemcpyHostToDevice, h.stream);
   cudaMemsetAsync(color, 0xFF, (size_t)nv * 4, h.stream);
-  KL(k_iota, grid_for(nv, kBlock))(h.s_q0.as<int32_t>(), nv);
-  int32_t* cnt = h.s_cnt.as<int32_t>();
-  DevBuf* cur = &h.s_q0;
-  DevBuf* nxt = &h.s_q1;
-  int32_t wn = nv;
+  cudaMemsetAsync(found, 0, (size_t)nv * 4, h.stream);
+  int32_t* cnt = h.s_cnt.as<int32_t>();  // [0] worklist, [1] entries
+  cudaMemsetAsync(cnt, 0, 8, h.stream);
+  KL(k_gc_first, grid_for(nv, kBlock))(h.view, w, h.d_deg.as<int32_t>(), nv, h.s_q0.as<int32_t>(), cnt,
+                                       h.s_d.as<int32_t>(), cnt + 1);
+  DevBuf *wl = &h.s_q0, *nwl = &h.s_q1, *en = &h.s_d, *nen = &h.s_e;
+  int32_t wn = nv, ne = 0;
+  cudaMemcpyAsync(&h.h_pinned[24], cnt + 1, 4, cudaMemcpyDeviceToHost, h.stream);
+  TGA_CUDA_TRY(cudaStreamSynchronize(h.stream));
+  ne = (int32_t)h.h_pinned[24];
   int round = 0;
   while (wn != 0 && round < 512) {
-    cudaMemsetAsync(cnt, 0, 4, h.stream);
-    cudaEvent_t* ev = h.kernel_begin();
-    KL(k_gc_round, grid_for(wn, kBlock))(h.view, cur->as<int32_t>(), wn, nxt->as<int32_t>(), cnt,
-                                                              color, prio, (uint32_t)round, flags & TGA_GC_JAVA_ISOLATED,
-                                                              edges);
-    h.kernel_end(ev);
-    cudaMemcpyAsync(&h.h_pinned[24], cnt, 4, cudaMemcpyDeviceToHost, h.stream);
+    cudaMemsetAsync(cnt, 0, 8, h.stream);
+    if (ne > 0) {
+      cudaEvent_t* ev = h.kernel_begin();
+      KL(k_gc_check, grid_for(ne, kBlock))(h.view, w, en->as<int32_t>(), ne, color, prio, (uint32_t)round, found, edges);
+      h.kernel_end(ev);
+    }
+    KL(k_gc_decide, grid_for(wn, kBlock))(h.view, w, wl->as<int32_t>(), wn, h.d_deg.as<int32_t>(), color, found,
+                                          (uint32_t)round, flags & TGA_GC_JAVA_ISOLATED, nwl->as<int32_t>(), cnt,
+                                          nen->as<int32_t>(), cnt + 1);
+    cudaMemcpyAsync(&h.h_pinned[24], cnt, 8, cudaMemcpyDeviceToHost, h.stream);
     TGA_CUDA_TRY(cudaStreamSynchronize(h.stream));
     wn = (int32_t)h.h_pinned[24];
-    std::swap(cur, nxt);
+    ne = (int32_t)h.h_pinned[25];
+    std::swap(wl, nwl);
+    std::swap(en, nen);
     ++round;
   }
   if (color_out) cudaMemcpyAsync(color_out, color, (size_t)nv * 4, cudaMemcpyDeviceToHost, h.stream);

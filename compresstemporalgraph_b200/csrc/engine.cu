@@ -46,8 +46,8 @@ void DevBuf::release() {
 
 GraphHandle::~GraphHandle() {
   if (stream) cudaStreamSynchronize(stream);
-  for (DevBuf* b : {&d_graph, &d_ts, &d_gl, &d_gu, &d_gs, &d_tl, &d_tu, &d_ts_samples, &d_err, &d_deg, &s_a, &s_b,
-                    &s_c, &s_d, &s_e, &s_f, &s_g, &s_q0, &s_q1, &s_cnt, &s_sum})
+  for (DevBuf* b : {&d_graph, &d_ts, &d_gl, &d_gu, &d_gs, &d_tl, &d_tu, &d_ts_samples, &d_err, &d_deg, &d_slices,
+                    &d_items, &d_slice_first, &s_a, &s_b, &s_c, &s_d, &s_e, &s_f, &s_g, &s_q0, &s_q1, &s_cnt, &s_sum})
     b->release();
   for (auto& k : ktimers) {
     if (k.a) cudaEventDestroy(k.a);
@@ -304,6 +304,100 @@ int load_graph(GraphHandle& h, const std::string& dir, const std::string& base, 
   v.max_list = (int32_t)std::min<int64_t>(INT32_MAX / 4, std::max<int64_t>(maxd, 1));
   h.info_edges = m;
   h.degrees = std::move(deg);
+  const char* env_slice = std::getenv("TGA_SLICE_EDGES");
+  const char* env_item = std::getenv("TGA_ITEM_EDGES");
+  return build_work(h, env_slice ? std::atoi(env_slice) : 1024, env_item ? std::atoi(env_item) : 256);
+}
+
+int build_work(GraphHandle& h, int32_t slice_len, int32_t item_edges) {
+  if (slice_len < 16 || item_edges < 1) return fail(TGA_E_ARG, "slice length must be >= 16 and item size >= 1");
+  const GraphView& v = h.view;
+  const int32_t nd = (int32_t)h.degrees.size();
+  std::vector<int32_t> big_v;
+  std::vector<int64_t> slot_base{0};
+  for (int32_t x = 0; x < nd; ++x) {
+    const int32_t d = h.degrees[(size_t)x];
+    if (d > slice_len) {
+      big_v.push_back(x);
+      slot_base.push_back(slot_base.back() + (d + slice_len - 1) / slice_len);
+    }
+  }
+  const int32_t nbig = (int32_t)big_v.size();
+  std::vector<int32_t> nsl((size_t)nbig, 0);
+  std::vector<SliceState> slices;
+  if (nbig) {
+    DevBuf bv, sb, ns, tmp;
+    int rc;
+    if ((rc = bv.ensure((size_t)nbig * 4)) || (rc = sb.ensure(slot_base.size() * 8)) || (rc = ns.ensure((size_t)nbig * 4)) ||
+        (rc = tmp.ensure((size_t)slot_base.back() * sizeof(SliceState))))
+      return rc;
+    TGA_CUDA_TRY(cudaMemcpyAsync(bv.p, big_v.data(), (size_t)nbig * 4, cudaMemcpyHostToDevice, h.stream));
+    TGA_CUDA_TRY(cudaMemcpyAsync(sb.p, slot_base.data(), slot_base.size() * 8, cudaMemcpyHostToDevice, h.stream));
+    k_build_slices<<<grid_for(nbig, 64), 64, 0, h.stream>>>(v, bv.as<int32_t>(), sb.as<int64_t>(), nbig, slice_len,
+                                                           tmp.as<SliceState>(), ns.as<int32_t>());
+    TGA_CUDA_TRY(cudaGetLastError());
+    slices.resize((size_t)slot_base.back());
+    TGA_CUDA_TRY(cudaMemcpyAsync(nsl.data(), ns.p, (size_t)nbig * 4, cudaMemcpyDeviceToHost, h.stream));
+    TGA_CUDA_TRY(cudaMemcpyAsync(slices.data(), tmp.p, slices.size() * sizeof(SliceState), cudaMemcpyDeviceToHost,
+                                 h.stream));
+    if ((rc = h.check_device_error())) return rc;
+    bv.release(); sb.release(); ns.release(); tmp.release();
+  }
+  // Compact the slices, build slice_first and the work items (slices first, then short lists).
+  std::vector<SliceState> packed;
+  std::vector<int32_t> slice_first((size_t)nd + 1, 0);
+  std::vector<WorkItem> items;
+  {
+    int32_t b = 0;
+    for (int32_t x = 0; x < nd; ++x) {
+      slice_first[(size_t)x] = (int32_t)packed.size();
+      if (b < nbig && big_v[(size_t)b] == x) {
+        for (int32_t j = 0; j < nsl[(size_t)b]; ++j) {
+          items.push_back(WorkItem{x, x + 1, (int32_t)packed.size()});
+          packed.push_back(slices[(size_t)(slot_base[(size_t)b] + j)]);
+        }
+        ++b;
+      }
+    }
+    slice_first[(size_t)nd] = (int32_t)packed.size();
+  }
+  h.nslice_items = (int32_t)items.size();
+  {
+    constexpr int32_t kVertexCost = 4, kMaxRange = 4096;
+    int32_t start = -1, cost = 0;
+    for (int32_t x = 0; x < nd; ++x) {
+      const bool big = slice_first[(size_t)x + 1] != slice_first[(size_t)x];
+      if (big) {
+        if (start >= 0) items.push_back(WorkItem{start, x, -1});
+        start = -1;
+        cost = 0;
+        continue;
+      }
+      if (start < 0) start = x;
+      cost += h.degrees[(size_t)x] + kVertexCost;
+      if (cost >= item_edges || x + 1 - start >= kMaxRange) {
+        items.push_back(WorkItem{start, x + 1, -1});
+        start = -1;
+        cost = 0;
+      }
+    }
+    if (start >= 0) items.push_back(WorkItem{start, nd, -1});
+  }
+  h.nitems = (int32_t)items.size();
+  h.nslices = (int64_t)packed.size();
+  h.slice_len = slice_len;
+  h.item_edges = item_edges;
+  int rc;
+  if ((rc = h.d_items.ensure(std::max<size_t>(1, items.size()) * sizeof(WorkItem))) ||
+      (rc = h.d_slices.ensure(std::max<size_t>(1, packed.size()) * sizeof(SliceState))) ||
+      (rc = h.d_slice_first.ensure(slice_first.size() * 4)))
+    return rc;
+  if (!items.empty())
+    TGA_CUDA_TRY(cudaMemcpy(h.d_items.p, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice));
+  if (!packed.empty())
+    TGA_CUDA_TRY(cudaMemcpy(h.d_slices.p, packed.data(), packed.size() * sizeof(SliceState), cudaMemcpyHostToDevice));
+  TGA_CUDA_TRY(cudaMemcpy(h.d_slice_first.p, slice_first.data(), slice_first.size() * 4, cudaMemcpyHostToDevice));
+  h.slice_first_host = std::move(slice_first);
   return TGA_OK;
 }
 

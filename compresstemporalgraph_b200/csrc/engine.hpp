@@ -7,7 +7,7 @@
 #include <vector>
 
 #include "../../include/tga.h"
-#include "dview.cuh"
+#include "slices.cuh"
 
 namespace tga {
 
@@ -46,6 +46,13 @@ struct GraphHandle {
   DevBuf d_graph, d_ts, d_gl, d_gu, d_gs, d_tl, d_tu, d_ts_samples, d_err;
   // per-vertex outdegrees (int32, filled once at load by a decode kernel)
   DevBuf d_deg;
+  // edge-balanced work decomposition (slices.cuh): slices of long lists, work items, and
+  // slice_first[v]..slice_first[v+1] = slices of vertex v (empty for short lists)
+  DevBuf d_slices, d_items, d_slice_first;
+  int32_t nitems = 0, nslice_items = 0;
+  int64_t nslices = 0;
+  int32_t slice_len = 0, item_edges = 0;
+  std::vector<int32_t> slice_first_host;
   // scratch used by the algorithms
   DevBuf s_a, s_b, s_c, s_d, s_e, s_f, s_g, s_q0, s_q1, s_cnt, s_sum;
   uint32_t* h_pinned = nullptr;  // small pinned readback area
@@ -67,6 +74,9 @@ struct GraphHandle {
 };
 
 int load_graph(GraphHandle& h, const std::string& dir, const std::string& base, const tga_dataset_cfg& cfg);
+// (Re)builds slices and work items: lists longer than slice_len edges are cut into slices,
+// the others grouped into items of about item_edges edges.
+int build_work(GraphHandle& h, int32_t slice_len, int32_t item_edges);
 
 // Launch helpers shared by the algorithm files.
 inline unsigned grid_for(int64_t items, int block) { return (unsigned)((items + block - 1) / block); }

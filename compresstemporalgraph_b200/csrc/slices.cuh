@@ -1,0 +1,80 @@
+// Edge-balanced work decomposition of the successor lists.
+//
+// Power-law outdegrees make one-thread-per-vertex kernels wait for their largest list (a 163K-edge
+// list decoded by one thread takes longer than the rest of the graph together).  At load time every
+// list longer than the slice length is cut into slices: a slice holds the complete decoder state at
+// its first edge (reference-chain levels, timestamp cursor, previous timestamp), so any thread can
+// resume decoding there.  Slices start only where the successor id changes, so the "first
+// in-window occurrence of equal consecutive successors" rule never spans two slices.
+// The remaining (short) lists are grouped into work items of consecutive vertices holding about the
+// same number of edges as a slice.
+#pragma once
+#include "decoder.cuh"
+
+namespace tga {
+
+struct SliceState {
+  ChainState cs;
+  uint64_t tpos;    // bit position of the slice's first timestamp code
+  int64_t prev;     // timestamp preceding the slice's first edge
+  int32_t v;        // vertex
+  int32_t count;    // edges in the slice
+  int32_t first;    // index of the slice's first edge in the list of v
+  int32_t pad;
+};
+
+// slice >= 0: one slice; slice < 0: every vertex of [v0, v1) whole.
+struct WorkItem {
+  int32_t v0, v1, slice;
+};
+
+__device__ __forceinline__ void cursor_restore(const GraphView& g, EdgeCursor& c, const SliceState& s) {
+  c.cs = s.cs;
+  c.ts.init(g.t, s.tpos);
+  c.prev = s.prev;
+  c.remaining = s.count;
+  c.x = s.v;
+}
+
+__device__ __forceinline__ void cursor_save(const EdgeCursor& c, SliceState& s, int v, int first) {
+  s.cs = c.cs;
+  s.tpos = c.ts.pos();
+  s.prev = c.prev;
+  s.v = v;
+  s.first = first;
+  s.count = 0;
+}
+
+// One thread per long list: walks the list once and records a slice every >= `len` edges, at the
+// next edge whose successor differs from the previous one.  cap[b] slots are reserved per list.
+static __global__ void k_build_slices(GraphView g, const int32_t* big_v, const int64_t* slot_base, int32_t nbig, int32_t len,
+                               SliceState* out, int32_t* nslices) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nbig) return;
+  const int v = big_v[b];
+  SliceState* dst = out + slot_base[b];
+  const int cap = (int)(slot_base[b + 1] - slot_base[b]);
+  EdgeCursor c;
+  const int d = c.open(g, v);
+  cursor_save(c, dst[0], v, 0);
+  int k = 1, last = 0, prev_y = -1;
+  for (int i = 0; i < d; ++i) {
+    const bool cand = (i - last >= len) && k < cap;
+    EdgeCursor saved;
+    if (cand) saved = c;
+    int y;
+    int64_t t;
+    if (!c.next(g, y, t)) break;
+    if (cand && y != prev_y) {
+      dst[k - 1].count = i - last;
+      cursor_save(saved, dst[k], v, i);
+      last = i;
+      ++k;
+    }
+    prev_y = y;
+  }
+  dst[k - 1].count = d - last;
+  nslices[b] = k;
+}
+
+}  // namespace tga

@@ -102,7 +102,7 @@ void* tga_stream(tga_graph* g);
 /* Neighbour access / "RA" (neighbor_access.cu:1438-1642, main 1909-1930): decodes every list of
  * [active_vertex_begin, max_label) with its timestamps.  small_out[v] = outdegree(v) < 4 (the
  * reference's dv2), checksum_out[v] = order-sensitive hash of v's (successor, timestamp)
- * sequence, degree_out[v] = outdegree.  Any output may be NULL (then it stays on the device). */
+ * sequence (sum mod 2^64 of a 64-bit mix of (v, edge index, successor, timestamp)), degree_out[v] = outdegree.  Any output may be NULL (then it stays on the device). */
 int tga_neighbor_access(tga_graph* g, uint8_t* small_out, uint64_t* checksum_out, int32_t* degree_out);
 
 /* Successors and timestamps of one vertex in list order (EvolvingMultiGraph.successors,
@@ -115,8 +115,9 @@ int tga_decode_all(tga_graph* g, int64_t* offsets, int32_t* dst, int64_t* ts, in
 /* Temporal BFS (bfs.cu:1218-1692, host loop 1999-2038).  Edge (x->y,t) with t in [t_lo, t_hi)
  * relaxes y when arrival(x) <= t; only the first in-window occurrence of consecutive equal
  * successors counts.  arrival_out[v] = earliest arrival (INT32_MAX unreached, source = max(t_lo,0));
- * hops_out[v] = least hop count among the earliest arrivals (the deterministic form of the
- * reference's racy d_Ca level).  src < 0 -> bfs_start_vertex. */
+ * hops_out[v] = fewest edges of a path from the source that reaches every vertex on it at that
+ * vertex's earliest arrival (a BFS over edges with arrival(x) <= t == arrival(y)); this is the
+ * deterministic form of the reference's racy d_Ca level.  src < 0 -> bfs_start_vertex. */
 int tga_bfs(tga_graph* g, int32_t src, int64_t t_lo, int64_t t_hi, int32_t* arrival_out, int32_t* hops_out);
 
 /* Connected components by temporal reach (connected_components.cu:1210-1233,1679-1776, seed loop

@@ -325,18 +325,24 @@ void orc_csr(orc* o, int64_t* off, int32_t* dst, int64_t* ts) {
   memcpy(ts, o->ts, (size_t)o->m * 8);
 }
 
-/* Same order-sensitive hash as the engine's neighbour-access checksum. */
-static uint64_t orc_mix(uint64_t h, int32_t y, int64_t t) {
-  const uint64_t k = ((uint64_t)(uint32_t)y * 0x9E3779B97F4A7C15ull) ^ ((uint64_t)t * 0xC2B2AE3D27D4EB4Full);
-  h ^= k;
-  h = (h << 23) | (h >> 41);
-  return h * 0x165667B19E3779F9ull;
+/* Neighbour-access checksum of a list: sum mod 2^64 over its edges of a mix of (vertex, edge
+ * index, successor, timestamp) -- the engine's definition, additive so that it can be split. */
+static uint64_t orc_edge_hash(uint32_t v, uint32_t i, int32_t y, int64_t t) {
+  uint64_t z = (((uint64_t)v << 32) | i) * 0x9E3779B97F4A7C15ull;
+  z ^= (uint64_t)(uint32_t)y * 0xC2B2AE3D27D4EB4Full;
+  z ^= (uint64_t)t * 0x165667B19E3779F9ull;
+  z ^= z >> 31;
+  z *= 0xBF58476D1CE4E5B9ull;
+  z ^= z >> 29;
+  z *= 0x94D049BB133111EBull;
+  return z ^ (z >> 32);
 }
 
 void orc_checksums(orc* o, int64_t begin, int64_t end, uint64_t* csum, uint8_t* small) {
   for (int64_t x = begin; x < end; ++x) {
-    uint64_t h = 0x27D4EB2F165667C5ull ^ (uint64_t)(uint32_t)x;
-    for (int64_t e = o->off[x]; e < o->off[x + 1]; ++e) h = orc_mix(h, o->dst[e], o->ts[e]);
+    uint64_t h = 0;
+    for (int64_t e = o->off[x]; e < o->off[x + 1]; ++e)
+      h += orc_edge_hash((uint32_t)x, (uint32_t)(e - o->off[x]), o->dst[e], o->ts[e]);
     csum[x] = h;
     small[x] = o->deg[x] < 4;
   }
@@ -396,7 +402,8 @@ static hent hpop(heap* h) {
   return top;
 }
 
-/* Temporal reach with lexicographic (arrival, hops) keys; returns the touched count (excl. src). */
+/* Earliest arrival by Dijkstra on arrival times (the relaxation fixpoint is unique); returns the
+ * number of vertices other than src that were reached.  key[] holds arrival << 32. */
 static int64_t bfs_core(orc* o, const orc_cfg* c, int32_t src, int64_t lo, int64_t hi, uint64_t* key) {
   heap h = {0};
   const uint64_t start = (uint64_t)(lo > 0 ? lo : 0) << 32;
@@ -408,11 +415,11 @@ static int64_t bfs_core(orc* o, const orc_cfg* c, int32_t src, int64_t lo, int64
     const int32_t x = top.v;
     if (top.key != key[x]) continue;
     if (x < c->active || x > c->max_label || x >= o->n) continue;
-    const uint64_t ax = top.key >> 32, hx = top.key & 0xffffffffull;
+    const uint64_t ax = top.key >> 32;
     FOR_DEDUP_EDGES(o, x, lo, hi, y, t, {
       if (y < c->active || y >= c->max_vertex) continue;
       if ((int64_t)ax > t || t >= 0xFFFFFFFFll) continue;
-      const uint64_t nv = ((uint64_t)t << 32) | (hx + 1);
+      const uint64_t nv = (uint64_t)t << 32;
       if (nv < key[y]) {
         if (key[y] == ~0ull) ++touched;
         key[y] = nv;
@@ -424,16 +431,39 @@ static int64_t bfs_core(orc* o, const orc_cfg* c, int32_t src, int64_t lo, int64
   return touched;
 }
 
+/* Hop counts: breadth-first over tight edges (arrival(x) <= t == arrival(y)) from src. */
+static void bfs_hops(orc* o, const orc_cfg* c, int32_t src, int64_t lo, int64_t hi, const uint64_t* key,
+                     int32_t* hops) {
+  int32_t* q = (int32_t*)malloc((size_t)c->max_vertex * 4 + 4);
+  int64_t qh = 0, qt = 0;
+  hops[src] = 0;
+  q[qt++] = src;
+  while (qh < qt) {
+    const int32_t x = q[qh++];
+    if (x < c->active || x > c->max_label || x >= o->n) continue;
+    const int64_t ax = (int64_t)(key[x] >> 32);
+    FOR_DEDUP_EDGES(o, x, lo, hi, y, t, {
+      if (y < c->active || y >= c->max_vertex) continue;
+      if (ax > t || t >= 0xFFFFFFFFll) continue;
+      if ((int64_t)(key[y] >> 32) != t || hops[y] != ORC_INF32) continue;
+      hops[y] = hops[x] + 1;
+      q[qt++] = y;
+    });
+  }
+  free(q);
+}
+
 void orc_bfs(orc* o, int32_t max_label, int32_t max_vertex, int32_t active, int32_t src, int64_t lo, int64_t hi,
              int32_t* arr, int32_t* hops) {
   orc_cfg c = {max_label, max_vertex, active};
   uint64_t* key = (uint64_t*)malloc((size_t)max_vertex * 8);
-  for (int32_t i = 0; i < max_vertex; ++i) key[i] = ~0ull;
+  for (int32_t i = 0; i < max_vertex; ++i) { key[i] = ~0ull; hops[i] = ORC_INF32; }
   bfs_core(o, &c, src, lo, hi, key);
+  bfs_hops(o, &c, src, lo, hi, key, hops);
   for (int32_t i = 0; i < max_vertex; ++i) {
     const int inf = (key[i] >> 32) == 0xFFFFFFFFull;
     arr[i] = inf ? ORC_INF32 : (int32_t)(key[i] >> 32);
-    hops[i] = inf ? ORC_INF32 : (int32_t)(key[i] & 0xffffffffull);
+    if (inf) hops[i] = ORC_INF32;
   }
   free(key);
 }
@@ -687,8 +717,8 @@ int64_t orc_stream_decode(orc* o, int64_t begin, int64_t end, uint64_t* csum, in
 #pragma omp for schedule(dynamic, 256)
     for (int64_t x = begin; x < end; ++x) {
       const int64_t k = stream_list(o, x, &L, &tsb, &cap);
-      uint64_t h = 0x27D4EB2F165667C5ull ^ (uint64_t)(uint32_t)x;
-      for (int64_t i = 0; i < k; ++i) h = orc_mix(h, L.v[i], tsb[i]);
+      uint64_t h = 0;
+      for (int64_t i = 0; i < k; ++i) h += orc_edge_hash((uint32_t)x, (uint32_t)i, L.v[i], tsb[i]);
       if (csum) csum[x] = h;
       edges += k;
     }
