@@ -111,6 +111,9 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+ONLY = None  # --only: run a single workload per step (profiling runs; not a bench line)
+
+
 def suite(g, outputs: bool):
     """One step: the seven workloads; returns (edges decoded, launches, per-workload timing)."""
     cfg = g.cfg
@@ -124,13 +127,20 @@ def suite(g, outputs: bool):
         edges += t["edges_decoded"]
         launches += t["launches"]
 
-    g.neighbor_access(outputs=outputs); rec("RA")
-    g.bfs(cfg.bfs_start_vertex, outputs=outputs); rec("BFS")
-    g.connected_components(outputs=outputs); rec("CC")
-    g.pagerank(30, outputs=outputs); rec("PR")
-    g.hits(30, outputs=outputs); rec("HITS")
-    g.degree_centrality(0, 0, outputs=outputs); rec("DC")
-    g.color(0, outputs=outputs); rec("GC")
+    runs = {
+        "RA": lambda: g.neighbor_access(outputs=outputs),
+        "BFS": lambda: g.bfs(cfg.bfs_start_vertex, outputs=outputs),
+        "CC": lambda: g.connected_components(outputs=outputs),
+        "PR": lambda: g.pagerank(30, outputs=outputs),
+        "HITS": lambda: g.hits(30, outputs=outputs),
+        "DC": lambda: g.degree_centrality(0, 0, outputs=outputs),
+        "GC": lambda: g.color(0, outputs=outputs),
+    }
+    for name, fn in runs.items():
+        if ONLY and name != ONLY:
+            continue
+        fn()
+        rec(name)
     return edges, launches, per
 
 
@@ -214,7 +224,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--only", choices=["RA", "BFS", "CC", "PR", "HITS", "DC", "GC"],
+                    help="run one workload per step (for profiling; the line is not the benchmark)")
     args = ap.parse_args()
+    global ONLY
+    ONLY = args.only
     if args.impl == "reference":
         return run_reference(args)
 
@@ -278,6 +292,10 @@ def main():
     value = total_edges / (ms / 1e3) / 1e9
     e2e_value = e2e_edges * world / (e2e_ms / 1e3) / 1e9
 
+    if ONLY:
+        print(json.dumps({"only": ONLY, "ms": ms, "edges": edges, "workloads": {k: v for k, v in per_all[0].items()}}))
+        g.close()
+        return 0
     # Roofline of the PageRank iteration kernel (30 launches per step, one full decode pass each).
     pr = [p["PR"] for p in per_all]
     pr_launch_ms = sum(p["decode_ms"] for p in pr) / max(1, sum(p["decode_launches"] for p in pr))

@@ -87,6 +87,9 @@ def _load() -> C.CDLL:
         "tga_get_info": (C.c_int, [P, C.POINTER(_Info)]),
         "tga_get_timing": (C.c_int, [P, C.POINTER(_Timing)]),
         "tga_stream": (P, [P]),
+        "tga_set_work_params": (C.c_int, [P, C.c_int32, C.c_int32]),
+        "tga_get_work_params": (C.c_int, [P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int64),
+                                          C.POINTER(C.c_int32)]),
         "tga_neighbor_access": (C.c_int, [P, P, P, P]),
         "tga_neighbors": (C.c_int, [P, C.c_int32, P, P, C.c_int32, C.POINTER(C.c_int32)]),
         "tga_decode_all": (C.c_int, [P, P, P, P, C.c_int64]),
@@ -218,6 +221,14 @@ class Graph:
     @property
     def stream(self) -> int:
         return _lib.tga_stream(self._h) or 0
+
+    def set_work_params(self, slice_edges: int, item_edges: int) -> None:
+        _check(_lib.tga_set_work_params(self._h, slice_edges, item_edges))
+
+    def work_params(self) -> dict:
+        a, b, c, d = C.c_int32(), C.c_int32(), C.c_int64(), C.c_int32()
+        _check(_lib.tga_get_work_params(self._h, C.byref(a), C.byref(b), C.byref(c), C.byref(d)))
+        return {"slice_edges": a.value, "item_edges": b.value, "slices": c.value, "items": d.value}
 
     def timing(self) -> dict:
         t = _Timing()

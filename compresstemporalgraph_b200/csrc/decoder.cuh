@@ -26,14 +26,58 @@ struct LevelState {
   int rleft;                 // residuals left including the head
   int bleft, cur_left;       // copy blocks still to read, values left in the current copy block
                              // (-1: copy everything that remains)
+  int x;                     // vertex whose list this level decodes
+  int emitted;               // values of this list returned so far
 };
 
 struct ChainState {
   LevelState lv[kMaxLevels];
 };
 
+// Complete decoder state at one edge of a long list (see slices.cuh).
+struct SliceState {
+  ChainState cs;
+  uint64_t tpos;    // bit position of the slice's first timestamp code
+  int64_t prev;     // timestamp preceding the slice's first edge
+  int32_t v;        // vertex
+  int32_t count;    // edges in the slice
+  int32_t first;    // index of the slice's first edge in the list of v
+  int32_t pad;
+};
+
 template <int L>
 __device__ __forceinline__ int list_next(const GraphView& g, ChainState& s);
+
+// Skips k values of the list decoded at level L.  A long skip over a list that has slice
+// checkpoints restores the last checkpoint at or before the target (its levels 0.. become levels
+// L.. here: a list referenced at level L has a chain of at most kMaxLevels-1-L further levels),
+// so the walk is bounded by one slice instead of the skip length.
+template <int L>
+__device__ __forceinline__ void skip_values(const GraphView& g, ChainState& s, int k) {
+  LevelState& st = s.lv[L];
+  if (L > 0 && k > g.seek_min && g.slice_first) {
+    const int a = g.slice_first[st.x], b = g.slice_first[st.x + 1];
+    const int target = st.emitted + k;
+    if (b - a > 1) {
+      int lo = a, hi = b - 1;  // last slice with first <= target
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (g.slices[mid].first <= target) lo = mid;
+        else hi = mid - 1;
+      }
+      const SliceState& cp = g.slices[lo];
+      if (cp.first > st.emitted) {
+        s.lv[L] = cp.cs.lv[0];
+        if constexpr (L + 1 < kMaxLevels) s.lv[L + 1] = cp.cs.lv[1];
+        if constexpr (L + 2 < kMaxLevels) s.lv[L + 2] = cp.cs.lv[2];
+        if constexpr (L + 3 < kMaxLevels) s.lv[L + 3] = cp.cs.lv[3];
+        k = target - cp.first;
+      }
+    }
+  }
+  for (int i = 0; i < k && i <= g.max_list; ++i)
+    if (list_next<L>(g, s) == kInf) break;
+}
 
 template <int L>
 __device__ __forceinline__ int masked_next(const GraphView& g, ChainState& s) {
@@ -47,8 +91,7 @@ __device__ __forceinline__ int masked_next(const GraphView& g, ChainState& s) {
       if (st.cur_left == 0 && st.bleft > 0) {
         const int skip = (int)read_gamma(g, g.g, st.bpos) + 1;
         --st.bleft;
-        for (int k = 0; k < skip && k <= g.max_list; ++k)
-          if (list_next<L + 1>(g, s) == kInf) break;
+        skip_values<L + 1>(g, s, skip);
         if (st.bleft > 0) {
           st.cur_left = (int)read_gamma(g, g.g, st.bpos) + 1;
           --st.bleft;
@@ -97,15 +140,18 @@ __device__ __forceinline__ int list_next(const GraphView& g, ChainState& s) {
   if constexpr (L + 1 < kMaxLevels) {
     if (st.hc == v) st.hc = masked_next<L>(g, s);
   }
+  ++st.emitted;
   return v;
 }
 
 // Parses the record of vertex x into level L; returns its outdegree.
 template <int L>
-__device__ int level_init(const GraphView& g, ChainState& s, int x) {
+__device__ __forceinline__ int level_init(const GraphView& g, ChainState& s, int x) {
   LevelState& st = s.lv[L];
   st.hm = st.hi = st.hr = st.hc = kInf;
   st.rleft = 0;
+  st.x = x;
+  st.emitted = 0;
   if (x < 0 || x >= g.n) { set_err(g, kErrId); return 0; }
   uint64_t pos = ef_get(g, g.gef, (uint64_t)x);
   const int d = (int)read_gamma(g, g.g, pos);
@@ -138,8 +184,7 @@ __device__ int level_init(const GraphView& g, ChainState& s, int x) {
         if (st.cur_left == 0 && st.bleft > 0) {
           const int skip = (int)read_gamma(g, g.g, st.bpos) + 1;
           --st.bleft;
-          for (int k = 0; k < skip && k <= g.max_list; ++k)
-            if (list_next<L + 1>(g, s) == kInf) break;
+          skip_values<L + 1>(g, s, skip);
           if (st.bleft > 0) {
             st.cur_left = (int)read_gamma(g, g.g, st.bpos) + 1;
             --st.bleft;

@@ -52,6 +52,11 @@ struct GraphView {
   int32_t active_begin;  // ACTIVE_VERTEX_BEGIN
   int32_t min_interval;  // minintervallength of the successor format
   int32_t max_list;      // largest outdegree in the graph (bounds every header-driven loop)
+  // Slice checkpoints of long lists (slices.cuh), used by the decoder to seek over long skip
+  // blocks of a referenced list; null until the work decomposition is built.
+  const struct SliceState* slices;
+  const int32_t* slice_first;
+  int32_t seek_min;      // skip blocks longer than this seek through a checkpoint
   int64_t min_ts;        // header of the .timestamps stream
   uint32_t* err;         // device error word
 };

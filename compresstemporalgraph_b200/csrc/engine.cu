@@ -311,7 +311,11 @@ int load_graph(GraphHandle& h, const std::string& dir, const std::string& base, 
 
 int build_work(GraphHandle& h, int32_t slice_len, int32_t item_edges) {
   if (slice_len < 16 || item_edges < 1) return fail(TGA_E_ARG, "slice length must be >= 16 and item size >= 1");
-  const GraphView& v = h.view;
+  GraphView& v = h.view;
+  // The build walks the lists without seeking (checkpoints are being made).
+  v.slices = nullptr;
+  v.slice_first = nullptr;
+  v.seek_min = INT32_MAX;
   const int32_t nd = (int32_t)h.degrees.size();
   std::vector<int32_t> big_v;
   std::vector<int64_t> slot_base{0};
@@ -398,6 +402,9 @@ int build_work(GraphHandle& h, int32_t slice_len, int32_t item_edges) {
     TGA_CUDA_TRY(cudaMemcpy(h.d_slices.p, packed.data(), packed.size() * sizeof(SliceState), cudaMemcpyHostToDevice));
   TGA_CUDA_TRY(cudaMemcpy(h.d_slice_first.p, slice_first.data(), slice_first.size() * 4, cudaMemcpyHostToDevice));
   h.slice_first_host = std::move(slice_first);
+  v.slices = h.d_slices.as<SliceState>();
+  v.slice_first = h.d_slice_first.as<int32_t>();
+  v.seek_min = std::max(16, slice_len / 2);
   return TGA_OK;
 }
 
@@ -481,5 +488,20 @@ int tga_get_timing(tga_graph* g, tga_timing* out) {
 }
 
 void* tga_stream(tga_graph* g) { return g ? (void*)g->stream : nullptr; }
+
+int tga_set_work_params(tga_graph* g, int32_t slice_edges, int32_t item_edges) {
+  if (!g) return fail(TGA_E_ARG, "null graph");
+  if (cudaStreamSynchronize(g->stream) != cudaSuccess) return fail(TGA_E_CUDA, "stream synchronisation failed");
+  return build_work(*g, slice_edges, item_edges);
+}
+
+int tga_get_work_params(tga_graph* g, int32_t* slice_edges, int32_t* item_edges, int64_t* slices, int32_t* items) {
+  if (!g) return fail(TGA_E_ARG, "null graph");
+  if (slice_edges) *slice_edges = g->slice_len;
+  if (item_edges) *item_edges = g->item_edges;
+  if (slices) *slices = g->nslices;
+  if (items) *items = g->nitems;
+  return TGA_OK;
+}
 
 }  // extern "C"

@@ -13,15 +13,7 @@
 
 namespace tga {
 
-struct SliceState {
-  ChainState cs;
-  uint64_t tpos;    // bit position of the slice's first timestamp code
-  int64_t prev;     // timestamp preceding the slice's first edge
-  int32_t v;        // vertex
-  int32_t count;    // edges in the slice
-  int32_t first;    // index of the slice's first edge in the list of v
-  int32_t pad;
-};
+// SliceState (decoder.cuh) holds the complete decoder state at the first edge of a slice.
 
 // slice >= 0: one slice; slice < 0: every vertex of [v0, v1) whole.
 struct WorkItem {

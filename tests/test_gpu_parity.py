@@ -207,3 +207,37 @@ def test_timing_reports_device_time(pairs):
     t = p.g.timing()
     assert t["total_ms"] > 0 and t["decode_ms"] > 0 and t["decode_launches"] == 3
     assert t["edges_decoded"] == 3 * p.o.m - 3 * int(np.diff(p.o.csr()[0])[p.ml:].sum())
+
+
+@pytest.mark.parametrize("shape", ["hubs", "chains", "small"])
+@pytest.mark.parametrize("slice_edges,item_edges", [(16, 8), (64, 300), (4096, 2048)])
+def test_work_decomposition_does_not_change_results(pairs, shape, slice_edges, item_edges):
+    """Tiny slices force checkpoint restores (including seeks over long skip blocks of a
+    referenced list); results must not depend on the decomposition."""
+    p = pairs[shape]
+    g = p.g
+    g.set_work_params(slice_edges, item_edges)
+    try:
+        wp = g.work_params()
+        assert wp["slice_edges"] == slice_edges and wp["items"] > 0
+        off, dst, ts = g.decode_all()
+        ooff, odst, ots = p.o.csr()
+        assert np.array_equal(dst, odst) and np.array_equal(ts, ots)
+        _, csum, _ = g.neighbor_access()
+        end = min(p.ml, p.n)
+        _, ocs = p.o.checksums(p.act, end, p.mv)
+        assert np.array_equal(csum[p.act:end], ocs[p.act:end])
+        src = int(np.argmax(np.diff(ooff)))
+        arr, hops = g.bfs(src)
+        oarr, ohops = p.o.bfs(p.ml, p.mv, p.act, src)
+        assert np.array_equal(arr, oarr) and np.array_equal(hops, ohops)
+        r = g.pagerank(5)
+        assert float(np.abs(r - p.o.pagerank(p.ml, p.mv, p.act, 5)).sum()) <= 1e-5
+        col, prio, _ = g.color(0)
+        ocol, _ = p.o.color(p.ml, p.mv, p.act, prio)
+        assert np.array_equal(col, ocol)
+        deg, avg = g.degree_centrality(0, 0)
+        odeg, oavg = p.o.degree(p.ml, p.mv, p.act, 0, 0)
+        assert np.array_equal(deg, odeg) and np.array_equal(avg, oavg)
+    finally:
+        g.set_work_params(1024, 256)
