@@ -94,7 +94,8 @@ __device__ __forceinline__ unsigned long long sweep_item(const GraphView& g, con
   const int vend = it.slice >= 0 ? it.v0 + 1 : it.v1;
   for (int v = it.v0; v < vend; ++v) {  // one call site keeps the body inlined and the cursor in registers
     if (!want(v)) continue;
-    EdgeCursor c;
+    DeepState deep_;
+    EdgeCursor c(&deep_);
     int first = 0, count;
     if (it.slice >= 0) {
       const SliceState& s = w.slices[it.slice];
@@ -113,7 +114,7 @@ __device__ __forceinline__ unsigned long long sweep_item(const GraphView& g, con
 // ---------------------------------------------------------------------------------------------
 // Neighbour access and raw decode
 
-__global__ void __launch_bounds__(kBlock) k_neighbor_access(GraphView g, Work w, int32_t begin, int32_t end,
+__global__ void __launch_bounds__(kBlock, 2) k_neighbor_access(GraphView g, Work w, int32_t begin, int32_t end,
                                                             unsigned long long* csum, unsigned long long* edges) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long mine = 0;
@@ -154,7 +155,8 @@ __global__ void k_decode_csr(GraphView g, Work w, const int64_t* off, int32_t* d
 }
 
 __global__ void k_neighbors(GraphView g, int32_t v, int32_t* dst, int64_t* ts, int32_t cap, int32_t* count) {
-  EdgeCursor c;
+  DeepState deep_;
+  EdgeCursor c(&deep_);
   const int d = c.open(g, v);
   int i = 0, y;
   int64_t t;
@@ -191,11 +193,12 @@ struct BfsArgs {
 
 // Phase 1: tp[v] holds arrival << 32, so the 64-bit atomicMin is an arrival minimum; a vertex
 // whose arrival drops is enqueued once per level (stamp) and relaxes its successors again.
-__global__ void __launch_bounds__(kBlock) k_bfs_level(GraphView g, Work w, BfsArgs a, int32_t qn) {
+__global__ void __launch_bounds__(kBlock, 2) k_bfs_level(GraphView g, Work w, BfsArgs a, int32_t qn) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long mine = 0;
   if (i < qn) {
-    EdgeCursor c;
+    DeepState deep_;
+    EdgeCursor c(&deep_);
     int cnt;
     const int x = open_entry(g, w, a.q[i], c, cnt);
     if (x >= g.active_begin && x <= g.max_label) {
@@ -220,12 +223,13 @@ __global__ void __launch_bounds__(kBlock) k_bfs_level(GraphView g, Work w, BfsAr
 
 // Phase 2: with the final arrivals fixed, an edge passing the same filters is tight when
 // arrival(x) <= t == arrival(y); hops = BFS level over tight edges, each vertex claimed once.
-__global__ void __launch_bounds__(kBlock) k_bfs_hops(GraphView g, Work w, BfsArgs a, int32_t qn, uint32_t* hops,
+__global__ void __launch_bounds__(kBlock, 2) k_bfs_hops(GraphView g, Work w, BfsArgs a, int32_t qn, uint32_t* hops,
                                                      uint32_t level) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long mine = 0;
   if (i < qn) {
-    EdgeCursor c;
+    DeepState deep_;
+    EdgeCursor c(&deep_);
     int cnt;
     const int x = open_entry(g, w, a.q[i], c, cnt);
     if (x >= g.active_begin && x <= g.max_label) {
@@ -365,7 +369,7 @@ __device__ __forceinline__ float temporal_weight(float alpha, int64_t t) {
   return a > 18.0f ? 1.0f : 1.0f - expf(-a);
 }
 
-__global__ void __launch_bounds__(kBlock) k_pr_iter(GraphView g, Work w, PrArgs a) {
+__global__ void __launch_bounds__(kBlock, 2) k_pr_iter(GraphView g, Work w, PrArgs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   for (int x = i; x < g.max_vertex; x += gridDim.x * blockDim.x) a.reset[x] = a.base;
   double local = 0;
@@ -407,7 +411,7 @@ __global__ void k_pr_final(const float* buf, const double* sums, int k, float* o
 }
 
 // In-window outdegree of each source, counted over items, then inverted.
-__global__ void __launch_bounds__(kBlock) k_window_count(GraphView g, Work w, int64_t lo, int64_t hi, int32_t* cnt,
+__global__ void __launch_bounds__(kBlock, 2) k_window_count(GraphView g, Work w, int64_t lo, int64_t hi, int32_t* cnt,
                                                          unsigned long long* edges) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long mine = 0;
@@ -442,7 +446,7 @@ __global__ void k_hits_base(float* hub, const float* auth_in, float* auth_next, 
   auth_next[x] = java ? 0.0f : auth_in[x] * sa;
 }
 
-__global__ void __launch_bounds__(kBlock) k_hits_hub(GraphView g, Work w, float* hub, const float* auth_in,
+__global__ void __launch_bounds__(kBlock, 2) k_hits_hub(GraphView g, Work w, float* hub, const float* auth_in,
                                                      const double* aprev, int64_t lo, int64_t hi, unsigned long long* edges) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long mine = 0;
@@ -464,7 +468,7 @@ __global__ void __launch_bounds__(kBlock) k_hits_hub(GraphView g, Work w, float*
   add_edges(edges, mine);
 }
 
-__global__ void __launch_bounds__(kBlock) k_hits_auth(GraphView g, Work w, const float* hub, const double* hsum,
+__global__ void __launch_bounds__(kBlock, 2) k_hits_auth(GraphView g, Work w, const float* hub, const double* hsum,
                                                       float* auth_next, int64_t lo, int64_t hi, unsigned long long* edges) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long mine = 0;
@@ -503,7 +507,7 @@ __global__ void k_scale(const float* v, const double* sumsq, float* out, int32_t
 // Degree centrality (Java semantics).  The running integer mean is sequential per list, so a
 // long list is processed whole by the thread that owns its first slice.
 
-__global__ void __launch_bounds__(kBlock) k_degree(GraphView g, Work w, int64_t s, int64_t e, int32_t* deg,
+__global__ void __launch_bounds__(kBlock, 2) k_degree(GraphView g, Work w, int64_t s, int64_t e, int32_t* deg,
                                                    int64_t* avg, unsigned long long* edges) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long mine = 0;
@@ -517,7 +521,8 @@ __global__ void __launch_bounds__(kBlock) k_degree(GraphView g, Work w, int64_t 
       if (x < g.active_begin || x > g.max_label) continue;
       int32_t d = 0;
       int64_t mean = 0;
-      EdgeCursor c;
+      DeepState deep_;
+      EdgeCursor c(&deep_);
       mine += (unsigned long long)c.open(g, x);
       int y;
       int64_t t;
@@ -549,13 +554,14 @@ __global__ void k_gc_prio_curand(uint32_t* prio, int32_t n) {
   prio[i] = curand(&st) % 256u;
 }
 
-__global__ void __launch_bounds__(kBlock) k_gc_check(GraphView g, Work w, const int32_t* entries, int32_t en,
+__global__ void __launch_bounds__(kBlock, 2) k_gc_check(GraphView g, Work w, const int32_t* entries, int32_t en,
                                                      const uint32_t* color, const uint32_t* prio, uint32_t round,
                                                      uint32_t* found, unsigned long long* edges) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long mine = 0;
   if (i < en) {
-    EdgeCursor c;
+    DeepState deep_;
+    EdgeCursor c(&deep_);
     int cnt;
     const int x = open_entry(g, w, entries[i], c, cnt);
     const uint32_t px = prio[x];

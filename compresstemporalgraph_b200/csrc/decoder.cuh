@@ -8,9 +8,11 @@
 //   ResidualIntIterator (BVMultiGraph.java:655-707);
 //   EvolvingMultiGraph.SuccessorIterator (EvolvingMultiGraph.java:396-443) for timestamps.
 //
-// A reference chain of depth <= 3 is decoded with one state block per level; levels are
-// template parameters so every field access is static.  The referenced lists are decoded only
-// as far as the copy mask needs them.  Exhausted sub-iterators hold kInf, which is never a
+// Layout of the state: the list being decoded (level 0) lives in registers and its merge step is
+// inlined into every kernel.  A reference chain (levels 1..3, maxrefcount 3) is only needed for
+// the copied successors, so its state sits in a DeepState in local memory and is advanced by a
+// few out-of-line routines; this keeps the hot loop small (the whole chain inlined at every call
+// site overflowed the instruction cache).  Exhausted sub-iterators hold kInf, which is never a
 // vertex id (the reference decoder uses MAX_LABEL and breaks on a successor equal to it,
 // gpu_cuda/shared/bfs.cu:763-776).
 #pragma once
@@ -18,99 +20,48 @@
 
 namespace tga {
 
-struct LevelState {
-  uint64_t mpos, ipos, rpos, bpos;
+// One successor list being merged.
+struct ListState {
+  uint64_t mpos, ipos, rpos;
   int hm, hi, hr, hc;        // heads of multiples, intervals, residuals, copied values
   int mleft, mrem;           // multiples runs still to read, copies left of the current run
   int ileft, iend;           // intervals still to read, end (exclusive) of the current one
   int rleft;                 // residuals left including the head
-  int bleft, cur_left;       // copy blocks still to read, values left in the current copy block
-                             // (-1: copy everything that remains)
-  int x;                     // vertex whose list this level decodes
-  int emitted;               // values of this list returned so far
+  int x;                     // vertex whose list this is
+  int emitted;               // values returned so far (maintained below level 0)
 };
 
-struct ChainState {
-  LevelState lv[kMaxLevels];
+// Copy mask of one level over the next level's list.
+struct MaskState {
+  uint64_t bpos;             // next block length in the stream
+  int bleft;                 // blocks still to read
+  int cur_left;              // values left in the current copy block (-1: copy all that remains)
+};
+
+// Levels 1..kMaxLevels-1 of a reference chain (lv[j] is level j+1) and the masks of levels
+// 0..kMaxLevels-2 (mask[j] selects from lv[j]).
+struct DeepState {
+  MaskState mask[kMaxLevels - 1];
+  ListState lv[kMaxLevels - 1];
 };
 
 // Complete decoder state at one edge of a long list (see slices.cuh).
 struct SliceState {
-  ChainState cs;
+  ListState top;
+  DeepState deep;   // meaningful only when chain != 0
   uint64_t tpos;    // bit position of the slice's first timestamp code
   int64_t prev;     // timestamp preceding the slice's first edge
   int32_t v;        // vertex
   int32_t count;    // edges in the slice
   int32_t first;    // index of the slice's first edge in the list of v
-  int32_t pad;
+  int32_t chain;    // the list copies from a reference chain
 };
 
-template <int L>
-__device__ __forceinline__ int list_next(const GraphView& g, ChainState& s);
+// ---- merge step shared by all levels ---------------------------------------------------------
 
-// Skips k values of the list decoded at level L.  A long skip over a list that has slice
-// checkpoints restores the last checkpoint at or before the target (its levels 0.. become levels
-// L.. here: a list referenced at level L has a chain of at most kMaxLevels-1-L further levels),
-// so the walk is bounded by one slice instead of the skip length.
-template <int L>
-__device__ __forceinline__ void skip_values(const GraphView& g, ChainState& s, int k) {
-  LevelState& st = s.lv[L];
-  if (L > 0 && k > g.seek_min && g.slice_first) {
-    const int a = g.slice_first[st.x], b = g.slice_first[st.x + 1];
-    const int target = st.emitted + k;
-    if (b - a > 1) {
-      int lo = a, hi = b - 1;  // last slice with first <= target
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (g.slices[mid].first <= target) lo = mid;
-        else hi = mid - 1;
-      }
-      const SliceState& cp = g.slices[lo];
-      if (cp.first > st.emitted) {
-        s.lv[L] = cp.cs.lv[0];
-        if constexpr (L + 1 < kMaxLevels) s.lv[L + 1] = cp.cs.lv[1];
-        if constexpr (L + 2 < kMaxLevels) s.lv[L + 2] = cp.cs.lv[2];
-        if constexpr (L + 3 < kMaxLevels) s.lv[L + 3] = cp.cs.lv[3];
-        k = target - cp.first;
-      }
-    }
-  }
-  for (int i = 0; i < k && i <= g.max_list; ++i)
-    if (list_next<L>(g, s) == kInf) break;
-}
-
-template <int L>
-__device__ __forceinline__ int masked_next(const GraphView& g, ChainState& s) {
-  if constexpr (L + 1 < kMaxLevels) {
-    LevelState& st = s.lv[L];
-    if (st.cur_left == 0) return kInf;
-    const int v = list_next<L + 1>(g, s);
-    if (v == kInf) return kInf;
-    if (st.cur_left > 0) {
-      --st.cur_left;
-      if (st.cur_left == 0 && st.bleft > 0) {
-        const int skip = (int)read_gamma(g, g.g, st.bpos) + 1;
-        --st.bleft;
-        skip_values<L + 1>(g, s, skip);
-        if (st.bleft > 0) {
-          st.cur_left = (int)read_gamma(g, g.g, st.bpos) + 1;
-          --st.bleft;
-        } else {
-          st.cur_left = -1;
-        }
-      }
-    }
-    return v;
-  } else {
-    return kInf;
-  }
-}
-
-template <int L>
-__device__ __forceinline__ int list_next(const GraphView& g, ChainState& s) {
-  LevelState& st = s.lv[L];
-  const int v = min(min(st.hm, st.hi), min(st.hr, st.hc));
-  if (v == kInf) return kInf;
+// Advances the sub-iterators whose head equals v (equal heads are emitted once, as
+// MergedIntIterator does).  Returns true if the copied-values head must advance too.
+__device__ __forceinline__ bool merge_advance(const GraphView& g, ListState& st, int v) {
   if (st.hm == v) {
     if (--st.mrem == 0) {
       if (st.mleft > 0) {
@@ -137,71 +88,47 @@ __device__ __forceinline__ int list_next(const GraphView& g, ChainState& s) {
     if (--st.rleft > 0) st.hr += (int)read_zeta<3>(g, g.g, st.rpos) + 1;
     else st.hr = kInf;
   }
-  if constexpr (L + 1 < kMaxLevels) {
-    if (st.hc == v) st.hc = masked_next<L>(g, s);
-  }
-  ++st.emitted;
-  return v;
+  return st.hc == v;
 }
 
-// Parses the record of vertex x into level L; returns its outdegree.
-template <int L>
-__device__ __forceinline__ int level_init(const GraphView& g, ChainState& s, int x) {
-  LevelState& st = s.lv[L];
+// Header of the record of x: outdegree, reference, copy blocks (scanned).  Returns the outdegree
+// (0 for an empty list, -1 for a corrupt record); *ref, *bc, *copied, *total describe the copy
+// part, mask.bpos points at the first block, pos just past the blocks.
+__device__ __forceinline__ int parse_record(const GraphView& g, ListState& st, MaskState& mask, int x, int& ref,
+                                            int& bc, int& copied, int& total, uint64_t& pos) {
   st.hm = st.hi = st.hr = st.hc = kInf;
   st.rleft = 0;
   st.x = x;
   st.emitted = 0;
-  if (x < 0 || x >= g.n) { set_err(g, kErrId); return 0; }
-  uint64_t pos = ef_get(g, g.gef, (uint64_t)x);
+  ref = 0;
+  bc = 0;
+  copied = total = 0;
+  if (x < 0 || x >= g.n) { set_err(g, kErrId); return -1; }
+  pos = ef_get(g, g.gef, (uint64_t)x);
   const int d = (int)read_gamma(g, g.g, pos);
   if (d == 0) return 0;
-  if (d < 0 || d > g.max_list) { set_err(g, kErrCode); return 0; }
-  const int ref = (int)read_unary(g, g.g, pos);
-  int extra = d;
+  if (d < 0 || d > g.max_list) { set_err(g, kErrCode); return -1; }
+  ref = (int)read_unary(g, g.g, pos);
   if (ref > 0) {
-    if constexpr (L + 1 < kMaxLevels) {
-      const int bc = (int)read_gamma(g, g.g, pos);
-      // A copy mask alternates copy/skip blocks over the referenced list, so a valid record
-      // has at most 2*(its degree + the referenced degree)+1 blocks; anything larger is corrupt.
-      if (bc < 0 || bc > 2 * d + 2 * g.max_list + 1) { set_err(g, kErrCode); return 0; }
-      st.bpos = pos;
-      int total = 0, copied = 0;
-      for (int i = 0; i < bc; ++i) {
-        const int b = (int)read_gamma(g, g.g, pos) + (i ? 1 : 0);
-        total += b;
-        if (!(i & 1)) copied += b;
-      }
-      const int dref = level_init<L + 1>(g, s, x - ref);
-      if (!(bc & 1)) copied += dref - total;
-      extra = d - copied;
-      if (bc == 0) {
-        st.cur_left = -1;
-        st.bleft = 0;
-      } else {
-        st.cur_left = (int)read_gamma(g, g.g, st.bpos);
-        st.bleft = bc - 1;
-        if (st.cur_left == 0 && st.bleft > 0) {
-          const int skip = (int)read_gamma(g, g.g, st.bpos) + 1;
-          --st.bleft;
-          skip_values<L + 1>(g, s, skip);
-          if (st.bleft > 0) {
-            st.cur_left = (int)read_gamma(g, g.g, st.bpos) + 1;
-            --st.bleft;
-          } else {
-            st.cur_left = -1;
-          }
-        }
-      }
-      st.hc = masked_next<L>(g, s);
-    } else {
-      set_err(g, kErrChain);
-      return 0;
+    bc = (int)read_gamma(g, g.g, pos);
+    // A copy mask alternates copy/skip blocks over the referenced list, so a valid record has at
+    // most 2*(its degree + the largest degree)+1 blocks; anything larger is corrupt.
+    if (bc < 0 || bc > 2 * d + 2 * g.max_list + 1) { set_err(g, kErrCode); return -1; }
+    mask.bpos = pos;
+    for (int i = 0; i < bc; ++i) {
+      const int b = (int)read_gamma(g, g.g, pos) + (i ? 1 : 0);
+      total += b;
+      if (!(i & 1)) copied += b;
     }
   }
+  return d;
+}
+
+// Multiples, intervals and residuals of a record; `extra` = outdegree minus copied values.
+__device__ __forceinline__ bool parse_extra(const GraphView& g, ListState& st, int x, int d, int extra, uint64_t pos) {
   if (extra > 0) {
     const int mc = (int)read_gamma(g, g.g, pos);
-    if (mc < 0 || mc > d) { set_err(g, kErrCode); return 0; }
+    if (mc < 0 || mc > d) { set_err(g, kErrCode); return false; }
     if (mc) {
       st.mpos = pos;
       for (int i = 0; i < mc; ++i) {
@@ -215,7 +142,7 @@ __device__ __forceinline__ int level_init(const GraphView& g, ChainState& s, int
   }
   if (extra > 0) {
     const int ic = (int)read_gamma(g, g.g, pos);
-    if (ic < 0 || ic > d) { set_err(g, kErrCode); return 0; }
+    if (ic < 0 || ic > d) { set_err(g, kErrCode); return false; }
     if (ic) {
       st.ipos = pos;
       for (int i = 0; i < ic; ++i) {
@@ -232,23 +159,211 @@ __device__ __forceinline__ int level_init(const GraphView& g, ChainState& s, int
     st.rpos = pos;
     st.hr = x + (int)d_nat2int(read_zeta<3>(g, g.g, st.rpos));
   }
+  return true;
+}
+
+// ---- reference-chain levels (local memory, out of line) ---------------------------------------
+
+template <int L>
+__device__ __forceinline__ int deep_next(const GraphView& g, DeepState& d);
+
+// Skips k values of level L (>= 1).  A long skip over a list that has slice checkpoints restores
+// the last checkpoint at or before the target: the checkpoint's level 0 becomes level L and its
+// chain levels L+1.. (a list referenced at level L has at most kMaxLevels-1-L further levels), so
+// the walk is bounded by one slice instead of the skip length.
+template <int L>
+__device__ __forceinline__ void deep_skip(const GraphView& g, DeepState& d, int k) {
+  ListState& st = d.lv[L - 1];
+  if (k > g.seek_min && g.slice_first) {
+    const int a = g.slice_first[st.x], b = g.slice_first[st.x + 1];
+    const int target = st.emitted + k;
+    if (b - a > 1) {
+      int lo = a, hi = b - 1;  // last slice with first <= target
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (g.slices[mid].first <= target) lo = mid;
+        else hi = mid - 1;
+      }
+      const SliceState& cp = g.slices[lo];
+      if (cp.first > st.emitted) {
+        d.lv[L - 1] = cp.top;
+        d.lv[L - 1].x = cp.v;
+        d.lv[L - 1].emitted = cp.first;
+        if (cp.chain) {
+          if constexpr (L < kMaxLevels - 1) {
+            d.mask[L] = cp.deep.mask[0];
+            d.lv[L] = cp.deep.lv[0];
+          }
+          if constexpr (L + 1 < kMaxLevels - 1) {
+            d.mask[L + 1] = cp.deep.mask[1];
+            d.lv[L + 1] = cp.deep.lv[1];
+          }
+        }
+        k = target - cp.first;
+      }
+    }
+  }
+  for (int i = 0; i < k && i <= g.max_list; ++i)
+    if (deep_next<L>(g, d) == kInf) break;
+}
+
+// Next value selected by the copy mask of level M (0..kMaxLevels-2) over level M+1.
+template <int M>
+__device__ __forceinline__ int deep_masked(const GraphView& g, DeepState& d) {
+  MaskState& mk = d.mask[M];
+  if (mk.cur_left == 0) return kInf;
+  const int v = deep_next<M + 1>(g, d);
+  if (v == kInf) return kInf;
+  if (mk.cur_left > 0) {
+    --mk.cur_left;
+    if (mk.cur_left == 0 && mk.bleft > 0) {
+      const int skip = (int)read_gamma(g, g.g, mk.bpos) + 1;
+      --mk.bleft;
+      deep_skip<M + 1>(g, d, skip);
+      if (mk.bleft > 0) {
+        mk.cur_left = (int)read_gamma(g, g.g, mk.bpos) + 1;
+        --mk.bleft;
+      } else {
+        mk.cur_left = -1;
+      }
+    }
+  }
+  return v;
+}
+
+template <int L>
+__device__ __forceinline__ int deep_next(const GraphView& g, DeepState& d) {
+  ListState& st = d.lv[L - 1];
+  const int v = min(min(st.hm, st.hi), min(st.hr, st.hc));
+  if (v == kInf) return kInf;
+  if (merge_advance(g, st, v)) {
+    if constexpr (L < kMaxLevels - 1) st.hc = deep_masked<L>(g, d);
+    else st.hc = kInf;
+  }
+  ++st.emitted;
+  return v;
+}
+
+// Starts the copy mask of level M (bc blocks at mask[M].bpos): first block read, a leading empty
+// copy block skipped.
+template <int M>
+__device__ __forceinline__ void mask_start(const GraphView& g, DeepState& d, int bc) {
+  MaskState& mk = d.mask[M];
+  if (bc == 0) {
+    mk.cur_left = -1;
+    mk.bleft = 0;
+    return;
+  }
+  mk.cur_left = (int)read_gamma(g, g.g, mk.bpos);
+  mk.bleft = bc - 1;
+  if (mk.cur_left == 0 && mk.bleft > 0) {
+    const int skip = (int)read_gamma(g, g.g, mk.bpos) + 1;
+    --mk.bleft;
+    deep_skip<M + 1>(g, d, skip);
+    if (mk.bleft > 0) {
+      mk.cur_left = (int)read_gamma(g, g.g, mk.bpos) + 1;
+      --mk.bleft;
+    } else {
+      mk.cur_left = -1;
+    }
+  }
+}
+
+// Opens level L (>= 1) on vertex x; returns its outdegree.
+template <int L>
+__device__ __forceinline__ int deep_open(const GraphView& g, DeepState& d, int x) {
+  ListState& st = d.lv[L - 1];
+  int ref, bc, copied, total;
+  uint64_t pos;
+  MaskState own;
+  const int dd = parse_record(g, st, own, x, ref, bc, copied, total, pos);
+  if (dd <= 0) return 0;
+  int extra = dd;
+  if (ref > 0) {
+    if constexpr (L < kMaxLevels - 1) {
+      const int dref = deep_open<L + 1>(g, d, x - ref);
+      if (!(bc & 1)) copied += dref - total;
+      extra = dd - copied;
+      d.mask[L] = own;
+      mask_start<L>(g, d, bc);
+      st.hc = deep_masked<L>(g, d);
+    } else {
+      set_err(g, kErrChain);
+      return 0;
+    }
+  }
+  if (!parse_extra(g, st, x, dd, extra, pos)) return 0;
+  return dd;
+}
+
+// Out-of-line entry points used by level 0.
+struct OpenRef {
+  int dref;   // outdegree of the referenced list
+  int head;   // first copied value (kInf if none)
+};
+
+static __device__ __noinline__ OpenRef deep_open_ref(const GraphView& g, DeepState& d, int xref, int bc, uint64_t bpos) {
+  OpenRef r;
+  r.dref = deep_open<1>(g, d, xref);
+  d.mask[0].bpos = bpos;
+  mask_start<0>(g, d, bc);
+  r.head = deep_masked<0>(g, d);
+  return r;
+}
+
+static __device__ __noinline__ int deep_copy_next(const GraphView& g, DeepState& d) { return deep_masked<0>(g, d); }
+
+// ---- level 0 --------------------------------------------------------------------------------
+
+__device__ __forceinline__ int top_next(const GraphView& g, ListState& st, DeepState* deep) {
+  const int v = min(min(st.hm, st.hi), min(st.hr, st.hc));
+  if (v == kInf) return kInf;
+  if (merge_advance(g, st, v)) st.hc = deep_copy_next(g, *deep);
+  return v;
+}
+
+// Parses the record of x into level 0 (and its reference chain); returns the outdegree.
+// *chain is set when the list copies from a reference chain.
+__device__ __forceinline__ int top_open(const GraphView& g, ListState& st, DeepState* deep, int x, int& chain) {
+  int ref, bc, copied, total;
+  uint64_t pos;
+  MaskState mk;
+  const int d = parse_record(g, st, mk, x, ref, bc, copied, total, pos);
+  chain = 0;
+  if (d <= 0) return 0;
+  int extra = d;
+  if (ref > 0) {
+    chain = 1;
+    const OpenRef r = deep_open_ref(g, *deep, x - ref, bc, mk.bpos);
+    if (!(bc & 1)) copied += r.dref - total;
+    extra = d - copied;
+    st.hc = r.head;
+  }
+  if (!parse_extra(g, st, x, d, extra, pos)) return 0;
   return d;
 }
 
 // Temporal edge iterator of one vertex: successor ids in list order with their timestamps.
+// The reference-chain state lives in a separate local object (see the file comment), so that the
+// cursor's own fields stay in registers.
 struct EdgeCursor {
-  ChainState cs;
+  ListState top;
+  DeepState* deep;
   SeqReader ts;
   int64_t prev;
   int remaining;
   int x;
+  int chain;
+
+  __device__ __forceinline__ explicit EdgeCursor(DeepState* d) : deep(d) {}
 
   // Returns the outdegree.
   __device__ __forceinline__ int open(const GraphView& g, int v) {
     x = v;
     remaining = 0;
+    chain = 0;
     if (v >= g.n) return 0;  // ids past the files' vertex count have empty lists
-    remaining = level_init<0>(g, cs, v);
+    remaining = top_open(g, top, deep, v, chain);
     if (remaining > 0) {
       ts.init(g.t, ef_get(g, g.tef, (uint64_t)v));
       prev = g.min_ts;
@@ -259,7 +374,7 @@ struct EdgeCursor {
   __device__ __forceinline__ bool next(const GraphView& g, int& y, int64_t& t) {
     if (remaining <= 0) return false;
     --remaining;
-    y = list_next<0>(g, cs);
+    y = top_next(g, top, deep);
     int len = 0;
     bool bad = false;
     const uint64_t z = win_zeta<2>(ts.window(), &len, &bad);

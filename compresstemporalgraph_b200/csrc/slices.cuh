@@ -21,7 +21,9 @@ struct WorkItem {
 };
 
 __device__ __forceinline__ void cursor_restore(const GraphView& g, EdgeCursor& c, const SliceState& s) {
-  c.cs = s.cs;
+  c.top = s.top;
+  c.chain = s.chain;
+  if (s.chain) *c.deep = s.deep;
   c.ts.init(g.t, s.tpos);
   c.prev = s.prev;
   c.remaining = s.count;
@@ -29,7 +31,9 @@ __device__ __forceinline__ void cursor_restore(const GraphView& g, EdgeCursor& c
 }
 
 __device__ __forceinline__ void cursor_save(const EdgeCursor& c, SliceState& s, int v, int first) {
-  s.cs = c.cs;
+  s.top = c.top;
+  s.chain = c.chain;
+  if (c.chain) s.deep = *c.deep;
   s.tpos = c.ts.pos();
   s.prev = c.prev;
   s.v = v;
@@ -46,14 +50,19 @@ static __global__ void k_build_slices(GraphView g, const int32_t* big_v, const i
   const int v = big_v[b];
   SliceState* dst = out + slot_base[b];
   const int cap = (int)(slot_base[b + 1] - slot_base[b]);
-  EdgeCursor c;
+  DeepState deep, saved_deep;
+  EdgeCursor c(&deep);
   const int d = c.open(g, v);
   cursor_save(c, dst[0], v, 0);
   int k = 1, last = 0, prev_y = -1;
   for (int i = 0; i < d; ++i) {
     const bool cand = (i - last >= len) && k < cap;
-    EdgeCursor saved;
-    if (cand) saved = c;
+    EdgeCursor saved(&saved_deep);
+    if (cand) {
+      saved = c;
+      saved.deep = &saved_deep;
+      if (c.chain) saved_deep = deep;
+    }
     int y;
     int64_t t;
     if (!c.next(g, y, t)) break;
