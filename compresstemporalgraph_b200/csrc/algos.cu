@@ -2,9 +2,12 @@
 // successor lists and timestamps it needs straight from the compressed streams; decoded edges
 // live only in registers.
 //
-// Work decomposition (slices.cuh): sweeps over all lists run one thread per work item (a run of
-// short lists or one slice of a long list); frontier kernels expand a long list into its slices
-// when they enqueue it.  Queue entries are vertex ids (>= 0) or -(slice + 1).
+// Work decomposition (slices.cuh): lists longer than a slice are cut into resumable slices, short
+// lists are grouped into work items.  Every decode kernel is persistent: each thread pulls work
+// (an item, or a queue entry = a vertex id >= 0 or -(slice + 1)) from an atomic counter and runs
+// a flat loop in which one iteration either decodes one edge of its current list or opens the
+// next list.  Lanes of a warp therefore never wait for a neighbour's longer list at a list
+// boundary, which with power-law outdegrees would leave most lanes idle.
 #include <curand_kernel.h>
 
 #include <algorithm>
@@ -22,6 +25,8 @@ constexpr uint32_t kColorInf = 0xFFFFFFFFu;
 
 // Launches a kernel of kBlock threads on the handle's stream and counts it in the call's timing.
 #define KL(kernel, grid) ++h.timing.launches, kernel<<<(grid), kBlock, 0, h.stream>>>
+// Decode kernels: 2 blocks of 256 threads per SM (128 registers, no spills).
+#define TGA_DECODE_BOUNDS __launch_bounds__(kBlock, 2)
 
 // Per-edge term of the neighbour-access checksum: the checksum of a list is the sum (mod 2^64)
 // of edge_hash over its edges, so slices can add their parts; the edge index keeps it
@@ -59,17 +64,21 @@ struct Work {
   const WorkItem* items;
   const SliceState* slices;
   const int32_t* slice_first;
+  int32_t* next;          // work counter of the launch (zeroed before it)
   int32_t nitems;
 };
 
 // Opens queue entry e: a whole list (e >= 0) or one slice.  Returns the vertex.
-__device__ __forceinline__ int open_entry(const GraphView& g, const Work& w, int e, EdgeCursor& c, int& count) {
+__device__ __forceinline__ int open_entry(const GraphView& g, const Work& w, int e, EdgeCursor& c, int& first,
+                                          int& count) {
   if (e >= 0) {
+    first = 0;
     count = c.open(g, e);
     return e;
   }
   const SliceState& s = w.slices[-e - 1];
   cursor_restore(g, c, s);
+  first = s.first;
   count = s.count;
   return s.v;
 }
@@ -85,28 +94,102 @@ __device__ __forceinline__ void enqueue(const Work& w, int y, int32_t* q, int32_
   }
 }
 
-// Runs `body(c, v, first, count)` for work item i: every vertex of a run of short lists that
-// `want(v)`, or one slice.  Returns the edges handed to the body.
-template <class Want, class Body>
-__device__ __forceinline__ unsigned long long sweep_item(const GraphView& g, const Work& w, int i, Want want, Body body) {
-  const WorkItem it = w.items[i];
+// Edge filter shared by every traversal: in-window, first of equal consecutive successors,
+// successor inside [active_begin, max_vertex).
+__device__ __forceinline__ bool keep_edge(const GraphView& g, int64_t lo, int64_t hi, int y, int64_t t, int& prev_y) {
+  if (t < lo || t >= hi) return false;
+  if (y == prev_y) return false;
+  prev_y = y;
+  return y >= g.active_begin && y < g.max_vertex;
+}
+
+// Flat loop over work items.  Hooks (each inlined at its single call site):
+//   want(x) -> bool, begin(x, first, count) -> bool (false: skip the list),
+//   edge(x, y, t) -> bool (false: stop this list), end(x).
+// kWhole: a sliced list is decoded whole by the thread that draws its first slice (for workloads
+// that are sequential per list); its other slices are skipped.  Returns the edges decoded.
+template <bool kWhole, class Want, class Begin, class Edge, class End>
+__device__ __forceinline__ unsigned long long drive_items(const GraphView& g, const Work& w, Want want, Begin begin,
+                                                          Edge edge, End end) {
+  DeepState deep;
+  EdgeCursor c(&deep);
+  c.remaining = 0;
+  int v = 0, vend = 0, slice = -1, cur = -1;
   unsigned long long edges = 0;
-  const int vend = it.slice >= 0 ? it.v0 + 1 : it.v1;
-  for (int v = it.v0; v < vend; ++v) {  // one call site keeps the body inlined and the cursor in registers
-    if (!want(v)) continue;
-    DeepState deep_;
-    EdgeCursor c(&deep_);
-    int first = 0, count;
-    if (it.slice >= 0) {
-      const SliceState& s = w.slices[it.slice];
-      cursor_restore(g, c, s);
-      first = s.first;
-      count = s.count;
-    } else {
-      count = c.open(g, v);
+  for (;;) {
+    if (c.remaining <= 0) {
+      if (cur >= 0) {
+        end(cur);
+        cur = -1;
+      }
+      if (v >= vend) {
+        const int i = atomicAdd(w.next, 1);
+        if (i >= w.nitems) break;
+        const WorkItem it = w.items[i];
+        v = it.v0;
+        vend = it.slice >= 0 ? it.v0 + 1 : it.v1;
+        slice = it.slice;
+        if (kWhole && slice >= 0 && w.slices[slice].first != 0) v = vend;
+        continue;
+      }
+      const int x = v++;
+      if (!want(x)) continue;
+      int first = 0, count;
+      if (!kWhole && slice >= 0) {
+        const SliceState& s = w.slices[slice];
+        cursor_restore(g, c, s);
+        first = s.first;
+        count = s.count;
+      } else {
+        count = c.open(g, x);
+      }
+      if (count <= 0 || !begin(x, first, count)) {
+        c.remaining = 0;
+        continue;
+      }
+      cur = x;
+      continue;
     }
-    edges += (unsigned long long)count;
-    body(c, v, first, count);
+    int y;
+    int64_t t;
+    if (!c.next(g, y, t)) continue;
+    ++edges;
+    if (!edge(cur, y, t)) c.remaining = 0;
+  }
+  return edges;
+}
+
+// Flat loop over the entries q[0..qn) of a queue (vertices or slices).
+template <class Begin, class Edge, class End>
+__device__ __forceinline__ unsigned long long drive_queue(const GraphView& g, const Work& w, const int32_t* q, int qn,
+                                                          Begin begin, Edge edge, End end) {
+  DeepState deep;
+  EdgeCursor c(&deep);
+  c.remaining = 0;
+  int cur = -1;
+  unsigned long long edges = 0;
+  for (;;) {
+    if (c.remaining <= 0) {
+      if (cur >= 0) {
+        end(cur);
+        cur = -1;
+      }
+      const int i = atomicAdd(w.next, 1);
+      if (i >= qn) break;
+      int first, count;
+      const int x = open_entry(g, w, q[i], c, first, count);
+      if (count <= 0 || !begin(x, first, count)) {
+        c.remaining = 0;
+        continue;
+      }
+      cur = x;
+      continue;
+    }
+    int y;
+    int64_t t;
+    if (!c.next(g, y, t)) continue;
+    ++edges;
+    if (!edge(cur, y, t)) c.remaining = 0;
   }
   return edges;
 }
@@ -114,22 +197,22 @@ __device__ __forceinline__ unsigned long long sweep_item(const GraphView& g, con
 // ---------------------------------------------------------------------------------------------
 // Neighbour access and raw decode
 
-__global__ void __launch_bounds__(kBlock, 2) k_neighbor_access(GraphView g, Work w, int32_t begin, int32_t end,
-                                                            unsigned long long* csum, unsigned long long* edges) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  unsigned long long mine = 0;
-  if (i < w.nitems) {
-    mine = sweep_item(
-        g, w, i, [&](int v) { return v >= begin && v < end; },
-        [&](EdgeCursor& c, int v, int first, int) {
-          uint64_t h = 0;
-          uint32_t k = (uint32_t)first;
-          int y;
-          int64_t t;
-          while (c.next(g, y, t)) h += edge_hash((uint32_t)v, k++, y, t);
-          atomicAdd(&csum[v], (unsigned long long)h);
-        });
-  }
+__global__ void TGA_DECODE_BOUNDS k_neighbor_access(GraphView g, Work w, int32_t begin, int32_t end,
+                                                    unsigned long long* csum, unsigned long long* edges) {
+  uint64_t h = 0;
+  uint32_t k = 0;
+  const unsigned long long mine = drive_items<false>(
+      g, w, [&](int v) { return v >= begin && v < end; },
+      [&](int, int first, int) {
+        h = 0;
+        k = (uint32_t)first;
+        return true;
+      },
+      [&](int v, int y, int64_t t) {
+        h += edge_hash((uint32_t)v, k++, y, t);
+        return true;
+      },
+      [&](int v) { atomicAdd(&csum[v], (unsigned long long)h); });
   add_edges(edges, mine);
 }
 
@@ -138,30 +221,37 @@ __global__ void k_small_flags(const int32_t* deg, uint8_t* small, int32_t begin,
   if (v < end) small[v] = deg[v] < 4;
 }
 
-__global__ void k_decode_csr(GraphView g, Work w, const int64_t* off, int32_t* dst, int64_t* ts, int64_t cap) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= w.nitems) return;
-  sweep_item(
-      g, w, i, [&](int) { return true; },
-      [&](EdgeCursor& c, int v, int first, int) {
-        int64_t o = off[v] + first;
-        int y;
-        int64_t t;
-        while (c.next(g, y, t)) {
-          if (o < cap) { dst[o] = y; ts[o] = t; }
-          ++o;
+__global__ void TGA_DECODE_BOUNDS k_decode_csr(GraphView g, Work w, const int64_t* off, int32_t* dst, int64_t* ts,
+                                               int64_t cap) {
+  int64_t o = 0;
+  drive_items<false>(
+      g, w, [&](int) { return true; },
+      [&](int v, int first, int) {
+        o = off[v] + first;
+        return true;
+      },
+      [&](int, int y, int64_t t) {
+        if (o < cap) {
+          dst[o] = y;
+          ts[o] = t;
         }
-      });
+        ++o;
+        return true;
+      },
+      [&](int) {});
 }
 
 __global__ void k_neighbors(GraphView g, int32_t v, int32_t* dst, int64_t* ts, int32_t cap, int32_t* count) {
-  DeepState deep_;
-  EdgeCursor c(&deep_);
+  DeepState deep;
+  EdgeCursor c(&deep);
   const int d = c.open(g, v);
   int i = 0, y;
   int64_t t;
   while (c.next(g, y, t)) {
-    if (i < cap) { dst[i] = y; ts[i] = t; }
+    if (i < cap) {
+      dst[i] = y;
+      ts[i] = t;
+    }
     ++i;
   }
   *count = d;
@@ -183,68 +273,56 @@ struct BfsArgs {
   unsigned long long* edges;
 };
 
-// Edge filter shared by every traversal: in-window, first of equal consecutive successors,
-// successor inside [active_begin, max_vertex).
-#define TGA_EDGE_FILTER(g, lo, hi, y, t, prev_y)                          \
-  if ((t) < (lo) || (t) >= (hi)) continue;                                \
-  if ((y) == (prev_y)) continue;                                          \
-  (prev_y) = (y);                                                         \
-  if ((y) < (g).active_begin || (y) >= (g).max_vertex) continue;
-
 // Phase 1: tp[v] holds arrival << 32, so the 64-bit atomicMin is an arrival minimum; a vertex
 // whose arrival drops is enqueued once per level (stamp) and relaxes its successors again.
-__global__ void __launch_bounds__(kBlock, 2) k_bfs_level(GraphView g, Work w, BfsArgs a, int32_t qn) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  unsigned long long mine = 0;
-  if (i < qn) {
-    DeepState deep_;
-    EdgeCursor c(&deep_);
-    int cnt;
-    const int x = open_entry(g, w, a.q[i], c, cnt);
-    if (x >= g.active_begin && x <= g.max_label) {
-      const uint32_t ax = (uint32_t)(a.tp[x] >> 32);
-      mine = (unsigned long long)cnt;
-      int y, prev_y = -1;
-      int64_t t;
-      while (c.next(g, y, t)) {
-        TGA_EDGE_FILTER(g, a.lo, a.hi, y, t, prev_y)
-        if ((int64_t)ax > t || t >= 0xFFFFFFFFll) continue;
+__global__ void TGA_DECODE_BOUNDS k_bfs_level(GraphView g, Work w, BfsArgs a, int32_t qn) {
+  uint32_t ax = 0;
+  int prev_y = -1;
+  const unsigned long long mine = drive_queue(
+      g, w, a.q, qn,
+      [&](int x, int, int) {
+        if (x < g.active_begin || x > g.max_label) return false;
+        ax = (uint32_t)(a.tp[x] >> 32);
+        prev_y = -1;
+        return true;
+      },
+      [&](int, int y, int64_t t) {
+        if (!keep_edge(g, a.lo, a.hi, y, t, prev_y)) return true;
+        if ((int64_t)ax > t || t >= 0xFFFFFFFFll) return true;
         const uint64_t nv = (uint64_t)t << 32;
         const uint64_t old = atomicMin((unsigned long long*)&a.tp[y], (unsigned long long)nv);
         if (nv < old) {
           if (a.touched && (old >> 32) == 0xFFFFFFFFull) a.touched[atomicAdd(a.tcnt, 1)] = y;
           if (atomicMax(&a.stamp[y], a.wave) < a.wave) enqueue(w, y, a.nq, a.ncnt);
         }
-      }
-    }
-  }
+        return true;
+      },
+      [&](int) {});
   add_edges(a.edges, mine);
 }
 
 // Phase 2: with the final arrivals fixed, an edge passing the same filters is tight when
 // arrival(x) <= t == arrival(y); hops = BFS level over tight edges, each vertex claimed once.
-__global__ void __launch_bounds__(kBlock, 2) k_bfs_hops(GraphView g, Work w, BfsArgs a, int32_t qn, uint32_t* hops,
-                                                     uint32_t level) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  unsigned long long mine = 0;
-  if (i < qn) {
-    DeepState deep_;
-    EdgeCursor c(&deep_);
-    int cnt;
-    const int x = open_entry(g, w, a.q[i], c, cnt);
-    if (x >= g.active_begin && x <= g.max_label) {
-      const uint32_t ax = (uint32_t)(a.tp[x] >> 32);
-      mine = (unsigned long long)cnt;
-      int y, prev_y = -1;
-      int64_t t;
-      while (c.next(g, y, t)) {
-        TGA_EDGE_FILTER(g, a.lo, a.hi, y, t, prev_y)
-        if ((int64_t)ax > t || t >= 0xFFFFFFFFll) continue;
-        if ((int64_t)(a.tp[y] >> 32) != t) continue;
+__global__ void TGA_DECODE_BOUNDS k_bfs_hops(GraphView g, Work w, BfsArgs a, int32_t qn, uint32_t* hops,
+                                             uint32_t level) {
+  uint32_t ax = 0;
+  int prev_y = -1;
+  const unsigned long long mine = drive_queue(
+      g, w, a.q, qn,
+      [&](int x, int, int) {
+        if (x < g.active_begin || x > g.max_label) return false;
+        ax = (uint32_t)(a.tp[x] >> 32);
+        prev_y = -1;
+        return true;
+      },
+      [&](int, int y, int64_t t) {
+        if (!keep_edge(g, a.lo, a.hi, y, t, prev_y)) return true;
+        if ((int64_t)ax > t || t >= 0xFFFFFFFFll) return true;
+        if ((int64_t)(a.tp[y] >> 32) != t) return true;
         if (atomicCAS(&hops[y], 0xFFFFFFFFu, level + 1) == 0xFFFFFFFFu) enqueue(w, y, a.nq, a.ncnt);
-      }
-    }
-  }
+        return true;
+      },
+      [&](int) {});
   add_edges(a.edges, mine);
 }
 
@@ -269,55 +347,6 @@ __global__ void k_unpack_bfs(const uint64_t* tp, const uint32_t* hops_in, int32_
   arr[i] = inf ? INT32_MAX : (int32_t)(wd >> 32);
   const uint32_t hv = hops_in[i];
   hops[i] = (inf || hv == 0xFFFFFFFFu) ? INT32_MAX : (int32_t)hv;
-}
-
-// Host side: the queue entries of one vertex (itself or its slices).
-static int32_t seed_entries(const GraphHandle& h, int32_t v, std::vector<int32_t>& out) {
-  out.clear();
-  const int32_t a = h.slice_first_host[(size_t)v], b = h.slice_first_host[(size_t)v + 1];
-  if (a == b) out.push_back(v);
-  else
-    for (int32_t j = a; j < b; ++j) out.push_back(-(j + 1));
-  return (int32_t)out.size();
-}
-
-static Work work_of(const GraphHandle& h) {
-  return Work{h.d_items.as<WorkItem>(), h.d_slices.as<SliceState>(), h.d_slice_first.as<int32_t>(), h.nitems};
-}
-
-// Level loop of phase 1 from an initialised queue of qn entries; returns the levels executed.
-static int run_bfs_levels(GraphHandle& h, BfsArgs a, DevBuf& q0, DevBuf& q1, int32_t qn, uint32_t& wave, int& rc) {
-  int levels = 0;
-  DevBuf* cur = &q0;
-  DevBuf* nxt = &q1;
-  const Work w = work_of(h);
-  rc = TGA_OK;
-  while (qn > 0) {
-    if (levels > (1 << 22)) { rc = fail(TGA_E_TIMEOUT, "BFS level cap reached"); return levels; }
-    a.q = cur->as<int32_t>();
-    a.nq = nxt->as<int32_t>();
-    a.wave = ++wave;
-    cudaMemsetAsync(a.ncnt, 0, sizeof(int32_t), h.stream);
-    cudaEvent_t* ev = h.kernel_begin();
-    KL(k_bfs_level, grid_for(qn, kBlock))(h.view, w, a, qn);
-    h.kernel_end(ev);
-    cudaMemcpyAsync(h.h_pinned, a.ncnt, sizeof(int32_t), cudaMemcpyDeviceToHost, h.stream);
-    if (cudaStreamSynchronize(h.stream) != cudaSuccess) { rc = fail(TGA_E_CUDA, "BFS level failed"); return levels; }
-    qn = (int32_t)h.h_pinned[0];
-    std::swap(cur, nxt);
-    ++levels;
-  }
-  return levels;
-}
-
-static int bfs_buffers(GraphHandle& h) {
-  const size_t nv = (size_t)h.view.max_vertex;
-  const size_t qcap = nv + (size_t)h.nslices + 1;
-  int rc;
-  if ((rc = h.s_a.ensure(nv * 8)) || (rc = h.s_b.ensure(nv * 4)) || (rc = h.s_q0.ensure(qcap * 4)) ||
-      (rc = h.s_q1.ensure(qcap * 4)) || (rc = h.s_cnt.ensure(64)) || (rc = h.s_c.ensure(nv * 4)))
-    return rc;
-  return TGA_OK;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -369,34 +398,35 @@ __device__ __forceinline__ float temporal_weight(float alpha, int64_t t) {
   return a > 18.0f ? 1.0f : 1.0f - expf(-a);
 }
 
-__global__ void __launch_bounds__(kBlock, 2) k_pr_iter(GraphView g, Work w, PrArgs a) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  for (int x = i; x < g.max_vertex; x += gridDim.x * blockDim.x) a.reset[x] = a.base;
-  double local = 0;
-  unsigned long long mine = 0;
-  if (i < w.nitems) {
-    const double s = a.k == 0 ? 1.0 : 1.0 / a.sums[a.k - 1];
-    mine = sweep_item(
-        g, w, i,
-        [&](int v) {
-          if (v < g.active_begin || v >= g.max_label) return false;
-          return a.invdeg ? a.invdeg[v] > 0.0f : a.deg[v] > 0;
-        },
-        [&](EdgeCursor& c, int v, int, int) {
-          const float inv = a.invdeg ? a.invdeg[v] : 1.0f / (float)a.deg[v];
-          const float c0 = a.damping * (float)((double)a.in[v] * s) * inv;
-          int y, prev_y = -1;
-          int64_t t;
-          while (c.next(g, y, t)) {
-            TGA_EDGE_FILTER(g, a.lo, a.hi, y, t, prev_y)
-            const float contrib = c0 * temporal_weight(a.alpha, t);
-            atomicAdd(&a.out[y], contrib);
-            local += contrib;
-          }
-        });
-  }
+__global__ void TGA_DECODE_BOUNDS k_pr_iter(GraphView g, Work w, PrArgs a) {
+  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < g.max_vertex; x += gridDim.x * blockDim.x) a.reset[x] = a.base;
+  const double s = a.k == 0 ? 1.0 : 1.0 / a.sums[a.k - 1];
+  float local = 0.0f, c0 = 0.0f;
+  double total = 0.0;
+  int prev_y = -1;
+  const unsigned long long mine = drive_items<false>(
+      g, w,
+      [&](int v) {
+        if (v < g.active_begin || v >= g.max_label) return false;
+        return a.invdeg ? a.invdeg[v] > 0.0f : a.deg[v] > 0;
+      },
+      [&](int v, int, int) {
+        const float inv = a.invdeg ? a.invdeg[v] : 1.0f / (float)a.deg[v];
+        c0 = a.damping * (float)((double)a.in[v] * s) * inv;
+        prev_y = -1;
+        local = 0.0f;
+        return true;
+      },
+      [&](int, int y, int64_t t) {
+        if (!keep_edge(g, a.lo, a.hi, y, t, prev_y)) return true;
+        const float contrib = c0 * temporal_weight(a.alpha, t);
+        atomicAdd(&a.out[y], contrib);
+        local += contrib;
+        return true;
+      },
+      [&](int) { total += (double)local; });
   add_edges(a.edges, mine);
-  const double bs = block_sum(local);
+  const double bs = block_sum(total);
   if (threadIdx.x == 0 && bs != 0.0) atomicAdd(&a.sums[a.k], bs);
 }
 
@@ -411,20 +441,22 @@ __global__ void k_pr_final(const float* buf, const double* sums, int k, float* o
 }
 
 // In-window outdegree of each source, counted over items, then inverted.
-__global__ void __launch_bounds__(kBlock, 2) k_window_count(GraphView g, Work w, int64_t lo, int64_t hi, int32_t* cnt,
-                                                         unsigned long long* edges) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  unsigned long long mine = 0;
-  if (i < w.nitems) {
-    mine = sweep_item(
-        g, w, i, [&](int v) { return v >= g.active_begin && v < g.max_label; },
-        [&](EdgeCursor& c, int v, int, int) {
-          int k = 0, y;
-          int64_t t;
-          while (c.next(g, y, t)) k += (t >= lo && t < hi);
-          if (k) atomicAdd(&cnt[v], k);
-        });
-  }
+__global__ void TGA_DECODE_BOUNDS k_window_count(GraphView g, Work w, int64_t lo, int64_t hi, int32_t* cnt,
+                                                 unsigned long long* edges) {
+  int k = 0;
+  const unsigned long long mine = drive_items<false>(
+      g, w, [&](int v) { return v >= g.active_begin && v < g.max_label; },
+      [&](int, int, int) {
+        k = 0;
+        return true;
+      },
+      [&](int, int, int64_t t) {
+        k += (t >= lo && t < hi);
+        return true;
+      },
+      [&](int v) {
+        if (k) atomicAdd(&cnt[v], k);
+      });
   add_edges(edges, mine);
 }
 
@@ -446,46 +478,45 @@ __global__ void k_hits_base(float* hub, const float* auth_in, float* auth_next, 
   auth_next[x] = java ? 0.0f : auth_in[x] * sa;
 }
 
-__global__ void __launch_bounds__(kBlock, 2) k_hits_hub(GraphView g, Work w, float* hub, const float* auth_in,
-                                                     const double* aprev, int64_t lo, int64_t hi, unsigned long long* edges) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  unsigned long long mine = 0;
-  if (i < w.nitems) {
-    const float sa = (aprev && *aprev > 0) ? (float)(1.0 / sqrt(*aprev)) : 1.0f;
-    mine = sweep_item(
-        g, w, i, [&](int v) { return v >= g.active_begin && v < g.max_label; },
-        [&](EdgeCursor& c, int v, int, int) {
-          float acc = 0.0f;
-          int y, prev_y = -1;
-          int64_t t;
-          while (c.next(g, y, t)) {
-            TGA_EDGE_FILTER(g, lo, hi, y, t, prev_y)
-            acc += auth_in[y];
-          }
-          if (acc != 0.0f) atomicAdd(&hub[v], acc * sa);
-        });
-  }
+__global__ void TGA_DECODE_BOUNDS k_hits_hub(GraphView g, Work w, float* hub, const float* auth_in, const double* aprev,
+                                             int64_t lo, int64_t hi, unsigned long long* edges) {
+  const float sa = (aprev && *aprev > 0) ? (float)(1.0 / sqrt(*aprev)) : 1.0f;
+  float acc = 0.0f;
+  int prev_y = -1;
+  const unsigned long long mine = drive_items<false>(
+      g, w, [&](int v) { return v >= g.active_begin && v < g.max_label; },
+      [&](int, int, int) {
+        acc = 0.0f;
+        prev_y = -1;
+        return true;
+      },
+      [&](int, int y, int64_t t) {
+        if (keep_edge(g, lo, hi, y, t, prev_y)) acc += auth_in[y];
+        return true;
+      },
+      [&](int v) {
+        if (acc != 0.0f) atomicAdd(&hub[v], acc * sa);
+      });
   add_edges(edges, mine);
 }
 
-__global__ void __launch_bounds__(kBlock, 2) k_hits_auth(GraphView g, Work w, const float* hub, const double* hsum,
-                                                      float* auth_next, int64_t lo, int64_t hi, unsigned long long* edges) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  unsigned long long mine = 0;
-  if (i < w.nitems) {
-    const float sh = *hsum > 0 ? (float)(1.0 / sqrt(*hsum)) : 1.0f;
-    mine = sweep_item(
-        g, w, i, [&](int v) { return v >= g.active_begin && v < g.max_label && hub[v] != 0.0f; },
-        [&](EdgeCursor& c, int v, int, int) {
-          const float hn = hub[v] * sh;
-          int y, prev_y = -1;
-          int64_t t;
-          while (c.next(g, y, t)) {
-            TGA_EDGE_FILTER(g, lo, hi, y, t, prev_y)
-            atomicAdd(&auth_next[y], hn);
-          }
-        });
-  }
+__global__ void TGA_DECODE_BOUNDS k_hits_auth(GraphView g, Work w, const float* hub, const double* hsum,
+                                              float* auth_next, int64_t lo, int64_t hi, unsigned long long* edges) {
+  const float sh = *hsum > 0 ? (float)(1.0 / sqrt(*hsum)) : 1.0f;
+  float hn = 0.0f;
+  int prev_y = -1;
+  const unsigned long long mine = drive_items<false>(
+      g, w, [&](int v) { return v >= g.active_begin && v < g.max_label && hub[v] != 0.0f; },
+      [&](int v, int, int) {
+        hn = hub[v] * sh;
+        prev_y = -1;
+        return true;
+      },
+      [&](int, int y, int64_t t) {
+        if (keep_edge(g, lo, hi, y, t, prev_y)) atomicAdd(&auth_next[y], hn);
+        return true;
+      },
+      [&](int) {});
   add_edges(edges, mine);
 }
 
@@ -505,40 +536,42 @@ __global__ void k_scale(const float* v, const double* sumsq, float* out, int32_t
 
 // ---------------------------------------------------------------------------------------------
 // Degree centrality (Java semantics).  The running integer mean is sequential per list, so a
-// long list is processed whole by the thread that owns its first slice.
+// long list is decoded whole by the thread that draws its first slice.
 
-__global__ void __launch_bounds__(kBlock, 2) k_degree(GraphView g, Work w, int64_t s, int64_t e, int32_t* deg,
-                                                   int64_t* avg, unsigned long long* edges) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  unsigned long long mine = 0;
-  if (i < w.nitems) {
-    const WorkItem it = w.items[i];
-    int v0 = it.v0, v1 = it.v1;
-    if (it.slice >= 0 && w.slices[it.slice].first != 0) v1 = v0;  // later slices: owned by slice 0
-    const bool all = (s == 0 && e == 0);
-    const int lim = min(g.max_label + 1, g.max_vertex);
-    for (int x = v0; x < v1; ++x) {
-      if (x < g.active_begin || x > g.max_label) continue;
-      int32_t d = 0;
-      int64_t mean = 0;
-      DeepState deep_;
-      EdgeCursor c(&deep_);
-      mine += (unsigned long long)c.open(g, x);
-      int y;
-      int64_t t;
-      while (c.next(g, y, t)) {
-        if (y < g.active_begin || y >= lim) continue;
-        if (all || (s <= t && e >= t)) {
+__global__ void TGA_DECODE_BOUNDS k_degree(GraphView g, Work w, int64_t s, int64_t e, int32_t* deg, int64_t* avg,
+                                           unsigned long long* edges) {
+  const bool all = (s == 0 && e == 0);
+  const int lim = min(g.max_label + 1, g.max_vertex);
+  int32_t d = 0;
+  int64_t mean = 0;
+  const unsigned long long mine = drive_items<true>(
+      g, w, [&](int v) { return v >= g.active_begin && v <= g.max_label; },
+      [&](int, int, int) {
+        d = 0;
+        mean = 0;
+        return true;
+      },
+      [&](int, int y, int64_t t) {
+        if (y >= g.active_begin && y < lim && (all || (s <= t && e >= t))) {
           ++d;
           mean += (t - mean) / d;
         }
-      }
-      if (s != e) d = (int32_t)(0.85 * d + 0.15 * d * (double)(mean - s) / (double)(e - s) + 1);
-      deg[x] = d;
-      avg[x] = mean;
-    }
-  }
+        return true;
+      },
+      [&](int v) {
+        if (s != e) d = (int32_t)(0.85 * d + 0.15 * d * (double)(mean - s) / (double)(e - s) + 1);
+        deg[v] = d;
+        avg[v] = mean;
+      });
   add_edges(edges, mine);
+}
+
+// Lists of length zero never reach the loop above; their centrality is the formula at d = 0.
+__global__ void k_degree_empty(const int32_t* outdeg, int32_t active, int32_t max_label, int32_t n, int64_t s, int64_t e,
+                               int32_t* deg) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= n || v < active || v > max_label || outdeg[v] != 0) return;
+  deg[v] = (s != e) ? 1 : 0;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -554,31 +587,30 @@ __global__ void k_gc_prio_curand(uint32_t* prio, int32_t n) {
   prio[i] = curand(&st) % 256u;
 }
 
-__global__ void __launch_bounds__(kBlock, 2) k_gc_check(GraphView g, Work w, const int32_t* entries, int32_t en,
-                                                     const uint32_t* color, const uint32_t* prio, uint32_t round,
-                                                     uint32_t* found, unsigned long long* edges) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  unsigned long long mine = 0;
-  if (i < en) {
-    DeepState deep_;
-    EdgeCursor c(&deep_);
-    int cnt;
-    const int x = open_entry(g, w, entries[i], c, cnt);
-    const uint32_t px = prio[x];
-    int y, prev_y = -1;
-    int64_t t;
-    while (c.next(g, y, t)) {
-      ++mine;
-      if (y == prev_y) continue;
-      prev_y = y;
-      if (y < g.active_begin || y >= g.max_vertex) continue;
-      const uint32_t py = prio[y];
-      if ((py > px || (py == px && y < x)) && color[y] >= round) {
-        found[x] = round + 1;
-        break;
-      }
-    }
-  }
+__global__ void TGA_DECODE_BOUNDS k_gc_check(GraphView g, Work w, const int32_t* entries, int32_t en,
+                                             const uint32_t* color, const uint32_t* prio, uint32_t round,
+                                             uint32_t* found, unsigned long long* edges) {
+  uint32_t px = 0;
+  int prev_y = -1;
+  const unsigned long long mine = drive_queue(
+      g, w, entries, en,
+      [&](int x, int, int) {
+        px = prio[x];
+        prev_y = -1;
+        return true;
+      },
+      [&](int x, int y, int64_t) {
+        if (y == prev_y) return true;
+        prev_y = y;
+        if (y < g.active_begin || y >= g.max_vertex) return true;
+        const uint32_t py = prio[y];
+        if ((py > px || (py == px && y < x)) && color[y] >= round) {
+          found[x] = round + 1;
+          return false;
+        }
+        return true;
+      },
+      [&](int) {});
   add_edges(edges, mine);
 }
 
@@ -607,6 +639,64 @@ __global__ void k_gc_first(GraphView g, Work w, const int32_t* deg, int32_t n, i
   if (x >= n) return;
   wl[atomicAdd(wn, 1)] = x;
   if (x >= g.active_begin && x <= g.max_label && x < g.n && deg[x] > 0) enqueue(w, x, entries, en);
+}
+
+// Host side: the queue entries of one vertex (itself or its slices).
+static int32_t seed_entries(const GraphHandle& h, int32_t v, std::vector<int32_t>& out) {
+  out.clear();
+  const int32_t a = h.slice_first_host[(size_t)v], b = h.slice_first_host[(size_t)v + 1];
+  if (a == b) out.push_back(v);
+  else
+    for (int32_t j = a; j < b; ++j) out.push_back(-(j + 1));
+  return (int32_t)out.size();
+}
+
+// Work view of a handle with a freshly zeroed counter (one per decode launch, in stream order).
+static Work work_of(GraphHandle& h) {
+  int32_t* ctr = reinterpret_cast<int32_t*>(h.s_sum.as<char>() + 4000);
+  cudaMemsetAsync(ctr, 0, sizeof(int32_t), h.stream);
+  return Work{h.d_items.as<WorkItem>(), h.d_slices.as<SliceState>(), h.d_slice_first.as<int32_t>(), ctr, h.nitems};
+}
+
+// Grid of a persistent decode launch over `work` units.
+static unsigned decode_grid(const GraphHandle& h, int64_t work) {
+  const int64_t cap = (int64_t)h.sm_count * 2;
+  return (unsigned)std::max<int64_t>(1, std::min<int64_t>(cap, (work + kBlock - 1) / kBlock));
+}
+
+// Level loop of phase 1 from an initialised queue of qn entries; returns the levels executed.
+static int run_bfs_levels(GraphHandle& h, BfsArgs a, DevBuf& q0, DevBuf& q1, int32_t qn, uint32_t& wave, int& rc) {
+  int levels = 0;
+  DevBuf* cur = &q0;
+  DevBuf* nxt = &q1;
+  rc = TGA_OK;
+  while (qn > 0) {
+    if (levels > (1 << 22)) { rc = fail(TGA_E_TIMEOUT, "BFS level cap reached"); return levels; }
+    a.q = cur->as<int32_t>();
+    a.nq = nxt->as<int32_t>();
+    a.wave = ++wave;
+    cudaMemsetAsync(a.ncnt, 0, sizeof(int32_t), h.stream);
+    const Work w = work_of(h);
+    cudaEvent_t* ev = h.kernel_begin();
+    KL(k_bfs_level, decode_grid(h, qn))(h.view, w, a, qn);
+    h.kernel_end(ev);
+    cudaMemcpyAsync(h.h_pinned, a.ncnt, sizeof(int32_t), cudaMemcpyDeviceToHost, h.stream);
+    if (cudaStreamSynchronize(h.stream) != cudaSuccess) { rc = fail(TGA_E_CUDA, "BFS level failed"); return levels; }
+    qn = (int32_t)h.h_pinned[0];
+    std::swap(cur, nxt);
+    ++levels;
+  }
+  return levels;
+}
+
+static int bfs_buffers(GraphHandle& h) {
+  const size_t nv = (size_t)h.view.max_vertex;
+  const size_t qcap = nv + (size_t)h.nslices + 1;
+  int rc;
+  if ((rc = h.s_a.ensure(nv * 8)) || (rc = h.s_b.ensure(nv * 4)) || (rc = h.s_q0.ensure(qcap * 4)) ||
+      (rc = h.s_q1.ensure(qcap * 4)) || (rc = h.s_cnt.ensure(64)) || (rc = h.s_c.ensure(nv * 4)))
+    return rc;
+  return TGA_OK;
 }
 
 }  // namespace tga
@@ -662,7 +752,7 @@ int tga_neighbor_access(tga_graph* gp, uint8_t* small_out, uint64_t* checksum_ou
   if (e > b) {
     const Work w = work_of(h);
     cudaEvent_t* ev = h.kernel_begin();
-    KL(k_neighbor_access, grid_for(w.nitems, kBlock))(h.view, w, b, e, h.s_b.as<unsigned long long>(), edges);
+    KL(k_neighbor_access, decode_grid(h, w.nitems))(h.view, w, b, e, h.s_b.as<unsigned long long>(), edges);
     h.kernel_end(ev);
     KL(k_small_flags, grid_for(e - b, kBlock))(h.d_deg.as<int32_t>(), h.s_a.as<uint8_t>(), b, e);
   }
@@ -713,7 +803,7 @@ int tga_decode_all(tga_graph* gp, int64_t* offsets, int32_t* dst, int64_t* ts, i
   TGA_CUDA_TRY(cudaMemcpy(h.s_e.p, offsets, (size_t)(n + 1) * 8, cudaMemcpyHostToDevice));
   TGA_TRY(h.begin_call());
   const Work w = work_of(h);
-  KL(k_decode_csr, grid_for(w.nitems, kBlock))(h.view, w, h.s_e.as<int64_t>(), h.s_f.as<int32_t>(),
+  KL(k_decode_csr, decode_grid(h, w.nitems))(h.view, w, h.s_e.as<int64_t>(), h.s_f.as<int32_t>(),
                                                 h.s_g.as<int64_t>(), m);
   cudaMemcpyAsync(dst, h.s_f.p, (size_t)m * 4, cudaMemcpyDeviceToHost, h.stream);
   cudaMemcpyAsync(ts, h.s_g.p, (size_t)m * 8, cudaMemcpyDeviceToHost, h.stream);
@@ -754,7 +844,6 @@ int tga_bfs(tga_graph* gp, int32_t src, int64_t t_lo, int64_t t_hi, int32_t* arr
   cudaMemsetAsync(hops_u + src, 0, 4, h.stream);
   if (sq) cudaMemcpyAsync(h.s_q0.p, seed.data(), (size_t)sq * 4, cudaMemcpyHostToDevice, h.stream);
   {
-    const Work w = work_of(h);
     DevBuf* cur = &h.s_q0;
     DevBuf* nxt = &h.s_q1;
     int32_t qn = sq;
@@ -762,8 +851,9 @@ int tga_bfs(tga_graph* gp, int32_t src, int64_t t_lo, int64_t t_hi, int32_t* arr
       a.q = cur->as<int32_t>();
       a.nq = nxt->as<int32_t>();
       cudaMemsetAsync(a.ncnt, 0, sizeof(int32_t), h.stream);
+      const Work w = work_of(h);
       cudaEvent_t* ev = h.kernel_begin();
-      KL(k_bfs_hops, grid_for(qn, kBlock))(h.view, w, a, qn, hops_u, level);
+      KL(k_bfs_hops, decode_grid(h, qn))(h.view, w, a, qn, hops_u, level);
       h.kernel_end(ev);
       cudaMemcpyAsync(h.h_pinned, a.ncnt, sizeof(int32_t), cudaMemcpyDeviceToHost, h.stream);
       TGA_CUDA_TRY(cudaStreamSynchronize(h.stream));
@@ -873,7 +963,6 @@ int tga_pagerank(tga_graph* gp, int32_t iters, float damping, float alpha, int64
   const float base = (1.0f - damping) / (float)h.view.max_label;
   float* bufs[3] = {h.s_a.as<float>(), h.s_b.as<float>(), h.s_c.as<float>()};
   double* sums = h.s_g.as<double>();
-  const Work w = work_of(h);
   KL(k_fill_f32, grid_for(nv, kBlock))(bufs[0], 1.0f / (float)nv, nv);
   KL(k_fill_f32, grid_for(nv, kBlock))(bufs[1], base, nv);
   KL(k_pr_init_sums, grid_for(iters, kBlock))(sums, iters, (double)base * (double)nv);
@@ -882,13 +971,15 @@ int tga_pagerank(tga_graph* gp, int32_t iters, float damping, float alpha, int64
     int32_t* cnt = h.s_e.as<int32_t>();
     invdeg = h.s_d.as<float>();
     cudaMemsetAsync(cnt, 0, (size_t)nv * 4, h.stream);
+    const Work w = work_of(h);
     cudaEvent_t* ev = h.kernel_begin();
-    KL(k_window_count, grid_for(w.nitems, kBlock))(h.view, w, t_lo, t_hi, cnt, edges);
+    KL(k_window_count, decode_grid(h, w.nitems))(h.view, w, t_lo, t_hi, cnt, edges);
     h.kernel_end(ev);
     KL(k_invert, grid_for(nv, kBlock))(cnt, invdeg, nv);
   }
-  const unsigned grid = std::max(grid_for(w.nitems, kBlock), 1u);
+  const unsigned grid = decode_grid(h, h.nitems);
   for (int k = 0; k < iters; ++k) {
+    const Work w = work_of(h);
     PrArgs a{invdeg, h.d_deg.as<int32_t>(), bufs[k % 3], bufs[(k + 1) % 3], bufs[(k + 2) % 3], sums, k,
              damping, alpha, base, t_lo, t_hi, edges};
     cudaEvent_t* ev = h.kernel_begin();
@@ -921,7 +1012,6 @@ int tga_hits(tga_graph* gp, int32_t iters, int32_t mode, int64_t t_lo, int64_t t
   float* hub = h.s_a.as<float>();
   float* auth[2] = {h.s_b.as<float>(), h.s_c.as<float>()};
   double* sums = h.s_g.as<double>();
-  const Work w = work_of(h);
   const int java = mode == TGA_HITS_JAVA;
   KL(k_fill_f32, grid_for(nv, kBlock))(hub, 1.0f, nv);
   KL(k_fill_f32, grid_for(nv, kBlock))(auth[0], 1.0f, nv);
@@ -932,12 +1022,14 @@ int tga_hits(tga_graph* gp, int32_t iters, int32_t mode, int64_t t_lo, int64_t t
     float* ain = auth[k & 1];
     float* anext = auth[(k + 1) & 1];
     KL(k_hits_base, grid_for(nv, kBlock))(hub, ain, anext, aprev, java, nv);
+    Work w = work_of(h);
     cudaEvent_t* ev = h.kernel_begin();
-    KL(k_hits_hub, grid_for(w.nitems, kBlock))(h.view, w, hub, ain, aprev, t_lo, t_hi, edges);
+    KL(k_hits_hub, decode_grid(h, w.nitems))(h.view, w, hub, ain, aprev, t_lo, t_hi, edges);
     h.kernel_end(ev);
     KL(k_sumsq, grid_for(nv, kBlock))(hub, nv, sums + 2 * k);
+    w = work_of(h);
     ev = h.kernel_begin();
-    KL(k_hits_auth, grid_for(w.nitems, kBlock))(h.view, w, hub, sums + 2 * k, anext, t_lo, t_hi, edges);
+    KL(k_hits_auth, decode_grid(h, w.nitems))(h.view, w, hub, sums + 2 * k, anext, t_lo, t_hi, edges);
     h.kernel_end(ev);
     KL(k_scale, grid_for(nv, kBlock))(hub, sums + 2 * k, hub, nv);
     KL(k_sumsq, grid_for(nv, kBlock))(anext, nv, sums + 2 * k + 1);
@@ -965,8 +1057,10 @@ int tga_degree(tga_graph* gp, int64_t t_start, int64_t t_end, int32_t* degree_ou
   cudaMemsetAsync(h.s_b.p, 0, (size_t)nv * 8, h.stream);
   const Work w = work_of(h);
   cudaEvent_t* ev = h.kernel_begin();
-  KL(k_degree, grid_for(w.nitems, kBlock))(h.view, w, t_start, t_end, h.s_a.as<int32_t>(), h.s_b.as<int64_t>(), edges);
+  KL(k_degree, decode_grid(h, w.nitems))(h.view, w, t_start, t_end, h.s_a.as<int32_t>(), h.s_b.as<int64_t>(), edges);
   h.kernel_end(ev);
+  KL(k_degree_empty, grid_for(nv, kBlock))(h.d_deg.as<int32_t>(), h.view.active_begin, h.view.max_label,
+                                           std::min(nv, h.view.n), t_start, t_end, h.s_a.as<int32_t>());
   if (degree_out) cudaMemcpyAsync(degree_out, h.s_a.p, (size_t)nv * 4, cudaMemcpyDeviceToHost, h.stream);
   if (avg_out) cudaMemcpyAsync(avg_out, h.s_b.p, (size_t)nv * 8, cudaMemcpyDeviceToHost, h.stream);
   h.timing.iterations = 1;
@@ -1030,8 +1124,9 @@ int tga_color(tga_graph* gp, int32_t prio_mode, const uint32_t* prio_in, int32_t
   while (wn != 0 && round < 512) {
     cudaMemsetAsync(cnt, 0, 8, h.stream);
     if (ne > 0) {
+      const Work wc = work_of(h);
       cudaEvent_t* ev = h.kernel_begin();
-      KL(k_gc_check, grid_for(ne, kBlock))(h.view, w, en->as<int32_t>(), ne, color, prio, (uint32_t)round, found, edges);
+      KL(k_gc_check, decode_grid(h, ne))(h.view, wc, en->as<int32_t>(), ne, color, prio, (uint32_t)round, found, edges);
       h.kernel_end(ev);
     }
     KL(k_gc_decide, grid_for(wn, kBlock))(h.view, w, wl->as<int32_t>(), wn, h.d_deg.as<int32_t>(), color, found,

@@ -62,6 +62,7 @@ GraphHandle::~GraphHandle() {
 int GraphHandle::begin_call() {
   timing = tga_timing{};
   ktimer_used = 0;
+  if (int rc = s_sum.ensure(4096)) return rc;  // work and edge counters
   TGA_CUDA_TRY(cudaMemsetAsync(d_err.p, 0, sizeof(uint32_t), stream));
   TGA_CUDA_TRY(cudaEventRecord(ev_begin, stream));
   return TGA_OK;
@@ -257,6 +258,7 @@ int load_graph(GraphHandle& h, const std::string& dir, const std::string& base, 
   h.info.timestamp_ef_low_bits = lt;
 
   TGA_CUDA_TRY(cudaGetDevice(&h.device));
+  TGA_CUDA_TRY(cudaDeviceGetAttribute(&h.sm_count, cudaDevAttrMultiProcessorCount, h.device));
   TGA_CUDA_TRY(cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking));
   TGA_CUDA_TRY(cudaEventCreate(&h.ev_begin));
   TGA_CUDA_TRY(cudaEventCreate(&h.ev_end));

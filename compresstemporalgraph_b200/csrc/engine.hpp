@@ -42,6 +42,7 @@ struct GraphHandle {
   GraphView view{};
   cudaStream_t stream = nullptr;
   int device = 0;
+  int sm_count = 1;
   // resident format data
   DevBuf d_graph, d_ts, d_gl, d_gu, d_gs, d_tl, d_tu, d_ts_samples, d_err;
   // per-vertex outdegrees (int32, filled once at load by a decode kernel)
