@@ -75,7 +75,7 @@ class _GenSummary(C.Structure):
 
 def _load() -> C.CDLL:
     if not LIB_PATH.exists():
-        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m compresstemporalgraph_b200.build`")
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python compresstemporalgraph_b200/build.py`")
     lib = C.CDLL(str(LIB_PATH))
     P = C.c_void_p
     sig = {

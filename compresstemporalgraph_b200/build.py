@@ -1,7 +1,7 @@
 """Builds the engine in-tree: compresstemporalgraph_b200/libtga.so (sm_100a) and the drop-in
 executables under compresstemporalgraph_b200/bin/.
 
-Run ``python -m compresstemporalgraph_b200.build`` (or call ``build()``); objects go to
+Run ``python compresstemporalgraph_b200/build.py`` (or call ``build()``); objects go to
 compresstemporalgraph_b200/_build/ and are rebuilt when a source or header is newer.
 """
 from __future__ import annotations

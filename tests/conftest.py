@@ -21,7 +21,11 @@ def pytest_configure(config):
 
 
 def _build():
-    from compresstemporalgraph_b200 import build as b
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("tga_build", ROOT / "compresstemporalgraph_b200" / "build.py")
+    b = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(b)  # the package itself refuses to import before libtga.so exists
 
     b.build()
     import pyoracle
