@@ -2,12 +2,13 @@
 // successor lists and timestamps it needs straight from the compressed streams; decoded edges
 // live only in registers.
 //
-// Work decomposition (slices.cuh): lists longer than a slice are cut into resumable slices, short
-// lists are grouped into work items.  Every decode kernel is persistent: each thread pulls work
-// (an item, or a queue entry = a vertex id >= 0 or -(slice + 1)) from an atomic counter and runs
-// a flat loop in which one iteration either decodes one edge of its current list or opens the
-// next list.  Lanes of a warp therefore never wait for a neighbour's longer list at a list
-// boundary, which with power-law outdegrees would leave most lanes idle.
+// Work decomposition (slices.cuh): lists longer than a slice are cut into resumable slices.
+// Sweeps over all lists follow a schedule built at load time in which lists are grouped by work
+// class (outdegree bins), so the 32 lanes of a warp open lists together and decode lists of nearly
+// equal length: with power-law outdegrees, lanes of mixed lists spend most of their time waiting
+// for the longest list or for a neighbour opening its next one.  Traversals pull queue entries (a
+// vertex id >= 0 or -(slice + 1)) from an atomic counter in a flat loop in which one iteration
+// either decodes one edge or opens the next list.
 #include <curand_kernel.h>
 
 #include <algorithm>
@@ -66,6 +67,8 @@ struct Work {
   const int32_t* slice_first;
   int32_t* next;          // work counter of the launch (zeroed before it)
   int32_t nitems;
+  const int32_t* order;   // sweep schedule grouped by work class (vertex ids and -(slice+1))
+  int32_t norder;
 };
 
 // Opens queue entry e: a whole list (e >= 0) or one slice.  Returns the vertex.
@@ -103,58 +106,46 @@ __device__ __forceinline__ bool keep_edge(const GraphView& g, int64_t lo, int64_
   return y >= g.active_begin && y < g.max_vertex;
 }
 
-// Flat loop over work items.  Hooks (each inlined at its single call site):
-//   want(x) -> bool, begin(x, first, count) -> bool (false: skip the list),
-//   edge(x, y, t) -> bool (false: stop this list), end(x).
-// kWhole: a sliced list is decoded whole by the thread that draws its first slice (for workloads
-// that are sequential per list); its other slices are skipped.  Returns the edges decoded.
+// Sweep over the class-ordered schedule: thread i decodes entry i (a whole list or a slice).
+// Entries of one warp belong to the same work class, so the lanes open their lists together and
+// finish together.  Hooks (each inlined at its single call site): want(x) -> bool,
+// begin(x, first, count) -> bool (false: skip the list), edge(x, y, t) -> bool (false: stop the
+// list), end(x).  kWhole: a sliced list is decoded whole by the thread that draws its first slice
+// (for workloads that are sequential per list); its other slices are skipped.
 template <bool kWhole, class Want, class Begin, class Edge, class End>
-__device__ __forceinline__ unsigned long long drive_items(const GraphView& g, const Work& w, Want want, Begin begin,
-                                                          Edge edge, End end) {
-  DeepState deep;
-  EdgeCursor c(&deep);
-  c.remaining = 0;
-  int v = 0, vend = 0, slice = -1, cur = -1;
+__device__ __forceinline__ unsigned long long run_order(const GraphView& g, const Work& w, Want want, Begin begin,
+                                                        Edge edge, End end) {
   unsigned long long edges = 0;
-  for (;;) {
-    if (c.remaining <= 0) {
-      if (cur >= 0) {
-        end(cur);
-        cur = -1;
-      }
-      if (v >= vend) {
-        const int i = atomicAdd(w.next, 1);
-        if (i >= w.nitems) break;
-        const WorkItem it = w.items[i];
-        v = it.v0;
-        vend = it.slice >= 0 ? it.v0 + 1 : it.v1;
-        slice = it.slice;
-        if (kWhole && slice >= 0 && w.slices[slice].first != 0) v = vend;
-        continue;
-      }
-      const int x = v++;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < w.norder; i += gridDim.x * blockDim.x) {
+    const int e = w.order[i];
+    DeepState deep;
+    EdgeCursor c(&deep);
+    int x, first = 0, count;
+    if (e >= 0) {
+      x = e;
       if (!want(x)) continue;
-      int first = 0, count;
-      if (!kWhole && slice >= 0) {
-        const SliceState& s = w.slices[slice];
+      count = c.open(g, x);
+    } else {
+      const SliceState& s = w.slices[-e - 1];
+      x = s.v;
+      if (!want(x)) continue;
+      if (kWhole) {
+        if (s.first != 0) continue;
+        count = c.open(g, x);
+      } else {
         cursor_restore(g, c, s);
         first = s.first;
         count = s.count;
-      } else {
-        count = c.open(g, x);
       }
-      if (count <= 0 || !begin(x, first, count)) {
-        c.remaining = 0;
-        continue;
-      }
-      cur = x;
-      continue;
     }
+    if (count <= 0 || !begin(x, first, count)) continue;
     int y;
     int64_t t;
-    if (!c.next(g, y, t)) continue;
-    ++edges;
-    if (!edge(cur, y, t)) c.remaining = 0;
+    while (c.next(g, y, t)) {
+      ++edges;
+      if (!edge(x, y, t)) break;
+    }
+    end(x);
   }
   return edges;
 }
@@ -201,7 +192,7 @@ __global__ void TGA_DECODE_BOUNDS k_neighbor_access(GraphView g, Work w, int32_t
                                                     unsigned long long* csum, unsigned long long* edges) {
   uint64_t h = 0;
   uint32_t k = 0;
-  const unsigned long long mine = drive_items<false>(
+  const unsigned long long mine = run_order<false>(
       g, w, [&](int v) { return v >= begin && v < end; },
       [&](int, int first, int) {
         h = 0;
@@ -224,7 +215,7 @@ __global__ void k_small_flags(const int32_t* deg, uint8_t* small, int32_t begin,
 __global__ void TGA_DECODE_BOUNDS k_decode_csr(GraphView g, Work w, const int64_t* off, int32_t* dst, int64_t* ts,
                                                int64_t cap) {
   int64_t o = 0;
-  drive_items<false>(
+  run_order<false>(
       g, w, [&](int) { return true; },
       [&](int v, int first, int) {
         o = off[v] + first;
@@ -404,7 +395,7 @@ __global__ void TGA_DECODE_BOUNDS k_pr_iter(GraphView g, Work w, PrArgs a) {
   float local = 0.0f, c0 = 0.0f;
   double total = 0.0;
   int prev_y = -1;
-  const unsigned long long mine = drive_items<false>(
+  const unsigned long long mine = run_order<false>(
       g, w,
       [&](int v) {
         if (v < g.active_begin || v >= g.max_label) return false;
@@ -444,7 +435,7 @@ __global__ void k_pr_final(const float* buf, const double* sums, int k, float* o
 __global__ void TGA_DECODE_BOUNDS k_window_count(GraphView g, Work w, int64_t lo, int64_t hi, int32_t* cnt,
                                                  unsigned long long* edges) {
   int k = 0;
-  const unsigned long long mine = drive_items<false>(
+  const unsigned long long mine = run_order<false>(
       g, w, [&](int v) { return v >= g.active_begin && v < g.max_label; },
       [&](int, int, int) {
         k = 0;
@@ -483,7 +474,7 @@ __global__ void TGA_DECODE_BOUNDS k_hits_hub(GraphView g, Work w, float* hub, co
   const float sa = (aprev && *aprev > 0) ? (float)(1.0 / sqrt(*aprev)) : 1.0f;
   float acc = 0.0f;
   int prev_y = -1;
-  const unsigned long long mine = drive_items<false>(
+  const unsigned long long mine = run_order<false>(
       g, w, [&](int v) { return v >= g.active_begin && v < g.max_label; },
       [&](int, int, int) {
         acc = 0.0f;
@@ -505,7 +496,7 @@ __global__ void TGA_DECODE_BOUNDS k_hits_auth(GraphView g, Work w, const float* 
   const float sh = *hsum > 0 ? (float)(1.0 / sqrt(*hsum)) : 1.0f;
   float hn = 0.0f;
   int prev_y = -1;
-  const unsigned long long mine = drive_items<false>(
+  const unsigned long long mine = run_order<false>(
       g, w, [&](int v) { return v >= g.active_begin && v < g.max_label && hub[v] != 0.0f; },
       [&](int v, int, int) {
         hn = hub[v] * sh;
@@ -544,7 +535,7 @@ __global__ void TGA_DECODE_BOUNDS k_degree(GraphView g, Work w, int64_t s, int64
   const int lim = min(g.max_label + 1, g.max_vertex);
   int32_t d = 0;
   int64_t mean = 0;
-  const unsigned long long mine = drive_items<true>(
+  const unsigned long long mine = run_order<true>(
       g, w, [&](int v) { return v >= g.active_begin && v <= g.max_label; },
       [&](int, int, int) {
         d = 0;
@@ -655,7 +646,8 @@ static int32_t seed_entries(const GraphHandle& h, int32_t v, std::vector<int32_t
 static Work work_of(GraphHandle& h) {
   int32_t* ctr = reinterpret_cast<int32_t*>(h.s_sum.as<char>() + 4000);
   cudaMemsetAsync(ctr, 0, sizeof(int32_t), h.stream);
-  return Work{h.d_items.as<WorkItem>(), h.d_slices.as<SliceState>(), h.d_slice_first.as<int32_t>(), ctr, h.nitems};
+  return Work{h.d_items.as<WorkItem>(), h.d_slices.as<SliceState>(), h.d_slice_first.as<int32_t>(), ctr, h.nitems,
+              h.d_order.as<int32_t>(), h.norder};
 }
 
 // Grid of a persistent decode launch over `work` units.
@@ -663,6 +655,9 @@ static unsigned decode_grid(const GraphHandle& h, int64_t work) {
   const int64_t cap = (int64_t)h.sm_count * 2;
   return (unsigned)std::max<int64_t>(1, std::min<int64_t>(cap, (work + kBlock - 1) / kBlock));
 }
+
+// Grid of a sweep over the schedule: one entry per thread.
+static unsigned sweep_grid(const GraphHandle& h) { return std::max(1u, grid_for(h.norder, kBlock)); }
 
 // Level loop of phase 1 from an initialised queue of qn entries; returns the levels executed.
 static int run_bfs_levels(GraphHandle& h, BfsArgs a, DevBuf& q0, DevBuf& q1, int32_t qn, uint32_t& wave, int& rc) {
@@ -752,7 +747,7 @@ int tga_neighbor_access(tga_graph* gp, uint8_t* small_out, uint64_t* checksum_ou
   if (e > b) {
     const Work w = work_of(h);
     cudaEvent_t* ev = h.kernel_begin();
-    KL(k_neighbor_access, decode_grid(h, w.nitems))(h.view, w, b, e, h.s_b.as<unsigned long long>(), edges);
+    KL(k_neighbor_access, sweep_grid(h))(h.view, w, b, e, h.s_b.as<unsigned long long>(), edges);
     h.kernel_end(ev);
     KL(k_small_flags, grid_for(e - b, kBlock))(h.d_deg.as<int32_t>(), h.s_a.as<uint8_t>(), b, e);
   }
@@ -803,7 +798,7 @@ int tga_decode_all(tga_graph* gp, int64_t* offsets, int32_t* dst, int64_t* ts, i
   TGA_CUDA_TRY(cudaMemcpy(h.s_e.p, offsets, (size_t)(n + 1) * 8, cudaMemcpyHostToDevice));
   TGA_TRY(h.begin_call());
   const Work w = work_of(h);
-  KL(k_decode_csr, decode_grid(h, w.nitems))(h.view, w, h.s_e.as<int64_t>(), h.s_f.as<int32_t>(),
+  KL(k_decode_csr, sweep_grid(h))(h.view, w, h.s_e.as<int64_t>(), h.s_f.as<int32_t>(),
                                                 h.s_g.as<int64_t>(), m);
   cudaMemcpyAsync(dst, h.s_f.p, (size_t)m * 4, cudaMemcpyDeviceToHost, h.stream);
   cudaMemcpyAsync(ts, h.s_g.p, (size_t)m * 8, cudaMemcpyDeviceToHost, h.stream);
@@ -973,11 +968,11 @@ int tga_pagerank(tga_graph* gp, int32_t iters, float damping, float alpha, int64
     cudaMemsetAsync(cnt, 0, (size_t)nv * 4, h.stream);
     const Work w = work_of(h);
     cudaEvent_t* ev = h.kernel_begin();
-    KL(k_window_count, decode_grid(h, w.nitems))(h.view, w, t_lo, t_hi, cnt, edges);
+    KL(k_window_count, sweep_grid(h))(h.view, w, t_lo, t_hi, cnt, edges);
     h.kernel_end(ev);
     KL(k_invert, grid_for(nv, kBlock))(cnt, invdeg, nv);
   }
-  const unsigned grid = decode_grid(h, h.nitems);
+  const unsigned grid = sweep_grid(h);
   for (int k = 0; k < iters; ++k) {
     const Work w = work_of(h);
     PrArgs a{invdeg, h.d_deg.as<int32_t>(), bufs[k % 3], bufs[(k + 1) % 3], bufs[(k + 2) % 3], sums, k,
@@ -1024,12 +1019,12 @@ int tga_hits(tga_graph* gp, int32_t iters, int32_t mode, int64_t t_lo, int64_t t
     KL(k_hits_base, grid_for(nv, kBlock))(hub, ain, anext, aprev, java, nv);
     Work w = work_of(h);
     cudaEvent_t* ev = h.kernel_begin();
-    KL(k_hits_hub, decode_grid(h, w.nitems))(h.view, w, hub, ain, aprev, t_lo, t_hi, edges);
+    KL(k_hits_hub, sweep_grid(h))(h.view, w, hub, ain, aprev, t_lo, t_hi, edges);
     h.kernel_end(ev);
     KL(k_sumsq, grid_for(nv, kBlock))(hub, nv, sums + 2 * k);
     w = work_of(h);
     ev = h.kernel_begin();
-    KL(k_hits_auth, decode_grid(h, w.nitems))(h.view, w, hub, sums + 2 * k, anext, t_lo, t_hi, edges);
+    KL(k_hits_auth, sweep_grid(h))(h.view, w, hub, sums + 2 * k, anext, t_lo, t_hi, edges);
     h.kernel_end(ev);
     KL(k_scale, grid_for(nv, kBlock))(hub, sums + 2 * k, hub, nv);
     KL(k_sumsq, grid_for(nv, kBlock))(anext, nv, sums + 2 * k + 1);
@@ -1057,7 +1052,7 @@ int tga_degree(tga_graph* gp, int64_t t_start, int64_t t_end, int32_t* degree_ou
   cudaMemsetAsync(h.s_b.p, 0, (size_t)nv * 8, h.stream);
   const Work w = work_of(h);
   cudaEvent_t* ev = h.kernel_begin();
-  KL(k_degree, decode_grid(h, w.nitems))(h.view, w, t_start, t_end, h.s_a.as<int32_t>(), h.s_b.as<int64_t>(), edges);
+  KL(k_degree, sweep_grid(h))(h.view, w, t_start, t_end, h.s_a.as<int32_t>(), h.s_b.as<int64_t>(), edges);
   h.kernel_end(ev);
   KL(k_degree_empty, grid_for(nv, kBlock))(h.d_deg.as<int32_t>(), h.view.active_begin, h.view.max_label,
                                            std::min(nv, h.view.n), t_start, t_end, h.s_a.as<int32_t>());

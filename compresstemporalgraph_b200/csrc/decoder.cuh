@@ -318,7 +318,7 @@ static __device__ __noinline__ int deep_copy_next(const GraphView& g, DeepState&
 __device__ __forceinline__ int top_next(const GraphView& g, ListState& st, DeepState* deep) {
   const int v = min(min(st.hm, st.hi), min(st.hr, st.hc));
   if (v == kInf) return kInf;
-  if (merge_advance(g, st, v)) st.hc = deep_copy_next(g, *deep);
+  if (merge_advance(g, st, v)) st.hc = deep_copy_next(*g.self, *deep);
   return v;
 }
 
@@ -334,7 +334,7 @@ __device__ __forceinline__ int top_open(const GraphView& g, ListState& st, DeepS
   int extra = d;
   if (ref > 0) {
     chain = 1;
-    const OpenRef r = deep_open_ref(g, *deep, x - ref, bc, mk.bpos);
+    const OpenRef r = deep_open_ref(*g.self, *deep, x - ref, bc, mk.bpos);
     if (!(bc & 1)) copied += r.dref - total;
     extra = d - copied;
     st.hc = r.head;

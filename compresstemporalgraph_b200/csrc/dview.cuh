@@ -57,6 +57,9 @@ struct GraphView {
   const struct SliceState* slices;
   const int32_t* slice_first;
   int32_t seek_min;      // skip blocks longer than this seek through a checkpoint
+  // Device-global copy of this view.  Out-of-line decoder routines take it instead of the kernel
+  // parameter, whose address would otherwise force a local-memory copy read by the hot loop.
+  const struct GraphView* self;
   int64_t min_ts;        // header of the .timestamps stream
   uint32_t* err;         // device error word
 };

@@ -2,6 +2,7 @@
 // samples, uploads everything into HBM in the layout documented in dview.cuh, and computes the
 // per-vertex outdegrees once.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -47,7 +48,7 @@ void DevBuf::release() {
 GraphHandle::~GraphHandle() {
   if (stream) cudaStreamSynchronize(stream);
   for (DevBuf* b : {&d_graph, &d_ts, &d_gl, &d_gu, &d_gs, &d_tl, &d_tu, &d_ts_samples, &d_err, &d_deg, &d_slices,
-                    &d_items, &d_slice_first, &s_a, &s_b, &s_c, &s_d, &s_e, &s_f, &s_g, &s_q0, &s_q1, &s_cnt, &s_sum})
+                    &d_items, &d_slice_first, &d_order, &d_view, &s_a, &s_b, &s_c, &s_d, &s_e, &s_f, &s_g, &s_q0, &s_q1, &s_cnt, &s_sum})
     b->release();
   for (auto& k : ktimers) {
     if (k.a) cudaEventDestroy(k.a);
@@ -182,11 +183,14 @@ static int upload(GraphHandle& h, DevBuf& b, const std::vector<T>& v) {
   return TGA_OK;
 }
 
-__global__ void k_outdegrees(GraphView g, int32_t* deg, int32_t count) {
+// Outdegree of every list and whether it copies from a reference chain.
+__global__ void k_outdegrees(GraphView g, int32_t* deg, uint8_t* chain, int32_t count) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= count) return;
   uint64_t pos = ef_get(g, g.gef, (uint64_t)x);
-  deg[x] = (int32_t)read_gamma(g, g.g, pos);
+  const int d = (int)read_gamma(g, g.g, pos);
+  deg[x] = d;
+  chain[x] = d > 0 && read_unary(g, g.g, pos) > 0;
 }
 
 int load_graph(GraphHandle& h, const std::string& dir, const std::string& base, const tga_dataset_cfg& cfg) {
@@ -283,15 +287,20 @@ int load_graph(GraphHandle& h, const std::string& dir, const std::string& base, 
   v.min_interval = min_interval;
   v.min_ts = header;
   v.err = h.d_err.as<uint32_t>();
+  if ((rc = publish_view(h))) return rc;
 
   const int32_t ndeg = (int32_t)std::min<int64_t>(n, (int64_t)cfg.max_vertex);
   if ((rc = h.d_deg.ensure((size_t)cfg.max_vertex * sizeof(int32_t)))) return rc;
   h.info.device_bytes += (size_t)cfg.max_vertex * sizeof(int32_t);
   TGA_CUDA_TRY(cudaMemsetAsync(h.d_deg.p, 0, (size_t)cfg.max_vertex * sizeof(int32_t), h.stream));
-  k_outdegrees<<<grid_for(ndeg, 256), 256, 0, h.stream>>>(v, h.d_deg.as<int32_t>(), ndeg);
+  DevBuf chain_dev;
+  if ((rc = chain_dev.ensure((size_t)std::max(ndeg, 1)))) return rc;
+  k_outdegrees<<<grid_for(ndeg, 256), 256, 0, h.stream>>>(v, h.d_deg.as<int32_t>(), chain_dev.as<uint8_t>(), ndeg);
   TGA_CUDA_TRY(cudaGetLastError());
   std::vector<int32_t> deg((size_t)ndeg);
+  h.chain_host.assign((size_t)ndeg, 0);
   TGA_CUDA_TRY(cudaMemcpyAsync(deg.data(), h.d_deg.p, (size_t)ndeg * 4, cudaMemcpyDeviceToHost, h.stream));
+  TGA_CUDA_TRY(cudaMemcpyAsync(h.chain_host.data(), chain_dev.p, (size_t)ndeg, cudaMemcpyDeviceToHost, h.stream));
   if ((rc = h.check_device_error())) return rc;
   int64_t maxd = 0, m = 0;
   for (int32_t d : deg) {
@@ -311,6 +320,14 @@ int load_graph(GraphHandle& h, const std::string& dir, const std::string& base, 
   return build_work(h, env_slice ? std::atoi(env_slice) : 1024, env_item ? std::atoi(env_item) : 256);
 }
 
+int publish_view(GraphHandle& h) {
+  if (int rc = h.d_view.ensure(sizeof(GraphView))) return rc;
+  h.view.self = h.d_view.as<GraphView>();
+  TGA_CUDA_TRY(cudaMemcpyAsync(h.d_view.p, &h.view, sizeof(GraphView), cudaMemcpyHostToDevice, h.stream));
+  TGA_CUDA_TRY(cudaStreamSynchronize(h.stream));
+  return TGA_OK;
+}
+
 int build_work(GraphHandle& h, int32_t slice_len, int32_t item_edges) {
   if (slice_len < 16 || item_edges < 1) return fail(TGA_E_ARG, "slice length must be >= 16 and item size >= 1");
   GraphView& v = h.view;
@@ -318,6 +335,7 @@ int build_work(GraphHandle& h, int32_t slice_len, int32_t item_edges) {
   v.slices = nullptr;
   v.slice_first = nullptr;
   v.seek_min = INT32_MAX;
+  if (int rc = publish_view(h)) return rc;
   const int32_t nd = (int32_t)h.degrees.size();
   std::vector<int32_t> big_v;
   std::vector<int64_t> slot_base{0};
@@ -390,10 +408,32 @@ int build_work(GraphHandle& h, int32_t slice_len, int32_t item_edges) {
     if (start >= 0) items.push_back(WorkItem{start, nd, -1});
   }
   h.nitems = (int32_t)items.size();
+  // Decode order for the sweeps: every slice, then every non-empty short list, grouped by work
+  // class (quarter-octave of the outdegree, lists that copy from a reference chain apart) from the
+  // largest class down, so the 32 lanes of a warp open their lists together and decode lists of
+  // nearly equal length.
+  std::vector<int32_t> order;
+  order.reserve(packed.size() + (size_t)nd);
+  for (size_t j = 0; j < packed.size(); ++j) order.push_back(-(int32_t)j - 1);
+  {
+    auto cls = [&](int32_t d) { return (int)std::floor(4.0 * std::log2((double)d)); };
+    const int ncls = cls(std::max(slice_len, 1)) + 2;
+    std::vector<std::vector<int32_t>> bins((size_t)ncls * 2);
+    for (int32_t x = 0; x < nd; ++x) {
+      const int32_t d = h.degrees[(size_t)x];
+      if (d <= 0 || slice_first[(size_t)x + 1] != slice_first[(size_t)x]) continue;
+      bins[(size_t)(std::min(cls(d), ncls - 1) * 2 + (h.chain_host[(size_t)x] ? 1 : 0))].push_back(x);
+    }
+    for (int b = (int)bins.size() - 1; b >= 0; --b) order.insert(order.end(), bins[(size_t)b].begin(), bins[(size_t)b].end());
+  }
+  h.norder = (int32_t)order.size();
   h.nslices = (int64_t)packed.size();
   h.slice_len = slice_len;
   h.item_edges = item_edges;
   int rc;
+  if ((rc = h.d_order.ensure(std::max<size_t>(1, order.size()) * 4))) return rc;
+  if (!order.empty())
+    TGA_CUDA_TRY(cudaMemcpy(h.d_order.p, order.data(), order.size() * 4, cudaMemcpyHostToDevice));
   if ((rc = h.d_items.ensure(std::max<size_t>(1, items.size()) * sizeof(WorkItem))) ||
       (rc = h.d_slices.ensure(std::max<size_t>(1, packed.size()) * sizeof(SliceState))) ||
       (rc = h.d_slice_first.ensure(slice_first.size() * 4)))
@@ -407,7 +447,7 @@ int build_work(GraphHandle& h, int32_t slice_len, int32_t item_edges) {
   v.slices = h.d_slices.as<SliceState>();
   v.slice_first = h.d_slice_first.as<int32_t>();
   v.seek_min = std::max(16, slice_len / 2);
-  return TGA_OK;
+  return publish_view(h);
 }
 
 }  // namespace tga

@@ -50,6 +50,11 @@ struct GraphHandle {
   // edge-balanced work decomposition (slices.cuh): slices of long lists, work items, and
   // slice_first[v]..slice_first[v+1] = slices of vertex v (empty for short lists)
   DevBuf d_slices, d_items, d_slice_first;
+  // decode order of the sweeps (vertex ids >= 0 and -(slice+1)), grouped by work class
+  DevBuf d_order;
+  DevBuf d_view;                     // device-global copy of `view` (GraphView::self)
+  int32_t norder = 0;
+  std::vector<uint8_t> chain_host;   // list copies from a reference chain
   int32_t nitems = 0, nslice_items = 0;
   int64_t nslices = 0;
   int32_t slice_len = 0, item_edges = 0;
@@ -78,6 +83,8 @@ int load_graph(GraphHandle& h, const std::string& dir, const std::string& base, 
 // (Re)builds slices and work items: lists longer than slice_len edges are cut into slices,
 // the others grouped into items of about item_edges edges.
 int build_work(GraphHandle& h, int32_t slice_len, int32_t item_edges);
+// Uploads the current view to its device-global copy (after any change of `view`).
+int publish_view(GraphHandle& h);
 
 // Launch helpers shared by the algorithm files.
 inline unsigned grid_for(int64_t items, int block) { return (unsigned)((items + block - 1) / block); }
