@@ -96,6 +96,7 @@ def _load() -> C.CDLL:
         "tga_bfs": (C.c_int, [P, C.c_int32, C.c_int64, C.c_int64, P, P]),
         "tga_cc": (C.c_int, [P, C.c_int64, C.c_int64, C.c_int32, P, C.POINTER(C.c_int32)]),
         "tga_pagerank": (C.c_int, [P, C.c_int32, C.c_float, C.c_float, C.c_int64, C.c_int64, P]),
+        "tga_pagerank_noalloc": (C.c_int, [P, C.c_int32, C.c_float, C.c_float, C.c_int64, C.c_int64, P]),
         "tga_hits": (C.c_int, [P, C.c_int32, C.c_int32, C.c_int64, C.c_int64, P, P]),
         "tga_degree": (C.c_int, [P, C.c_int64, C.c_int64, P, P]),
         "tga_color": (C.c_int, [P, C.c_int32, P, C.c_int32, P, P, C.POINTER(C.c_int32)]),

@@ -1142,4 +1142,70 @@ int tga_color(tga_graph* gp, int32_t prio_mode, const uint32_t* prio_in, int32_t
   return finish(h, edges);
 }
 
+// tga_pagerank without any device allocation: the same kernels in the same order, with the
+// handle's growable scratch replaced by the fixed per-device array of noalloc.cu and the result
+// written to a caller-owned device buffer.  Only the call's total time is recorded (no per-kernel
+// timers).  The scratch is shared by every handle on a device, so overlapping calls race.
+int tga_pagerank_noalloc(tga_graph* gp, int32_t iters, float damping, float alpha, int64_t t_lo, int64_t t_hi,
+                         float* rank_out_dev) {
+  if (!gp) return fail(TGA_E_ARG, "null graph");
+  GraphHandle& h = *gp;
+  if (iters <= 0) iters = h.cfg.pr_iters;
+  if (t_lo >= t_hi) return fail(TGA_E_ARG, "empty time window");
+  if (!rank_out_dev) return fail(TGA_E_ARG, "null rank_out_dev");
+  const int32_t nv = h.view.max_vertex;
+  if (nv > kPrNoAllocMaxVertices)
+    return fail(TGA_E_ARG, "tga_pagerank_noalloc: max_vertex " + std::to_string(nv) + " exceeds its fixed scratch of " +
+                               std::to_string(kPrNoAllocMaxVertices) + " vertices; use tga_pagerank");
+  if (iters > kPrNoAllocMaxIters)
+    return fail(TGA_E_ARG, "tga_pagerank_noalloc: " + std::to_string(iters) + " iterations exceed its fixed scratch of " +
+                               std::to_string(kPrNoAllocMaxIters) + "; use tga_pagerank");
+  cudaPointerAttributes pa{};
+  TGA_CUDA_TRY(cudaPointerGetAttributes(&pa, rank_out_dev));
+  if ((pa.type != cudaMemoryTypeDevice && pa.type != cudaMemoryTypeManaged) || pa.device != h.device)
+    return fail(TGA_E_ARG, "tga_pagerank_noalloc: rank_out_dev must be device memory of the graph's device");
+  unsigned char* s = nullptr;
+  TGA_TRY(pr_noalloc_scratch(h.device, &s));
+  float* bufs[3] = {reinterpret_cast<float*>(s), reinterpret_cast<float*>(s + kPrNoAllocVec),
+                    reinterpret_cast<float*>(s + 2 * kPrNoAllocVec)};
+  float* invdeg_buf = reinterpret_cast<float*>(s + 3 * kPrNoAllocVec);
+  int32_t* cnt = reinterpret_cast<int32_t*>(s + 4 * kPrNoAllocVec);
+  double* sums = reinterpret_cast<double*>(s + kPrNoAllocSumsOff);
+  unsigned long long* edges = reinterpret_cast<unsigned long long*>(s + kPrNoAllocCountersOff);
+  int32_t* next = reinterpret_cast<int32_t*>(s + kPrNoAllocCountersOff + 8);
+
+  h.timing = tga_timing{};
+  h.ktimer_used = 0;
+  TGA_CUDA_TRY(cudaMemsetAsync(h.d_err.p, 0, sizeof(uint32_t), h.stream));
+  TGA_CUDA_TRY(cudaEventRecord(h.ev_begin, h.stream));
+  // Edge counter and work counter start at zero.
+  TGA_CUDA_TRY(cudaMemsetAsync(s + kPrNoAllocCountersOff, 0, 256, h.stream));
+  const Work w{h.d_items.as<WorkItem>(), h.d_slices.as<SliceState>(), h.d_slice_first.as<int32_t>(), next, h.nitems,
+               h.d_order.as<int32_t>(), h.norder};
+  const bool windowed = !(t_lo <= 0 && t_hi == TGA_T_MAX);
+  const float base = (1.0f - damping) / (float)h.view.max_label;
+  KL(k_fill_f32, grid_for(nv, kBlock))(bufs[0], 1.0f / (float)nv, nv);
+  KL(k_fill_f32, grid_for(nv, kBlock))(bufs[1], base, nv);
+  KL(k_pr_init_sums, grid_for(iters, kBlock))(sums, iters, (double)base * (double)nv);
+  float* invdeg = nullptr;
+  if (windowed) {
+    invdeg = invdeg_buf;
+    // The in-window outdegrees are accumulated with atomics and start at zero.
+    TGA_CUDA_TRY(cudaMemsetAsync(cnt, 0, (size_t)nv * 4, h.stream));
+    KL(k_window_count, sweep_grid(h))(h.view, w, t_lo, t_hi, cnt, edges);
+    KL(k_invert, grid_for(nv, kBlock))(cnt, invdeg, nv);
+  }
+  const unsigned grid = sweep_grid(h);
+  for (int k = 0; k < iters; ++k) {
+    PrArgs a{invdeg, h.d_deg.as<int32_t>(), bufs[k % 3], bufs[(k + 1) % 3], bufs[(k + 2) % 3], sums, k,
+             damping, alpha, base, t_lo, t_hi, edges};
+    KL(k_pr_iter, grid)(h.view, w, a);
+  }
+  KL(k_pr_final, grid_for(nv, kBlock))(bufs[iters % 3], sums, iters - 1, rank_out_dev, nv);
+  h.timing.iterations = iters;
+  const int rc = finish(h, edges);
+  h.timing.compressed_bytes = (uint64_t)(iters + (windowed ? 1 : 0)) * pass_bytes(h);
+  return rc;
+}
+
 }  // extern "C"

@@ -89,6 +89,19 @@ int publish_view(GraphHandle& h);
 // Launch helpers shared by the algorithm files.
 inline unsigned grid_for(int64_t items, int block) { return (unsigned)((items + block - 1) / block); }
 
+// Fixed device scratch of tga_pagerank_noalloc (noalloc.cu), one per device: three rank vectors,
+// the in-window outdegree and its inverse (kPrNoAllocMaxVertices entries each), the per-iteration
+// rank sums (kPrNoAllocMaxIters) and a 256-byte block of counters that each call zeroes.
+constexpr int32_t kPrNoAllocMaxVertices = 1 << 20;
+constexpr int32_t kPrNoAllocMaxIters = 1024;
+constexpr size_t kPrNoAllocVec = (size_t)kPrNoAllocMaxVertices * 4;
+constexpr size_t kPrNoAllocSumsOff = 5 * kPrNoAllocVec;
+constexpr size_t kPrNoAllocCountersOff = kPrNoAllocSumsOff + (size_t)kPrNoAllocMaxIters * 8;
+constexpr size_t kPrNoAllocScratchBytes = kPrNoAllocCountersOff + 256;
+// Device address of that scratch on `device`, looked up once per device (with the device made
+// current) and cached.
+int pr_noalloc_scratch(int device, unsigned char** out);
+
 }  // namespace tga
 
 struct tga_graph : tga::GraphHandle {};

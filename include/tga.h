@@ -143,6 +143,23 @@ int tga_cc(tga_graph* g, int64_t t_lo, int64_t t_hi, int32_t flags, int32_t* lab
  * pr_iters of the configuration; alpha is TEMPORAL_ALPHA (0.1 in the reference). */
 int tga_pagerank(tga_graph* g, int32_t iters, float damping, float alpha, int64_t t_lo, int64_t t_hi, float* rank_out);
 
+/* tga_pagerank that allocates no device memory (no counterpart in the reference).  For callers
+ * that cannot allocate in the middle of their work: a server that reserved its device memory up
+ * front and must not grow it per request, or a pipeline whose other streams must not be stalled
+ * by cudaMalloc/cudaFree (they synchronise the device).  Same kernels and result as tga_pagerank;
+ * the working vectors live in one fixed file-scope device array per device (about 20 MiB), and
+ * the result goes to rank_out_dev, a caller-owned device buffer of max_vertex floats on the
+ * graph's device.
+ *   Limits: max_vertex <= 1048576 and iters <= 1024 (after iters <= 0 -> pr_iters); larger
+ *   requests fail with TGA_E_ARG and a message naming the limit (use tga_pagerank).
+ *   First call on a device: looks the array up with cudaGetSymbolAddress (this loads the module
+ *   holding it); make one call before capturing a stream or starting latency-critical work.
+ *   Concurrency: the array is shared by all handles on a device; overlapping calls race, so
+ *   serialise them (one call at a time per device).
+ *   Timing: only total_ms, iterations and edges_decoded are recorded (no per-kernel timers). */
+int tga_pagerank_noalloc(tga_graph* g, int32_t iters, float damping, float alpha, int64_t t_lo, int64_t t_hi,
+                         float* rank_out_dev);
+
 /* HITS (hits.cu:1428-1987, loop 2284-2349) in FP32.  mode 0 = reference GPU semantics (hub and
  * authority accumulate without reset, L2-normalised each half step); mode 1 = Java semantics
  * (reset before each half step, BaselineRunner.java:493-549). */
