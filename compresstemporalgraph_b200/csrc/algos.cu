@@ -1,4 +1,5 @@
-// Fused decode + algorithm kernels and their C ABI entry points.  Every kernel decodes the
+// Fused decode + algorithm kernels and their C ABI entry points (sweeps: neighbour access, raw
+// decode, PageRank, HITS, degree centrality; colouring).  Every kernel decodes the
 // successor lists and timestamps it needs straight from the compressed streams; decoded edges
 // live only in registers.
 //
@@ -16,174 +17,9 @@
 #include <cstring>
 #include <vector>
 
-#include "engine.hpp"
+#include "sweep.cuh"
 
 namespace tga {
-
-constexpr int kBlock = 256;
-constexpr uint64_t kTpInf = ~0ull;
-constexpr uint32_t kColorInf = 0xFFFFFFFFu;
-
-// Launches a kernel of kBlock threads on the handle's stream and counts it in the call's timing.
-#define KL(kernel, grid) ++h.timing.launches, kernel<<<(grid), kBlock, 0, h.stream>>>
-// Decode kernels: 2 blocks of 256 threads per SM (128 registers, no spills).
-#define TGA_DECODE_BOUNDS __launch_bounds__(kBlock, 2)
-
-// Per-edge term of the neighbour-access checksum: the checksum of a list is the sum (mod 2^64)
-// of edge_hash over its edges, so slices can add their parts; the edge index keeps it
-// order-sensitive.  The oracle computes the same sum.
-__host__ __device__ __forceinline__ uint64_t edge_hash(uint32_t v, uint32_t i, int32_t y, int64_t t) {
-  uint64_t z = (((uint64_t)v << 32) | i) * 0x9E3779B97F4A7C15ull;
-  z ^= (uint64_t)(uint32_t)y * 0xC2B2AE3D27D4EB4Full;
-  z ^= (uint64_t)t * 0x165667B19E3779F9ull;
-  z ^= z >> 31;
-  z *= 0xBF58476D1CE4E5B9ull;
-  z ^= z >> 29;
-  z *= 0x94D049BB133111EBull;
-  return z ^ (z >> 32);
-}
-
-__device__ __forceinline__ void add_edges(unsigned long long* ctr, unsigned long long mine) {
-  for (int o = 16; o; o >>= 1) mine += __shfl_down_sync(0xffffffffu, mine, o);
-  if ((threadIdx.x & 31) == 0 && mine) atomicAdd(ctr, mine);
-}
-
-__device__ __forceinline__ double block_sum(double v) {
-  __shared__ double red[kBlock / 32];
-  for (int o = 16; o; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
-  __syncthreads();
-  double s = 0;
-  if (threadIdx.x < 32) {
-    s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
-    for (int o = 16; o; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-  }
-  return s;  // valid in thread 0
-}
-
-struct Work {
-  const WorkItem* items;
-  const SliceState* slices;
-  const int32_t* slice_first;
-  int32_t* next;          // work counter of the launch (zeroed before it)
-  int32_t nitems;
-  const int32_t* order;   // sweep schedule grouped by work class (vertex ids and -(slice+1))
-  int32_t norder;
-};
-
-// Opens queue entry e: a whole list (e >= 0) or one slice.  Returns the vertex.
-__device__ __forceinline__ int open_entry(const GraphView& g, const Work& w, int e, EdgeCursor& c, int& first,
-                                          int& count) {
-  if (e >= 0) {
-    first = 0;
-    count = c.open(g, e);
-    return e;
-  }
-  const SliceState& s = w.slices[-e - 1];
-  cursor_restore(g, c, s);
-  first = s.first;
-  count = s.count;
-  return s.v;
-}
-
-// Appends y (or all slices of y) to a queue.
-__device__ __forceinline__ void enqueue(const Work& w, int y, int32_t* q, int32_t* cnt) {
-  const int a = w.slice_first[y], b = w.slice_first[y + 1];
-  if (a == b) {
-    q[atomicAdd(cnt, 1)] = y;
-  } else {
-    const int base = atomicAdd(cnt, b - a);
-    for (int j = a; j < b; ++j) q[base + j - a] = -(j + 1);
-  }
-}
-
-// Edge filter shared by every traversal: in-window, first of equal consecutive successors,
-// successor inside [active_begin, max_vertex).
-__device__ __forceinline__ bool keep_edge(const GraphView& g, int64_t lo, int64_t hi, int y, int64_t t, int& prev_y) {
-  if (t < lo || t >= hi) return false;
-  if (y == prev_y) return false;
-  prev_y = y;
-  return y >= g.active_begin && y < g.max_vertex;
-}
-
-// Sweep over the class-ordered schedule: thread i decodes entry i (a whole list or a slice).
-// Entries of one warp belong to the same work class, so the lanes open their lists together and
-// finish together.  Hooks (each inlined at its single call site): want(x) -> bool,
-// begin(x, first, count) -> bool (false: skip the list), edge(x, y, t) -> bool (false: stop the
-// list), end(x).  kWhole: a sliced list is decoded whole by the thread that draws its first slice
-// (for workloads that are sequential per list); its other slices are skipped.
-template <bool kWhole, class Want, class Begin, class Edge, class End>
-__device__ __forceinline__ unsigned long long run_order(const GraphView& g, const Work& w, Want want, Begin begin,
-                                                        Edge edge, End end) {
-  unsigned long long edges = 0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < w.norder; i += gridDim.x * blockDim.x) {
-    const int e = w.order[i];
-    DeepState deep;
-    EdgeCursor c(&deep);
-    int x, first = 0, count;
-    if (e >= 0) {
-      x = e;
-      if (!want(x)) continue;
-      count = c.open(g, x);
-    } else {
-      const SliceState& s = w.slices[-e - 1];
-      x = s.v;
-      if (!want(x)) continue;
-      if (kWhole) {
-        if (s.first != 0) continue;
-        count = c.open(g, x);
-      } else {
-        cursor_restore(g, c, s);
-        first = s.first;
-        count = s.count;
-      }
-    }
-    if (count <= 0 || !begin(x, first, count)) continue;
-    int y;
-    int64_t t;
-    while (c.next(g, y, t)) {
-      ++edges;
-      if (!edge(x, y, t)) break;
-    }
-    end(x);
-  }
-  return edges;
-}
-
-// Flat loop over the entries q[0..qn) of a queue (vertices or slices).
-template <class Begin, class Edge, class End>
-__device__ __forceinline__ unsigned long long drive_queue(const GraphView& g, const Work& w, const int32_t* q, int qn,
-                                                          Begin begin, Edge edge, End end) {
-  DeepState deep;
-  EdgeCursor c(&deep);
-  c.remaining = 0;
-  int cur = -1;
-  unsigned long long edges = 0;
-  for (;;) {
-    if (c.remaining <= 0) {
-      if (cur >= 0) {
-        end(cur);
-        cur = -1;
-      }
-      const int i = atomicAdd(w.next, 1);
-      if (i >= qn) break;
-      int first, count;
-      const int x = open_entry(g, w, q[i], c, first, count);
-      if (count <= 0 || !begin(x, first, count)) {
-        c.remaining = 0;
-        continue;
-      }
-      cur = x;
-      continue;
-    }
-    int y;
-    int64_t t;
-    if (!c.next(g, y, t)) continue;
-    ++edges;
-    if (!edge(cur, y, t)) c.remaining = 0;
-  }
-  return edges;
-}
 
 // ---------------------------------------------------------------------------------------------
 // Neighbour access and raw decode
@@ -246,123 +82,6 @@ __global__ void k_neighbors(GraphView g, int32_t v, int32_t* dst, int64_t* ts, i
     ++i;
   }
   *count = d;
-}
-
-// ---------------------------------------------------------------------------------------------
-// Temporal BFS: phase 1 earliest arrival (label-correcting minimum), phase 2 hop levels.
-
-struct BfsArgs {
-  const int32_t* q;
-  int32_t* nq;
-  int32_t* ncnt;
-  uint64_t* tp;          // arrival << 32 per vertex (all ones = unreached)
-  uint32_t* stamp;       // last wave in which the vertex was enqueued
-  uint32_t wave;
-  int64_t lo, hi;
-  int32_t* touched;      // optional: vertices whose arrival became finite (CC)
-  int32_t* tcnt;
-  unsigned long long* edges;
-};
-
-// Phase 1: tp[v] holds arrival << 32, so the 64-bit atomicMin is an arrival minimum; a vertex
-// whose arrival drops is enqueued once per level (stamp) and relaxes its successors again.
-__global__ void TGA_DECODE_BOUNDS k_bfs_level(GraphView g, Work w, BfsArgs a, int32_t qn) {
-  uint32_t ax = 0;
-  int prev_y = -1;
-  const unsigned long long mine = drive_queue(
-      g, w, a.q, qn,
-      [&](int x, int, int) {
-        if (x < g.active_begin || x > g.max_label) return false;
-        ax = (uint32_t)(a.tp[x] >> 32);
-        prev_y = -1;
-        return true;
-      },
-      [&](int, int y, int64_t t) {
-        if (!keep_edge(g, a.lo, a.hi, y, t, prev_y)) return true;
-        if ((int64_t)ax > t || t >= 0xFFFFFFFFll) return true;
-        const uint64_t nv = (uint64_t)t << 32;
-        const uint64_t old = atomicMin((unsigned long long*)&a.tp[y], (unsigned long long)nv);
-        if (nv < old) {
-          if (a.touched && (old >> 32) == 0xFFFFFFFFull) a.touched[atomicAdd(a.tcnt, 1)] = y;
-          if (atomicMax(&a.stamp[y], a.wave) < a.wave) enqueue(w, y, a.nq, a.ncnt);
-        }
-        return true;
-      },
-      [&](int) {});
-  add_edges(a.edges, mine);
-}
-
-// Phase 2: with the final arrivals fixed, an edge passing the same filters is tight when
-// arrival(x) <= t == arrival(y); hops = BFS level over tight edges, each vertex claimed once.
-__global__ void TGA_DECODE_BOUNDS k_bfs_hops(GraphView g, Work w, BfsArgs a, int32_t qn, uint32_t* hops,
-                                             uint32_t level) {
-  uint32_t ax = 0;
-  int prev_y = -1;
-  const unsigned long long mine = drive_queue(
-      g, w, a.q, qn,
-      [&](int x, int, int) {
-        if (x < g.active_begin || x > g.max_label) return false;
-        ax = (uint32_t)(a.tp[x] >> 32);
-        prev_y = -1;
-        return true;
-      },
-      [&](int, int y, int64_t t) {
-        if (!keep_edge(g, a.lo, a.hi, y, t, prev_y)) return true;
-        if ((int64_t)ax > t || t >= 0xFFFFFFFFll) return true;
-        if ((int64_t)(a.tp[y] >> 32) != t) return true;
-        if (atomicCAS(&hops[y], 0xFFFFFFFFu, level + 1) == 0xFFFFFFFFu) enqueue(w, y, a.nq, a.ncnt);
-        return true;
-      },
-      [&](int) {});
-  add_edges(a.edges, mine);
-}
-
-__global__ void k_fill_u64(uint64_t* p, uint64_t v, int64_t n) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) p[i] = v;
-}
-__global__ void k_fill_f32(float* p, float v, int64_t n) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) p[i] = v;
-}
-__global__ void k_fill_i32(int32_t* p, int32_t v, int64_t n) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) p[i] = v;
-}
-
-__global__ void k_unpack_bfs(const uint64_t* tp, const uint32_t* hops_in, int32_t* arr, int32_t* hops, int32_t n) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const uint64_t wd = tp[i];
-  const bool inf = (wd >> 32) == 0xFFFFFFFFull;
-  arr[i] = inf ? INT32_MAX : (int32_t)(wd >> 32);
-  const uint32_t hv = hops_in[i];
-  hops[i] = (inf || hv == 0xFFFFFFFFu) ? INT32_MAX : (int32_t)hv;
-}
-
-// ---------------------------------------------------------------------------------------------
-// Connected components (per-seed temporal reach)
-
-__global__ void k_cc_label(const int32_t* touched, const int32_t* tcnt, int32_t seed, int32_t comp, uint64_t* tp,
-                           int32_t* label, uint8_t* reached) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int n = *tcnt;
-  if (i < n) {
-    const int y = touched[i];
-    label[y] = comp;
-    reached[y] = 1;
-    tp[y] = kTpInf;
-  }
-  if (i == 0) {
-    label[seed] = comp;
-    reached[seed] = 1;
-    tp[seed] = kTpInf;
-  }
-}
-
-__global__ void k_cc_find_seed(const uint8_t* reached, const int32_t* deg, int32_t from, int32_t to, int32_t* best) {
-  const int v = from + blockIdx.x * blockDim.x + threadIdx.x;
-  if (v < to && !reached[v] && deg[v] > 9) atomicMin(best, v);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -633,102 +352,12 @@ __global__ void k_gc_first(GraphView g, Work w, const int32_t* deg, int32_t n, i
 }
 
 // Host side: the queue entries of one vertex (itself or its slices).
-static int32_t seed_entries(const GraphHandle& h, int32_t v, std::vector<int32_t>& out) {
-  out.clear();
-  const int32_t a = h.slice_first_host[(size_t)v], b = h.slice_first_host[(size_t)v + 1];
-  if (a == b) out.push_back(v);
-  else
-    for (int32_t j = a; j < b; ++j) out.push_back(-(j + 1));
-  return (int32_t)out.size();
-}
-
-// Work view of a handle with a freshly zeroed counter (one per decode launch, in stream order).
-static Work work_of(GraphHandle& h) {
-  int32_t* ctr = reinterpret_cast<int32_t*>(h.s_sum.as<char>() + 4000);
-  cudaMemsetAsync(ctr, 0, sizeof(int32_t), h.stream);
-  return Work{h.d_items.as<WorkItem>(), h.d_slices.as<SliceState>(), h.d_slice_first.as<int32_t>(), ctr, h.nitems,
-              h.d_order.as<int32_t>(), h.norder};
-}
-
-// Grid of a persistent decode launch over `work` units.
-static unsigned decode_grid(const GraphHandle& h, int64_t work) {
-  const int64_t cap = (int64_t)h.sm_count * 2;
-  return (unsigned)std::max<int64_t>(1, std::min<int64_t>(cap, (work + kBlock - 1) / kBlock));
-}
-
-// Grid of a sweep over the schedule: one entry per thread.
-static unsigned sweep_grid(const GraphHandle& h) { return std::max(1u, grid_for(h.norder, kBlock)); }
-
-// Level loop of phase 1 from an initialised queue of qn entries; returns the levels executed.
-static int run_bfs_levels(GraphHandle& h, BfsArgs a, DevBuf& q0, DevBuf& q1, int32_t qn, uint32_t& wave, int& rc) {
-  int levels = 0;
-  DevBuf* cur = &q0;
-  DevBuf* nxt = &q1;
-  rc = TGA_OK;
-  while (qn > 0) {
-    if (levels > (1 << 22)) { rc = fail(TGA_E_TIMEOUT, "BFS level cap reached"); return levels; }
-    a.q = cur->as<int32_t>();
-    a.nq = nxt->as<int32_t>();
-    a.wave = ++wave;
-    cudaMemsetAsync(a.ncnt, 0, sizeof(int32_t), h.stream);
-    const Work w = work_of(h);
-    cudaEvent_t* ev = h.kernel_begin();
-    KL(k_bfs_level, decode_grid(h, qn))(h.view, w, a, qn);
-    h.kernel_end(ev);
-    cudaMemcpyAsync(h.h_pinned, a.ncnt, sizeof(int32_t), cudaMemcpyDeviceToHost, h.stream);
-    if (cudaStreamSynchronize(h.stream) != cudaSuccess) { rc = fail(TGA_E_CUDA, "BFS level failed"); return levels; }
-    qn = (int32_t)h.h_pinned[0];
-    std::swap(cur, nxt);
-    ++levels;
-  }
-  return levels;
-}
-
-static int bfs_buffers(GraphHandle& h) {
-  const size_t nv = (size_t)h.view.max_vertex;
-  const size_t qcap = nv + (size_t)h.nslices + 1;
-  int rc;
-  if ((rc = h.s_a.ensure(nv * 8)) || (rc = h.s_b.ensure(nv * 4)) || (rc = h.s_q0.ensure(qcap * 4)) ||
-      (rc = h.s_q1.ensure(qcap * 4)) || (rc = h.s_cnt.ensure(64)) || (rc = h.s_c.ensure(nv * 4)))
-    return rc;
-  return TGA_OK;
-}
-
 }  // namespace tga
 
 using namespace tga;
 
 // ---------------------------------------------------------------------------------------------
 // C ABI
-
-#define TGA_TRY(expr)            \
-  do {                           \
-    int rc_ = (expr);            \
-    if (rc_) return rc_;         \
-  } while (0)
-
-static int finish(GraphHandle& h, unsigned long long* edges_dev) {
-  if (edges_dev) {
-    unsigned long long e = 0;
-    cudaMemcpyAsync(&h.h_pinned[8], edges_dev, sizeof e, cudaMemcpyDeviceToHost, h.stream);
-    const int rc = h.end_call();
-    std::memcpy(&e, &h.h_pinned[8], sizeof e);
-    h.timing.edges_decoded = (int64_t)e;
-    return rc;
-  }
-  return h.end_call();
-}
-
-static unsigned long long* edge_counter(GraphHandle& h) {
-  if (h.s_sum.ensure(4096)) return nullptr;
-  unsigned long long* p = reinterpret_cast<unsigned long long*>(h.s_sum.as<char>() + 4032);
-  cudaMemsetAsync(p, 0, sizeof(unsigned long long), h.stream);
-  return p;
-}
-
-static uint64_t pass_bytes(const GraphHandle& h) {
-  return h.info.graph_bytes + h.info.timestamp_bytes + h.info.index_bytes;
-}
 
 extern "C" {
 
@@ -803,141 +432,6 @@ int tga_decode_all(tga_graph* gp, int64_t* offsets, int32_t* dst, int64_t* ts, i
   cudaMemcpyAsync(dst, h.s_f.p, (size_t)m * 4, cudaMemcpyDeviceToHost, h.stream);
   cudaMemcpyAsync(ts, h.s_g.p, (size_t)m * 8, cudaMemcpyDeviceToHost, h.stream);
   return h.end_call();
-}
-
-int tga_bfs(tga_graph* gp, int32_t src, int64_t t_lo, int64_t t_hi, int32_t* arrival_out, int32_t* hops_out) {
-  if (!gp) return fail(TGA_E_ARG, "null graph");
-  GraphHandle& h = *gp;
-  if (src < 0) src = h.cfg.bfs_start_vertex;
-  if (src < 0 || src >= h.view.max_vertex) return fail(TGA_E_ARG, "source out of range");
-  if (t_lo >= t_hi) return fail(TGA_E_ARG, "empty time window");
-  const int32_t nv = h.view.max_vertex;
-  TGA_TRY(bfs_buffers(h));
-  TGA_TRY(h.begin_call());
-  unsigned long long* edges = edge_counter(h);
-  BfsArgs a{};
-  a.tp = h.s_a.as<uint64_t>();
-  a.stamp = h.s_b.as<uint32_t>();
-  a.ncnt = h.s_cnt.as<int32_t>();
-  a.lo = t_lo;
-  a.hi = t_hi;
-  a.edges = edges;
-  KL(k_fill_u64, grid_for(nv, kBlock))(a.tp, kTpInf, nv);
-  cudaMemsetAsync(a.stamp, 0, (size_t)nv * 4, h.stream);
-  const uint64_t start = (uint64_t)std::max<int64_t>(t_lo, 0) << 32;
-  cudaMemcpyAsync(a.tp + src, &start, 8, cudaMemcpyHostToDevice, h.stream);
-  std::vector<int32_t> seed;
-  const int32_t sq = src < h.view.n ? seed_entries(h, src, seed) : 0;
-  if (sq) cudaMemcpyAsync(h.s_q0.p, seed.data(), (size_t)sq * 4, cudaMemcpyHostToDevice, h.stream);
-  uint32_t wave = 0;
-  int rc = TGA_OK;
-  int levels = run_bfs_levels(h, a, h.s_q0, h.s_q1, sq, wave, rc);
-  if (rc) return rc;
-  // Phase 2: hop levels over tight edges.
-  uint32_t* hops_u = h.s_c.as<uint32_t>();
-  cudaMemsetAsync(hops_u, 0xFF, (size_t)nv * 4, h.stream);
-  cudaMemsetAsync(hops_u + src, 0, 4, h.stream);
-  if (sq) cudaMemcpyAsync(h.s_q0.p, seed.data(), (size_t)sq * 4, cudaMemcpyHostToDevice, h.stream);
-  {
-    DevBuf* cur = &h.s_q0;
-    DevBuf* nxt = &h.s_q1;
-    int32_t qn = sq;
-    for (uint32_t level = 0; qn > 0; ++level) {
-      a.q = cur->as<int32_t>();
-      a.nq = nxt->as<int32_t>();
-      cudaMemsetAsync(a.ncnt, 0, sizeof(int32_t), h.stream);
-      const Work w = work_of(h);
-      cudaEvent_t* ev = h.kernel_begin();
-      KL(k_bfs_hops, decode_grid(h, qn))(h.view, w, a, qn, hops_u, level);
-      h.kernel_end(ev);
-      cudaMemcpyAsync(h.h_pinned, a.ncnt, sizeof(int32_t), cudaMemcpyDeviceToHost, h.stream);
-      TGA_CUDA_TRY(cudaStreamSynchronize(h.stream));
-      qn = (int32_t)h.h_pinned[0];
-      std::swap(cur, nxt);
-      ++levels;
-    }
-  }
-  int32_t* arr = h.s_q0.as<int32_t>();
-  int32_t* hops = h.s_q1.as<int32_t>();
-  KL(k_unpack_bfs, grid_for(nv, kBlock))(a.tp, hops_u, arr, hops, nv);
-  if (arrival_out) cudaMemcpyAsync(arrival_out, arr, (size_t)nv * 4, cudaMemcpyDeviceToHost, h.stream);
-  if (hops_out) cudaMemcpyAsync(hops_out, hops, (size_t)nv * 4, cudaMemcpyDeviceToHost, h.stream);
-  h.timing.iterations = levels;
-  return finish(h, edges);
-}
-
-int tga_cc(tga_graph* gp, int64_t t_lo, int64_t t_hi, int32_t flags, int32_t* label_out, int32_t* components_out) {
-  if (!gp) return fail(TGA_E_ARG, "null graph");
-  GraphHandle& h = *gp;
-  if (t_lo >= t_hi) return fail(TGA_E_ARG, "empty time window");
-  const int32_t nv = h.view.max_vertex;
-  TGA_TRY(bfs_buffers(h));
-  TGA_TRY(h.s_d.ensure((size_t)nv * 4));   // labels
-  TGA_TRY(h.s_e.ensure((size_t)nv));       // reached
-  TGA_TRY(h.s_f.ensure((size_t)nv * 4));   // touched list
-  TGA_TRY(h.begin_call());
-  unsigned long long* edges = edge_counter(h);
-  BfsArgs a{};
-  a.tp = h.s_a.as<uint64_t>();
-  a.stamp = h.s_b.as<uint32_t>();
-  a.ncnt = h.s_cnt.as<int32_t>();
-  a.tcnt = h.s_cnt.as<int32_t>() + 4;
-  a.touched = h.s_f.as<int32_t>();
-  int32_t* best = h.s_cnt.as<int32_t>() + 8;
-  a.lo = t_lo;
-  a.hi = t_hi;
-  a.edges = edges;
-  int32_t* label = h.s_d.as<int32_t>();
-  uint8_t* reached = h.s_e.as<uint8_t>();
-  KL(k_fill_u64, grid_for(nv, kBlock))(a.tp, kTpInf, nv);
-  KL(k_fill_i32, grid_for(nv, kBlock))(label, -1, nv);
-  cudaMemsetAsync(a.stamp, 0, (size_t)nv * 4, h.stream);
-  cudaMemsetAsync(reached, 0, (size_t)nv, h.stream);
-  const int32_t limit = (int32_t)(0.8 * h.view.max_label);
-  const int32_t end = std::min(std::min(h.view.max_label, nv), h.view.n);
-  int64_t total = 0;
-  int small_run = 0, comp = 0, levels = 0;
-  uint32_t wave = 0;
-  int32_t v = std::max(h.cfg.cc_vertex_begin, 0);
-  const uint64_t start = (uint64_t)std::max<int64_t>(t_lo, 0) << 32;
-  std::vector<int32_t> seedq;
-  while (v < end) {
-    if ((flags & TGA_CC_EARLY_EXIT) && total > limit) break;
-    // Next seed: smallest unreached vertex >= v with outdegree > 9, searched in growing chunks.
-    int32_t seed = INT32_MAX;
-    for (int32_t from = v, chunk = 4096; from < end && seed == INT32_MAX; from += chunk, chunk *= 2) {
-      const int32_t to = (int32_t)std::min<int64_t>((int64_t)from + chunk, end);
-      h.h_pinned[20] = INT32_MAX;
-      cudaMemcpyAsync(best, &h.h_pinned[20], 4, cudaMemcpyHostToDevice, h.stream);
-      KL(k_cc_find_seed, grid_for(to - from, kBlock))(reached, h.d_deg.as<int32_t>(), from, to, best);
-      cudaMemcpyAsync(&h.h_pinned[21], best, 4, cudaMemcpyDeviceToHost, h.stream);
-      TGA_CUDA_TRY(cudaStreamSynchronize(h.stream));
-      seed = (int32_t)h.h_pinned[21];
-    }
-    if (seed == INT32_MAX) break;
-    h.h_pinned[22] = 0;
-    cudaMemcpyAsync(a.tcnt, &h.h_pinned[22], 4, cudaMemcpyHostToDevice, h.stream);
-    cudaMemcpyAsync(a.tp + seed, &start, 8, cudaMemcpyHostToDevice, h.stream);
-    const int32_t sq = seed_entries(h, seed, seedq);
-    cudaMemcpyAsync(h.s_q0.p, seedq.data(), (size_t)sq * 4, cudaMemcpyHostToDevice, h.stream);
-    int rc = TGA_OK;
-    levels += run_bfs_levels(h, a, h.s_q0, h.s_q1, sq, wave, rc);
-    if (rc) return rc;
-    cudaMemcpyAsync(&h.h_pinned[23], a.tcnt, 4, cudaMemcpyDeviceToHost, h.stream);
-    TGA_CUDA_TRY(cudaStreamSynchronize(h.stream));
-    const int32_t reach = (int32_t)h.h_pinned[23];
-    KL(k_cc_label, grid_for(std::max(reach, 1), kBlock))(a.touched, a.tcnt, seed, comp, a.tp, label, reached);
-    ++comp;
-    total += reach + 1;
-    if (reach + 1 < 5) ++small_run;
-    else small_run = 0;
-    if ((flags & TGA_CC_EARLY_EXIT) && small_run > 50) break;
-    v = seed + 1;
-  }
-  if (label_out) cudaMemcpyAsync(label_out, label, (size_t)nv * 4, cudaMemcpyDeviceToHost, h.stream);
-  if (components_out) *components_out = comp;
-  h.timing.iterations = levels;
-  return finish(h, edges);
 }
 
 int tga_pagerank(tga_graph* gp, int32_t iters, float damping, float alpha, int64_t t_lo, int64_t t_hi, float* rank_out) {

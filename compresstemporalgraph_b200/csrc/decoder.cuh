@@ -115,6 +115,7 @@ __device__ __forceinline__ int parse_record(const GraphView& g, ListState& st, M
     // most 2*(its degree + the largest degree)+1 blocks; anything larger is corrupt.
     if (bc < 0 || bc > 2 * d + 2 * g.max_list + 1) { set_err(g, kErrCode); return -1; }
     mask.bpos = pos;
+#pragma unroll 1
     for (int i = 0; i < bc; ++i) {
       const int b = (int)read_gamma(g, g.g, pos) + (i ? 1 : 0);
       total += b;
@@ -131,6 +132,7 @@ __device__ __forceinline__ bool parse_extra(const GraphView& g, ListState& st, i
     if (mc < 0 || mc > d) { set_err(g, kErrCode); return false; }
     if (mc) {
       st.mpos = pos;
+#pragma unroll 1
       for (int i = 0; i < mc; ++i) {
         read_gamma(g, g.g, pos);
         extra -= (int)read_gamma(g, g.g, pos) + 2;
@@ -145,6 +147,7 @@ __device__ __forceinline__ bool parse_extra(const GraphView& g, ListState& st, i
     if (ic < 0 || ic > d) { set_err(g, kErrCode); return false; }
     if (ic) {
       st.ipos = pos;
+#pragma unroll 1
       for (int i = 0; i < ic; ++i) {
         read_gamma(g, g.g, pos);
         extra -= (int)read_gamma(g, g.g, pos) + g.min_interval;
@@ -167,6 +170,33 @@ __device__ __forceinline__ bool parse_extra(const GraphView& g, ListState& st, i
 template <int L>
 __device__ __forceinline__ int deep_next(const GraphView& g, DeepState& d);
 
+// Loads checkpoint cp (list cp.v at its edge cp.first) into level L and its chain into the levels
+// below (a list at level L has at most kMaxLevels-1-L further levels).
+template <int L>
+__device__ __forceinline__ void load_checkpoint(DeepState& d, const SliceState& cp) {
+  d.lv[L - 1] = cp.top;
+  d.lv[L - 1].x = cp.v;
+  d.lv[L - 1].emitted = cp.first;
+  if (cp.chain) {
+    if constexpr (L < kMaxLevels - 1) {
+      d.mask[L] = cp.deep.mask[0];
+      d.lv[L] = cp.deep.lv[0];
+    }
+    if constexpr (L + 1 < kMaxLevels - 1) {
+      d.mask[L + 1] = cp.deep.mask[1];
+      d.lv[L + 1] = cp.deep.lv[1];
+    }
+  }
+}
+
+// First slice of x (its checkpoint at edge 0 is the state right after parsing the record), or
+// null if x is not sliced (or checkpoints are not available yet).
+__device__ __forceinline__ const SliceState* first_checkpoint(const GraphView& g, int x) {
+  if (!g.slice_first || x < 0 || x >= g.n) return nullptr;
+  const int s0 = g.slice_first[x];
+  return s0 != g.slice_first[x + 1] ? &g.slices[s0] : nullptr;
+}
+
 // Skips k values of level L (>= 1).  A long skip over a list that has slice checkpoints restores
 // the last checkpoint at or before the target: the checkpoint's level 0 becomes level L and its
 // chain levels L+1.. (a list referenced at level L has at most kMaxLevels-1-L further levels), so
@@ -186,23 +216,12 @@ __device__ __forceinline__ void deep_skip(const GraphView& g, DeepState& d, int 
       }
       const SliceState& cp = g.slices[lo];
       if (cp.first > st.emitted) {
-        d.lv[L - 1] = cp.top;
-        d.lv[L - 1].x = cp.v;
-        d.lv[L - 1].emitted = cp.first;
-        if (cp.chain) {
-          if constexpr (L < kMaxLevels - 1) {
-            d.mask[L] = cp.deep.mask[0];
-            d.lv[L] = cp.deep.lv[0];
-          }
-          if constexpr (L + 1 < kMaxLevels - 1) {
-            d.mask[L + 1] = cp.deep.mask[1];
-            d.lv[L + 1] = cp.deep.lv[1];
-          }
-        }
+        load_checkpoint<L>(d, cp);
         k = target - cp.first;
       }
     }
   }
+#pragma unroll 1
   for (int i = 0; i < k && i <= g.max_list; ++i)
     if (deep_next<L>(g, d) == kInf) break;
 }
@@ -269,9 +288,14 @@ __device__ __forceinline__ void mask_start(const GraphView& g, DeepState& d, int
   }
 }
 
-// Opens level L (>= 1) on vertex x; returns its outdegree.
+// Opens level L (>= 1) on vertex x; returns its outdegree.  A sliced (long) list is opened from
+// its first checkpoint: parsing its record would walk its whole multiples and intervals sections.
 template <int L>
 __device__ __forceinline__ int deep_open(const GraphView& g, DeepState& d, int x) {
+  if (const SliceState* cp = first_checkpoint(g, x)) {
+    load_checkpoint<L>(d, *cp);
+    return g.deg[x];
+  }
   ListState& st = d.lv[L - 1];
   int ref, bc, copied, total;
   uint64_t pos;
@@ -357,12 +381,21 @@ struct EdgeCursor {
 
   __device__ __forceinline__ explicit EdgeCursor(DeepState* d) : deep(d) {}
 
-  // Returns the outdegree.
+  // Returns the outdegree.  A sliced list starts from its first checkpoint (see deep_open).
   __device__ __forceinline__ int open(const GraphView& g, int v) {
     x = v;
     remaining = 0;
     chain = 0;
     if (v >= g.n) return 0;  // ids past the files' vertex count have empty lists
+    if (const SliceState* cp = first_checkpoint(g, v)) {
+      top = cp->top;
+      chain = cp->chain;
+      if (chain) *deep = cp->deep;
+      ts.init(g.t, cp->tpos);
+      prev = cp->prev;
+      remaining = g.deg[v];
+      return remaining;
+    }
     remaining = top_open(g, top, deep, v, chain);
     if (remaining > 0) {
       ts.init(g.t, ef_get(g, g.tef, (uint64_t)v));

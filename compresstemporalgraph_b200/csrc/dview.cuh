@@ -56,6 +56,7 @@ struct GraphView {
   // blocks of a referenced list; null until the work decomposition is built.
   const struct SliceState* slices;
   const int32_t* slice_first;
+  const int32_t* deg;    // outdegrees (set with the slices)
   int32_t seek_min;      // skip blocks longer than this seek through a checkpoint
   // Device-global copy of this view.  Out-of-line decoder routines take it instead of the kernel
   // parameter, whose address would otherwise force a local-memory copy read by the hot loop.
@@ -139,11 +140,25 @@ __device__ __forceinline__ uint64_t read_zeta(const GraphView& g, const Stream& 
 
 // ---- Elias-Fano access ---------------------------------------------------------------------
 
+// Position of the (r+1)-th set bit of w (r < popcount(w)), by halving with population counts.
 __device__ __forceinline__ int nth_set_bit64(uint64_t w, int r) {
-  const uint32_t lo = (uint32_t)w;
-  const int c = __popc(lo);
-  if (r < c) return (int)__fns(lo, 0, r + 1);
-  return 32 + (int)__fns((uint32_t)(w >> 32), 0, r - c + 1);
+  int pos = 0;
+  uint32_t x = (uint32_t)w;
+  int c = __popc(x);
+  if (r >= c) {
+    r -= c;
+    pos = 32;
+    x = (uint32_t)(w >> 32);
+  }
+  for (int half = 16; half >= 2; half >>= 1) {
+    c = __popc(x & ((1u << half) - 1u));
+    if (r >= c) {
+      r -= c;
+      pos += half;
+      x >>= half;
+    }
+  }
+  return pos + (r >= (int)(x & 1u));
 }
 
 // Position of the i-th one (0-based) of the upper bits.
@@ -152,6 +167,7 @@ __device__ __forceinline__ uint64_t ef_select(const GraphView& g, const EFView& 
   int r = (int)(i & 63);
   uint64_t wi = p >> 6;
   uint64_t w = __ldg(e.upper + wi) & (~0ull << (p & 63));
+#pragma unroll 1
   for (int guard = 0; guard < 4096; ++guard) {
     const int c = __popcll(w);
     if (r < c) return wi * 64 + (uint64_t)nth_set_bit64(w, r);

@@ -317,7 +317,7 @@ int load_graph(GraphHandle& h, const std::string& dir, const std::string& base, 
   h.degrees = std::move(deg);
   const char* env_slice = std::getenv("TGA_SLICE_EDGES");
   const char* env_item = std::getenv("TGA_ITEM_EDGES");
-  return build_work(h, env_slice ? std::atoi(env_slice) : 1024, env_item ? std::atoi(env_item) : 256);
+  return build_work(h, env_slice ? std::atoi(env_slice) : kDefaultSliceEdges, env_item ? std::atoi(env_item) : 256);
 }
 
 int publish_view(GraphHandle& h) {
@@ -334,6 +334,7 @@ int build_work(GraphHandle& h, int32_t slice_len, int32_t item_edges) {
   // The build walks the lists without seeking (checkpoints are being made).
   v.slices = nullptr;
   v.slice_first = nullptr;
+  v.deg = nullptr;
   v.seek_min = INT32_MAX;
   if (int rc = publish_view(h)) return rc;
   const int32_t nd = (int32_t)h.degrees.size();
@@ -427,6 +428,11 @@ int build_work(GraphHandle& h, int32_t slice_len, int32_t item_edges) {
     for (int b = (int)bins.size() - 1; b >= 0; --b) order.insert(order.end(), bins[(size_t)b].begin(), bins[(size_t)b].end());
   }
   h.norder = (int32_t)order.size();
+  // A traversal level sweeps all lists instead of its queue once the queue holds at least
+  // 1/TGA_DENSE_DIV (default 16) of the schedule's entries.
+  const char* env_dense = std::getenv("TGA_DENSE_DIV");
+  const int dense_div = env_dense ? std::max(1, std::atoi(env_dense)) : 16;
+  h.dense_min = std::max<int32_t>(1, h.norder / dense_div);
   h.nslices = (int64_t)packed.size();
   h.slice_len = slice_len;
   h.item_edges = item_edges;
@@ -446,6 +452,7 @@ int build_work(GraphHandle& h, int32_t slice_len, int32_t item_edges) {
   h.slice_first_host = std::move(slice_first);
   v.slices = h.d_slices.as<SliceState>();
   v.slice_first = h.d_slice_first.as<int32_t>();
+  v.deg = h.d_deg.as<int32_t>();
   v.seek_min = std::max(16, slice_len / 2);
   return publish_view(h);
 }

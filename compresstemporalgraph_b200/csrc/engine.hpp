@@ -54,6 +54,7 @@ struct GraphHandle {
   DevBuf d_order;
   DevBuf d_view;                     // device-global copy of `view` (GraphView::self)
   int32_t norder = 0;
+  int32_t dense_min = 1;             // traversal levels with at least this many entries sweep all lists
   std::vector<uint8_t> chain_host;   // list copies from a reference chain
   int32_t nitems = 0, nslice_items = 0;
   int64_t nslices = 0;
@@ -78,6 +79,11 @@ struct GraphHandle {
   int check_device_error();
   ~GraphHandle();
 };
+
+// Default slice length: short enough that a frontier level holding one slice of a hub is not
+// bound by a single thread's sequential decode, long enough that checkpoints stay a fraction of
+// the compressed bytes.
+constexpr int32_t kDefaultSliceEdges = 64;
 
 int load_graph(GraphHandle& h, const std::string& dir, const std::string& base, const tga_dataset_cfg& cfg);
 // (Re)builds slices and work items: lists longer than slice_len edges are cut into slices,

@@ -1,0 +1,267 @@
+// Shared pieces of the fused decode kernels: the launch macro, work views, queue handling and
+// the two sweep drivers (class-ordered schedule and frontier queues), plus the host-side helpers
+// that every entry point uses.
+#pragma once
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "engine.hpp"
+
+namespace tga {
+
+constexpr int kBlock = 256;
+constexpr uint64_t kTpInf = ~0ull;
+constexpr uint32_t kColorInf = 0xFFFFFFFFu;
+
+// Launches a kernel of kBlock threads on the handle's stream and counts it in the call's timing.
+#define KL(kernel, grid) ++h.timing.launches, kernel<<<(grid), kBlock, 0, h.stream>>>
+// Decode kernels: 2 blocks of 256 threads per SM (128 registers, no spills).
+#define TGA_DECODE_BOUNDS __launch_bounds__(kBlock, 2)
+
+// Per-edge term of the neighbour-access checksum: the checksum of a list is the sum (mod 2^64)
+// of edge_hash over its edges, so slices can add their parts; the edge index keeps it
+// order-sensitive.  The oracle computes the same sum.
+__host__ __device__ __forceinline__ uint64_t edge_hash(uint32_t v, uint32_t i, int32_t y, int64_t t) {
+  uint64_t z = (((uint64_t)v << 32) | i) * 0x9E3779B97F4A7C15ull;
+  z ^= (uint64_t)(uint32_t)y * 0xC2B2AE3D27D4EB4Full;
+  z ^= (uint64_t)t * 0x165667B19E3779F9ull;
+  z ^= z >> 31;
+  z *= 0xBF58476D1CE4E5B9ull;
+  z ^= z >> 29;
+  z *= 0x94D049BB133111EBull;
+  return z ^ (z >> 32);
+}
+
+__device__ __forceinline__ void add_edges(unsigned long long* ctr, unsigned long long mine) {
+  for (int o = 16; o; o >>= 1) mine += __shfl_down_sync(0xffffffffu, mine, o);
+  if ((threadIdx.x & 31) == 0 && mine) atomicAdd(ctr, mine);
+}
+
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double red[kBlock / 32];
+  for (int o = 16; o; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double s = 0;
+  if (threadIdx.x < 32) {
+    s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  }
+  return s;  // valid in thread 0
+}
+
+struct Work {
+  const WorkItem* items;
+  const SliceState* slices;
+  const int32_t* slice_first;
+  int32_t* next;          // work counter of the launch (zeroed before it)
+  int32_t nitems;
+  const int32_t* order;   // sweep schedule grouped by work class (vertex ids and -(slice+1))
+  int32_t norder;
+};
+
+// Opens queue entry e: a whole list (e >= 0) or one slice.  Returns the vertex.
+__device__ __forceinline__ int open_entry(const GraphView& g, const Work& w, int e, EdgeCursor& c, int& first,
+                                          int& count) {
+  if (e >= 0) {
+    first = 0;
+    count = c.open(g, e);
+    return e;
+  }
+  const SliceState& s = w.slices[-e - 1];
+  cursor_restore(g, c, s);
+  first = s.first;
+  count = s.count;
+  return s.v;
+}
+
+// Appends y (or all slices of y) to a queue.
+__device__ __forceinline__ void enqueue(const Work& w, int y, int32_t* q, int32_t* cnt) {
+  const int a = w.slice_first[y], b = w.slice_first[y + 1];
+  if (a == b) {
+    q[atomicAdd(cnt, 1)] = y;
+  } else {
+    const int base = atomicAdd(cnt, b - a);
+    for (int j = a; j < b; ++j) q[base + j - a] = -(j + 1);
+  }
+}
+
+// Edge filter shared by every traversal: in-window, first of equal consecutive successors,
+// successor inside [active_begin, max_vertex).
+__device__ __forceinline__ bool keep_edge(const GraphView& g, int64_t lo, int64_t hi, int y, int64_t t, int& prev_y) {
+  if (t < lo || t >= hi) return false;
+  if (y == prev_y) return false;
+  prev_y = y;
+  return y >= g.active_begin && y < g.max_vertex;
+}
+
+// Rank of the calling warp when warps are dealt round-robin over the blocks (warp k of block b has
+// rank k * gridDim.x + b): consecutive 32-entry chunks then go to different blocks, so a run of
+// entries of one long list is spread over the SMs instead of filling the first blocks.
+__device__ __forceinline__ int spread_warp_rank() {
+  return (int)((threadIdx.x >> 5) * gridDim.x + blockIdx.x);
+}
+
+// Sweep over the class-ordered schedule: thread i decodes entry i (a whole list or a slice).
+// Entries of one warp belong to the same work class, so the lanes open their lists together and
+// finish together.  Hooks (each inlined at its single call site): want(x) -> bool,
+// begin(x, first, count) -> bool (false: skip the list), edge(x, y, t) -> bool (false: stop the
+// list), end(x).  kWhole: a sliced list is decoded whole by the thread that draws its first slice
+// (for workloads that are sequential per list); its other slices are skipped.
+// kSpread: chunks of 32 entries are dealt by spread_warp_rank() (for persistent grids, where the
+// blocks holding the first entries would otherwise get all the slices of the first long lists).
+template <bool kWhole, bool kSpread = false, class Want, class Begin, class Edge, class End>
+__device__ __forceinline__ unsigned long long run_order(const GraphView& g, const Work& w, Want want, Begin begin,
+                                                        Edge edge, End end) {
+  unsigned long long edges = 0;
+  const int start = kSpread ? spread_warp_rank() * 32 + (int)(threadIdx.x & 31) : (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  for (int i = start; i < w.norder; i += gridDim.x * blockDim.x) {
+    const int e = w.order[i];
+    DeepState deep;
+    EdgeCursor c(&deep);
+    int x, first = 0, count;
+    if (e >= 0) {
+      x = e;
+      if (!want(x)) continue;
+      count = c.open(g, x);
+    } else {
+      const SliceState& s = w.slices[-e - 1];
+      x = s.v;
+      if (!want(x)) continue;
+      if (kWhole) {
+        if (s.first != 0) continue;
+        count = c.open(g, x);
+      } else {
+        cursor_restore(g, c, s);
+        first = s.first;
+        count = s.count;
+      }
+    }
+    if (count <= 0 || !begin(x, first, count)) continue;
+    int y;
+    int64_t t;
+    while (c.next(g, y, t)) {
+      ++edges;
+      if (!edge(x, y, t)) break;
+    }
+    end(x);
+  }
+  return edges;
+}
+
+// Flat loop over the entries q[0..qn) of a queue (vertices or slices); q may have been written
+// earlier in the same launch by other blocks (it is read through L2).
+template <class Begin, class Edge, class End>
+__device__ __forceinline__ unsigned long long drive_queue(const GraphView& g, const Work& w, const int32_t* q, int qn,
+                                                          Begin begin, Edge edge, End end) {
+  DeepState deep;
+  EdgeCursor c(&deep);
+  c.remaining = 0;
+  int cur = -1;
+  unsigned long long edges = 0;
+  // The first entry of a thread comes from its spread warp rank (consecutive entries, such as the
+  // slices of one list, land on different SMs); later ones come from the counter, offset by the
+  // thread count, so a queue shorter than the grid costs no atomics at all.
+  int i = spread_warp_rank() * 32 + (int)(threadIdx.x & 31);
+  for (;;) {
+    if (c.remaining <= 0) {
+      if (cur >= 0) {
+        end(cur);
+        cur = -1;
+      }
+      if (i < 0) i = (int)(gridDim.x * blockDim.x) + atomicAdd(w.next, 1);
+      if (i >= qn) break;
+      int first, count;
+      const int x = open_entry(g, w, __ldcg(q + i), c, first, count);
+      i = -1;
+      if (count <= 0 || !begin(x, first, count)) {
+        c.remaining = 0;
+        continue;
+      }
+      cur = x;
+      continue;
+    }
+    int y;
+    int64_t t;
+    if (!c.next(g, y, t)) continue;
+    ++edges;
+    if (!edge(cur, y, t)) c.remaining = 0;
+  }
+  return edges;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Fills
+
+static __global__ void k_fill_u64(uint64_t* p, uint64_t v, int64_t n) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
+}
+static __global__ void k_fill_f32(float* p, float v, int64_t n) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
+}
+static __global__ void k_fill_i32(int32_t* p, int32_t v, int64_t n) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
+}
+
+
+static int32_t seed_entries(const GraphHandle& h, int32_t v, std::vector<int32_t>& out) {
+  out.clear();
+  const int32_t a = h.slice_first_host[(size_t)v], b = h.slice_first_host[(size_t)v + 1];
+  if (a == b) out.push_back(v);
+  else
+    for (int32_t j = a; j < b; ++j) out.push_back(-(j + 1));
+  return (int32_t)out.size();
+}
+
+// Work view of a handle with a freshly zeroed counter (one per decode launch, in stream order).
+static Work work_of(GraphHandle& h) {
+  int32_t* ctr = reinterpret_cast<int32_t*>(h.s_sum.as<char>() + 4000);
+  cudaMemsetAsync(ctr, 0, sizeof(int32_t), h.stream);
+  return Work{h.d_items.as<WorkItem>(), h.d_slices.as<SliceState>(), h.d_slice_first.as<int32_t>(), ctr, h.nitems,
+              h.d_order.as<int32_t>(), h.norder};
+}
+
+// Grid of a persistent decode launch over `work` units.
+static unsigned decode_grid(const GraphHandle& h, int64_t work) {
+  const int64_t cap = (int64_t)h.sm_count * 2;
+  return (unsigned)std::max<int64_t>(1, std::min<int64_t>(cap, (work + kBlock - 1) / kBlock));
+}
+
+// Grid of a sweep over the schedule: one entry per thread.
+static unsigned sweep_grid(const GraphHandle& h) { return std::max(1u, grid_for(h.norder, kBlock)); }
+
+#define TGA_TRY(expr)            \
+  do {                           \
+    int rc_ = (expr);            \
+    if (rc_) return rc_;         \
+  } while (0)
+
+static int finish(GraphHandle& h, unsigned long long* edges_dev) {
+  if (edges_dev) {
+    unsigned long long e = 0;
+    cudaMemcpyAsync(&h.h_pinned[8], edges_dev, sizeof e, cudaMemcpyDeviceToHost, h.stream);
+    const int rc = h.end_call();
+    std::memcpy(&e, &h.h_pinned[8], sizeof e);
+    h.timing.edges_decoded = (int64_t)e;
+    return rc;
+  }
+  return h.end_call();
+}
+
+static unsigned long long* edge_counter(GraphHandle& h) {
+  if (h.s_sum.ensure(4096)) return nullptr;
+  unsigned long long* p = reinterpret_cast<unsigned long long*>(h.s_sum.as<char>() + 4032);
+  cudaMemsetAsync(p, 0, sizeof(unsigned long long), h.stream);
+  return p;
+}
+
+static uint64_t pass_bytes(const GraphHandle& h) {
+  return h.info.graph_bytes + h.info.timestamp_bytes + h.info.index_bytes;
+}
+
+}  // namespace tga

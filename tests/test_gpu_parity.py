@@ -216,6 +216,7 @@ def test_work_decomposition_does_not_change_results(pairs, shape, slice_edges, i
     referenced list); results must not depend on the decomposition."""
     p = pairs[shape]
     g = p.g
+    default = g.work_params()
     g.set_work_params(slice_edges, item_edges)
     try:
         wp = g.work_params()
@@ -240,4 +241,4 @@ def test_work_decomposition_does_not_change_results(pairs, shape, slice_edges, i
         odeg, oavg = p.o.degree(p.ml, p.mv, p.act, 0, 0)
         assert np.array_equal(deg, odeg) and np.array_equal(avg, oavg)
     finally:
-        g.set_work_params(1024, 256)
+        g.set_work_params(default["slice_edges"], default["item_edges"])
