@@ -114,7 +114,7 @@ __global__ void TGA_DECODE_BOUNDS k_pr_iter(GraphView g, Work w, PrArgs a) {
   float local = 0.0f, c0 = 0.0f;
   double total = 0.0;
   int prev_y = -1;
-  const unsigned long long mine = run_order<false>(
+  const unsigned long long mine = run_order<false, false, true>(
       g, w,
       [&](int v) {
         if (v < g.active_begin || v >= g.max_label) return false;
@@ -193,7 +193,7 @@ __global__ void TGA_DECODE_BOUNDS k_hits_hub(GraphView g, Work w, float* hub, co
   const float sa = (aprev && *aprev > 0) ? (float)(1.0 / sqrt(*aprev)) : 1.0f;
   float acc = 0.0f;
   int prev_y = -1;
-  const unsigned long long mine = run_order<false>(
+  const unsigned long long mine = run_order<false, false, true>(
       g, w, [&](int v) { return v >= g.active_begin && v < g.max_label; },
       [&](int, int, int) {
         acc = 0.0f;
@@ -215,7 +215,7 @@ __global__ void TGA_DECODE_BOUNDS k_hits_auth(GraphView g, Work w, const float* 
   const float sh = *hsum > 0 ? (float)(1.0 / sqrt(*hsum)) : 1.0f;
   float hn = 0.0f;
   int prev_y = -1;
-  const unsigned long long mine = run_order<false>(
+  const unsigned long long mine = run_order<false, false, true>(
       g, w, [&](int v) { return v >= g.active_begin && v < g.max_label && hub[v] != 0.0f; },
       [&](int v, int, int) {
         hn = hub[v] * sh;
@@ -448,6 +448,7 @@ int tga_pagerank(tga_graph* gp, int32_t iters, float damping, float alpha, int64
   TGA_TRY(h.s_e.ensure((size_t)nv * 4));
   TGA_TRY(h.s_g.ensure((size_t)(iters + 1) * 8));
   TGA_TRY(h.begin_call());
+  prepare_runs(h, t_lo, t_hi);
   unsigned long long* edges = edge_counter(h);
   const float base = (1.0f - damping) / (float)h.view.max_label;
   float* bufs[3] = {h.s_a.as<float>(), h.s_b.as<float>(), h.s_c.as<float>()};
@@ -497,6 +498,7 @@ int tga_hits(tga_graph* gp, int32_t iters, int32_t mode, int64_t t_lo, int64_t t
   TGA_TRY(h.s_c.ensure((size_t)nv * 4));
   TGA_TRY(h.s_g.ensure((size_t)(2 * iters + 2) * 8));
   TGA_TRY(h.begin_call());
+  prepare_runs(h, t_lo, t_hi);
   unsigned long long* edges = edge_counter(h);
   float* hub = h.s_a.as<float>();
   float* auth[2] = {h.s_b.as<float>(), h.s_c.as<float>()};
@@ -675,7 +677,8 @@ int tga_pagerank_noalloc(tga_graph* gp, int32_t iters, float damping, float alph
   // Edge counter and work counter start at zero.
   TGA_CUDA_TRY(cudaMemsetAsync(s + kPrNoAllocCountersOff, 0, 256, h.stream));
   const Work w{h.d_items.as<WorkItem>(), h.d_slices.as<SliceState>(), h.d_slice_first.as<int32_t>(), next, h.nitems,
-               h.d_order.as<int32_t>(), h.norder};
+               h.d_order.as<int32_t>(), h.norder, h.d_run_first.as<int32_t>()};
+  prepare_runs(h, t_lo, t_hi);  // fills the handle's run table (allocated at open)
   const bool windowed = !(t_lo <= 0 && t_hi == TGA_T_MAX);
   const float base = (1.0f - damping) / (float)h.view.max_label;
   KL(k_fill_f32, grid_for(nv, kBlock))(bufs[0], 1.0f / (float)nv, nv);

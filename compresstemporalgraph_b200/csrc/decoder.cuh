@@ -55,6 +55,14 @@ struct SliceState {
   int32_t count;    // edges in the slice
   int32_t first;    // index of the slice's first edge in the list of v
   int32_t chain;    // the list copies from a reference chain
+  int32_t run;      // the slice starts inside a run of equal successors: that run's index, else -1
+  int32_t pad;
+};
+
+// A run of equal successors that slices cut (slices.cuh): list `v`, edges from list index
+// `start`, overlapping the slices first_slice .. first_slice + nslices - 1.
+struct RunInfo {
+  int32_t v, start, first_slice, nslices;
 };
 
 // ---- merge step shared by all levels ---------------------------------------------------------

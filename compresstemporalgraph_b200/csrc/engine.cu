@@ -48,7 +48,7 @@ void DevBuf::release() {
 GraphHandle::~GraphHandle() {
   if (stream) cudaStreamSynchronize(stream);
   for (DevBuf* b : {&d_graph, &d_ts, &d_gl, &d_gu, &d_gs, &d_tl, &d_tu, &d_ts_samples, &d_err, &d_deg, &d_slices,
-                    &d_items, &d_slice_first, &d_order, &d_view, &s_a, &s_b, &s_c, &s_d, &s_e, &s_f, &s_g, &s_q0, &s_q1, &s_cnt, &s_sum})
+                    &d_items, &d_slice_first, &d_order, &d_runs, &d_run_pairs, &d_run_first, &d_view, &s_a, &s_b, &s_c, &s_d, &s_e, &s_f, &s_g, &s_q0, &s_q1, &s_cnt, &s_sum})
     b->release();
   for (auto& k : ktimers) {
     if (k.a) cudaEventDestroy(k.a);
@@ -386,6 +386,33 @@ int build_work(GraphHandle& h, int32_t slice_len, int32_t item_edges) {
     }
     slice_first[(size_t)nd] = (int32_t)packed.size();
   }
+  // Runs of equal successors that slices cut: consecutive slices of a list that start inside the
+  // same run (the builder left the run's start index in `run`) form one run, which begins in the
+  // slice before the first of them.
+  std::vector<RunInfo> runs;
+  std::vector<int2> run_pairs;
+  for (int32_t x = 0; x < nd; ++x) {
+    const int32_t a = slice_first[(size_t)x], b = slice_first[(size_t)x + 1];
+    for (int32_t j = a; j < b; ++j) {
+      SliceState& sl = packed[(size_t)j];
+      const int32_t rs = sl.run;
+      if (rs < 0 || j == a) {
+        sl.run = -1;
+        continue;
+      }
+      if (!runs.empty() && runs.back().v == x && runs.back().start == rs &&
+          runs.back().first_slice + runs.back().nslices == j) {
+        ++runs.back().nslices;
+      } else {
+        runs.push_back(RunInfo{x, rs, j - 1, 2});
+      }
+      sl.run = (int32_t)runs.size() - 1;
+    }
+  }
+  for (size_t r = 0; r < runs.size(); ++r)
+    for (int32_t k = 0; k < runs[r].nslices; ++k) run_pairs.push_back(make_int2((int)r, runs[r].first_slice + k));
+  h.nruns = (int32_t)runs.size();
+  h.nrun_pairs = (int32_t)run_pairs.size();
   h.nslice_items = (int32_t)items.size();
   {
     constexpr int32_t kVertexCost = 4, kMaxRange = 4096;
@@ -440,6 +467,14 @@ int build_work(GraphHandle& h, int32_t slice_len, int32_t item_edges) {
   if ((rc = h.d_order.ensure(std::max<size_t>(1, order.size()) * 4))) return rc;
   if (!order.empty())
     TGA_CUDA_TRY(cudaMemcpy(h.d_order.p, order.data(), order.size() * 4, cudaMemcpyHostToDevice));
+  if ((rc = h.d_runs.ensure(std::max<size_t>(1, runs.size()) * sizeof(RunInfo))) ||
+      (rc = h.d_run_pairs.ensure(std::max<size_t>(1, run_pairs.size()) * sizeof(int2))) ||
+      (rc = h.d_run_first.ensure(std::max<size_t>(1, runs.size()) * 4)))
+    return rc;
+  if (!runs.empty()) {
+    TGA_CUDA_TRY(cudaMemcpy(h.d_runs.p, runs.data(), runs.size() * sizeof(RunInfo), cudaMemcpyHostToDevice));
+    TGA_CUDA_TRY(cudaMemcpy(h.d_run_pairs.p, run_pairs.data(), run_pairs.size() * sizeof(int2), cudaMemcpyHostToDevice));
+  }
   if ((rc = h.d_items.ensure(std::max<size_t>(1, items.size()) * sizeof(WorkItem))) ||
       (rc = h.d_slices.ensure(std::max<size_t>(1, packed.size()) * sizeof(SliceState))) ||
       (rc = h.d_slice_first.ensure(slice_first.size() * 4)))

@@ -52,6 +52,10 @@ struct GraphHandle {
   DevBuf d_slices, d_items, d_slice_first;
   // decode order of the sweeps (vertex ids >= 0 and -(slice+1)), grouped by work class
   DevBuf d_order;
+  // runs of equal successors cut by slices: RunInfo[nruns], (run, slice) pairs of the per-call
+  // pre-pass, and the per-call list index of each run's first in-window edge
+  DevBuf d_runs, d_run_pairs, d_run_first;
+  int32_t nruns = 0, nrun_pairs = 0;
   DevBuf d_view;                     // device-global copy of `view` (GraphView::self)
   int32_t norder = 0;
   int32_t dense_min = 1;             // traversal levels with at least this many entries sweep all lists

@@ -4,8 +4,10 @@
 // list decoded by one thread takes longer than the rest of the graph together).  At load time every
 // list longer than the slice length is cut into slices: a slice holds the complete decoder state at
 // its first edge (reference-chain levels, timestamp cursor, previous timestamp), so any thread can
-// resume decoding there.  Slices start only where the successor id changes, so the "first
-// in-window occurrence of equal consecutive successors" rule never spans two slices.
+// resume decoding there.  A slice may start inside a run of equal successors (lists are sorted, so
+// equal successors are adjacent); the "first in-window occurrence of equal consecutive successors"
+// rule then needs the position of the run's first in-window edge, which each call computes for
+// its window (k_run_first in sweep.cuh) for the few runs that slices cut.
 // The remaining (short) lists are grouped into work items of consecutive vertices holding about the
 // same number of edges as a slice.
 #pragma once
@@ -39,10 +41,13 @@ __device__ __forceinline__ void cursor_save(const EdgeCursor& c, SliceState& s, 
   s.v = v;
   s.first = first;
   s.count = 0;
+  s.run = -1;
+  s.pad = 0;
 }
 
-// One thread per long list: walks the list once and records a slice every >= `len` edges, at the
-// next edge whose successor differs from the previous one.  cap[b] slots are reserved per list.
+// One thread per long list: walks the list once and records a slice every `len` edges.  A slice
+// that starts inside a run of equal successors gets run = the list index where that run starts
+// (the host turns it into a run index).  cap[b] slots are reserved per list.
 static __global__ void k_build_slices(GraphView g, const int32_t* big_v, const int64_t* slot_base, int32_t nbig, int32_t len,
                                SliceState* out, int32_t* nslices) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
@@ -54,7 +59,7 @@ static __global__ void k_build_slices(GraphView g, const int32_t* big_v, const i
   EdgeCursor c(&deep);
   const int d = c.open(g, v);
   cursor_save(c, dst[0], v, 0);
-  int k = 1, last = 0, prev_y = -1;
+  int k = 1, last = 0, prev_y = -1, run_start = 0;
   for (int i = 0; i < d; ++i) {
     const bool cand = (i - last >= len) && k < cap;
     EdgeCursor saved(&saved_deep);
@@ -66,12 +71,14 @@ static __global__ void k_build_slices(GraphView g, const int32_t* big_v, const i
     int y;
     int64_t t;
     if (!c.next(g, y, t)) break;
-    if (cand && y != prev_y) {
+    if (cand) {
       dst[k - 1].count = i - last;
       cursor_save(saved, dst[k], v, i);
+      if (y == prev_y) dst[k].run = run_start;
       last = i;
       ++k;
     }
+    if (y != prev_y) run_start = i;
     prev_y = y;
   }
   dst[k - 1].count = d - last;

@@ -14,6 +14,7 @@ namespace tga {
 constexpr int kBlock = 256;
 constexpr uint64_t kTpInf = ~0ull;
 constexpr uint32_t kColorInf = 0xFFFFFFFFu;
+constexpr int kNoRunFilter = -2;
 
 // Launches a kernel of kBlock threads on the handle's stream and counts it in the call's timing.
 #define KL(kernel, grid) ++h.timing.launches, kernel<<<(grid), kBlock, 0, h.stream>>>
@@ -60,11 +61,16 @@ struct Work {
   int32_t nitems;
   const int32_t* order;   // sweep schedule grouped by work class (vertex ids and -(slice+1))
   int32_t norder;
+  // per run of equal successors cut by slices: list index of its first in-window edge for the
+  // call's window (INT32_MAX: none); read by the drivers with kRuns
+  const int32_t* run_first;
 };
 
-// Opens queue entry e: a whole list (e >= 0) or one slice.  Returns the vertex.
+// Opens queue entry e: a whole list (e >= 0) or one slice.  Returns the vertex; `lead` is the
+// leading-run filter of the entry (see RunFilter).
 __device__ __forceinline__ int open_entry(const GraphView& g, const Work& w, int e, EdgeCursor& c, int& first,
-                                          int& count) {
+                                          int& count, int& lead) {
+  lead = kNoRunFilter;
   if (e >= 0) {
     first = 0;
     count = c.open(g, e);
@@ -74,8 +80,33 @@ __device__ __forceinline__ int open_entry(const GraphView& g, const Work& w, int
   cursor_restore(g, c, s);
   first = s.first;
   count = s.count;
+  if (s.run >= 0 && w.run_first) lead = __ldg(w.run_first + s.run);
   return s.v;
 }
+
+// Dedup of a slice that starts inside a run of equal successors: while the slice's edges continue
+// that run, only the run's first in-window edge (list index `lead`, computed for the call's
+// window) reaches the algorithm; afterwards every edge does.  Algorithms that keep only the first
+// in-window occurrence of equal consecutive successors (keep_edge) run their sweeps with it.
+struct RunFilter {
+  int lead;   // list index to pass, or kNoRunFilter once past the leading run
+  int y_run;  // successor of the leading run (-1 before the first edge)
+  int idx;    // list index of the next edge
+  __device__ __forceinline__ void start(int lead_idx, int first) {
+    lead = lead_idx;
+    y_run = -1;
+    idx = first;
+  }
+  // true if edge (y) passes the filter
+  __device__ __forceinline__ bool pass(int y) {
+    const int i = idx++;
+    if (lead == kNoRunFilter) return true;
+    if (y_run < 0) y_run = y;
+    if (y == y_run) return i == lead;
+    lead = kNoRunFilter;
+    return true;
+  }
+};
 
 // Appends y (or all slices of y) to a queue.
 __device__ __forceinline__ void enqueue(const Work& w, int y, int32_t* q, int32_t* cnt) {
@@ -112,7 +143,8 @@ __device__ __forceinline__ int spread_warp_rank() {
 // (for workloads that are sequential per list); its other slices are skipped.
 // kSpread: chunks of 32 entries are dealt by spread_warp_rank() (for persistent grids, where the
 // blocks holding the first entries would otherwise get all the slices of the first long lists).
-template <bool kWhole, bool kSpread = false, class Want, class Begin, class Edge, class End>
+// kRuns: slices that start inside a run of equal successors pass their edges through RunFilter.
+template <bool kWhole, bool kSpread = false, bool kRuns = false, class Want, class Begin, class Edge, class End>
 __device__ __forceinline__ unsigned long long run_order(const GraphView& g, const Work& w, Want want, Begin begin,
                                                         Edge edge, End end) {
   unsigned long long edges = 0;
@@ -121,7 +153,8 @@ __device__ __forceinline__ unsigned long long run_order(const GraphView& g, cons
     const int e = w.order[i];
     DeepState deep;
     EdgeCursor c(&deep);
-    int x, first = 0, count;
+    RunFilter rf;
+    int x, first = 0, count, lead = kNoRunFilter;
     if (e >= 0) {
       x = e;
       if (!want(x)) continue;
@@ -137,13 +170,16 @@ __device__ __forceinline__ unsigned long long run_order(const GraphView& g, cons
         cursor_restore(g, c, s);
         first = s.first;
         count = s.count;
+        if (kRuns && s.run >= 0) lead = __ldg(w.run_first + s.run);
       }
     }
     if (count <= 0 || !begin(x, first, count)) continue;
+    if (kRuns) rf.start(lead, first);
     int y;
     int64_t t;
     while (c.next(g, y, t)) {
       ++edges;
+      if (kRuns && !rf.pass(y)) continue;
       if (!edge(x, y, t)) break;
     }
     end(x);
@@ -152,12 +188,14 @@ __device__ __forceinline__ unsigned long long run_order(const GraphView& g, cons
 }
 
 // Flat loop over the entries q[0..qn) of a queue (vertices or slices); q may have been written
-// earlier in the same launch by other blocks (it is read through L2).
-template <class Begin, class Edge, class End>
+// earlier in the same launch by other blocks (it is read through L2).  kRuns as in run_order.
+template <bool kRuns = false, class Begin, class Edge, class End>
 __device__ __forceinline__ unsigned long long drive_queue(const GraphView& g, const Work& w, const int32_t* q, int qn,
                                                           Begin begin, Edge edge, End end) {
   DeepState deep;
   EdgeCursor c(&deep);
+  RunFilter rf;
+  rf.start(kNoRunFilter, 0);
   c.remaining = 0;
   int cur = -1;
   unsigned long long edges = 0;
@@ -173,13 +211,14 @@ __device__ __forceinline__ unsigned long long drive_queue(const GraphView& g, co
       }
       if (i < 0) i = (int)(gridDim.x * blockDim.x) + atomicAdd(w.next, 1);
       if (i >= qn) break;
-      int first, count;
-      const int x = open_entry(g, w, __ldcg(q + i), c, first, count);
+      int first, count, lead;
+      const int x = open_entry(g, w, __ldcg(q + i), c, first, count, lead);
       i = -1;
       if (count <= 0 || !begin(x, first, count)) {
         c.remaining = 0;
         continue;
       }
+      if (kRuns) rf.start(lead, first);
       cur = x;
       continue;
     }
@@ -187,6 +226,7 @@ __device__ __forceinline__ unsigned long long drive_queue(const GraphView& g, co
     int64_t t;
     if (!c.next(g, y, t)) continue;
     ++edges;
+    if (kRuns && !rf.pass(y)) continue;
     if (!edge(cur, y, t)) c.remaining = 0;
   }
   return edges;
@@ -199,6 +239,34 @@ static __global__ void k_fill_u64(uint64_t* p, uint64_t v, int64_t n) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) p[i] = v;
 }
+// Per-call pre-pass for the runs of equal successors that slices cut: one thread per (run, slice
+// overlapping it) decodes the slice from its checkpoint and lowers run_first[run] to the list
+// index of the first in-window edge of the run within that slice.
+static __global__ void TGA_DECODE_BOUNDS k_run_first(GraphView g, const SliceState* slices, const RunInfo* runs,
+                                                     const int2* pairs, int32_t npairs, int64_t lo, int64_t hi,
+                                                     int32_t* run_first) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npairs) return;
+  const int2 pr = pairs[p];
+  const RunInfo r = runs[pr.x];
+  const SliceState& s = slices[pr.y];
+  DeepState deep;
+  EdgeCursor c(&deep);
+  cursor_restore(g, c, s);
+  int idx = s.first, y_run = -1, y;
+  int64_t t;
+  while (c.next(g, y, t)) {
+    const int i = idx++;
+    if (i < r.start) continue;
+    if (y_run < 0) y_run = y;
+    else if (y != y_run) break;
+    if (t >= lo && t < hi) {
+      atomicMin(&run_first[pr.x], i);
+      break;
+    }
+  }
+}
+
 static __global__ void k_fill_f32(float* p, float v, int64_t n) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) p[i] = v;
@@ -223,7 +291,17 @@ static Work work_of(GraphHandle& h) {
   int32_t* ctr = reinterpret_cast<int32_t*>(h.s_sum.as<char>() + 4000);
   cudaMemsetAsync(ctr, 0, sizeof(int32_t), h.stream);
   return Work{h.d_items.as<WorkItem>(), h.d_slices.as<SliceState>(), h.d_slice_first.as<int32_t>(), ctr, h.nitems,
-              h.d_order.as<int32_t>(), h.norder};
+              h.d_order.as<int32_t>(), h.norder, h.d_run_first.as<int32_t>()};
+}
+
+// Computes the handle's run_first table for the window [lo, hi) (one small kernel over the slices
+// that overlap a cut run; nothing when no run is cut).
+static void prepare_runs(GraphHandle& h, int64_t lo, int64_t hi) {
+  if (h.nruns == 0) return;
+  int32_t* rf = h.d_run_first.as<int32_t>();
+  KL(k_fill_i32, grid_for(h.nruns, kBlock))(rf, INT32_MAX, h.nruns);
+  KL(k_run_first, grid_for(h.nrun_pairs, kBlock))(h.view, h.d_slices.as<SliceState>(), h.d_runs.as<RunInfo>(),
+                                                  h.d_run_pairs.as<int2>(), h.nrun_pairs, lo, hi, rf);
 }
 
 // Grid of a persistent decode launch over `work` units.

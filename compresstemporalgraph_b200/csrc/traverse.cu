@@ -241,8 +241,8 @@ __device__ __forceinline__ unsigned long long relax_level(const GraphView& g, Tr
     atomicOr(&a.dirty[y >> 5], 1u << (y & 31));
     return true;
   };
-  if (dense) return run_order<false, true>(g, w, [&](int x) { return __ldcg(&mcur[x]) == wcur; }, begin, edge, [](int) {});
-  return drive_queue(g, w, q, qn, begin, edge, [](int) {});
+  if (dense) return run_order<false, true, true>(g, w, [&](int x) { return __ldcg(&mcur[x]) == wcur; }, begin, edge, [](int) {});
+  return drive_queue<true>(g, w, q, qn, begin, edge, [](int) {});
 }
 
 template <bool kTouched>
@@ -280,8 +280,8 @@ __device__ __forceinline__ unsigned long long hop_level(const GraphView& g, Trav
     atomicOr(&a.dirty[y >> 5], 1u << (y & 31));
     return true;
   };
-  if (dense) return run_order<false, true>(g, w, [&](int x) { return __ldcg(&a.hops[x]) == h; }, begin, edge, [](int) {});
-  return drive_queue(g, w, q, qn, begin, edge, [](int) {});
+  if (dense) return run_order<false, true, true>(g, w, [&](int x) { return __ldcg(&a.hops[x]) == h; }, begin, edge, [](int) {});
+  return drive_queue<true>(g, w, q, qn, begin, edge, [](int) {});
 }
 
 __global__ void TGA_DECODE_BOUNDS k_bfs(GraphView g, TravArgs a) {
@@ -415,7 +415,8 @@ static TravArgs trav_args(GraphHandle& h, int64_t t_lo, int64_t t_hi, unsigned l
   const int32_t nv = h.view.max_vertex;
   TravArgs a{};
   a.w = Work{h.d_items.as<WorkItem>(), h.d_slices.as<SliceState>(), h.d_slice_first.as<int32_t>(), nullptr, h.nitems,
-             h.d_order.as<int32_t>(), h.norder};
+             h.d_order.as<int32_t>(), h.norder, h.d_run_first.as<int32_t>()};
+  prepare_runs(h, t_lo, t_hi);
   a.ctl = h.s_cnt.as<TravCtl>();
   a.q[0] = h.s_q0.as<int32_t>();
   a.q[1] = h.s_q1.as<int32_t>();

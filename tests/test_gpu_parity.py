@@ -240,5 +240,20 @@ def test_work_decomposition_does_not_change_results(pairs, shape, slice_edges, i
         deg, avg = g.degree_centrality(0, 0)
         odeg, oavg = p.o.degree(p.ml, p.mv, p.act, 0, 0)
         assert np.array_equal(deg, odeg) and np.array_equal(avg, oavg)
+        # Windowed calls: slices that start inside a run of equal successors must keep exactly the
+        # run's first in-window edge, whose position depends on the window.
+        lo, hi = _windows(p)[1]
+        arr, hops = g.bfs(src, lo, hi)
+        oarr, ohops = p.o.bfs(p.ml, p.mv, p.act, src, lo, hi)
+        assert np.array_equal(arr, oarr) and np.array_equal(hops, ohops)
+        lab, k = g.connected_components(lo, hi)
+        olab, ok = p.o.cc(p.ml, p.mv, p.act, p.cfg.connected_components_vertex_begin, lo, hi, True)
+        assert k == ok and np.array_equal(lab, olab)
+        r = g.pagerank(5, 0.85, 0.1, lo, hi)
+        assert float(np.abs(r - p.o.pagerank(p.ml, p.mv, p.act, 5, 0.85, 0.1, lo, hi)).sum()) <= 1e-5
+        hub, auth = g.hits(5, tga.HITS_JAVA, lo, hi)
+        ohub, oauth = p.o.hits(p.ml, p.mv, p.act, 5, True, lo, hi)
+        assert float(np.abs(hub.astype(np.float64) - ohub).max()) <= 1e-5
+        assert float(np.abs(auth.astype(np.float64) - oauth).max()) <= 1e-5
     finally:
         g.set_work_params(default["slice_edges"], default["item_edges"])
