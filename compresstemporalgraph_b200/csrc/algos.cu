@@ -245,8 +245,7 @@ __global__ void k_scale(const float* v, const double* sumsq, float* out, int32_t
 }
 
 // ---------------------------------------------------------------------------------------------
-// Degree centrality (Java semantics).  The running integer mean is sequential per list, so a
-// long list is decoded whole by the thread that draws its first slice.
+// Degree centrality (Java semantics).  Short lists: one thread per list.
 
 __global__ void TGA_DECODE_BOUNDS k_degree(GraphView g, Work w, int64_t s, int64_t e, int32_t* deg, int64_t* avg,
                                            unsigned long long* edges) {
@@ -255,7 +254,8 @@ __global__ void TGA_DECODE_BOUNDS k_degree(GraphView g, Work w, int64_t s, int64
   int32_t d = 0;
   int64_t mean = 0;
   const unsigned long long mine = run_order<true>(
-      g, w, [&](int v) { return v >= g.active_begin && v <= g.max_label; },
+      g, w,
+      [&](int v) { return v >= g.active_begin && v <= g.max_label && g.slice_first[v] == g.slice_first[v + 1]; },
       [&](int, int, int) {
         d = 0;
         mean = 0;
@@ -274,6 +274,59 @@ __global__ void TGA_DECODE_BOUNDS k_degree(GraphView g, Work w, int64_t s, int64
         avg[v] = mean;
       });
   add_edges(edges, mine);
+}
+
+// Long (sliced) lists in two phases: every slice decodes its edges in parallel and writes each
+// edge's timestamp, or kDcSkip when the edge does not count, at its list position; then one thread
+// per long list runs the sequential running mean over its segment (the Java mean truncates at
+// every step, so it cannot be split), with a 32-bit division whenever the difference fits.
+constexpr int64_t kDcSkip = INT64_MIN;
+
+__global__ void TGA_DECODE_BOUNDS k_degree_slices(GraphView g, const SliceState* slices, const int64_t* ebase,
+                                                  int32_t nslices, int64_t s, int64_t e, int64_t* buf,
+                                                  unsigned long long* edges) {
+  const bool all = (s == 0 && e == 0);
+  const int lim = min(g.max_label + 1, g.max_vertex);
+  unsigned long long mine = 0;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < nslices) {
+    const SliceState& sl = slices[j];
+    if (sl.v >= g.active_begin && sl.v <= g.max_label) {
+      DeepState deep;
+      EdgeCursor c(&deep);
+      cursor_restore(g, c, sl);
+      int64_t* out = buf + ebase[j];
+      int y;
+      int64_t t;
+      while (c.next(g, y, t)) {
+        *out++ = (y >= g.active_begin && y < lim && (all || (s <= t && e >= t))) ? t : kDcSkip;
+        ++mine;
+      }
+    }
+  }
+  add_edges(edges, mine);
+}
+
+__global__ void k_degree_long(const LongList* longs, int32_t nlong, const int32_t* outdeg, const int64_t* buf,
+                              int32_t active, int32_t max_label, int64_t s, int64_t e, int32_t* deg, int64_t* avg) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nlong) return;
+  const int v = longs[i].v;
+  if (v < active || v > max_label) return;
+  const int64_t* p = buf + longs[i].base;
+  const int n = outdeg[v];
+  int32_t d = 0;
+  int64_t mean = 0;
+  for (int k = 0; k < n; ++k) {
+    const int64_t t = p[k];
+    if (t == kDcSkip) continue;
+    ++d;
+    const int64_t a = t - mean;
+    mean += (a >= INT32_MIN && a <= INT32_MAX) ? (int64_t)((int32_t)a / d) : a / d;
+  }
+  if (s != e) d = (int32_t)(0.85 * d + 0.15 * d * (double)(mean - s) / (double)(e - s) + 1);
+  deg[v] = d;
+  avg[v] = mean;
 }
 
 // Lists of length zero never reach the loop above; their centrality is the formula at d = 0.
@@ -542,6 +595,7 @@ int tga_degree(tga_graph* gp, int64_t t_start, int64_t t_end, int32_t* degree_ou
   const int32_t nv = h.view.max_vertex;
   TGA_TRY(h.s_a.ensure((size_t)nv * 4));
   TGA_TRY(h.s_b.ensure((size_t)nv * 8));
+  if (h.nlong > 0) TGA_TRY(h.s_edges.ensure((size_t)h.long_edges * 8));
   TGA_TRY(h.begin_call());
   unsigned long long* edges = edge_counter(h);
   cudaMemsetAsync(h.s_a.p, 0, (size_t)nv * 4, h.stream);
@@ -550,6 +604,15 @@ int tga_degree(tga_graph* gp, int64_t t_start, int64_t t_end, int32_t* degree_ou
   cudaEvent_t* ev = h.kernel_begin();
   KL(k_degree, sweep_grid(h))(h.view, w, t_start, t_end, h.s_a.as<int32_t>(), h.s_b.as<int64_t>(), edges);
   h.kernel_end(ev);
+  if (h.nlong > 0) {
+    cudaEvent_t* ev2 = h.kernel_begin();
+    KL(k_degree_slices, grid_for(h.nslices, kBlock))(h.view, h.d_slices.as<SliceState>(), h.d_slice_ebase.as<int64_t>(),
+                                                     (int32_t)h.nslices, t_start, t_end, h.s_edges.as<int64_t>(), edges);
+    h.kernel_end(ev2);
+    KL(k_degree_long, grid_for(h.nlong, kBlock))(h.d_long.as<LongList>(), h.nlong, h.d_deg.as<int32_t>(),
+                                                 h.s_edges.as<int64_t>(), h.view.active_begin, h.view.max_label,
+                                                 t_start, t_end, h.s_a.as<int32_t>(), h.s_b.as<int64_t>());
+  }
   KL(k_degree_empty, grid_for(nv, kBlock))(h.d_deg.as<int32_t>(), h.view.active_begin, h.view.max_label,
                                            std::min(nv, h.view.n), t_start, t_end, h.s_a.as<int32_t>());
   if (degree_out) cudaMemcpyAsync(degree_out, h.s_a.p, (size_t)nv * 4, cudaMemcpyDeviceToHost, h.stream);

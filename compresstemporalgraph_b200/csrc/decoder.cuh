@@ -36,6 +36,8 @@ struct MaskState {
   uint64_t bpos;             // next block length in the stream
   int bleft;                 // blocks still to read
   int cur_left;              // values left in the current copy block (-1: copy all that remains)
+  int skip;                  // values of the next level to skip before the next copied one
+  int pad;
 };
 
 // Levels 1..kMaxLevels-1 of a reference chain (lv[j] is level j+1) and the masks of levels
@@ -63,6 +65,12 @@ struct SliceState {
 // `start`, overlapping the slices first_slice .. first_slice + nslices - 1.
 struct RunInfo {
   int32_t v, start, first_slice, nslices;
+};
+
+// A sliced list and the base of its segment in a per-edge buffer over all sliced lists.
+struct LongList {
+  int32_t v, pad;
+  int64_t base;
 };
 
 // ---- merge step shared by all levels ---------------------------------------------------------
@@ -205,48 +213,50 @@ __device__ __forceinline__ const SliceState* first_checkpoint(const GraphView& g
   return s0 != g.slice_first[x + 1] ? &g.slices[s0] : nullptr;
 }
 
-// Skips k values of level L (>= 1).  A long skip over a list that has slice checkpoints restores
-// the last checkpoint at or before the target: the checkpoint's level 0 becomes level L and its
-// chain levels L+1.. (a list referenced at level L has at most kMaxLevels-1-L further levels), so
-// the walk is bounded by one slice instead of the skip length.
+// Seeks over a pending skip of k values of level L (>= 1) when it is long: the last checkpoint
+// of level L's list at or before the target becomes level L, its chain the levels below (a list
+// referenced at level L has at most kMaxLevels-1-L further levels), and k shrinks to the values
+// still to skip from there, so a skip costs at most one slice of decoding.
 template <int L>
-__device__ __forceinline__ void deep_skip(const GraphView& g, DeepState& d, int k) {
-  ListState& st = d.lv[L - 1];
-  if (k > g.seek_min && g.slice_first) {
-    const int a = g.slice_first[st.x], b = g.slice_first[st.x + 1];
-    const int target = st.emitted + k;
-    if (b - a > 1) {
-      int lo = a, hi = b - 1;  // last slice with first <= target
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (g.slices[mid].first <= target) lo = mid;
-        else hi = mid - 1;
-      }
-      const SliceState& cp = g.slices[lo];
-      if (cp.first > st.emitted) {
-        load_checkpoint<L>(d, cp);
-        k = target - cp.first;
-      }
-    }
-  }
+__device__ __forceinline__ void deep_seek(const GraphView& g, DeepState& d, int& k) {
+  if (k <= g.seek_min || !g.slice_first) return;
+  const ListState& st = d.lv[L - 1];
+  const int a = g.slice_first[st.x], b = g.slice_first[st.x + 1];
+  if (b - a <= 1) return;
+  const int target = st.emitted + k;
+  int lo = a, hi = b - 1;  // last slice with first <= target
 #pragma unroll 1
-  for (int i = 0; i < k && i <= g.max_list; ++i)
-    if (deep_next<L>(g, d) == kInf) break;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (g.slices[mid].first <= target) lo = mid;
+    else hi = mid - 1;
+  }
+  const SliceState& cp = g.slices[lo];
+  if (cp.first > st.emitted) {
+    load_checkpoint<L>(d, cp);
+    k = target - cp.first;
+  }
 }
 
-// Next value selected by the copy mask of level M (0..kMaxLevels-2) over level M+1.
+// Next value selected by the copy mask of level M (0..kMaxLevels-2) over level M+1.  The skip
+// block after a copy block is left pending in the mask and consumed by the next call, so level
+// M+1 is advanced from a single place (one inlined copy of each level's step).
 template <int M>
 __device__ __forceinline__ int deep_masked(const GraphView& g, DeepState& d) {
   MaskState& mk = d.mask[M];
   if (mk.cur_left == 0) return kInf;
-  const int v = deep_next<M + 1>(g, d);
-  if (v == kInf) return kInf;
-  if (mk.cur_left > 0) {
-    --mk.cur_left;
-    if (mk.cur_left == 0 && mk.bleft > 0) {
-      const int skip = (int)read_gamma(g, g.g, mk.bpos) + 1;
+  if (mk.skip > 0) deep_seek<M + 1>(g, d, mk.skip);
+#pragma unroll 1
+  for (;;) {
+    const int v = deep_next<M + 1>(g, d);
+    if (v == kInf) return kInf;
+    if (mk.skip > 0) {
+      --mk.skip;
+      continue;
+    }
+    if (mk.cur_left > 0 && --mk.cur_left == 0 && mk.bleft > 0) {
+      mk.skip = (int)read_gamma(g, g.g, mk.bpos) + 1;
       --mk.bleft;
-      deep_skip<M + 1>(g, d, skip);
       if (mk.bleft > 0) {
         mk.cur_left = (int)read_gamma(g, g.g, mk.bpos) + 1;
         --mk.bleft;
@@ -254,8 +264,8 @@ __device__ __forceinline__ int deep_masked(const GraphView& g, DeepState& d) {
         mk.cur_left = -1;
       }
     }
+    return v;
   }
-  return v;
 }
 
 template <int L>
@@ -271,11 +281,12 @@ __device__ __forceinline__ int deep_next(const GraphView& g, DeepState& d) {
   return v;
 }
 
-// Starts the copy mask of level M (bc blocks at mask[M].bpos): first block read, a leading empty
-// copy block skipped.
+// Starts the copy mask of level M (bc blocks at mask[M].bpos): first block read; after a leading
+// empty copy block the following skip block is left pending.
 template <int M>
 __device__ __forceinline__ void mask_start(const GraphView& g, DeepState& d, int bc) {
   MaskState& mk = d.mask[M];
+  mk.skip = 0;
   if (bc == 0) {
     mk.cur_left = -1;
     mk.bleft = 0;
@@ -284,9 +295,8 @@ __device__ __forceinline__ void mask_start(const GraphView& g, DeepState& d, int
   mk.cur_left = (int)read_gamma(g, g.g, mk.bpos);
   mk.bleft = bc - 1;
   if (mk.cur_left == 0 && mk.bleft > 0) {
-    const int skip = (int)read_gamma(g, g.g, mk.bpos) + 1;
+    mk.skip = (int)read_gamma(g, g.g, mk.bpos) + 1;
     --mk.bleft;
-    deep_skip<M + 1>(g, d, skip);
     if (mk.bleft > 0) {
       mk.cur_left = (int)read_gamma(g, g.g, mk.bpos) + 1;
       --mk.bleft;
@@ -334,16 +344,16 @@ struct OpenRef {
   int head;   // first copied value (kInf if none)
 };
 
+static __device__ __noinline__ int deep_copy_next(const GraphView& g, DeepState& d) { return deep_masked<0>(g, d); }
+
 static __device__ __noinline__ OpenRef deep_open_ref(const GraphView& g, DeepState& d, int xref, int bc, uint64_t bpos) {
   OpenRef r;
   r.dref = deep_open<1>(g, d, xref);
   d.mask[0].bpos = bpos;
   mask_start<0>(g, d, bc);
-  r.head = deep_masked<0>(g, d);
+  r.head = deep_copy_next(g, d);
   return r;
 }
-
-static __device__ __noinline__ int deep_copy_next(const GraphView& g, DeepState& d) { return deep_masked<0>(g, d); }
 
 // ---- level 0 --------------------------------------------------------------------------------
 

@@ -48,7 +48,8 @@ void DevBuf::release() {
 GraphHandle::~GraphHandle() {
   if (stream) cudaStreamSynchronize(stream);
   for (DevBuf* b : {&d_graph, &d_ts, &d_gl, &d_gu, &d_gs, &d_tl, &d_tu, &d_ts_samples, &d_err, &d_deg, &d_slices,
-                    &d_items, &d_slice_first, &d_order, &d_runs, &d_run_pairs, &d_run_first, &d_view, &s_a, &s_b, &s_c, &s_d, &s_e, &s_f, &s_g, &s_q0, &s_q1, &s_cnt, &s_sum})
+                    &d_items, &d_slice_first, &d_order, &d_runs, &d_run_pairs, &d_run_first, &d_long, &d_slice_ebase,
+                    &d_view, &s_edges, &s_a, &s_b, &s_c, &s_d, &s_e, &s_f, &s_g, &s_q0, &s_q1, &s_cnt, &s_sum})
     b->release();
   for (auto& k : ktimers) {
     if (k.a) cudaEventDestroy(k.a);
@@ -413,6 +414,19 @@ int build_work(GraphHandle& h, int32_t slice_len, int32_t item_edges) {
     for (int32_t k = 0; k < runs[r].nslices; ++k) run_pairs.push_back(make_int2((int)r, runs[r].first_slice + k));
   h.nruns = (int32_t)runs.size();
   h.nrun_pairs = (int32_t)run_pairs.size();
+  // Per-edge segments of the sliced lists (for workloads that are sequential per list).
+  std::vector<LongList> longs;
+  std::vector<int64_t> slice_ebase(packed.size(), 0);
+  int64_t long_edges = 0;
+  for (int32_t x = 0; x < nd; ++x) {
+    const int32_t a = slice_first[(size_t)x], b = slice_first[(size_t)x + 1];
+    if (a == b) continue;
+    longs.push_back(LongList{x, 0, long_edges});
+    for (int32_t j = a; j < b; ++j) slice_ebase[(size_t)j] = long_edges + packed[(size_t)j].first;
+    long_edges += h.degrees[(size_t)x];
+  }
+  h.nlong = (int32_t)longs.size();
+  h.long_edges = long_edges;
   h.nslice_items = (int32_t)items.size();
   {
     constexpr int32_t kVertexCost = 4, kMaxRange = 4096;
@@ -467,6 +481,13 @@ int build_work(GraphHandle& h, int32_t slice_len, int32_t item_edges) {
   if ((rc = h.d_order.ensure(std::max<size_t>(1, order.size()) * 4))) return rc;
   if (!order.empty())
     TGA_CUDA_TRY(cudaMemcpy(h.d_order.p, order.data(), order.size() * 4, cudaMemcpyHostToDevice));
+  if ((rc = h.d_long.ensure(std::max<size_t>(1, longs.size()) * sizeof(LongList))) ||
+      (rc = h.d_slice_ebase.ensure(std::max<size_t>(1, slice_ebase.size()) * 8)))
+    return rc;
+  if (!longs.empty()) {
+    TGA_CUDA_TRY(cudaMemcpy(h.d_long.p, longs.data(), longs.size() * sizeof(LongList), cudaMemcpyHostToDevice));
+    TGA_CUDA_TRY(cudaMemcpy(h.d_slice_ebase.p, slice_ebase.data(), slice_ebase.size() * 8, cudaMemcpyHostToDevice));
+  }
   if ((rc = h.d_runs.ensure(std::max<size_t>(1, runs.size()) * sizeof(RunInfo))) ||
       (rc = h.d_run_pairs.ensure(std::max<size_t>(1, run_pairs.size()) * sizeof(int2))) ||
       (rc = h.d_run_first.ensure(std::max<size_t>(1, runs.size()) * 4)))

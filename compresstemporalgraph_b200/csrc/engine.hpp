@@ -56,6 +56,11 @@ struct GraphHandle {
   // pre-pass, and the per-call list index of each run's first in-window edge
   DevBuf d_runs, d_run_pairs, d_run_first;
   int32_t nruns = 0, nrun_pairs = 0;
+  // sliced (long) lists: LongList[nlong] with the base of each list's segment in a buffer of one
+  // entry per edge of all long lists (long_edges entries), and that base + first for each slice
+  DevBuf d_long, d_slice_ebase;
+  int32_t nlong = 0;
+  int64_t long_edges = 0;
   DevBuf d_view;                     // device-global copy of `view` (GraphView::self)
   int32_t norder = 0;
   int32_t dense_min = 1;             // traversal levels with at least this many entries sweep all lists
@@ -65,7 +70,7 @@ struct GraphHandle {
   int32_t slice_len = 0, item_edges = 0;
   std::vector<int32_t> slice_first_host;
   // scratch used by the algorithms
-  DevBuf s_a, s_b, s_c, s_d, s_e, s_f, s_g, s_q0, s_q1, s_cnt, s_sum;
+  DevBuf s_a, s_b, s_c, s_d, s_e, s_f, s_g, s_q0, s_q1, s_cnt, s_sum, s_edges;
   uint32_t* h_pinned = nullptr;  // small pinned readback area
   // timing of the last call
   cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
