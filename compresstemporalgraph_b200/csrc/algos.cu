@@ -317,13 +317,32 @@ __global__ void k_degree_long(const LongList* longs, int32_t nlong, const int32_
   const int n = outdeg[v];
   int32_t d = 0;
   int64_t mean = 0;
-  for (int k = 0; k < n; ++k) {
-    const int64_t t = p[k];
-    if (t == kDcSkip) continue;
+  auto step = [&](int64_t t) {
+    if (t == kDcSkip) return;
     ++d;
     const int64_t a = t - mean;
     mean += (a >= INT32_MIN && a <= INT32_MAX) ? (int64_t)((int32_t)a / d) : a / d;
+  };
+  // The recurrence is sequential; its inputs are not, so they are loaded a batch ahead: the next
+  // batch's loads are in flight while the current batch is folded in.
+  constexpr int kBatch = 16;
+  int64_t cur[kBatch], nxt[kBatch];
+  int k = 0;
+  if (n >= kBatch) {
+#pragma unroll
+    for (int j = 0; j < kBatch; ++j) cur[j] = __ldcs(p + j);
+    for (k = kBatch; k + kBatch <= n; k += kBatch) {
+#pragma unroll
+      for (int j = 0; j < kBatch; ++j) nxt[j] = __ldcs(p + k + j);
+#pragma unroll
+      for (int j = 0; j < kBatch; ++j) step(cur[j]);
+#pragma unroll
+      for (int j = 0; j < kBatch; ++j) cur[j] = nxt[j];
+    }
+#pragma unroll
+    for (int j = 0; j < kBatch; ++j) step(cur[j]);
   }
+  for (; k < n; ++k) step(p[k]);
   if (s != e) d = (int32_t)(0.85 * d + 0.15 * d * (double)(mean - s) / (double)(e - s) + 1);
   deg[v] = d;
   avg[v] = mean;

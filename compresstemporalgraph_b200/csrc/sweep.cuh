@@ -201,15 +201,23 @@ __device__ __forceinline__ unsigned long long drive_queue(const GraphView& g, co
   unsigned long long edges = 0;
   // The first entry of a thread comes from its spread warp rank (consecutive entries, such as the
   // slices of one list, land on different SMs); later ones come from the counter, offset by the
-  // thread count, so a queue shorter than the grid costs no atomics at all.
-  int i = spread_warp_rank() * 32 + (int)(threadIdx.x & 31);
+  // thread count, so a queue shorter than the grid costs no atomics at all.  A short queue is
+  // dealt to m lanes per warp, m the smallest power of two that covers it: lanes decoding
+  // different lists diverge, so fewer lanes per warp finish a small level sooner.
+  const int nthreads = (int)(gridDim.x * blockDim.x), lane = (int)(threadIdx.x & 31);
+  int m = 32;
+  if (qn < nthreads) {
+    m = 1;
+    while (m < 32 && m * (nthreads >> 5) < qn) m <<= 1;
+  }
+  int i = lane < m ? spread_warp_rank() * m + lane : qn;
   for (;;) {
     if (c.remaining <= 0) {
       if (cur >= 0) {
         end(cur);
         cur = -1;
       }
-      if (i < 0) i = (int)(gridDim.x * blockDim.x) + atomicAdd(w.next, 1);
+      if (i < 0) i = nthreads + atomicAdd(w.next, 1);
       if (i >= qn) break;
       int first, count, lead;
       const int x = open_entry(g, w, __ldcg(q + i), c, first, count, lead);
