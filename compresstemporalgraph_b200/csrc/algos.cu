@@ -24,7 +24,7 @@ namespace tga {
 // ---------------------------------------------------------------------------------------------
 // Neighbour access and raw decode
 
-__global__ void TGA_DECODE_BOUNDS k_neighbor_access(GraphView g, Work w, int32_t begin, int32_t end,
+__global__ void TGA_SWEEP_BOUNDS k_neighbor_access(GraphView g, Work w, int32_t begin, int32_t end,
                                                     unsigned long long* csum, unsigned long long* edges) {
   uint64_t h = 0;
   uint32_t k = 0;
@@ -48,7 +48,7 @@ __global__ void k_small_flags(const int32_t* deg, uint8_t* small, int32_t begin,
   if (v < end) small[v] = deg[v] < 4;
 }
 
-__global__ void TGA_DECODE_BOUNDS k_decode_csr(GraphView g, Work w, const int64_t* off, int32_t* dst, int64_t* ts,
+__global__ void TGA_SWEEP_BOUNDS k_decode_csr(GraphView g, Work w, const int64_t* off, int32_t* dst, int64_t* ts,
                                                int64_t cap) {
   int64_t o = 0;
   run_order<false>(
@@ -108,7 +108,7 @@ __device__ __forceinline__ float temporal_weight(float alpha, int64_t t) {
   return a > 18.0f ? 1.0f : 1.0f - expf(-a);
 }
 
-__global__ void TGA_DECODE_BOUNDS k_pr_iter(GraphView g, Work w, PrArgs a) {
+__global__ void TGA_SWEEP_BOUNDS k_pr_iter(GraphView g, Work w, PrArgs a) {
   for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < g.max_vertex; x += gridDim.x * blockDim.x) a.reset[x] = a.base;
   const double s = a.k == 0 ? 1.0 : 1.0 / a.sums[a.k - 1];
   float local = 0.0f, c0 = 0.0f;
@@ -136,8 +136,7 @@ __global__ void TGA_DECODE_BOUNDS k_pr_iter(GraphView g, Work w, PrArgs a) {
       },
       [&](int) { total += (double)local; });
   add_edges(a.edges, mine);
-  const double bs = block_sum(total);
-  if (threadIdx.x == 0 && bs != 0.0) atomicAdd(&a.sums[a.k], bs);
+  warp_add(&a.sums[a.k], total);
 }
 
 __global__ void k_pr_init_sums(double* sums, int n, double v) {
@@ -151,7 +150,7 @@ __global__ void k_pr_final(const float* buf, const double* sums, int k, float* o
 }
 
 // In-window outdegree of each source, counted over items, then inverted.
-__global__ void TGA_DECODE_BOUNDS k_window_count(GraphView g, Work w, int64_t lo, int64_t hi, int32_t* cnt,
+__global__ void TGA_SWEEP_BOUNDS k_window_count(GraphView g, Work w, int64_t lo, int64_t hi, int32_t* cnt,
                                                  unsigned long long* edges) {
   int k = 0;
   const unsigned long long mine = run_order<false>(
@@ -188,7 +187,7 @@ __global__ void k_hits_base(float* hub, const float* auth_in, float* auth_next, 
   auth_next[x] = java ? 0.0f : auth_in[x] * sa;
 }
 
-__global__ void TGA_DECODE_BOUNDS k_hits_hub(GraphView g, Work w, float* hub, const float* auth_in, const double* aprev,
+__global__ void TGA_SWEEP_BOUNDS k_hits_hub(GraphView g, Work w, float* hub, const float* auth_in, const double* aprev,
                                              int64_t lo, int64_t hi, unsigned long long* edges) {
   const float sa = (aprev && *aprev > 0) ? (float)(1.0 / sqrt(*aprev)) : 1.0f;
   float acc = 0.0f;
@@ -210,7 +209,7 @@ __global__ void TGA_DECODE_BOUNDS k_hits_hub(GraphView g, Work w, float* hub, co
   add_edges(edges, mine);
 }
 
-__global__ void TGA_DECODE_BOUNDS k_hits_auth(GraphView g, Work w, const float* hub, const double* hsum,
+__global__ void TGA_SWEEP_BOUNDS k_hits_auth(GraphView g, Work w, const float* hub, const double* hsum,
                                               float* auth_next, int64_t lo, int64_t hi, unsigned long long* edges) {
   const float sh = *hsum > 0 ? (float)(1.0 / sqrt(*hsum)) : 1.0f;
   float hn = 0.0f;

@@ -18,8 +18,14 @@ constexpr int kNoRunFilter = -2;
 
 // Launches a kernel of kBlock threads on the handle's stream and counts it in the call's timing.
 #define KL(kernel, grid) ++h.timing.launches, kernel<<<(grid), kBlock, 0, h.stream>>>
-// Decode kernels: 2 blocks of 256 threads per SM (128 registers, no spills).
+// Decode kernels of traversals and colouring: 2 blocks of 256 threads per SM (up to 128
+// registers).  Their levels are short and latency-bound, and the extra spills of a tighter cap
+// cost more than the added warps gain.
 #define TGA_DECODE_BOUNDS __launch_bounds__(kBlock, 2)
+// Full sweeps over the schedule (neighbour access, PageRank, HITS, window counts, raw decode):
+// 4 blocks per SM (up to 64 registers, a few spills), measured faster than 2 on these kernels
+// because more resident warps hide the decoder's dependent loads.
+#define TGA_SWEEP_BOUNDS __launch_bounds__(kBlock, 4)
 
 // Per-edge term of the neighbour-access checksum: the checksum of a list is the sum (mod 2^64)
 // of edge_hash over its edges, so slices can add their parts; the edge index keeps it
@@ -51,6 +57,12 @@ __device__ __forceinline__ double block_sum(double v) {
     for (int o = 16; o; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
   }
   return s;  // valid in thread 0
+}
+
+// Sum of v over the warp, added to *out by lane 0 (no block barrier: warps leave independently).
+__device__ __forceinline__ void warp_add(double* out, double v) {
+  for (int o = 16; o; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(out, v);
 }
 
 struct Work {
