@@ -451,12 +451,16 @@ int build_work(GraphHandle& h, int32_t slice_len, int32_t item_edges) {
   }
   h.nitems = (int32_t)items.size();
   // Decode order for the sweeps: every slice, then every non-empty short list, grouped by work
-  // class (quarter-octave of the outdegree, lists that copy from a reference chain apart) from the
-  // largest class down, so the 32 lanes of a warp open their lists together and decode lists of
-  // nearly equal length.
+  // class (quarter-octave of the outdegree) from the largest class down, so the 32 lanes of a warp
+  // open their lists together and decode lists of nearly equal length.
   std::vector<int32_t> order;
   order.reserve(packed.size() + (size_t)nd);
-  for (size_t j = 0; j < packed.size(); ++j) order.push_back(-(int32_t)j - 1);
+  // Slices and lists that do not copy from a reference chain come first, those that do last:
+  // only the latter run the (large) chain decoder, and keeping them together keeps the two code
+  // paths from competing for the instruction cache.
+  for (int c = 0; c < 2; ++c)
+    for (size_t j = 0; j < packed.size(); ++j)
+      if ((packed[j].chain != 0) == (c == 1)) order.push_back(-(int32_t)j - 1);
   {
     auto cls = [&](int32_t d) { return (int)std::floor(4.0 * std::log2((double)d)); };
     const int ncls = cls(std::max(slice_len, 1)) + 2;
@@ -466,7 +470,8 @@ int build_work(GraphHandle& h, int32_t slice_len, int32_t item_edges) {
       if (d <= 0 || slice_first[(size_t)x + 1] != slice_first[(size_t)x]) continue;
       bins[(size_t)(std::min(cls(d), ncls - 1) * 2 + (h.chain_host[(size_t)x] ? 1 : 0))].push_back(x);
     }
-    for (int b = (int)bins.size() - 1; b >= 0; --b) order.insert(order.end(), bins[(size_t)b].begin(), bins[(size_t)b].end());
+    for (int c = 0; c < 2; ++c)
+      for (int b = (int)bins.size() - 2 + c; b >= 0; b -= 2) order.insert(order.end(), bins[(size_t)b].begin(), bins[(size_t)b].end());
   }
   h.norder = (int32_t)order.size();
   // A traversal level sweeps all lists instead of its queue once the queue holds at least
