@@ -47,18 +47,19 @@ struct DeepState {
   ListState lv[kMaxLevels - 1];
 };
 
-// Complete decoder state at one edge of a long list (see slices.cuh).
+// Decoder state at the first edge of a slice (see slices.cuh).  The reference-chain levels of a
+// list that copies from a chain are kept apart (GraphView::slice_deep[deep]), so a checkpoint of a
+// plain list is one cache line.
 struct SliceState {
   ListState top;
-  DeepState deep;   // meaningful only when chain != 0
   uint64_t tpos;    // bit position of the slice's first timestamp code
   int64_t prev;     // timestamp preceding the slice's first edge
   int32_t v;        // vertex
   int32_t count;    // edges in the slice
   int32_t first;    // index of the slice's first edge in the list of v
   int32_t chain;    // the list copies from a reference chain
+  int32_t deep;     // its chain levels: index into slice_deep (-1 when chain == 0)
   int32_t run;      // the slice starts inside a run of equal successors: that run's index, else -1
-  int32_t pad;
 };
 
 // A run of equal successors that slices cut (slices.cuh): list `v`, edges from list index
@@ -189,18 +190,19 @@ __device__ __forceinline__ int deep_next(const GraphView& g, DeepState& d);
 // Loads checkpoint cp (list cp.v at its edge cp.first) into level L and its chain into the levels
 // below (a list at level L has at most kMaxLevels-1-L further levels).
 template <int L>
-__device__ __forceinline__ void load_checkpoint(DeepState& d, const SliceState& cp) {
+__device__ __forceinline__ void load_checkpoint(const GraphView& g, DeepState& d, const SliceState& cp) {
   d.lv[L - 1] = cp.top;
   d.lv[L - 1].x = cp.v;
   d.lv[L - 1].emitted = cp.first;
   if (cp.chain) {
+    const DeepState& cd = g.slice_deep[cp.deep];
     if constexpr (L < kMaxLevels - 1) {
-      d.mask[L] = cp.deep.mask[0];
-      d.lv[L] = cp.deep.lv[0];
+      d.mask[L] = cd.mask[0];
+      d.lv[L] = cd.lv[0];
     }
     if constexpr (L + 1 < kMaxLevels - 1) {
-      d.mask[L + 1] = cp.deep.mask[1];
-      d.lv[L + 1] = cp.deep.lv[1];
+      d.mask[L + 1] = cd.mask[1];
+      d.lv[L + 1] = cd.lv[1];
     }
   }
 }
@@ -233,7 +235,7 @@ __device__ __forceinline__ void deep_seek(const GraphView& g, DeepState& d, int&
   }
   const SliceState& cp = g.slices[lo];
   if (cp.first > st.emitted) {
-    load_checkpoint<L>(d, cp);
+    load_checkpoint<L>(g, d, cp);
     k = target - cp.first;
   }
 }
@@ -311,7 +313,7 @@ __device__ __forceinline__ void mask_start(const GraphView& g, DeepState& d, int
 template <int L>
 __device__ __forceinline__ int deep_open(const GraphView& g, DeepState& d, int x) {
   if (const SliceState* cp = first_checkpoint(g, x)) {
-    load_checkpoint<L>(d, *cp);
+    load_checkpoint<L>(g, d, *cp);
     return g.deg[x];
   }
   ListState& st = d.lv[L - 1];
@@ -408,7 +410,7 @@ struct EdgeCursor {
     if (const SliceState* cp = first_checkpoint(g, v)) {
       top = cp->top;
       chain = cp->chain;
-      if (chain) *deep = cp->deep;
+      if (chain) *deep = g.slice_deep[cp->deep];
       ts.init(g.t, cp->tpos);
       prev = cp->prev;
       remaining = g.deg[v];

@@ -55,6 +55,7 @@ struct GraphView {
   // Slice checkpoints of long lists (slices.cuh), used by the decoder to seek over long skip
   // blocks of a referenced list; null until the work decomposition is built.
   const struct SliceState* slices;
+  const struct DeepState* slice_deep;  // chain levels of the checkpoints that have some
   const int32_t* slice_first;
   const int32_t* deg;    // outdegrees (set with the slices)
   int32_t seek_min;      // skip blocks longer than this seek through a checkpoint

@@ -48,7 +48,7 @@ void DevBuf::release() {
 GraphHandle::~GraphHandle() {
   if (stream) cudaStreamSynchronize(stream);
   for (DevBuf* b : {&d_graph, &d_ts, &d_gl, &d_gu, &d_gs, &d_tl, &d_tu, &d_ts_samples, &d_err, &d_deg, &d_slices,
-                    &d_items, &d_slice_first, &d_order, &d_runs, &d_run_pairs, &d_run_first, &d_long, &d_slice_ebase,
+                    &d_items, &d_slice_first, &d_slice_deep, &d_order, &d_runs, &d_run_pairs, &d_run_first, &d_long, &d_slice_ebase,
                     &d_view, &s_edges, &s_a, &s_b, &s_c, &s_d, &s_e, &s_f, &s_g, &s_q0, &s_q1, &s_cnt, &s_sum})
     b->release();
   for (auto& k : ktimers) {
@@ -334,6 +334,7 @@ int build_work(GraphHandle& h, int32_t slice_len, int32_t item_edges) {
   GraphView& v = h.view;
   // The build walks the lists without seeking (checkpoints are being made).
   v.slices = nullptr;
+  v.slice_deep = nullptr;
   v.slice_first = nullptr;
   v.deg = nullptr;
   v.seek_min = INT32_MAX;
@@ -343,7 +344,11 @@ int build_work(GraphHandle& h, int32_t slice_len, int32_t item_edges) {
   std::vector<int64_t> slot_base{0};
   for (int32_t x = 0; x < nd; ++x) {
     const int32_t d = h.degrees[(size_t)x];
-    if (d > slice_len) {
+    // Long lists are sliced; so is every list that copies from a reference chain, whatever its
+    // length: opening one parses the records along its chain (and walks the referenced lists to
+    // the first copied value), which costs more than decoding a short list, so its state after
+    // opening is kept as a checkpoint (a single slice when the list is short).
+    if (d > slice_len || (d > 0 && h.chain_host[(size_t)x])) {
       big_v.push_back(x);
       slot_base.push_back(slot_base.back() + (d + slice_len - 1) / slice_len);
     }
@@ -351,26 +356,32 @@ int build_work(GraphHandle& h, int32_t slice_len, int32_t item_edges) {
   const int32_t nbig = (int32_t)big_v.size();
   std::vector<int32_t> nsl((size_t)nbig, 0);
   std::vector<SliceState> slices;
+  std::vector<DeepState> slice_deep_tmp;
   if (nbig) {
-    DevBuf bv, sb, ns, tmp;
+    DevBuf bv, sb, ns, tmp, tmpd;
     int rc;
     if ((rc = bv.ensure((size_t)nbig * 4)) || (rc = sb.ensure(slot_base.size() * 8)) || (rc = ns.ensure((size_t)nbig * 4)) ||
-        (rc = tmp.ensure((size_t)slot_base.back() * sizeof(SliceState))))
+        (rc = tmp.ensure((size_t)slot_base.back() * sizeof(SliceState))) ||
+        (rc = tmpd.ensure((size_t)slot_base.back() * sizeof(DeepState))))
       return rc;
     TGA_CUDA_TRY(cudaMemcpyAsync(bv.p, big_v.data(), (size_t)nbig * 4, cudaMemcpyHostToDevice, h.stream));
     TGA_CUDA_TRY(cudaMemcpyAsync(sb.p, slot_base.data(), slot_base.size() * 8, cudaMemcpyHostToDevice, h.stream));
     k_build_slices<<<grid_for(nbig, 64), 64, 0, h.stream>>>(v, bv.as<int32_t>(), sb.as<int64_t>(), nbig, slice_len,
-                                                           tmp.as<SliceState>(), ns.as<int32_t>());
+                                                           tmp.as<SliceState>(), tmpd.as<DeepState>(), ns.as<int32_t>());
     TGA_CUDA_TRY(cudaGetLastError());
     slices.resize((size_t)slot_base.back());
     TGA_CUDA_TRY(cudaMemcpyAsync(nsl.data(), ns.p, (size_t)nbig * 4, cudaMemcpyDeviceToHost, h.stream));
     TGA_CUDA_TRY(cudaMemcpyAsync(slices.data(), tmp.p, slices.size() * sizeof(SliceState), cudaMemcpyDeviceToHost,
                                  h.stream));
+    slice_deep_tmp.resize((size_t)slot_base.back());
+    TGA_CUDA_TRY(cudaMemcpyAsync(slice_deep_tmp.data(), tmpd.p, slice_deep_tmp.size() * sizeof(DeepState),
+                                 cudaMemcpyDeviceToHost, h.stream));
     if ((rc = h.check_device_error())) return rc;
-    bv.release(); sb.release(); ns.release(); tmp.release();
+    bv.release(); sb.release(); ns.release(); tmp.release(); tmpd.release();
   }
   // Compact the slices, build slice_first and the work items (slices first, then short lists).
   std::vector<SliceState> packed;
+  std::vector<DeepState> packed_deep;
   std::vector<int32_t> slice_first((size_t)nd + 1, 0);
   std::vector<WorkItem> items;
   {
@@ -380,7 +391,13 @@ int build_work(GraphHandle& h, int32_t slice_len, int32_t item_edges) {
       if (b < nbig && big_v[(size_t)b] == x) {
         for (int32_t j = 0; j < nsl[(size_t)b]; ++j) {
           items.push_back(WorkItem{x, x + 1, (int32_t)packed.size()});
-          packed.push_back(slices[(size_t)(slot_base[(size_t)b] + j)]);
+          const size_t slot = (size_t)(slot_base[(size_t)b] + j);
+          SliceState sl = slices[slot];
+          if (sl.chain) {
+            sl.deep = (int32_t)packed_deep.size();
+            packed_deep.push_back(slice_deep_tmp[slot]);
+          }
+          packed.push_back(sl);
         }
         ++b;
       }
@@ -458,9 +475,15 @@ int build_work(GraphHandle& h, int32_t slice_len, int32_t item_edges) {
   // Slices and lists that do not copy from a reference chain come first, those that do last:
   // only the latter run the (large) chain decoder, and keeping them together keeps the two code
   // paths from competing for the instruction cache.
-  for (int c = 0; c < 2; ++c)
+  for (int c = 0; c < 2; ++c) {
+    std::vector<int32_t> grp;
     for (size_t j = 0; j < packed.size(); ++j)
-      if ((packed[j].chain != 0) == (c == 1)) order.push_back(-(int32_t)j - 1);
+      if ((packed[j].chain != 0) == (c == 1)) grp.push_back((int32_t)j);
+    // longest slices first, so the lanes of a warp decode slices of equal length
+    std::stable_sort(grp.begin(), grp.end(),
+                     [&](int32_t a, int32_t b) { return packed[(size_t)a].count > packed[(size_t)b].count; });
+    for (int32_t j : grp) order.push_back(-j - 1);
+  }
   {
     auto cls = [&](int32_t d) { return (int)std::floor(4.0 * std::log2((double)d)); };
     const int ncls = cls(std::max(slice_len, 1)) + 2;
@@ -503,17 +526,24 @@ int build_work(GraphHandle& h, int32_t slice_len, int32_t item_edges) {
   }
   if ((rc = h.d_items.ensure(std::max<size_t>(1, items.size()) * sizeof(WorkItem))) ||
       (rc = h.d_slices.ensure(std::max<size_t>(1, packed.size()) * sizeof(SliceState))) ||
+      (rc = h.d_slice_deep.ensure(std::max<size_t>(1, packed_deep.size()) * sizeof(DeepState))) ||
       (rc = h.d_slice_first.ensure(slice_first.size() * 4)))
     return rc;
   if (!items.empty())
     TGA_CUDA_TRY(cudaMemcpy(h.d_items.p, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice));
   if (!packed.empty())
     TGA_CUDA_TRY(cudaMemcpy(h.d_slices.p, packed.data(), packed.size() * sizeof(SliceState), cudaMemcpyHostToDevice));
+  if (!packed_deep.empty())
+    TGA_CUDA_TRY(cudaMemcpy(h.d_slice_deep.p, packed_deep.data(), packed_deep.size() * sizeof(DeepState),
+                            cudaMemcpyHostToDevice));
   TGA_CUDA_TRY(cudaMemcpy(h.d_slice_first.p, slice_first.data(), slice_first.size() * 4, cudaMemcpyHostToDevice));
   h.slice_first_host = std::move(slice_first);
   v.slices = h.d_slices.as<SliceState>();
+  v.slice_deep = h.d_slice_deep.as<DeepState>();
   v.slice_first = h.d_slice_first.as<int32_t>();
   v.deg = h.d_deg.as<int32_t>();
+  h.work_bytes = h.d_slices.bytes + h.d_slice_deep.bytes + h.d_slice_first.bytes + h.d_items.bytes + h.d_order.bytes +
+                 h.d_runs.bytes + h.d_run_pairs.bytes + h.d_run_first.bytes + h.d_long.bytes + h.d_slice_ebase.bytes;
   v.seek_min = std::max(16, slice_len / 2);
   return publish_view(h);
 }
@@ -588,6 +618,11 @@ int tga_close(tga_graph* g) {
 int tga_get_info(tga_graph* g, tga_info* out) {
   if (!g || !out) return fail(TGA_E_ARG, "null argument");
   *out = g->info;
+  // streams and index (counted at load) + work decomposition + scratch grown by the calls so far
+  out->device_bytes += g->work_bytes;
+  for (const DevBuf* b : {&g->s_a, &g->s_b, &g->s_c, &g->s_d, &g->s_e, &g->s_f, &g->s_g, &g->s_q0, &g->s_q1, &g->s_cnt,
+                          &g->s_sum, &g->s_edges})
+    out->device_bytes += b->bytes;
   return TGA_OK;
 }
 

@@ -49,7 +49,8 @@ struct GraphHandle {
   DevBuf d_deg;
   // edge-balanced work decomposition (slices.cuh): slices of long lists, work items, and
   // slice_first[v]..slice_first[v+1] = slices of vertex v (empty for short lists)
-  DevBuf d_slices, d_items, d_slice_first;
+  DevBuf d_slices, d_items, d_slice_first, d_slice_deep;
+  uint64_t work_bytes = 0;           // device bytes of the work decomposition (slices, schedule, runs)
   // decode order of the sweeps (vertex ids >= 0 and -(slice+1)), grouped by work class
   DevBuf d_order;
   // runs of equal successors cut by slices: RunInfo[nruns], (run, slice) pairs of the per-call

@@ -25,40 +25,43 @@ struct WorkItem {
 __device__ __forceinline__ void cursor_restore(const GraphView& g, EdgeCursor& c, const SliceState& s) {
   c.top = s.top;
   c.chain = s.chain;
-  if (s.chain) *c.deep = s.deep;
+  if (s.chain) *c.deep = g.slice_deep[s.deep];
   c.ts.init(g.t, s.tpos);
   c.prev = s.prev;
   c.remaining = s.count;
   c.x = s.v;
 }
 
-__device__ __forceinline__ void cursor_save(const EdgeCursor& c, SliceState& s, int v, int first) {
+// Writes the cursor's state at edge `first` of v; the chain levels go to *deep (kept only for
+// lists that copy from a chain; the host moves them to the compact slice_deep array).
+__device__ __forceinline__ void cursor_save(const EdgeCursor& c, SliceState& s, DeepState& deep, int v, int first) {
   s.top = c.top;
   s.chain = c.chain;
-  if (c.chain) s.deep = *c.deep;
+  s.deep = -1;
+  if (c.chain) deep = *c.deep;
   s.tpos = c.ts.pos();
   s.prev = c.prev;
   s.v = v;
   s.first = first;
   s.count = 0;
   s.run = -1;
-  s.pad = 0;
 }
 
 // One thread per long list: walks the list once and records a slice every `len` edges.  A slice
 // that starts inside a run of equal successors gets run = the list index where that run starts
 // (the host turns it into a run index).  cap[b] slots are reserved per list.
 static __global__ void k_build_slices(GraphView g, const int32_t* big_v, const int64_t* slot_base, int32_t nbig, int32_t len,
-                               SliceState* out, int32_t* nslices) {
+                               SliceState* out, DeepState* deep_out, int32_t* nslices) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= nbig) return;
   const int v = big_v[b];
   SliceState* dst = out + slot_base[b];
+  DeepState* ddst = deep_out + slot_base[b];
   const int cap = (int)(slot_base[b + 1] - slot_base[b]);
   DeepState deep, saved_deep;
   EdgeCursor c(&deep);
   const int d = c.open(g, v);
-  cursor_save(c, dst[0], v, 0);
+  cursor_save(c, dst[0], ddst[0], v, 0);
   int k = 1, last = 0, prev_y = -1, run_start = 0;
   for (int i = 0; i < d; ++i) {
     const bool cand = (i - last >= len) && k < cap;
@@ -73,7 +76,7 @@ static __global__ void k_build_slices(GraphView g, const int32_t* big_v, const i
     if (!c.next(g, y, t)) break;
     if (cand) {
       dst[k - 1].count = i - last;
-      cursor_save(saved, dst[k], v, i);
+      cursor_save(saved, dst[k], ddst[k], v, i);
       if (y == prev_y) dst[k].run = run_start;
       last = i;
       ++k;
