@@ -93,7 +93,7 @@ struct GraphHandle {
 // Default slice length: short enough that a frontier level holding one slice of a hub is not
 // bound by a single thread's sequential decode, long enough that checkpoints stay a fraction of
 // the compressed bytes.
-constexpr int32_t kDefaultSliceEdges = 64;
+constexpr int32_t kDefaultSliceEdges = 32;
 
 int load_graph(GraphHandle& h, const std::string& dir, const std::string& base, const tga_dataset_cfg& cfg);
 // (Re)builds slices and work items: lists longer than slice_len edges are cut into slices,

@@ -98,7 +98,7 @@ int tga_get_info(tga_graph* g, tga_info* out);
 int tga_get_timing(tga_graph* g, tga_timing* out);
 /* Work decomposition of the sweeps and traversals: lists longer than slice_edges are cut into
  * resumable slices (decoder checkpoints built once), shorter lists are grouped into work items of
- * about item_edges edges.  Defaults 64 / 256, or $TGA_SLICE_EDGES / $TGA_ITEM_EDGES at open.
+ * about item_edges edges.  Defaults 32 / 256, or $TGA_SLICE_EDGES / $TGA_ITEM_EDGES at open.
  * The reference has no counterpart (one thread per vertex, shared/neighbor_access.cu:1599-1642). */
 int tga_set_work_params(tga_graph* g, int32_t slice_edges, int32_t item_edges);
 int tga_get_work_params(tga_graph* g, int32_t* slice_edges, int32_t* item_edges, int64_t* slices, int32_t* items);
