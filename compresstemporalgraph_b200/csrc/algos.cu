@@ -13,6 +13,7 @@
 #include <curand_kernel.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -41,6 +42,20 @@ __global__ void TGA_SWEEP_BOUNDS k_neighbor_access(GraphView g, Work w, int32_t 
       },
       [&](int v) { atomicAdd(&csum[v], (unsigned long long)h); });
   add_edges(edges, mine);
+}
+
+// Largest timestamp over all lists (a pass over the timestamp streams; run once at load).
+__global__ void TGA_SWEEP_BOUNDS k_max_timestamp(GraphView g, Work w, long long* out) {
+  long long m = LLONG_MIN;
+  run_order<false>(
+      g, w, [&](int) { return true; }, [&](int, int, int) { return true; },
+      [&](int, int, int64_t t) {
+        m = max(m, (long long)t);
+        return true;
+      },
+      [&](int) {});
+  for (int o = 16; o; o >>= 1) m = max(m, __shfl_down_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0 && m != LLONG_MIN) atomicMax(out, m);
 }
 
 __global__ void k_small_flags(const int32_t* deg, uint8_t* small, int32_t begin, int32_t end) {
@@ -187,12 +202,13 @@ __global__ void k_hits_base(float* hub, const float* auth_in, float* auth_next, 
   auth_next[x] = java ? 0.0f : auth_in[x] * sa;
 }
 
+template <bool kTimes>
 __global__ void TGA_SWEEP_BOUNDS k_hits_hub(GraphView g, Work w, float* hub, const float* auth_in, const double* aprev,
                                              int64_t lo, int64_t hi, unsigned long long* edges) {
   const float sa = (aprev && *aprev > 0) ? (float)(1.0 / sqrt(*aprev)) : 1.0f;
   float acc = 0.0f;
   int prev_y = -1;
-  const unsigned long long mine = run_order<false, false, true>(
+  const unsigned long long mine = run_order<false, false, true, kTimes>(
       g, w, [&](int v) { return v >= g.active_begin && v < g.max_label; },
       [&](int, int, int) {
         acc = 0.0f;
@@ -209,12 +225,13 @@ __global__ void TGA_SWEEP_BOUNDS k_hits_hub(GraphView g, Work w, float* hub, con
   add_edges(edges, mine);
 }
 
+template <bool kTimes>
 __global__ void TGA_SWEEP_BOUNDS k_hits_auth(GraphView g, Work w, const float* hub, const double* hsum,
                                               float* auth_next, int64_t lo, int64_t hi, unsigned long long* edges) {
   const float sh = *hsum > 0 ? (float)(1.0 / sqrt(*hsum)) : 1.0f;
   float hn = 0.0f;
   int prev_y = -1;
-  const unsigned long long mine = run_order<false, false, true>(
+  const unsigned long long mine = run_order<false, false, true, kTimes>(
       g, w, [&](int v) { return v >= g.active_begin && v < g.max_label && hub[v] != 0.0f; },
       [&](int v, int, int) {
         hn = hub[v] * sh;
@@ -373,7 +390,7 @@ __global__ void TGA_DECODE_BOUNDS k_gc_check(GraphView g, Work w, const int32_t*
                                              uint32_t* found, unsigned long long* edges) {
   uint32_t px = 0;
   int prev_y = -1;
-  const unsigned long long mine = drive_queue(
+  const unsigned long long mine = drive_queue<false, false>(
       g, w, entries, en,
       [&](int x, int, int) {
         px = prio[x];
@@ -423,6 +440,23 @@ __global__ void k_gc_first(GraphView g, Work w, const int32_t* deg, int32_t n, i
 }
 
 // Host side: the queue entries of one vertex (itself or its slices).
+int compute_max_timestamp(GraphHandle& h) {
+  h.max_ts = INT64_MAX;
+  if (int rc = h.s_sum.ensure(4096)) return rc;
+  long long* out = reinterpret_cast<long long*>(h.s_sum.as<char>() + 3968);
+  const long long init = LLONG_MIN;
+  TGA_CUDA_TRY(cudaMemcpyAsync(out, &init, 8, cudaMemcpyHostToDevice, h.stream));
+  const Work w = work_of(h);
+  k_max_timestamp<<<sweep_grid(h), kBlock, 0, h.stream>>>(h.view, w, out);
+  TGA_CUDA_TRY(cudaGetLastError());
+  long long m = LLONG_MIN;
+  TGA_CUDA_TRY(cudaMemcpyAsync(&m, out, 8, cudaMemcpyDeviceToHost, h.stream));
+  TGA_CUDA_TRY(cudaStreamSynchronize(h.stream));
+  if (int rc = h.check_device_error()) return rc;
+  h.max_ts = (m == LLONG_MIN) ? h.view.min_ts : (int64_t)m;
+  return TGA_OK;
+}
+
 }  // namespace tga
 
 using namespace tga;
@@ -569,6 +603,9 @@ int tga_hits(tga_graph* gp, int32_t iters, int32_t mode, int64_t t_lo, int64_t t
   TGA_TRY(h.s_c.ensure((size_t)nv * 4));
   TGA_TRY(h.s_g.ensure((size_t)(2 * iters + 2) * 8));
   TGA_TRY(h.begin_call());
+  // With a window that holds every timestamp, HITS depends only on the successor order: the
+  // timestamp streams are not decoded.
+  const bool all_times = window_covers_all(h, t_lo, t_hi);
   prepare_runs(h, t_lo, t_hi);
   unsigned long long* edges = edge_counter(h);
   float* hub = h.s_a.as<float>();
@@ -586,12 +623,15 @@ int tga_hits(tga_graph* gp, int32_t iters, int32_t mode, int64_t t_lo, int64_t t
     KL(k_hits_base, grid_for(nv, kBlock))(hub, ain, anext, aprev, java, nv);
     Work w = work_of(h);
     cudaEvent_t* ev = h.kernel_begin();
-    KL(k_hits_hub, sweep_grid(h))(h.view, w, hub, ain, aprev, t_lo, t_hi, edges);
+    // (without decoded timestamps every edge reports t = 0, so the window check is opened fully)
+    if (all_times) KL(k_hits_hub<false>, sweep_grid(h))(h.view, w, hub, ain, aprev, INT64_MIN, INT64_MAX, edges);
+    else KL(k_hits_hub<true>, sweep_grid(h))(h.view, w, hub, ain, aprev, t_lo, t_hi, edges);
     h.kernel_end(ev);
     KL(k_sumsq, grid_for(nv, kBlock))(hub, nv, sums + 2 * k);
     w = work_of(h);
     ev = h.kernel_begin();
-    KL(k_hits_auth, sweep_grid(h))(h.view, w, hub, sums + 2 * k, anext, t_lo, t_hi, edges);
+    if (all_times) KL(k_hits_auth<false>, sweep_grid(h))(h.view, w, hub, sums + 2 * k, anext, INT64_MIN, INT64_MAX, edges);
+    else KL(k_hits_auth<true>, sweep_grid(h))(h.view, w, hub, sums + 2 * k, anext, t_lo, t_hi, edges);
     h.kernel_end(ev);
     KL(k_scale, grid_for(nv, kBlock))(hub, sums + 2 * k, hub, nv);
     KL(k_sumsq, grid_for(nv, kBlock))(anext, nv, sums + 2 * k + 1);

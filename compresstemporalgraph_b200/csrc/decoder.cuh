@@ -423,18 +423,25 @@ struct EdgeCursor {
     }
     return remaining;
   }
-  // Next (successor, timestamp); returns false when the list is exhausted.
+  // Next (successor, timestamp); returns false when the list is exhausted.  kTimes = false skips
+  // the timestamp stream (t is then 0 and the cursor's timestamp state is left behind): for
+  // workloads whose result does not depend on time.
+  template <bool kTimes = true>
   __device__ __forceinline__ bool next(const GraphView& g, int& y, int64_t& t) {
     if (remaining <= 0) return false;
     --remaining;
     y = top_next(g, top, deep);
-    int len = 0;
-    bool bad = false;
-    const uint64_t z = win_zeta<2>(ts.window(), &len, &bad);
-    if (bad) set_err(g, kErrCode);
-    ts.skip(len);
-    prev += d_nat2int(z);
-    t = prev;
+    if (kTimes) {
+      int len = 0;
+      bool bad = false;
+      const uint64_t z = win_zeta<2>(ts.window(), &len, &bad);
+      if (bad) set_err(g, kErrCode);
+      ts.skip(len);
+      prev += d_nat2int(z);
+      t = prev;
+    } else {
+      t = 0;
+    }
     if (y == kInf || y < 0 || y >= g.n) {
       set_err(g, y == kInf ? kErrCount : kErrId);
       remaining = 0;

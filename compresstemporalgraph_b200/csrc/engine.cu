@@ -318,7 +318,9 @@ int load_graph(GraphHandle& h, const std::string& dir, const std::string& base, 
   h.degrees = std::move(deg);
   const char* env_slice = std::getenv("TGA_SLICE_EDGES");
   const char* env_item = std::getenv("TGA_ITEM_EDGES");
-  return build_work(h, env_slice ? std::atoi(env_slice) : kDefaultSliceEdges, env_item ? std::atoi(env_item) : 256);
+  if (int rc = build_work(h, env_slice ? std::atoi(env_slice) : kDefaultSliceEdges, env_item ? std::atoi(env_item) : 256))
+    return rc;
+  return compute_max_timestamp(h);
 }
 
 int publish_view(GraphHandle& h) {

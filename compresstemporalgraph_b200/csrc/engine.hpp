@@ -80,6 +80,7 @@ struct GraphHandle {
   tga_timing timing{};
   bool time_kernels = true;
   int64_t info_edges = 0;            // total temporal edges (sum of outdegrees)
+  int64_t max_ts = INT64_MAX;        // largest timestamp of the graph (computed at load)
   std::vector<int32_t> degrees;      // host copy of the outdegrees
 
   int begin_call();                 // resets timing, records the start event
@@ -101,6 +102,13 @@ int load_graph(GraphHandle& h, const std::string& dir, const std::string& base, 
 int build_work(GraphHandle& h, int32_t slice_len, int32_t item_edges);
 // Uploads the current view to its device-global copy (after any change of `view`).
 int publish_view(GraphHandle& h);
+
+// Computes h.max_ts with one timestamp-only pass (after the work decomposition exists).
+int compute_max_timestamp(GraphHandle& h);
+// True when [lo, hi) contains every timestamp of the graph.
+inline bool window_covers_all(const GraphHandle& h, int64_t lo, int64_t hi) {
+  return lo <= h.view.min_ts && hi > h.max_ts;
+}
 
 // Launch helpers shared by the algorithm files.
 inline unsigned grid_for(int64_t items, int block) { return (unsigned)((items + block - 1) / block); }

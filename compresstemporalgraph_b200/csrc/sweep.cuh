@@ -156,7 +156,9 @@ __device__ __forceinline__ int spread_warp_rank() {
 // kSpread: chunks of 32 entries are dealt by spread_warp_rank() (for persistent grids, where the
 // blocks holding the first entries would otherwise get all the slices of the first long lists).
 // kRuns: slices that start inside a run of equal successors pass their edges through RunFilter.
-template <bool kWhole, bool kSpread = false, bool kRuns = false, class Want, class Begin, class Edge, class End>
+// kTimes = false: timestamps are not decoded (edge() sees t = 0).
+template <bool kWhole, bool kSpread = false, bool kRuns = false, bool kTimes = true, class Want, class Begin, class Edge,
+          class End>
 __device__ __forceinline__ unsigned long long run_order(const GraphView& g, const Work& w, Want want, Begin begin,
                                                         Edge edge, End end) {
   unsigned long long edges = 0;
@@ -189,7 +191,7 @@ __device__ __forceinline__ unsigned long long run_order(const GraphView& g, cons
     if (kRuns) rf.start(lead, first);
     int y;
     int64_t t;
-    while (c.next(g, y, t)) {
+    while (c.template next<kTimes>(g, y, t)) {
       ++edges;
       if (kRuns && !rf.pass(y)) continue;
       if (!edge(x, y, t)) break;
@@ -200,8 +202,9 @@ __device__ __forceinline__ unsigned long long run_order(const GraphView& g, cons
 }
 
 // Flat loop over the entries q[0..qn) of a queue (vertices or slices); q may have been written
-// earlier in the same launch by other blocks (it is read through L2).  kRuns as in run_order.
-template <bool kRuns = false, class Begin, class Edge, class End>
+// earlier in the same launch by other blocks (it is read through L2).  kRuns, kTimes as in
+// run_order.
+template <bool kRuns = false, bool kTimes = true, class Begin, class Edge, class End>
 __device__ __forceinline__ unsigned long long drive_queue(const GraphView& g, const Work& w, const int32_t* q, int qn,
                                                           Begin begin, Edge edge, End end) {
   DeepState deep;
@@ -244,7 +247,7 @@ __device__ __forceinline__ unsigned long long drive_queue(const GraphView& g, co
     }
     int y;
     int64_t t;
-    if (!c.next(g, y, t)) continue;
+    if (!c.template next<kTimes>(g, y, t)) continue;
     ++edges;
     if (kRuns && !rf.pass(y)) continue;
     if (!edge(cur, y, t)) c.remaining = 0;
