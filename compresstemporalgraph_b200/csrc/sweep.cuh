@@ -81,8 +81,9 @@ struct Work {
 // Opens queue entry e: a whole list (e >= 0) or one slice.  Returns the vertex; `lead` is the
 // leading-run filter of the entry (see RunFilter).
 __device__ __forceinline__ int open_entry(const GraphView& g, const Work& w, int e, EdgeCursor& c, int& first,
-                                          int& count, int& lead) {
+                                          int& count, int& lead, int& run) {
   lead = kNoRunFilter;
+  run = -1;
   if (e >= 0) {
     first = 0;
     count = c.open(g, e);
@@ -93,6 +94,7 @@ __device__ __forceinline__ int open_entry(const GraphView& g, const Work& w, int
   first = s.first;
   count = s.count;
   if (s.run >= 0 && w.run_first) lead = __ldg(w.run_first + s.run);
+  run = s.run;
   return s.v;
 }
 
@@ -157,8 +159,10 @@ __device__ __forceinline__ int spread_warp_rank() {
 // blocks holding the first entries would otherwise get all the slices of the first long lists).
 // kRuns: slices that start inside a run of equal successors pass their edges through RunFilter.
 // kTimes = false: timestamps are not decoded (edge() sees t = 0).
-template <bool kWhole, bool kSpread = false, bool kRuns = false, bool kTimes = true, class Want, class Begin, class Edge,
-          class End>
+// kRunArg: begin() takes a fourth argument, the index of the run of equal successors that a slice
+// starts inside (-1 for whole lists and slices that start at a new successor).
+template <bool kWhole, bool kSpread = false, bool kRuns = false, bool kTimes = true, bool kRunArg = false, class Want,
+          class Begin, class Edge, class End>
 __device__ __forceinline__ unsigned long long run_order(const GraphView& g, const Work& w, Want want, Begin begin,
                                                         Edge edge, End end) {
   unsigned long long edges = 0;
@@ -168,7 +172,7 @@ __device__ __forceinline__ unsigned long long run_order(const GraphView& g, cons
     DeepState deep;
     EdgeCursor c(&deep);
     RunFilter rf;
-    int x, first = 0, count, lead = kNoRunFilter;
+    int x, first = 0, count, lead = kNoRunFilter, run = -1;
     if (e >= 0) {
       x = e;
       if (!want(x)) continue;
@@ -185,9 +189,13 @@ __device__ __forceinline__ unsigned long long run_order(const GraphView& g, cons
         first = s.first;
         count = s.count;
         if (kRuns && s.run >= 0) lead = __ldg(w.run_first + s.run);
+        run = s.run;
       }
     }
-    if (count <= 0 || !begin(x, first, count)) continue;
+    bool go;
+    if constexpr (kRunArg) go = count > 0 && begin(x, first, count, run);
+    else go = count > 0 && begin(x, first, count);
+    if (!go) continue;
     if (kRuns) rf.start(lead, first);
     int y;
     int64_t t;
@@ -202,9 +210,9 @@ __device__ __forceinline__ unsigned long long run_order(const GraphView& g, cons
 }
 
 // Flat loop over the entries q[0..qn) of a queue (vertices or slices); q may have been written
-// earlier in the same launch by other blocks (it is read through L2).  kRuns, kTimes as in
-// run_order.
-template <bool kRuns = false, bool kTimes = true, class Begin, class Edge, class End>
+// earlier in the same launch by other blocks (it is read through L2).  kRuns, kTimes, kRunArg as
+// in run_order.
+template <bool kRuns = false, bool kTimes = true, bool kRunArg = false, class Begin, class Edge, class End>
 __device__ __forceinline__ unsigned long long drive_queue(const GraphView& g, const Work& w, const int32_t* q, int qn,
                                                           Begin begin, Edge edge, End end) {
   DeepState deep;
@@ -234,10 +242,13 @@ __device__ __forceinline__ unsigned long long drive_queue(const GraphView& g, co
       }
       if (i < 0) i = nthreads + atomicAdd(w.next, 1);
       if (i >= qn) break;
-      int first, count, lead;
-      const int x = open_entry(g, w, __ldcg(q + i), c, first, count, lead);
+      int first, count, lead, run;
+      const int x = open_entry(g, w, __ldcg(q + i), c, first, count, lead, run);
       i = -1;
-      if (count <= 0 || !begin(x, first, count)) {
+      bool go;
+      if constexpr (kRunArg) go = count > 0 && begin(x, first, count, run);
+      else go = count > 0 && begin(x, first, count);
+      if (!go) {
         c.remaining = 0;
         continue;
       }

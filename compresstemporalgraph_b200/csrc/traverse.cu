@@ -23,25 +23,9 @@
 #include <cstring>
 #include <vector>
 
-#include "sweep.cuh"
+#include "gridsync.cuh"
 
 namespace tga {
-
-constexpr uint64_t kBarrierNs = 10ull * 1000 * 1000 * 1000;  // longest wait at a grid barrier
-
-// Control block of one launch (zeroed by the host before the launch, best = INT32_MAX).
-struct TravCtl {
-  int32_t cnt[3];        // queue lengths (rotating, see above)
-  int32_t next[3];       // work counters of the levels (same rotation)
-  uint32_t bar_count;    // grid barrier: blocks arrived
-  uint32_t bar_gen;      // grid barrier: generation
-  int32_t status;        // nonzero: a barrier wait ran out
-  int32_t levels;        // levels executed
-  int32_t tcnt;          // CC: vertices whose arrival became finite for the current seed
-  int32_t best;          // CC: seed search minimum
-  int32_t comps;         // CC: components
-  int32_t pad[3];
-};
 
 struct TravArgs {
   Work w;
@@ -68,50 +52,6 @@ struct TravArgs {
   int32_t cc_begin, cc_end, limit, early;
 };
 
-__device__ __forceinline__ uint64_t global_ns() {
-  uint64_t t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-// Barrier over all blocks of the cooperative launch; false if the launch has failed (this block
-// must return at once).
-__device__ bool grid_sync(TravCtl* ctl, const GraphView& g) {
-  __shared__ int failed;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    failed = 0;
-    volatile uint32_t* gen = &ctl->bar_gen;
-    volatile int32_t* status = &ctl->status;
-    const uint32_t mine = *gen;
-    __threadfence();
-    if (atomicAdd(&ctl->bar_count, 1u) == gridDim.x - 1) {
-      ctl->bar_count = 0;
-      __threadfence();
-      atomicAdd(&ctl->bar_gen, 1u);
-    } else {
-      const uint64_t t0 = global_ns();
-      for (uint32_t spin = 0; *gen == mine; ++spin) {
-        if (*status) {
-          failed = 1;
-          break;
-        }
-        if ((spin & 255u) == 255u && global_ns() - t0 > kBarrierNs) {
-          atomicExch(&ctl->status, 1);
-          set_err(g, kErrTimeout);
-          failed = 1;
-          break;
-        }
-        __nanosleep(100);
-      }
-    }
-    if (*status) failed = 1;
-    __threadfence();
-  }
-  __syncthreads();
-  return !failed;
-}
-
 // Appends the entries of vertex v (v itself or its slices) to q at L's slot; one thread.
 __device__ __forceinline__ void seed_queue(const Work& w, TravArgs& a, int L, int v) {
   int32_t* q = a.q[L & 1];
@@ -121,35 +61,6 @@ __device__ __forceinline__ void seed_queue(const Work& w, TravArgs& a, int L, in
   else
     for (int j = s0; j < s1; ++j) q[k++] = -(j + 1);
   a.ctl->cnt[L % 3] = k;
-}
-
-// Reserves n slots per lane with one atomic per warp (all 32 lanes must call it together); returns
-// this lane's first slot.
-__device__ __forceinline__ int warp_reserve(int32_t* cnt, int n) {
-  const unsigned full = 0xffffffffu;
-  const int lane = threadIdx.x & 31;
-  int incl = n;
-  for (int o = 1; o < 32; o <<= 1) {
-    const int v = __shfl_up_sync(full, incl, o);
-    if (lane >= o) incl += v;
-  }
-  const int total = __shfl_sync(full, incl, 31);
-  int base = 0;
-  if (lane == 31 && total) base = atomicAdd(cnt, total);
-  base = __shfl_sync(full, base, 31);
-  return base + incl - n;
-}
-
-// Entries of vertex v in a queue: v itself or all its slices.
-__device__ __forceinline__ int entry_count(const Work& w, int v) {
-  const int n = __ldg(w.slice_first + v + 1) - __ldg(w.slice_first + v);
-  return n ? n : 1;
-}
-__device__ __forceinline__ void write_entries(const Work& w, int v, int32_t* q, int at) {
-  const int s0 = __ldg(w.slice_first + v), s1 = __ldg(w.slice_first + v + 1);
-  if (s0 == s1) q[at] = v;
-  else
-    for (int j = s0; j < s1; ++j) q[at++] = -(j + 1);
 }
 
 // Scan over the dirty bitmap after a level: keep(v) decides (once per marked vertex, by the one

@@ -190,6 +190,23 @@ def test_batched_bfs_equals_single(pairs):
         assert np.array_equal(out[i], arr)
 
 
+@pytest.mark.parametrize("shape", ["hubs", "intervals"])
+def test_batched_bfs_many_sources_vs_oracle(pairs, shape):
+    """300 sources (two launches of at most 256), each with its own window, duplicates included."""
+    p = pairs[shape]
+    rng = np.random.default_rng(4)
+    lo0, span = p.d["params"].min_timestamp, p.d["params"].ts_span
+    srcs = rng.integers(0, p.n, 300).astype(np.int32)
+    srcs[10] = srcs[11]
+    lo = lo0 + rng.integers(0, span // 2, 300)
+    hi = lo + rng.integers(span // 20, span // 2, 300)
+    lo[:5], hi[:5] = 0, T_MAX
+    out = p.g.bfs_batch(srcs, lo, hi)
+    for i in list(range(0, 300, 7)) + [10, 11, 255, 256, 299]:
+        oarr, _ = p.o.bfs(p.ml, p.mv, p.act, int(srcs[i]), int(lo[i]), int(hi[i]))
+        assert np.array_equal(out[i], oarr), i
+
+
 def test_batched_pagerank_equals_single(pairs):
     p = pairs["small"]
     span = p.d["params"].ts_span
@@ -251,6 +268,13 @@ def test_work_decomposition_does_not_change_results(pairs, shape, slice_edges, i
         assert k == ok and np.array_equal(lab, olab)
         r = g.pagerank(5, 0.85, 0.1, lo, hi)
         assert float(np.abs(r - p.o.pagerank(p.ml, p.mv, p.act, 5, 0.85, 0.1, lo, hi)).sum()) <= 1e-5
+        srcs = np.array([src, src, 0, p.n - 1, src], np.int32)
+        blo = np.array([lo, 0, lo, 0, lo + (hi - lo) // 2], np.int64)
+        bhi = np.array([hi, T_MAX, hi, hi, hi], np.int64)
+        bout = g.bfs_batch(srcs, blo, bhi)
+        for i in range(len(srcs)):
+            oarr, _ = p.o.bfs(p.ml, p.mv, p.act, int(srcs[i]), int(blo[i]), int(bhi[i]))
+            assert np.array_equal(bout[i], oarr), i
         hub, auth = g.hits(5, tga.HITS_JAVA, lo, hi)
         ohub, oauth = p.o.hits(p.ml, p.mv, p.act, 5, True, lo, hi)
         assert float(np.abs(hub.astype(np.float64) - ohub).max()) <= 1e-5
