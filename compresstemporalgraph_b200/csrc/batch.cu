@@ -347,13 +347,239 @@ static int bfs_multi_batch(GraphHandle& h, int32_t nsrc, const int32_t* src, con
   return finish(h, edges);
 }
 
+// ---------------------------------------------------------------------------------------------
+// Multi-query PageRank: up to kMaxRankQueries windowed PageRanks as one strided vector
+// (rank[v * kMaxRankQueries + q]), each list decoded once per iteration.  Per edge the temporal
+// weight is computed once and the contribution scattered to every query whose window holds the
+// edge (first in-window occurrence of equal consecutive successors per query, as tga_pagerank).
+
+constexpr int kMaxRankQueries = 32;
+
+struct PrMultiArgs {
+  const float* invdeg;       // [nv][kMaxRankQueries] 1 / in-window outdegree (windowed queries)
+  const int32_t* deg;        // outdegrees (other queries)
+  const float* in;
+  float* out;
+  float* reset;
+  const double* sums_prev;   // [kMaxRankQueries] sums of the previous iteration, or null
+  const int64_t* lo;
+  const int64_t* hi;
+  const int32_t* run_first;  // [nruns][kMaxSources]
+  uint32_t windowed;         // bit q: query q uses its in-window outdegree
+  int32_t nq, nv;
+  float damping, alpha, base;
+  unsigned long long* edges;
+};
+
+__device__ __forceinline__ float temporal_weight_multi(float alpha, int64_t t) {
+  const float a = alpha * (float)t;
+  return a > 18.0f ? 1.0f : 1.0f - expf(-a);
+}
+
+__global__ void TGA_DECODE_BOUNDS k_pr_multi_iter(GraphView g, Work w, PrMultiArgs a) {
+  __shared__ int64_t slo[kMaxRankQueries], shi[kMaxRankQueries];
+  __shared__ float sinv[kMaxRankQueries];
+  for (int q = threadIdx.x; q < kMaxRankQueries; q += blockDim.x) {
+    slo[q] = q < a.nq ? a.lo[q] : 0;
+    shi[q] = q < a.nq ? a.hi[q] : 0;
+    sinv[q] = (q < a.nq && a.sums_prev) ? (float)(1.0 / a.sums_prev[q]) : 1.0f;
+  }
+  __syncthreads();
+  const int64_t total = (int64_t)a.nv * kMaxRankQueries;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x)
+    a.reset[i] = a.base;
+  float c0[kMaxRankQueries];
+  uint32_t act = 0, seen = 0;
+  int yprev = -1;
+  constexpr int kKeepSeen = -3;
+  const unsigned long long mine = run_order<false, false, false, true, true>(
+      g, w, [&](int v) { return v >= g.active_begin && v < g.max_label; },
+      [&](int x, int first, int, int run) {
+        act = 0;
+        const float inv_all = a.deg[x] > 0 ? 1.0f / (float)a.deg[x] : 0.0f;
+#pragma unroll
+        for (int q = 0; q < kMaxRankQueries; ++q) {
+          float c = 0.0f;
+          if (q < a.nq) {
+            const float inv = ((a.windowed >> q) & 1u) ? a.invdeg[(size_t)x * kMaxRankQueries + q] : inv_all;
+            if (inv > 0.0f) c = a.damping * (a.in[(size_t)x * kMaxRankQueries + q] * sinv[q]) * inv;
+          }
+          c0[q] = c;
+          if (c != 0.0f) act |= 1u << q;
+        }
+        seen = 0;
+        yprev = -1;
+        if (run >= 0) {
+          const int32_t* rf = a.run_first + (size_t)run * kMaxSources;
+          for (uint32_t c = act; c; c &= c - 1) {
+            const int q = __ffs(c) - 1;
+            if (__ldg(rf + q) < first) seen |= 1u << q;
+          }
+          yprev = kKeepSeen;
+        }
+        return act != 0;
+      },
+      [&](int, int y, int64_t t) {
+        if (yprev == kKeepSeen) {
+          yprev = y;
+        } else if (y != yprev) {
+          seen = 0;
+          yprev = y;
+        }
+        const bool usable = y >= g.active_begin && y < g.max_vertex;
+        float wgt = 0.0f;
+        bool have_w = false;
+        for (uint32_t c = act & ~seen; c; c &= c - 1) {
+          const int q = __ffs(c) - 1;
+          if (t < slo[q] || t >= shi[q]) continue;
+          seen |= 1u << q;
+          if (!usable) continue;
+          if (!have_w) {
+            wgt = temporal_weight_multi(a.alpha, t);
+            have_w = true;
+          }
+          atomicAdd(&a.out[(size_t)y * kMaxRankQueries + q], c0[q] * wgt);
+        }
+        return true;
+      },
+      [](int) {});
+  add_edges(a.edges, mine);
+}
+
+// In-window outdegree per query (lists counted by slices), then 1/count.
+__global__ void TGA_DECODE_BOUNDS k_window_count_multi(GraphView g, Work w, const int64_t* lo, const int64_t* hi,
+                                                     int32_t nq, int32_t* cnt, unsigned long long* edges) {
+  __shared__ int64_t slo[kMaxRankQueries], shi[kMaxRankQueries];
+  for (int q = threadIdx.x; q < kMaxRankQueries; q += blockDim.x) {
+    slo[q] = q < nq ? lo[q] : 0;
+    shi[q] = q < nq ? hi[q] : 0;
+  }
+  __syncthreads();
+  int k[kMaxRankQueries];
+  const unsigned long long mine = run_order<false>(
+      g, w, [&](int v) { return v >= g.active_begin && v < g.max_label; },
+      [&](int, int, int) {
+#pragma unroll
+        for (int q = 0; q < kMaxRankQueries; ++q) k[q] = 0;
+        return true;
+      },
+      [&](int, int, int64_t t) {
+#pragma unroll
+        for (int q = 0; q < kMaxRankQueries; ++q) k[q] += (t >= slo[q] && t < shi[q]);
+        return true;
+      },
+      [&](int v) {
+#pragma unroll
+        for (int q = 0; q < kMaxRankQueries; ++q)
+          if (q < nq && k[q]) atomicAdd(&cnt[(size_t)v * kMaxRankQueries + q], k[q]);
+      });
+  add_edges(edges, mine);
+}
+
+__global__ void k_invert_multi(const int32_t* cnt, float* inv, int64_t n) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) inv[i] = cnt[i] ? 1.0f / (float)cnt[i] : 0.0f;
+}
+
+// sums[q] = sum over v of buf[v][q] (FP64), one block per query.
+__global__ void k_sums_multi(const float* buf, int32_t nv, double* sums) {
+  const int q = blockIdx.x;
+  double s = 0.0;
+  for (int v = threadIdx.x; v < nv; v += blockDim.x) s += (double)buf[(size_t)v * kMaxRankQueries + q];
+  const double bs = block_sum(s);
+  if (threadIdx.x == 0) sums[q] = bs;
+}
+
+__global__ void k_pr_multi_final(const float* buf, const double* sums, int32_t nq, int32_t nv, float* out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (int64_t)nq * nv) return;
+  const int q = (int)(i / nv), v = (int)(i % nv);
+  out[i] = (float)((double)buf[(size_t)v * kMaxRankQueries + q] / sums[q]);
+}
+
+static int pagerank_multi_batch(GraphHandle& h, int32_t nq, int32_t iters, float damping, float alpha,
+                                const int64_t* t_lo, const int64_t* t_hi, float* rank_out) {
+  const size_t nv = (size_t)h.view.max_vertex;
+  const size_t vec = nv * kMaxRankQueries;
+  // s_a: 3 rank buffers | invdeg; s_b: counts; s_d: windows + sums + run table; s_e: output
+  TGA_TRY(h.s_a.ensure(vec * 4 * 4));
+  TGA_TRY(h.s_b.ensure(vec * 4));
+  const size_t run_bytes = (size_t)std::max(h.nruns, 1) * kMaxSources * 4;
+  const size_t sums_off = kMaxSources * 16;
+  TGA_TRY(h.s_d.ensure(sums_off + (size_t)(iters + 1) * kMaxRankQueries * 8 + run_bytes));
+  TGA_TRY(h.s_e.ensure((size_t)nq * nv * 4));
+  TGA_TRY(h.begin_call());
+  unsigned long long* edges = edge_counter(h);
+  float* bufs[3] = {h.s_a.as<float>(), h.s_a.as<float>() + vec, h.s_a.as<float>() + 2 * vec};
+  float* invdeg = h.s_a.as<float>() + 3 * vec;
+  int32_t* cnt = h.s_b.as<int32_t>();
+  int64_t* dlo = h.s_d.as<int64_t>();
+  int64_t* dhi = dlo + kMaxSources;
+  double* sums = reinterpret_cast<double*>(h.s_d.as<char>() + sums_off);
+  int32_t* drf = reinterpret_cast<int32_t*>(sums + (size_t)(iters + 1) * kMaxRankQueries);
+  TGA_CUDA_TRY(cudaMemcpyAsync(dlo, t_lo, (size_t)nq * 8, cudaMemcpyHostToDevice, h.stream));
+  TGA_CUDA_TRY(cudaMemcpyAsync(dhi, t_hi, (size_t)nq * 8, cudaMemcpyHostToDevice, h.stream));
+  uint32_t windowed = 0;
+  for (int q = 0; q < nq; ++q)
+    if (!(t_lo[q] <= 0 && t_hi[q] == TGA_T_MAX)) windowed |= 1u << q;
+  if (h.nruns > 0) {
+    KL(k_fill_i32, grid_for((int64_t)h.nruns * kMaxSources, kBlock))(drf, INT32_MAX, (int64_t)h.nruns * kMaxSources);
+    KL(k_run_first_multi, grid_for(h.nrun_pairs, kBlock))(h.view, h.d_slices.as<SliceState>(), h.d_runs.as<RunInfo>(),
+                                                         h.d_run_pairs.as<int2>(), h.nrun_pairs, dlo, dhi, nq, drf);
+  }
+  const float base = (1.0f - damping) / (float)h.view.max_label;
+  KL(k_fill_f32, grid_for((int64_t)vec, kBlock))(bufs[0], 1.0f / (float)nv, (int64_t)vec);
+  KL(k_fill_f32, grid_for((int64_t)vec, kBlock))(bufs[1], base, (int64_t)vec);
+  if (windowed) {
+    TGA_CUDA_TRY(cudaMemsetAsync(cnt, 0, vec * 4, h.stream));
+    const Work w = work_of(h);
+    cudaEvent_t* ev = h.kernel_begin();
+    KL(k_window_count_multi, sweep_grid(h))(h.view, w, dlo, dhi, nq, cnt, edges);
+    h.kernel_end(ev);
+    KL(k_invert_multi, grid_for((int64_t)vec, kBlock))(cnt, invdeg, (int64_t)vec);
+  }
+  for (int k = 0; k < iters; ++k) {
+    Work w = work_of(h);
+    PrMultiArgs a{};
+    a.invdeg = invdeg;
+    a.deg = h.d_deg.as<int32_t>();
+    a.in = bufs[k % 3];
+    a.out = bufs[(k + 1) % 3];
+    a.reset = bufs[(k + 2) % 3];
+    a.sums_prev = k == 0 ? nullptr : sums + (size_t)(k - 1) * kMaxRankQueries;
+    a.lo = dlo;
+    a.hi = dhi;
+    a.run_first = drf;
+    a.windowed = windowed;
+    a.nq = nq;
+    a.nv = (int32_t)nv;
+    a.damping = damping;
+    a.alpha = alpha;
+    a.base = base;
+    a.edges = edges;
+    cudaEvent_t* ev = h.kernel_begin();
+    KL(k_pr_multi_iter, sweep_grid(h))(h.view, w, a);
+    h.kernel_end(ev);
+    k_sums_multi<<<nq, kBlock, 0, h.stream>>>(a.out, (int32_t)nv, sums + (size_t)k * kMaxRankQueries);
+    ++h.timing.launches;
+  }
+  float* out = h.s_e.as<float>();
+  KL(k_pr_multi_final, grid_for((int64_t)nq * (int64_t)nv, kBlock))(bufs[iters % 3],
+                                                                    sums + (size_t)(iters - 1) * kMaxRankQueries, nq,
+                                                                    (int32_t)nv, out);
+  if (rank_out) TGA_CUDA_TRY(cudaMemcpyAsync(rank_out, out, (size_t)nq * nv * 4, cudaMemcpyDeviceToHost, h.stream));
+  h.timing.iterations = iters;
+  const int rc = finish(h, edges);
+  h.timing.compressed_bytes = (uint64_t)(iters + (windowed ? 1 : 0)) *
+                              (h.info.graph_bytes + h.info.timestamp_bytes + h.info.index_bytes);
+  return rc;
+}
+
 }  // namespace tga
 
 using namespace tga;
 
 extern "C" {
-
-int tga_pagerank(tga_graph*, int32_t, float, float, int64_t, int64_t, float*);
 
 int tga_bfs_batch(tga_graph* g, int32_t nsrc, const int32_t* src, const int64_t* t_lo, const int64_t* t_hi,
                   int32_t* arrival_out) {
@@ -383,11 +609,26 @@ int tga_bfs_batch(tga_graph* g, int32_t nsrc, const int32_t* src, const int64_t*
 int tga_pagerank_batch(tga_graph* g, int32_t nq, int32_t iters, float damping, float alpha, const int64_t* t_lo,
                        const int64_t* t_hi, float* rank_out) {
   if (!g || nq < 0 || (nq && (!t_lo || !t_hi))) return fail(TGA_E_ARG, "bad argument");
-  const size_t nv = (size_t)g->view.max_vertex;
-  for (int32_t i = 0; i < nq; ++i) {
-    const int rc = tga_pagerank(g, iters, damping, alpha, t_lo[i], t_hi[i], rank_out ? rank_out + i * nv : nullptr);
+  GraphHandle& h = *g;
+  if (iters <= 0) iters = h.cfg.pr_iters;
+  for (int32_t i = 0; i < nq; ++i)
+    if (t_lo[i] >= t_hi[i]) return fail(TGA_E_ARG, "empty time window");
+  const size_t nv = (size_t)h.view.max_vertex;
+  tga_timing total{};
+  for (int32_t b = 0; b < nq; b += kMaxRankQueries) {
+    const int32_t k = std::min(kMaxRankQueries, nq - b);
+    const int rc = pagerank_multi_batch(h, k, iters, damping, alpha, t_lo + b, t_hi + b,
+                                        rank_out ? rank_out + (size_t)b * nv : nullptr);
     if (rc) return rc;
+    total.total_ms += h.timing.total_ms;
+    total.decode_ms += h.timing.decode_ms;
+    total.decode_launches += h.timing.decode_launches;
+    total.edges_decoded += h.timing.edges_decoded;
+    total.compressed_bytes += h.timing.compressed_bytes;
+    total.iterations = h.timing.iterations;
+    total.launches += h.timing.launches;
   }
+  h.timing = total;
   return TGA_OK;
 }
 

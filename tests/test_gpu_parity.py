@@ -218,6 +218,23 @@ def test_batched_pagerank_equals_single(pairs):
         assert np.allclose(out[i], r, rtol=1e-4, atol=1e-9)
 
 
+@pytest.mark.parametrize("shape", ["hubs", "chains"])
+def test_batched_pagerank_many_queries_vs_oracle(pairs, shape):
+    """40 queries (two launches of at most 32), full and windowed, against the FP64 oracle with the
+    tolerance of test_pagerank_fp32_vs_fp64."""
+    p = pairs[shape]
+    rng = np.random.default_rng(6)
+    lo0, span = p.d["params"].min_timestamp, p.d["params"].ts_span
+    lo = lo0 + rng.integers(0, span // 2, 40)
+    hi = lo + rng.integers(span // 20, span // 2, 40)
+    lo[:3], hi[:3] = 0, T_MAX
+    out = p.g.pagerank_batch(lo, hi, iters=8)
+    for i in list(range(0, 40, 6)) + [1, 31, 32, 39]:
+        o = p.o.pagerank(p.ml, p.mv, p.act, 8, 0.85, 0.1, int(lo[i]), int(hi[i]))
+        assert float(np.abs(out[i].astype(np.float64) - o).sum()) <= 1e-5, i
+        assert np.allclose(out[i], o, rtol=1e-4, atol=1e-9), i
+
+
 def test_timing_reports_device_time(pairs):
     p = pairs["small"]
     p.g.pagerank(3)
@@ -275,6 +292,9 @@ def test_work_decomposition_does_not_change_results(pairs, shape, slice_edges, i
         for i in range(len(srcs)):
             oarr, _ = p.o.bfs(p.ml, p.mv, p.act, int(srcs[i]), int(blo[i]), int(bhi[i]))
             assert np.array_equal(bout[i], oarr), i
+        rb = g.pagerank_batch(np.array([lo, 0], np.int64), np.array([hi, T_MAX], np.int64), iters=5)
+        assert float(np.abs(rb[0] - p.o.pagerank(p.ml, p.mv, p.act, 5, 0.85, 0.1, lo, hi)).sum()) <= 1e-5
+        assert float(np.abs(rb[1] - p.o.pagerank(p.ml, p.mv, p.act, 5)).sum()) <= 1e-5
         hub, auth = g.hits(5, tga.HITS_JAVA, lo, hi)
         ohub, oauth = p.o.hits(p.ml, p.mv, p.act, 5, True, lo, hi)
         assert float(np.abs(hub.astype(np.float64) - ohub).max()) <= 1e-5
