@@ -59,6 +59,16 @@ class _Timing(C.Structure):
                 ("edges_decoded", C.c_int64), ("compressed_bytes", C.c_uint64), ("iterations", C.c_int32), ("launches", C.c_int64)]
 
 
+class _Query(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("graph", C.c_int32), ("src", C.c_int32), ("iters", C.c_int32),
+                ("t_lo", C.c_int64), ("t_hi", C.c_int64), ("out", C.c_void_p)]
+
+
+class _ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("failed", C.c_int64), ("rounds", C.c_int64),
+                ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("mean_ms", C.c_double), ("queries_per_s", C.c_double)]
+
+
 class _GenParams(C.Structure):
     _fields_ = [("n", C.c_int64), ("m", C.c_int64), ("deg_exponent", C.c_double), ("max_degree", C.c_int64),
                 ("repeat_frac", C.c_double), ("local_frac", C.c_double), ("local_radius", C.c_int32),
@@ -102,6 +112,13 @@ def _load() -> C.CDLL:
         "tga_color": (C.c_int, [P, C.c_int32, P, C.c_int32, P, P, C.POINTER(C.c_int32)]),
         "tga_bfs_batch": (C.c_int, [P, C.c_int32, P, P, P, P]),
         "tga_pagerank_batch": (C.c_int, [P, C.c_int32, C.c_int32, C.c_float, C.c_float, P, P, P]),
+        "tga_server_create": (C.c_int, [C.c_int64, C.POINTER(P)]),
+        "tga_server_add_graph": (C.c_int, [P, P, C.POINTER(C.c_int32)]),
+        "tga_submit": (C.c_int, [P, C.POINTER(_Query), C.POINTER(C.c_int64)]),
+        "tga_poll": (C.c_int, [P, C.c_int64, C.POINTER(C.c_double)]),
+        "tga_server_drain": (C.c_int, [P]),
+        "tga_server_get_stats": (C.c_int, [P, C.POINTER(_ServerStats)]),
+        "tga_server_destroy": (C.c_int, [P]),
         "tga_generate": (C.c_int, [C.POINTER(_GenParams), C.c_char_p, C.c_char_p, C.c_char_p,
                                    C.POINTER(_GenSummary)]),
         "tga_encode_raw": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int64, C.POINTER(_GenSummary)]),
@@ -322,6 +339,66 @@ class Graph:
         out = np.zeros((len(lo), self.max_vertex), np.float32)
         _check(_lib.tga_pagerank_batch(self._h, len(lo), iters, damping, alpha, _ptr(lo), _ptr(hi), _ptr(out)))
         return out
+
+
+# ---- served form -------------------------------------------------------------------------------
+
+Q_BFS, Q_PAGERANK, Q_CC = 0, 1, 2
+
+
+class Server:
+    """Request loop over resident graphs (tga_server_*): submit queries, poll or drain, read the
+    latency statistics.  Result arrays are owned here until the query finished."""
+
+    def __init__(self, budget_bytes: int):
+        h = C.c_void_p()
+        _check(_lib.tga_server_create(int(budget_bytes), C.byref(h)))
+        self._h = h
+        self._graphs: list[Graph] = []
+        self._keep: dict[int, np.ndarray] = {}
+
+    def add_graph(self, g: Graph) -> int:
+        gid = C.c_int32()
+        _check(_lib.tga_server_add_graph(self._h, g.handle, C.byref(gid)))
+        self._graphs.append(g)
+        return gid.value
+
+    def submit(self, kind: int, graph: int, src: int = 0, t_lo: int = 0, t_hi: int = T_MAX, iters: int = 0) -> int:
+        nv = self._graphs[graph].max_vertex
+        out = np.zeros(nv, np.float32 if kind == Q_PAGERANK else np.int32)
+        q = _Query(kind, graph, src, iters, t_lo, t_hi, out.ctypes.data)
+        ticket = C.c_int64()
+        _check(_lib.tga_submit(self._h, C.byref(q), C.byref(ticket)))
+        self._keep[ticket.value] = out
+        return ticket.value
+
+    def poll(self, ticket: int):
+        """None while pending; (result array, latency ms) when done."""
+        lat = C.c_double()
+        rc = _lib.tga_poll(self._h, ticket, C.byref(lat))
+        if rc == TGA_E_AGAIN:
+            return None
+        _check(rc)
+        return self._keep[ticket], lat.value
+
+    def drain(self) -> None:
+        _check(_lib.tga_server_drain(self._h))
+
+    def stats(self) -> dict:
+        st = _ServerStats()
+        _check(_lib.tga_server_get_stats(self._h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in _ServerStats._fields_}
+
+    def close(self) -> None:
+        if self._h:
+            _lib.tga_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 # ---- format layer -----------------------------------------------------------------------------

@@ -1,0 +1,286 @@
+// Served form: several resident graphs answer a stream of (algorithm, source, window) queries.
+//
+// One worker thread per graph repeatedly takes the queries that arrived since its last round,
+// admits them while the device working memory they need fits the server's budget (shared by all
+// graphs), and runs them together: the BFS queries as one batched traversal (tga_bfs_batch), the
+// PageRank queries with equal iteration counts as one strided vector (tga_pagerank_batch), and CC
+// queries one by one.  Queries that arrive during a round join the next one, and each graph's work
+// runs on that graph's own stream, so rounds of different graphs overlap on the device.  Latency
+// is measured from tga_submit to the moment the result is in the caller's buffer.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/tga.h"
+
+namespace tga {
+int fail(int code, const std::string& msg);
+}
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Pending {
+  tga_query q;
+  int64_t ticket;
+  int64_t bytes;
+  Clock::time_point submitted;
+};
+
+struct Outcome {
+  int status = TGA_E_AGAIN;
+  double latency_ms = 0.0;
+};
+
+struct GraphSlot {
+  tga_graph* g = nullptr;
+  int32_t nv = 0;
+  std::deque<Pending> pending;
+  std::thread worker;
+};
+
+// Device working bytes of one query (per vertex of its graph): BFS arrival + last-enqueued arrival
+// + result; PageRank three rank vectors + inverse degree + result; CC the single traversal's arrays.
+int64_t query_bytes(const tga_query& q, int32_t nv) {
+  const int64_t per_vertex = q.kind == TGA_Q_BFS ? 12 : q.kind == TGA_Q_PAGERANK ? 20 : 40;
+  return per_vertex * (int64_t)nv;
+}
+
+}  // namespace
+
+struct tga_server {
+  int64_t budget = 0;
+  int64_t in_use = 0;
+  std::mutex mu;
+  std::condition_variable work_cv, done_cv;
+  std::vector<std::unique_ptr<GraphSlot>> graphs;
+  std::unordered_map<int64_t, Outcome> outcomes;
+  int64_t next_ticket = 1;
+  bool stopping = false;
+  int64_t submitted = 0, completed = 0, failed = 0, rounds = 0, running = 0;
+  std::vector<double> latencies;
+  bool any_submitted = false;
+  Clock::time_point first_submit, last_done;
+
+  void worker(GraphSlot* slot);
+  void run_round(GraphSlot* slot, std::vector<Pending>& round, std::vector<int>& status);
+};
+
+void tga_server::run_round(GraphSlot* slot, std::vector<Pending>& round, std::vector<int>& status) {
+  const size_t nv = (size_t)slot->nv;
+  status.assign(round.size(), TGA_OK);
+  // BFS: one batched traversal.
+  {
+    std::vector<size_t> idx;
+    std::vector<int32_t> src;
+    std::vector<int64_t> lo, hi;
+    for (size_t i = 0; i < round.size(); ++i)
+      if (round[i].q.kind == TGA_Q_BFS) {
+        idx.push_back(i);
+        src.push_back(round[i].q.src);
+        lo.push_back(round[i].q.t_lo);
+        hi.push_back(round[i].q.t_hi);
+      }
+    if (!idx.empty()) {
+      std::vector<int32_t> out(idx.size() * nv);
+      const int rc = tga_bfs_batch(slot->g, (int32_t)idx.size(), src.data(), lo.data(), hi.data(), out.data());
+      for (size_t k = 0; k < idx.size(); ++k) {
+        status[idx[k]] = rc;
+        if (rc == TGA_OK && round[idx[k]].q.out) std::memcpy(round[idx[k]].q.out, out.data() + k * nv, nv * 4);
+      }
+    }
+  }
+  // PageRank: one strided batch per iteration count.
+  {
+    std::vector<int32_t> iters_seen;
+    for (const Pending& p : round)
+      if (p.q.kind == TGA_Q_PAGERANK) {
+        const int32_t it = p.q.iters > 0 ? p.q.iters : 0;  // 0: the graph's configured count
+        if (std::find(iters_seen.begin(), iters_seen.end(), it) == iters_seen.end()) iters_seen.push_back(it);
+      }
+    for (int32_t it : iters_seen) {
+      std::vector<size_t> idx;
+      std::vector<int64_t> lo, hi;
+      for (size_t i = 0; i < round.size(); ++i) {
+        const tga_query& q = round[i].q;
+        if (q.kind == TGA_Q_PAGERANK && (q.iters > 0 ? q.iters : 0) == it) {
+          idx.push_back(i);
+          lo.push_back(q.t_lo);
+          hi.push_back(q.t_hi);
+        }
+      }
+      std::vector<float> out(idx.size() * nv);
+      const int rc = tga_pagerank_batch(slot->g, (int32_t)idx.size(), it, 0.85f, 0.1f, lo.data(), hi.data(), out.data());
+      for (size_t k = 0; k < idx.size(); ++k) {
+        status[idx[k]] = rc;
+        if (rc == TGA_OK && round[idx[k]].q.out) std::memcpy(round[idx[k]].q.out, out.data() + k * nv, nv * 4);
+      }
+    }
+  }
+  // CC: one traversal per query.
+  for (size_t i = 0; i < round.size(); ++i) {
+    const tga_query& q = round[i].q;
+    if (q.kind != TGA_Q_CC) continue;
+    status[i] = tga_cc(slot->g, q.t_lo, q.t_hi, TGA_CC_EARLY_EXIT, static_cast<int32_t*>(q.out), nullptr);
+  }
+}
+
+void tga_server::worker(GraphSlot* slot) {
+  std::unique_lock<std::mutex> lk(mu);
+  for (;;) {
+    work_cv.wait(lk, [&] { return stopping || !slot->pending.empty(); });
+    if (slot->pending.empty()) {
+      if (stopping) return;
+      continue;
+    }
+    // Admit queued queries while they fit the budget (at least one when nothing else runs).
+    std::vector<Pending> round;
+    while (!slot->pending.empty()) {
+      const Pending& p = slot->pending.front();
+      if (in_use + p.bytes > budget && !(round.empty() && in_use == 0)) break;
+      in_use += p.bytes;
+      round.push_back(p);
+      slot->pending.pop_front();
+    }
+    if (round.empty()) {  // the budget is held by other graphs: wait until some is released
+      work_cv.wait(lk);
+      continue;
+    }
+    ++rounds;
+    running += (int64_t)round.size();
+    lk.unlock();
+    std::vector<int> status;
+    run_round(slot, round, status);
+    const Clock::time_point now = Clock::now();
+    lk.lock();
+    for (size_t i = 0; i < round.size(); ++i) {
+      Outcome& o = outcomes[round[i].ticket];
+      o.status = status[i];
+      o.latency_ms = std::chrono::duration<double, std::milli>(now - round[i].submitted).count();
+      in_use -= round[i].bytes;
+      if (status[i] == TGA_OK) {
+        ++completed;
+        latencies.push_back(o.latency_ms);
+      } else {
+        ++failed;
+      }
+    }
+    running -= (int64_t)round.size();
+    last_done = now;
+    done_cv.notify_all();
+    work_cv.notify_all();
+  }
+}
+
+using tga::fail;
+
+extern "C" {
+
+int tga_server_create(int64_t budget_bytes, tga_server** out) {
+  if (!out || budget_bytes <= 0) return fail(TGA_E_ARG, "tga_server_create: need a positive budget and an output");
+  *out = new tga_server();
+  (*out)->budget = budget_bytes;
+  return TGA_OK;
+}
+
+int tga_server_add_graph(tga_server* s, tga_graph* g, int32_t* graph_id) {
+  if (!s || !g) return fail(TGA_E_ARG, "null server or graph");
+  tga_info info;
+  if (int rc = tga_get_info(g, &info)) return rc;
+  auto slot = std::make_unique<GraphSlot>();
+  slot->g = g;
+  slot->nv = info.max_vertex;
+  std::lock_guard<std::mutex> lk(s->mu);
+  const int32_t id = (int32_t)s->graphs.size();
+  GraphSlot* raw = slot.get();
+  s->graphs.push_back(std::move(slot));
+  raw->worker = std::thread([s, raw] { s->worker(raw); });
+  if (graph_id) *graph_id = id;
+  return TGA_OK;
+}
+
+int tga_submit(tga_server* s, const tga_query* q, int64_t* ticket) {
+  if (!s || !q) return fail(TGA_E_ARG, "null server or query");
+  if (q->kind < TGA_Q_BFS || q->kind > TGA_Q_CC) return fail(TGA_E_ARG, "unknown query kind");
+  if (q->t_lo >= q->t_hi) return fail(TGA_E_ARG, "empty time window");
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (s->stopping) return fail(TGA_E_ARG, "server is stopping");
+  if (q->graph < 0 || q->graph >= (int32_t)s->graphs.size()) return fail(TGA_E_ARG, "unknown graph id");
+  GraphSlot* slot = s->graphs[(size_t)q->graph].get();
+  if (q->kind == TGA_Q_BFS && (q->src < 0 || q->src >= slot->nv)) return fail(TGA_E_ARG, "source out of range");
+  Pending p{*q, s->next_ticket++, query_bytes(*q, slot->nv), Clock::now()};
+  if (p.bytes > s->budget) return fail(TGA_E_OOM, "query needs more device memory than the server's budget");
+  if (!s->any_submitted) {
+    s->any_submitted = true;
+    s->first_submit = p.submitted;
+  }
+  s->outcomes[p.ticket] = Outcome{};
+  slot->pending.push_back(p);
+  ++s->submitted;
+  if (ticket) *ticket = p.ticket;
+  s->work_cv.notify_all();
+  return TGA_OK;
+}
+
+int tga_poll(tga_server* s, int64_t ticket, double* latency_ms) {
+  if (!s) return fail(TGA_E_ARG, "null server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->outcomes.find(ticket);
+  if (it == s->outcomes.end()) return fail(TGA_E_ARG, "unknown ticket");
+  if (latency_ms) *latency_ms = it->second.latency_ms;
+  return it->second.status;
+}
+
+int tga_server_drain(tga_server* s) {
+  if (!s) return fail(TGA_E_ARG, "null server");
+  std::unique_lock<std::mutex> lk(s->mu);
+  s->done_cv.wait(lk, [&] { return s->completed + s->failed == s->submitted; });
+  return TGA_OK;
+}
+
+int tga_server_get_stats(tga_server* s, tga_server_stats* out) {
+  if (!s || !out) return fail(TGA_E_ARG, "null argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  std::memset(out, 0, sizeof *out);
+  out->submitted = s->submitted;
+  out->completed = s->completed;
+  out->failed = s->failed;
+  out->rounds = s->rounds;
+  if (!s->latencies.empty()) {
+    std::vector<double> l = s->latencies;
+    std::sort(l.begin(), l.end());
+    auto pct = [&](double p) { return l[(size_t)std::min<double>((double)l.size() - 1, p * (double)(l.size() - 1) + 0.5)]; };
+    out->p50_ms = pct(0.50);
+    out->p99_ms = pct(0.99);
+    double sum = 0;
+    for (double x : l) sum += x;
+    out->mean_ms = sum / (double)l.size();
+    const double span = std::chrono::duration<double>(s->last_done - s->first_submit).count();
+    out->queries_per_s = span > 0 ? (double)s->completed / span : 0.0;
+  }
+  return TGA_OK;
+}
+
+int tga_server_destroy(tga_server* s) {
+  if (!s) return fail(TGA_E_ARG, "null server");
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stopping = true;
+    s->work_cv.notify_all();
+  }
+  for (auto& g : s->graphs)
+    if (g->worker.joinable()) g->worker.join();
+  delete s;
+  return TGA_OK;
+}
+
+}  // extern "C"

@@ -187,15 +187,64 @@ int tga_color(tga_graph* g, int32_t prio_mode, const uint32_t* prio_in, int32_t 
               uint32_t* prio_out, int32_t* rounds_out);
 
 /* ---- batched form ---------------------------------------------------------------------------
- * Many temporal BFS queries in one traversal: sources are packed 64 per 64-bit word of a
- * bitmask frontier, each with its own window [t_lo[i], t_hi[i]).  arrival_out is nsrc x max_vertex
- * (row i = query i), same semantics as tga_bfs; hops are not produced. */
+ * No counterpart in the reference (one query per executable run).
+ * Many temporal BFS queries in one traversal: up to 256 sources per launch, packed 64 per 64-bit
+ * word of a bitmask frontier, each with its own window [t_lo[i], t_hi[i]); larger batches run as
+ * several launches.  arrival_out is nsrc x max_vertex (row i = query i), same semantics as
+ * tga_bfs; hops are not produced. */
 int tga_bfs_batch(tga_graph* g, int32_t nsrc, const int32_t* src, const int64_t* t_lo, const int64_t* t_hi,
                   int32_t* arrival_out);
 
-/* Many windowed PageRanks as one strided vector (rank_out is nq x max_vertex, row i = query i). */
+/* Many windowed PageRanks as one strided vector: up to 32 queries per launch (more run as several
+ * launches), each list decoded once per iteration; rank_out is nq x max_vertex (row i = query i),
+ * same semantics as tga_pagerank with that window. */
 int tga_pagerank_batch(tga_graph* g, int32_t nq, int32_t iters, float damping, float alpha, const int64_t* t_lo,
                        const int64_t* t_hi, float* rank_out);
+
+/* ---- served form ----------------------------------------------------------------------------
+ * No counterpart in the reference.  A server keeps several opened graphs resident and answers a
+ * stream of queries: one worker thread per graph takes the queries that arrived since its last
+ * round, admits them while their device working memory fits the server's budget, and runs them
+ * together (BFS queries as one batched traversal, PageRank queries with equal iteration counts as
+ * one strided vector, CC one by one); queries that arrive meanwhile join the next round.  Graphs
+ * run on their own streams, so work of different graphs overlaps on the device.  While a graph is
+ * attached to a running server, only the server may use its handle. */
+typedef struct tga_server tga_server;
+
+#define TGA_Q_BFS 0
+#define TGA_Q_PAGERANK 1
+#define TGA_Q_CC 2
+
+typedef struct {
+  int32_t kind;        /* TGA_Q_BFS, TGA_Q_PAGERANK or TGA_Q_CC */
+  int32_t graph;       /* id from tga_server_add_graph */
+  int32_t src;         /* BFS source */
+  int32_t iters;       /* PageRank iterations (<= 0: pr_iters of the graph's configuration) */
+  int64_t t_lo, t_hi;  /* time window */
+  void* out;           /* caller-owned host buffer of max_vertex entries: BFS int32 arrivals, PageRank
+                          float ranks (damping 0.85, alpha 0.1), CC int32 labels; NULL: results dropped */
+} tga_query;
+
+typedef struct {
+  int64_t submitted, completed, failed, rounds;
+  double p50_ms, p99_ms, mean_ms;  /* latency from tga_submit to completion */
+  double queries_per_s;            /* completed / (last completion - first submission) */
+} tga_server_stats;
+
+/* budget_bytes: device working memory that admitted queries may hold at once (BFS about
+ * 12 bytes, PageRank about 20 bytes, CC about 40 bytes per vertex of their graph). */
+int tga_server_create(int64_t budget_bytes, tga_server** out);
+int tga_server_add_graph(tga_server* s, tga_graph* g, int32_t* graph_id);
+/* Queues q; *ticket identifies it.  A query larger than the whole budget fails with TGA_E_OOM. */
+int tga_submit(tga_server* s, const tga_query* q, int64_t* ticket);
+/* TGA_OK when the query finished (its result is in q.out; *latency_ms if not NULL), TGA_E_AGAIN
+ * while it is queued or running, or the query's own error code. */
+int tga_poll(tga_server* s, int64_t ticket, double* latency_ms);
+/* Blocks until every query submitted so far has finished. */
+int tga_server_drain(tga_server* s);
+int tga_server_get_stats(tga_server* s, tga_server_stats* out);
+/* Stops the workers after the queued queries and frees the server (not the graphs). */
+int tga_server_destroy(tga_server* s);
 
 /* ---- format layer (host only, no GPU needed) ----------------------------------------------- */
 
