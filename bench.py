@@ -184,6 +184,108 @@ def cpu_baseline(ddir: Path, summary: dict, threads: int):
                       f"from the compressed streams by the C oracle port ({edges} edges, {dt:.2f}s)"}
 
 
+def random_windows(rng, k, span, lo_frac=0.05, hi_frac=0.5):
+    """Windows of 5-50% of the timestamp span at random positions (the batched/served query mix)."""
+    import numpy as np
+
+    w = rng.uniform(lo_frac, hi_frac, k) * span
+    lo = rng.uniform(0, 1, k) * (span - w)
+    return lo.astype(np.int64), (lo + w).astype(np.int64)
+
+
+def batched_section(tga, g, n, span):
+    """256 windowed BFS sources as one batched traversal and 32 windowed PageRanks (20 iterations)
+    as one strided vector, against the same queries one call each.  Results stay on the device
+    (NULL outputs) on both sides, so the comparison is the device work of the two forms."""
+    import ctypes as C
+
+    import numpy as np
+
+    L = tga.lib()
+    rng = np.random.default_rng(3)
+    src = rng.integers(0, n, 256).astype(np.int32)
+    blo, bhi = random_windows(rng, 256, span)
+    plo, phi = random_windows(rng, 32, span)
+    d, a = C.c_float(0.85), C.c_float(0.1)
+    _check = tga._check
+    _check(L.tga_bfs_batch(g.handle, 16, src.ctypes.data, blo.ctypes.data, bhi.ctypes.data, None))  # warm-up
+    _check(L.tga_bfs_batch(g.handle, 256, src.ctypes.data, blo.ctypes.data, bhi.ctypes.data, None))
+    bfs_batch_ms = g.timing()["total_ms"]
+    _check(L.tga_pagerank_batch(g.handle, 32, 20, d, a, plo.ctypes.data, phi.ctypes.data, None))
+    pr_batch_ms = g.timing()["total_ms"]
+    bfs_plain_ms = pr_plain_ms = 0.0
+    for i in range(256):
+        _check(L.tga_bfs(g.handle, int(src[i]), int(blo[i]), int(bhi[i]), None, None))
+        bfs_plain_ms += g.timing()["total_ms"]
+    for i in range(32):
+        _check(L.tga_pagerank(g.handle, 20, d, a, int(plo[i]), int(phi[i]), None))
+        pr_plain_ms += g.timing()["total_ms"]
+    qs = 256 + 32
+    return {"workload": "256 BFS (random sources, windows 5-50% of span) + 32 windowed PageRank x20 on the "
+                        "2M/40M graph",
+            "queries_per_s": qs / ((bfs_batch_ms + pr_batch_ms) / 1e3),
+            "plain_queries_per_s": qs / ((bfs_plain_ms + pr_plain_ms) / 1e3),
+            "bfs_batch_ms": bfs_batch_ms, "bfs_plain_ms": bfs_plain_ms, "pr_batch_ms": pr_batch_ms,
+            "pr_plain_ms": pr_plain_ms, "timing": "device time (CUDA events), results left on the device"}
+
+
+def served_section(tga, graphs, spans, rate, count):
+    """Open-loop Poisson arrivals at `rate` queries/s over the resident graphs: 60% BFS, 25% PageRank
+    (10-50 iterations), 15% CC, random windows.  The same arrival sequence is replayed serially, one
+    query per call (each query starts when it has arrived and the previous one finished)."""
+    import numpy as np
+
+    rng = np.random.default_rng(4)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, count))
+    queries = []
+    for i in range(count):
+        gi = int(rng.integers(0, len(graphs)))
+        lo, hi = random_windows(rng, 1, spans[gi])
+        r = rng.random()
+        if r < 0.6:
+            queries.append(dict(kind=tga.Q_BFS, graph=gi, src=int(rng.integers(0, graphs[gi].max_vertex)),
+                                t_lo=int(lo[0]), t_hi=int(hi[0])))
+        elif r < 0.85:
+            queries.append(dict(kind=tga.Q_PAGERANK, graph=gi, iters=int(rng.integers(10, 51)), t_lo=int(lo[0]),
+                                t_hi=int(hi[0])))
+        else:
+            queries.append(dict(kind=tga.Q_CC, graph=gi, t_lo=int(lo[0]), t_hi=int(hi[0])))
+    with tga.Server(budget_bytes=120 << 30) as srv:
+        for g in graphs:
+            srv.add_graph(g)
+        t0 = time.perf_counter()
+        for q, at in zip(queries, arrivals):
+            wait = at - (time.perf_counter() - t0)
+            if wait > 0:
+                time.sleep(wait)
+            srv.submit(**q)
+        srv.drain()
+        st = srv.stats()
+    # Serial replay: service times of single calls, queued behind each other in arrival order.
+    service = []
+    for q in queries:
+        g = graphs[q["graph"]]
+        t = time.perf_counter()
+        if q["kind"] == tga.Q_BFS:
+            g.bfs(q["src"], q["t_lo"], q["t_hi"])
+        elif q["kind"] == tga.Q_PAGERANK:
+            g.pagerank(q["iters"], 0.85, 0.1, q["t_lo"], q["t_hi"])
+        else:
+            g.connected_components(q["t_lo"], q["t_hi"])
+        service.append(time.perf_counter() - t)
+    finish, lat = 0.0, []
+    for at, sv in zip(arrivals, service):
+        finish = max(finish, at) + sv
+        lat.append((finish - at) * 1e3)
+    lat = np.sort(np.array(lat))
+    return {"workload": f"open-loop Poisson {rate} queries/s, {count} queries over graphs of "
+                        f"{[gg.max_vertex for gg in graphs]} vertices; 60% BFS, 25% PageRank x10-50, 15% CC; "
+                        "windows 5-50% of span; results to host buffers",
+            "queries_per_s": st["queries_per_s"], "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+            "rounds": st["rounds"], "serial_queries_per_s": count / finish,
+            "serial_p50_ms": float(lat[len(lat) // 2]), "serial_p99_ms": float(lat[int(0.99 * (len(lat) - 1))])}
+
+
 def run_reference(args):
     rank, local, world = dist_env()
     if rank != 0:
@@ -224,6 +326,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip the batched and served measurements")
+    ap.add_argument("--served-rate", type=float, default=200.0)
+    ap.add_argument("--served-count", type=int, default=400)
     ap.add_argument("--only", choices=["RA", "BFS", "CC", "PR", "HITS", "DC", "GC"],
                     help="run one workload per step (for profiling; the line is not the benchmark)")
     args = ap.parse_args()
@@ -328,6 +433,22 @@ def main():
         "gpu_launches": launches,
         "workloads": breakdown,
     }
+    if rank == 0 and not args.no_forms and not ONLY:
+        try:
+            line["batched"] = batched_section(tga, g, n, int(tga.CONFIGS[CONFIG_NAME].ts_span))
+            extra = []
+            for name in ("small", "served1m"):
+                dd = Path(tempfile.gettempdir()) / f"tga_bench_{name}"
+                if not (dd / f"{name}.graph").exists():
+                    tga.generate(tga.CONFIGS[name], dd, name)
+                nn = tga.CONFIGS[name].n
+                extra.append(tga.Graph.open_dir(dd, name, tga.DatasetConfig(name=name, max_label=nn - 1, max_vertex=nn)))
+            spans = [int(tga.CONFIGS[nm].ts_span) for nm in ("small", "served1m", CONFIG_NAME)]
+            line["served"] = served_section(tga, extra + [g], spans, args.served_rate, args.served_count)
+            for gg in extra:
+                gg.close()
+        except Exception as e:  # reported, not fatal
+            line["served_error"] = str(e)
     if rank == 0 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(ddir, summary, 0)

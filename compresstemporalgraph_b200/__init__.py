@@ -26,6 +26,7 @@ TGA_UNSET_TS = -(1 << 63)
 T_MAX = (1 << 63) - 1
 HITS_GPU, HITS_JAVA = 0, 1
 CC_EARLY_EXIT = 1
+CC_ONE_SEED = 2
 GC_JAVA_ISOLATED = 1
 UINT32_INF = 0xFFFFFFFF
 INT32_INF = 0x7FFFFFFF
@@ -291,10 +292,14 @@ class Graph:
         _check(_lib.tga_bfs(self._h, src, t_lo, t_hi, _ptr(arr), _ptr(hops)))
         return arr, hops
 
-    def connected_components(self, t_lo: int = 0, t_hi: int = T_MAX, early_exit: bool = True, outputs: bool = True):
+    def connected_components(self, t_lo: int = 0, t_hi: int = T_MAX, early_exit: bool = True, outputs: bool = True,
+                             one_seed: bool = False):
+        """Labels by temporal reach (tga_cc).  Seeds run as validated batches of a multi-source
+        traversal; one_seed=True runs one seed per traversal (same labels)."""
         comps = C.c_int32()
         lab = np.zeros(self.max_vertex, np.int32) if outputs else None
-        _check(_lib.tga_cc(self._h, t_lo, t_hi, CC_EARLY_EXIT if early_exit else 0, _ptr(lab), C.byref(comps)))
+        flags = (CC_EARLY_EXIT if early_exit else 0) | (CC_ONE_SEED if one_seed else 0)
+        _check(_lib.tga_cc(self._h, t_lo, t_hi, flags, _ptr(lab), C.byref(comps)))
         return lab, comps.value
 
     def pagerank(self, iters: int = 0, damping: float = 0.85, alpha: float = 0.1, t_lo: int = 0, t_hi: int = T_MAX,
@@ -431,6 +436,10 @@ CONFIGS = {
     "batched": GenParams(n=20_000_000, m=500_000_000, deg_exponent=1.9, max_degree=1_000_000, repeat_frac=0.30,
                          local_frac=0.70, local_radius=64, pref_frac=0.5, copy_frac=0.20, ts_kind=1,
                          ts_span=100_000_000, seed=3),
+    # Served-form resident graph of 1M vertices / 20M temporal edges (same generator).
+    "served1m": GenParams(n=1_000_000, m=20_000_000, deg_exponent=2.0, max_degree=50_000, repeat_frac=0.30,
+                          local_frac=0.70, local_radius=64, pref_frac=0.5, copy_frac=0.20, ts_kind=1,
+                          ts_span=100_000_000, seed=4),
     "skew": GenParams(n=100_000_000, m=2_000_000_000, deg_exponent=1.6, max_degree=5_000_000, repeat_frac=0.30,
                       local_frac=0.70, local_radius=64, pref_frac=0.5, copy_frac=0.20, ts_kind=2,
                       ts_span=100_000_000, seed=5),

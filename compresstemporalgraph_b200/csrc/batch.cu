@@ -36,6 +36,10 @@ struct MultiArgs {
   const int64_t* lo;         // [nsrc] windows [lo, hi)
   const int64_t* hi;
   const int32_t* run_first;  // [nruns][kMaxSources] list index of a cut run's first in-window edge
+  uint32_t* stamp;           // [nv] epoch of the traversal that last touched the vertex
+  int32_t* touched;          // vertices touched by this traversal (arrival set for some source)
+  int32_t* ntouched;
+  uint32_t epoch;
   int32_t nsrc, nv;
   int32_t dense_min, level_cap;
   unsigned long long* edges;
@@ -169,10 +173,18 @@ __device__ __forceinline__ void multi_scan(MultiArgs& a, const int32_t* cq, int 
       }
     }
     int at = warp_reserve(ncnt, n);
+    uint32_t fresh = 0;  // kept vertices this traversal has not touched before
     for (uint32_t b = keep_bits; b; b &= b - 1) {
       const int v = i * 32 + __ffs(b) - 1;
       write_entries(a.w, v, nq, at);
       at += entry_count(a.w, v);
+      if (__ldcg(&a.stamp[v]) != a.epoch) fresh |= b & (~b + 1);
+    }
+    int tat = warp_reserve(a.ntouched, __popc(fresh));
+    for (uint32_t b = fresh; b; b &= b - 1) {
+      const int v = i * 32 + __ffs(b) - 1;
+      a.stamp[v] = a.epoch;
+      a.touched[tat++] = v;
     }
   }
 }
@@ -223,6 +235,7 @@ __global__ void k_bfs_multi_seed(MultiArgs a, const int32_t* src, int32_t n) {
   const int v = src[s];
   const int64_t start = a.lo[s] > 0 ? a.lo[s] : 0;
   a.arr[(size_t)s * a.nv + v] = (uint32_t)start;
+  if (atomicExch(&a.stamp[v], a.epoch) != a.epoch) a.touched[atomicAdd(a.ntouched, 1)] = v;
   if (v < n) {
     atomicOr((unsigned long long*)(a.F[1] + (size_t)v * kWords + s / 64), (unsigned long long)(1ull << (s & 63)));
     atomicOr(&a.dirty[v >> 5], 1u << (v & 31));
@@ -260,6 +273,19 @@ __global__ void TGA_DECODE_BOUNDS k_run_first_multi(GraphView g, const SliceStat
   }
 }
 
+// Back to "unreached" for every source at every vertex the traversal touched (all the entries it
+// can have set), so the next traversal starts without clearing the whole [sources][vertices] state.
+__global__ void k_multi_reset(uint32_t* arr, uint32_t* prev, int32_t nv, const int32_t* touched,
+                              const int32_t* ntouched, int32_t nsrc) {
+  const int64_t total = (int64_t)(*ntouched) * nsrc;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int u = touched[i / nsrc];
+    const size_t at = (size_t)(i % nsrc) * nv + u;
+    arr[at] = kNoArrival;
+    prev[at] = kNoArrival;
+  }
+}
+
 __global__ void k_multi_unpack(const uint32_t* arr, int32_t* out, int64_t total) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < total) {
@@ -268,71 +294,109 @@ __global__ void k_multi_unpack(const uint32_t* arr, int32_t* out, int64_t total)
   }
 }
 
-// One batch of at most kMaxSources sources: arrivals to arrival_out (nsrc x max_vertex, host).
-static int bfs_multi_batch(GraphHandle& h, int32_t nsrc, const int32_t* src, const int64_t* t_lo, const int64_t* t_hi,
-                           int32_t* arrival_out) {
+// Scratch of a multi-source traversal of up to `cap` sources: the persistent state (m_*) and, in
+// s_d, the windows, sources and per-source run table.  Growing the state (capacity rounded up to
+// a power of two, at least 32) clears it; so does a traversal that ended early (m_clean false).
+static int multi_buffers(GraphHandle& h, int32_t cap) {
   const size_t nv = (size_t)h.view.max_vertex;
   const size_t qcap = nv + (size_t)h.nslices + 1;
-  const size_t ndirty = (nv + 31) / 32;
-  const size_t state = (size_t)nsrc * nv * 4;
-  // s_a: arr | prev; s_b: F[0] | F[1]; s_c: dirty; s_q0/s_q1 queues; s_d: windows, sources and run table;
-  // s_e: int32 output
-  TGA_TRY(h.s_a.ensure(2 * state));
-  TGA_TRY(h.s_b.ensure(2 * nv * kWords * 8));
-  TGA_TRY(h.s_c.ensure(ndirty * 4));
-  TGA_TRY(h.s_q0.ensure(qcap * 4));
-  TGA_TRY(h.s_q1.ensure(qcap * 4));
-  TGA_TRY(h.s_cnt.ensure(sizeof(TravCtl)));
+  int rc;
   const size_t run_bytes = (size_t)std::max(h.nruns, 1) * kMaxSources * 4;
-  TGA_TRY(h.s_d.ensure(kMaxSources * 20 + run_bytes));
-  TGA_TRY(h.s_e.ensure(state));
-  TGA_TRY(h.begin_call());
-  unsigned long long* edges = edge_counter(h);
-  MultiArgs a{};
+  if ((rc = h.s_q0.ensure(qcap * 4)) || (rc = h.s_q1.ensure(qcap * 4)) || (rc = h.s_cnt.ensure(sizeof(TravCtl))) ||
+      (rc = h.s_d.ensure(kMaxSources * 20 + run_bytes)))
+    return rc;
+  if (cap > h.m_cap || !h.m_clean) {
+    int32_t c = std::max(h.m_cap, 32);
+    while (c < cap) c *= 2;
+    c = std::min(c, kMaxSources);
+    h.m_clean = false;
+    if ((rc = h.m_state.ensure(2 * (size_t)c * nv * 4)) || (rc = h.m_mask.ensure(2 * nv * kWords * 8)) ||
+        (rc = h.m_dirty.ensure(((nv + 31) / 32) * 4)) || (rc = h.m_stamp.ensure(nv * 4)) ||
+        (rc = h.m_touched.ensure((nv + 1) * 4)))
+      return rc;
+    TGA_CUDA_TRY(cudaMemsetAsync(h.m_state.p, 0xFF, 2 * (size_t)c * nv * 4, h.stream));
+    TGA_CUDA_TRY(cudaMemsetAsync(h.m_mask.p, 0, 2 * nv * kWords * 8, h.stream));
+    TGA_CUDA_TRY(cudaMemsetAsync(h.m_dirty.p, 0, ((nv + 31) / 32) * 4, h.stream));
+    TGA_CUDA_TRY(cudaMemsetAsync(h.m_stamp.p, 0, nv * 4, h.stream));
+    TGA_CUDA_TRY(cudaMemsetAsync(h.m_touched.as<int32_t>() + nv, 0, 4, h.stream));
+    h.m_cap = c;
+    h.m_pending = 0;
+    h.m_epoch = 0;
+    h.m_clean = true;
+  }
+  return TGA_OK;
+}
+
+static int64_t* multi_lo(GraphHandle& h) { return h.s_d.as<int64_t>(); }
+static int64_t* multi_hi(GraphHandle& h) { return h.s_d.as<int64_t>() + kMaxSources; }
+static int32_t* multi_src(GraphHandle& h) { return reinterpret_cast<int32_t*>(h.s_d.as<int64_t>() + 2 * kMaxSources); }
+static int32_t* multi_run_table(GraphHandle& h) { return multi_src(h) + kMaxSources; }
+
+// Per-source run table of the windows in multi_lo/multi_hi (sources 0..nsrc-1).
+static int multi_runs(GraphHandle& h, int32_t nsrc) {
+  if (h.nruns <= 0) return TGA_OK;
+  int32_t* drf = multi_run_table(h);
+  KL(k_fill_i32, grid_for((int64_t)h.nruns * kMaxSources, kBlock))(drf, INT32_MAX, (int64_t)h.nruns * kMaxSources);
+  KL(k_run_first_multi, grid_for(h.nrun_pairs, kBlock))(h.view, h.d_slices.as<SliceState>(), h.d_runs.as<RunInfo>(),
+                                                       h.d_run_pairs.as<int2>(), h.nrun_pairs, multi_lo(h),
+                                                       multi_hi(h), nsrc, drf);
+  return TGA_OK;
+}
+
+// Runs one multi-source traversal of nsrc sources whose vertices and windows are already in
+// multi_src/multi_lo/multi_hi and whose run table is built (multi_runs); multi_buffers(h, >= nsrc)
+// must have run.  Leaves the arrivals in a.arr ([nsrc][max_vertex], kNoArrival: unreached) and the
+// vertices with any finite arrival on a.touched (count in *a.ntouched) until the next call.
+// *levels gets the levels run.
+static int multi_run(GraphHandle& h, int32_t nsrc, unsigned long long* edges, MultiArgs& a, int32_t* levels) {
+  const size_t nv = (size_t)h.view.max_vertex;
+  if (nsrc > h.m_cap || !h.m_clean) return fail(TGA_E_ARG, "multi-source state not prepared");
+  a = MultiArgs{};
   a.w = Work{h.d_items.as<WorkItem>(), h.d_slices.as<SliceState>(), h.d_slice_first.as<int32_t>(), nullptr, h.nitems,
              h.d_order.as<int32_t>(), h.norder, nullptr};
   a.ctl = h.s_cnt.as<TravCtl>();
   a.q[0] = h.s_q0.as<int32_t>();
   a.q[1] = h.s_q1.as<int32_t>();
-  a.arr = h.s_a.as<uint32_t>();
-  a.prev = a.arr + (size_t)nsrc * nv;
-  a.F[0] = h.s_b.as<uint64_t>();
+  a.arr = h.m_state.as<uint32_t>();
+  a.prev = a.arr + (size_t)h.m_cap * nv;
+  a.F[0] = h.m_mask.as<uint64_t>();
   a.F[1] = a.F[0] + nv * kWords;
-  a.dirty = h.s_c.as<uint32_t>();
-  a.ndirty = (int32_t)ndirty;
-  int64_t* dlo = h.s_d.as<int64_t>();
-  int64_t* dhi = dlo + kMaxSources;
-  int32_t* dsrc = reinterpret_cast<int32_t*>(dhi + kMaxSources);
-  int32_t* drf = dsrc + kMaxSources;
-  a.lo = dlo;
-  a.hi = dhi;
-  a.run_first = drf;
+  a.dirty = h.m_dirty.as<uint32_t>();
+  a.ndirty = (int32_t)((nv + 31) / 32);
+  a.lo = multi_lo(h);
+  a.hi = multi_hi(h);
+  a.run_first = multi_run_table(h);
+  a.stamp = h.m_stamp.as<uint32_t>();
+  a.touched = h.m_touched.as<int32_t>();
+  a.ntouched = a.touched + nv;  // the count follows the list; it outlives the shared control block
   a.nsrc = nsrc;
   a.nv = (int32_t)nv;
   a.dense_min = std::max<int32_t>(h.dense_min, 1);
   a.level_cap = 1 << 20;
   a.edges = edges;
-  TGA_CUDA_TRY(cudaMemcpyAsync(dlo, t_lo, (size_t)nsrc * 8, cudaMemcpyHostToDevice, h.stream));
-  TGA_CUDA_TRY(cudaMemcpyAsync(dhi, t_hi, (size_t)nsrc * 8, cudaMemcpyHostToDevice, h.stream));
-  TGA_CUDA_TRY(cudaMemcpyAsync(dsrc, src, (size_t)nsrc * 4, cudaMemcpyHostToDevice, h.stream));
-  TGA_CUDA_TRY(cudaMemsetAsync(a.arr, 0xFF, 2 * state, h.stream));
-  TGA_CUDA_TRY(cudaMemsetAsync(a.F[0], 0, 2 * nv * kWords * 8, h.stream));
-  TGA_CUDA_TRY(cudaMemsetAsync(a.dirty, 0, ndirty * 4, h.stream));
+  // The previous traversal's entries back to "unreached", then an empty touched list.
+  if (h.m_pending > 0) {
+    KL(k_multi_reset, 4 * h.sm_count)(a.arr, a.prev, a.nv, a.touched, a.ntouched, h.m_pending);
+    h.m_pending = 0;
+  }
+  TGA_CUDA_TRY(cudaMemsetAsync(a.ntouched, 0, 4, h.stream));
+  if (++h.m_epoch == 0) {  // stamps wrapped: clear them
+    TGA_CUDA_TRY(cudaMemsetAsync(a.stamp, 0, nv * 4, h.stream));
+    h.m_epoch = 1;
+  }
+  a.epoch = h.m_epoch;
   TravCtl ctl{};
   std::memcpy(h.h_pinned + 32, &ctl, sizeof ctl);
   TGA_CUDA_TRY(cudaMemcpyAsync(a.ctl, h.h_pinned + 32, sizeof ctl, cudaMemcpyHostToDevice, h.stream));
-  if (h.nruns > 0) {
-    KL(k_fill_i32, grid_for((int64_t)h.nruns * kMaxSources, kBlock))(drf, INT32_MAX, (int64_t)h.nruns * kMaxSources);
-    KL(k_run_first_multi, grid_for(h.nrun_pairs, kBlock))(h.view, h.d_slices.as<SliceState>(), h.d_runs.as<RunInfo>(),
-                                                         h.d_run_pairs.as<int2>(), h.nrun_pairs, dlo, dhi, nsrc, drf);
-  }
-  KL(k_bfs_multi_seed, grid_for(nsrc, kBlock))(a, dsrc, h.view.n);
+  KL(k_bfs_multi_seed, grid_for(nsrc, kBlock))(a, multi_src(h), h.view.n);
   int per_sm = 0;
   TGA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bfs_multi, kBlock, 0));
   if (per_sm < 1) return fail(TGA_E_CUDA, "batched traversal kernel cannot be resident");
   void* args[] = {&h.view, &a};
   cudaEvent_t* ev = h.kernel_begin();
   ++h.timing.launches;
+  h.m_pending = nsrc;
+  h.m_clean = false;  // until the traversal is known to have finished
   TGA_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_bfs_multi, dim3(per_sm * h.sm_count), dim3(kBlock), args, 0,
                                            h.stream));
   h.kernel_end(ev);
@@ -340,10 +404,221 @@ static int bfs_multi_batch(GraphHandle& h, int32_t nsrc, const int32_t* src, con
   TGA_CUDA_TRY(cudaStreamSynchronize(h.stream));
   std::memcpy(&ctl, h.h_pinned + 32, sizeof ctl);
   if (ctl.status) return fail(TGA_E_TIMEOUT, "a grid barrier wait ran out");
+  h.m_clean = true;
+  *levels = ctl.levels;
+  return TGA_OK;
+}
+
+// One batch of at most kMaxSources sources: arrivals to arrival_out (nsrc x max_vertex, host).
+static int bfs_multi_batch(GraphHandle& h, int32_t nsrc, const int32_t* src, const int64_t* t_lo, const int64_t* t_hi,
+                           int32_t* arrival_out) {
+  const size_t nv = (size_t)h.view.max_vertex;
+  const size_t state = (size_t)nsrc * nv * 4;
+  TGA_TRY(multi_buffers(h, nsrc));
+  TGA_TRY(h.s_e.ensure(state));
+  TGA_TRY(h.begin_call());
+  unsigned long long* edges = edge_counter(h);
+  TGA_CUDA_TRY(cudaMemcpyAsync(multi_lo(h), t_lo, (size_t)nsrc * 8, cudaMemcpyHostToDevice, h.stream));
+  TGA_CUDA_TRY(cudaMemcpyAsync(multi_hi(h), t_hi, (size_t)nsrc * 8, cudaMemcpyHostToDevice, h.stream));
+  TGA_CUDA_TRY(cudaMemcpyAsync(multi_src(h), src, (size_t)nsrc * 4, cudaMemcpyHostToDevice, h.stream));
+  TGA_TRY(multi_runs(h, nsrc));
+  MultiArgs a;
+  int32_t levels = 0;
+  TGA_TRY(multi_run(h, nsrc, edges, a, &levels));
   int32_t* out = h.s_e.as<int32_t>();
   KL(k_multi_unpack, grid_for((int64_t)nsrc * (int64_t)nv, kBlock))(a.arr, out, (int64_t)nsrc * (int64_t)nv);
   if (arrival_out) TGA_CUDA_TRY(cudaMemcpyAsync(arrival_out, out, state, cudaMemcpyDeviceToHost, h.stream));
-  h.timing.iterations = ctl.levels;
+  h.timing.iterations = levels;
+  return finish(h, edges);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Connected components with seeds run as speculative batches.  The seed loop (traverse.cu,
+// k_cc) takes the smallest unreached vertex with outdegree > 9 as the next seed and labels its
+// temporal reach.  Here the next K such vertices become the sources of one multi-source traversal
+// (each with its own fresh arrivals, as the sequential loop has); then, in seed order, a candidate
+// is a real seed iff no earlier real seed of the batch reached it, the early-exit rules run on the
+// exact reach counts, and every vertex takes the component number of the last real seed that
+// reached it.  The labels equal the sequential loop's; K doubles while all candidates of a batch
+// turn out to be real seeds and halves otherwise.
+
+struct CcBatchState {
+  int64_t total;       // reach counts so far (early-exit rule)
+  int32_t v;           // candidates start here
+  int32_t comp;        // components so far
+  int32_t small_run;   // consecutive components smaller than 5
+  int32_t stop;        // the seed loop has ended
+  int32_t ncand;       // candidates of the current batch
+  int32_t nvalid, ninvalid;
+  int32_t pad;
+};
+
+// The first K vertices >= v below end that are unreached and have outdegree > 9, in order.
+__global__ void k_cc_candidates(const uint8_t* reached, const int32_t* deg, CcBatchState* st, int32_t end, int32_t K,
+                                int32_t* cand) {
+  __shared__ int wcount[32];
+  __shared__ int count;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (threadIdx.x == 0) count = 0;
+  __syncthreads();
+  if (!st->stop) {
+    for (int64_t base = st->v; base < end; base += blockDim.x) {
+      const int64_t u = base + threadIdx.x;
+      const bool f = u < end && !reached[u] && deg[u] > 9;
+      const unsigned ballot = __ballot_sync(0xffffffffu, f);
+      if (lane == 0) wcount[wid] = __popc(ballot);
+      __syncthreads();
+      int before = 0, total = 0;
+      for (int k = 0; k < nw; ++k) {
+        if (k < wid) before += wcount[k];
+        total += wcount[k];
+      }
+      const int pos = count + before + __popc(ballot & ((1u << lane) - 1));
+      if (f && pos < K) cand[pos] = (int32_t)u;
+      __syncthreads();
+      if (threadIdx.x == 0) count += total;
+      __syncthreads();
+      if (count >= K) break;
+    }
+  }
+  if (threadIdx.x == 0) st->ncand = min(count, K);
+}
+
+// Finite arrivals per source (its reach plus the seed itself), over the touched vertices.
+__global__ void k_multi_count(const uint32_t* arr, int32_t nv, const int32_t* touched, const int32_t* ntouched,
+                              unsigned long long* counts) {
+  const int s = blockIdx.y;
+  const int nt = *ntouched;
+  unsigned long long c = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nt; i += gridDim.x * blockDim.x)
+    c += arr[(size_t)s * nv + touched[i]] != kNoArrival;
+  for (int o = 16; o; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(&counts[s], c);
+}
+
+// Candidates in seed order: real seeds, component numbers, reach counts and the early exits.
+__global__ void k_cc_validate(CcBatchState* st, const int32_t* cand, const uint32_t* arr, int32_t nv,
+                              const unsigned long long* counts, int32_t* comp_of, int32_t early, int64_t limit) {
+  __shared__ uint32_t reaches[kMaxSources][kMaxSources / 32];  // bit i of row j: candidate i reached j
+  const int n = st->ncand;
+  for (int e = threadIdx.x; e < kMaxSources * (kMaxSources / 32); e += blockDim.x) (&reaches[0][0])[e] = 0;
+  __syncthreads();
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    const int j = e / n, i = e % n;
+    if (i < j && arr[(size_t)i * nv + cand[j]] != kNoArrival) atomicOr(&reaches[j][i >> 5], 1u << (i & 31));
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  uint32_t real[kMaxSources / 32] = {};
+  int nvalid = 0, ninvalid = 0;
+  for (int j = 0; j < n; ++j) {
+    comp_of[j] = -1;
+    bool reached = false;
+    for (int k = 0; k < kMaxSources / 32; ++k) reached |= (reaches[j][k] & real[k]) != 0;
+    if (reached) {
+      ++ninvalid;
+      continue;
+    }
+    if (early && st->total > limit) {
+      st->stop = 1;
+      break;
+    }
+    real[j >> 5] |= 1u << (j & 31);
+    ++nvalid;
+    const int64_t reach = (int64_t)counts[j] - 1;  // the seed's own arrival is set before its traversal
+    comp_of[j] = st->comp++;
+    st->total += reach + 1;
+    st->small_run = (reach + 1 < 5) ? st->small_run + 1 : 0;
+    st->v = cand[j] + 1;
+    if (early && st->small_run > 50) {
+      st->stop = 1;
+      break;
+    }
+  }
+  for (int j = nvalid + ninvalid; j < n; ++j) comp_of[j] = -1;
+  if (!st->stop && n > 0) st->v = cand[n - 1] + 1;
+  st->nvalid = nvalid;
+  st->ninvalid = ninvalid;
+}
+
+// Every touched vertex takes the component of the last real seed of the batch that reached it.
+__global__ void k_cc_label_multi(const uint32_t* arr, int32_t nv, const int32_t* touched, const int32_t* ntouched,
+                                 const int32_t* comp_of, int32_t n, int32_t* label, uint8_t* reached) {
+  const int nt = *ntouched;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nt; i += gridDim.x * blockDim.x) {
+    const int u = touched[i];
+    for (int j = n - 1; j >= 0; --j) {
+      const int c = comp_of[j];
+      if (c >= 0 && arr[(size_t)j * nv + u] != kNoArrival) {
+        label[u] = c;
+        reached[u] = 1;
+        break;
+      }
+    }
+  }
+}
+
+__global__ void k_fill_windows(int64_t* lo, int64_t* hi, int64_t t_lo, int64_t t_hi) {
+  lo[threadIdx.x] = t_lo;
+  hi[threadIdx.x] = t_hi;
+}
+
+static int cc_batched(GraphHandle& h, int64_t t_lo, int64_t t_hi, int32_t flags, int32_t* label_out,
+                      int32_t* components_out) {
+  const int32_t nv = h.view.max_vertex;
+  TGA_TRY(multi_buffers(h, kMaxSources));
+  TGA_TRY(h.s_e.ensure((size_t)nv * 4 + (size_t)nv));                       // labels | reached
+  TGA_TRY(h.s_f.ensure(sizeof(CcBatchState) + kMaxSources * (8 + 4)));      // state | counts | comp_of
+  TGA_TRY(h.begin_call());
+  unsigned long long* edges = edge_counter(h);
+  int32_t* label = h.s_e.as<int32_t>();
+  uint8_t* reached = reinterpret_cast<uint8_t*>(label + nv);
+  CcBatchState* st = h.s_f.as<CcBatchState>();
+  unsigned long long* counts = reinterpret_cast<unsigned long long*>(h.s_f.as<char>() + sizeof(CcBatchState));
+  int32_t* comp_of = reinterpret_cast<int32_t*>(counts + kMaxSources);
+  KL(k_fill_i32, grid_for(nv, kBlock))(label, -1, nv);
+  TGA_CUDA_TRY(cudaMemsetAsync(reached, 0, (size_t)nv, h.stream));
+  CcBatchState init{};
+  init.v = std::max(h.cfg.cc_vertex_begin, 0);
+  std::memcpy(h.h_pinned + 64, &init, sizeof init);
+  TGA_CUDA_TRY(cudaMemcpyAsync(st, h.h_pinned + 64, sizeof init, cudaMemcpyHostToDevice, h.stream));
+  k_fill_windows<<<1, kMaxSources, 0, h.stream>>>(multi_lo(h), multi_hi(h), t_lo, t_hi);
+  ++h.timing.launches;
+  TGA_TRY(multi_runs(h, kMaxSources));  // one table serves every batch: all windows are the same
+  const int32_t end = std::min(std::min(h.view.max_label, nv), h.view.n);
+  const int64_t limit = (int64_t)(0.8 * h.view.max_label);
+  const int32_t early = (flags & TGA_CC_EARLY_EXIT) ? 1 : 0;
+  int32_t K = 4, levels = 0;
+  for (int batch = 0;; ++batch) {
+    if (batch > (1 << 22)) return fail(TGA_E_TIMEOUT, "CC batch cap reached");
+    k_cc_candidates<<<1, 1024, 0, h.stream>>>(reached, h.d_deg.as<int32_t>(), st, end, K, multi_src(h));
+    ++h.timing.launches;
+    TGA_CUDA_TRY(cudaMemcpyAsync(h.h_pinned + 64, st, sizeof(CcBatchState), cudaMemcpyDeviceToHost, h.stream));
+    TGA_CUDA_TRY(cudaStreamSynchronize(h.stream));
+    CcBatchState cur;
+    std::memcpy(&cur, h.h_pinned + 64, sizeof cur);
+    if (batch > 0) K = cur.ninvalid == 0 ? std::min(2 * K, kMaxSources) : std::max(4, K / 2);
+    if (cur.stop || cur.ncand == 0) break;
+    const int32_t n = cur.ncand;
+    MultiArgs a;
+    int32_t lv = 0;
+    TGA_TRY(multi_run(h, n, edges, a, &lv));
+    levels += lv;
+    TGA_CUDA_TRY(cudaMemsetAsync(counts, 0, kMaxSources * 8, h.stream));
+    KL(k_multi_count, dim3(std::max(1u, std::min(64u, grid_for(nv, kBlock))), n))(a.arr, nv, a.touched, a.ntouched,
+                                                                                    counts);
+    k_cc_validate<<<1, 1024, 0, h.stream>>>(st, multi_src(h), a.arr, nv, counts, comp_of, early, limit);
+    ++h.timing.launches;
+    KL(k_cc_label_multi, std::min(grid_for(nv, kBlock), 8u * h.sm_count))(a.arr, nv, a.touched, a.ntouched, comp_of, n,
+                                                                           label, reached);
+  }
+  CcBatchState fin;
+  TGA_CUDA_TRY(cudaMemcpyAsync(h.h_pinned + 64, st, sizeof fin, cudaMemcpyDeviceToHost, h.stream));
+  TGA_CUDA_TRY(cudaStreamSynchronize(h.stream));
+  std::memcpy(&fin, h.h_pinned + 64, sizeof fin);
+  if (label_out) TGA_CUDA_TRY(cudaMemcpyAsync(label_out, label, (size_t)nv * 4, cudaMemcpyDeviceToHost, h.stream));
+  if (components_out) *components_out = fin.comp;
+  h.timing.iterations = levels;
   return finish(h, edges);
 }
 
@@ -573,6 +848,11 @@ static int pagerank_multi_batch(GraphHandle& h, int32_t nq, int32_t iters, float
   h.timing.compressed_bytes = (uint64_t)(iters + (windowed ? 1 : 0)) *
                               (h.info.graph_bytes + h.info.timestamp_bytes + h.info.index_bytes);
   return rc;
+}
+
+int cc_seed_batches(GraphHandle& h, int64_t t_lo, int64_t t_hi, int32_t flags, int32_t* label_out,
+                    int32_t* components_out) {
+  return cc_batched(h, t_lo, t_hi, flags, label_out, components_out);
 }
 
 }  // namespace tga

@@ -72,6 +72,14 @@ struct GraphHandle {
   std::vector<int32_t> slice_first_host;
   // scratch used by the algorithms
   DevBuf s_a, s_b, s_c, s_d, s_e, s_f, s_g, s_q0, s_q1, s_cnt, s_sum, s_edges;
+  // multi-source traversal state kept between calls (batch.cu): arrivals | last-enqueued arrivals
+  // ([m_cap][max_vertex] each), frontier masks, dirty bits, per-vertex epoch stamps and the list of
+  // vertices the last traversal touched.  With m_clean, everything is "unreached"/zero except the
+  // m_pending sources' entries at the touched vertices, which the next traversal resets first.
+  DevBuf m_state, m_mask, m_dirty, m_stamp, m_touched;
+  int32_t m_cap = 0, m_pending = 0;
+  uint32_t m_epoch = 0;
+  bool m_clean = false;
   uint32_t* h_pinned = nullptr;  // small pinned readback area
   // timing of the last call
   cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
@@ -109,6 +117,11 @@ int compute_max_timestamp(GraphHandle& h);
 inline bool window_covers_all(const GraphHandle& h, int64_t lo, int64_t hi) {
   return lo <= h.view.min_ts && hi > h.max_ts;
 }
+
+// Connected components with seeds run as speculative batches of a multi-source traversal
+// (batch.cu); same results as the one-seed-at-a-time loop.
+int cc_seed_batches(GraphHandle& h, int64_t t_lo, int64_t t_hi, int32_t flags, int32_t* label_out,
+                    int32_t* components_out);
 
 // Launch helpers shared by the algorithm files.
 inline unsigned grid_for(int64_t items, int block) { return (unsigned)((items + block - 1) / block); }

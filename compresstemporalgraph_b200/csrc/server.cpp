@@ -72,13 +72,37 @@ struct tga_server {
   Clock::time_point first_submit, last_done;
 
   void worker(GraphSlot* slot);
-  void run_round(GraphSlot* slot, std::vector<Pending>& round, std::vector<int>& status);
+  void run_round(GraphSlot* slot, std::vector<Pending>& round);
+  void publish(const std::vector<Pending>& round, const std::vector<size_t>& idx, const std::vector<int>& status);
 };
 
-void tga_server::run_round(GraphSlot* slot, std::vector<Pending>& round, std::vector<int>& status) {
+// Records the outcome of the queries round[idx[k]] (status[k]) and releases their budget.
+void tga_server::publish(const std::vector<Pending>& round, const std::vector<size_t>& idx,
+                         const std::vector<int>& status) {
+  const Clock::time_point now = Clock::now();
+  std::lock_guard<std::mutex> lk(mu);
+  for (size_t k = 0; k < idx.size(); ++k) {
+    const Pending& p = round[idx[k]];
+    Outcome& o = outcomes[p.ticket];
+    o.status = status[k];
+    o.latency_ms = std::chrono::duration<double, std::milli>(now - p.submitted).count();
+    in_use -= p.bytes;
+    if (status[k] == TGA_OK) {
+      ++completed;
+      latencies.push_back(o.latency_ms);
+    } else {
+      ++failed;
+    }
+  }
+  running -= (int64_t)idx.size();
+  last_done = now;
+  done_cv.notify_all();
+  work_cv.notify_all();
+}
+
+void tga_server::run_round(GraphSlot* slot, std::vector<Pending>& round) {
   const size_t nv = (size_t)slot->nv;
-  status.assign(round.size(), TGA_OK);
-  // BFS: one batched traversal.
+  // BFS: one batched traversal; results published as soon as it is done.
   {
     std::vector<size_t> idx;
     std::vector<int32_t> src;
@@ -93,10 +117,9 @@ void tga_server::run_round(GraphSlot* slot, std::vector<Pending>& round, std::ve
     if (!idx.empty()) {
       std::vector<int32_t> out(idx.size() * nv);
       const int rc = tga_bfs_batch(slot->g, (int32_t)idx.size(), src.data(), lo.data(), hi.data(), out.data());
-      for (size_t k = 0; k < idx.size(); ++k) {
-        status[idx[k]] = rc;
+      for (size_t k = 0; k < idx.size(); ++k)
         if (rc == TGA_OK && round[idx[k]].q.out) std::memcpy(round[idx[k]].q.out, out.data() + k * nv, nv * 4);
-      }
+      publish(round, idx, std::vector<int>(idx.size(), rc));
     }
   }
   // PageRank: one strided batch per iteration count.
@@ -120,17 +143,17 @@ void tga_server::run_round(GraphSlot* slot, std::vector<Pending>& round, std::ve
       }
       std::vector<float> out(idx.size() * nv);
       const int rc = tga_pagerank_batch(slot->g, (int32_t)idx.size(), it, 0.85f, 0.1f, lo.data(), hi.data(), out.data());
-      for (size_t k = 0; k < idx.size(); ++k) {
-        status[idx[k]] = rc;
+      for (size_t k = 0; k < idx.size(); ++k)
         if (rc == TGA_OK && round[idx[k]].q.out) std::memcpy(round[idx[k]].q.out, out.data() + k * nv, nv * 4);
-      }
+      publish(round, idx, std::vector<int>(idx.size(), rc));
     }
   }
   // CC: one traversal per query.
   for (size_t i = 0; i < round.size(); ++i) {
     const tga_query& q = round[i].q;
     if (q.kind != TGA_Q_CC) continue;
-    status[i] = tga_cc(slot->g, q.t_lo, q.t_hi, TGA_CC_EARLY_EXIT, static_cast<int32_t*>(q.out), nullptr);
+    const int rc = tga_cc(slot->g, q.t_lo, q.t_hi, TGA_CC_EARLY_EXIT, static_cast<int32_t*>(q.out), nullptr);
+    publish(round, std::vector<size_t>{i}, std::vector<int>{rc});
   }
 }
 
@@ -158,26 +181,8 @@ void tga_server::worker(GraphSlot* slot) {
     ++rounds;
     running += (int64_t)round.size();
     lk.unlock();
-    std::vector<int> status;
-    run_round(slot, round, status);
-    const Clock::time_point now = Clock::now();
+    run_round(slot, round);
     lk.lock();
-    for (size_t i = 0; i < round.size(); ++i) {
-      Outcome& o = outcomes[round[i].ticket];
-      o.status = status[i];
-      o.latency_ms = std::chrono::duration<double, std::milli>(now - round[i].submitted).count();
-      in_use -= round[i].bytes;
-      if (status[i] == TGA_OK) {
-        ++completed;
-        latencies.push_back(o.latency_ms);
-      } else {
-        ++failed;
-      }
-    }
-    running -= (int64_t)round.size();
-    last_done = now;
-    done_cv.notify_all();
-    work_cv.notify_all();
   }
 }
 

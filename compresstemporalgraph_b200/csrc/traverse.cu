@@ -413,6 +413,7 @@ int tga_cc(tga_graph* gp, int64_t t_lo, int64_t t_hi, int32_t flags, int32_t* la
   if (!gp) return fail(TGA_E_ARG, "null graph");
   GraphHandle& h = *gp;
   if (t_lo >= t_hi) return fail(TGA_E_ARG, "empty time window");
+  if (!(flags & TGA_CC_ONE_SEED)) return cc_seed_batches(h, t_lo, t_hi, flags, label_out, components_out);
   const int32_t nv = h.view.max_vertex;
   TGA_TRY(trav_buffers(h));
   TGA_TRY(h.s_e.ensure((size_t)nv));       // reached

@@ -132,8 +132,12 @@ int tga_bfs(tga_graph* g, int32_t src, int64_t t_lo, int64_t t_hi, int32_t* arri
  * unreached; every vertex a seed reaches gets that seed's component number (last seed wins).
  * flags & 1: apply the reference's early exits (stop once > 0.8*max_label vertices were reached,
  * or after more than 50 consecutive components smaller than 5) on exact reach counts.
- * label_out[v] = -1 when never reached. */
+ * label_out[v] = -1 when never reached.  Seeds run as speculative batches of one multi-source
+ * traversal (the next K candidates at once, validated in seed order; same labels as one seed per
+ * traversal); flags & 2 runs one seed per traversal instead, the plain form batching is measured
+ * against. */
 #define TGA_CC_EARLY_EXIT 1
+#define TGA_CC_ONE_SEED 2
 int tga_cc(tga_graph* g, int64_t t_lo, int64_t t_hi, int32_t flags, int32_t* label_out, int32_t* components_out);
 
 /* Temporal PageRank (pagerank.cu:1221-1660, loop 1956-2007) in FP32: rank starts at 1/max_vertex;

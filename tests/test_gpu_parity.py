@@ -100,13 +100,36 @@ def test_bfs_arrival_and_hops(pairs, shape):
 
 @pytest.mark.parametrize("shape", ALL)
 @pytest.mark.parametrize("early", [True, False])
-def test_connected_components(pairs, shape, early):
+@pytest.mark.parametrize("one_seed", [False, True])
+def test_connected_components(pairs, shape, early, one_seed):
     p = pairs[shape]
     for lo, hi in _windows(p)[:2]:
-        lab, k = p.g.connected_components(lo, hi, early_exit=early)
+        lab, k = p.g.connected_components(lo, hi, early_exit=early, one_seed=one_seed)
         olab, ok = p.o.cc(p.ml, p.mv, p.act, p.cfg.connected_components_vertex_begin, lo, hi, early)
         assert k == ok
         assert np.array_equal(lab, olab)
+
+
+def test_multi_source_state_survives_other_calls(pairs):
+    """The batched traversal keeps its per-source arrays between calls and resets only the
+    vertices the previous traversal touched; single-source traversals, batched CC and batched
+    BFS interleaved on one handle must each still match the oracle."""
+    p = pairs["hubs"]
+    lo, hi = _windows(p)[1]
+    n = p.n
+    srcs = np.array([0, n // 3, n - 1, 7], np.int32)
+    blo = np.array([lo, 0, lo, lo], np.int64)
+    bhi = np.array([hi, T_MAX, T_MAX, hi], np.int64)
+    for _ in range(2):
+        out = p.g.bfs_batch(srcs, blo, bhi)
+        for i in range(len(srcs)):
+            oarr, _ = p.o.bfs(p.ml, p.mv, p.act, int(srcs[i]), int(blo[i]), int(bhi[i]))
+            assert np.array_equal(out[i], oarr), i
+        arr, _ = p.g.bfs(int(srcs[1]), lo, hi)
+        assert np.array_equal(arr, p.o.bfs(p.ml, p.mv, p.act, int(srcs[1]), lo, hi)[0])
+        lab, k = p.g.connected_components(lo, hi)
+        olab, ok = p.o.cc(p.ml, p.mv, p.act, p.cfg.connected_components_vertex_begin, lo, hi, True)
+        assert k == ok and np.array_equal(lab, olab)
 
 
 @pytest.mark.parametrize("shape", ALL)
