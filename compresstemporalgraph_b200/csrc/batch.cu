@@ -41,6 +41,7 @@ struct MultiArgs {
   int32_t* ntouched;
   uint32_t epoch;
   int32_t nsrc, nv;
+  int32_t nv_lists;          // vertices with an out-list (graph n)
   int32_t dense_min, level_cap;
   unsigned long long* edges;
 };
@@ -92,6 +93,7 @@ __device__ __forceinline__ unsigned long long multi_relax(const GraphView& g, Mu
     bool any = false;
 #pragma unroll
     for (int k = 0; k < kWords; ++k) {
+      uint64_t add = 0;
       for (uint64_t c = M[k] & ~seen[k]; c; c &= c - 1) {
         const int b = __ffsll((long long)c) - 1;
         const int s = k * 64 + b;
@@ -101,7 +103,10 @@ __device__ __forceinline__ unsigned long long multi_relax(const GraphView& g, Mu
         const uint32_t ax = __ldcg(a.arr + (size_t)s * nv + xcur);
         if ((int64_t)ax > t) continue;
         atomicMin(a.arr + (size_t)s * nv + y, (uint32_t)t);
-        atomicOr((unsigned long long*)(Fn + (size_t)y * kWords + k), (unsigned long long)(1ull << b));
+        add |= 1ull << b;
+      }
+      if (add) {
+        atomicOr((unsigned long long*)(Fn + (size_t)y * kWords + k), (unsigned long long)add);
         any = true;
       }
     }
@@ -189,18 +194,15 @@ __device__ __forceinline__ void multi_scan(MultiArgs& a, const int32_t* cq, int 
   }
 }
 
-__global__ void TGA_DECODE_BOUNDS k_bfs_multi(GraphView g, MultiArgs a) {
-  __shared__ int64_t slo[kMaxSources], shi[kMaxSources];
-  for (int s = threadIdx.x; s < kMaxSources; s += blockDim.x) {
-    slo[s] = s < a.nsrc ? a.lo[s] : 0;
-    shi[s] = s < a.nsrc ? a.hi[s] : 0;
-  }
-  __syncthreads();
-  unsigned long long mine = 0;
+// Levels 1.. of a multi-source traversal whose sources are seeded (level-0 relaxations in F[1]
+// and the dirty bits); the control block's queue and work counters must be zero.  All blocks of
+// the cooperative launch call it together; false if the launch has failed (return at once).
+__device__ bool multi_levels(const GraphView& g, MultiArgs& a, const int64_t* slo, const int64_t* shi,
+                             unsigned long long& mine, int& levels) {
   const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
   // The sources were seeded as level 0's relaxations: the scan turns them into level 1's queue.
   multi_scan(a, a.q[0], 0, a.q[1], &a.ctl->cnt[1], 0);
-  if (!grid_sync(a.ctl, g)) return;
+  if (!grid_sync(a.ctl, g)) return false;
   int L = 1;
   for (;;) {
     const int qn = __ldcg(&a.ctl->cnt[L % 3]);
@@ -210,7 +212,7 @@ __global__ void TGA_DECODE_BOUNDS k_bfs_multi(GraphView g, MultiArgs a) {
         set_err(g, kErrTimeout);
         a.ctl->status = 1;
       }
-      return;
+      return false;
     }
     if (lead) {
       a.ctl->cnt[(L + 2) % 3] = 0;
@@ -219,28 +221,50 @@ __global__ void TGA_DECODE_BOUNDS k_bfs_multi(GraphView g, MultiArgs a) {
     Work w = a.w;
     w.next = &a.ctl->next[L % 3];
     mine += multi_relax(g, a, w, slo, shi, a.q[L & 1], qn, L, qn >= a.dense_min);
-    if (!grid_sync(a.ctl, g)) return;
+    if (!grid_sync(a.ctl, g)) return false;
     multi_scan(a, a.q[L & 1], qn, a.q[(L + 1) & 1], &a.ctl->cnt[(L + 1) % 3], L);
-    if (!grid_sync(a.ctl, g)) return;
+    if (!grid_sync(a.ctl, g)) return false;
     ++L;
   }
+  levels = L;
+  return true;
+}
+
+// Sources 0..nsrc-1 of a traversal (grid-stride over the calling threads): the arrival of each
+// source vertex (max(lo, 0)) as its level-0 relaxation.
+__device__ __forceinline__ void multi_seed(MultiArgs& a, const int32_t* src, int32_t nsrc, int32_t n) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nsrc; s += gridDim.x * blockDim.x) {
+    const int v = __ldcg(src + s);
+    const int64_t lo = __ldcg(a.lo + s);
+    a.arr[(size_t)s * a.nv + v] = (uint32_t)(lo > 0 ? lo : 0);
+    if (atomicExch(&a.stamp[v], a.epoch) != a.epoch) a.touched[atomicAdd(a.ntouched, 1)] = v;
+    if (v < n) {
+      atomicOr((unsigned long long*)(a.F[1] + (size_t)v * kWords + s / 64), (unsigned long long)(1ull << (s & 63)));
+      atomicOr(&a.dirty[v >> 5], 1u << (v & 31));
+    }
+  }
+}
+
+__device__ __forceinline__ void load_windows(const MultiArgs& a, int64_t* slo, int64_t* shi) {
+  for (int s = threadIdx.x; s < kMaxSources; s += blockDim.x) {
+    slo[s] = s < a.nsrc ? a.lo[s] : 0;
+    shi[s] = s < a.nsrc ? a.hi[s] : 0;
+  }
+  __syncthreads();
+}
+
+__global__ void TGA_DECODE_BOUNDS k_bfs_multi(GraphView g, MultiArgs a) {
+  __shared__ int64_t slo[kMaxSources], shi[kMaxSources];
+  load_windows(a, slo, shi);
+  unsigned long long mine = 0;
+  int levels = 0;
+  if (!multi_levels(g, a, slo, shi, mine, levels)) return;
   add_edges(a.edges, mine);
-  if (lead) a.ctl->levels = L;
+  if (blockIdx.x == 0 && threadIdx.x == 0) a.ctl->levels = levels;
 }
 
 // Sources of the batch: arrival and level-0 relaxation of each source vertex.
-__global__ void k_bfs_multi_seed(MultiArgs a, const int32_t* src, int32_t n) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= a.nsrc) return;
-  const int v = src[s];
-  const int64_t start = a.lo[s] > 0 ? a.lo[s] : 0;
-  a.arr[(size_t)s * a.nv + v] = (uint32_t)start;
-  if (atomicExch(&a.stamp[v], a.epoch) != a.epoch) a.touched[atomicAdd(a.ntouched, 1)] = v;
-  if (v < n) {
-    atomicOr((unsigned long long*)(a.F[1] + (size_t)v * kWords + s / 64), (unsigned long long)(1ull << (s & 63)));
-    atomicOr(&a.dirty[v >> 5], 1u << (v & 31));
-  }
-}
+__global__ void k_bfs_multi_seed(MultiArgs a, const int32_t* src) { multi_seed(a, src, a.nsrc, a.nv_lists); }
 
 // Per-source first in-window edge of each run of equal successors cut by slices: one thread per
 // (run, overlapping slice) decodes the run's part of the slice and lowers run_first[run][s] for
@@ -343,12 +367,12 @@ static int multi_runs(GraphHandle& h, int32_t nsrc) {
   return TGA_OK;
 }
 
-// Runs one multi-source traversal of nsrc sources whose vertices and windows are already in
-// multi_src/multi_lo/multi_hi and whose run table is built (multi_runs); multi_buffers(h, >= nsrc)
-// must have run.  Leaves the arrivals in a.arr ([nsrc][max_vertex], kNoArrival: unreached) and the
-// vertices with any finite arrival on a.touched (count in *a.ntouched) until the next call.
-// *levels gets the levels run.
-static int multi_run(GraphHandle& h, int32_t nsrc, unsigned long long* edges, MultiArgs& a, int32_t* levels) {
+// Fills `a` for traversals of up to nsrc sources whose windows are in multi_lo/multi_hi and whose
+// run table is built (multi_runs), after multi_buffers(h, >= nsrc), and prepares the state: the
+// previous traversal's entries back to "unreached", an empty touched list, a fresh epoch (a.epoch;
+// a launch running several traversals uses a.epoch, a.epoch + 1, ... and records the last in
+// h.m_epoch) and a zero control block.
+static int multi_prepare(GraphHandle& h, int32_t nsrc, unsigned long long* edges, MultiArgs& a) {
   const size_t nv = (size_t)h.view.max_vertex;
   if (nsrc > h.m_cap || !h.m_clean) return fail(TGA_E_ARG, "multi-source state not prepared");
   a = MultiArgs{};
@@ -371,40 +395,58 @@ static int multi_run(GraphHandle& h, int32_t nsrc, unsigned long long* edges, Mu
   a.ntouched = a.touched + nv;  // the count follows the list; it outlives the shared control block
   a.nsrc = nsrc;
   a.nv = (int32_t)nv;
+  a.nv_lists = h.view.n;
   a.dense_min = std::max<int32_t>(h.dense_min, 1);
   a.level_cap = 1 << 20;
   a.edges = edges;
-  // The previous traversal's entries back to "unreached", then an empty touched list.
   if (h.m_pending > 0) {
     KL(k_multi_reset, 4 * h.sm_count)(a.arr, a.prev, a.nv, a.touched, a.ntouched, h.m_pending);
     h.m_pending = 0;
   }
   TGA_CUDA_TRY(cudaMemsetAsync(a.ntouched, 0, 4, h.stream));
-  if (++h.m_epoch == 0) {  // stamps wrapped: clear them
+  if (h.m_epoch >= 0x7fffffffu) {  // far from wrapping: clear the stamps and start again
     TGA_CUDA_TRY(cudaMemsetAsync(a.stamp, 0, nv * 4, h.stream));
-    h.m_epoch = 1;
+    h.m_epoch = 0;
   }
-  a.epoch = h.m_epoch;
+  a.epoch = ++h.m_epoch;
   TravCtl ctl{};
   std::memcpy(h.h_pinned + 32, &ctl, sizeof ctl);
   TGA_CUDA_TRY(cudaMemcpyAsync(a.ctl, h.h_pinned + 32, sizeof ctl, cudaMemcpyHostToDevice, h.stream));
-  KL(k_bfs_multi_seed, grid_for(nsrc, kBlock))(a, multi_src(h), h.view.n);
+  return TGA_OK;
+}
+
+// Cooperative launch of a multi-source kernel (one grid of all resident blocks), then the control
+// block back to *ctl.  The state counts as cleared-or-pending only once the launch has finished
+// without a barrier timeout.
+static int multi_launch(GraphHandle& h, const void* kernel, void** args, TravCtl* ctl) {
   int per_sm = 0;
-  TGA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bfs_multi, kBlock, 0));
+  TGA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBlock, 0));
   if (per_sm < 1) return fail(TGA_E_CUDA, "batched traversal kernel cannot be resident");
-  void* args[] = {&h.view, &a};
   cudaEvent_t* ev = h.kernel_begin();
   ++h.timing.launches;
-  h.m_pending = nsrc;
-  h.m_clean = false;  // until the traversal is known to have finished
-  TGA_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_bfs_multi, dim3(per_sm * h.sm_count), dim3(kBlock), args, 0,
-                                           h.stream));
+  h.m_clean = false;
+  TGA_CUDA_TRY(cudaLaunchCooperativeKernel(kernel, dim3(per_sm * h.sm_count), dim3(kBlock), args, 0, h.stream));
   h.kernel_end(ev);
-  TGA_CUDA_TRY(cudaMemcpyAsync(h.h_pinned + 32, a.ctl, sizeof(TravCtl), cudaMemcpyDeviceToHost, h.stream));
+  TGA_CUDA_TRY(cudaMemcpyAsync(h.h_pinned + 32, h.s_cnt.p, sizeof(TravCtl), cudaMemcpyDeviceToHost, h.stream));
   TGA_CUDA_TRY(cudaStreamSynchronize(h.stream));
-  std::memcpy(&ctl, h.h_pinned + 32, sizeof ctl);
-  if (ctl.status) return fail(TGA_E_TIMEOUT, "a grid barrier wait ran out");
+  std::memcpy(ctl, h.h_pinned + 32, sizeof *ctl);
+  if (ctl->status) return fail(TGA_E_TIMEOUT, "a grid barrier wait ran out");
   h.m_clean = true;
+  return TGA_OK;
+}
+
+// Runs one multi-source traversal of nsrc sources whose vertices and windows are already in
+// multi_src/multi_lo/multi_hi and whose run table is built (multi_runs); multi_buffers(h, >= nsrc)
+// must have run.  Leaves the arrivals in a.arr ([nsrc][max_vertex], kNoArrival: unreached) and the
+// vertices with any finite arrival on a.touched (count in *a.ntouched) until the next call.
+// *levels gets the levels run.
+static int multi_run(GraphHandle& h, int32_t nsrc, unsigned long long* edges, MultiArgs& a, int32_t* levels) {
+  TGA_TRY(multi_prepare(h, nsrc, edges, a));
+  KL(k_bfs_multi_seed, grid_for(nsrc, kBlock))(a, multi_src(h));
+  h.m_pending = nsrc;
+  void* args[] = {&h.view, &a};
+  TravCtl ctl;
+  TGA_TRY(multi_launch(h, (const void*)k_bfs_multi, args, &ctl));
   *levels = ctl.levels;
   return TGA_OK;
 }
@@ -439,8 +481,15 @@ static int bfs_multi_batch(GraphHandle& h, int32_t nsrc, const int32_t* src, con
 // (each with its own fresh arrivals, as the sequential loop has); then, in seed order, a candidate
 // is a real seed iff no earlier real seed of the batch reached it, the early-exit rules run on the
 // exact reach counts, and every vertex takes the component number of the last real seed that
-// reached it.  The labels equal the sequential loop's; K doubles while all candidates of a batch
-// turn out to be real seeds and halves otherwise.
+// reached it.  The labels equal the sequential loop's.
+//
+// The whole loop is one cooperative launch.  Per batch: block 0 picks the candidates; all blocks
+// seed and traverse; all count the reach of each source over the touched vertices; block 0
+// validates in seed order and chooses the next K; all blocks label the touched vertices and reset
+// their arrivals.  Grid barriers separate the phases, so no batch waits for the host.  K doubles
+// while the reach of the candidates that turned out not to be seeds (traversal work thrown away)
+// stays below an eighth of the real seeds' reach plus a fixed allowance, and halves when it
+// exceeds the real seeds' reach plus that allowance.
 
 struct CcBatchState {
   int64_t total;       // reach counts so far (early-exit rule)
@@ -449,112 +498,233 @@ struct CcBatchState {
   int32_t small_run;   // consecutive components smaller than 5
   int32_t stop;        // the seed loop has ended
   int32_t ncand;       // candidates of the current batch
-  int32_t nvalid, ninvalid;
+  int32_t K;           // candidates per batch
+  int32_t batches;
   int32_t pad;
 };
 
-// The first K vertices >= v below end that are unreached and have outdegree > 9, in order.
-__global__ void k_cc_candidates(const uint8_t* reached, const int32_t* deg, CcBatchState* st, int32_t end, int32_t K,
-                                int32_t* cand) {
-  __shared__ int wcount[32];
-  __shared__ int count;
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  if (threadIdx.x == 0) count = 0;
+struct CcArgs {
+  CcBatchState* st;
+  const int32_t* deg;
+  uint8_t* reached;             // [max_vertex] labelled already
+  int32_t* label;               // [max_vertex]
+  int32_t* cand;                // sources of the current batch
+  unsigned long long* counts;   // [kMaxSources] finite arrivals per source
+  int32_t* comp_of;             // [kMaxSources] component of a real seed, -1 otherwise
+  uint32_t* reach_bits;         // [kMaxSources][kMaxSources / 32] pair matrix of the batch
+  int32_t end;                  // candidates lie below this vertex
+  int32_t early;                // apply the early exits
+  int64_t limit;                // early exit: reach total above this
+};
+
+constexpr int kCcMinK = 4;
+constexpr int64_t kCcWasteAllowance = 4096;  // reach a batch may throw away and still grow K
+
+// Block 0: the first K vertices >= st->v below end that are unreached and have outdegree > 9, in
+// order, to cand; st->ncand = their number (0 once the loop has stopped).  Each thread tests 8
+// consecutive vertices per step.
+__device__ void cc_candidates(const CcArgs& c, int32_t* s_wsum, int32_t* s_count) {
+  constexpr int kPer = 8;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int K = __ldcg(&c.st->K);
+  if (threadIdx.x == 0) *s_count = 0;
   __syncthreads();
-  if (!st->stop) {
-    for (int64_t base = st->v; base < end; base += blockDim.x) {
-      const int64_t u = base + threadIdx.x;
-      const bool f = u < end && !reached[u] && deg[u] > 9;
-      const unsigned ballot = __ballot_sync(0xffffffffu, f);
-      if (lane == 0) wcount[wid] = __popc(ballot);
+  if (!__ldcg(&c.st->stop)) {
+    for (int64_t base = __ldcg(&c.st->v); base < c.end; base += (int64_t)kBlock * kPer) {
+      const int64_t u0 = base + (int64_t)threadIdx.x * kPer;
+      uint32_t f = 0;
+#pragma unroll
+      for (int k = 0; k < kPer; ++k) {
+        const int64_t u = u0 + k;
+        if (u < c.end && !__ldcg(c.reached + u) && __ldg(c.deg + u) > 9) f |= 1u << k;
+      }
+      const int cnt = __popc(f);
+      int incl = cnt;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+      }
+      if (lane == 31) s_wsum[wid] = incl;
       __syncthreads();
       int before = 0, total = 0;
-      for (int k = 0; k < nw; ++k) {
-        if (k < wid) before += wcount[k];
-        total += wcount[k];
+      for (int k = 0; k < kBlock / 32; ++k) {
+        if (k < wid) before += s_wsum[k];
+        total += s_wsum[k];
       }
-      const int pos = count + before + __popc(ballot & ((1u << lane) - 1));
-      if (f && pos < K) cand[pos] = (int32_t)u;
+      int pos = *s_count + before + incl - cnt;
+      for (uint32_t b = f; b; b &= b - 1, ++pos)
+        if (pos < K) c.cand[pos] = (int32_t)(u0 + __ffs(b) - 1);
       __syncthreads();
-      if (threadIdx.x == 0) count += total;
+      if (threadIdx.x == 0) *s_count += total;
       __syncthreads();
-      if (count >= K) break;
+      if (*s_count >= K) break;
     }
   }
-  if (threadIdx.x == 0) st->ncand = min(count, K);
+  if (threadIdx.x == 0) c.st->ncand = min(*s_count, K);
 }
 
-// Finite arrivals per source (its reach plus the seed itself), over the touched vertices.
-__global__ void k_multi_count(const uint32_t* arr, int32_t nv, const int32_t* touched, const int32_t* ntouched,
-                              unsigned long long* counts) {
-  const int s = blockIdx.y;
-  const int nt = *ntouched;
-  unsigned long long c = 0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nt; i += gridDim.x * blockDim.x)
-    c += arr[(size_t)s * nv + touched[i]] != kNoArrival;
-  for (int o = 16; o; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
-  if ((threadIdx.x & 31) == 0 && c) atomicAdd(&counts[s], c);
-}
-
-// Candidates in seed order: real seeds, component numbers, reach counts and the early exits.
-__global__ void k_cc_validate(CcBatchState* st, const int32_t* cand, const uint32_t* arr, int32_t nv,
-                              const unsigned long long* counts, int32_t* comp_of, int32_t early, int64_t limit) {
-  __shared__ uint32_t reaches[kMaxSources][kMaxSources / 32];  // bit i of row j: candidate i reached j
-  const int n = st->ncand;
-  for (int e = threadIdx.x; e < kMaxSources * (kMaxSources / 32); e += blockDim.x) (&reaches[0][0])[e] = 0;
+// All blocks: finite arrivals per source over the touched vertices (one warp per vertex, lane l
+// reading sources l, l + 32, ...; block-local sums first), and the pair matrix of the batch:
+// bit i of reach_bits[j] set when candidate i < j reached candidate j.
+__device__ void cc_count(const MultiArgs& a, const CcArgs& c, int n, uint32_t* s_cnt) {
+  for (int s = threadIdx.x; s < kMaxSources; s += blockDim.x) s_cnt[s] = 0;
   __syncthreads();
-  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const int nt = __ldcg(a.ntouched);
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int i = warp; i < nt; i += nwarps) {
+    const int u = __ldcg(a.touched + i);
+    uint32_t hit[kMaxSources / 32];
+#pragma unroll
+    for (int k = 0; k < kMaxSources / 32; ++k) {
+      const int j = k * 32 + lane;
+      hit[k] = j < n && __ldcg(a.arr + (size_t)j * a.nv + u) != kNoArrival;
+    }
+#pragma unroll
+    for (int k = 0; k < kMaxSources / 32; ++k)
+      if (hit[k]) atomicAdd(&s_cnt[k * 32 + lane], 1u);
+  }
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
+  for (int e = tid; e < n * n; e += nthreads) {
     const int j = e / n, i = e % n;
-    if (i < j && arr[(size_t)i * nv + cand[j]] != kNoArrival) atomicOr(&reaches[j][i >> 5], 1u << (i & 31));
+    if (i < j && __ldcg(a.arr + (size_t)i * a.nv + __ldcg(c.cand + j)) != kNoArrival)
+      atomicOr(&c.reach_bits[j * (kMaxSources / 32) + (i >> 5)], 1u << (i & 31));
+  }
+  __syncthreads();
+  for (int s = threadIdx.x; s < n; s += blockDim.x)
+    if (s_cnt[s]) atomicAdd(&c.counts[s], (unsigned long long)s_cnt[s]);
+}
+
+// Block 0: candidates in seed order -- real seeds, component numbers, reach counts, the early
+// exits -- and the next batch size, from a shared copy of the pair matrix, counts and candidates.
+__device__ void cc_validate(const CcArgs& c, int n, uint32_t (*reaches)[kMaxSources / 32], uint32_t* s_cnt,
+                            int32_t* s_cand) {
+  for (int e = threadIdx.x; e < n * (kMaxSources / 32); e += blockDim.x)
+    (&reaches[0][0])[e] = __ldcg(c.reach_bits + e);
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    s_cnt[j] = (uint32_t)__ldcg(c.counts + j);
+    s_cand[j] = __ldcg(c.cand + j);
   }
   __syncthreads();
   if (threadIdx.x != 0) return;
+  int64_t total = __ldcg(&c.st->total);
+  int32_t v = __ldcg(&c.st->v), comp = __ldcg(&c.st->comp), small_run = __ldcg(&c.st->small_run);
+  int32_t K = __ldcg(&c.st->K);
+  bool stop = false;
   uint32_t real[kMaxSources / 32] = {};
-  int nvalid = 0, ninvalid = 0;
+  int checked = 0, ninvalid = 0;
+  int64_t useful = 0, wasted = 0;
   for (int j = 0; j < n; ++j) {
-    comp_of[j] = -1;
-    bool reached = false;
-    for (int k = 0; k < kMaxSources / 32; ++k) reached |= (reaches[j][k] & real[k]) != 0;
-    if (reached) {
+    const int64_t cnt = s_cnt[j];
+    bool hit = false;
+#pragma unroll
+    for (int k = 0; k < kMaxSources / 32; ++k) hit |= (reaches[j][k] & real[k]) != 0;
+    if (hit) {
+      ++checked;
       ++ninvalid;
+      wasted += cnt;
+      c.comp_of[j] = -1;
       continue;
     }
-    if (early && st->total > limit) {
-      st->stop = 1;
+    if (c.early && total > c.limit) {
+      stop = true;
       break;
     }
+    ++checked;
     real[j >> 5] |= 1u << (j & 31);
-    ++nvalid;
-    const int64_t reach = (int64_t)counts[j] - 1;  // the seed's own arrival is set before its traversal
-    comp_of[j] = st->comp++;
-    st->total += reach + 1;
-    st->small_run = (reach + 1 < 5) ? st->small_run + 1 : 0;
-    st->v = cand[j] + 1;
-    if (early && st->small_run > 50) {
-      st->stop = 1;
+    useful += cnt;
+    const int64_t reach = cnt - 1;  // the seed's own arrival is set before its traversal
+    c.comp_of[j] = comp++;
+    total += reach + 1;
+    small_run = (reach + 1 < 5) ? small_run + 1 : 0;
+    v = s_cand[j] + 1;
+    if (c.early && small_run > 50) {
+      stop = true;
       break;
     }
   }
-  for (int j = nvalid + ninvalid; j < n; ++j) comp_of[j] = -1;
-  if (!st->stop && n > 0) st->v = cand[n - 1] + 1;
-  st->nvalid = nvalid;
-  st->ninvalid = ninvalid;
+  for (int j = checked; j < n; ++j) c.comp_of[j] = -1;
+  if (!stop && n > 0) v = s_cand[n - 1] + 1;
+  // Over the limit now: the next real seed would stop the loop before labelling anything.
+  if (c.early && total > c.limit) stop = true;
+  if (8 * wasted <= useful + kCcWasteAllowance) K = min(2 * K, kMaxSources);
+  else if (wasted > useful + kCcWasteAllowance) K = max(kCcMinK, K / 2);
+  c.st->total = total;
+  c.st->v = v;
+  c.st->comp = comp;
+  c.st->small_run = small_run;
+  c.st->K = K;
+  if (stop) c.st->stop = 1;
 }
 
-// Every touched vertex takes the component of the last real seed of the batch that reached it.
-__global__ void k_cc_label_multi(const uint32_t* arr, int32_t nv, const int32_t* touched, const int32_t* ntouched,
-                                 const int32_t* comp_of, int32_t n, int32_t* label, uint8_t* reached) {
-  const int nt = *ntouched;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nt; i += gridDim.x * blockDim.x) {
-    const int u = touched[i];
-    for (int j = n - 1; j >= 0; --j) {
-      const int c = comp_of[j];
-      if (c >= 0 && arr[(size_t)j * nv + u] != kNoArrival) {
-        label[u] = c;
-        reached[u] = 1;
-        break;
+// All blocks: every touched vertex takes the component of the last real seed of the batch that
+// reached it, and its arrivals of the batch's sources go back to "unreached" (one warp per vertex).
+__device__ void cc_label_reset(const MultiArgs& a, const CcArgs& c, int n) {
+  const int lane = threadIdx.x & 31;
+  const int nt = __ldcg(a.ntouched);
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int i = warp; i < nt; i += nwarps) {
+    const int u = __ldcg(a.touched + i);
+    int best = -1;  // highest real seed j reaching u
+#pragma unroll
+    for (int k = 0; k < kMaxSources / 32; ++k) {
+      const int j = k * 32 + lane;
+      if (j < n) {
+        const size_t at = (size_t)j * a.nv + u;
+        if (__ldcg(a.arr + at) != kNoArrival && __ldcg(c.comp_of + j) >= 0) best = j;
+        a.arr[at] = kNoArrival;
+        a.prev[at] = kNoArrival;
       }
     }
+    for (int o = 16; o; o >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
+    if (lane == 0 && best >= 0) {
+      c.label[u] = __ldcg(c.comp_of + best);
+      c.reached[u] = 1;
+    }
+  }
+}
+
+__global__ void TGA_DECODE_BOUNDS k_cc_batches(GraphView g, MultiArgs a, CcArgs c) {
+  __shared__ int64_t slo[kMaxSources], shi[kMaxSources];
+  __shared__ uint32_t reaches[kMaxSources][kMaxSources / 32];
+  __shared__ uint32_t s_cnt[kMaxSources];
+  __shared__ int32_t s_cand[kMaxSources];
+  __shared__ int32_t s_wsum[kBlock / 32], s_count;
+  load_windows(a, slo, shi);
+  const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
+  const uint32_t epoch0 = a.epoch;
+  unsigned long long mine = 0;
+  int levels = 0, batch = 0;
+  for (;; ++batch) {
+    if (blockIdx.x == 0) {
+      cc_candidates(c, s_wsum, &s_count);
+      for (int s = threadIdx.x; s < kMaxSources; s += blockDim.x) c.counts[s] = 0;
+      for (int e = threadIdx.x; e < kMaxSources * (kMaxSources / 32); e += blockDim.x) c.reach_bits[e] = 0;
+      if (threadIdx.x == 0) {
+        for (int k = 0; k < 3; ++k) a.ctl->cnt[k] = a.ctl->next[k] = 0;
+        *a.ntouched = 0;
+      }
+    }
+    if (!grid_sync(a.ctl, g)) return;
+    const int n = __ldcg(&c.st->ncand);
+    if (n == 0) break;
+    a.epoch = epoch0 + (uint32_t)batch;
+    multi_seed(a, c.cand, n, a.nv_lists);
+    if (!grid_sync(a.ctl, g)) return;
+    int lv = 0;
+    if (!multi_levels(g, a, slo, shi, mine, lv)) return;
+    levels += lv;
+    cc_count(a, c, n, s_cnt);
+    if (!grid_sync(a.ctl, g)) return;
+    if (blockIdx.x == 0) cc_validate(c, n, reaches, s_cnt, s_cand);
+    if (!grid_sync(a.ctl, g)) return;
+    cc_label_reset(a, c, n);
+    if (!grid_sync(a.ctl, g)) return;
+  }
+  add_edges(a.edges, mine);
+  if (lead) {
+    a.ctl->levels = levels;
+    c.st->batches = batch;
   }
 }
 
@@ -568,57 +738,45 @@ static int cc_batched(GraphHandle& h, int64_t t_lo, int64_t t_hi, int32_t flags,
   const int32_t nv = h.view.max_vertex;
   TGA_TRY(multi_buffers(h, kMaxSources));
   TGA_TRY(h.s_e.ensure((size_t)nv * 4 + (size_t)nv));                       // labels | reached
-  TGA_TRY(h.s_f.ensure(sizeof(CcBatchState) + kMaxSources * (8 + 4)));      // state | counts | comp_of
+  // state | counts | comp_of | pair matrix
+  TGA_TRY(h.s_f.ensure(sizeof(CcBatchState) + kMaxSources * (8 + 4) + kMaxSources * kMaxSources / 8));
   TGA_TRY(h.begin_call());
   unsigned long long* edges = edge_counter(h);
-  int32_t* label = h.s_e.as<int32_t>();
-  uint8_t* reached = reinterpret_cast<uint8_t*>(label + nv);
-  CcBatchState* st = h.s_f.as<CcBatchState>();
-  unsigned long long* counts = reinterpret_cast<unsigned long long*>(h.s_f.as<char>() + sizeof(CcBatchState));
-  int32_t* comp_of = reinterpret_cast<int32_t*>(counts + kMaxSources);
-  KL(k_fill_i32, grid_for(nv, kBlock))(label, -1, nv);
-  TGA_CUDA_TRY(cudaMemsetAsync(reached, 0, (size_t)nv, h.stream));
+  CcArgs c{};
+  c.label = h.s_e.as<int32_t>();
+  c.reached = reinterpret_cast<uint8_t*>(c.label + nv);
+  c.st = h.s_f.as<CcBatchState>();
+  c.counts = reinterpret_cast<unsigned long long*>(h.s_f.as<char>() + sizeof(CcBatchState));
+  c.comp_of = reinterpret_cast<int32_t*>(c.counts + kMaxSources);
+  c.reach_bits = reinterpret_cast<uint32_t*>(c.comp_of + kMaxSources);
+  c.deg = h.d_deg.as<int32_t>();
+  c.cand = multi_src(h);
+  c.end = std::min(std::min(h.view.max_label, nv), h.view.n);
+  c.early = (flags & TGA_CC_EARLY_EXIT) ? 1 : 0;
+  c.limit = (int64_t)(0.8 * h.view.max_label);
+  KL(k_fill_i32, grid_for(nv, kBlock))(c.label, -1, nv);
+  TGA_CUDA_TRY(cudaMemsetAsync(c.reached, 0, (size_t)nv, h.stream));
   CcBatchState init{};
   init.v = std::max(h.cfg.cc_vertex_begin, 0);
+  init.K = kCcMinK;
   std::memcpy(h.h_pinned + 64, &init, sizeof init);
-  TGA_CUDA_TRY(cudaMemcpyAsync(st, h.h_pinned + 64, sizeof init, cudaMemcpyHostToDevice, h.stream));
+  TGA_CUDA_TRY(cudaMemcpyAsync(c.st, h.h_pinned + 64, sizeof init, cudaMemcpyHostToDevice, h.stream));
   k_fill_windows<<<1, kMaxSources, 0, h.stream>>>(multi_lo(h), multi_hi(h), t_lo, t_hi);
   ++h.timing.launches;
   TGA_TRY(multi_runs(h, kMaxSources));  // one table serves every batch: all windows are the same
-  const int32_t end = std::min(std::min(h.view.max_label, nv), h.view.n);
-  const int64_t limit = (int64_t)(0.8 * h.view.max_label);
-  const int32_t early = (flags & TGA_CC_EARLY_EXIT) ? 1 : 0;
-  int32_t K = 4, levels = 0;
-  for (int batch = 0;; ++batch) {
-    if (batch > (1 << 22)) return fail(TGA_E_TIMEOUT, "CC batch cap reached");
-    k_cc_candidates<<<1, 1024, 0, h.stream>>>(reached, h.d_deg.as<int32_t>(), st, end, K, multi_src(h));
-    ++h.timing.launches;
-    TGA_CUDA_TRY(cudaMemcpyAsync(h.h_pinned + 64, st, sizeof(CcBatchState), cudaMemcpyDeviceToHost, h.stream));
-    TGA_CUDA_TRY(cudaStreamSynchronize(h.stream));
-    CcBatchState cur;
-    std::memcpy(&cur, h.h_pinned + 64, sizeof cur);
-    if (batch > 0) K = cur.ninvalid == 0 ? std::min(2 * K, kMaxSources) : std::max(4, K / 2);
-    if (cur.stop || cur.ncand == 0) break;
-    const int32_t n = cur.ncand;
-    MultiArgs a;
-    int32_t lv = 0;
-    TGA_TRY(multi_run(h, n, edges, a, &lv));
-    levels += lv;
-    TGA_CUDA_TRY(cudaMemsetAsync(counts, 0, kMaxSources * 8, h.stream));
-    KL(k_multi_count, dim3(std::max(1u, std::min(64u, grid_for(nv, kBlock))), n))(a.arr, nv, a.touched, a.ntouched,
-                                                                                    counts);
-    k_cc_validate<<<1, 1024, 0, h.stream>>>(st, multi_src(h), a.arr, nv, counts, comp_of, early, limit);
-    ++h.timing.launches;
-    KL(k_cc_label_multi, std::min(grid_for(nv, kBlock), 8u * h.sm_count))(a.arr, nv, a.touched, a.ntouched, comp_of, n,
-                                                                           label, reached);
-  }
+  MultiArgs a;
+  TGA_TRY(multi_prepare(h, kMaxSources, edges, a));
+  void* args[] = {&h.view, &a, &c};
+  TravCtl ctl;
+  TGA_TRY(multi_launch(h, (const void*)k_cc_batches, args, &ctl));
   CcBatchState fin;
-  TGA_CUDA_TRY(cudaMemcpyAsync(h.h_pinned + 64, st, sizeof fin, cudaMemcpyDeviceToHost, h.stream));
+  TGA_CUDA_TRY(cudaMemcpyAsync(h.h_pinned + 64, c.st, sizeof fin, cudaMemcpyDeviceToHost, h.stream));
   TGA_CUDA_TRY(cudaStreamSynchronize(h.stream));
   std::memcpy(&fin, h.h_pinned + 64, sizeof fin);
-  if (label_out) TGA_CUDA_TRY(cudaMemcpyAsync(label_out, label, (size_t)nv * 4, cudaMemcpyDeviceToHost, h.stream));
+  h.m_epoch = a.epoch + (uint32_t)std::max(fin.batches, 0);  // every batch reset its own entries
+  if (label_out) TGA_CUDA_TRY(cudaMemcpyAsync(label_out, c.label, (size_t)nv * 4, cudaMemcpyDeviceToHost, h.stream));
   if (components_out) *components_out = fin.comp;
-  h.timing.iterations = levels;
+  h.timing.iterations = ctl.levels;
   return finish(h, edges);
 }
 
