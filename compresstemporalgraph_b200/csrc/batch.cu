@@ -10,8 +10,15 @@
 // mask of the sources that have already seen an in-window edge.  Relaxations are reductions
 // without a return value (RED.MIN on the source's arrival, RED.OR on the successor's next mask)
 // plus a dirty bit; after a grid barrier a scan keeps only the sources whose arrival really
-// dropped, clears the finished level's masks and builds the next queue.  Same queue rotation,
+// dropped, clears the finished level's masks and builds the next queues.  Same queue rotation,
 // dense-level sweep and bounded barrier as the single-source traversal (traverse.cu).
+//
+// Arrivals are vertex-major (row v holds the arrivals of all sources at v), so the sources of one
+// list touch a few adjacent sectors.  The scan splits the frontier by the number of sources in a
+// vertex's mask: lists with fewer than kWarpSources go to the sparse queue, one thread per entry;
+// the others to the wide queue, one warp per entry, where lane 0 decodes and each lane handles the
+// sources lane, lane + 32, ... with their arrivals at the list's vertex held in registers, so an
+// edge costs a lane at most kSlots checks instead of one thread walking every source.
 #include <algorithm>
 #include <cstring>
 #include <vector>
@@ -22,14 +29,18 @@ namespace tga {
 
 constexpr int kMaxSources = 256;
 constexpr int kWords = kMaxSources / 64;
+constexpr int kSlots = kMaxSources / 32;   // sources per lane in the wide relax
+constexpr int kWarpSources = 8;            // masks with at least this many sources take the wide queue
 constexpr uint32_t kNoArrival = 0xFFFFFFFFu;
+constexpr int kKeepSeen = -3;  // the first successor continues a run begun in an earlier slice
 
 struct MultiArgs {
   Work w;
   TravCtl* ctl;
-  int32_t* q[2];
-  uint32_t* arr;             // [nsrc][nv] arrival of v for source s (kNoArrival: unreached)
-  uint32_t* prev;            // [nsrc][nv] arrival at which v was last enqueued for s
+  int32_t* q[2];             // sparse queues (rotating with the levels)
+  int32_t* dq[2];            // wide queues
+  uint32_t* arr;             // [nv][stride] arrival of v for source s (kNoArrival: unreached)
+  uint32_t* prev;            // [nv][stride] arrival at which v was last enqueued for s
   uint64_t* F[2];            // [nv][kWords] frontier masks: level L reads F[L & 1], fills F[(L+1) & 1]
   uint32_t* dirty;           // bit per vertex: relaxed in the current level
   int32_t ndirty;
@@ -41,21 +52,30 @@ struct MultiArgs {
   int32_t* ntouched;
   uint32_t epoch;
   int32_t nsrc, nv;
+  int32_t stride;            // sources per arrival row (the state's capacity)
   int32_t nv_lists;          // vertices with an out-list (graph n)
   int32_t dense_min, level_cap;
   unsigned long long* edges;
 };
 
-// Relaxes one level of the multi-source traversal.
-__device__ __forceinline__ unsigned long long multi_relax(const GraphView& g, MultiArgs& a, const Work& w,
-                                                          const int64_t* slo, const int64_t* shi, const int32_t* q,
-                                                          int qn, int L, bool dense) {
+__device__ __forceinline__ size_t arr_at(const MultiArgs& a, int v, int s) { return (size_t)v * a.stride + s; }
+
+__device__ __forceinline__ int mask_sources(const uint64_t* F, int v) {
+  int n = 0;
+#pragma unroll
+  for (int k = 0; k < kWords; ++k) n += __popcll(__ldcg(F + (size_t)v * kWords + k));
+  return n;
+}
+
+// Sparse part of a level: one thread per list whose mask has fewer than kWarpSources sources
+// (the queue, or with `dense` every such list in schedule order).
+__device__ __forceinline__ unsigned long long multi_relax_sparse(const GraphView& g, MultiArgs& a, const Work& w,
+                                                                 const int64_t* slo, const int64_t* shi,
+                                                                 const int32_t* q, int qn, int L, bool dense) {
   const uint64_t* Fc = a.F[L & 1];
   uint64_t* Fn = a.F[(L + 1) & 1];
-  const size_t nv = (size_t)a.nv;
   uint64_t M[kWords], seen[kWords];
   int xcur = 0, yprev = -1;
-  constexpr int kKeepSeen = -3;  // the first successor continues a run begun in an earlier slice
   auto begin = [&](int x, int first, int, int run) {
     if (x < g.active_begin || x > g.max_label) return false;
     uint64_t any = 0;
@@ -100,9 +120,9 @@ __device__ __forceinline__ unsigned long long multi_relax(const GraphView& g, Mu
         if (t < slo[s] || t >= shi[s]) continue;
         seen[k] |= 1ull << b;
         if (!usable) continue;
-        const uint32_t ax = __ldcg(a.arr + (size_t)s * nv + xcur);
+        const uint32_t ax = __ldcg(a.arr + arr_at(a, xcur, s));
         if ((int64_t)ax > t) continue;
-        atomicMin(a.arr + (size_t)s * nv + y, (uint32_t)t);
+        atomicMin(a.arr + arr_at(a, y, s), (uint32_t)t);
         add |= 1ull << b;
       }
       if (add) {
@@ -117,27 +137,110 @@ __device__ __forceinline__ unsigned long long multi_relax(const GraphView& g, Mu
     return run_order<false, true, false, true, true>(
         g, w,
         [&](int x) {
-          uint64_t any = 0;
-#pragma unroll
-          for (int k = 0; k < kWords; ++k) any |= __ldcg(Fc + (size_t)x * kWords + k);
-          return any != 0;
+          const int n = mask_sources(Fc, x);
+          return n > 0 && n < kWarpSources;
         },
         begin, edge, [](int) {});
   }
   return drive_queue<false, true, true>(g, w, q, qn, begin, edge, [](int) {});
 }
 
-// After level L (targets F[(L+1) & 1]): clears the masks of level L's frontier (queue cq, cn), keeps
-// per dirty vertex only the sources whose arrival dropped, and appends the vertices with any such
-// source to the next queue.
-__device__ __forceinline__ void multi_scan(MultiArgs& a, const int32_t* cq, int cn, int32_t* nq, int32_t* ncnt,
-                                           int L) {
+// Wide part of a level: one warp per entry of the wide queue (entries taken from *counter).
+__device__ unsigned long long multi_relax_wide(const GraphView& g, MultiArgs& a, const int64_t* slo,
+                                               const int64_t* shi, const int32_t* dq, int dn, int32_t* counter,
+                                               int L) {
+  constexpr unsigned kFull = 0xffffffffu;
+  const uint64_t* Fc = a.F[L & 1];
+  uint64_t* Fn = a.F[(L + 1) & 1];
+  const int lane = threadIdx.x & 31;
+  DeepState deep;
+  EdgeCursor c(&deep);
+  unsigned long long edges = 0;
+  for (;;) {
+    int i = 0;
+    if (lane == 0) i = atomicAdd(counter, 1);
+    i = __shfl_sync(kFull, i, 0);
+    if (i >= dn) break;
+    const int e = __ldcg(dq + i);
+    int x = e, first = 0, run = -1;
+    if (e < 0) {
+      const SliceState& s = a.w.slices[-e - 1];
+      x = s.v;
+      first = s.first;
+      run = s.run;
+    }
+    if (x < g.active_begin || x > g.max_label) continue;
+    // Slot k of this lane is source k * 32 + lane (bit 32 * (k & 1) + lane of mask word k / 2).
+    uint32_t mine = 0, seen = 0;
+    uint32_t ax[kSlots];
+#pragma unroll
+    for (int k = 0; k < kSlots; ++k) {
+      const int s = k * 32 + lane;
+      ax[k] = kNoArrival;
+      if ((__ldcg(Fc + (size_t)x * kWords + (k >> 1)) >> (s & 63)) & 1) {
+        mine |= 1u << k;
+        ax[k] = __ldcg(a.arr + arr_at(a, x, s));
+        if (run >= 0 && __ldg(a.run_first + (size_t)run * kMaxSources + s) < first) seen |= 1u << k;
+      }
+    }
+    int count = 0;
+    if (lane == 0) {
+      int f, lead, r;
+      open_entry(g, a.w, e, c, f, count, lead, r);
+    }
+    if (__shfl_sync(kFull, count, 0) <= 0) continue;
+    int yprev = run >= 0 ? kKeepSeen : -1;
+    for (;;) {
+      int y = 0, more = 0;
+      int64_t t = 0;
+      if (lane == 0) more = c.next(g, y, t);
+      if (!__shfl_sync(kFull, more, 0)) break;
+      y = __shfl_sync(kFull, y, 0);
+      t = __shfl_sync(kFull, t, 0);
+      edges += lane == 0;
+      if (yprev == kKeepSeen) {
+        yprev = y;
+      } else if (y != yprev) {
+        seen = 0;
+        yprev = y;
+      }
+      const bool usable = y >= g.active_begin && y < g.max_vertex && t >= 0 && t < 0xFFFFFFFFll;
+      uint32_t add = 0;
+#pragma unroll
+      for (int k = 0; k < kSlots; ++k) {
+        if (!(((mine & ~seen) >> k) & 1)) continue;
+        const int s = k * 32 + lane;
+        if (t < slo[s] || t >= shi[s]) continue;
+        seen |= 1u << k;
+        if (!usable || (int64_t)ax[k] > t) continue;
+        atomicMin(a.arr + arr_at(a, y, s), (uint32_t)t);
+        add |= 1u << k;
+      }
+      if (__any_sync(kFull, add != 0)) {
+#pragma unroll
+        for (int wd = 0; wd < kWords; ++wd) {
+          const uint32_t lo = __ballot_sync(kFull, (add >> (2 * wd)) & 1);
+          const uint32_t hi = __ballot_sync(kFull, (add >> (2 * wd + 1)) & 1);
+          const uint64_t bits = (uint64_t)lo | ((uint64_t)hi << 32);
+          if (lane == 0 && bits) atomicOr((unsigned long long*)(Fn + (size_t)y * kWords + wd), (unsigned long long)bits);
+        }
+        if (lane == 0) atomicOr(&a.dirty[y >> 5], 1u << (y & 31));
+      }
+    }
+  }
+  return edges;
+}
+
+// After level L (targets F[(L+1) & 1]): clears the masks of level L's frontier (queues cq/cn and
+// cdq/cdn), keeps per dirty vertex only the sources whose arrival dropped, and appends the
+// vertices with any such source to the next sparse or wide queue by their number of sources.
+__device__ __forceinline__ void multi_scan(MultiArgs& a, const int32_t* cq, int cn, const int32_t* cdq, int cdn,
+                                           int32_t* nq, int32_t* ncnt, int32_t* ndq, int32_t* ndcnt, int L) {
   uint64_t* Fc = a.F[L & 1];
   uint64_t* Fn = a.F[(L + 1) & 1];
-  const size_t nv = (size_t)a.nv;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
-  for (int i = tid; i < cn; i += nthreads) {
-    const int e = __ldcg(cq + i);
+  for (int i = tid; i < cn + cdn; i += nthreads) {
+    const int e = i < cn ? __ldcg(cq + i) : __ldcg(cdq + i - cn);
     const int x = e >= 0 ? e : a.w.slices[-e - 1].v;
 #pragma unroll
     for (int k = 0; k < kWords; ++k) Fc[(size_t)x * kWords + k] = 0;
@@ -151,18 +254,18 @@ __device__ __forceinline__ void multi_scan(MultiArgs& a, const int32_t* cq, int 
       bits = __ldcg(a.dirty + i);
       if (bits) a.dirty[i] = 0;
     }
-    uint32_t keep_bits = 0;
-    int n = 0;
+    uint32_t keep_bits = 0, wide_bits = 0;
+    int n = 0, nw = 0;
     for (uint32_t b = bits; b; b &= b - 1) {
       const int v = i * 32 + __ffs(b) - 1;
-      bool keep = false;
+      int nkept = 0;
 #pragma unroll
       for (int k = 0; k < kWords; ++k) {
         const uint64_t m = __ldcg(Fn + (size_t)v * kWords + k);
         uint64_t kept = 0;
         for (uint64_t c = m; c; c &= c - 1) {
           const int bb = __ffsll((long long)c) - 1;
-          const size_t at = (size_t)(k * 64 + bb) * nv + v;
+          const size_t at = arr_at(a, v, k * 64 + bb);
           const uint32_t now = __ldcg(a.arr + at), before = __ldcg(a.prev + at);
           if (now < before) {
             a.prev[at] = now;
@@ -170,19 +273,31 @@ __device__ __forceinline__ void multi_scan(MultiArgs& a, const int32_t* cq, int 
           }
         }
         if (kept != m) Fn[(size_t)v * kWords + k] = kept;
-        keep |= kept != 0;
+        nkept += __popcll(kept);
       }
-      if (keep) {
+      if (nkept >= kWarpSources) {
+        wide_bits |= b & (~b + 1);
+        nw += entry_count(a.w, v);
+      } else if (nkept > 0) {
         keep_bits |= b & (~b + 1);
         n += entry_count(a.w, v);
       }
     }
     int at = warp_reserve(ncnt, n);
-    uint32_t fresh = 0;  // kept vertices this traversal has not touched before
     for (uint32_t b = keep_bits; b; b &= b - 1) {
       const int v = i * 32 + __ffs(b) - 1;
       write_entries(a.w, v, nq, at);
       at += entry_count(a.w, v);
+    }
+    at = warp_reserve(ndcnt, nw);
+    for (uint32_t b = wide_bits; b; b &= b - 1) {
+      const int v = i * 32 + __ffs(b) - 1;
+      write_entries(a.w, v, ndq, at);
+      at += entry_count(a.w, v);
+    }
+    uint32_t fresh = 0;  // kept vertices this traversal has not touched before
+    for (uint32_t b = keep_bits | wide_bits; b; b &= b - 1) {
+      const int v = i * 32 + __ffs(b) - 1;
       if (__ldcg(&a.stamp[v]) != a.epoch) fresh |= b & (~b + 1);
     }
     int tat = warp_reserve(a.ntouched, __popc(fresh));
@@ -200,30 +315,37 @@ __device__ __forceinline__ void multi_scan(MultiArgs& a, const int32_t* cq, int 
 __device__ bool multi_levels(const GraphView& g, MultiArgs& a, const int64_t* slo, const int64_t* shi,
                              unsigned long long& mine, int& levels) {
   const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
-  // The sources were seeded as level 0's relaxations: the scan turns them into level 1's queue.
-  multi_scan(a, a.q[0], 0, a.q[1], &a.ctl->cnt[1], 0);
-  if (!grid_sync(a.ctl, g)) return false;
+  TravCtl* ctl = a.ctl;
+  // The sources were seeded as level 0's relaxations: the scan turns them into level 1's queues.
+  multi_scan(a, a.q[0], 0, a.dq[0], 0, a.q[1], &ctl->cnt[1], a.dq[1], &ctl->dcnt[1], 0);
+  if (!grid_sync(ctl, g)) return false;
   int L = 1;
   for (;;) {
-    const int qn = __ldcg(&a.ctl->cnt[L % 3]);
-    if (qn == 0) break;
+    const int qn = __ldcg(&ctl->cnt[L % 3]), dn = __ldcg(&ctl->dcnt[L % 3]);
+    if (qn == 0 && dn == 0) break;
     if (L >= a.level_cap) {
       if (lead) {
         set_err(g, kErrTimeout);
-        a.ctl->status = 1;
+        ctl->status = 1;
       }
       return false;
     }
     if (lead) {
-      a.ctl->cnt[(L + 2) % 3] = 0;
-      a.ctl->next[(L + 1) % 3] = 0;
+      ctl->cnt[(L + 2) % 3] = 0;
+      ctl->next[(L + 1) % 3] = 0;
+      ctl->dcnt[(L + 2) % 3] = 0;
+      ctl->dnext[(L + 1) % 3] = 0;
     }
-    Work w = a.w;
-    w.next = &a.ctl->next[L % 3];
-    mine += multi_relax(g, a, w, slo, shi, a.q[L & 1], qn, L, qn >= a.dense_min);
-    if (!grid_sync(a.ctl, g)) return false;
-    multi_scan(a, a.q[L & 1], qn, a.q[(L + 1) & 1], &a.ctl->cnt[(L + 1) % 3], L);
-    if (!grid_sync(a.ctl, g)) return false;
+    if (dn > 0) mine += multi_relax_wide(g, a, slo, shi, a.dq[L & 1], dn, &ctl->dnext[L % 3], L);
+    if (qn > 0) {
+      Work w = a.w;
+      w.next = &ctl->next[L % 3];
+      mine += multi_relax_sparse(g, a, w, slo, shi, a.q[L & 1], qn, L, qn >= a.dense_min);
+    }
+    if (!grid_sync(ctl, g)) return false;
+    multi_scan(a, a.q[L & 1], qn, a.dq[L & 1], dn, a.q[(L + 1) & 1], &ctl->cnt[(L + 1) % 3], a.dq[(L + 1) & 1],
+               &ctl->dcnt[(L + 1) % 3], L);
+    if (!grid_sync(ctl, g)) return false;
     ++L;
   }
   levels = L;
@@ -236,7 +358,7 @@ __device__ __forceinline__ void multi_seed(MultiArgs& a, const int32_t* src, int
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nsrc; s += gridDim.x * blockDim.x) {
     const int v = __ldcg(src + s);
     const int64_t lo = __ldcg(a.lo + s);
-    a.arr[(size_t)s * a.nv + v] = (uint32_t)(lo > 0 ? lo : 0);
+    a.arr[arr_at(a, v, s)] = (uint32_t)(lo > 0 ? lo : 0);
     if (atomicExch(&a.stamp[v], a.epoch) != a.epoch) a.touched[atomicAdd(a.ntouched, 1)] = v;
     if (v < n) {
       atomicOr((unsigned long long*)(a.F[1] + (size_t)v * kWords + s / 64), (unsigned long long)(1ull << (s & 63)));
@@ -299,22 +421,33 @@ __global__ void TGA_DECODE_BOUNDS k_run_first_multi(GraphView g, const SliceStat
 
 // Back to "unreached" for every source at every vertex the traversal touched (all the entries it
 // can have set), so the next traversal starts without clearing the whole [sources][vertices] state.
-__global__ void k_multi_reset(uint32_t* arr, uint32_t* prev, int32_t nv, const int32_t* touched,
+__global__ void k_multi_reset(uint32_t* arr, uint32_t* prev, int32_t stride, const int32_t* touched,
                               const int32_t* ntouched, int32_t nsrc) {
   const int64_t total = (int64_t)(*ntouched) * nsrc;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
     const int u = touched[i / nsrc];
-    const size_t at = (size_t)(i % nsrc) * nv + u;
+    const size_t at = (size_t)u * stride + i % nsrc;
     arr[at] = kNoArrival;
     prev[at] = kNoArrival;
   }
 }
 
-__global__ void k_multi_unpack(const uint32_t* arr, int32_t* out, int64_t total) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < total) {
-    const uint32_t v = arr[i];
-    out[i] = v == kNoArrival ? INT32_MAX : (int32_t)v;
+// Arrivals of sources 0..nsrc-1 to the source-major result layout (out[s][v], INT32_MAX for
+// unreached): 32 x 32 tiles through shared memory, so both sides are read and written in rows.
+__global__ void k_multi_unpack(const uint32_t* arr, int32_t stride, int32_t nsrc, int32_t nv, int32_t* out) {
+  __shared__ uint32_t tile[32][33];
+  const int v0 = blockIdx.x * 32, s0 = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int v = v0 + r, s = s0 + threadIdx.x;
+    tile[r][threadIdx.x] = (v < nv && s < nsrc) ? arr[(size_t)v * stride + s] : kNoArrival;
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int s = s0 + r, v = v0 + threadIdx.x;
+    if (s < nsrc && v < nv) {
+      const uint32_t x = tile[threadIdx.x][r];
+      out[(size_t)s * nv + v] = x == kNoArrival ? INT32_MAX : (int32_t)x;
+    }
   }
 }
 
@@ -327,7 +460,7 @@ static int multi_buffers(GraphHandle& h, int32_t cap) {
   int rc;
   const size_t run_bytes = (size_t)std::max(h.nruns, 1) * kMaxSources * 4;
   if ((rc = h.s_q0.ensure(qcap * 4)) || (rc = h.s_q1.ensure(qcap * 4)) || (rc = h.s_cnt.ensure(sizeof(TravCtl))) ||
-      (rc = h.s_d.ensure(kMaxSources * 20 + run_bytes)))
+      (rc = h.s_d.ensure(kMaxSources * 20 + run_bytes)) || (rc = h.m_dq.ensure(2 * qcap * 4)))
     return rc;
   if (cap > h.m_cap || !h.m_clean) {
     int32_t c = std::max(h.m_cap, 32);
@@ -381,6 +514,8 @@ static int multi_prepare(GraphHandle& h, int32_t nsrc, unsigned long long* edges
   a.ctl = h.s_cnt.as<TravCtl>();
   a.q[0] = h.s_q0.as<int32_t>();
   a.q[1] = h.s_q1.as<int32_t>();
+  a.dq[0] = h.m_dq.as<int32_t>();
+  a.dq[1] = a.dq[0] + nv + (size_t)h.nslices + 1;
   a.arr = h.m_state.as<uint32_t>();
   a.prev = a.arr + (size_t)h.m_cap * nv;
   a.F[0] = h.m_mask.as<uint64_t>();
@@ -395,12 +530,13 @@ static int multi_prepare(GraphHandle& h, int32_t nsrc, unsigned long long* edges
   a.ntouched = a.touched + nv;  // the count follows the list; it outlives the shared control block
   a.nsrc = nsrc;
   a.nv = (int32_t)nv;
+  a.stride = h.m_cap;
   a.nv_lists = h.view.n;
   a.dense_min = std::max<int32_t>(h.dense_min, 1);
   a.level_cap = 1 << 20;
   a.edges = edges;
   if (h.m_pending > 0) {
-    KL(k_multi_reset, 4 * h.sm_count)(a.arr, a.prev, a.nv, a.touched, a.ntouched, h.m_pending);
+    KL(k_multi_reset, 4 * h.sm_count)(a.arr, a.prev, a.stride, a.touched, a.ntouched, h.m_pending);
     h.m_pending = 0;
   }
   TGA_CUDA_TRY(cudaMemsetAsync(a.ntouched, 0, 4, h.stream));
@@ -468,7 +604,9 @@ static int bfs_multi_batch(GraphHandle& h, int32_t nsrc, const int32_t* src, con
   int32_t levels = 0;
   TGA_TRY(multi_run(h, nsrc, edges, a, &levels));
   int32_t* out = h.s_e.as<int32_t>();
-  KL(k_multi_unpack, grid_for((int64_t)nsrc * (int64_t)nv, kBlock))(a.arr, out, (int64_t)nsrc * (int64_t)nv);
+  k_multi_unpack<<<dim3(grid_for(nv, 32), grid_for(nsrc, 32)), dim3(32, 8), 0, h.stream>>>(a.arr, a.stride, nsrc, (int32_t)nv,
+                                                                                         out);
+  ++h.timing.launches;
   if (arrival_out) TGA_CUDA_TRY(cudaMemcpyAsync(arrival_out, out, state, cudaMemcpyDeviceToHost, h.stream));
   h.timing.iterations = levels;
   return finish(h, edges);
@@ -578,7 +716,7 @@ __device__ void cc_count(const MultiArgs& a, const CcArgs& c, int n, uint32_t* s
 #pragma unroll
     for (int k = 0; k < kMaxSources / 32; ++k) {
       const int j = k * 32 + lane;
-      hit[k] = j < n && __ldcg(a.arr + (size_t)j * a.nv + u) != kNoArrival;
+      hit[k] = j < n && __ldcg(a.arr + arr_at(a, u, j)) != kNoArrival;
     }
 #pragma unroll
     for (int k = 0; k < kMaxSources / 32; ++k)
@@ -587,7 +725,7 @@ __device__ void cc_count(const MultiArgs& a, const CcArgs& c, int n, uint32_t* s
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
   for (int e = tid; e < n * n; e += nthreads) {
     const int j = e / n, i = e % n;
-    if (i < j && __ldcg(a.arr + (size_t)i * a.nv + __ldcg(c.cand + j)) != kNoArrival)
+    if (i < j && __ldcg(a.arr + arr_at(a, __ldcg(c.cand + j), i)) != kNoArrival)
       atomicOr(&c.reach_bits[j * (kMaxSources / 32) + (i >> 5)], 1u << (i & 31));
   }
   __syncthreads();
@@ -670,7 +808,7 @@ __device__ void cc_label_reset(const MultiArgs& a, const CcArgs& c, int n) {
     for (int k = 0; k < kMaxSources / 32; ++k) {
       const int j = k * 32 + lane;
       if (j < n) {
-        const size_t at = (size_t)j * a.nv + u;
+        const size_t at = arr_at(a, u, j);
         if (__ldcg(a.arr + at) != kNoArrival && __ldcg(c.comp_of + j) >= 0) best = j;
         a.arr[at] = kNoArrival;
         a.prev[at] = kNoArrival;
@@ -701,7 +839,7 @@ __global__ void TGA_DECODE_BOUNDS k_cc_batches(GraphView g, MultiArgs a, CcArgs 
       for (int s = threadIdx.x; s < kMaxSources; s += blockDim.x) c.counts[s] = 0;
       for (int e = threadIdx.x; e < kMaxSources * (kMaxSources / 32); e += blockDim.x) c.reach_bits[e] = 0;
       if (threadIdx.x == 0) {
-        for (int k = 0; k < 3; ++k) a.ctl->cnt[k] = a.ctl->next[k] = 0;
+        for (int k = 0; k < 3; ++k) a.ctl->cnt[k] = a.ctl->next[k] = a.ctl->dcnt[k] = a.ctl->dnext[k] = 0;
         *a.ntouched = 0;
       }
     }

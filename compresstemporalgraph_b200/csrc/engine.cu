@@ -50,7 +50,7 @@ GraphHandle::~GraphHandle() {
   for (DevBuf* b : {&d_graph, &d_ts, &d_gl, &d_gu, &d_gs, &d_tl, &d_tu, &d_ts_samples, &d_err, &d_deg, &d_slices,
                     &d_items, &d_slice_first, &d_slice_deep, &d_order, &d_runs, &d_run_pairs, &d_run_first, &d_long, &d_slice_ebase,
                     &d_view, &s_edges, &s_a, &s_b, &s_c, &s_d, &s_e, &s_f, &s_g, &s_q0, &s_q1, &s_cnt, &s_sum,
-                    &m_state, &m_mask, &m_dirty, &m_stamp, &m_touched})
+                    &m_state, &m_mask, &m_dirty, &m_stamp, &m_touched, &m_dq})
     b->release();
   for (auto& k : ktimers) {
     if (k.a) cudaEventDestroy(k.a);
@@ -624,7 +624,7 @@ int tga_get_info(tga_graph* g, tga_info* out) {
   // streams and index (counted at load) + work decomposition + scratch grown by the calls so far
   out->device_bytes += g->work_bytes;
   for (const DevBuf* b : {&g->s_a, &g->s_b, &g->s_c, &g->s_d, &g->s_e, &g->s_f, &g->s_g, &g->s_q0, &g->s_q1, &g->s_cnt,
-                          &g->s_sum, &g->s_edges, &g->m_state, &g->m_mask, &g->m_dirty, &g->m_stamp, &g->m_touched})
+                          &g->s_sum, &g->s_edges, &g->m_state, &g->m_mask, &g->m_dirty, &g->m_stamp, &g->m_touched, &g->m_dq})
     out->device_bytes += b->bytes;
   return TGA_OK;
 }

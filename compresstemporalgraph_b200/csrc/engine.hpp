@@ -73,10 +73,10 @@ struct GraphHandle {
   // scratch used by the algorithms
   DevBuf s_a, s_b, s_c, s_d, s_e, s_f, s_g, s_q0, s_q1, s_cnt, s_sum, s_edges;
   // multi-source traversal state kept between calls (batch.cu): arrivals | last-enqueued arrivals
-  // ([m_cap][max_vertex] each), frontier masks, dirty bits, per-vertex epoch stamps and the list of
+  // ([max_vertex][m_cap] each), the wide queues, frontier masks, dirty bits, per-vertex epoch stamps and the list of
   // vertices the last traversal touched.  With m_clean, everything is "unreached"/zero except the
   // m_pending sources' entries at the touched vertices, which the next traversal resets first.
-  DevBuf m_state, m_mask, m_dirty, m_stamp, m_touched;
+  DevBuf m_state, m_mask, m_dirty, m_stamp, m_touched, m_dq;
   int32_t m_cap = 0, m_pending = 0;
   uint32_t m_epoch = 0;
   bool m_clean = false;

@@ -19,8 +19,12 @@ struct TravCtl {
   int32_t tcnt;          // CC: vertices whose arrival became finite for the current seed
   int32_t best;          // CC: seed search minimum
   int32_t comps;         // CC: components
-  int32_t pad[3];
+  int32_t dcnt[3];       // multi-source: wide queue lengths (same rotation as cnt)
+  int32_t dnext[3];      // multi-source: wide queue work counters
+  int32_t pad[2];
 };
+// The host reads the block back into a 128-byte slot of its pinned area.
+static_assert(sizeof(TravCtl) <= 128, "TravCtl outgrew its pinned readback slot");
 
 __device__ __forceinline__ uint64_t global_ns() {
   uint64_t t;
