@@ -112,6 +112,12 @@ def _load() -> C.CDLL:
         "tga_degree": (C.c_int, [P, C.c_int64, C.c_int64, P, P]),
         "tga_color": (C.c_int, [P, C.c_int32, P, C.c_int32, P, P, C.POINTER(C.c_int32)]),
         "tga_bfs_batch": (C.c_int, [P, C.c_int32, P, P, P, P]),
+        "tga_cc_batch": (C.c_int, [P, C.c_int32, P, P, C.c_int32, P, P]),
+        "tga_cc_job_create": (C.c_int, [P, C.c_int32, C.c_int32, P]),
+        "tga_cc_job_add": (C.c_int, [P, C.c_int64, C.c_int64, P]),
+        "tga_cc_job_step": (C.c_int, [P, C.c_double, P]),
+        "tga_cc_job_take": (C.c_int, [P, C.c_int32, P, P]),
+        "tga_cc_job_destroy": (C.c_int, [P]),
         "tga_pagerank_batch": (C.c_int, [P, C.c_int32, C.c_int32, C.c_float, C.c_float, P, P, P]),
         "tga_server_create": (C.c_int, [C.c_int64, C.POINTER(P)]),
         "tga_server_add_graph": (C.c_int, [P, P, C.POINTER(C.c_int32)]),
@@ -338,6 +344,17 @@ class Graph:
         _check(_lib.tga_bfs_batch(self._h, len(src), _ptr(src), _ptr(lo), _ptr(hi), _ptr(out)))
         return out
 
+    def cc_batch(self, t_lo, t_hi, early_exit: bool = True):
+        """Connected components of many windows in one launch (tga_cc_batch): labels [n, max_vertex]
+        and component counts [n], each row equal to connected_components for that window."""
+        lo = np.ascontiguousarray(t_lo, np.int64)
+        hi = np.ascontiguousarray(t_hi, np.int64)
+        lab = np.zeros((len(lo), self.max_vertex), np.int32)
+        comps = np.zeros(len(lo), np.int32)
+        _check(_lib.tga_cc_batch(self._h, len(lo), _ptr(lo), _ptr(hi), CC_EARLY_EXIT if early_exit else 0, _ptr(lab),
+                                 _ptr(comps)))
+        return lab, comps
+
     def pagerank_batch(self, t_lo, t_hi, iters: int = 20, damping: float = 0.85, alpha: float = 0.1):
         lo = np.ascontiguousarray(t_lo, np.int64)
         hi = np.ascontiguousarray(t_hi, np.int64)
@@ -349,6 +366,45 @@ class Graph:
 # ---- served form -------------------------------------------------------------------------------
 
 Q_BFS, Q_PAGERANK, Q_CC = 0, 1, 2
+
+
+class CcJob:
+    """Resumable connected components over several windows (tga_cc_job_*): add windows, step with a
+    device-time budget, take finished windows; each window's result equals connected_components."""
+
+    def __init__(self, graph: "Graph", capacity: int = 32, early_exit: bool = True):
+        self.graph = graph
+        h = C.c_void_p()
+        _check(_lib.tga_cc_job_create(graph.handle, capacity, CC_EARLY_EXIT if early_exit else 0, C.byref(h)))
+        self._h = h
+
+    def add(self, t_lo: int, t_hi: int) -> int:
+        slot = C.c_int32()
+        _check(_lib.tga_cc_job_add(self._h, t_lo, t_hi, C.byref(slot)))
+        return slot.value
+
+    def step(self, budget_ms: float = 0.0) -> list:
+        """Runs batches for about budget_ms (<= 0: to the end); returns the finished slots."""
+        fin = C.c_uint32()
+        _check(_lib.tga_cc_job_step(self._h, budget_ms, C.byref(fin)))
+        return [s for s in range(32) if fin.value >> s & 1]
+
+    def take(self, slot: int):
+        lab = np.zeros(self.graph.max_vertex, np.int32)
+        k = C.c_int32()
+        _check(_lib.tga_cc_job_take(self._h, slot, _ptr(lab), C.byref(k)))
+        return lab, k.value
+
+    def close(self):
+        if self._h:
+            _check(_lib.tga_cc_job_destroy(self._h))
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 class Server:

@@ -20,6 +20,7 @@
 // sources lane, lane + 32, ... with their arrivals at the list's vertex held in registers, so an
 // edge costs a lane at most kSlots checks instead of one thread walking every source.
 #include <algorithm>
+#include <memory>
 #include <cstring>
 #include <vector>
 
@@ -46,7 +47,8 @@ struct MultiArgs {
   int32_t ndirty;
   const int64_t* lo;         // [nsrc] windows [lo, hi)
   const int64_t* hi;
-  const int32_t* run_first;  // [nruns][kMaxSources] list index of a cut run's first in-window edge
+  const int32_t* run_first;  // [nruns][run_stride] list index of a cut run's first in-window edge
+  int32_t run_stride;        // columns of run_first (a source s reads column scol[s])
   uint32_t* stamp;           // [nv] epoch of the traversal that last touched the vertex
   int32_t* touched;          // vertices touched by this traversal (arrival set for some source)
   int32_t* ntouched;
@@ -71,7 +73,8 @@ __device__ __forceinline__ int mask_sources(const uint64_t* F, int v) {
 // (the queue, or with `dense` every such list in schedule order).
 __device__ __forceinline__ unsigned long long multi_relax_sparse(const GraphView& g, MultiArgs& a, const Work& w,
                                                                  const int64_t* slo, const int64_t* shi,
-                                                                 const int32_t* q, int qn, int L, bool dense) {
+                                                                 const int32_t* scol, const int32_t* q, int qn, int L,
+                                                                 bool dense) {
   const uint64_t* Fc = a.F[L & 1];
   uint64_t* Fn = a.F[(L + 1) & 1];
   uint64_t M[kWords], seen[kWords];
@@ -90,12 +93,12 @@ __device__ __forceinline__ unsigned long long multi_relax_sparse(const GraphView
     yprev = -1;
     if (run >= 0) {
       // Sources whose first in-window edge of this run lies before the slice saw the run already.
-      const int32_t* rf = a.run_first + (size_t)run * kMaxSources;
+      const int32_t* rf = a.run_first + (size_t)run * a.run_stride;
 #pragma unroll
       for (int k = 0; k < kWords; ++k)
         for (uint64_t c = M[k]; c; c &= c - 1) {
           const int b = __ffsll((long long)c) - 1;
-          if (__ldg(rf + k * 64 + b) < first) seen[k] |= 1ull << b;
+          if (__ldg(rf + scol[k * 64 + b]) < first) seen[k] |= 1ull << b;
         }
       yprev = kKeepSeen;
     }
@@ -147,8 +150,8 @@ __device__ __forceinline__ unsigned long long multi_relax_sparse(const GraphView
 
 // Wide part of a level: one warp per entry of the wide queue (entries taken from *counter).
 __device__ unsigned long long multi_relax_wide(const GraphView& g, MultiArgs& a, const int64_t* slo,
-                                               const int64_t* shi, const int32_t* dq, int dn, int32_t* counter,
-                                               int L) {
+                                               const int64_t* shi, const int32_t* scol, const int32_t* dq, int dn,
+                                               int32_t* counter, int L) {
   constexpr unsigned kFull = 0xffffffffu;
   const uint64_t* Fc = a.F[L & 1];
   uint64_t* Fn = a.F[(L + 1) & 1];
@@ -180,7 +183,7 @@ __device__ unsigned long long multi_relax_wide(const GraphView& g, MultiArgs& a,
       if ((__ldcg(Fc + (size_t)x * kWords + (k >> 1)) >> (s & 63)) & 1) {
         mine |= 1u << k;
         ax[k] = __ldcg(a.arr + arr_at(a, x, s));
-        if (run >= 0 && __ldg(a.run_first + (size_t)run * kMaxSources + s) < first) seen |= 1u << k;
+        if (run >= 0 && __ldg(a.run_first + (size_t)run * a.run_stride + scol[s]) < first) seen |= 1u << k;
       }
     }
     int count = 0;
@@ -313,7 +316,7 @@ __device__ __forceinline__ void multi_scan(MultiArgs& a, const int32_t* cq, int 
 // and the dirty bits); the control block's queue and work counters must be zero.  All blocks of
 // the cooperative launch call it together; false if the launch has failed (return at once).
 __device__ bool multi_levels(const GraphView& g, MultiArgs& a, const int64_t* slo, const int64_t* shi,
-                             unsigned long long& mine, int& levels) {
+                             const int32_t* scol, unsigned long long& mine, int& levels) {
   const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
   TravCtl* ctl = a.ctl;
   // The sources were seeded as level 0's relaxations: the scan turns them into level 1's queues.
@@ -336,11 +339,11 @@ __device__ bool multi_levels(const GraphView& g, MultiArgs& a, const int64_t* sl
       ctl->dcnt[(L + 2) % 3] = 0;
       ctl->dnext[(L + 1) % 3] = 0;
     }
-    if (dn > 0) mine += multi_relax_wide(g, a, slo, shi, a.dq[L & 1], dn, &ctl->dnext[L % 3], L);
+    if (dn > 0) mine += multi_relax_wide(g, a, slo, shi, scol, a.dq[L & 1], dn, &ctl->dnext[L % 3], L);
     if (qn > 0) {
       Work w = a.w;
       w.next = &ctl->next[L % 3];
-      mine += multi_relax_sparse(g, a, w, slo, shi, a.q[L & 1], qn, L, qn >= a.dense_min);
+      mine += multi_relax_sparse(g, a, w, slo, shi, scol, a.q[L & 1], qn, L, qn >= a.dense_min);
     }
     if (!grid_sync(ctl, g)) return false;
     multi_scan(a, a.q[L & 1], qn, a.dq[L & 1], dn, a.q[(L + 1) & 1], &ctl->cnt[(L + 1) % 3], a.dq[(L + 1) & 1],
@@ -367,20 +370,23 @@ __device__ __forceinline__ void multi_seed(MultiArgs& a, const int32_t* src, int
   }
 }
 
-__device__ __forceinline__ void load_windows(const MultiArgs& a, int64_t* slo, int64_t* shi) {
+// Per-source windows and run-table columns in shared memory (source s: window s, column s).
+__device__ __forceinline__ void load_windows(const MultiArgs& a, int64_t* slo, int64_t* shi, int32_t* scol) {
   for (int s = threadIdx.x; s < kMaxSources; s += blockDim.x) {
     slo[s] = s < a.nsrc ? a.lo[s] : 0;
     shi[s] = s < a.nsrc ? a.hi[s] : 0;
+    scol[s] = s;
   }
   __syncthreads();
 }
 
 __global__ void TGA_DECODE_BOUNDS k_bfs_multi(GraphView g, MultiArgs a) {
   __shared__ int64_t slo[kMaxSources], shi[kMaxSources];
-  load_windows(a, slo, shi);
+  __shared__ int32_t scol[kMaxSources];
+  load_windows(a, slo, shi, scol);
   unsigned long long mine = 0;
   int levels = 0;
-  if (!multi_levels(g, a, slo, shi, mine, levels)) return;
+  if (!multi_levels(g, a, slo, shi, scol, mine, levels)) return;
   add_edges(a.edges, mine);
   if (blockIdx.x == 0 && threadIdx.x == 0) a.ctl->levels = levels;
 }
@@ -393,7 +399,8 @@ __global__ void k_bfs_multi_seed(MultiArgs a, const int32_t* src) { multi_seed(a
 // every source s whose window holds one of those edges.
 __global__ void TGA_DECODE_BOUNDS k_run_first_multi(GraphView g, const SliceState* slices, const RunInfo* runs,
                                                     const int2* pairs, int32_t npairs, const int64_t* lo,
-                                                    const int64_t* hi, int32_t nsrc, int32_t* run_first) {
+                                                    const int64_t* hi, int32_t nsrc, int32_t* run_first,
+                                                    int32_t stride) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= npairs) return;
   const int2 pr = pairs[p];
@@ -414,7 +421,7 @@ __global__ void TGA_DECODE_BOUNDS k_run_first_multi(GraphView g, const SliceStat
       const uint64_t bit = 1ull << (q & 63);
       if ((found[q >> 6] & bit) || t < lo[q] || t >= hi[q]) continue;
       found[q >> 6] |= bit;
-      atomicMin(&run_first[(size_t)pr.x * kMaxSources + q], i);
+      atomicMin(&run_first[(size_t)pr.x * stride + q], i);
     }
   }
 }
@@ -496,7 +503,7 @@ static int multi_runs(GraphHandle& h, int32_t nsrc) {
   KL(k_fill_i32, grid_for((int64_t)h.nruns * kMaxSources, kBlock))(drf, INT32_MAX, (int64_t)h.nruns * kMaxSources);
   KL(k_run_first_multi, grid_for(h.nrun_pairs, kBlock))(h.view, h.d_slices.as<SliceState>(), h.d_runs.as<RunInfo>(),
                                                        h.d_run_pairs.as<int2>(), h.nrun_pairs, multi_lo(h),
-                                                       multi_hi(h), nsrc, drf);
+                                                       multi_hi(h), nsrc, drf, kMaxSources);
   return TGA_OK;
 }
 
@@ -525,6 +532,7 @@ static int multi_prepare(GraphHandle& h, int32_t nsrc, unsigned long long* edges
   a.lo = multi_lo(h);
   a.hi = multi_hi(h);
   a.run_first = multi_run_table(h);
+  a.run_stride = kMaxSources;
   a.stamp = h.m_stamp.as<uint32_t>();
   a.touched = h.m_touched.as<int32_t>();
   a.ntouched = a.touched + nv;  // the count follows the list; it outlives the shared control block
@@ -621,60 +629,99 @@ static int bfs_multi_batch(GraphHandle& h, int32_t nsrc, const int32_t* src, con
 // exact reach counts, and every vertex takes the component number of the last real seed that
 // reached it.  The labels equal the sequential loop's.
 //
-// The whole loop is one cooperative launch.  Per batch: block 0 picks the candidates; all blocks
-// seed and traverse; all count the reach of each source over the touched vertices; block 0
-// validates in seed order and chooses the next K; all blocks label the touched vertices and reset
-// their arrivals.  Grid barriers separate the phases, so no batch waits for the host.  K doubles
-// while the reach of the candidates that turned out not to be seeds (traversal work thrown away)
-// stays below an eighth of the real seeds' reach plus a fixed allowance, and halves when it
-// exceeds the real seeds' reach plus that allowance.
+// The whole loop is one cooperative launch, for up to kMaxCcQueries queries (windows) at once:
+// each batch splits the kMaxSources source slots among the queries still running (query q gets a
+// contiguous range of min(K_q, kMaxSources / active) slots).  Per batch: block q picks query q's
+// candidates; all blocks seed and traverse every query's sources together; all count the reach of
+// each slot over the touched vertices and mark which candidates of a query reached which; block q
+// validates query q in seed order and chooses its next K; all blocks label the touched vertices
+// for every query and reset their arrivals.  Grid barriers separate the phases, so no batch waits
+// for the host.  K_q doubles while the reach of the candidates that turned out not to be seeds
+// (traversal work thrown away) stays below an eighth of the real seeds' reach plus a fixed
+// allowance, and halves when it exceeds the real seeds' reach plus that allowance.
+
+constexpr int kMaxCcQueries = 32;
 
 struct CcBatchState {
   int64_t total;       // reach counts so far (early-exit rule)
   int32_t v;           // candidates start here
   int32_t comp;        // components so far
   int32_t small_run;   // consecutive components smaller than 5
-  int32_t stop;        // the seed loop has ended
+  int32_t stop;        // the seed loop has ended (early exit)
+  int32_t done;        // no candidates left below the end (read by the slot allotment)
+  int32_t exhausted;   // this batch's scan reached the end (becomes `done` after validation)
   int32_t ncand;       // candidates of the current batch
-  int32_t K;           // candidates per batch
-  int32_t batches;
+  int32_t K;           // candidates wanted per batch
   int32_t pad;
 };
 
 struct CcArgs {
-  CcBatchState* st;
+  CcBatchState* st;             // [nq]
   const int32_t* deg;
-  uint8_t* reached;             // [max_vertex] labelled already
-  int32_t* label;               // [max_vertex]
-  int32_t* cand;                // sources of the current batch
-  unsigned long long* counts;   // [kMaxSources] finite arrivals per source
+  uint8_t* reached;             // [nq][max_vertex] labelled already
+  int32_t* label;               // [nq][max_vertex]
+  const int64_t* q_lo;          // [nq] windows
+  const int64_t* q_hi;
+  int32_t* cand;                // [kMaxSources] source vertex of each slot
+  unsigned long long* counts;   // [kMaxSources] finite arrivals per slot
   int32_t* comp_of;             // [kMaxSources] component of a real seed, -1 otherwise
-  uint32_t* reach_bits;         // [kMaxSources][kMaxSources / 32] pair matrix of the batch
+  uint32_t* reach_bits;         // [kMaxSources][kMaxSources / 32] slot i reached slot j's vertex
+  int32_t nq;
   int32_t end;                  // candidates lie below this vertex
   int32_t early;                // apply the early exits
   int64_t limit;                // early exit: reach total above this
+  int64_t budget_ns;            // stop at a batch boundary once the launch ran this long (0: never)
+};
+
+// Per-block view of the current batch's slot ranges.
+struct CcSlots {
+  int32_t base[kMaxCcQueries];  // first slot of query q
+  int32_t k[kMaxCcQueries];     // slots offered to query q this batch
+  int32_t n[kMaxCcQueries];     // candidates found (live slots from base)
+  int32_t total;                // live slots of the batch
 };
 
 constexpr int kCcMinK = 4;
 constexpr int64_t kCcWasteAllowance = 4096;  // reach a batch may throw away and still grow K
 
-// Block 0: the first K vertices >= st->v below end that are unreached and have outdegree > 9, in
-// order, to cand; st->ncand = their number (0 once the loop has stopped).  Each thread tests 8
-// consecutive vertices per step.
-__device__ void cc_candidates(const CcArgs& c, int32_t* s_wsum, int32_t* s_count) {
+// Every block: slot ranges of this batch from the queries' states (same result in every block).
+__device__ void cc_allot(const CcArgs& c, CcSlots& sl) {
+  if (threadIdx.x == 0) {
+    int active = 0;
+    for (int q = 0; q < c.nq; ++q) active += !__ldcg(&c.st[q].stop) && !__ldcg(&c.st[q].done);
+    const int share = active ? kMaxSources / active : 0;
+    int base = 0;
+    for (int q = 0; q < c.nq; ++q) {
+      const bool on = !__ldcg(&c.st[q].stop) && !__ldcg(&c.st[q].done);
+      sl.base[q] = base;
+      sl.k[q] = on ? min(__ldcg(&c.st[q].K), share) : 0;
+      base += sl.k[q];
+    }
+  }
+  __syncthreads();
+}
+
+// Block q: the first K vertices >= v below end that are unreached by query q and have outdegree
+// > 9, in order, to cand[base..]; st->ncand = their number, st->exhausted once the scan reached
+// the end (`done` itself changes only in the validation phase, never while blocks allot slots).
+// Each thread tests 8 consecutive vertices per step.
+__device__ void cc_candidates(const CcArgs& c, int q, int base, int K, int64_t nv, int32_t* s_wsum,
+                              int32_t* s_count) {
   constexpr int kPer = 8;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int K = __ldcg(&c.st->K);
+  CcBatchState* st = c.st + q;
+  const uint8_t* reached = c.reached + (size_t)q * nv;
   if (threadIdx.x == 0) *s_count = 0;
   __syncthreads();
-  if (!__ldcg(&c.st->stop)) {
-    for (int64_t base = __ldcg(&c.st->v); base < c.end; base += (int64_t)kBlock * kPer) {
-      const int64_t u0 = base + (int64_t)threadIdx.x * kPer;
+  bool exhausted = true;
+  if (K > 0) {
+    for (int64_t b0 = __ldcg(&st->v); b0 < c.end; b0 += (int64_t)kBlock * kPer) {
+      const int64_t u0 = b0 + (int64_t)threadIdx.x * kPer;
       uint32_t f = 0;
 #pragma unroll
       for (int k = 0; k < kPer; ++k) {
         const int64_t u = u0 + k;
-        if (u < c.end && !__ldcg(c.reached + u) && __ldg(c.deg + u) > 9) f |= 1u << k;
+        if (u < c.end && !__ldcg(reached + u) && __ldg(c.deg + u) > 9) f |= 1u << k;
       }
       const int cnt = __popc(f);
       int incl = cnt;
@@ -690,66 +737,77 @@ __device__ void cc_candidates(const CcArgs& c, int32_t* s_wsum, int32_t* s_count
         total += s_wsum[k];
       }
       int pos = *s_count + before + incl - cnt;
-      for (uint32_t b = f; b; b &= b - 1, ++pos)
-        if (pos < K) c.cand[pos] = (int32_t)(u0 + __ffs(b) - 1);
+      for (uint32_t bb = f; bb; bb &= bb - 1, ++pos)
+        if (pos < K) c.cand[base + pos] = (int32_t)(u0 + __ffs(bb) - 1);
       __syncthreads();
       if (threadIdx.x == 0) *s_count += total;
       __syncthreads();
-      if (*s_count >= K) break;
+      if (*s_count >= K) {
+        exhausted = false;
+        break;
+      }
     }
   }
-  if (threadIdx.x == 0) c.st->ncand = min(*s_count, K);
+  if (threadIdx.x == 0) {
+    st->ncand = K > 0 ? min(*s_count, K) : 0;
+    if (K > 0 && exhausted) st->exhausted = 1;
+  }
 }
 
-// All blocks: finite arrivals per source over the touched vertices (one warp per vertex, lane l
-// reading sources l, l + 32, ...; block-local sums first), and the pair matrix of the batch:
-// bit i of reach_bits[j] set when candidate i < j reached candidate j.
-__device__ void cc_count(const MultiArgs& a, const CcArgs& c, int n, uint32_t* s_cnt) {
+// All blocks: finite arrivals per slot over the touched vertices (one warp per vertex, lane l
+// reading slots l, l + 32, ...; block-local sums first), and the pair matrix of the batch: bit i
+// of reach_bits[j] set when slot i < j of the same query reached slot j's vertex.
+__device__ void cc_count(const MultiArgs& a, const CcArgs& c, const CcSlots& sl, const int32_t* scol,
+                         uint32_t* s_cnt) {
   for (int s = threadIdx.x; s < kMaxSources; s += blockDim.x) s_cnt[s] = 0;
   __syncthreads();
   const int lane = threadIdx.x & 31;
+  const int nslots = sl.base[c.nq - 1] + sl.n[c.nq - 1];
   const int nt = __ldcg(a.ntouched);
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
   for (int i = warp; i < nt; i += nwarps) {
     const int u = __ldcg(a.touched + i);
-    uint32_t hit[kMaxSources / 32];
+    uint32_t hit[kSlots];
 #pragma unroll
-    for (int k = 0; k < kMaxSources / 32; ++k) {
+    for (int k = 0; k < kSlots; ++k) {
       const int j = k * 32 + lane;
-      hit[k] = j < n && __ldcg(a.arr + arr_at(a, u, j)) != kNoArrival;
+      hit[k] = j < nslots && __ldcg(a.arr + arr_at(a, u, j)) != kNoArrival;
     }
 #pragma unroll
-    for (int k = 0; k < kMaxSources / 32; ++k)
+    for (int k = 0; k < kSlots; ++k)
       if (hit[k]) atomicAdd(&s_cnt[k * 32 + lane], 1u);
   }
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
-  for (int e = tid; e < n * n; e += nthreads) {
-    const int j = e / n, i = e % n;
-    if (i < j && __ldcg(a.arr + arr_at(a, __ldcg(c.cand + j), i)) != kNoArrival)
+  for (int e = tid; e < nslots * nslots; e += nthreads) {
+    const int j = e / nslots, i = e % nslots;
+    const int q = scol[j];
+    if (i < j && scol[i] == q && i >= sl.base[q] && j < sl.base[q] + sl.n[q] &&
+        __ldcg(a.arr + arr_at(a, __ldcg(c.cand + j), i)) != kNoArrival)
       atomicOr(&c.reach_bits[j * (kMaxSources / 32) + (i >> 5)], 1u << (i & 31));
   }
   __syncthreads();
-  for (int s = threadIdx.x; s < n; s += blockDim.x)
+  for (int s = threadIdx.x; s < nslots; s += blockDim.x)
     if (s_cnt[s]) atomicAdd(&c.counts[s], (unsigned long long)s_cnt[s]);
 }
 
-// Block 0: candidates in seed order -- real seeds, component numbers, reach counts, the early
-// exits -- and the next batch size, from a shared copy of the pair matrix, counts and candidates.
-__device__ void cc_validate(const CcArgs& c, int n, uint32_t (*reaches)[kMaxSources / 32], uint32_t* s_cnt,
-                            int32_t* s_cand) {
+// Block q: query q's candidates in seed order -- real seeds, component numbers, reach counts, the
+// early exits -- and its next K, from a shared copy of its rows of the pair matrix.
+__device__ void cc_validate(const CcArgs& c, int q, int base, int n, uint32_t (*reaches)[kMaxSources / 32],
+                            uint32_t* s_cnt, int32_t* s_cand) {
   for (int e = threadIdx.x; e < n * (kMaxSources / 32); e += blockDim.x)
-    (&reaches[0][0])[e] = __ldcg(c.reach_bits + e);
+    (&reaches[0][0])[e] = __ldcg(c.reach_bits + (size_t)base * (kMaxSources / 32) + e);
   for (int j = threadIdx.x; j < n; j += blockDim.x) {
-    s_cnt[j] = (uint32_t)__ldcg(c.counts + j);
-    s_cand[j] = __ldcg(c.cand + j);
+    s_cnt[j] = (uint32_t)__ldcg(c.counts + base + j);
+    s_cand[j] = __ldcg(c.cand + base + j);
   }
   __syncthreads();
   if (threadIdx.x != 0) return;
-  int64_t total = __ldcg(&c.st->total);
-  int32_t v = __ldcg(&c.st->v), comp = __ldcg(&c.st->comp), small_run = __ldcg(&c.st->small_run);
-  int32_t K = __ldcg(&c.st->K);
+  CcBatchState* st = c.st + q;
+  int64_t total = __ldcg(&st->total);
+  int32_t v = __ldcg(&st->v), comp = __ldcg(&st->comp), small_run = __ldcg(&st->small_run);
+  int32_t K = __ldcg(&st->K);
   bool stop = false;
-  uint32_t real[kMaxSources / 32] = {};
+  uint32_t real[kMaxSources / 32] = {};  // bits by slot
   int checked = 0, ninvalid = 0;
   int64_t useful = 0, wasted = 0;
   for (int j = 0; j < n; ++j) {
@@ -761,7 +819,7 @@ __device__ void cc_validate(const CcArgs& c, int n, uint32_t (*reaches)[kMaxSour
       ++checked;
       ++ninvalid;
       wasted += cnt;
-      c.comp_of[j] = -1;
+      c.comp_of[base + j] = -1;
       continue;
     }
     if (c.early && total > c.limit) {
@@ -769,10 +827,10 @@ __device__ void cc_validate(const CcArgs& c, int n, uint32_t (*reaches)[kMaxSour
       break;
     }
     ++checked;
-    real[j >> 5] |= 1u << (j & 31);
+    real[(base + j) >> 5] |= 1u << ((base + j) & 31);
     useful += cnt;
     const int64_t reach = cnt - 1;  // the seed's own arrival is set before its traversal
-    c.comp_of[j] = comp++;
+    c.comp_of[base + j] = comp++;
     total += reach + 1;
     small_run = (reach + 1 < 5) ? small_run + 1 : 0;
     v = s_cand[j] + 1;
@@ -781,61 +839,85 @@ __device__ void cc_validate(const CcArgs& c, int n, uint32_t (*reaches)[kMaxSour
       break;
     }
   }
-  for (int j = checked; j < n; ++j) c.comp_of[j] = -1;
+  for (int j = checked; j < n; ++j) c.comp_of[base + j] = -1;
   if (!stop && n > 0) v = s_cand[n - 1] + 1;
   // Over the limit now: the next real seed would stop the loop before labelling anything.
   if (c.early && total > c.limit) stop = true;
   if (8 * wasted <= useful + kCcWasteAllowance) K = min(2 * K, kMaxSources);
   else if (wasted > useful + kCcWasteAllowance) K = max(kCcMinK, K / 2);
-  c.st->total = total;
-  c.st->v = v;
-  c.st->comp = comp;
-  c.st->small_run = small_run;
-  c.st->K = K;
-  if (stop) c.st->stop = 1;
+  st->total = total;
+  st->v = v;
+  st->comp = comp;
+  st->small_run = small_run;
+  st->K = K;
+  if (stop) st->stop = 1;
 }
 
-// All blocks: every touched vertex takes the component of the last real seed of the batch that
-// reached it, and its arrivals of the batch's sources go back to "unreached" (one warp per vertex).
-__device__ void cc_label_reset(const MultiArgs& a, const CcArgs& c, int n) {
+// All blocks: every touched vertex takes, for each query, the component of the query's last real
+// seed of the batch that reached it; then its arrivals of the batch go back to "unreached" (one
+// warp per vertex; lane q < nq resolves query q from the warp's 256-bit mask of real seeds).
+__device__ void cc_label_reset(const MultiArgs& a, const CcArgs& c, const CcSlots& sl) {
+  constexpr unsigned kFull = 0xffffffffu;
   const int lane = threadIdx.x & 31;
+  const int nslots = sl.base[c.nq - 1] + sl.n[c.nq - 1];
   const int nt = __ldcg(a.ntouched);
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int64_t nv = a.nv;
   for (int i = warp; i < nt; i += nwarps) {
     const int u = __ldcg(a.touched + i);
-    int best = -1;  // highest real seed j reaching u
+    uint32_t realw[kSlots];  // word k: slots k * 32 .. k * 32 + 31 that are real seeds reaching u
 #pragma unroll
-    for (int k = 0; k < kMaxSources / 32; ++k) {
+    for (int k = 0; k < kSlots; ++k) {
       const int j = k * 32 + lane;
-      if (j < n) {
+      bool r = false;
+      if (j < nslots) {
         const size_t at = arr_at(a, u, j);
-        if (__ldcg(a.arr + at) != kNoArrival && __ldcg(c.comp_of + j) >= 0) best = j;
+        r = __ldcg(a.arr + at) != kNoArrival && __ldcg(c.comp_of + j) >= 0;
         a.arr[at] = kNoArrival;
         a.prev[at] = kNoArrival;
       }
+      realw[k] = __ballot_sync(kFull, r);
     }
-    for (int o = 16; o; o >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
-    if (lane == 0 && best >= 0) {
-      c.label[u] = __ldcg(c.comp_of + best);
-      c.reached[u] = 1;
+    if (lane < c.nq && sl.n[lane] > 0) {
+      const int lo = sl.base[lane], hi = lo + sl.n[lane];  // slots [lo, hi)
+      int best = -1;
+      for (int k = (hi - 1) >> 5; k >= (lo >> 5) && best < 0; --k) {
+        uint32_t w = realw[0];
+#pragma unroll
+        for (int kk = 1; kk < kSlots; ++kk)
+          if (kk == k) w = realw[kk];
+        const int wlo = k * 32;
+        if (hi - wlo < 32) w &= (1u << (hi - wlo)) - 1;
+        if (lo > wlo) w &= ~((1u << (lo - wlo)) - 1);
+        if (w) best = wlo + 31 - __clz(w);
+      }
+      if (best >= 0) {
+        c.label[(size_t)lane * nv + u] = __ldcg(c.comp_of + best);
+        c.reached[(size_t)lane * nv + u] = 1;
+      }
     }
   }
 }
 
 __global__ void TGA_DECODE_BOUNDS k_cc_batches(GraphView g, MultiArgs a, CcArgs c) {
   __shared__ int64_t slo[kMaxSources], shi[kMaxSources];
+  __shared__ int32_t scol[kMaxSources];
   __shared__ uint32_t reaches[kMaxSources][kMaxSources / 32];
   __shared__ uint32_t s_cnt[kMaxSources];
   __shared__ int32_t s_cand[kMaxSources];
   __shared__ int32_t s_wsum[kBlock / 32], s_count;
-  load_windows(a, slo, shi);
+  __shared__ CcSlots sl;
   const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
   const uint32_t epoch0 = a.epoch;
+  const uint64_t t_start = global_ns();
   unsigned long long mine = 0;
   int levels = 0, batch = 0;
   for (;; ++batch) {
+    // Decided by one thread, read by all after the barrier: every block leaves at the same batch.
+    if (lead) a.ctl->yield = c.budget_ns > 0 && batch > 0 && (int64_t)(global_ns() - t_start) > c.budget_ns;
+    cc_allot(c, sl);
+    if (blockIdx.x < c.nq) cc_candidates(c, blockIdx.x, sl.base[blockIdx.x], sl.k[blockIdx.x], a.nv, s_wsum, &s_count);
     if (blockIdx.x == 0) {
-      cc_candidates(c, s_wsum, &s_count);
       for (int s = threadIdx.x; s < kMaxSources; s += blockDim.x) c.counts[s] = 0;
       for (int e = threadIdx.x; e < kMaxSources * (kMaxSources / 32); e += blockDim.x) c.reach_bits[e] = 0;
       if (threadIdx.x == 0) {
@@ -844,78 +926,251 @@ __global__ void TGA_DECODE_BOUNDS k_cc_batches(GraphView g, MultiArgs a, CcArgs 
       }
     }
     if (!grid_sync(a.ctl, g)) return;
-    const int n = __ldcg(&c.st->ncand);
-    if (n == 0) break;
+    // A batch left here is redone by the next launch: its candidate scan changed nothing but
+    // ncand/exhausted, which the scan recomputes from the same state.
+    if (__ldcg(&a.ctl->yield)) break;
+    // Live slots: [base_q, base_q + n_q) hold query q's candidates.
+    if (threadIdx.x == 0) {
+      int total = 0;
+      for (int q = 0; q < c.nq; ++q) {
+        sl.n[q] = __ldcg(&c.st[q].ncand);
+        total += sl.n[q];
+      }
+      sl.total = total;
+    }
+    __syncthreads();
+    if (sl.total == 0) {
+      // No window has candidates: the exhausted ones are done (no block allots slots any more).
+      if (lead)
+        for (int q = 0; q < c.nq; ++q)
+          if (__ldcg(&c.st[q].exhausted)) c.st[q].done = 1;
+      break;
+    }
+    for (int s = threadIdx.x; s < kMaxSources; s += blockDim.x) {
+      int q = 0;
+      while (q + 1 < c.nq && s >= sl.base[q + 1]) ++q;
+      const bool live = s >= sl.base[q] && s < sl.base[q] + sl.n[q];
+      slo[s] = live ? c.q_lo[q] : 0;
+      shi[s] = live ? c.q_hi[q] : 0;
+      scol[s] = live ? q : 0;
+    }
+    __syncthreads();
     a.epoch = epoch0 + (uint32_t)batch;
-    multi_seed(a, c.cand, n, a.nv_lists);
+    // Seeds: each live slot's candidate at max(lo, 0), as level 0's relaxation.
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < kMaxSources; s += gridDim.x * blockDim.x) {
+      if (shi[s] <= slo[s]) continue;
+      const int v = __ldcg(c.cand + s);
+      a.arr[arr_at(a, v, s)] = (uint32_t)(slo[s] > 0 ? slo[s] : 0);
+      if (atomicExch(&a.stamp[v], a.epoch) != a.epoch) a.touched[atomicAdd(a.ntouched, 1)] = v;
+      if (v < a.nv_lists) {
+        atomicOr((unsigned long long*)(a.F[1] + (size_t)v * kWords + s / 64), (unsigned long long)(1ull << (s & 63)));
+        atomicOr(&a.dirty[v >> 5], 1u << (v & 31));
+      }
+    }
     if (!grid_sync(a.ctl, g)) return;
     int lv = 0;
-    if (!multi_levels(g, a, slo, shi, mine, lv)) return;
+    if (!multi_levels(g, a, slo, shi, scol, mine, lv)) return;
     levels += lv;
-    cc_count(a, c, n, s_cnt);
+    cc_count(a, c, sl, scol, s_cnt);
     if (!grid_sync(a.ctl, g)) return;
-    if (blockIdx.x == 0) cc_validate(c, n, reaches, s_cnt, s_cand);
+    if (blockIdx.x < c.nq) {
+      if (threadIdx.x == 0 && __ldcg(&c.st[blockIdx.x].exhausted)) c.st[blockIdx.x].done = 1;
+      if (sl.n[blockIdx.x] > 0) cc_validate(c, blockIdx.x, sl.base[blockIdx.x], sl.n[blockIdx.x], reaches, s_cnt, s_cand);
+    }
     if (!grid_sync(a.ctl, g)) return;
-    cc_label_reset(a, c, n);
+    cc_label_reset(a, c, sl);
     if (!grid_sync(a.ctl, g)) return;
   }
   add_edges(a.edges, mine);
   if (lead) {
     a.ctl->levels = levels;
-    c.st->batches = batch;
+    a.ctl->batches = batch;
   }
 }
 
-__global__ void k_fill_windows(int64_t* lo, int64_t* hi, int64_t t_lo, int64_t t_hi) {
-  lo[threadIdx.x] = t_lo;
-  hi[threadIdx.x] = t_hi;
+__global__ void k_fill_column(int32_t* p, int32_t v, int64_t rows, int32_t stride) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < rows) p[i * stride] = v;
 }
 
-static int cc_batched(GraphHandle& h, int64_t t_lo, int64_t t_hi, int32_t flags, int32_t* label_out,
-                      int32_t* components_out) {
-  const int32_t nv = h.view.max_vertex;
-  TGA_TRY(multi_buffers(h, kMaxSources));
-  TGA_TRY(h.s_e.ensure((size_t)nv * 4 + (size_t)nv));                       // labels | reached
-  // state | counts | comp_of | pair matrix
-  TGA_TRY(h.s_f.ensure(sizeof(CcBatchState) + kMaxSources * (8 + 4) + kMaxSources * kMaxSources / 8));
-  TGA_TRY(h.begin_call());
-  unsigned long long* edges = edge_counter(h);
-  CcArgs c{};
-  c.label = h.s_e.as<int32_t>();
-  c.reached = reinterpret_cast<uint8_t*>(c.label + nv);
-  c.st = h.s_f.as<CcBatchState>();
-  c.counts = reinterpret_cast<unsigned long long*>(h.s_f.as<char>() + sizeof(CcBatchState));
+}  // namespace tga
+
+// A CC job: up to `cap` windows in flight through k_cc_batches, each in its own slot with its own
+// state, labels and run-table column.  Windows are added and taken between steps; a step runs
+// batches until its time budget is used, always stopping at a batch boundary, where every batch
+// has reset the multi-source state it used (other batched calls on the handle may run between
+// steps).
+struct tga_cc_job {
+  tga::GraphHandle* h = nullptr;
+  int32_t cap = 0, flags = 0;
+  tga::DevBuf lab;    // labels [cap][nv] | reached [cap][nv]
+  tga::DevBuf meta;   // states [cap] | lo [cap] | hi [cap] | counts | comp_of | pair matrix | run table [nruns][cap]
+  std::vector<uint8_t> used;
+  std::vector<tga::CcBatchState> st;  // host copy after the last step
+  tga::CcArgs args{};
+  int32_t* run_table = nullptr;
+  ~tga_cc_job() {
+    lab.release();
+    meta.release();
+  }
+};
+
+void tga::CcJobDeleter::operator()(tga_cc_job* j) const { delete j; }
+
+size_t tga::cc_cache_bytes(const GraphHandle& h) {
+  return h.cc_cache ? h.cc_cache->lab.bytes + h.cc_cache->meta.bytes : 0;
+}
+
+namespace tga {
+
+static int cc_job_create(GraphHandle& h, int32_t cap, int32_t flags, tga_cc_job** out) {
+  if (cap < 1 || cap > kMaxCcQueries) return fail(TGA_E_ARG, "CC job capacity must be 1..32");
+  auto j = std::make_unique<tga_cc_job>();
+  j->h = &h;
+  j->cap = cap;
+  j->flags = flags;
+  const size_t nv = (size_t)h.view.max_vertex;
+  const size_t st_bytes = (size_t)cap * sizeof(CcBatchState);
+  const size_t fixed = st_bytes + (size_t)cap * 16 + kMaxSources * (8 + 4) + kMaxSources * kMaxSources / 8;
+  TGA_TRY(j->lab.ensure((size_t)cap * nv * 5));
+  TGA_TRY(j->meta.ensure(fixed + (size_t)std::max(h.nruns, 1) * cap * 4));
+  CcArgs& c = j->args;
+  c.nq = cap;
+  c.label = j->lab.as<int32_t>();
+  c.reached = reinterpret_cast<uint8_t*>(c.label + (size_t)cap * nv);
+  c.st = j->meta.as<CcBatchState>();
+  int64_t* win = reinterpret_cast<int64_t*>(j->meta.as<char>() + st_bytes);
+  c.q_lo = win;
+  c.q_hi = win + cap;
+  c.counts = reinterpret_cast<unsigned long long*>(win + 2 * cap);
   c.comp_of = reinterpret_cast<int32_t*>(c.counts + kMaxSources);
   c.reach_bits = reinterpret_cast<uint32_t*>(c.comp_of + kMaxSources);
+  j->run_table = reinterpret_cast<int32_t*>(j->meta.as<char>() + fixed);
   c.deg = h.d_deg.as<int32_t>();
-  c.cand = multi_src(h);
-  c.end = std::min(std::min(h.view.max_label, nv), h.view.n);
+  c.cand = nullptr;  // set per step (the handle's source slots)
+  c.end = std::min(std::min(h.view.max_label, (int32_t)nv), h.view.n);
   c.early = (flags & TGA_CC_EARLY_EXIT) ? 1 : 0;
   c.limit = (int64_t)(0.8 * h.view.max_label);
-  KL(k_fill_i32, grid_for(nv, kBlock))(c.label, -1, nv);
-  TGA_CUDA_TRY(cudaMemsetAsync(c.reached, 0, (size_t)nv, h.stream));
-  CcBatchState init{};
-  init.v = std::max(h.cfg.cc_vertex_begin, 0);
-  init.K = kCcMinK;
-  std::memcpy(h.h_pinned + 64, &init, sizeof init);
-  TGA_CUDA_TRY(cudaMemcpyAsync(c.st, h.h_pinned + 64, sizeof init, cudaMemcpyHostToDevice, h.stream));
-  k_fill_windows<<<1, kMaxSources, 0, h.stream>>>(multi_lo(h), multi_hi(h), t_lo, t_hi);
-  ++h.timing.launches;
-  TGA_TRY(multi_runs(h, kMaxSources));  // one table serves every batch: all windows are the same
+  j->used.assign((size_t)cap, 0);
+  j->st.assign((size_t)cap, CcBatchState{});
+  for (auto& s0 : j->st) s0.done = 1;  // free slots take no source slots
+  TGA_CUDA_TRY(cudaMemcpyAsync(c.st, j->st.data(), st_bytes, cudaMemcpyHostToDevice, h.stream));
+  TGA_CUDA_TRY(cudaStreamSynchronize(h.stream));
+  *out = j.release();
+  return TGA_OK;
+}
+
+static int cc_job_add(tga_cc_job* j, int64_t t_lo, int64_t t_hi, int32_t* slot) {
+  GraphHandle& h = *j->h;
+  if (t_lo >= t_hi) return fail(TGA_E_ARG, "empty time window");
+  int32_t q = 0;
+  while (q < j->cap && j->used[(size_t)q]) ++q;
+  if (q == j->cap) return fail(TGA_E_AGAIN, "CC job full");
+  const size_t nv = (size_t)h.view.max_vertex;
+  CcArgs& c = j->args;
+  CcBatchState s0{};
+  s0.v = std::max(h.cfg.cc_vertex_begin, 0);
+  s0.K = kCcMinK;
+  j->st[(size_t)q] = s0;
+  // Pageable sources: each copy is staged before the call returns.
+  TGA_CUDA_TRY(cudaMemcpyAsync(c.st + q, &s0, sizeof s0, cudaMemcpyHostToDevice, h.stream));
+  TGA_CUDA_TRY(cudaMemcpyAsync(const_cast<int64_t*>(c.q_lo) + q, &t_lo, 8, cudaMemcpyHostToDevice, h.stream));
+  TGA_CUDA_TRY(cudaMemcpyAsync(const_cast<int64_t*>(c.q_hi) + q, &t_hi, 8, cudaMemcpyHostToDevice, h.stream));
+  KL(k_fill_i32, grid_for((int64_t)nv, kBlock))(c.label + (size_t)q * nv, -1, (int64_t)nv);
+  TGA_CUDA_TRY(cudaMemsetAsync(c.reached + (size_t)q * nv, 0, nv, h.stream));
+  if (h.nruns > 0) {
+    KL(k_fill_column, grid_for(h.nruns, kBlock))(j->run_table + q, INT32_MAX, h.nruns, j->cap);
+    KL(k_run_first_multi, grid_for(h.nrun_pairs, kBlock))(h.view, h.d_slices.as<SliceState>(), h.d_runs.as<RunInfo>(),
+                                                         h.d_run_pairs.as<int2>(), h.nrun_pairs, c.q_lo + q,
+                                                         c.q_hi + q, 1, j->run_table + q, j->cap);
+  }
+  TGA_CUDA_TRY(cudaGetLastError());
+  j->used[(size_t)q] = 1;
+  *slot = q;
+  return TGA_OK;
+}
+
+// Runs batches until the windows in flight are all finished or budget_ms (> 0) of device time has
+// passed.  finished (may be NULL): bit q set when slot q holds a finished window.
+static int cc_job_step(tga_cc_job* j, double budget_ms, uint32_t* finished) {
+  GraphHandle& h = *j->h;
+  TGA_TRY(multi_buffers(h, kMaxSources));
+  TGA_TRY(h.begin_call());
+  unsigned long long* edges = edge_counter(h);
   MultiArgs a;
   TGA_TRY(multi_prepare(h, kMaxSources, edges, a));
+  a.run_first = j->run_table;
+  a.run_stride = j->cap;
+  CcArgs c = j->args;
+  c.cand = multi_src(h);
+  c.budget_ns = budget_ms > 0 ? (int64_t)(budget_ms * 1e6) : 0;
   void* args[] = {&h.view, &a, &c};
   TravCtl ctl;
   TGA_TRY(multi_launch(h, (const void*)k_cc_batches, args, &ctl));
-  CcBatchState fin;
-  TGA_CUDA_TRY(cudaMemcpyAsync(h.h_pinned + 64, c.st, sizeof fin, cudaMemcpyDeviceToHost, h.stream));
-  TGA_CUDA_TRY(cudaStreamSynchronize(h.stream));
-  std::memcpy(&fin, h.h_pinned + 64, sizeof fin);
-  h.m_epoch = a.epoch + (uint32_t)std::max(fin.batches, 0);  // every batch reset its own entries
-  if (label_out) TGA_CUDA_TRY(cudaMemcpyAsync(label_out, c.label, (size_t)nv * 4, cudaMemcpyDeviceToHost, h.stream));
-  if (components_out) *components_out = fin.comp;
+  h.m_epoch = a.epoch + (uint32_t)std::max(ctl.batches, 0);  // every batch reset its own entries
+  TGA_CUDA_TRY(cudaMemcpyAsync(j->st.data(), j->args.st, (size_t)j->cap * sizeof(CcBatchState), cudaMemcpyDeviceToHost,
+                               h.stream));
   h.timing.iterations = ctl.levels;
-  return finish(h, edges);
+  const int rc = finish(h, edges);  // synchronizes the stream
+  if (rc) return rc;
+  if (finished) {
+    uint32_t f = 0;
+    for (int q = 0; q < j->cap; ++q)
+      if (j->used[(size_t)q] && (j->st[(size_t)q].stop || j->st[(size_t)q].done)) f |= 1u << q;
+    *finished = f;
+  }
+  return TGA_OK;
+}
+
+// Frees a slot whatever its state (a window left behind by a failed call).
+static int cc_job_drop(tga_cc_job* j, int32_t slot) {
+  GraphHandle& h = *j->h;
+  CcBatchState off{};
+  off.done = 1;
+  j->st[(size_t)slot] = off;
+  TGA_CUDA_TRY(cudaMemcpyAsync(j->args.st + slot, &off, sizeof off, cudaMemcpyHostToDevice, h.stream));
+  j->used[(size_t)slot] = 0;
+  return TGA_OK;
+}
+
+static int cc_job_take(tga_cc_job* j, int32_t slot, int32_t* label_out, int32_t* components_out) {
+  GraphHandle& h = *j->h;
+  if (slot < 0 || slot >= j->cap || !j->used[(size_t)slot]) return fail(TGA_E_ARG, "no window in this CC job slot");
+  const CcBatchState& s0 = j->st[(size_t)slot];
+  if (!s0.stop && !s0.done) return fail(TGA_E_AGAIN, "CC window not finished");
+  const size_t nv = (size_t)h.view.max_vertex;
+  if (label_out)
+    TGA_CUDA_TRY(cudaMemcpyAsync(label_out, j->args.label + (size_t)slot * nv, nv * 4, cudaMemcpyDeviceToHost, h.stream));
+  TGA_CUDA_TRY(cudaStreamSynchronize(h.stream));
+  if (components_out) *components_out = s0.comp;
+  j->used[(size_t)slot] = 0;
+  return TGA_OK;
+}
+
+// One-shot form: nq (<= kMaxCcQueries) windows to completion in one launch, through the handle's
+// cached job (kept between calls, so repeated calls allocate nothing).
+static int cc_multi(GraphHandle& h, int32_t nq, const int64_t* t_lo, const int64_t* t_hi, int32_t flags,
+                    int32_t* label_out, int32_t* components_out) {
+  const size_t nv = (size_t)h.view.max_vertex;
+  if (!h.cc_cache || h.cc_cache->flags != flags || h.cc_cache->cap < nq) {
+    tga_cc_job* j = nullptr;
+    h.cc_cache.reset();
+    TGA_TRY(cc_job_create(h, kMaxCcQueries, flags, &j));
+    h.cc_cache.reset(j);
+  }
+  tga_cc_job* j = h.cc_cache.get();
+  for (int q = 0; q < j->cap; ++q)
+    if (j->used[(size_t)q]) TGA_TRY(cc_job_drop(j, q));  // left over by a failed call
+  std::vector<int32_t> slots((size_t)nq);
+  for (int q = 0; q < nq; ++q) TGA_TRY(cc_job_add(j, t_lo[q], t_hi[q], &slots[(size_t)q]));
+  uint32_t fin = 0;
+  TGA_TRY(cc_job_step(j, 0.0, &fin));
+  const tga_timing t = h.timing;
+  for (int q = 0; q < nq; ++q)
+    TGA_TRY(cc_job_take(j, slots[(size_t)q], label_out ? label_out + (size_t)q * nv : nullptr,
+                        components_out ? components_out + q : nullptr));
+  h.timing = t;
+  return TGA_OK;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1096,7 +1351,8 @@ static int pagerank_multi_batch(GraphHandle& h, int32_t nq, int32_t iters, float
   if (h.nruns > 0) {
     KL(k_fill_i32, grid_for((int64_t)h.nruns * kMaxSources, kBlock))(drf, INT32_MAX, (int64_t)h.nruns * kMaxSources);
     KL(k_run_first_multi, grid_for(h.nrun_pairs, kBlock))(h.view, h.d_slices.as<SliceState>(), h.d_runs.as<RunInfo>(),
-                                                         h.d_run_pairs.as<int2>(), h.nrun_pairs, dlo, dhi, nq, drf);
+                                                         h.d_run_pairs.as<int2>(), h.nrun_pairs, dlo, dhi, nq, drf,
+                                                         kMaxSources);
   }
   const float base = (1.0f - damping) / (float)h.view.max_label;
   KL(k_fill_f32, grid_for((int64_t)vec, kBlock))(bufs[0], 1.0f / (float)nv, (int64_t)vec);
@@ -1148,7 +1404,7 @@ static int pagerank_multi_batch(GraphHandle& h, int32_t nq, int32_t iters, float
 
 int cc_seed_batches(GraphHandle& h, int64_t t_lo, int64_t t_hi, int32_t flags, int32_t* label_out,
                     int32_t* components_out) {
-  return cc_batched(h, t_lo, t_hi, flags, label_out, components_out);
+  return cc_multi(h, 1, &t_lo, &t_hi, flags, label_out, components_out);
 }
 
 }  // namespace tga
@@ -1156,6 +1412,59 @@ int cc_seed_batches(GraphHandle& h, int64_t t_lo, int64_t t_hi, int32_t flags, i
 using namespace tga;
 
 extern "C" {
+
+int tga_cc_job_create(tga_graph* g, int32_t capacity, int32_t flags, tga_cc_job** out) {
+  if (!g || !out) return fail(TGA_E_ARG, "null argument");
+  if (flags & ~TGA_CC_EARLY_EXIT) return fail(TGA_E_ARG, "tga_cc_job_create: only TGA_CC_EARLY_EXIT applies");
+  return cc_job_create(*g, capacity, flags, out);
+}
+
+int tga_cc_job_add(tga_cc_job* j, int64_t t_lo, int64_t t_hi, int32_t* slot) {
+  if (!j || !slot) return fail(TGA_E_ARG, "null argument");
+  return cc_job_add(j, t_lo, t_hi, slot);
+}
+
+int tga_cc_job_step(tga_cc_job* j, double budget_ms, uint32_t* finished) {
+  if (!j) return fail(TGA_E_ARG, "null job");
+  return cc_job_step(j, budget_ms, finished);
+}
+
+int tga_cc_job_take(tga_cc_job* j, int32_t slot, int32_t* label_out, int32_t* components_out) {
+  if (!j) return fail(TGA_E_ARG, "null job");
+  return cc_job_take(j, slot, label_out, components_out);
+}
+
+int tga_cc_job_destroy(tga_cc_job* j) {
+  if (!j) return fail(TGA_E_ARG, "null job");
+  cudaStreamSynchronize(j->h->stream);
+  delete j;
+  return TGA_OK;
+}
+
+int tga_cc_batch(tga_graph* g, int32_t nq, const int64_t* t_lo, const int64_t* t_hi, int32_t flags,
+                 int32_t* label_out, int32_t* components_out) {
+  if (!g || nq < 0 || (nq && (!t_lo || !t_hi))) return fail(TGA_E_ARG, "bad argument");
+  if (flags & ~TGA_CC_EARLY_EXIT) return fail(TGA_E_ARG, "tga_cc_batch: only TGA_CC_EARLY_EXIT applies");
+  GraphHandle& h = *g;
+  const size_t nv = (size_t)h.view.max_vertex;
+  for (int32_t i = 0; i < nq; ++i)
+    if (t_lo[i] >= t_hi[i]) return fail(TGA_E_ARG, "empty time window");
+  tga_timing total{};
+  for (int32_t b = 0; b < nq; b += kMaxCcQueries) {
+    const int32_t k = std::min(kMaxCcQueries, nq - b);
+    const int rc = cc_multi(h, k, t_lo + b, t_hi + b, flags, label_out ? label_out + (size_t)b * nv : nullptr,
+                            components_out ? components_out + b : nullptr);
+    if (rc) return rc;
+    total.total_ms += h.timing.total_ms;
+    total.decode_ms += h.timing.decode_ms;
+    total.decode_launches += h.timing.decode_launches;
+    total.edges_decoded += h.timing.edges_decoded;
+    total.iterations += h.timing.iterations;
+    total.launches += h.timing.launches;
+  }
+  h.timing = total;
+  return TGA_OK;
+}
 
 int tga_bfs_batch(tga_graph* g, int32_t nsrc, const int32_t* src, const int64_t* t_lo, const int64_t* t_hi,
                   int32_t* arrival_out) {

@@ -626,6 +626,7 @@ int tga_get_info(tga_graph* g, tga_info* out) {
   for (const DevBuf* b : {&g->s_a, &g->s_b, &g->s_c, &g->s_d, &g->s_e, &g->s_f, &g->s_g, &g->s_q0, &g->s_q1, &g->s_cnt,
                           &g->s_sum, &g->s_edges, &g->m_state, &g->m_mask, &g->m_dirty, &g->m_stamp, &g->m_touched, &g->m_dq})
     out->device_bytes += b->bytes;
+  out->device_bytes += cc_cache_bytes(*g);
   return TGA_OK;
 }
 

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -33,6 +34,10 @@ struct DevBuf {
 
 struct KernelTimer {
   cudaEvent_t a = nullptr, b = nullptr;
+};
+
+struct CcJobDeleter {
+  void operator()(tga_cc_job* j) const;
 };
 
 struct GraphHandle {
@@ -77,6 +82,8 @@ struct GraphHandle {
   // vertices the last traversal touched.  With m_clean, everything is "unreached"/zero except the
   // m_pending sources' entries at the touched vertices, which the next traversal resets first.
   DevBuf m_state, m_mask, m_dirty, m_stamp, m_touched, m_dq;
+  // connected-components job reused by tga_cc / tga_cc_batch (batch.cu)
+  std::unique_ptr<tga_cc_job, CcJobDeleter> cc_cache;
   int32_t m_cap = 0, m_pending = 0;
   uint32_t m_epoch = 0;
   bool m_clean = false;
@@ -117,6 +124,9 @@ int compute_max_timestamp(GraphHandle& h);
 inline bool window_covers_all(const GraphHandle& h, int64_t lo, int64_t hi) {
   return lo <= h.view.min_ts && hi > h.max_ts;
 }
+
+// Device bytes held by the handle's cached connected-components job (batch.cu).
+size_t cc_cache_bytes(const GraphHandle& h);
 
 // Connected components with seeds run as speculative batches of a multi-source traversal
 // (batch.cu); same results as the one-seed-at-a-time loop.

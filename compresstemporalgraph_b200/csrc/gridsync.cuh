@@ -21,7 +21,8 @@ struct TravCtl {
   int32_t comps;         // CC: components
   int32_t dcnt[3];       // multi-source: wide queue lengths (same rotation as cnt)
   int32_t dnext[3];      // multi-source: wide queue work counters
-  int32_t pad[2];
+  int32_t yield;         // batched CC: the launch's time budget ran out (stop at this batch)
+  int32_t batches;       // batched CC: batches run by the launch
 };
 // The host reads the block back into a 128-byte slot of its pinned area.
 static_assert(sizeof(TravCtl) <= 128, "TravCtl outgrew its pinned readback slot");

@@ -3,10 +3,12 @@
 // One worker thread per graph repeatedly takes the queries that arrived since its last round,
 // admits them while the device working memory they need fits the server's budget (shared by all
 // graphs), and runs them together: the BFS queries as one batched traversal (tga_bfs_batch), the
-// PageRank queries with equal iteration counts as one strided vector (tga_pagerank_batch), and CC
-// queries one by one.  Queries that arrive during a round join the next one, and each graph's work
-// runs on that graph's own stream, so rounds of different graphs overlap on the device.  Latency
-// is measured from tga_submit to the moment the result is in the caller's buffer.
+// PageRank queries with equal iteration counts as one strided vector (tga_pagerank_batch).  CC
+// queries join the graph's resumable CC job (tga_cc_job_*, up to 32 windows in flight): each round
+// advances it by one time slice, so a long CC never holds back the short queries that arrive
+// meanwhile, and every window is published the moment it finishes.  Each graph's work runs on that
+// graph's own stream, so rounds of different graphs overlap on the device.  Latency is measured
+// from tga_submit to the moment the result is in the caller's buffer.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -46,7 +48,13 @@ struct GraphSlot {
   int32_t nv = 0;
   std::deque<Pending> pending;
   std::thread worker;
+  tga_cc_job* cc = nullptr;                 // created at the first CC query
+  std::vector<Pending> cc_slot;             // query in each job slot (ticket 0: free)
+  std::deque<Pending> cc_waiting;           // admitted CC queries waiting for a free job slot
 };
+
+constexpr int32_t kCcJobWindows = 32;
+constexpr double kCcSliceMs = 15.0;         // device time per CC job step between rounds
 
 // Device working bytes of one query (per vertex of its graph): BFS arrival + last-enqueued arrival
 // + result; PageRank three rank vectors + inverse degree + result; CC the single traversal's arrays.
@@ -73,16 +81,16 @@ struct tga_server {
 
   void worker(GraphSlot* slot);
   void run_round(GraphSlot* slot, std::vector<Pending>& round);
-  void publish(const std::vector<Pending>& round, const std::vector<size_t>& idx, const std::vector<int>& status);
+  void step_cc(GraphSlot* slot);
+  void publish(const std::vector<const Pending*>& done, const std::vector<int>& status);
 };
 
-// Records the outcome of the queries round[idx[k]] (status[k]) and releases their budget.
-void tga_server::publish(const std::vector<Pending>& round, const std::vector<size_t>& idx,
-                         const std::vector<int>& status) {
+// Records the outcome of the queries done[k] (status[k]) and releases their budget.
+void tga_server::publish(const std::vector<const Pending*>& done, const std::vector<int>& status) {
   const Clock::time_point now = Clock::now();
   std::lock_guard<std::mutex> lk(mu);
-  for (size_t k = 0; k < idx.size(); ++k) {
-    const Pending& p = round[idx[k]];
+  for (size_t k = 0; k < done.size(); ++k) {
+    const Pending& p = *done[k];
     Outcome& o = outcomes[p.ticket];
     o.status = status[k];
     o.latency_ms = std::chrono::duration<double, std::milli>(now - p.submitted).count();
@@ -94,7 +102,7 @@ void tga_server::publish(const std::vector<Pending>& round, const std::vector<si
       ++failed;
     }
   }
-  running -= (int64_t)idx.size();
+  running -= (int64_t)done.size();
   last_done = now;
   done_cv.notify_all();
   work_cv.notify_all();
@@ -104,22 +112,22 @@ void tga_server::run_round(GraphSlot* slot, std::vector<Pending>& round) {
   const size_t nv = (size_t)slot->nv;
   // BFS: one batched traversal; results published as soon as it is done.
   {
-    std::vector<size_t> idx;
+    std::vector<const Pending*> done;
     std::vector<int32_t> src;
     std::vector<int64_t> lo, hi;
-    for (size_t i = 0; i < round.size(); ++i)
-      if (round[i].q.kind == TGA_Q_BFS) {
-        idx.push_back(i);
-        src.push_back(round[i].q.src);
-        lo.push_back(round[i].q.t_lo);
-        hi.push_back(round[i].q.t_hi);
+    for (const Pending& p : round)
+      if (p.q.kind == TGA_Q_BFS) {
+        done.push_back(&p);
+        src.push_back(p.q.src);
+        lo.push_back(p.q.t_lo);
+        hi.push_back(p.q.t_hi);
       }
-    if (!idx.empty()) {
-      std::vector<int32_t> out(idx.size() * nv);
-      const int rc = tga_bfs_batch(slot->g, (int32_t)idx.size(), src.data(), lo.data(), hi.data(), out.data());
-      for (size_t k = 0; k < idx.size(); ++k)
-        if (rc == TGA_OK && round[idx[k]].q.out) std::memcpy(round[idx[k]].q.out, out.data() + k * nv, nv * 4);
-      publish(round, idx, std::vector<int>(idx.size(), rc));
+    if (!done.empty()) {
+      std::vector<int32_t> out(done.size() * nv);
+      const int rc = tga_bfs_batch(slot->g, (int32_t)done.size(), src.data(), lo.data(), hi.data(), out.data());
+      for (size_t k = 0; k < done.size(); ++k)
+        if (rc == TGA_OK && done[k]->q.out) std::memcpy(done[k]->q.out, out.data() + k * nv, nv * 4);
+      publish(done, std::vector<int>(done.size(), rc));
     }
   }
   // PageRank: one strided batch per iteration count.
@@ -131,38 +139,95 @@ void tga_server::run_round(GraphSlot* slot, std::vector<Pending>& round) {
         if (std::find(iters_seen.begin(), iters_seen.end(), it) == iters_seen.end()) iters_seen.push_back(it);
       }
     for (int32_t it : iters_seen) {
-      std::vector<size_t> idx;
+      std::vector<const Pending*> done;
       std::vector<int64_t> lo, hi;
-      for (size_t i = 0; i < round.size(); ++i) {
-        const tga_query& q = round[i].q;
-        if (q.kind == TGA_Q_PAGERANK && (q.iters > 0 ? q.iters : 0) == it) {
-          idx.push_back(i);
-          lo.push_back(q.t_lo);
-          hi.push_back(q.t_hi);
+      for (const Pending& p : round)
+        if (p.q.kind == TGA_Q_PAGERANK && (p.q.iters > 0 ? p.q.iters : 0) == it) {
+          done.push_back(&p);
+          lo.push_back(p.q.t_lo);
+          hi.push_back(p.q.t_hi);
         }
-      }
-      std::vector<float> out(idx.size() * nv);
-      const int rc = tga_pagerank_batch(slot->g, (int32_t)idx.size(), it, 0.85f, 0.1f, lo.data(), hi.data(), out.data());
-      for (size_t k = 0; k < idx.size(); ++k)
-        if (rc == TGA_OK && round[idx[k]].q.out) std::memcpy(round[idx[k]].q.out, out.data() + k * nv, nv * 4);
-      publish(round, idx, std::vector<int>(idx.size(), rc));
+      std::vector<float> out(done.size() * nv);
+      const int rc = tga_pagerank_batch(slot->g, (int32_t)done.size(), it, 0.85f, 0.1f, lo.data(), hi.data(), out.data());
+      for (size_t k = 0; k < done.size(); ++k)
+        if (rc == TGA_OK && done[k]->q.out) std::memcpy(done[k]->q.out, out.data() + k * nv, nv * 4);
+      publish(done, std::vector<int>(done.size(), rc));
     }
   }
-  // CC: one traversal per query.
-  for (size_t i = 0; i < round.size(); ++i) {
-    const tga_query& q = round[i].q;
-    if (q.kind != TGA_Q_CC) continue;
-    const int rc = tga_cc(slot->g, q.t_lo, q.t_hi, TGA_CC_EARLY_EXIT, static_cast<int32_t*>(q.out), nullptr);
-    publish(round, std::vector<size_t>{i}, std::vector<int>{rc});
+  for (const Pending& p : round)
+    if (p.q.kind == TGA_Q_CC) slot->cc_waiting.push_back(p);
+}
+
+// Moves waiting CC windows into free job slots, advances the job by one slice and publishes the
+// windows that finished.  A job error fails every window in flight and drops the job.
+void tga_server::step_cc(GraphSlot* slot) {
+  std::vector<const Pending*> done;
+  std::vector<int> status;
+  std::vector<Pending> failed_now;
+  int rc = TGA_OK;
+  if (!slot->cc && !slot->cc_waiting.empty()) {
+    rc = tga_cc_job_create(slot->g, kCcJobWindows, TGA_CC_EARLY_EXIT, &slot->cc);
+    if (rc == TGA_OK) slot->cc_slot.assign(kCcJobWindows, Pending{});
   }
+  while (rc == TGA_OK && !slot->cc_waiting.empty()) {
+    int32_t s = -1;
+    const Pending& p = slot->cc_waiting.front();
+    const int arc = tga_cc_job_add(slot->cc, p.q.t_lo, p.q.t_hi, &s);
+    if (arc == TGA_E_AGAIN) break;  // job full: wait for a slot
+    if (arc != TGA_OK) {
+      rc = arc;
+      break;
+    }
+    slot->cc_slot[(size_t)s] = p;
+    slot->cc_waiting.pop_front();
+  }
+  bool inflight = false;
+  for (const Pending& p : slot->cc_slot) inflight |= p.ticket != 0;
+  uint32_t finished = 0;
+  if (rc == TGA_OK && inflight) rc = tga_cc_job_step(slot->cc, kCcSliceMs, &finished);
+  std::vector<Pending> out_list;
+  if (rc == TGA_OK) {
+    for (int32_t s = 0; s < kCcJobWindows; ++s)
+      if (finished & (1u << s)) {
+        Pending& p = slot->cc_slot[(size_t)s];
+        const int trc = tga_cc_job_take(slot->cc, s, static_cast<int32_t*>(p.q.out), nullptr);
+        out_list.push_back(p);
+        status.push_back(trc);
+        p = Pending{};
+      }
+  } else {
+    for (Pending& p : slot->cc_slot)
+      if (p.ticket != 0) {
+        out_list.push_back(p);
+        status.push_back(rc);
+        p = Pending{};
+      }
+    while (!slot->cc_waiting.empty()) {
+      out_list.push_back(slot->cc_waiting.front());
+      status.push_back(rc);
+      slot->cc_waiting.pop_front();
+    }
+    if (slot->cc) tga_cc_job_destroy(slot->cc);
+    slot->cc = nullptr;
+  }
+  for (const Pending& p : out_list) done.push_back(&p);
+  if (!done.empty()) publish(done, status);
+}
+
+static bool cc_busy(const GraphSlot* slot) {
+  if (!slot->cc_waiting.empty()) return true;
+  for (const Pending& p : slot->cc_slot)
+    if (p.ticket != 0) return true;
+  return false;
 }
 
 void tga_server::worker(GraphSlot* slot) {
   std::unique_lock<std::mutex> lk(mu);
   for (;;) {
-    work_cv.wait(lk, [&] { return stopping || !slot->pending.empty(); });
-    if (slot->pending.empty()) {
-      if (stopping) return;
+    // CC windows in flight keep the worker going without waiting for new queries.
+    work_cv.wait(lk, [&] { return stopping || !slot->pending.empty() || cc_busy(slot); });
+    if (slot->pending.empty() && !cc_busy(slot)) {
+      if (stopping) break;
       continue;
     }
     // Admit queued queries while they fit the budget (at least one when nothing else runs).
@@ -174,7 +239,7 @@ void tga_server::worker(GraphSlot* slot) {
       round.push_back(p);
       slot->pending.pop_front();
     }
-    if (round.empty()) {  // the budget is held by other graphs: wait until some is released
+    if (round.empty() && !cc_busy(slot)) {  // the budget is held by other graphs: wait until some is released
       work_cv.wait(lk);
       continue;
     }
@@ -182,8 +247,12 @@ void tga_server::worker(GraphSlot* slot) {
     running += (int64_t)round.size();
     lk.unlock();
     run_round(slot, round);
+    step_cc(slot);
     lk.lock();
   }
+  lk.unlock();
+  if (slot->cc) tga_cc_job_destroy(slot->cc);
+  slot->cc = nullptr;
 }
 
 using tga::fail;

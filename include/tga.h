@@ -199,6 +199,30 @@ int tga_color(tga_graph* g, int32_t prio_mode, const uint32_t* prio_in, int32_t 
 int tga_bfs_batch(tga_graph* g, int32_t nsrc, const int32_t* src, const int64_t* t_lo, const int64_t* t_hi,
                   int32_t* arrival_out);
 
+/* Many connected-components queries (one per window [t_lo[i], t_hi[i])) in one launch: up to 32
+ * windows share the 256 source slots of each speculative seed batch, every window keeping its own
+ * candidates, validation, early exits and labels; larger counts run as several launches.
+ * label_out is nq x max_vertex (row i = window i), components_out[nq]; each row equals tga_cc's
+ * result for that window.  flags: TGA_CC_EARLY_EXIT only. */
+int tga_cc_batch(tga_graph* g, int32_t nq, const int64_t* t_lo, const int64_t* t_hi, int32_t flags,
+                 int32_t* label_out, int32_t* components_out);
+
+/* Resumable connected components for continuous batching: a job holds up to `capacity` (<= 32)
+ * windows in flight, each in a slot.  tga_cc_job_add puts a window in a free slot (TGA_E_AGAIN when
+ * none is free); tga_cc_job_step runs speculative seed batches for every window in flight until
+ * all are finished or about budget_ms of device time has passed (budget_ms <= 0: until finished),
+ * always stopping between batches, so other calls on the same graph may run between steps;
+ * *finished gets bit s set for each slot whose window is finished; tga_cc_job_take copies a
+ * finished window's labels (max_vertex entries, may be NULL) and component count and frees the
+ * slot.  A window's result equals tga_cc's.  The job owns its device memory and uses the graph's
+ * stream; destroy it before closing the graph. */
+typedef struct tga_cc_job tga_cc_job;
+int tga_cc_job_create(tga_graph* g, int32_t capacity, int32_t flags, tga_cc_job** out);
+int tga_cc_job_add(tga_cc_job* job, int64_t t_lo, int64_t t_hi, int32_t* slot);
+int tga_cc_job_step(tga_cc_job* job, double budget_ms, uint32_t* finished);
+int tga_cc_job_take(tga_cc_job* job, int32_t slot, int32_t* label_out, int32_t* components_out);
+int tga_cc_job_destroy(tga_cc_job* job);
+
 /* Many windowed PageRanks as one strided vector: up to 32 queries per launch (more run as several
  * launches), each list decoded once per iteration; rank_out is nq x max_vertex (row i = query i),
  * same semantics as tga_pagerank with that window. */

@@ -110,6 +110,70 @@ def test_connected_components(pairs, shape, early, one_seed):
         assert np.array_equal(lab, olab)
 
 
+@pytest.mark.parametrize("shape", ["hubs", "chains"])
+def test_cc_batch_equals_single_windows(pairs, shape):
+    """Several CC windows in one launch (slots shared between the windows, each with its own
+    candidates, early exits and labels) give every window the oracle's labels."""
+    p = pairs[shape]
+    lo0, span = p.d["params"].min_timestamp, p.d["params"].ts_span
+    rng = np.random.default_rng(21)
+    lo = lo0 + rng.integers(0, span // 2, 6)
+    hi = lo + rng.integers(span // 20, span // 2, 6)
+    lo[0], hi[0] = 0, T_MAX
+    lo[3], hi[3] = lo[2], hi[2]  # the same window twice
+    for early in (True, False):
+        lab, comps = p.g.cc_batch(lo, hi, early_exit=early)
+        for i in range(len(lo)):
+            olab, ok = p.o.cc(p.ml, p.mv, p.act, p.cfg.connected_components_vertex_begin, int(lo[i]), int(hi[i]), early)
+            assert comps[i] == ok, (i, early)
+            assert np.array_equal(lab[i], olab), (i, early)
+
+
+def test_cc_batch_more_windows_than_one_launch(pairs):
+    """35 windows run as two launches (32 + 3); each row equals the single-window call."""
+    p = pairs["hubs"]
+    lo0, span = p.d["params"].min_timestamp, p.d["params"].ts_span
+    rng = np.random.default_rng(22)
+    lo = lo0 + rng.integers(0, span // 2, 35)
+    hi = lo + rng.integers(span // 20, span // 2, 35)
+    lab, comps = p.g.cc_batch(lo, hi)
+    for i in (0, 5, 31, 32, 34):
+        one, k = p.g.connected_components(int(lo[i]), int(hi[i]))
+        assert comps[i] == k and np.array_equal(lab[i], one), i
+
+
+def test_cc_job_resumes_across_steps_and_reuses_slots(pairs):
+    """A CC job stepped with a tiny budget (one batch per step), with batched BFS and a plain CC
+    run on the handle between steps and windows added as slots free up, gives each window the
+    single-call result."""
+    p = pairs["hubs"]
+    lo0, span = p.d["params"].min_timestamp, p.d["params"].ts_span
+    rng = np.random.default_rng(23)
+    lo = [int(x) for x in lo0 + rng.integers(0, span // 2, 5)]
+    hi = [int(l + w) for l, w in zip(lo, rng.integers(span // 20, span // 2, 5))]
+    lo[0], hi[0] = 0, T_MAX
+    want = [p.g.connected_components(lo[i], hi[i], early_exit=False) for i in range(5)]
+    got, steps = {}, 0
+    with tga.CcJob(p.g, capacity=2, early_exit=False) as job:
+        slot_of = {job.add(lo[0], hi[0]): 0, job.add(lo[1], hi[1]): 1}
+        nxt = 2
+        while slot_of:
+            fin = job.step(budget_ms=1e-6)
+            steps += 1
+            p.g.bfs_batch(np.array([0, 5], np.int32), np.array([lo[2], 0], np.int64), np.array([hi[2], T_MAX], np.int64))
+            if steps == 2:
+                p.g.connected_components(lo[3], hi[3])
+            for s in fin:
+                got[slot_of.pop(s)] = job.take(s)
+                if nxt < 5:
+                    slot_of[job.add(lo[nxt], hi[nxt])] = nxt
+                    nxt += 1
+            assert steps < 100000
+    assert steps > 5  # the budget really split the work (no early exit: every window runs to the end)
+    for i in range(5):
+        assert got[i][1] == want[i][1] and np.array_equal(got[i][0], want[i][0]), i
+
+
 def test_multi_source_state_survives_other_calls(pairs):
     """The batched traversal keeps its per-source arrays between calls and resets only the
     vertices the previous traversal touched; single-source traversals, batched CC and batched
