@@ -279,18 +279,35 @@ def served_section(tga, graphs, spans, load, count):
     def pct(x, p):
         return float(x[min(len(x) - 1, int(p * (len(x) - 1) + 0.5))])
 
+    kinds = {tga.Q_BFS: "bfs", tga.Q_PAGERANK: "pagerank", tga.Q_CC: "cc"}
+
+    def by_kind(lat_ms):
+        out = {}
+        for k, name in kinds.items():
+            x = np.sort(np.array([l for l, q in zip(lat_ms, queries) if q["kind"] == k]))
+            if len(x):
+                out[name] = {"n": int(len(x)), "p50_ms": pct(x, 0.5), "p99_ms": pct(x, 0.99)}
+        return out
+
+    plain_lat = []
+    finish = 0.0
+    for at, sv in zip(arrivals, service):
+        finish = max(finish, at) + sv
+        plain_lat.append((finish - at) * 1e3)
     # 2. open loop through the server
     with tga.Server(budget_bytes=120 << 30) as srv:
         for g in graphs:
             srv.add_graph(g)
         t0 = time.perf_counter()
+        tickets = []
         for q, at in zip(queries, arrivals):
             wait = at - (time.perf_counter() - t0)
             if wait > 0:
                 time.sleep(wait)
-            srv.submit(**q)
+            tickets.append(srv.submit(**q))
         srv.drain()
         st = srv.stats()
+        served_lat = [srv.poll(t)[1] for t in tickets]
     # 3. burst
     with tga.Server(budget_bytes=120 << 30) as srv:
         for g in graphs:
@@ -307,9 +324,12 @@ def served_section(tga, graphs, spans, load, count):
             "offered_queries_per_s": rate,
             "served": {"p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
                        "rounds": st["rounds"], "burst_queries_per_s": count / burst_s,
-                       "burst_p50_ms": bst["p50_ms"], "burst_p99_ms": bst["p99_ms"]},
+                       "burst_p50_ms": bst["p50_ms"], "burst_p99_ms": bst["p99_ms"], "by_kind": by_kind(served_lat)},
             "plain": {"p50_ms": pct(lat, 0.5), "p99_ms": pct(lat, 0.99), "mean_ms": float(lat.mean()),
-                      "capacity_queries_per_s": plain_capacity}}
+                      "capacity_queries_per_s": plain_capacity, "by_kind": by_kind(plain_lat),
+                      "service_ms_by_kind": {name: float(np.mean([sv for sv, q in zip(service, queries)
+                                                                  if q["kind"] == k]) * 1e3)
+                                             for k, name in kinds.items()}}}
 
 
 def run_reference(args):

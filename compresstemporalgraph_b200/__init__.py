@@ -113,6 +113,7 @@ def _load() -> C.CDLL:
         "tga_color": (C.c_int, [P, C.c_int32, P, C.c_int32, P, P, C.POINTER(C.c_int32)]),
         "tga_bfs_batch": (C.c_int, [P, C.c_int32, P, P, P, P]),
         "tga_cc_batch": (C.c_int, [P, C.c_int32, P, P, C.c_int32, P, P]),
+        "tga_pagerank_batch_iters": (C.c_int, [P, C.c_int32, P, C.c_float, C.c_float, P, P, P]),
         "tga_cc_job_create": (C.c_int, [P, C.c_int32, C.c_int32, P]),
         "tga_cc_job_add": (C.c_int, [P, C.c_int64, C.c_int64, P]),
         "tga_cc_job_step": (C.c_int, [P, C.c_double, P]),
@@ -355,11 +356,17 @@ class Graph:
                                  _ptr(comps)))
         return lab, comps
 
-    def pagerank_batch(self, t_lo, t_hi, iters: int = 20, damping: float = 0.85, alpha: float = 0.1):
+    def pagerank_batch(self, t_lo, t_hi, iters=20, damping: float = 0.85, alpha: float = 0.1):
+        """Windowed PageRanks as one strided vector; iters is one count for all or one per query."""
         lo = np.ascontiguousarray(t_lo, np.int64)
         hi = np.ascontiguousarray(t_hi, np.int64)
         out = np.zeros((len(lo), self.max_vertex), np.float32)
-        _check(_lib.tga_pagerank_batch(self._h, len(lo), iters, damping, alpha, _ptr(lo), _ptr(hi), _ptr(out)))
+        if np.ndim(iters) == 0:
+            _check(_lib.tga_pagerank_batch(self._h, len(lo), int(iters), damping, alpha, _ptr(lo), _ptr(hi), _ptr(out)))
+        else:
+            it = np.ascontiguousarray(iters, np.int32)
+            _check(_lib.tga_pagerank_batch_iters(self._h, len(lo), _ptr(it), damping, alpha, _ptr(lo), _ptr(hi),
+                                                 _ptr(out)))
         return out
 
 

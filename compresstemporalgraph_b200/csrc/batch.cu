@@ -1175,14 +1175,18 @@ static int cc_multi(GraphHandle& h, int32_t nq, const int64_t* t_lo, const int64
 
 // ---------------------------------------------------------------------------------------------
 // Multi-query PageRank: up to kMaxRankQueries windowed PageRanks as one strided vector
-// (rank[v * kMaxRankQueries + q]), each list decoded once per iteration.  Per edge the temporal
-// weight is computed once and the contribution scattered to every query whose window holds the
-// edge (first in-window occurrence of equal consecutive successors per query, as tga_pagerank).
+// (rank[v * S + q], S the smallest power of two >= the query count), each list decoded once per
+// iteration.  Per edge the temporal weight is computed once and the contribution scattered to
+// every query whose window holds the edge (first in-window occurrence of equal consecutive
+// successors per query, as tga_pagerank).  Queries may ask for different iteration counts: the
+// batch runs the largest, each query's result is taken after its own last iteration, and from then
+// on its column is no longer scattered.
 
 constexpr int kMaxRankQueries = 32;
+constexpr int kSumParts = 128;  // blocks per query of the per-iteration sum
 
 struct PrMultiArgs {
-  const float* invdeg;       // [nv][kMaxRankQueries] 1 / in-window outdegree (windowed queries)
+  const float* invdeg;       // [nv][S] 1 / in-window outdegree (windowed queries)
   const int32_t* deg;        // outdegrees (other queries)
   const float* in;
   float* out;
@@ -1192,7 +1196,8 @@ struct PrMultiArgs {
   const int64_t* hi;
   const int32_t* run_first;  // [nruns][kMaxSources]
   uint32_t windowed;         // bit q: query q uses its in-window outdegree
-  int32_t nq, nv;
+  uint32_t active;           // bit q: query q still iterating
+  int32_t nq, nv, S;
   float damping, alpha, base;
   unsigned long long* edges;
 };
@@ -1211,7 +1216,8 @@ __global__ void TGA_DECODE_BOUNDS k_pr_multi_iter(GraphView g, Work w, PrMultiAr
     sinv[q] = (q < a.nq && a.sums_prev) ? (float)(1.0 / a.sums_prev[q]) : 1.0f;
   }
   __syncthreads();
-  const int64_t total = (int64_t)a.nv * kMaxRankQueries;
+  const size_t S = (size_t)a.S;
+  const int64_t total = (int64_t)a.nv * a.S;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x)
     a.reset[i] = a.base;
   float c0[kMaxRankQueries];
@@ -1226,9 +1232,9 @@ __global__ void TGA_DECODE_BOUNDS k_pr_multi_iter(GraphView g, Work w, PrMultiAr
 #pragma unroll
         for (int q = 0; q < kMaxRankQueries; ++q) {
           float c = 0.0f;
-          if (q < a.nq) {
-            const float inv = ((a.windowed >> q) & 1u) ? a.invdeg[(size_t)x * kMaxRankQueries + q] : inv_all;
-            if (inv > 0.0f) c = a.damping * (a.in[(size_t)x * kMaxRankQueries + q] * sinv[q]) * inv;
+          if ((a.active >> q) & 1u) {
+            const float inv = ((a.windowed >> q) & 1u) ? a.invdeg[(size_t)x * S + q] : inv_all;
+            if (inv > 0.0f) c = a.damping * (a.in[(size_t)x * S + q] * sinv[q]) * inv;
           }
           c0[q] = c;
           if (c != 0.0f) act |= 1u << q;
@@ -1264,7 +1270,7 @@ __global__ void TGA_DECODE_BOUNDS k_pr_multi_iter(GraphView g, Work w, PrMultiAr
             wgt = temporal_weight_multi(a.alpha, t);
             have_w = true;
           }
-          atomicAdd(&a.out[(size_t)y * kMaxRankQueries + q], c0[q] * wgt);
+          atomicAdd(&a.out[(size_t)y * S + q], c0[q] * wgt);
         }
         return true;
       },
@@ -1274,7 +1280,7 @@ __global__ void TGA_DECODE_BOUNDS k_pr_multi_iter(GraphView g, Work w, PrMultiAr
 
 // In-window outdegree per query (lists counted by slices), then 1/count.
 __global__ void TGA_DECODE_BOUNDS k_window_count_multi(GraphView g, Work w, const int64_t* lo, const int64_t* hi,
-                                                     int32_t nq, int32_t* cnt, unsigned long long* edges) {
+                                                     int32_t nq, int32_t S, int32_t* cnt, unsigned long long* edges) {
   __shared__ int64_t slo[kMaxRankQueries], shi[kMaxRankQueries];
   for (int q = threadIdx.x; q < kMaxRankQueries; q += blockDim.x) {
     slo[q] = q < nq ? lo[q] : 0;
@@ -1297,7 +1303,7 @@ __global__ void TGA_DECODE_BOUNDS k_window_count_multi(GraphView g, Work w, cons
       [&](int v) {
 #pragma unroll
         for (int q = 0; q < kMaxRankQueries; ++q)
-          if (q < nq && k[q]) atomicAdd(&cnt[(size_t)v * kMaxRankQueries + q], k[q]);
+          if (q < nq && k[q]) atomicAdd(&cnt[(size_t)v * S + q], k[q]);
       });
   add_edges(edges, mine);
 }
@@ -1307,32 +1313,50 @@ __global__ void k_invert_multi(const int32_t* cnt, float* inv, int64_t n) {
   if (i < n) inv[i] = cnt[i] ? 1.0f / (float)cnt[i] : 0.0f;
 }
 
-// sums[q] = sum over v of buf[v][q] (FP64), one block per query.
-__global__ void k_sums_multi(const float* buf, int32_t nv, double* sums) {
-  const int q = blockIdx.x;
+// Per-iteration sums in FP64, deterministic: block (b, q) sums query q's entries of vertices
+// b, b + kSumParts, ... into part[q][b]; then one thread per query adds its parts in order.
+__global__ void k_sums_multi_part(const float* buf, int32_t nv, int32_t S, double* part) {
+  const int q = blockIdx.y, b = blockIdx.x;
   double s = 0.0;
-  for (int v = threadIdx.x; v < nv; v += blockDim.x) s += (double)buf[(size_t)v * kMaxRankQueries + q];
+  for (int v = b * blockDim.x + threadIdx.x; v < nv; v += kSumParts * blockDim.x) s += (double)buf[(size_t)v * S + q];
   const double bs = block_sum(s);
-  if (threadIdx.x == 0) sums[q] = bs;
+  if (threadIdx.x == 0) part[q * kSumParts + b] = bs;
 }
 
-__global__ void k_pr_multi_final(const float* buf, const double* sums, int32_t nq, int32_t nv, float* out) {
+__global__ void k_sums_multi_fin(const double* part, int32_t nq, double* sums) {
+  const int q = threadIdx.x;
+  if (q >= nq) return;
+  double s = 0.0;
+  for (int b = 0; b < kSumParts; ++b) s += part[q * kSumParts + b];
+  sums[q] = s;
+}
+
+// Results of the queries in `done` (bit q): out[q][v] = buf[v][q] / sums[q].
+__global__ void k_pr_multi_final(const float* buf, const double* sums, uint32_t done, int32_t nq, int32_t nv,
+                                 int32_t S, float* out) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= (int64_t)nq * nv) return;
   const int q = (int)(i / nv), v = (int)(i % nv);
-  out[i] = (float)((double)buf[(size_t)v * kMaxRankQueries + q] / sums[q]);
+  if ((done >> q) & 1u) out[i] = (float)((double)buf[(size_t)v * S + q] / sums[q]);
 }
 
-static int pagerank_multi_batch(GraphHandle& h, int32_t nq, int32_t iters, float damping, float alpha,
+// nq (<= kMaxRankQueries) queries, query q running iters[q] (>= 1) iterations.
+static int pagerank_multi_batch(GraphHandle& h, int32_t nq, const int32_t* iters, float damping, float alpha,
                                 const int64_t* t_lo, const int64_t* t_hi, float* rank_out) {
   const size_t nv = (size_t)h.view.max_vertex;
-  const size_t vec = nv * kMaxRankQueries;
-  // s_a: 3 rank buffers | invdeg; s_b: counts; s_d: windows + sums + run table; s_e: output
+  int32_t S = 1;
+  while (S < nq) S <<= 1;
+  int32_t maxit = 0;
+  for (int q = 0; q < nq; ++q) maxit = std::max(maxit, iters[q]);
+  const size_t vec = nv * (size_t)S;
+  // s_a: 3 rank buffers | invdeg; s_b: counts; s_d: windows | sums | parts | run table; s_e: output
   TGA_TRY(h.s_a.ensure(vec * 4 * 4));
   TGA_TRY(h.s_b.ensure(vec * 4));
   const size_t run_bytes = (size_t)std::max(h.nruns, 1) * kMaxSources * 4;
   const size_t sums_off = kMaxSources * 16;
-  TGA_TRY(h.s_d.ensure(sums_off + (size_t)(iters + 1) * kMaxRankQueries * 8 + run_bytes));
+  const size_t sums_bytes = (size_t)(maxit + 1) * kMaxRankQueries * 8;
+  const size_t part_bytes = (size_t)kMaxRankQueries * kSumParts * 8;
+  TGA_TRY(h.s_d.ensure(sums_off + sums_bytes + part_bytes + run_bytes));
   TGA_TRY(h.s_e.ensure((size_t)nq * nv * 4));
   TGA_TRY(h.begin_call());
   unsigned long long* edges = edge_counter(h);
@@ -1342,7 +1366,8 @@ static int pagerank_multi_batch(GraphHandle& h, int32_t nq, int32_t iters, float
   int64_t* dlo = h.s_d.as<int64_t>();
   int64_t* dhi = dlo + kMaxSources;
   double* sums = reinterpret_cast<double*>(h.s_d.as<char>() + sums_off);
-  int32_t* drf = reinterpret_cast<int32_t*>(sums + (size_t)(iters + 1) * kMaxRankQueries);
+  double* part = reinterpret_cast<double*>(h.s_d.as<char>() + sums_off + sums_bytes);
+  int32_t* drf = reinterpret_cast<int32_t*>(h.s_d.as<char>() + sums_off + sums_bytes + part_bytes);
   TGA_CUDA_TRY(cudaMemcpyAsync(dlo, t_lo, (size_t)nq * 8, cudaMemcpyHostToDevice, h.stream));
   TGA_CUDA_TRY(cudaMemcpyAsync(dhi, t_hi, (size_t)nq * 8, cudaMemcpyHostToDevice, h.stream));
   uint32_t windowed = 0;
@@ -1361,11 +1386,12 @@ static int pagerank_multi_batch(GraphHandle& h, int32_t nq, int32_t iters, float
     TGA_CUDA_TRY(cudaMemsetAsync(cnt, 0, vec * 4, h.stream));
     const Work w = work_of(h);
     cudaEvent_t* ev = h.kernel_begin();
-    KL(k_window_count_multi, sweep_grid(h))(h.view, w, dlo, dhi, nq, cnt, edges);
+    KL(k_window_count_multi, sweep_grid(h))(h.view, w, dlo, dhi, nq, S, cnt, edges);
     h.kernel_end(ev);
     KL(k_invert_multi, grid_for((int64_t)vec, kBlock))(cnt, invdeg, (int64_t)vec);
   }
-  for (int k = 0; k < iters; ++k) {
+  float* out = h.s_e.as<float>();
+  for (int k = 0; k < maxit; ++k) {
     Work w = work_of(h);
     PrMultiArgs a{};
     a.invdeg = invdeg;
@@ -1378,8 +1404,15 @@ static int pagerank_multi_batch(GraphHandle& h, int32_t nq, int32_t iters, float
     a.hi = dhi;
     a.run_first = drf;
     a.windowed = windowed;
+    uint32_t active = 0, done = 0;
+    for (int q = 0; q < nq; ++q) {
+      if (iters[q] > k) active |= 1u << q;
+      if (iters[q] == k + 1) done |= 1u << q;
+    }
+    a.active = active;
     a.nq = nq;
     a.nv = (int32_t)nv;
+    a.S = S;
     a.damping = damping;
     a.alpha = alpha;
     a.base = base;
@@ -1387,17 +1420,17 @@ static int pagerank_multi_batch(GraphHandle& h, int32_t nq, int32_t iters, float
     cudaEvent_t* ev = h.kernel_begin();
     KL(k_pr_multi_iter, sweep_grid(h))(h.view, w, a);
     h.kernel_end(ev);
-    k_sums_multi<<<nq, kBlock, 0, h.stream>>>(a.out, (int32_t)nv, sums + (size_t)k * kMaxRankQueries);
-    ++h.timing.launches;
+    k_sums_multi_part<<<dim3(kSumParts, nq), kBlock, 0, h.stream>>>(a.out, (int32_t)nv, S, part);
+    k_sums_multi_fin<<<1, kMaxRankQueries, 0, h.stream>>>(part, nq, sums + (size_t)k * kMaxRankQueries);
+    h.timing.launches += 2;
+    if (done)
+      KL(k_pr_multi_final, grid_for((int64_t)nq * (int64_t)nv, kBlock))(a.out, sums + (size_t)k * kMaxRankQueries, done,
+                                                                        nq, (int32_t)nv, S, out);
   }
-  float* out = h.s_e.as<float>();
-  KL(k_pr_multi_final, grid_for((int64_t)nq * (int64_t)nv, kBlock))(bufs[iters % 3],
-                                                                    sums + (size_t)(iters - 1) * kMaxRankQueries, nq,
-                                                                    (int32_t)nv, out);
   if (rank_out) TGA_CUDA_TRY(cudaMemcpyAsync(rank_out, out, (size_t)nq * nv * 4, cudaMemcpyDeviceToHost, h.stream));
-  h.timing.iterations = iters;
+  h.timing.iterations = maxit;
   const int rc = finish(h, edges);
-  h.timing.compressed_bytes = (uint64_t)(iters + (windowed ? 1 : 0)) *
+  h.timing.compressed_bytes = (uint64_t)(maxit + (windowed ? 1 : 0)) *
                               (h.info.graph_bytes + h.info.timestamp_bytes + h.info.index_bytes);
   return rc;
 }
@@ -1491,18 +1524,18 @@ int tga_bfs_batch(tga_graph* g, int32_t nsrc, const int32_t* src, const int64_t*
   return TGA_OK;
 }
 
-int tga_pagerank_batch(tga_graph* g, int32_t nq, int32_t iters, float damping, float alpha, const int64_t* t_lo,
-                       const int64_t* t_hi, float* rank_out) {
-  if (!g || nq < 0 || (nq && (!t_lo || !t_hi))) return fail(TGA_E_ARG, "bad argument");
+static int pagerank_batch_all(tga_graph* g, int32_t nq, const int32_t* iters, float damping, float alpha,
+                              const int64_t* t_lo, const int64_t* t_hi, float* rank_out) {
   GraphHandle& h = *g;
-  if (iters <= 0) iters = h.cfg.pr_iters;
   for (int32_t i = 0; i < nq; ++i)
     if (t_lo[i] >= t_hi[i]) return fail(TGA_E_ARG, "empty time window");
   const size_t nv = (size_t)h.view.max_vertex;
+  std::vector<int32_t> it((size_t)nq);
+  for (int32_t i = 0; i < nq; ++i) it[(size_t)i] = iters[i] > 0 ? iters[i] : std::max(h.cfg.pr_iters, 1);
   tga_timing total{};
   for (int32_t b = 0; b < nq; b += kMaxRankQueries) {
     const int32_t k = std::min(kMaxRankQueries, nq - b);
-    const int rc = pagerank_multi_batch(h, k, iters, damping, alpha, t_lo + b, t_hi + b,
+    const int rc = pagerank_multi_batch(h, k, it.data() + b, damping, alpha, t_lo + b, t_hi + b,
                                         rank_out ? rank_out + (size_t)b * nv : nullptr);
     if (rc) return rc;
     total.total_ms += h.timing.total_ms;
@@ -1510,11 +1543,24 @@ int tga_pagerank_batch(tga_graph* g, int32_t nq, int32_t iters, float damping, f
     total.decode_launches += h.timing.decode_launches;
     total.edges_decoded += h.timing.edges_decoded;
     total.compressed_bytes += h.timing.compressed_bytes;
-    total.iterations = h.timing.iterations;
+    total.iterations = std::max(total.iterations, h.timing.iterations);
     total.launches += h.timing.launches;
   }
   h.timing = total;
   return TGA_OK;
+}
+
+int tga_pagerank_batch(tga_graph* g, int32_t nq, int32_t iters, float damping, float alpha, const int64_t* t_lo,
+                       const int64_t* t_hi, float* rank_out) {
+  if (!g || nq < 0 || (nq && (!t_lo || !t_hi))) return fail(TGA_E_ARG, "bad argument");
+  std::vector<int32_t> it((size_t)nq, iters);
+  return pagerank_batch_all(g, nq, it.data(), damping, alpha, t_lo, t_hi, rank_out);
+}
+
+int tga_pagerank_batch_iters(tga_graph* g, int32_t nq, const int32_t* iters, float damping, float alpha,
+                             const int64_t* t_lo, const int64_t* t_hi, float* rank_out) {
+  if (!g || nq < 0 || (nq && (!iters || !t_lo || !t_hi))) return fail(TGA_E_ARG, "bad argument");
+  return pagerank_batch_all(g, nq, iters, damping, alpha, t_lo, t_hi, rank_out);
 }
 
 }  // extern "C"

@@ -3,7 +3,8 @@
 // One worker thread per graph repeatedly takes the queries that arrived since its last round,
 // admits them while the device working memory they need fits the server's budget (shared by all
 // graphs), and runs them together: the BFS queries as one batched traversal (tga_bfs_batch), the
-// PageRank queries with equal iteration counts as one strided vector (tga_pagerank_batch).  CC
+// PageRank queries as one strided vector (tga_pagerank_batch_iters, each with its own iteration
+// count).  CC
 // queries join the graph's resumable CC job (tga_cc_job_*, up to 32 windows in flight): each round
 // advances it by one time slice, so a long CC never holds back the short queries that arrive
 // meanwhile, and every window is published the moment it finishes.  Each graph's work runs on that
@@ -54,7 +55,13 @@ struct GraphSlot {
 };
 
 constexpr int32_t kCcJobWindows = 32;
-constexpr double kCcSliceMs = 15.0;         // device time per CC job step between rounds
+// Windows in flight per graph.  Windows sharing a job split its source slots, so each finishes
+// later while the throughput stays about the same; a short first-come queue keeps the tail low.
+constexpr int32_t kCcInFlight = 2;
+// Device time of a CC job step: at least kCcSliceMs and kCcShare x the time the round spent on
+// the other queries, so CC keeps about two thirds of the device while its windows wait.
+constexpr double kCcSliceMs = 15.0;
+constexpr double kCcShare = 2.0;
 
 // Device working bytes of one query (per vertex of its graph): BFS arrival + last-enqueued arrival
 // + result; PageRank three rank vectors + inverse degree + result; CC the single traversal's arrays.
@@ -81,7 +88,7 @@ struct tga_server {
 
   void worker(GraphSlot* slot);
   void run_round(GraphSlot* slot, std::vector<Pending>& round);
-  void step_cc(GraphSlot* slot);
+  void step_cc(GraphSlot* slot, double budget_ms);
   void publish(const std::vector<const Pending*>& done, const std::vector<int>& status);
 };
 
@@ -130,25 +137,22 @@ void tga_server::run_round(GraphSlot* slot, std::vector<Pending>& round) {
       publish(done, std::vector<int>(done.size(), rc));
     }
   }
-  // PageRank: one strided batch per iteration count.
+  // PageRank: one strided batch, each query taken after its own iteration count.
   {
-    std::vector<int32_t> iters_seen;
+    std::vector<const Pending*> done;
+    std::vector<int32_t> iters;
+    std::vector<int64_t> lo, hi;
     for (const Pending& p : round)
       if (p.q.kind == TGA_Q_PAGERANK) {
-        const int32_t it = p.q.iters > 0 ? p.q.iters : 0;  // 0: the graph's configured count
-        if (std::find(iters_seen.begin(), iters_seen.end(), it) == iters_seen.end()) iters_seen.push_back(it);
+        done.push_back(&p);
+        iters.push_back(p.q.iters);  // <= 0: the graph's configured count
+        lo.push_back(p.q.t_lo);
+        hi.push_back(p.q.t_hi);
       }
-    for (int32_t it : iters_seen) {
-      std::vector<const Pending*> done;
-      std::vector<int64_t> lo, hi;
-      for (const Pending& p : round)
-        if (p.q.kind == TGA_Q_PAGERANK && (p.q.iters > 0 ? p.q.iters : 0) == it) {
-          done.push_back(&p);
-          lo.push_back(p.q.t_lo);
-          hi.push_back(p.q.t_hi);
-        }
+    if (!done.empty()) {
       std::vector<float> out(done.size() * nv);
-      const int rc = tga_pagerank_batch(slot->g, (int32_t)done.size(), it, 0.85f, 0.1f, lo.data(), hi.data(), out.data());
+      const int rc = tga_pagerank_batch_iters(slot->g, (int32_t)done.size(), iters.data(), 0.85f, 0.1f, lo.data(),
+                                              hi.data(), out.data());
       for (size_t k = 0; k < done.size(); ++k)
         if (rc == TGA_OK && done[k]->q.out) std::memcpy(done[k]->q.out, out.data() + k * nv, nv * 4);
       publish(done, std::vector<int>(done.size(), rc));
@@ -160,7 +164,7 @@ void tga_server::run_round(GraphSlot* slot, std::vector<Pending>& round) {
 
 // Moves waiting CC windows into free job slots, advances the job by one slice and publishes the
 // windows that finished.  A job error fails every window in flight and drops the job.
-void tga_server::step_cc(GraphSlot* slot) {
+void tga_server::step_cc(GraphSlot* slot, double budget_ms) {
   std::vector<const Pending*> done;
   std::vector<int> status;
   std::vector<Pending> failed_now;
@@ -169,7 +173,9 @@ void tga_server::step_cc(GraphSlot* slot) {
     rc = tga_cc_job_create(slot->g, kCcJobWindows, TGA_CC_EARLY_EXIT, &slot->cc);
     if (rc == TGA_OK) slot->cc_slot.assign(kCcJobWindows, Pending{});
   }
-  while (rc == TGA_OK && !slot->cc_waiting.empty()) {
+  int32_t inflight_now = 0;
+  for (const Pending& p : slot->cc_slot) inflight_now += p.ticket != 0;
+  while (rc == TGA_OK && !slot->cc_waiting.empty() && inflight_now < kCcInFlight) {
     int32_t s = -1;
     const Pending& p = slot->cc_waiting.front();
     const int arc = tga_cc_job_add(slot->cc, p.q.t_lo, p.q.t_hi, &s);
@@ -180,11 +186,12 @@ void tga_server::step_cc(GraphSlot* slot) {
     }
     slot->cc_slot[(size_t)s] = p;
     slot->cc_waiting.pop_front();
+    ++inflight_now;
   }
   bool inflight = false;
   for (const Pending& p : slot->cc_slot) inflight |= p.ticket != 0;
   uint32_t finished = 0;
-  if (rc == TGA_OK && inflight) rc = tga_cc_job_step(slot->cc, kCcSliceMs, &finished);
+  if (rc == TGA_OK && inflight) rc = tga_cc_job_step(slot->cc, budget_ms, &finished);
   std::vector<Pending> out_list;
   if (rc == TGA_OK) {
     for (int32_t s = 0; s < kCcJobWindows; ++s)
@@ -246,8 +253,10 @@ void tga_server::worker(GraphSlot* slot) {
     ++rounds;
     running += (int64_t)round.size();
     lk.unlock();
+    const Clock::time_point t0 = Clock::now();
     run_round(slot, round);
-    step_cc(slot);
+    const double other_ms = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+    step_cc(slot, std::max(kCcSliceMs, kCcShare * other_ms));
     lk.lock();
   }
   lk.unlock();

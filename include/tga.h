@@ -229,6 +229,12 @@ int tga_cc_job_destroy(tga_cc_job* job);
 int tga_pagerank_batch(tga_graph* g, int32_t nq, int32_t iters, float damping, float alpha, const int64_t* t_lo,
                        const int64_t* t_hi, float* rank_out);
 
+/* As tga_pagerank_batch with a per-query iteration count (iters[i] <= 0: the graph's pr_iters):
+ * the batch runs the largest count and takes each query's result after its own last iteration, so
+ * row i equals tga_pagerank(iters[i], ...) for that window. */
+int tga_pagerank_batch_iters(tga_graph* g, int32_t nq, const int32_t* iters, float damping, float alpha,
+                             const int64_t* t_lo, const int64_t* t_hi, float* rank_out);
+
 /* ---- served form ----------------------------------------------------------------------------
  * No counterpart in the reference.  A server keeps several opened graphs resident and answers a
  * stream of queries: one worker thread per graph takes the queries that arrived since its last

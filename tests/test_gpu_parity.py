@@ -142,6 +142,26 @@ def test_cc_batch_more_windows_than_one_launch(pairs):
         assert comps[i] == k and np.array_equal(lab[i], one), i
 
 
+@pytest.mark.parametrize("shape", ["hubs", "chains"])
+def test_pagerank_batch_mixed_iteration_counts(pairs, shape):
+    """One batch with a different iteration count per query (1, 3, 8, ...): row i equals the
+    single-query PageRank with iters[i] within the FP32 tolerance of the other batched tests."""
+    p = pairs[shape]
+    lo0, span = p.d["params"].min_timestamp, p.d["params"].ts_span
+    rng = np.random.default_rng(24)
+    nq = 7
+    lo = lo0 + rng.integers(0, span // 2, nq)
+    hi = lo + rng.integers(span // 20, span // 2, nq)
+    lo[0], hi[0] = 0, T_MAX
+    iters = np.array([1, 3, 8, 3, 5, 2, 8], np.int32)
+    out = p.g.pagerank_batch(lo, hi, iters=iters)
+    for i in range(nq):
+        one = p.g.pagerank(int(iters[i]), 0.85, 0.1, int(lo[i]), int(hi[i]))
+        assert np.allclose(out[i], one, rtol=1e-4, atol=1e-9), i
+        o = p.o.pagerank(p.ml, p.mv, p.act, int(iters[i]), 0.85, 0.1, int(lo[i]), int(hi[i]))
+        assert float(np.abs(out[i].astype(np.float64) - o).sum()) <= 1e-5, i
+
+
 def test_cc_job_resumes_across_steps_and_reuses_slots(pairs):
     """A CC job stepped with a tiny budget (one batch per step), with batched BFS and a plain CC
     run on the handle between steps and windows added as slots free up, gives each window the
