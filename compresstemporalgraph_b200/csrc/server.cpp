@@ -52,16 +52,20 @@ struct GraphSlot {
   tga_cc_job* cc = nullptr;                 // created at the first CC query
   std::vector<Pending> cc_slot;             // query in each job slot (ticket 0: free)
   std::deque<Pending> cc_waiting;           // admitted CC queries waiting for a free job slot
+  bool wants_device = false;                // has a round to run (guarded by the server mutex)
+  Clock::time_point oldest{};               // submit time of its oldest outstanding query
 };
 
 constexpr int32_t kCcJobWindows = 32;
 // Windows in flight per graph.  Windows sharing a job split its source slots, so each finishes
 // later while the throughput stays about the same; a short first-come queue keeps the tail low.
 constexpr int32_t kCcInFlight = 2;
-// Device time of a CC job step: at least kCcSliceMs and kCcShare x the time the round spent on
-// the other queries, so CC keeps about two thirds of the device while its windows wait.
+// Device time of a CC job step, by age: the step lasts until the oldest non-CC query waiting for
+// the next round would be as old as the oldest CC window (at least kCcSliceMs), or kCcIdleMs when
+// nothing else waits.  Across kinds that is first come first served, while BFS and PageRank still
+// batch within their kind.
 constexpr double kCcSliceMs = 15.0;
-constexpr double kCcShare = 2.0;
+constexpr double kCcIdleMs = 100.0;
 
 // Device working bytes of one query (per vertex of its graph): BFS arrival + last-enqueued arrival
 // + result; PageRank three rank vectors + inverse degree + result; CC the single traversal's arrays.
@@ -76,7 +80,8 @@ struct tga_server {
   int64_t budget = 0;
   int64_t in_use = 0;
   std::mutex mu;
-  std::condition_variable work_cv, done_cv;
+  std::condition_variable work_cv, done_cv, turn_cv;
+  bool device_busy = false;  // a worker is running its round (one at a time, oldest query first)
   std::vector<std::unique_ptr<GraphSlot>> graphs;
   std::unordered_map<int64_t, Outcome> outcomes;
   int64_t next_ticket = 1;
@@ -89,6 +94,7 @@ struct tga_server {
   void worker(GraphSlot* slot);
   void run_round(GraphSlot* slot, std::vector<Pending>& round);
   void step_cc(GraphSlot* slot, double budget_ms);
+  double cc_budget_ms(GraphSlot* slot);
   void publish(const std::vector<const Pending*>& done, const std::vector<int>& status);
 };
 
@@ -228,6 +234,33 @@ static bool cc_busy(const GraphSlot* slot) {
   return false;
 }
 
+double tga_server::cc_budget_ms(GraphSlot* slot) {
+  bool have_cc = false;
+  Clock::time_point cc_oldest{};
+  for (const Pending& p : slot->cc_slot)
+    if (p.ticket != 0 && (!have_cc || p.submitted < cc_oldest)) {
+      cc_oldest = p.submitted;
+      have_cc = true;
+    }
+  if (!slot->cc_waiting.empty() && (!have_cc || slot->cc_waiting.front().submitted < cc_oldest)) {
+    cc_oldest = slot->cc_waiting.front().submitted;
+    have_cc = true;
+  }
+  if (!have_cc) return kCcSliceMs;
+  std::lock_guard<std::mutex> lk(mu);
+  bool have_other = false;
+  Clock::time_point other{};
+  for (const auto& o : graphs)
+    for (const Pending& p : o->pending)  // arrival order: the first non-CC one is the oldest
+      if (p.q.kind != TGA_Q_CC) {
+        if (!have_other || p.submitted < other) other = p.submitted;
+        have_other = true;
+        break;
+      }
+  if (!have_other) return kCcIdleMs;
+  return std::max(kCcSliceMs, std::chrono::duration<double, std::milli>(other - cc_oldest).count());
+}
+
 void tga_server::worker(GraphSlot* slot) {
   std::unique_lock<std::mutex> lk(mu);
   for (;;) {
@@ -250,14 +283,31 @@ void tga_server::worker(GraphSlot* slot) {
       work_cv.wait(lk);
       continue;
     }
+    // Device turn: rounds of different graphs run one at a time, the graph holding the oldest
+    // outstanding query first, so a query is not overtaken by newer work on another graph.
+    Clock::time_point oldest = Clock::time_point::max();
+    for (const Pending& p : round) oldest = std::min(oldest, p.submitted);
+    for (const Pending& p : slot->cc_waiting) oldest = std::min(oldest, p.submitted);
+    for (const Pending& p : slot->cc_slot)
+      if (p.ticket != 0) oldest = std::min(oldest, p.submitted);
+    slot->oldest = oldest;
+    slot->wants_device = true;
+    turn_cv.wait(lk, [&] {
+      if (device_busy) return false;
+      for (const auto& o : graphs)
+        if (o.get() != slot && o->wants_device && o->oldest < slot->oldest) return false;
+      return true;
+    });
+    device_busy = true;
+    slot->wants_device = false;
     ++rounds;
     running += (int64_t)round.size();
     lk.unlock();
-    const Clock::time_point t0 = Clock::now();
     run_round(slot, round);
-    const double other_ms = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
-    step_cc(slot, std::max(kCcSliceMs, kCcShare * other_ms));
+    step_cc(slot, cc_budget_ms(slot));
     lk.lock();
+    device_busy = false;
+    turn_cv.notify_all();
   }
   lk.unlock();
   if (slot->cc) tga_cc_job_destroy(slot->cc);
