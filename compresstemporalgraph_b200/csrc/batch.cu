@@ -70,36 +70,55 @@ __device__ __forceinline__ int mask_sources(const uint64_t* F, int v) {
 }
 
 // Sparse part of a level: one thread per list whose mask has fewer than kWarpSources sources
-// (the queue, or with `dense` every such list in schedule order).
+// (the queue, or with `dense` every such list in schedule order).  The list's sources and their
+// arrivals at the list's vertex sit in kSparseSlots register slots, loaded once per list, so an
+// edge costs one window test (and a fire-and-forget RED.MIN) per source, not a dependent load.
+constexpr int kSparseSlots = kWarpSources - 1;
+
 __device__ __forceinline__ unsigned long long multi_relax_sparse(const GraphView& g, MultiArgs& a, const Work& w,
                                                                  const int64_t* slo, const int64_t* shi,
                                                                  const int32_t* scol, const int32_t* q, int qn, int L,
                                                                  bool dense) {
   const uint64_t* Fc = a.F[L & 1];
   uint64_t* Fn = a.F[(L + 1) & 1];
-  uint64_t M[kWords], seen[kWords];
-  int xcur = 0, yprev = -1;
+  int src[kSparseSlots];     // source of slot i (-1: empty)
+  uint32_t ax[kSparseSlots];  // its arrival at the list's vertex
+  uint32_t seen = 0;          // bit i: slot i took an edge of the current run of equal successors
+  int yprev = -1;
   auto begin = [&](int x, int first, int, int run) {
     if (x < g.active_begin || x > g.max_label) return false;
-    uint64_t any = 0;
+    uint64_t m0 = __ldcg(Fc + (size_t)x * kWords + 0), m1 = __ldcg(Fc + (size_t)x * kWords + 1);
+    uint64_t m2 = __ldcg(Fc + (size_t)x * kWords + 2), m3 = __ldcg(Fc + (size_t)x * kWords + 3);
+    if (!(m0 | m1 | m2 | m3)) return false;
 #pragma unroll
-    for (int k = 0; k < kWords; ++k) {
-      M[k] = __ldcg(Fc + (size_t)x * kWords + k);
-      seen[k] = 0;
-      any |= M[k];
+    for (int i = 0; i < kSparseSlots; ++i) {
+      int s = -1;
+      if (m0) {
+        s = __ffsll((long long)m0) - 1;
+        m0 &= m0 - 1;
+      } else if (m1) {
+        s = 64 + __ffsll((long long)m1) - 1;
+        m1 &= m1 - 1;
+      } else if (m2) {
+        s = 128 + __ffsll((long long)m2) - 1;
+        m2 &= m2 - 1;
+      } else if (m3) {
+        s = 192 + __ffsll((long long)m3) - 1;
+        m3 &= m3 - 1;
+      }
+      src[i] = s;
+      ax[i] = s >= 0 ? __ldcg(a.arr + arr_at(a, x, s)) : kNoArrival;
     }
-    if (!any) return false;
-    xcur = x;
+    // The scan sends lists with kWarpSources or more sources to the wide queue; more here is a bug.
+    if (m0 | m1 | m2 | m3) set_err(g, kErrCode);
+    seen = 0;
     yprev = -1;
     if (run >= 0) {
       // Sources whose first in-window edge of this run lies before the slice saw the run already.
       const int32_t* rf = a.run_first + (size_t)run * a.run_stride;
 #pragma unroll
-      for (int k = 0; k < kWords; ++k)
-        for (uint64_t c = M[k]; c; c &= c - 1) {
-          const int b = __ffsll((long long)c) - 1;
-          if (__ldg(rf + scol[k * 64 + b]) < first) seen[k] |= 1ull << b;
-        }
+      for (int i = 0; i < kSparseSlots; ++i)
+        if (src[i] >= 0 && __ldg(rf + scol[src[i]]) < first) seen |= 1u << i;
       yprev = kKeepSeen;
     }
     return true;
@@ -108,32 +127,34 @@ __device__ __forceinline__ unsigned long long multi_relax_sparse(const GraphView
     if (yprev == kKeepSeen) {
       yprev = y;
     } else if (y != yprev) {
-#pragma unroll
-      for (int k = 0; k < kWords; ++k) seen[k] = 0;
+      seen = 0;
       yprev = y;
     }
     const bool usable = y >= g.active_begin && y < g.max_vertex && t >= 0 && t < 0xFFFFFFFFll;
-    bool any = false;
+    uint64_t add0 = 0, add1 = 0, add2 = 0, add3 = 0;
 #pragma unroll
-    for (int k = 0; k < kWords; ++k) {
-      uint64_t add = 0;
-      for (uint64_t c = M[k] & ~seen[k]; c; c &= c - 1) {
-        const int b = __ffsll((long long)c) - 1;
-        const int s = k * 64 + b;
-        if (t < slo[s] || t >= shi[s]) continue;
-        seen[k] |= 1ull << b;
-        if (!usable) continue;
-        const uint32_t ax = __ldcg(a.arr + arr_at(a, xcur, s));
-        if ((int64_t)ax > t) continue;
-        atomicMin(a.arr + arr_at(a, y, s), (uint32_t)t);
-        add |= 1ull << b;
-      }
-      if (add) {
-        atomicOr((unsigned long long*)(Fn + (size_t)y * kWords + k), (unsigned long long)add);
-        any = true;
-      }
+    for (int i = 0; i < kSparseSlots; ++i) {
+      const int s = src[i];
+      if (s < 0 || ((seen >> i) & 1u)) continue;
+      if (t < slo[s] || t >= shi[s]) continue;
+      seen |= 1u << i;
+      if (!usable || (int64_t)ax[i] > t) continue;
+      atomicMin(a.arr + arr_at(a, y, s), (uint32_t)t);
+      const uint64_t bit = 1ull << (s & 63);
+      const int wd = s >> 6;
+      add0 |= wd == 0 ? bit : 0;
+      add1 |= wd == 1 ? bit : 0;
+      add2 |= wd == 2 ? bit : 0;
+      add3 |= wd == 3 ? bit : 0;
     }
-    if (any) atomicOr(&a.dirty[y >> 5], 1u << (y & 31));
+    if (add0 | add1 | add2 | add3) {
+      unsigned long long* f = (unsigned long long*)(Fn + (size_t)y * kWords);
+      if (add0) atomicOr(f + 0, (unsigned long long)add0);
+      if (add1) atomicOr(f + 1, (unsigned long long)add1);
+      if (add2) atomicOr(f + 2, (unsigned long long)add2);
+      if (add3) atomicOr(f + 3, (unsigned long long)add3);
+      atomicOr(&a.dirty[y >> 5], 1u << (y & 31));
+    }
     return true;
   };
   if (dense) {
@@ -1008,7 +1029,8 @@ struct tga_cc_job {
   std::vector<uint8_t> used;
   std::vector<tga::CcBatchState> st;  // host copy after the last step
   tga::CcArgs args{};
-  int32_t* run_table = nullptr;
+  int32_t* run_table = nullptr;  // [nruns][cap] for the decomposition of generation work_gen
+  uint32_t work_gen = 0;
   ~tga_cc_job() {
     lab.release();
     meta.release();
@@ -1029,6 +1051,7 @@ static int cc_job_create(GraphHandle& h, int32_t cap, int32_t flags, tga_cc_job*
   j->h = &h;
   j->cap = cap;
   j->flags = flags;
+  j->work_gen = h.work_gen;
   const size_t nv = (size_t)h.view.max_vertex;
   const size_t st_bytes = (size_t)cap * sizeof(CcBatchState);
   const size_t fixed = st_bytes + (size_t)cap * 16 + kMaxSources * (8 + 4) + kMaxSources * kMaxSources / 8;
@@ -1060,8 +1083,15 @@ static int cc_job_create(GraphHandle& h, int32_t cap, int32_t flags, tga_cc_job*
   return TGA_OK;
 }
 
+static int cc_job_current(const tga_cc_job* j) {
+  if (j->work_gen != j->h->work_gen)
+    return fail(TGA_E_ARG, "the graph's work decomposition changed after the CC job was created");
+  return TGA_OK;
+}
+
 static int cc_job_add(tga_cc_job* j, int64_t t_lo, int64_t t_hi, int32_t* slot) {
   GraphHandle& h = *j->h;
+  TGA_TRY(cc_job_current(j));
   if (t_lo >= t_hi) return fail(TGA_E_ARG, "empty time window");
   int32_t q = 0;
   while (q < j->cap && j->used[(size_t)q]) ++q;
@@ -1094,6 +1124,7 @@ static int cc_job_add(tga_cc_job* j, int64_t t_lo, int64_t t_hi, int32_t* slot) 
 // passed.  finished (may be NULL): bit q set when slot q holds a finished window.
 static int cc_job_step(tga_cc_job* j, double budget_ms, uint32_t* finished) {
   GraphHandle& h = *j->h;
+  TGA_TRY(cc_job_current(j));
   TGA_TRY(multi_buffers(h, kMaxSources));
   TGA_TRY(h.begin_call());
   unsigned long long* edges = edge_counter(h);

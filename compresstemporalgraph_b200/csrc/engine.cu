@@ -334,6 +334,10 @@ int publish_view(GraphHandle& h) {
 
 int build_work(GraphHandle& h, int32_t slice_len, int32_t item_edges) {
   if (slice_len < 16 || item_edges < 1) return fail(TGA_E_ARG, "slice length must be >= 16 and item size >= 1");
+  // State sized for the old decomposition (the cached CC job's run table) goes; CC jobs made by
+  // callers see the new generation and refuse to run.
+  h.cc_cache.reset();
+  ++h.work_gen;
   GraphView& v = h.view;
   // The build walks the lists without seeking (checkpoints are being made).
   v.slices = nullptr;

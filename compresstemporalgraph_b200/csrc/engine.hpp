@@ -82,8 +82,10 @@ struct GraphHandle {
   // vertices the last traversal touched.  With m_clean, everything is "unreached"/zero except the
   // m_pending sources' entries at the touched vertices, which the next traversal resets first.
   DevBuf m_state, m_mask, m_dirty, m_stamp, m_touched, m_dq;
-  // connected-components job reused by tga_cc / tga_cc_batch (batch.cu)
+  // connected-components job reused by tga_cc / tga_cc_batch (batch.cu); dropped by build_work,
+  // since its run table is sized for the decomposition's cut runs
   std::unique_ptr<tga_cc_job, CcJobDeleter> cc_cache;
+  uint32_t work_gen = 0;             // bumped by every build_work (jobs made earlier refuse to run)
   int32_t m_cap = 0, m_pending = 0;
   uint32_t m_epoch = 0;
   bool m_clean = false;
@@ -109,7 +111,7 @@ struct GraphHandle {
 // Default slice length: short enough that a frontier level holding one slice of a hub is not
 // bound by a single thread's sequential decode, long enough that checkpoints stay a fraction of
 // the compressed bytes.
-constexpr int32_t kDefaultSliceEdges = 32;
+constexpr int32_t kDefaultSliceEdges = 24;
 
 int load_graph(GraphHandle& h, const std::string& dir, const std::string& base, const tga_dataset_cfg& cfg);
 // (Re)builds slices and work items: lists longer than slice_len edges are cut into slices,

@@ -98,7 +98,7 @@ int tga_get_info(tga_graph* g, tga_info* out);
 int tga_get_timing(tga_graph* g, tga_timing* out);
 /* Work decomposition of the sweeps and traversals: lists longer than slice_edges are cut into
  * resumable slices (decoder checkpoints built once), shorter lists are grouped into work items of
- * about item_edges edges.  Defaults 32 / 256, or $TGA_SLICE_EDGES / $TGA_ITEM_EDGES at open.
+ * about item_edges edges.  Defaults 24 / 256, or $TGA_SLICE_EDGES / $TGA_ITEM_EDGES at open.
  * The reference has no counterpart (one thread per vertex, shared/neighbor_access.cu:1599-1642). */
 int tga_set_work_params(tga_graph* g, int32_t slice_edges, int32_t item_edges);
 int tga_get_work_params(tga_graph* g, int32_t* slice_edges, int32_t* item_edges, int64_t* slices, int32_t* items);
@@ -215,7 +215,8 @@ int tga_cc_batch(tga_graph* g, int32_t nq, const int64_t* t_lo, const int64_t* t
  * *finished gets bit s set for each slot whose window is finished; tga_cc_job_take copies a
  * finished window's labels (max_vertex entries, may be NULL) and component count and frees the
  * slot.  A window's result equals tga_cc's.  The job owns its device memory and uses the graph's
- * stream; destroy it before closing the graph. */
+ * stream; destroy it before closing the graph.  After tga_set_work_params the job's add and step
+ * return TGA_E_ARG (its per-run table belongs to the old decomposition): make a new job. */
 typedef struct tga_cc_job tga_cc_job;
 int tga_cc_job_create(tga_graph* g, int32_t capacity, int32_t flags, tga_cc_job** out);
 int tga_cc_job_add(tga_cc_job* job, int64_t t_lo, int64_t t_hi, int32_t* slot);

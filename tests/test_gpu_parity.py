@@ -194,6 +194,30 @@ def test_cc_job_resumes_across_steps_and_reuses_slots(pairs):
         assert got[i][1] == want[i][1] and np.array_equal(got[i][0], want[i][0]), i
 
 
+def test_cc_after_work_decomposition_change(pairs):
+    """The cached CC job (and a caller's job) hold a per-run table sized for the decomposition they
+    were made under: after set_work_params the cached one is rebuilt (results still exact) and a
+    caller's job refuses to run instead of using the stale table."""
+    p = pairs["hubs"]
+    lo, hi = _windows(p)[1]
+    olab, ok = p.o.cc(p.ml, p.mv, p.act, p.cfg.connected_components_vertex_begin, lo, hi, True)
+    default = p.g.work_params()
+    job = tga.CcJob(p.g, capacity=2)
+    try:
+        lab, k = p.g.connected_components(lo, hi)  # makes the cached job
+        assert k == ok and np.array_equal(lab, olab)
+        for sl in (16, 4096):
+            p.g.set_work_params(sl, default["item_edges"])
+            lab, k = p.g.connected_components(lo, hi)
+            assert k == ok and np.array_equal(lab, olab), sl
+        with pytest.raises(tga.TgaError) as e:
+            job.add(lo, hi)
+        assert e.value.code == tga.TGA_E_ARG
+    finally:
+        job.close()
+        p.g.set_work_params(default["slice_edges"], default["item_edges"])
+
+
 def test_multi_source_state_survives_other_calls(pairs):
     """The batched traversal keeps its per-source arrays between calls and resets only the
     vertices the previous traversal touched; single-source traversals, batched CC and batched
