@@ -62,7 +62,8 @@ class _Timing(C.Structure):
 
 class _Query(C.Structure):
     _fields_ = [("kind", C.c_int32), ("graph", C.c_int32), ("src", C.c_int32), ("iters", C.c_int32),
-                ("t_lo", C.c_int64), ("t_hi", C.c_int64), ("out", C.c_void_p)]
+                ("dst", C.c_int32), ("reserved", C.c_int32), ("t_lo", C.c_int64), ("t_hi", C.c_int64),
+                ("out", C.c_void_p)]
 
 
 class _ServerStats(C.Structure):
@@ -113,6 +114,7 @@ def _load() -> C.CDLL:
         "tga_color": (C.c_int, [P, C.c_int32, P, C.c_int32, P, P, C.POINTER(C.c_int32)]),
         "tga_bfs_batch": (C.c_int, [P, C.c_int32, P, P, P, P]),
         "tga_cc_batch": (C.c_int, [P, C.c_int32, P, P, C.c_int32, P, P]),
+        "tga_is_neighbor": (C.c_int, [P, C.c_int32, P, P, P, P, P]),
         "tga_pagerank_batch_iters": (C.c_int, [P, C.c_int32, P, C.c_float, C.c_float, P, P, P]),
         "tga_cc_job_create": (C.c_int, [P, C.c_int32, C.c_int32, P]),
         "tga_cc_job_add": (C.c_int, [P, C.c_int64, C.c_int64, P]),
@@ -345,6 +347,17 @@ class Graph:
         _check(_lib.tga_bfs_batch(self._h, len(src), _ptr(src), _ptr(lo), _ptr(hi), _ptr(out)))
         return out
 
+    def is_neighbor(self, node, neighbor, t_from=None, t_to=None):
+        """Windowed point queries (tga_is_neighbor): True where some edge node->neighbor has a
+        timestamp in [t_from, t_to] (inclusive); no bounds when t_from/t_to are None."""
+        x = np.ascontiguousarray(node, np.int32)
+        y = np.ascontiguousarray(neighbor, np.int32)
+        lo = None if t_from is None else np.ascontiguousarray(np.broadcast_to(t_from, x.shape), np.int64)
+        hi = None if t_to is None else np.ascontiguousarray(np.broadcast_to(t_to, x.shape), np.int64)
+        out = np.zeros(len(x), np.uint8)
+        _check(_lib.tga_is_neighbor(self._h, len(x), _ptr(x), _ptr(y), _ptr(lo), _ptr(hi), _ptr(out)))
+        return out.astype(bool)
+
     def cc_batch(self, t_lo, t_hi, early_exit: bool = True):
         """Connected components of many windows in one launch (tga_cc_batch): labels [n, max_vertex]
         and component counts [n], each row equal to connected_components for that window."""
@@ -372,7 +385,7 @@ class Graph:
 
 # ---- served form -------------------------------------------------------------------------------
 
-Q_BFS, Q_PAGERANK, Q_CC = 0, 1, 2
+Q_BFS, Q_PAGERANK, Q_CC, Q_NEIGHBOR = 0, 1, 2, 3
 
 
 class CcJob:
@@ -431,10 +444,14 @@ class Server:
         self._graphs.append(g)
         return gid.value
 
-    def submit(self, kind: int, graph: int, src: int = 0, t_lo: int = 0, t_hi: int = T_MAX, iters: int = 0) -> int:
+    def submit(self, kind: int, graph: int, src: int = 0, t_lo: int = 0, t_hi: int = T_MAX, iters: int = 0,
+               dst: int = 0) -> int:
         nv = self._graphs[graph].max_vertex
-        out = np.zeros(nv, np.float32 if kind == Q_PAGERANK else np.int32)
-        q = _Query(kind, graph, src, iters, t_lo, t_hi, out.ctypes.data)
+        if kind == Q_NEIGHBOR:
+            out = np.zeros(1, np.uint8)
+        else:
+            out = np.zeros(nv, np.float32 if kind == Q_PAGERANK else np.int32)
+        q = _Query(kind, graph, src, iters, dst, 0, t_lo, t_hi, out.ctypes.data)
         ticket = C.c_int64()
         _check(_lib.tga_submit(self._h, C.byref(q), C.byref(ticket)))
         self._keep[ticket.value] = out

@@ -99,6 +99,65 @@ __global__ void k_neighbors(GraphView g, int32_t v, int32_t* dst, int64_t* ts, i
   *count = d;
 }
 
+// Windowed point queries, one thread each, as EvolvingMultiGraph.isNeighbor(node, neighbor, from,
+// to) (cpu_java/src/main/java/gr/uoa/di/networkanalysis/EvolvingMultiGraph.java:343-389): find the
+// run of `neighbor` in node's successor list and report whether one of its timestamps lies in
+// [from, to] (both ends inclusive).  Lists are sorted, so the run is the only one, and a sliced list
+// is entered at its last slice whose first successor is below `neighbor` (binary search over the
+// checkpoints, reading one successor per probe), then scanned slice by slice.
+__global__ void TGA_DECODE_BOUNDS k_is_neighbor(GraphView g, int32_t nq, const int32_t* node, const int32_t* nbr,
+                                                const int64_t* t_from, const int64_t* t_to, uint8_t* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nq) return;
+  const int x = node[i], want = nbr[i];
+  const int64_t lo = t_from[i], hi = t_to[i];
+  uint8_t found = 0;
+  if (x >= 0 && x < g.n && want >= 0) {
+    DeepState deep;
+    EdgeCursor c(&deep);
+    const int s0 = __ldg(g.slice_first + x), s1 = __ldg(g.slice_first + x + 1);
+    int y;
+    int64_t t;
+    if (s1 - s0 > 1) {
+      int a = s0, b = s1 - 1;
+#pragma unroll 1
+      while (a < b) {
+        const int mid = (a + b + 1) >> 1;
+        cursor_restore(g, c, g.slices[mid]);
+        if (c.next<false>(g, y, t) && y < want) a = mid;
+        else b = mid - 1;
+      }
+      bool stop = false;
+#pragma unroll 1
+      for (int k = a; k < s1 && !stop && !found; ++k) {
+        cursor_restore(g, c, g.slices[k]);
+        while (c.next(g, y, t)) {
+          if (y < want) continue;
+          if (y > want) {
+            stop = true;
+            break;
+          }
+          if (t >= lo && t <= hi) {
+            found = 1;
+            break;
+          }
+        }
+      }
+    } else {
+      c.open(g, x);
+      while (c.next(g, y, t)) {
+        if (y < want) continue;
+        if (y > want) break;
+        if (t >= lo && t <= hi) {
+          found = 1;
+          break;
+        }
+      }
+    }
+  }
+  out[i] = found;
+}
+
 // ---------------------------------------------------------------------------------------------
 // PageRank: one launch per iteration.  Three rank buffers rotate: iteration k reads IN (the
 // unnormalised result of k-1, scaled by 1/sum[k-1]), scatters into OUT (already set to the base
@@ -514,6 +573,31 @@ int tga_neighbors(tga_graph* gp, int32_t v, int32_t* dst, int64_t* ts, int32_t c
     if (ts) TGA_CUDA_TRY(cudaMemcpy(ts, h.s_d.p, (size_t)k * 8, cudaMemcpyDeviceToHost));
   }
   return TGA_OK;
+}
+
+int tga_is_neighbor(tga_graph* gp, int32_t nq, const int32_t* node, const int32_t* neighbor, const int64_t* t_from,
+                    const int64_t* t_to, uint8_t* out) {
+  if (!gp || nq < 0 || (nq && (!node || !neighbor || !out))) return fail(TGA_E_ARG, "bad argument");
+  GraphHandle& h = *gp;
+  if (nq == 0) return TGA_OK;
+  std::vector<int64_t> lo((size_t)nq, INT64_MIN), hi((size_t)nq, INT64_MAX);
+  if (t_from) std::memcpy(lo.data(), t_from, (size_t)nq * 8);
+  if (t_to) std::memcpy(hi.data(), t_to, (size_t)nq * 8);
+  TGA_TRY(h.s_c.ensure((size_t)nq * 8));
+  TGA_TRY(h.s_d.ensure((size_t)nq * 16));
+  TGA_TRY(h.s_e.ensure((size_t)nq));
+  TGA_TRY(h.begin_call());
+  int32_t* dnode = h.s_c.as<int32_t>();
+  int64_t* dlo = h.s_d.as<int64_t>();
+  TGA_CUDA_TRY(cudaMemcpyAsync(dnode, node, (size_t)nq * 4, cudaMemcpyHostToDevice, h.stream));
+  TGA_CUDA_TRY(cudaMemcpyAsync(dnode + nq, neighbor, (size_t)nq * 4, cudaMemcpyHostToDevice, h.stream));
+  TGA_CUDA_TRY(cudaMemcpyAsync(dlo, lo.data(), (size_t)nq * 8, cudaMemcpyHostToDevice, h.stream));
+  TGA_CUDA_TRY(cudaMemcpyAsync(dlo + nq, hi.data(), (size_t)nq * 8, cudaMemcpyHostToDevice, h.stream));
+  cudaEvent_t* ev = h.kernel_begin();
+  KL(k_is_neighbor, grid_for(nq, kBlock))(h.view, nq, dnode, dnode + nq, dlo, dlo + nq, h.s_e.as<uint8_t>());
+  h.kernel_end(ev);
+  TGA_CUDA_TRY(cudaMemcpyAsync(out, h.s_e.p, (size_t)nq, cudaMemcpyDeviceToHost, h.stream));
+  return h.end_call();
 }
 
 int tga_decode_all(tga_graph* gp, int64_t* offsets, int32_t* dst, int64_t* ts, int64_t cap) {

@@ -70,6 +70,7 @@ constexpr double kCcIdleMs = 100.0;
 // Device working bytes of one query (per vertex of its graph): BFS arrival + last-enqueued arrival
 // + result; PageRank three rank vectors + inverse degree + result; CC the single traversal's arrays.
 int64_t query_bytes(const tga_query& q, int32_t nv) {
+  if (q.kind == TGA_Q_NEIGHBOR) return 64;
   const int64_t per_vertex = q.kind == TGA_Q_BFS ? 12 : q.kind == TGA_Q_PAGERANK ? 20 : 40;
   return per_vertex * (int64_t)nv;
 }
@@ -161,6 +162,27 @@ void tga_server::run_round(GraphSlot* slot, std::vector<Pending>& round) {
                                               hi.data(), out.data());
       for (size_t k = 0; k < done.size(); ++k)
         if (rc == TGA_OK && done[k]->q.out) std::memcpy(done[k]->q.out, out.data() + k * nv, nv * 4);
+      publish(done, std::vector<int>(done.size(), rc));
+    }
+  }
+  // Point queries: one launch.
+  {
+    std::vector<const Pending*> done;
+    std::vector<int32_t> x, y;
+    std::vector<int64_t> lo, hi;
+    for (const Pending& p : round)
+      if (p.q.kind == TGA_Q_NEIGHBOR) {
+        done.push_back(&p);
+        x.push_back(p.q.src);
+        y.push_back(p.q.dst);
+        lo.push_back(p.q.t_lo);
+        hi.push_back(p.q.t_hi);
+      }
+    if (!done.empty()) {
+      std::vector<uint8_t> out(done.size());
+      const int rc = tga_is_neighbor(slot->g, (int32_t)done.size(), x.data(), y.data(), lo.data(), hi.data(), out.data());
+      for (size_t k = 0; k < done.size(); ++k)
+        if (rc == TGA_OK && done[k]->q.out) *static_cast<uint8_t*>(done[k]->q.out) = out[k];
       publish(done, std::vector<int>(done.size(), rc));
     }
   }
@@ -343,8 +365,8 @@ int tga_server_add_graph(tga_server* s, tga_graph* g, int32_t* graph_id) {
 
 int tga_submit(tga_server* s, const tga_query* q, int64_t* ticket) {
   if (!s || !q) return fail(TGA_E_ARG, "null server or query");
-  if (q->kind < TGA_Q_BFS || q->kind > TGA_Q_CC) return fail(TGA_E_ARG, "unknown query kind");
-  if (q->t_lo >= q->t_hi) return fail(TGA_E_ARG, "empty time window");
+  if (q->kind < TGA_Q_BFS || q->kind > TGA_Q_NEIGHBOR) return fail(TGA_E_ARG, "unknown query kind");
+  if (q->kind == TGA_Q_NEIGHBOR ? q->t_lo > q->t_hi : q->t_lo >= q->t_hi) return fail(TGA_E_ARG, "empty time window");
   std::lock_guard<std::mutex> lk(s->mu);
   if (s->stopping) return fail(TGA_E_ARG, "server is stopping");
   if (q->graph < 0 || q->graph >= (int32_t)s->graphs.size()) return fail(TGA_E_ARG, "unknown graph id");

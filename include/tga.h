@@ -116,6 +116,14 @@ int tga_neighbor_access(tga_graph* g, uint8_t* small_out, uint64_t* checksum_out
  * EvolvingMultiGraph.java:391-443).  Writes min(count, cap) entries; *count = outdegree. */
 int tga_neighbors(tga_graph* g, int32_t v, int32_t* dst, int64_t* ts, int32_t cap, int32_t* count);
 
+/* Windowed point queries (EvolvingMultiGraph.isNeighbor(node, neighbor, from, to),
+ * cpu_java/src/main/java/gr/uoa/di/networkanalysis/EvolvingMultiGraph.java:343-389): out[i] = 1 when
+ * some edge node[i] -> neighbor[i] has a timestamp in [t_from[i], t_to[i]] (both ends inclusive, as
+ * the reference), else 0.  t_from / t_to may be NULL (no bound), which is isNeighbor(node, neighbor)
+ * (EvolvingMultiGraph.java:328-341).  nq queries in one launch, one thread each. */
+int tga_is_neighbor(tga_graph* g, int32_t nq, const int32_t* node, const int32_t* neighbor, const int64_t* t_from,
+                    const int64_t* t_to, uint8_t* out);
+
 /* Whole graph as CSR: offsets[n+1], dst[m], ts[m] (cap = capacity of dst/ts). */
 int tga_decode_all(tga_graph* g, int64_t* offsets, int32_t* dst, int64_t* ts, int64_t cap);
 
@@ -236,28 +244,35 @@ int tga_pagerank_batch(tga_graph* g, int32_t nq, int32_t iters, float damping, f
 int tga_pagerank_batch_iters(tga_graph* g, int32_t nq, const int32_t* iters, float damping, float alpha,
                              const int64_t* t_lo, const int64_t* t_hi, float* rank_out);
 
-/* ---- served form ----------------------------------------------------------------------------
- * No counterpart in the reference.  A server keeps several opened graphs resident and answers a
- * stream of queries: one worker thread per graph takes the queries that arrived since its last
- * round, admits them while their device working memory fits the server's budget, and runs them
- * together (BFS queries as one batched traversal, PageRank queries with equal iteration counts as
- * one strided vector, CC one by one); queries that arrive meanwhile join the next round.  Graphs
- * run on their own streams, so work of different graphs overlaps on the device.  While a graph is
+/* ---- served form ---------------------------------------------------------------------------
+ * No counterpart in the reference.  A server keeps several graphs resident and answers a stream
+ * of queries.  One worker thread per graph repeatedly takes the queries that arrived since its
+ * last round, admits them while their device working memory fits the server's budget, and runs
+ * them together: BFS queries as one multi-source traversal, PageRank queries as one strided vector
+ * (each with its own iteration count), point queries in one launch; CC queries join the graph's
+ * resumable CC job (tga_cc_job_*), which each round advances by a time slice sized by the age of
+ * its oldest window against the oldest other waiting query.  Rounds of different graphs take the
+ * device one at a time, the graph with the oldest outstanding query first.  While a graph is
  * attached to a running server, only the server may use its handle. */
 typedef struct tga_server tga_server;
 
 #define TGA_Q_BFS 0
 #define TGA_Q_PAGERANK 1
 #define TGA_Q_CC 2
+#define TGA_Q_NEIGHBOR 3
 
 typedef struct {
-  int32_t kind;        /* TGA_Q_BFS, TGA_Q_PAGERANK or TGA_Q_CC */
+  int32_t kind;        /* TGA_Q_BFS, TGA_Q_PAGERANK, TGA_Q_CC or TGA_Q_NEIGHBOR */
   int32_t graph;       /* id from tga_server_add_graph */
-  int32_t src;         /* BFS source */
+  int32_t src;         /* BFS source; point query: node */
   int32_t iters;       /* PageRank iterations (<= 0: pr_iters of the graph's configuration) */
-  int64_t t_lo, t_hi;  /* time window */
-  void* out;           /* caller-owned host buffer of max_vertex entries: BFS int32 arrivals, PageRank
-                          float ranks (damping 0.85, alpha 0.1), CC int32 labels; NULL: results dropped */
+  int32_t dst;         /* point query: neighbor */
+  int32_t reserved;
+  int64_t t_lo, t_hi;  /* time window [t_lo, t_hi); point query: [t_lo, t_hi], both ends inclusive
+                          (tga_is_neighbor) */
+  void* out;           /* caller-owned host buffer: max_vertex entries of BFS int32 arrivals, PageRank
+                          float ranks (damping 0.85, alpha 0.1) or CC int32 labels; one uint8 for a
+                          point query; NULL: results dropped */
 } tga_query;
 
 typedef struct {
@@ -267,7 +282,8 @@ typedef struct {
 } tga_server_stats;
 
 /* budget_bytes: device working memory that admitted queries may hold at once (BFS about
- * 12 bytes, PageRank about 20 bytes, CC about 40 bytes per vertex of their graph). */
+ * 12 bytes, PageRank about 20 bytes, CC about 40 bytes per vertex of their graph; a point query
+ * 64 bytes). */
 int tga_server_create(int64_t budget_bytes, tga_server** out);
 int tga_server_add_graph(tga_server* s, tga_graph* g, int32_t* graph_id);
 /* Queues q; *ticket identifies it.  A query larger than the whole budget fails with TGA_E_OOM. */

@@ -162,6 +162,34 @@ def test_pagerank_batch_mixed_iteration_counts(pairs, shape):
         assert float(np.abs(out[i].astype(np.float64) - o).sum()) <= 1e-5, i
 
 
+@pytest.mark.parametrize("shape", ["hubs", "chains", "small"])
+def test_is_neighbor_vs_oracle(pairs, shape):
+    """Windowed point queries against the oracle's decoded lists: pairs taken from real edges (the
+    window exactly one edge's timestamp, both ends inclusive, as the reference) and random pairs,
+    hub lists entered through their checkpoints."""
+    p = pairs[shape]
+    off, dst, ts = p.o.csr()
+    rng = np.random.default_rng(25)
+    m = len(dst)
+    deg = np.diff(off)
+    hub = int(np.argmax(deg))
+    k = rng.integers(0, m, 300)
+    srcv = np.searchsorted(off, k, side="right") - 1
+    hub_k = off[hub] + rng.integers(0, deg[hub], 100)
+    x = np.concatenate([srcv, np.full(100, hub), rng.integers(0, p.n, 200)]).astype(np.int32)
+    y = np.concatenate([dst[k], dst[hub_k], rng.integers(0, p.mv, 200)]).astype(np.int32)
+    t_at = np.concatenate([ts[k], ts[hub_k], rng.integers(0, 10**8, 200)]).astype(np.int64)
+    lo = t_at - rng.integers(0, 3, len(x))
+    hi = t_at + rng.integers(-1, 3, len(x))  # hi < t_at in some rows: the edge itself is outside
+    got = p.g.is_neighbor(x, y, lo, hi)
+    any_t = p.g.is_neighbor(x, y)
+    for i in range(len(x)):
+        a, b = off[x[i]], off[x[i] + 1]
+        sel = dst[a:b] == y[i]
+        assert got[i] == bool(np.any(sel & (ts[a:b] >= lo[i]) & (ts[a:b] <= hi[i]))), i
+        assert any_t[i] == bool(np.any(sel)), i
+
+
 def test_cc_job_resumes_across_steps_and_reuses_slots(pairs):
     """A CC job stepped with a tiny budget (one batch per step), with batched BFS and a plain CC
     run on the handle between steps and windows added as slots free up, gives each window the

@@ -1,6 +1,7 @@
 """Served form: a request loop over two resident graphs.  Every result must equal the plain
-single-query call (BFS arrivals and CC labels bit-exact, PageRank within the batched-vs-single
-tolerance), and a query gives the same result alone and inside a mix of concurrent queries."""
+single-query call (BFS arrivals, CC labels and point queries bit-exact, PageRank within the
+batched-vs-single tolerance), and a query gives the same result alone and inside a mix of
+concurrent queries."""
 from __future__ import annotations
 
 import numpy as np
@@ -28,7 +29,10 @@ def _mix(rng, gid, d, count):
         if rng.random() < 0.2:
             lo, hi = 0, T_MAX
         r = rng.random()
-        if r < 0.6:
+        if r < 0.1:
+            out.append(dict(kind=tga.Q_NEIGHBOR, graph=gid, src=int(rng.integers(0, n)), dst=int(rng.integers(0, n)),
+                            t_lo=lo, t_hi=hi))
+        elif r < 0.6:
             out.append(dict(kind=tga.Q_BFS, graph=gid, src=int(rng.integers(0, n)), t_lo=lo, t_hi=hi))
         elif r < 0.85:
             out.append(dict(kind=tga.Q_PAGERANK, graph=gid, iters=int(rng.integers(3, 7)), t_lo=lo, t_hi=hi))
@@ -38,6 +42,8 @@ def _mix(rng, gid, d, count):
 
 
 def _plain(g, q):
+    if q["kind"] == tga.Q_NEIGHBOR:
+        return np.array([g.is_neighbor([q["src"]], [q["dst"]], q["t_lo"], q["t_hi"])[0]], np.uint8)
     if q["kind"] == tga.Q_BFS:
         return g.bfs(q["src"], q["t_lo"], q["t_hi"])[0]
     if q["kind"] == tga.Q_PAGERANK:
