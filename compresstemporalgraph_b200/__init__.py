@@ -132,6 +132,7 @@ def _load() -> C.CDLL:
         "tga_generate": (C.c_int, [C.POINTER(_GenParams), C.c_char_p, C.c_char_p, C.c_char_p,
                                    C.POINTER(_GenSummary)]),
         "tga_encode_raw": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int64, C.POINTER(_GenSummary)]),
+        "tga_build_index": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int64]),
         "tga_decode_table": (C.c_int, [C.c_int32, P]),
         "tga_encode_codes": (C.c_int, [C.c_int32, C.c_int32, P, C.c_int64, P, C.c_int64, C.POINTER(C.c_int64)]),
         "tga_ef_encode": (C.c_int, [P, C.c_int64, C.c_int32, P, C.c_int64, P, C.c_int64, C.POINTER(C.c_int64),
@@ -542,6 +543,11 @@ def encode_raw(raw_path: str | os.PathLike, directory: str | os.PathLike, basena
     _check(_lib.tga_encode_raw(str(raw_path).encode(), str(directory).encode(), basename.encode(), max_label,
                                C.byref(s)))
     return {k: getattr(s, k) for k, _ in _GenSummary._fields_}
+
+
+def build_index(directory: str | os.PathLike, basename: str, max_label: int) -> None:
+    """Writes the four GPU index files of a directory that has <base>.offsets (tga_build_index)."""
+    _check(_lib.tga_build_index(str(directory).encode(), basename.encode(), max_label))
 
 
 def decode_table(kind: int) -> np.ndarray:

@@ -136,6 +136,67 @@ class BitReader {
   uint64_t pos_;
 };
 
+// Word-at-a-time MSB-first reader for long host-side walks (same codes as BitReader): a 64-bit
+// look-ahead from any bit, clz for unary prefixes.  The buffer is read through a copy padded with
+// 16 zero bytes, so look-ahead past the end reads zeros; running past the end throws.
+class FastBitReader {
+ public:
+  FastBitReader(const std::vector<uint8_t>& d, uint64_t pos = 0) : d_(d), nbits_((uint64_t)d.size() * 8), pos_(pos) {
+    d_.resize(d.size() + 16, 0);
+  }
+  uint64_t pos() const { return pos_; }
+  void seek(uint64_t p) { pos_ = p; }
+  uint64_t peek64() const {
+    const uint64_t byte = pos_ >> 3;
+    const int sh = (int)(pos_ & 7);
+    uint64_t w = 0;
+    for (int i = 0; i < 8; ++i) w = (w << 8) | d_[byte + (uint64_t)i];
+    return sh ? (w << sh) | (uint64_t)(d_[byte + 8] >> (8 - sh)) : w;
+  }
+  void skip(uint64_t n) {
+    pos_ += n;
+    if (pos_ > nbits_) throw std::runtime_error("bit stream overrun at bit " + std::to_string(pos_));
+  }
+  uint64_t bits(int len) {
+    if (len == 0) return 0;
+    const uint64_t v = peek64() >> (64 - len);
+    skip((uint64_t)len);
+    return v;
+  }
+  uint64_t unary() {
+    uint64_t n = 0;
+    for (;;) {
+      if (pos_ >= nbits_) throw std::runtime_error("bit stream overrun at bit " + std::to_string(pos_));
+      const uint64_t w = peek64();
+      if (w) {
+        const int z = __builtin_clzll(w);
+        skip((uint64_t)z + 1);
+        return n + (uint64_t)z;
+      }
+      n += 64;
+      skip(64);
+    }
+  }
+  uint64_t gamma() {
+    const uint64_t m = unary();
+    if (m > 63) throw std::runtime_error("gamma code too long");
+    return ((1ull << m) | bits((int)m)) - 1;
+  }
+  uint64_t zeta(int k) {
+    const uint64_t h = unary();
+    if (h * k + k > 64) throw std::runtime_error("zeta code too long");
+    const uint64_t left = 1ull << (h * k);
+    const uint64_t val = bits((int)(h * k + k - 1));
+    if (val < left) return val + left - 1;
+    return ((val << 1) | bits(1)) - 1;
+  }
+
+ private:
+  std::vector<uint8_t> d_;
+  uint64_t nbits_;
+  uint64_t pos_;
+};
+
 // 16-bit look-ahead table in the reference's layout: entry w = (code length << 16) |
 // value for the code that starts at the top of the 16-bit window w, 0 when the code
 // does not fit in 16 bits.  kind 0 = gamma, kind 3 = zeta_3.

@@ -157,25 +157,6 @@ static uint64_t build_select_samples(const std::vector<uint64_t>& upper, std::ve
   return ones;
 }
 
-static std::map<std::string, std::string> read_properties(const std::string& path) {
-  std::map<std::string, std::string> m;
-  std::vector<uint8_t> raw;
-  if (!read_file(path, raw)) return m;
-  std::string s(raw.begin(), raw.end());
-  size_t p = 0;
-  while (p < s.size()) {
-    size_t e = s.find('\n', p);
-    if (e == std::string::npos) e = s.size();
-    std::string line = s.substr(p, e - p);
-    p = e + 1;
-    if (line.empty() || line[0] == '#') continue;
-    const size_t eq = line.find('=');
-    if (eq == std::string::npos) continue;
-    m[line.substr(0, eq)] = line.substr(eq + 1);
-  }
-  return m;
-}
-
 template <class T>
 static int upload(GraphHandle& h, DevBuf& b, const std::vector<T>& v) {
   int rc = b.ensure(v.size() * sizeof(T));
@@ -209,10 +190,31 @@ int load_graph(GraphHandle& h, const std::string& dir, const std::string& base, 
   const std::pair<const char*, std::vector<uint8_t>*> idx[] = {
       {"/graph_lower_bits.bin", &gl}, {"/graph_upper_bits.bin", &gu},
       {"/timestamp_lower_bits.bin", &tl}, {"/timestamp_upper_bits.bin", &tu}};
+  std::string missing;
   for (const auto& f : idx)
-    if (!read_file(dir + f.first, *f.second))
-      return fail(TGA_E_IO, "Cannot open required file: " + dir + f.first + " (set TGA_COMPRESS_ROOT if needed)");
+    if (missing.empty() && !read_file(dir + f.first, *f.second)) missing = dir + f.first;
   if (ts.size() < 8) return fail(TGA_E_FORMAT, "timestamps file shorter than its 64-bit header");
+  if (!missing.empty()) {
+    // No GPU index files (a directory written by the Java encoder): rebuild their content from
+    // <base>.offsets and the streams (index_from_offsets).
+    std::vector<uint8_t> offsets;
+    if (!read_file(bp + ".offsets", offsets))
+      return fail(TGA_E_IO, "Cannot open required file: " + missing + " (nor " + bp +
+                                ".offsets to rebuild it; set TGA_COMPRESS_ROOT if needed)");
+    const auto pr = read_properties(bp + ".properties");
+    const auto it = pr.find("nodes");
+    if (it == pr.end()) return fail(TGA_E_FORMAT, "rebuilding the index needs the nodes property of " + bp + ".properties");
+    try {
+      EFIndex ge, te;
+      index_from_offsets(graph, offsets, ts, std::atoll(it->second.c_str()), 2, cfg.max_label, &ge, &te);
+      gl = std::move(ge.lower);
+      gu = std::move(ge.upper);
+      tl = std::move(te.lower);
+      tu = std::move(te.upper);
+    } catch (const std::exception& e) {
+      return fail(TGA_E_FORMAT, std::string("rebuilding the index from .offsets: ") + e.what());
+    }
+  }
   int64_t header = 0;
   for (int i = 0; i < 8; ++i) header = (int64_t)(((uint64_t)header << 8) | ts[(size_t)i]);
   if (cfg.min_timestamp != TGA_UNSET_TS && cfg.min_timestamp != header)

@@ -4,6 +4,7 @@
 #include <sys/stat.h>
 
 #include <algorithm>
+#include <map>
 #include <cerrno>
 #include <cmath>
 #include <cstdio>
@@ -246,6 +247,30 @@ EFIndex ef_build(const std::vector<uint64_t>& v, int l) {
   return ef;
 }
 
+void index_from_offsets(const std::vector<uint8_t>& graph, const std::vector<uint8_t>& offsets,
+                        const std::vector<uint8_t>& timestamps, int64_t n, int ts_zeta_k, int64_t max_label,
+                        EFIndex* graph_ef, EFIndex* ts_ef) {
+  if (n <= 0) throw std::runtime_error("vertex count needed (the nodes property)");
+  std::vector<uint64_t> goff((size_t)n + 1), toff((size_t)n + 1);
+  FastBitReader ob(offsets);
+  uint64_t at = 0;
+  for (int64_t v = 0; v <= n; ++v) {
+    at += ob.gamma();
+    if (at > (uint64_t)graph.size() * 8) throw std::runtime_error("offsets point past the end of the graph stream");
+    goff[(size_t)v] = at;
+  }
+  FastBitReader gb(graph), tb(timestamps, 64);
+  for (int64_t v = 0; v < n; ++v) {
+    gb.seek(goff[(size_t)v]);
+    const uint64_t deg = goff[(size_t)v + 1] > goff[(size_t)v] ? gb.gamma() : 0;
+    toff[(size_t)v] = tb.pos();
+    for (uint64_t i = 0; i < deg; ++i) tb.zeta(ts_zeta_k);
+  }
+  toff[(size_t)n] = tb.pos();
+  *graph_ef = ef_build(goff, ef_low_bits(graph.size(), max_label));
+  *ts_ef = ef_build(toff, ef_low_bits(timestamps.size(), max_label));
+}
+
 uint64_t ef_get_host(const EFIndex& ef, uint64_t i) {
   uint64_t low = 0;
   for (int b = 0; b < ef.l; ++b) {
@@ -403,6 +428,26 @@ WrittenDataset encode_and_write(const RawGraph& g, const std::string& dir, const
   ge.finish();
   te.finish();
   return write_dataset(dir, base, ge, te, g.n, max_label);
+}
+
+// key=value lines of a .properties file (missing file: empty map).
+std::map<std::string, std::string> read_properties(const std::string& path) {
+  std::map<std::string, std::string> m;
+  std::vector<uint8_t> raw;
+  if (!read_file(path, raw)) return m;
+  std::string s(raw.begin(), raw.end());
+  size_t p = 0;
+  while (p < s.size()) {
+    size_t e = s.find('\n', p);
+    if (e == std::string::npos) e = s.size();
+    std::string line = s.substr(p, e - p);
+    p = e + 1;
+    if (line.empty() || line[0] == '#') continue;
+    const size_t eq = line.find('=');
+    if (eq == std::string::npos) continue;
+    m[line.substr(0, eq)] = line.substr(eq + 1);
+  }
+  return m;
 }
 
 }  // namespace tga

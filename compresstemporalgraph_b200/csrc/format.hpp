@@ -17,6 +17,7 @@
 //                      bfs.cu:1785-1786).  The reference ships no producer for these files.
 #pragma once
 #include <cstdint>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -114,6 +115,17 @@ WrittenDataset write_dataset(const std::string& dir, const std::string& base, co
 WrittenDataset encode_and_write(const RawGraph& g, const std::string& dir, const std::string& base,
                                 int64_t max_label, const EncoderParams& p = {});
 
+// The four GPU index files' content for a directory that holds the webgraph offsets the Java
+// encoder writes instead of them: graph record offsets from <base>.offsets (n+1 gamma-coded deltas,
+// BVMultiGraph.java:1913-1922), each record's outdegree from the gamma at its start, and the
+// timestamp offsets by walking the timestamp stream (after its 64-bit header, outdegree(v) zeta_k
+// codes per vertex, EvolvingMultiGraph.java:131-275).  EF widths as the reference reader expects
+// (ef_low_bits of each stream).  Throws std::runtime_error on malformed input.
+void index_from_offsets(const std::vector<uint8_t>& graph, const std::vector<uint8_t>& offsets,
+                        const std::vector<uint8_t>& timestamps, int64_t n, int ts_zeta_k, int64_t max_label,
+                        EFIndex* graph_ef, EFIndex* ts_ef);
+
+std::map<std::string, std::string> read_properties(const std::string& path);
 bool write_file(const std::string& path, const void* data, size_t n);
 bool read_file(const std::string& path, std::vector<uint8_t>& out);
 

@@ -1,4 +1,5 @@
 // Host-only C entry points of the format layer (no GPU needed).
+#include <cstdlib>
 #include <cstring>
 #include <stdexcept>
 #include <string>
@@ -73,6 +74,30 @@ int tga_encode_raw(const char* raw_path, const char* dir, const char* base, int6
     fill_summary(out, w.n, w.m, maxdeg, w.graph_bytes, w.ts_bytes, w.index_bytes, w.stats);
   } catch (const std::exception& e) {
     return fail(TGA_E_FORMAT, e.what());
+  }
+  return TGA_OK;
+}
+
+int tga_build_index(const char* dir, const char* base, int64_t max_label) {
+  if (!dir || !base || max_label < 0) return fail(TGA_E_ARG, "bad argument");
+  const std::string d(dir), bp = d + "/" + base;
+  std::vector<uint8_t> graph, offsets, ts;
+  if (!read_file(bp + ".graph", graph)) return fail(TGA_E_IO, "Cannot open required file: " + bp + ".graph");
+  if (!read_file(bp + ".timestamps", ts)) return fail(TGA_E_IO, "Cannot open required file: " + bp + ".timestamps");
+  if (!read_file(bp + ".offsets", offsets)) return fail(TGA_E_IO, "Cannot open required file: " + bp + ".offsets");
+  const auto pr = read_properties(bp + ".properties");
+  const auto it = pr.find("nodes");
+  if (it == pr.end()) return fail(TGA_E_FORMAT, "the nodes property of " + bp + ".properties is needed");
+  try {
+    EFIndex ge, te;
+    index_from_offsets(graph, offsets, ts, std::atoll(it->second.c_str()), 2, max_label, &ge, &te);
+    if (!write_file(d + "/graph_lower_bits.bin", ge.lower.data(), ge.lower.size()) ||
+        !write_file(d + "/graph_upper_bits.bin", ge.upper.data(), ge.upper.size()) ||
+        !write_file(d + "/timestamp_lower_bits.bin", te.lower.data(), te.lower.size()) ||
+        !write_file(d + "/timestamp_upper_bits.bin", te.upper.data(), te.upper.size()))
+      return fail(TGA_E_IO, "cannot write the index files into " + d);
+  } catch (const std::exception& e) {
+    return fail(TGA_E_FORMAT, std::string("rebuilding the index from .offsets: ") + e.what());
   }
   return TGA_OK;
 }

@@ -328,6 +328,14 @@ int tga_generate(const tga_gen_params* p, const char* dir, const char* base, con
  * max_label < 0 -> n-1. */
 int tga_encode_raw(const char* raw_path, const char* dir, const char* base, int64_t max_label, tga_gen_summary* out);
 
+/* Producer of the four GPU index files (graph_{lower,upper}_bits.bin, timestamp_{lower,upper}_bits.bin,
+ * the layout read by sh/bfs.cu:543-565,1785-1789, for which the reference ships no producer) for a
+ * directory the Java encoder wrote: graph offsets from <base>.offsets (gamma deltas,
+ * BVMultiGraph.java:1913-1922), timestamp offsets by walking <base>.timestamps with each record's
+ * outdegree (EvolvingMultiGraph.java:131-275); needs the nodes property of <base>.properties.
+ * tga_open does the same in memory when the index files are missing. */
+int tga_build_index(const char* dir, const char* base, int64_t max_label);
+
 /* 65536-entry 16-bit look-ahead decode table, (length << 16) | value, 0 if the code does not fit;
  * kind 0 = gamma (gpu_cuda/decode_tables/gammaInA.txt), 3 = zeta_3 (zetaInA.txt). */
 int tga_decode_table(int32_t kind, int32_t* out);
