@@ -45,17 +45,23 @@ __global__ void TGA_SWEEP_BOUNDS k_neighbor_access(GraphView g, Work w, int32_t 
 }
 
 // Largest timestamp over all lists (a pass over the timestamp streams; run once at load).
+// Largest (out[0]) and smallest (out[1]) timestamp of the graph.
 __global__ void TGA_SWEEP_BOUNDS k_max_timestamp(GraphView g, Work w, long long* out) {
-  long long m = LLONG_MIN;
+  long long m = LLONG_MIN, mn = LLONG_MAX;
   run_order<false>(
       g, w, [&](int) { return true; }, [&](int, int, int) { return true; },
       [&](int, int, int64_t t) {
         m = max(m, (long long)t);
+        mn = min(mn, (long long)t);
         return true;
       },
       [&](int) {});
-  for (int o = 16; o; o >>= 1) m = max(m, __shfl_down_sync(0xffffffffu, m, o));
+  for (int o = 16; o; o >>= 1) {
+    m = max(m, __shfl_down_sync(0xffffffffu, m, o));
+    mn = min(mn, __shfl_down_sync(0xffffffffu, mn, o));
+  }
   if ((threadIdx.x & 31) == 0 && m != LLONG_MIN) atomicMax(out, m);
+  if ((threadIdx.x & 31) == 0 && mn != LLONG_MAX) atomicMin(out + 1, mn);
 }
 
 __global__ void k_small_flags(const int32_t* deg, uint8_t* small, int32_t begin, int32_t end) {
@@ -382,8 +388,13 @@ __global__ void TGA_DECODE_BOUNDS k_degree_slices(GraphView g, const SliceState*
   add_edges(edges, mine);
 }
 
+// kNarrow: every timestamp t of the graph satisfies 0 <= t - base < 2^31 (base = the smallest),
+// so the mean is carried as mean - base in 32 bits; t - mean and every intermediate are the same
+// integers as in 64 bits, and the recurrence's critical path is single-word arithmetic.
+template <bool kNarrow>
 __global__ void k_degree_long(const LongList* longs, int32_t nlong, const int32_t* outdeg, const int64_t* buf,
-                              int32_t active, int32_t max_label, int64_t s, int64_t e, int32_t* deg, int64_t* avg) {
+                              const uint2* divtab, int64_t base, int32_t active, int32_t max_label, int64_t s,
+                              int64_t e, int32_t* deg, int64_t* avg) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nlong) return;
   const int v = longs[i].v;
@@ -391,33 +402,85 @@ __global__ void k_degree_long(const LongList* longs, int32_t nlong, const int32_
   const int64_t* p = buf + longs[i].base;
   const int n = outdeg[v];
   int32_t d = 0;
-  int64_t mean = 0;
-  auto step = [&](int64_t t) {
+  int64_t mean = 0;     // 64-bit form
+  int32_t mean32 = 0;   // narrow form: mean - base
+  bool first = true;
+  // One step of the truncating mean, mean += (t - mean) / d (Java long division, towards zero);
+  // when |t - mean| < 2^32 the quotient is a multiply-high and two shifts with d's entry ml of the
+  // division table, off the divide sequence on the recurrence's critical path.
+  auto step = [&](int64_t t, uint2 ml) {
     if (t == kDcSkip) return;
     ++d;
-    const int64_t a = t - mean;
-    mean += (a >= INT32_MIN && a <= INT32_MAX) ? (int64_t)((int32_t)a / d) : a / d;
+    if constexpr (kNarrow) {
+      // The first step sets mean = t (d = 1); afterwards both are within [0, 2^31) of base.
+      const int32_t t32 = (int32_t)(t - base);
+      if (first) {
+        mean32 = t32;
+        first = false;
+        return;
+      }
+      const int32_t a = t32 - mean32;
+      const uint32_t x = (uint32_t)(a < 0 ? -a : a);
+      const uint32_t th = __umulhi(ml.x, x);
+      const int32_t q = (int32_t)((th + ((x - th) >> 1)) >> (ml.y - 1));
+      mean32 += a < 0 ? -q : q;
+    } else {
+      const int64_t a = t - mean;
+      const uint64_t na = (uint64_t)(a < 0 ? -a : a);
+      if (na <= 0xFFFFFFFFull) {
+        const uint32_t x = (uint32_t)na;
+        uint32_t q = x;
+        if (d > 1) {
+          const uint32_t th = __umulhi(ml.x, x);
+          q = (th + ((x - th) >> 1)) >> (ml.y - 1);
+        }
+        mean += a < 0 ? -(int64_t)q : (int64_t)q;
+      } else {
+        mean += a / d;
+      }
+    }
   };
   // The recurrence is sequential; its inputs are not, so they are loaded a batch ahead: the next
-  // batch's loads are in flight while the current batch is folded in.
+  // batch's timestamps and the table entries of the counts it reaches are in flight while the
+  // current batch is folded in.
   constexpr int kBatch = 16;
   int64_t cur[kBatch], nxt[kBatch];
+  uint2 mcur[kBatch], mnxt[kBatch];
+  auto table_for = [&](const int64_t* tb, int d0, uint2* mt) {
+    int dd = d0;
+#pragma unroll
+    for (int j = 0; j < kBatch; ++j) {
+      dd += tb[j] != kDcSkip;
+      mt[j] = __ldg(divtab + dd);
+    }
+    return dd;
+  };
   int k = 0;
   if (n >= kBatch) {
 #pragma unroll
     for (int j = 0; j < kBatch; ++j) cur[j] = __ldcs(p + j);
+    int dnext = table_for(cur, 0, mcur);
     for (k = kBatch; k + kBatch <= n; k += kBatch) {
 #pragma unroll
       for (int j = 0; j < kBatch; ++j) nxt[j] = __ldcs(p + k + j);
+      const int dafter = table_for(nxt, dnext, mnxt);
 #pragma unroll
-      for (int j = 0; j < kBatch; ++j) step(cur[j]);
+      for (int j = 0; j < kBatch; ++j) step(cur[j], mcur[j]);
 #pragma unroll
-      for (int j = 0; j < kBatch; ++j) cur[j] = nxt[j];
+      for (int j = 0; j < kBatch; ++j) {
+        cur[j] = nxt[j];
+        mcur[j] = mnxt[j];
+      }
+      dnext = dafter;
     }
 #pragma unroll
-    for (int j = 0; j < kBatch; ++j) step(cur[j]);
+    for (int j = 0; j < kBatch; ++j) step(cur[j], mcur[j]);
   }
-  for (; k < n; ++k) step(p[k]);
+  for (; k < n; ++k) {
+    const int64_t t = p[k];
+    step(t, __ldg(divtab + d + (t != kDcSkip)));
+  }
+  if constexpr (kNarrow) mean = d > 0 ? base + (int64_t)mean32 : 0;
   if (s != e) d = (int32_t)(0.85 * d + 0.15 * d * (double)(mean - s) / (double)(e - s) + 1);
   deg[v] = d;
   avg[v] = mean;
@@ -501,18 +564,20 @@ __global__ void k_gc_first(GraphView g, Work w, const int32_t* deg, int32_t n, i
 // Host side: the queue entries of one vertex (itself or its slices).
 int compute_max_timestamp(GraphHandle& h) {
   h.max_ts = INT64_MAX;
+  h.min_ts_data = INT64_MIN;
   if (int rc = h.s_sum.ensure(4096)) return rc;
   long long* out = reinterpret_cast<long long*>(h.s_sum.as<char>() + 3968);
-  const long long init = LLONG_MIN;
-  TGA_CUDA_TRY(cudaMemcpyAsync(out, &init, 8, cudaMemcpyHostToDevice, h.stream));
+  const long long init[2] = {LLONG_MIN, LLONG_MAX};
+  TGA_CUDA_TRY(cudaMemcpyAsync(out, init, 16, cudaMemcpyHostToDevice, h.stream));
   const Work w = work_of(h);
   k_max_timestamp<<<sweep_grid(h), kBlock, 0, h.stream>>>(h.view, w, out);
   TGA_CUDA_TRY(cudaGetLastError());
-  long long m = LLONG_MIN;
-  TGA_CUDA_TRY(cudaMemcpyAsync(&m, out, 8, cudaMemcpyDeviceToHost, h.stream));
+  long long m[2] = {LLONG_MIN, LLONG_MAX};
+  TGA_CUDA_TRY(cudaMemcpyAsync(m, out, 16, cudaMemcpyDeviceToHost, h.stream));
   TGA_CUDA_TRY(cudaStreamSynchronize(h.stream));
   if (int rc = h.check_device_error()) return rc;
-  h.max_ts = (m == LLONG_MIN) ? h.view.min_ts : (int64_t)m;
+  h.max_ts = (m[0] == LLONG_MIN) ? h.view.min_ts : (int64_t)m[0];
+  h.min_ts_data = (m[1] == LLONG_MAX) ? h.view.min_ts : (int64_t)m[1];
   return TGA_OK;
 }
 
@@ -751,9 +816,13 @@ int tga_degree(tga_graph* gp, int64_t t_start, int64_t t_end, int32_t* degree_ou
     KL(k_degree_slices, grid_for(h.nslices, kBlock))(h.view, h.d_slices.as<SliceState>(), h.d_slice_ebase.as<int64_t>(),
                                                      (int32_t)h.nslices, t_start, t_end, h.s_edges.as<int64_t>(), edges);
     h.kernel_end(ev2);
-    KL(k_degree_long, grid_for(h.nlong, kBlock))(h.d_long.as<LongList>(), h.nlong, h.d_deg.as<int32_t>(),
-                                                 h.s_edges.as<int64_t>(), h.view.active_begin, h.view.max_label,
-                                                 t_start, t_end, h.s_a.as<int32_t>(), h.s_b.as<int64_t>());
+    // Narrow form when the graph's whole timestamp span fits 31 bits (max_ts found at load).
+    const bool narrow = h.max_ts != INT64_MAX && h.min_ts_data >= 0 && h.max_ts - h.min_ts_data < INT32_MAX;
+    auto long_kernel = narrow ? k_degree_long<true> : k_degree_long<false>;
+    KL(long_kernel, grid_for(h.nlong, kBlock))(h.d_long.as<LongList>(), h.nlong, h.d_deg.as<int32_t>(),
+                                               h.s_edges.as<int64_t>(), h.d_divtab.as<uint2>(), h.min_ts_data,
+                                               h.view.active_begin, h.view.max_label, t_start, t_end,
+                                               h.s_a.as<int32_t>(), h.s_b.as<int64_t>());
   }
   KL(k_degree_empty, grid_for(nv, kBlock))(h.d_deg.as<int32_t>(), h.view.active_begin, h.view.max_label,
                                            std::min(nv, h.view.n), t_start, t_end, h.s_a.as<int32_t>());

@@ -50,7 +50,7 @@ GraphHandle::~GraphHandle() {
   for (DevBuf* b : {&d_graph, &d_ts, &d_gl, &d_gu, &d_gs, &d_tl, &d_tu, &d_ts_samples, &d_err, &d_deg, &d_slices,
                     &d_items, &d_slice_first, &d_slice_deep, &d_order, &d_runs, &d_run_pairs, &d_run_first, &d_long, &d_slice_ebase,
                     &d_view, &s_edges, &s_a, &s_b, &s_c, &s_d, &s_e, &s_f, &s_g, &s_q0, &s_q1, &s_cnt, &s_sum,
-                    &m_state, &m_mask, &m_dirty, &m_stamp, &m_touched, &m_dq})
+                    &m_state, &m_mask, &m_dirty, &m_stamp, &m_touched, &m_dq, &d_divtab})
     b->release();
   for (auto& k : ktimers) {
     if (k.a) cudaEventDestroy(k.a);
@@ -317,6 +317,20 @@ int load_graph(GraphHandle& h, const std::string& dir, const std::string& base, 
     return fail(TGA_E_FORMAT, "outdegrees sum to " + std::to_string(m) + " edges, more than the .timestamps stream can hold");
   // The largest outdegree caps every header-driven loop of the decoder on damaged streams.
   v.max_list = (int32_t)std::min<int64_t>(INT32_MAX / 4, std::max<int64_t>(maxd, 1));
+  {
+    // Per count d: l = ceil(log2 d) and m = floor(2^32 (2^l - d) / d) + 1, so that for any 32-bit
+    // n, n / d = (t + ((n - t) >> 1)) >> (l - 1) with t = mulhi(m, n) (Granlund and Montgomery,
+    // "Division by Invariant Integers using Multiplication", PLDI 1994, Fig. 4.1); d = 1 divides
+    // trivially.  Entry 0 is unused.
+    std::vector<uint32_t> tab(2 * ((size_t)v.max_list + 2), 0);
+    for (uint64_t d = 2; d < (uint64_t)v.max_list + 2; ++d) {
+      int l = 0;
+      while ((1ull << l) < d) ++l;
+      tab[2 * d] = (uint32_t)(((1ull << 32) * ((1ull << l) - d)) / d + 1);
+      tab[2 * d + 1] = (uint32_t)l;
+    }
+    if ((rc = upload(h, h.d_divtab, tab))) return rc;
+  }
   h.info_edges = m;
   h.degrees = std::move(deg);
   const char* env_slice = std::getenv("TGA_SLICE_EDGES");

@@ -52,6 +52,9 @@ struct GraphHandle {
   DevBuf d_graph, d_ts, d_gl, d_gu, d_gs, d_tl, d_tu, d_ts_samples, d_err;
   // per-vertex outdegrees (int32, filled once at load by a decode kernel)
   DevBuf d_deg;
+  // division by a running count d in [1, max outdegree] by multiplication: (m, l) per d (algos.cu,
+  // degree centrality); built at load
+  DevBuf d_divtab;
   // edge-balanced work decomposition (slices.cuh): slices of long lists, work items, and
   // slice_first[v]..slice_first[v+1] = slices of vertex v (empty for short lists)
   DevBuf d_slices, d_items, d_slice_first, d_slice_deep;
@@ -98,6 +101,7 @@ struct GraphHandle {
   bool time_kernels = true;
   int64_t info_edges = 0;            // total temporal edges (sum of outdegrees)
   int64_t max_ts = INT64_MAX;        // largest timestamp of the graph (computed at load)
+  int64_t min_ts_data = INT64_MIN;   // smallest timestamp of the graph (same pass)
   std::vector<int32_t> degrees;      // host copy of the outdegrees
 
   int begin_call();                 // resets timing, records the start event

@@ -51,8 +51,9 @@ int tga_generate(const tga_gen_params* p, const char* dir, const char* base, con
   g.min_timestamp = p->min_timestamp;
   g.seed = p->seed;
   g.ref_safe = p->ref_safe != 0;
-  if (g.n > INT32_MAX || g.ts_span <= 0 || g.min_timestamp < 0 || g.min_timestamp + g.ts_span > INT32_MAX)
-    return fail(TGA_E_ARG, "vertex ids and timestamps must fit in [0, 2^31)");
+  if (g.n > INT32_MAX || g.ts_span <= 0 || g.min_timestamp < 0 || g.ts_span > (INT64_C(1) << 62) ||
+      g.min_timestamp > (INT64_C(1) << 62))
+    return fail(TGA_E_ARG, "vertex ids must fit in [0, 2^31) and timestamps in [0, 2^63)");
   try {
     const GenSummary s = generate_dataset(g, dir, base, raw_path ? raw_path : "");
     fill_summary(out, s.n, s.m, s.max_degree, s.graph_bytes, s.ts_bytes, s.index_bytes, s.stats);

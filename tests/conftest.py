@@ -53,6 +53,9 @@ SHAPES = {
     # A few hubs holding most edges; bursty timestamps over a 1e8 span.
     "hubs": tga.GenParams(n=2000, m=100000, deg_exponent=1.5, max_degree=50000, repeat_frac=0.3, local_frac=0.7,
                           local_radius=64, pref_frac=0.5, copy_frac=0.2, ts_kind=2, ts_span=100_000_000, seed=9),
+    # Timestamps spread over 6e9 (more than 2^31): the 64-bit paths (degree-centrality mean).
+    "widespan": tga.GenParams(n=2000, m=60000, deg_exponent=1.6, max_degree=20000, repeat_frac=0.3, local_frac=0.7,
+                              local_radius=64, pref_frac=0.3, copy_frac=0.2, ts_kind=0, ts_span=6_000_000_000, seed=17),
     # Long runs of consecutive successors (intervals) and a non-zero minimum timestamp.
     "intervals": tga.GenParams(n=4000, m=80000, deg_exponent=2.2, repeat_frac=0.05, local_frac=1.0, local_radius=1,
                                copy_frac=0.1, ts_kind=1, ts_span=5_000_000, min_timestamp=1_206_214_540 - 5_000_000,

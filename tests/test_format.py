@@ -171,10 +171,13 @@ def test_open_missing_file_is_io_error(datasets, tmp_path):
     d = datasets["sparse"]
     work = tmp_path / "w"
     shutil.copytree(d["dir"], work)
+    # An index file alone is rebuilt from <base>.offsets (test_index_rebuild.py); without both the
+    # open fails before any device work, naming the missing files.
     (work / "timestamp_upper_bits.bin").unlink()
+    (work / f"{d['base']}.offsets").unlink()
     with pytest.raises(tga.TgaError) as e:
         tga.Graph.open_dir(work, d["base"], _cfg(d["summary"]["n"]))
-    assert e.value.code == tga.TGA_E_IO and "timestamp_upper_bits.bin" in str(e.value)
+    assert e.value.code == tga.TGA_E_IO and "timestamp_upper_bits.bin" in str(e.value) and ".offsets" in str(e.value)
 
 
 def test_open_wrong_min_timestamp_is_format_error(datasets):
@@ -223,6 +226,7 @@ def test_drop_in_path_convention(datasets, tmp_path, monkeypatch):
         name = f.name.replace(d["base"] + ".", "Sparse.")
         shutil.copy(f, dst / name)
     (dst / "graph_upper_bits.bin").unlink()
+    (dst / "Sparse.offsets").unlink()  # else the index is rebuilt from it
     monkeypatch.setenv("TGA_COMPRESS_ROOT", str(root) + "/")
     with pytest.raises(tga.TgaError) as e:
         tga.Graph.open(_cfg(d["summary"]["n"], storage_name="Sparse"))
