@@ -202,6 +202,11 @@ def batched_section(tga, g, n, span):
     import numpy as np
 
     L = tga.lib()
+    # The batched form runs under the project autotuner's choice of slice length, item size and
+    # dense-level divisor (tga_autotune; its probe and choice are reported).
+    t0 = time.perf_counter()
+    tune = g.autotune()
+    tune["wall_s"] = time.perf_counter() - t0
     rng = np.random.default_rng(3)
     src = rng.integers(0, n, 256).astype(np.int32)
     blo, bhi = random_windows(rng, 256, span)
@@ -226,7 +231,8 @@ def batched_section(tga, g, n, span):
             "queries_per_s": qs / ((bfs_batch_ms + pr_batch_ms) / 1e3),
             "plain_queries_per_s": qs / ((bfs_plain_ms + pr_plain_ms) / 1e3),
             "bfs_batch_ms": bfs_batch_ms, "bfs_plain_ms": bfs_plain_ms, "pr_batch_ms": pr_batch_ms,
-            "pr_plain_ms": pr_plain_ms, "timing": "device time (CUDA events), results left on the device"}
+            "pr_plain_ms": pr_plain_ms, "timing": "device time (CUDA events), results left on the device",
+            "autotune": tune}
 
 
 def served_section(tga, graphs, spans, load, count):

@@ -66,6 +66,11 @@ class _Query(C.Structure):
                 ("out", C.c_void_p)]
 
 
+class _TuneResult(C.Structure):
+    _fields_ = [("slice_edges", C.c_int32), ("item_edges", C.c_int32), ("dense_div", C.c_int32),
+                ("candidates", C.c_int32), ("best_ms", C.c_double), ("default_ms", C.c_double)]
+
+
 class _ServerStats(C.Structure):
     _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("failed", C.c_int64), ("rounds", C.c_int64),
                 ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("mean_ms", C.c_double), ("queries_per_s", C.c_double)]
@@ -133,6 +138,7 @@ def _load() -> C.CDLL:
                                    C.POINTER(_GenSummary)]),
         "tga_encode_raw": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int64, C.POINTER(_GenSummary)]),
         "tga_build_index": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int64]),
+        "tga_autotune": (C.c_int, [P, P]),
         "tga_decode_table": (C.c_int, [C.c_int32, P]),
         "tga_encode_codes": (C.c_int, [C.c_int32, C.c_int32, P, C.c_int64, P, C.c_int64, C.POINTER(C.c_int64)]),
         "tga_ef_encode": (C.c_int, [P, C.c_int64, C.c_int32, P, C.c_int64, P, C.c_int64, C.POINTER(C.c_int64),
@@ -253,6 +259,12 @@ class Graph:
 
     def set_work_params(self, slice_edges: int, item_edges: int) -> None:
         _check(_lib.tga_set_work_params(self._h, slice_edges, item_edges))
+
+    def autotune(self) -> dict:
+        """Picks slice length, item size and dense-level divisor by timing (tga_autotune)."""
+        r = _TuneResult()
+        _check(_lib.tga_autotune(self._h, C.byref(r)))
+        return {k: getattr(r, k) for k, _ in _TuneResult._fields_}
 
     def work_params(self) -> dict:
         a, b, c, d = C.c_int32(), C.c_int32(), C.c_int64(), C.c_int32()

@@ -523,7 +523,7 @@ int build_work(GraphHandle& h, int32_t slice_len, int32_t item_edges) {
   // A traversal level sweeps all lists instead of its queue once the queue holds at least
   // 1/TGA_DENSE_DIV (default 16) of the schedule's entries.
   const char* env_dense = std::getenv("TGA_DENSE_DIV");
-  const int dense_div = env_dense ? std::max(1, std::atoi(env_dense)) : 16;
+  const int dense_div = h.dense_div > 0 ? h.dense_div : env_dense ? std::max(1, std::atoi(env_dense)) : 16;
   h.dense_min = std::max<int32_t>(1, h.norder / dense_div);
   h.nslices = (int64_t)packed.size();
   h.slice_len = slice_len;
@@ -662,6 +662,72 @@ int tga_set_work_params(tga_graph* g, int32_t slice_edges, int32_t item_edges) {
   if (!g) return fail(TGA_E_ARG, "null graph");
   if (cudaStreamSynchronize(g->stream) != cudaSuccess) return fail(TGA_E_CUDA, "stream synchronisation failed");
   return build_work(*g, slice_edges, item_edges);
+}
+
+// Autotuner: times the workloads whose speed depends on the work decomposition (one PageRank and
+// one HITS iteration, a full-window BFS, a full-window CC and a CC over the middle half of the
+// timestamp span; each run twice, the second timed) for each candidate and keeps the fastest
+// total.  Slice length and item size are tried as a grid, then the dense-level divisor at the
+// best of those.
+int tga_autotune(tga_graph* g, tga_tune_result* out) {
+  if (!g) return fail(TGA_E_ARG, "null graph");
+  GraphHandle& h = *g;
+  const int64_t span = h.max_ts - h.view.min_ts;
+  const int64_t wlo = h.view.min_ts + span / 4, whi = h.view.min_ts + 3 * (span / 4) + 1;
+  auto probe = [&](double* ms) -> int {
+    double total = 0;
+    for (int w = 0; w < 5; ++w)
+      for (int rep = 0; rep < 2; ++rep) {
+        int rc;
+        if (w == 0) rc = tga_pagerank(g, 1, 0.85f, 0.1f, TGA_T_MIN, TGA_T_MAX, nullptr);
+        else if (w == 1) rc = tga_hits(g, 1, TGA_HITS_GPU, TGA_T_MIN, TGA_T_MAX, nullptr, nullptr);
+        else if (w == 2) rc = tga_bfs(g, -1, TGA_T_MIN, TGA_T_MAX, nullptr, nullptr);
+        else if (w == 3) rc = tga_cc(g, TGA_T_MIN, TGA_T_MAX, TGA_CC_EARLY_EXIT, nullptr, nullptr);
+        else rc = tga_cc(g, wlo, whi, TGA_CC_EARLY_EXIT, nullptr, nullptr);
+        if (rc) return rc;
+        if (rep == 1) total += h.timing.total_ms;
+      }
+    *ms = total;
+    return TGA_OK;
+  };
+  if (cudaStreamSynchronize(h.stream) != cudaSuccess) return fail(TGA_E_CUDA, "stream synchronisation failed");
+  tga_tune_result r{};
+  r.slice_edges = h.slice_len;
+  r.item_edges = h.item_edges;
+  r.dense_div = h.dense_div > 0 ? h.dense_div : 16;
+  TGA_TRY(probe(&r.default_ms));
+  r.best_ms = r.default_ms;
+  r.candidates = 1;
+  for (int32_t sl : {16, 24, 32, 48})
+    for (int32_t it : {128, 256, 512}) {
+      if (sl == r.slice_edges && it == r.item_edges) continue;
+      TGA_TRY(build_work(h, sl, it));
+      double ms = 0;
+      TGA_TRY(probe(&ms));
+      ++r.candidates;
+      if (ms < r.best_ms) {
+        r.best_ms = ms;
+        r.slice_edges = sl;
+        r.item_edges = it;
+      }
+    }
+  const int32_t base_div = r.dense_div;
+  for (int32_t dd : {8, 16, 32}) {
+    if (dd == base_div) continue;
+    h.dense_div = dd;
+    TGA_TRY(build_work(h, r.slice_edges, r.item_edges));
+    double ms = 0;
+    TGA_TRY(probe(&ms));
+    ++r.candidates;
+    if (ms < r.best_ms) {
+      r.best_ms = ms;
+      r.dense_div = dd;
+    }
+  }
+  h.dense_div = r.dense_div;
+  TGA_TRY(build_work(h, r.slice_edges, r.item_edges));
+  if (out) *out = r;
+  return TGA_OK;
 }
 
 int tga_get_work_params(tga_graph* g, int32_t* slice_edges, int32_t* item_edges, int64_t* slices, int32_t* items) {

@@ -73,6 +73,7 @@ struct GraphHandle {
   DevBuf d_view;                     // device-global copy of `view` (GraphView::self)
   int32_t norder = 0;
   int32_t dense_min = 1;             // traversal levels with at least this many entries sweep all lists
+  int32_t dense_div = 0;             // dense_min = schedule entries / dense_div (0: $TGA_DENSE_DIV or 16)
   std::vector<uint8_t> chain_host;   // list copies from a reference chain
   int32_t nitems = 0, nslice_items = 0;
   int64_t nslices = 0;
@@ -138,6 +139,13 @@ size_t cc_cache_bytes(const GraphHandle& h);
 // (batch.cu); same results as the one-seed-at-a-time loop.
 int cc_seed_batches(GraphHandle& h, int64_t t_lo, int64_t t_hi, int32_t flags, int32_t* label_out,
                     int32_t* components_out);
+
+// Returns the status of expr from the calling function when it is not TGA_OK.
+#define TGA_TRY(expr)            \
+  do {                           \
+    int rc_ = (expr);            \
+    if (rc_) return rc_;         \
+  } while (0)
 
 // Launch helpers shared by the algorithm files.
 inline unsigned grid_for(int64_t items, int block) { return (unsigned)((items + block - 1) / block); }

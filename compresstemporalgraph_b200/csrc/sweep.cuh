@@ -347,12 +347,6 @@ static unsigned decode_grid(const GraphHandle& h, int64_t work) {
 // Grid of a sweep over the schedule: one entry per thread.
 static unsigned sweep_grid(const GraphHandle& h) { return std::max(1u, grid_for(h.norder, kBlock)); }
 
-#define TGA_TRY(expr)            \
-  do {                           \
-    int rc_ = (expr);            \
-    if (rc_) return rc_;         \
-  } while (0)
-
 static int finish(GraphHandle& h, unsigned long long* edges_dev) {
   if (edges_dev) {
     unsigned long long e = 0;

@@ -103,6 +103,19 @@ int tga_get_timing(tga_graph* g, tga_timing* out);
 int tga_set_work_params(tga_graph* g, int32_t slice_edges, int32_t item_edges);
 int tga_get_work_params(tga_graph* g, int32_t* slice_edges, int32_t* item_edges, int64_t* slices, int32_t* items);
 
+/* Project autotuner (no reference counterpart): times the workloads whose speed depends on the
+ * work decomposition (one PageRank and one HITS iteration, a full-window BFS, a full-window CC and
+ * a CC over the middle half of the timestamp span) for slice lengths {16, 24, 32, 48} x item sizes {128, 256, 512}, then the
+ * dense-level divisor {8, 16, 32} (a traversal level sweeps every list once its queue holds
+ * 1/dense_div of the schedule), and leaves the graph configured with the fastest.  Results of
+ * every call are independent of the choice.  CC jobs made before it refuse to run afterwards. */
+typedef struct {
+  int32_t slice_edges, item_edges, dense_div;  /* chosen */
+  int32_t candidates;                          /* configurations timed */
+  double best_ms, default_ms;                  /* probe time of the chosen and of the starting one */
+} tga_tune_result;
+int tga_autotune(tga_graph* g, tga_tune_result* out);
+
 /* cudaStream_t of the handle, as an opaque pointer (all work of the handle runs on it). */
 void* tga_stream(tga_graph* g);
 

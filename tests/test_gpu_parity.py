@@ -246,6 +246,29 @@ def test_cc_after_work_decomposition_change(pairs):
         p.g.set_work_params(default["slice_edges"], default["item_edges"])
 
 
+def test_autotune_keeps_results(pairs):
+    """The autotuner picks a configuration from its candidate sets, no slower than the starting
+    one on its own probe, and every result stays equal to the oracle under it."""
+    p = pairs["hubs"]
+    default = p.g.work_params()
+    try:
+        r = p.g.autotune()
+        assert r["slice_edges"] in (16, 24, 32, 48) and r["item_edges"] in (128, 256, 512)
+        # the starting configuration is timed once (one fewer grid point when it lies on the grid)
+        assert r["dense_div"] in (8, 16, 32) and r["candidates"] in (14, 15)
+        assert 0 < r["best_ms"] <= r["default_ms"]
+        assert p.g.work_params()["slice_edges"] == r["slice_edges"]
+        off, dst, ts = p.g.decode_all()
+        ooff, odst, ots = p.o.csr()
+        assert np.array_equal(dst, odst) and np.array_equal(ts, ots)
+        lo, hi = _windows(p)[1]
+        lab, k = p.g.connected_components(lo, hi)
+        olab, ok = p.o.cc(p.ml, p.mv, p.act, p.cfg.connected_components_vertex_begin, lo, hi, True)
+        assert k == ok and np.array_equal(lab, olab)
+    finally:
+        p.g.set_work_params(default["slice_edges"], default["item_edges"])
+
+
 def test_multi_source_state_survives_other_calls(pairs):
     """The batched traversal keeps its per-source arrays between calls and resets only the
     vertices the previous traversal touched; single-source traversals, batched CC and batched
