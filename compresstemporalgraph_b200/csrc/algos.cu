@@ -722,14 +722,21 @@ int tga_pagerank(tga_graph* gp, int32_t iters, float damping, float alpha, int64
     KL(k_invert, grid_for(nv, kBlock))(cnt, invdeg, nv);
   }
   const unsigned grid = sweep_grid(h);
-  for (int k = 0; k < iters; ++k) {
-    const Work w = work_of(h);
-    PrArgs a{invdeg, h.d_deg.as<int32_t>(), bufs[k % 3], bufs[(k + 1) % 3], bufs[(k + 2) % 3], sums, k,
-             damping, alpha, base, t_lo, t_hi, edges};
-    cudaEvent_t* ev = h.kernel_begin();
-    KL(k_pr_iter, grid)(h.view, w, a);
-    h.kernel_end(ev);
-  }
+  // The iterations as one CUDA graph, replayed by later calls with the same parameters.
+  const std::vector<uint64_t> key = {ptr_key(bufs[0]), ptr_key(bufs[1]), ptr_key(bufs[2]), ptr_key(sums),
+                                     ptr_key(invdeg), ptr_key(edges), (uint64_t)iters, (uint64_t)grid, (uint64_t)nv,
+                                     bits_of(damping), bits_of(alpha), (uint64_t)t_lo, (uint64_t)t_hi};
+  TGA_TRY(run_loop(h, h.pr_loop, key, (size_t)iters, [&]() -> int {
+    for (int k = 0; k < iters; ++k) {
+      const Work w = work_of(h);
+      PrArgs a{invdeg, h.d_deg.as<int32_t>(), bufs[k % 3], bufs[(k + 1) % 3], bufs[(k + 2) % 3], sums, k,
+               damping, alpha, base, t_lo, t_hi, edges};
+      cudaEvent_t* ev = h.kernel_begin();
+      KL(k_pr_iter, grid)(h.view, w, a);
+      h.kernel_end(ev);
+    }
+    return TGA_OK;
+  }));
   float* out = bufs[iters % 3];
   float* fin = h.s_d.as<float>();
   KL(k_pr_final, grid_for(nv, kBlock))(out, sums, iters - 1, fin, nv);
@@ -764,27 +771,35 @@ int tga_hits(tga_graph* gp, int32_t iters, int32_t mode, int64_t t_lo, int64_t t
   KL(k_fill_f32, grid_for(nv, kBlock))(hub, 1.0f, nv);
   KL(k_fill_f32, grid_for(nv, kBlock))(auth[0], 1.0f, nv);
   cudaMemsetAsync(sums, 0, (size_t)(2 * iters + 2) * 8, h.stream);
-  // sums[2k] = sum hub^2 of iteration k, sums[2k+1] = sum auth^2 of iteration k.
-  for (int k = 0; k < iters; ++k) {
-    const double* aprev = k == 0 ? nullptr : sums + 2 * k - 1;
-    float* ain = auth[k & 1];
-    float* anext = auth[(k + 1) & 1];
-    KL(k_hits_base, grid_for(nv, kBlock))(hub, ain, anext, aprev, java, nv);
-    Work w = work_of(h);
-    cudaEvent_t* ev = h.kernel_begin();
-    // (without decoded timestamps every edge reports t = 0, so the window check is opened fully)
-    if (all_times) KL(k_hits_hub<false>, sweep_grid(h))(h.view, w, hub, ain, aprev, INT64_MIN, INT64_MAX, edges);
-    else KL(k_hits_hub<true>, sweep_grid(h))(h.view, w, hub, ain, aprev, t_lo, t_hi, edges);
-    h.kernel_end(ev);
-    KL(k_sumsq, grid_for(nv, kBlock))(hub, nv, sums + 2 * k);
-    w = work_of(h);
-    ev = h.kernel_begin();
-    if (all_times) KL(k_hits_auth<false>, sweep_grid(h))(h.view, w, hub, sums + 2 * k, anext, INT64_MIN, INT64_MAX, edges);
-    else KL(k_hits_auth<true>, sweep_grid(h))(h.view, w, hub, sums + 2 * k, anext, t_lo, t_hi, edges);
-    h.kernel_end(ev);
-    KL(k_scale, grid_for(nv, kBlock))(hub, sums + 2 * k, hub, nv);
-    KL(k_sumsq, grid_for(nv, kBlock))(anext, nv, sums + 2 * k + 1);
-  }
+  // sums[2k] = sum hub^2 of iteration k, sums[2k+1] = sum auth^2 of iteration k.  The iterations
+  // run as one CUDA graph, replayed by later calls with the same parameters.
+  const std::vector<uint64_t> key = {ptr_key(hub), ptr_key(auth[0]), ptr_key(auth[1]), ptr_key(sums), ptr_key(edges),
+                                     (uint64_t)iters, (uint64_t)java, (uint64_t)all_times, (uint64_t)nv,
+                                     (uint64_t)t_lo, (uint64_t)t_hi};
+  TGA_TRY(run_loop(h, h.hits_loop, key, (size_t)(2 * iters), [&]() -> int {
+    for (int k = 0; k < iters; ++k) {
+      const double* aprev = k == 0 ? nullptr : sums + 2 * k - 1;
+      float* ain = auth[k & 1];
+      float* anext = auth[(k + 1) & 1];
+      KL(k_hits_base, grid_for(nv, kBlock))(hub, ain, anext, aprev, java, nv);
+      Work w = work_of(h);
+      cudaEvent_t* ev = h.kernel_begin();
+      // (without decoded timestamps every edge reports t = 0, so the window check is opened fully)
+      if (all_times) KL(k_hits_hub<false>, sweep_grid(h))(h.view, w, hub, ain, aprev, INT64_MIN, INT64_MAX, edges);
+      else KL(k_hits_hub<true>, sweep_grid(h))(h.view, w, hub, ain, aprev, t_lo, t_hi, edges);
+      h.kernel_end(ev);
+      KL(k_sumsq, grid_for(nv, kBlock))(hub, nv, sums + 2 * k);
+      w = work_of(h);
+      ev = h.kernel_begin();
+      if (all_times)
+        KL(k_hits_auth<false>, sweep_grid(h))(h.view, w, hub, sums + 2 * k, anext, INT64_MIN, INT64_MAX, edges);
+      else KL(k_hits_auth<true>, sweep_grid(h))(h.view, w, hub, sums + 2 * k, anext, t_lo, t_hi, edges);
+      h.kernel_end(ev);
+      KL(k_scale, grid_for(nv, kBlock))(hub, sums + 2 * k, hub, nv);
+      KL(k_sumsq, grid_for(nv, kBlock))(anext, nv, sums + 2 * k + 1);
+    }
+    return TGA_OK;
+  }));
   float* auth_fin = auth[iters & 1];
   float* out_auth = auth[(iters + 1) & 1];
   KL(k_scale, grid_for(nv, kBlock))(auth_fin, sums + 2 * iters - 1, out_auth, nv);

@@ -1422,42 +1422,50 @@ static int pagerank_multi_batch(GraphHandle& h, int32_t nq, const int32_t* iters
     KL(k_invert_multi, grid_for((int64_t)vec, kBlock))(cnt, invdeg, (int64_t)vec);
   }
   float* out = h.s_e.as<float>();
-  for (int k = 0; k < maxit; ++k) {
-    Work w = work_of(h);
-    PrMultiArgs a{};
-    a.invdeg = invdeg;
-    a.deg = h.d_deg.as<int32_t>();
-    a.in = bufs[k % 3];
-    a.out = bufs[(k + 1) % 3];
-    a.reset = bufs[(k + 2) % 3];
-    a.sums_prev = k == 0 ? nullptr : sums + (size_t)(k - 1) * kMaxRankQueries;
-    a.lo = dlo;
-    a.hi = dhi;
-    a.run_first = drf;
-    a.windowed = windowed;
-    uint32_t active = 0, done = 0;
-    for (int q = 0; q < nq; ++q) {
-      if (iters[q] > k) active |= 1u << q;
-      if (iters[q] == k + 1) done |= 1u << q;
+  // The iterations as one CUDA graph, replayed by later calls with the same parameters.
+  std::vector<uint64_t> key = {ptr_key(bufs[0]), ptr_key(invdeg), ptr_key(sums), ptr_key(part), ptr_key(drf),
+                               ptr_key(out), ptr_key(edges), (uint64_t)nq, (uint64_t)S, (uint64_t)nv,
+                               (uint64_t)windowed, bits_of(damping), bits_of(alpha), ptr_key(dlo)};
+  for (int q = 0; q < nq; ++q) key.push_back((uint64_t)iters[q]);
+  TGA_TRY(run_loop(h, h.prm_loop, key, (size_t)maxit, [&]() -> int {
+    for (int k = 0; k < maxit; ++k) {
+      Work w = work_of(h);
+      PrMultiArgs a{};
+      a.invdeg = invdeg;
+      a.deg = h.d_deg.as<int32_t>();
+      a.in = bufs[k % 3];
+      a.out = bufs[(k + 1) % 3];
+      a.reset = bufs[(k + 2) % 3];
+      a.sums_prev = k == 0 ? nullptr : sums + (size_t)(k - 1) * kMaxRankQueries;
+      a.lo = dlo;
+      a.hi = dhi;
+      a.run_first = drf;
+      a.windowed = windowed;
+      uint32_t active = 0, done = 0;
+      for (int q = 0; q < nq; ++q) {
+        if (iters[q] > k) active |= 1u << q;
+        if (iters[q] == k + 1) done |= 1u << q;
+      }
+      a.active = active;
+      a.nq = nq;
+      a.nv = (int32_t)nv;
+      a.S = S;
+      a.damping = damping;
+      a.alpha = alpha;
+      a.base = base;
+      a.edges = edges;
+      cudaEvent_t* ev = h.kernel_begin();
+      KL(k_pr_multi_iter, sweep_grid(h))(h.view, w, a);
+      h.kernel_end(ev);
+      k_sums_multi_part<<<dim3(kSumParts, nq), kBlock, 0, h.stream>>>(a.out, (int32_t)nv, S, part);
+      k_sums_multi_fin<<<1, kMaxRankQueries, 0, h.stream>>>(part, nq, sums + (size_t)k * kMaxRankQueries);
+      h.timing.launches += 2;
+      if (done)
+        KL(k_pr_multi_final, grid_for((int64_t)nq * (int64_t)nv, kBlock))(a.out, sums + (size_t)k * kMaxRankQueries, done,
+                                                                          nq, (int32_t)nv, S, out);
     }
-    a.active = active;
-    a.nq = nq;
-    a.nv = (int32_t)nv;
-    a.S = S;
-    a.damping = damping;
-    a.alpha = alpha;
-    a.base = base;
-    a.edges = edges;
-    cudaEvent_t* ev = h.kernel_begin();
-    KL(k_pr_multi_iter, sweep_grid(h))(h.view, w, a);
-    h.kernel_end(ev);
-    k_sums_multi_part<<<dim3(kSumParts, nq), kBlock, 0, h.stream>>>(a.out, (int32_t)nv, S, part);
-    k_sums_multi_fin<<<1, kMaxRankQueries, 0, h.stream>>>(part, nq, sums + (size_t)k * kMaxRankQueries);
-    h.timing.launches += 2;
-    if (done)
-      KL(k_pr_multi_final, grid_for((int64_t)nq * (int64_t)nv, kBlock))(a.out, sums + (size_t)k * kMaxRankQueries, done,
-                                                                        nq, (int32_t)nv, S, out);
-  }
+    return TGA_OK;
+  }));
   if (rank_out) TGA_CUDA_TRY(cudaMemcpyAsync(rank_out, out, (size_t)nq * nv * 4, cudaMemcpyDeviceToHost, h.stream));
   h.timing.iterations = maxit;
   const int rc = finish(h, edges);

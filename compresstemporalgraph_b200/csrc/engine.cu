@@ -56,6 +56,8 @@ GraphHandle::~GraphHandle() {
     if (k.a) cudaEventDestroy(k.a);
     if (k.b) cudaEventDestroy(k.b);
   }
+  for (LoopGraph* lg : {&pr_loop, &hits_loop, &prm_loop})
+    if (lg->exec) cudaGraphExecDestroy(lg->exec);
   if (ev_begin) cudaEventDestroy(ev_begin);
   if (ev_end) cudaEventDestroy(ev_end);
   if (h_pinned) cudaFreeHost(h_pinned);
@@ -71,6 +73,16 @@ int GraphHandle::begin_call() {
   return TGA_OK;
 }
 
+int GraphHandle::reserve_timers(size_t n) {
+  while (ktimers.size() < ktimer_used + n) {
+    KernelTimer k;
+    if (cudaEventCreate(&k.a) != cudaSuccess || cudaEventCreate(&k.b) != cudaSuccess)
+      return fail(TGA_E_CUDA, "cannot create timing events");
+    ktimers.push_back(k);
+  }
+  return TGA_OK;
+}
+
 cudaEvent_t* GraphHandle::kernel_begin() {
   if (!time_kernels) return nullptr;
   if (ktimer_used == ktimers.size()) {
@@ -79,14 +91,18 @@ cudaEvent_t* GraphHandle::kernel_begin() {
     ktimers.push_back(k);
   }
   KernelTimer& k = ktimers[ktimer_used++];
-  cudaEventRecord(k.a, stream);
+  // Inside a capture the record must be a graph node of its own (an external record), so the
+  // replayed graph still times the kernel.
+  if (capturing) cudaEventRecordWithFlags(k.a, stream, cudaEventRecordExternal);
+  else cudaEventRecord(k.a, stream);
   return &k.a;
 }
 
 void GraphHandle::kernel_end(cudaEvent_t* pair) {
   if (!pair) return;
   KernelTimer* k = reinterpret_cast<KernelTimer*>(pair);
-  cudaEventRecord(k->b, stream);
+  if (capturing) cudaEventRecordWithFlags(k->b, stream, cudaEventRecordExternal);
+  else cudaEventRecord(k->b, stream);
   timing.decode_launches++;
 }
 

@@ -36,6 +36,16 @@ struct KernelTimer {
   cudaEvent_t a = nullptr, b = nullptr;
 };
 
+// An instantiated CUDA graph of an iteration loop (sweep.cuh, run_loop), kept on the handle and
+// replayed while everything baked into its launches (its key) stays the same.
+struct LoopGraph {
+  cudaGraphExec_t exec = nullptr;
+  std::vector<uint64_t> key;
+  size_t timers = 0;      // kernel timer pairs the loop records
+  int64_t launches = 0;   // kernels the loop launches
+  int64_t decodes = 0;    // of those, decode launches (timing.decode_launches)
+};
+
 struct CcJobDeleter {
   void operator()(tga_cc_job* j) const;
 };
@@ -100,6 +110,8 @@ struct GraphHandle {
   size_t ktimer_used = 0;
   tga_timing timing{};
   bool time_kernels = true;
+  bool capturing = false;            // a loop is being captured into a CUDA graph (run_loop)
+  LoopGraph pr_loop, hits_loop, prm_loop;
   int64_t info_edges = 0;            // total temporal edges (sum of outdegrees)
   int64_t max_ts = INT64_MAX;        // largest timestamp of the graph (computed at load)
   int64_t min_ts_data = INT64_MIN;   // smallest timestamp of the graph (same pass)
@@ -108,6 +120,7 @@ struct GraphHandle {
   int begin_call();                 // resets timing, records the start event
   int end_call();                   // records the end event, syncs, checks the device error word
   cudaEvent_t* kernel_begin();      // event pair around one decode launch (nullptr if disabled)
+  int reserve_timers(size_t n);     // creates event pairs so that n more kernel_begin calls find them
   void kernel_end(cudaEvent_t* pair);
   int check_device_error();
   ~GraphHandle();

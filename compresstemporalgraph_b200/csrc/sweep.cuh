@@ -347,6 +347,65 @@ static unsigned decode_grid(const GraphHandle& h, int64_t work) {
 // Grid of a sweep over the schedule: one entry per thread.
 static unsigned sweep_grid(const GraphHandle& h) { return std::max(1u, grid_for(h.norder, kBlock)); }
 
+// Runs body (which enqueues an iteration loop on h.stream and returns a status) through a CUDA
+// graph: captured and instantiated the first time `key` is seen, replayed while it stays the
+// same.  The key must hold every pointer and value baked into the loop's launches; the handle's
+// decomposition generation, the view and the index of the first kernel timer are added here.
+// timers: kernel timer pairs the loop records (created before the capture starts).
+template <class Body>
+static int run_loop(GraphHandle& h, LoopGraph& lg, std::vector<uint64_t> key, size_t timers, Body body) {
+  key.push_back(h.work_gen);
+  key.push_back((uint64_t)(uintptr_t)h.view.self);
+  key.push_back((uint64_t)h.ktimer_used);
+  key.push_back(h.time_kernels ? 1u : 0u);
+  if (lg.exec && lg.key == key && h.ktimer_used + lg.timers <= h.ktimers.size()) {
+    h.ktimer_used += lg.timers;
+    h.timing.launches += lg.launches;
+    h.timing.decode_launches += lg.decodes;
+    TGA_CUDA_TRY(cudaGraphLaunch(lg.exec, h.stream));
+    return TGA_OK;
+  }
+  if (lg.exec) {
+    cudaGraphExecDestroy(lg.exec);
+    lg.exec = nullptr;
+  }
+  const size_t t0 = h.ktimer_used;
+  const int64_t l0 = h.timing.launches, d0 = h.timing.decode_launches;
+  if (h.time_kernels) TGA_TRY(h.reserve_timers(timers));
+  TGA_CUDA_TRY(cudaStreamBeginCapture(h.stream, cudaStreamCaptureModeThreadLocal));
+  h.capturing = true;
+  const int brc = body();
+  h.capturing = false;
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ec = cudaStreamEndCapture(h.stream, &graph);
+  if (brc || ec != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    return brc ? brc : fail(TGA_E_CUDA, std::string("loop capture failed: ") + cudaGetErrorString(ec));
+  }
+  cudaGraphExec_t exec = nullptr;
+  const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ei != cudaSuccess) {
+    cudaGetLastError();
+    return fail(TGA_E_CUDA, std::string("loop graph instantiation failed: ") + cudaGetErrorString(ei));
+  }
+  lg.exec = exec;
+  lg.key = std::move(key);
+  lg.timers = h.ktimer_used - t0;
+  lg.launches = h.timing.launches - l0;
+  lg.decodes = h.timing.decode_launches - d0;
+  TGA_CUDA_TRY(cudaGraphLaunch(exec, h.stream));
+  return TGA_OK;
+}
+
+static inline uint64_t bits_of(double x) {
+  uint64_t b;
+  std::memcpy(&b, &x, 8);
+  return b;
+}
+static inline uint64_t ptr_key(const void* p) { return (uint64_t)(uintptr_t)p; }
+
 static int finish(GraphHandle& h, unsigned long long* edges_dev) {
   if (edges_dev) {
     unsigned long long e = 0;

@@ -419,9 +419,11 @@ def test_batched_pagerank_many_queries_vs_oracle(pairs, shape):
 
 def test_timing_reports_device_time(pairs):
     p = pairs["small"]
-    p.g.pagerank(3)
-    t = p.g.timing()
-    assert t["total_ms"] > 0 and t["decode_ms"] > 0 and t["decode_launches"] == 3
+    for _ in range(2):  # the first call captures the iteration loop as a CUDA graph, the second replays it
+        p.g.pagerank(3)
+        t = p.g.timing()
+        assert t["total_ms"] > 0 and t["decode_ms"] > 0 and t["decode_launches"] == 3
+        assert t["decode_ms"] <= t["total_ms"] * 1.01
     assert t["edges_decoded"] == 3 * p.o.m - 3 * int(np.diff(p.o.csr()[0])[p.ml:].sum())
 
 
