@@ -193,7 +193,7 @@ def random_windows(rng, k, span, lo_frac=0.05, hi_frac=0.5):
     return lo.astype(np.int64), (lo + w).astype(np.int64)
 
 
-def batched_section(tga, g, n, span):
+def batched_section(tga, g, n, span, tune=True, plain_bfs=256, plain_pr=32):
     """256 windowed BFS sources as one batched traversal and 32 windowed PageRanks (20 iterations)
     as one strided vector, against the same queries one call each.  Results stay on the device
     (NULL outputs) on both sides, so the comparison is the device work of the two forms."""
@@ -204,9 +204,12 @@ def batched_section(tga, g, n, span):
     L = tga.lib()
     # The batched form runs under the project autotuner's choice of slice length, item size and
     # dense-level divisor (tga_autotune; its probe and choice are reported).
-    t0 = time.perf_counter()
-    tune = g.autotune()
-    tune["wall_s"] = time.perf_counter() - t0
+    if tune:
+        t0 = time.perf_counter()
+        tune = g.autotune()
+        tune["wall_s"] = time.perf_counter() - t0
+    else:
+        tune = None
     rng = np.random.default_rng(3)
     src = rng.integers(0, n, 256).astype(np.int32)
     blo, bhi = random_windows(rng, 256, span)
@@ -218,21 +221,24 @@ def batched_section(tga, g, n, span):
     bfs_batch_ms = g.timing()["total_ms"]
     _check(L.tga_pagerank_batch(g.handle, 32, 20, d, a, plo.ctypes.data, phi.ctypes.data, None))
     pr_batch_ms = g.timing()["total_ms"]
+    # Plain calls: every query, or the first plain_bfs / plain_pr of them scaled to all (large graphs).
     bfs_plain_ms = pr_plain_ms = 0.0
-    for i in range(256):
+    for i in range(plain_bfs):
         _check(L.tga_bfs(g.handle, int(src[i]), int(blo[i]), int(bhi[i]), None, None))
         bfs_plain_ms += g.timing()["total_ms"]
-    for i in range(32):
+    for i in range(plain_pr):
         _check(L.tga_pagerank(g.handle, 20, d, a, int(plo[i]), int(phi[i]), None))
         pr_plain_ms += g.timing()["total_ms"]
+    bfs_plain_ms *= 256 / plain_bfs
+    pr_plain_ms *= 32 / plain_pr
     qs = 256 + 32
-    return {"workload": "256 BFS (random sources, windows 5-50% of span) + 32 windowed PageRank x20 on the "
-                        "2M/40M graph",
+    return {"workload": f"256 BFS (random sources, windows 5-50% of span) + 32 windowed PageRank x20 on the "
+                        f"{n // 1_000_000}M-vertex graph",
             "queries_per_s": qs / ((bfs_batch_ms + pr_batch_ms) / 1e3),
             "plain_queries_per_s": qs / ((bfs_plain_ms + pr_plain_ms) / 1e3),
             "bfs_batch_ms": bfs_batch_ms, "bfs_plain_ms": bfs_plain_ms, "pr_batch_ms": pr_batch_ms,
             "pr_plain_ms": pr_plain_ms, "timing": "device time (CUDA events), results left on the device",
-            "autotune": tune}
+            "plain_sample": {"bfs": plain_bfs, "pagerank": plain_pr}, "autotune": tune}
 
 
 def served_section(tga, graphs, spans, load, count):
@@ -338,6 +344,39 @@ def served_section(tga, graphs, spans, load, count):
                                              for k, name in kinds.items()}}}
 
 
+def run_batched_scale(args):
+    """Batched form alone on a named configuration (the 20M/500M one by default): generated here,
+    loaded, one batched section with plain calls timed on a sample.  Prints one JSON line."""
+    import compresstemporalgraph_b200 as tga
+
+    name = args.batched_graph
+    p = tga.CONFIGS[name]
+    ddir = Path(tempfile.gettempdir()) / f"tga_bench_{name}"
+    t0 = time.perf_counter()
+    if not (ddir / f"{name}.graph").exists():
+        summary = tga.generate(p, ddir, name)
+    else:
+        summary = None
+    gen_s = time.perf_counter() - t0
+    n = int(p.n)
+    t0 = time.perf_counter()
+    g = tga.Graph.open_dir(ddir, name, tga.DatasetConfig(name=name, max_label=n - 1, max_vertex=n))
+    load_s = time.perf_counter() - t0
+    import ctypes as C
+
+    sec = batched_section(tga, g, n, int(p.ts_span), tune=False, plain_bfs=16, plain_pr=4)
+    info = tga._Info()
+    tga._check(tga.lib().tga_get_info(g.handle, C.byref(info)))  # device bytes now include the scratch
+    info = {k: getattr(info, k) for k, _ in tga._Info._fields_}
+    g.close()
+    line = {"metric": "batched queries/s (256 windowed BFS + 32 windowed PageRank x20)", "value": sec["queries_per_s"],
+            "unit": "queries/s", "n_gpus": 1, "higher_is_better": True, "data": "synthetic",
+            "config": {"workload": name, "vertices": n, "temporal_edges": int(p.m)}, "batched": sec,
+            "generate_s": gen_s, "load_s": load_s, "summary": summary, "info": info}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_reference(args):
     rank, local, world = dist_env()
     if rank != 0:
@@ -382,6 +421,8 @@ def main():
     ap.add_argument("--served-load", type=float, default=0.8,
                     help="offered load of the served open loop, as a fraction of the plain path's capacity")
     ap.add_argument("--served-count", type=int, default=300)
+    ap.add_argument("--batched-graph", default=None,
+                    help="run only the batched section on this generated configuration (e.g. batched: 20M/500M)")
     ap.add_argument("--only", choices=["RA", "BFS", "CC", "PR", "HITS", "DC", "GC"],
                     help="run one workload per step (for profiling; the line is not the benchmark)")
     args = ap.parse_args()
@@ -389,6 +430,8 @@ def main():
     ONLY = args.only
     if args.impl == "reference":
         return run_reference(args)
+    if args.batched_graph:
+        return run_batched_scale(args)
 
     import torch
 
