@@ -328,7 +328,7 @@ __global__ void k_scale(const float* v, const double* sumsq, float* out, int32_t
 // ---------------------------------------------------------------------------------------------
 // Degree centrality (Java semantics).  Short lists: one thread per list.
 
-__global__ void TGA_DECODE_BOUNDS k_degree(GraphView g, Work w, int64_t s, int64_t e, int32_t* deg, int64_t* avg,
+__global__ void TGA_TRAVERSE_BOUNDS k_degree(GraphView g, Work w, int64_t s, int64_t e, int32_t* deg, int64_t* avg,
                                            unsigned long long* edges) {
   const bool all = (s == 0 && e == 0);
   const int lim = min(g.max_label + 1, g.max_vertex);
@@ -363,7 +363,7 @@ __global__ void TGA_DECODE_BOUNDS k_degree(GraphView g, Work w, int64_t s, int64
 // every step, so it cannot be split), with a 32-bit division whenever the difference fits.
 constexpr int64_t kDcSkip = INT64_MIN;
 
-__global__ void TGA_DECODE_BOUNDS k_degree_slices(GraphView g, const SliceState* slices, const int64_t* ebase,
+__global__ void TGA_TRAVERSE_BOUNDS k_degree_slices(GraphView g, const SliceState* slices, const int64_t* ebase,
                                                   int32_t nslices, int64_t s, int64_t e, int64_t* buf,
                                                   unsigned long long* edges) {
   const bool all = (s == 0 && e == 0);

@@ -920,7 +920,7 @@ __device__ void cc_label_reset(const MultiArgs& a, const CcArgs& c, const CcSlot
   }
 }
 
-__global__ void TGA_DECODE_BOUNDS k_cc_batches(GraphView g, MultiArgs a, CcArgs c) {
+__global__ void TGA_TRAVERSE_BOUNDS k_cc_batches(GraphView g, MultiArgs a, CcArgs c) {
   __shared__ int64_t slo[kMaxSources], shi[kMaxSources];
   __shared__ int32_t scol[kMaxSources];
   __shared__ uint32_t reaches[kMaxSources][kMaxSources / 32];

@@ -18,10 +18,13 @@ constexpr int kNoRunFilter = -2;
 
 // Launches a kernel of kBlock threads on the handle's stream and counts it in the call's timing.
 #define KL(kernel, grid) ++h.timing.launches, kernel<<<(grid), kBlock, 0, h.stream>>>
-// Decode kernels of traversals and colouring: 2 blocks of 256 threads per SM (up to 128
-// registers).  Their levels are short and latency-bound, and the extra spills of a tighter cap
-// cost more than the added warps gain.
+// Decode kernels of colouring, batched BFS, point queries, batched PageRank and the run
+// pre-passes: 2 blocks of 256 threads per SM (up to 128 registers).
 #define TGA_DECODE_BOUNDS __launch_bounds__(kBlock, 2)
+// BFS, CC (single and batched seeds) and degree centrality: 3 blocks per SM (up to 85 registers);
+// measured against 2 on the 2M/40M graph: BFS 16.4 / 17.2 ms, CC 67.0 / 68.1 ms, DC 17.3 / 17.7 ms.
+// Colouring (22.9 / 22.1 ms) and the 256-source batched BFS (17.0 / 15.5 ms) were slower at 3.
+#define TGA_TRAVERSE_BOUNDS __launch_bounds__(kBlock, 3)
 // Full sweeps over the schedule (neighbour access, PageRank, HITS, window counts, raw decode):
 // 4 blocks per SM (up to 64 registers, a few spills), measured faster than 2 on these kernels
 // because more resident warps hide the decoder's dependent loads.

@@ -195,7 +195,7 @@ __device__ __forceinline__ unsigned long long hop_level(const GraphView& g, Trav
   return drive_queue<true>(g, w, q, qn, begin, edge, [](int) {});
 }
 
-__global__ void TGA_DECODE_BOUNDS k_bfs(GraphView g, TravArgs a) {
+__global__ void TGA_TRAVERSE_BOUNDS k_bfs(GraphView g, TravArgs a) {
   int L = 0;
   unsigned long long mine = 0;
   const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
@@ -236,7 +236,7 @@ __global__ void TGA_DECODE_BOUNDS k_bfs(GraphView g, TravArgs a) {
 
 // Seeds ascend from cc_begin below cc_end: the smallest unreached vertex with outdegree > 9
 // starts a phase-1 traversal; every vertex it reaches gets its component number (last seed wins).
-__global__ void TGA_DECODE_BOUNDS k_cc(GraphView g, TravArgs a) {
+__global__ void TGA_TRAVERSE_BOUNDS k_cc(GraphView g, TravArgs a) {
   const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
   int L = 0, comp = 0, small_run = 0;
