@@ -421,6 +421,8 @@ def main():
     ap.add_argument("--served-load", type=float, default=0.8,
                     help="offered load of the served open loop, as a fraction of the plain path's capacity")
     ap.add_argument("--served-count", type=int, default=300)
+    ap.add_argument("--served-graphs", default="small,served1m",
+                    help="resident graphs of the served section besides the benchmark graph (configuration names)")
     ap.add_argument("--batched-graph", default=None,
                     help="run only the batched section on this generated configuration (e.g. batched: 20M/500M)")
     ap.add_argument("--only", choices=["RA", "BFS", "CC", "PR", "HITS", "DC", "GC"],
@@ -533,13 +535,14 @@ def main():
         try:
             line["batched"] = batched_section(tga, g, n, int(tga.CONFIGS[CONFIG_NAME].ts_span))
             extra = []
-            for name in ("small", "served1m"):
+            names = [nm for nm in args.served_graphs.split(",") if nm and nm != CONFIG_NAME]
+            for name in names:
                 dd = Path(tempfile.gettempdir()) / f"tga_bench_{name}"
                 if not (dd / f"{name}.graph").exists():
                     tga.generate(tga.CONFIGS[name], dd, name)
                 nn = tga.CONFIGS[name].n
                 extra.append(tga.Graph.open_dir(dd, name, tga.DatasetConfig(name=name, max_label=nn - 1, max_vertex=nn)))
-            spans = [int(tga.CONFIGS[nm].ts_span) for nm in ("small", "served1m", CONFIG_NAME)]
+            spans = [int(tga.CONFIGS[nm].ts_span) for nm in names + [CONFIG_NAME]]
             line["served"] = served_section(tga, extra + [g], spans, args.served_load, args.served_count)
             for gg in extra:
                 gg.close()

@@ -533,6 +533,10 @@ CONFIGS = {
     "served1m": GenParams(n=1_000_000, m=20_000_000, deg_exponent=2.0, max_degree=50_000, repeat_frac=0.30,
                           local_frac=0.70, local_radius=64, pref_frac=0.5, copy_frac=0.20, ts_kind=1,
                           ts_span=100_000_000, seed=4),
+    # Served-form resident graph of 10M vertices / 200M temporal edges.
+    "served10m": GenParams(n=10_000_000, m=200_000_000, deg_exponent=2.0, max_degree=200_000, repeat_frac=0.30,
+                           local_frac=0.70, local_radius=64, pref_frac=0.5, copy_frac=0.20, ts_kind=1,
+                           ts_span=100_000_000, seed=4),
     "skew": GenParams(n=100_000_000, m=2_000_000_000, deg_exponent=1.6, max_degree=5_000_000, repeat_frac=0.30,
                       local_frac=0.70, local_radius=64, pref_frac=0.5, copy_frac=0.20, ts_kind=2,
                       ts_span=100_000_000, seed=5),

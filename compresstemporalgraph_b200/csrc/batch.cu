@@ -617,8 +617,10 @@ static int multi_run(GraphHandle& h, int32_t nsrc, unsigned long long* edges, Mu
 }
 
 // One batch of at most kMaxSources sources: arrivals to arrival_out (nsrc x max_vertex, host).
+// rows (optional): per source a destination of max_vertex entries (NULL: not copied) instead of
+// the contiguous arrival_out.
 static int bfs_multi_batch(GraphHandle& h, int32_t nsrc, const int32_t* src, const int64_t* t_lo, const int64_t* t_hi,
-                           int32_t* arrival_out) {
+                           int32_t* arrival_out, int32_t* const* rows = nullptr) {
   const size_t nv = (size_t)h.view.max_vertex;
   const size_t state = (size_t)nsrc * nv * 4;
   TGA_TRY(multi_buffers(h, nsrc));
@@ -637,6 +639,9 @@ static int bfs_multi_batch(GraphHandle& h, int32_t nsrc, const int32_t* src, con
                                                                                          out);
   ++h.timing.launches;
   if (arrival_out) TGA_CUDA_TRY(cudaMemcpyAsync(arrival_out, out, state, cudaMemcpyDeviceToHost, h.stream));
+  if (rows)
+    for (int32_t i = 0; i < nsrc; ++i)
+      if (rows[i]) TGA_CUDA_TRY(cudaMemcpyAsync(rows[i], out + (size_t)i * nv, nv * 4, cudaMemcpyDeviceToHost, h.stream));
   h.timing.iterations = levels;
   return finish(h, edges);
 }
@@ -1372,8 +1377,10 @@ __global__ void k_pr_multi_final(const float* buf, const double* sums, uint32_t 
 }
 
 // nq (<= kMaxRankQueries) queries, query q running iters[q] (>= 1) iterations.
+// rows (optional): per query a destination of max_vertex entries (NULL: not copied) instead of
+// the contiguous rank_out.
 static int pagerank_multi_batch(GraphHandle& h, int32_t nq, const int32_t* iters, float damping, float alpha,
-                                const int64_t* t_lo, const int64_t* t_hi, float* rank_out) {
+                                const int64_t* t_lo, const int64_t* t_hi, float* rank_out, float* const* rows = nullptr) {
   const size_t nv = (size_t)h.view.max_vertex;
   int32_t S = 1;
   while (S < nq) S <<= 1;
@@ -1467,11 +1474,41 @@ static int pagerank_multi_batch(GraphHandle& h, int32_t nq, const int32_t* iters
     return TGA_OK;
   }));
   if (rank_out) TGA_CUDA_TRY(cudaMemcpyAsync(rank_out, out, (size_t)nq * nv * 4, cudaMemcpyDeviceToHost, h.stream));
+  if (rows)
+    for (int32_t q = 0; q < nq; ++q)
+      if (rows[q]) TGA_CUDA_TRY(cudaMemcpyAsync(rows[q], out + (size_t)q * nv, nv * 4, cudaMemcpyDeviceToHost, h.stream));
   h.timing.iterations = maxit;
   const int rc = finish(h, edges);
   h.timing.compressed_bytes = (uint64_t)(maxit + (windowed ? 1 : 0)) *
                               (h.info.graph_bytes + h.info.timestamp_bytes + h.info.index_bytes);
   return rc;
+}
+
+int bfs_batch_rows(tga_graph* g, int32_t nsrc, const int32_t* src, const int64_t* t_lo, const int64_t* t_hi,
+                   int32_t* const* rows) {
+  if (!g || nsrc < 0 || (nsrc && (!src || !t_lo || !t_hi || !rows))) return fail(TGA_E_ARG, "bad argument");
+  GraphHandle& h = *g;
+  for (int32_t i = 0; i < nsrc; ++i) {
+    if (src[i] < 0 || src[i] >= h.view.max_vertex) return fail(TGA_E_ARG, "source out of range");
+    if (t_lo[i] >= t_hi[i]) return fail(TGA_E_ARG, "empty time window");
+  }
+  for (int32_t b = 0; b < nsrc; b += kMaxSources)
+    TGA_TRY(bfs_multi_batch(h, std::min(kMaxSources, nsrc - b), src + b, t_lo + b, t_hi + b, nullptr, rows + b));
+  return TGA_OK;
+}
+
+int pagerank_batch_rows(tga_graph* g, int32_t nq, const int32_t* iters, float damping, float alpha,
+                        const int64_t* t_lo, const int64_t* t_hi, float* const* rows) {
+  if (!g || nq < 0 || (nq && (!iters || !t_lo || !t_hi || !rows))) return fail(TGA_E_ARG, "bad argument");
+  GraphHandle& h = *g;
+  for (int32_t i = 0; i < nq; ++i)
+    if (t_lo[i] >= t_hi[i]) return fail(TGA_E_ARG, "empty time window");
+  std::vector<int32_t> it((size_t)nq);
+  for (int32_t i = 0; i < nq; ++i) it[(size_t)i] = iters[i] > 0 ? iters[i] : std::max(h.cfg.pr_iters, 1);
+  for (int32_t b = 0; b < nq; b += kMaxRankQueries)
+    TGA_TRY(pagerank_multi_batch(h, std::min(kMaxRankQueries, nq - b), it.data() + b, damping, alpha, t_lo + b, t_hi + b,
+                                 nullptr, rows + b));
+  return TGA_OK;
 }
 
 int cc_seed_batches(GraphHandle& h, int64_t t_lo, int64_t t_hi, int32_t flags, int32_t* label_out,

@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "../../include/tga.h"
+#include "serve_ops.hpp"
 
 namespace tga {
 int fail(int code, const std::string& msg);
@@ -123,7 +124,6 @@ void tga_server::publish(const std::vector<const Pending*>& done, const std::vec
 }
 
 void tga_server::run_round(GraphSlot* slot, std::vector<Pending>& round) {
-  const size_t nv = (size_t)slot->nv;
   // BFS: one batched traversal; results published as soon as it is done.
   {
     std::vector<const Pending*> done;
@@ -137,10 +137,9 @@ void tga_server::run_round(GraphSlot* slot, std::vector<Pending>& round) {
         hi.push_back(p.q.t_hi);
       }
     if (!done.empty()) {
-      std::vector<int32_t> out(done.size() * nv);
-      const int rc = tga_bfs_batch(slot->g, (int32_t)done.size(), src.data(), lo.data(), hi.data(), out.data());
-      for (size_t k = 0; k < done.size(); ++k)
-        if (rc == TGA_OK && done[k]->q.out) std::memcpy(done[k]->q.out, out.data() + k * nv, nv * 4);
+      std::vector<int32_t*> rows(done.size());
+      for (size_t k = 0; k < done.size(); ++k) rows[k] = static_cast<int32_t*>(done[k]->q.out);
+      const int rc = tga::bfs_batch_rows(slot->g, (int32_t)done.size(), src.data(), lo.data(), hi.data(), rows.data());
       publish(done, std::vector<int>(done.size(), rc));
     }
   }
@@ -157,11 +156,10 @@ void tga_server::run_round(GraphSlot* slot, std::vector<Pending>& round) {
         hi.push_back(p.q.t_hi);
       }
     if (!done.empty()) {
-      std::vector<float> out(done.size() * nv);
-      const int rc = tga_pagerank_batch_iters(slot->g, (int32_t)done.size(), iters.data(), 0.85f, 0.1f, lo.data(),
-                                              hi.data(), out.data());
-      for (size_t k = 0; k < done.size(); ++k)
-        if (rc == TGA_OK && done[k]->q.out) std::memcpy(done[k]->q.out, out.data() + k * nv, nv * 4);
+      std::vector<float*> rows(done.size());
+      for (size_t k = 0; k < done.size(); ++k) rows[k] = static_cast<float*>(done[k]->q.out);
+      const int rc = tga::pagerank_batch_rows(slot->g, (int32_t)done.size(), iters.data(), 0.85f, 0.1f, lo.data(),
+                                              hi.data(), rows.data());
       publish(done, std::vector<int>(done.size(), rc));
     }
   }
