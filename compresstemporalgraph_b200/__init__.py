@@ -139,6 +139,7 @@ def _load() -> C.CDLL:
         "tga_encode_raw": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int64, C.POINTER(_GenSummary)]),
         "tga_build_index": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int64]),
         "tga_autotune": (C.c_int, [P, P]),
+        "tga_barrier_selftest": (C.c_int, [C.c_double, P]),
         "tga_decode_table": (C.c_int, [C.c_int32, P]),
         "tga_encode_codes": (C.c_int, [C.c_int32, C.c_int32, P, C.c_int64, P, C.c_int64, C.POINTER(C.c_int64)]),
         "tga_ef_encode": (C.c_int, [P, C.c_int64, C.c_int32, P, C.c_int64, P, C.c_int64, C.POINTER(C.c_int64),
@@ -564,6 +565,14 @@ def encode_raw(raw_path: str | os.PathLike, directory: str | os.PathLike, basena
 def build_index(directory: str | os.PathLike, basename: str, max_label: int) -> None:
     """Writes the four GPU index files of a directory that has <base>.offsets (tga_build_index)."""
     _check(_lib.tga_build_index(str(directory).encode(), basename.encode(), max_label))
+
+
+def barrier_selftest(limit_ms: float = 200.0) -> bool:
+    """Makes a grid-barrier wait run out on the device (tga_barrier_selftest); True if it ended with
+    the timeout status."""
+    st = C.c_int32()
+    _check(_lib.tga_barrier_selftest(limit_ms, C.byref(st)))
+    return st.value == 1
 
 
 def decode_table(kind: int) -> np.ndarray:

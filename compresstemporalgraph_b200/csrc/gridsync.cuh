@@ -34,8 +34,9 @@ __device__ __forceinline__ uint64_t global_ns() {
 }
 
 // Barrier over all blocks of the cooperative launch; false if the launch has failed (this block
-// must return at once).
-static __device__ bool grid_sync(TravCtl* ctl, const GraphView& g) {
+// must return at once).  A wait longer than limit_ns sets ctl->status and the kErrTimeout bit of
+// *err, and every block leaves at its next barrier.
+static __device__ bool grid_sync_limit(TravCtl* ctl, uint32_t* err, uint64_t limit_ns) {
   __shared__ int failed;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -55,9 +56,9 @@ static __device__ bool grid_sync(TravCtl* ctl, const GraphView& g) {
           failed = 1;
           break;
         }
-        if ((spin & 255u) == 255u && global_ns() - t0 > kBarrierNs) {
+        if ((spin & 255u) == 255u && global_ns() - t0 > limit_ns) {
           atomicExch(&ctl->status, 1);
-          set_err(g, kErrTimeout);
+          atomicOr(err, kErrTimeout);
           failed = 1;
           break;
         }
@@ -69,6 +70,10 @@ static __device__ bool grid_sync(TravCtl* ctl, const GraphView& g) {
   }
   __syncthreads();
   return !failed;
+}
+
+static __device__ __forceinline__ bool grid_sync(TravCtl* ctl, const GraphView& g) {
+  return grid_sync_limit(ctl, g.err, kBarrierNs);
 }
 
 // Reserves n slots per lane with one atomic per warp (all 32 lanes must call it together); returns

@@ -195,6 +195,13 @@ __device__ __forceinline__ unsigned long long hop_level(const GraphView& g, Trav
   return drive_queue<true>(g, w, q, qn, begin, edge, [](int) {});
 }
 
+// Self-test of the bounded grid barrier: block 1 never arrives, so block 0's wait runs out after
+// limit_ns; the launch ends with ctl->status set instead of waiting for ever.
+__global__ void k_barrier_selftest(TravCtl* ctl, uint32_t* err, uint64_t limit_ns) {
+  if (blockIdx.x != 0) return;  // the block that never arrives
+  grid_sync_limit(ctl, err, limit_ns);
+}
+
 __global__ void TGA_TRAVERSE_BOUNDS k_bfs(GraphView g, TravArgs a) {
   int L = 0;
   unsigned long long mine = 0;
@@ -379,6 +386,28 @@ static int trav_launch(GraphHandle& h, K kernel, TravArgs& a, TravCtl& out) {
 using namespace tga;
 
 extern "C" {
+
+int tga_barrier_selftest(double limit_ms, int32_t* status_out) {
+  if (limit_ms <= 0 || limit_ms > 10000) return fail(TGA_E_ARG, "limit must be in (0, 10 s]");
+  TravCtl* ctl = nullptr;
+  uint32_t* err = nullptr;
+  TGA_CUDA_TRY(cudaMalloc((void**)&ctl, sizeof(TravCtl) + 16));
+  err = reinterpret_cast<uint32_t*>(reinterpret_cast<char*>(ctl) + sizeof(TravCtl));
+  int rc = TGA_OK;
+  TravCtl host{};
+  uint32_t herr = 0;
+  uint64_t limit = (uint64_t)(limit_ms * 1e6);
+  void* args[] = {&ctl, &err, &limit};
+  if (cudaMemset(ctl, 0, sizeof(TravCtl) + 16) != cudaSuccess ||
+      cudaLaunchCooperativeKernel((const void*)k_barrier_selftest, dim3(2), dim3(32), args, 0, nullptr) != cudaSuccess ||
+      cudaDeviceSynchronize() != cudaSuccess || cudaMemcpy(&host, ctl, sizeof host, cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(&herr, err, 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+    rc = fail(TGA_E_CUDA, std::string("barrier self-test: ") + cudaGetErrorString(cudaGetLastError()));
+  cudaFree(ctl);
+  if (rc) return rc;
+  if (status_out) *status_out = host.status && (herr & kErrTimeout) ? 1 : 0;
+  return TGA_OK;
+}
 
 int tga_bfs(tga_graph* gp, int32_t src, int64_t t_lo, int64_t t_hi, int32_t* arrival_out, int32_t* hops_out) {
   if (!gp) return fail(TGA_E_ARG, "null graph");

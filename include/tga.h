@@ -140,6 +140,12 @@ int tga_is_neighbor(tga_graph* g, int32_t nq, const int32_t* node, const int32_t
 /* Whole graph as CSR: offsets[n+1], dst[m], ts[m] (cap = capacity of dst/ts). */
 int tga_decode_all(tga_graph* g, int64_t* offsets, int32_t* dst, int64_t* ts, int64_t cap);
 
+/* Failure-detection self-test (no reference counterpart): launches a two-block cooperative grid
+ * whose second block never reaches the grid barrier, so the first block's wait runs out after
+ * limit_ms (<= 10 s; the traversals use 10 s).  *status_out = 1 when the wait ended with the
+ * timeout status, as every traversal's barriers do; the context stays usable. */
+int tga_barrier_selftest(double limit_ms, int32_t* status_out);
+
 /* Temporal BFS (bfs.cu:1218-1692, host loop 1999-2038).  Edge (x->y,t) with t in [t_lo, t_hi)
  * relaxes y when arrival(x) <= t; only the first in-window occurrence of consecutive equal
  * successors counts.  arrival_out[v] = earliest arrival (INT32_MAX unreached, source = max(t_lo,0));

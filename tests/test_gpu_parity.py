@@ -269,6 +269,19 @@ def test_autotune_keeps_results(pairs):
         p.g.set_work_params(default["slice_edges"], default["item_edges"])
 
 
+def test_bounded_barrier_wait_reports_timeout(pairs):
+    """A grid-barrier wait that nothing ends (a block that never arrives) runs out after its limit
+    and reports the timeout status; the context stays usable for the next traversal."""
+    import time as _time
+
+    t = _time.perf_counter()
+    assert tga.barrier_selftest(200.0)
+    assert _time.perf_counter() - t >= 0.2
+    p = pairs["chains"]
+    arr, _ = p.g.bfs(0)
+    assert np.array_equal(arr, p.o.bfs(p.ml, p.mv, p.act, 0)[0])
+
+
 def test_multi_source_state_survives_other_calls(pairs):
     """The batched traversal keeps its per-source arrays between calls and resets only the
     vertices the previous traversal touched; single-source traversals, batched CC and batched
