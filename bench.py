@@ -42,6 +42,21 @@ def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
 
 
+def replica_totals(ms: float, edges: int, world: int, device: str = "cuda") -> tuple[float, int]:
+    """Whole-job figures of N independent replicas: the slowest rank's time (max over ranks) and the
+    edges all ranks decoded (sum).  Every rank calls it at the same point (two collectives)."""
+    if world == 1:
+        return ms, edges
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e = torch.tensor([edges], dtype=torch.int64, device=device)
+    dist.all_reduce(e, op=dist.ReduceOp.SUM)
+    return float(t.item()), int(e.item())
+
+
 def dataset_dir() -> Path:
     return Path(os.environ.get("TGA_BENCH_DATA", Path(tempfile.gettempdir()) / "tga_bench_all7"))
 
@@ -479,21 +494,16 @@ def main():
         torch.cuda.synchronize()
         if barrier:
             barrier()
-        ms = ev0.elapsed_time(ev1)
-        if world > 1:
-            t = torch.tensor([ms], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms, edges, launches, per_all
+        ms, total = replica_totals(ev0.elapsed_time(ev1), edges, world)
+        return ms, edges, total, launches, per_all
 
     with Clocks(local) as clk:
-        ms, edges, launches, per_all = timed(outputs=False)
+        ms, edges, total_edges, launches, per_all = timed(outputs=False)
     clocks = clk.summary()
-    e2e_ms, e2e_edges, _, _ = timed(outputs=True)
+    e2e_ms, _, e2e_total, _, _ = timed(outputs=True)
 
-    total_edges = edges * world
     value = total_edges / (ms / 1e3) / 1e9
-    e2e_value = e2e_edges * world / (e2e_ms / 1e3) / 1e9
+    e2e_value = e2e_total / (e2e_ms / 1e3) / 1e9
 
     if ONLY:
         print(json.dumps({"only": ONLY, "ms": ms, "edges": edges, "workloads": {k: v for k, v in per_all[0].items()}}))
