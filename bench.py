@@ -9,8 +9,12 @@ host copies inside the timed region); roofline = the PageRank iteration kernel's
 per launch / its average launch time against the measured HBM copy bandwidth.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+  python bench.py --batched-graph batched      # batched form alone on the 20M/500M graph
 
-Multi-GPU runs are independent replicas (the north star is one GPU; nothing is exchanged).
+The line also carries the batched form (256 windowed BFS + 32 windowed PageRanks against one query
+per call) and the served form (open-loop queries through the server against plain calls).
+Multi-GPU runs are independent replicas (every graph fits one GPU; nothing is exchanged): time is
+the slowest rank's, edges are summed over ranks.
 """
 from __future__ import annotations
 
