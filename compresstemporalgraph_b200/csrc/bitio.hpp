@@ -15,6 +15,7 @@
 // zetaInA.txt) are regenerated from these definitions by table16() and match entry
 // for entry.
 #pragma once
+#include <cstddef>
 #include <cstdint>
 #include <cstring>
 #include <stdexcept>
@@ -76,6 +77,23 @@ class BitWriter {
     return u + write_minimal_binary(v - left, (left << k) - left);
   }
   int write_long(uint64_t x, int len) { write_bits(x, len); return len; }
+  // Appends all bits of o (whose bits past o.nbits are zero, as every BitWriter keeps them).
+  void append(const BitWriter& o) {
+    const uint64_t ob = (o.nbits + 7) / 8;
+    const int used = (int)(nbits & 7);
+    const size_t old = bytes.size();
+    if (used == 0) {
+      bytes.insert(bytes.end(), o.bytes.begin(), o.bytes.begin() + (ptrdiff_t)ob);
+    } else {
+      bytes.resize(old + ob, 0);
+      for (uint64_t i = 0; i < ob; ++i) {
+        bytes[old - 1 + i] |= (uint8_t)(o.bytes[i] >> used);
+        bytes[old + i] |= (uint8_t)(o.bytes[i] << (8 - used));
+      }
+    }
+    nbits += o.nbits;
+    bytes.resize((nbits + 7) / 8);
+  }
 };
 
 // Counts bits without storing them (the "NullOutputStream" bit counter of diffComp).

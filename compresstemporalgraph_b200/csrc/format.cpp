@@ -4,12 +4,14 @@
 #include <sys/stat.h>
 
 #include <algorithm>
-#include <map>
 #include <cerrno>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <exception>
+#include <map>
 #include <stdexcept>
+#include <thread>
 
 namespace tga {
 
@@ -82,76 +84,79 @@ static int split_intervals(const std::vector<int32_t>& v, int min_interval, std:
   return (int)left.size();
 }
 
+// One record's body (reference, copy blocks, multiples, intervals, residuals) relative to the list
+// ref_list at distance ref, written to obs (a BitWriter, or a BitCounter to cost it).  st: the
+// statistics to add to when the record is written for real, else nullptr.
 template <class Out>
-void GraphEncoder::diff_comp(Out& obs, int cur, int ref, const int32_t* ref_list, int ref_len,
-                             const int32_t* cur_list, int cur_len, bool for_real) {
-  const int mult_count = split_multiples(cur_list, cur_len, mult_left_, mult_len_, singles_);
-  const int32_t* cl = singles_.data();
-  const int cn = (int)singles_.size();
+static void diff_comp(Out& obs, const EncoderParams& params, DiffScratch& sc, EncoderStats* st, int cur, int ref,
+                      const int32_t* ref_list, int ref_len, const int32_t* cur_list, int cur_len) {
+  const int mult_count = split_multiples(cur_list, cur_len, sc.mult_left, sc.mult_len, sc.singles);
+  const int32_t* cl = sc.singles.data();
+  const int cn = (int)sc.singles.size();
   if (ref == 0) ref_len = 0;
-  extras_.clear();
-  blocks_.clear();
+  sc.extras.clear();
+  sc.blocks.clear();
   // Alternate copy/skip blocks over the reference list (BVMultiGraph.java:1668-1720).
   int j = 0, k = 0, blen = 0;
   bool copying = true;
   while (j < cn && k < ref_len) {
     if (copying) {
-      if (cl[j] > ref_list[k]) { blocks_.push_back(blen); copying = false; blen = 0; }
-      else if (cl[j] < ref_list[k]) extras_.push_back(cl[j++]);
-      else { ++j; ++k; ++blen; if (for_real) ++stats.copied_arcs; }
+      if (cl[j] > ref_list[k]) { sc.blocks.push_back(blen); copying = false; blen = 0; }
+      else if (cl[j] < ref_list[k]) sc.extras.push_back(cl[j++]);
+      else { ++j; ++k; ++blen; if (st) ++st->copied_arcs; }
     } else {
-      if (cl[j] < ref_list[k]) extras_.push_back(cl[j++]);
+      if (cl[j] < ref_list[k]) sc.extras.push_back(cl[j++]);
       else if (cl[j] > ref_list[k]) { ++k; ++blen; }
-      else { blocks_.push_back(blen); copying = true; blen = 0; }
+      else { sc.blocks.push_back(blen); copying = true; blen = 0; }
     }
   }
-  if (copying && k < ref_len) blocks_.push_back(blen);
-  while (j < cn) extras_.push_back(cl[j++]);
+  if (copying && k < ref_len) sc.blocks.push_back(blen);
+  while (j < cn) sc.extras.push_back(cl[j++]);
 
   int64_t t;
   if (params.window_size > 0) {
     t = obs.write_unary((uint64_t)ref);
-    if (for_real) stats.bits_references += t;
+    if (st) st->bits_references += t;
   }
   if (ref != 0) {
-    const int bc = (int)blocks_.size();
+    const int bc = (int)sc.blocks.size();
     t = obs.write_gamma((uint64_t)bc);
-    for (int i = 0; i < bc; ++i) t += obs.write_gamma((uint64_t)(i == 0 ? blocks_[0] : blocks_[i] - 1));
-    if (for_real) stats.bits_blocks += t;
+    for (int i = 0; i < bc; ++i) t += obs.write_gamma((uint64_t)(i == 0 ? sc.blocks[0] : sc.blocks[i] - 1));
+    if (st) st->bits_blocks += t;
   }
-  if ((int)extras_.size() + mult_count > 0) {
+  if ((int)sc.extras.size() + mult_count > 0) {
     t = obs.write_gamma((uint64_t)mult_count);
     int64_t prev = 0;
     for (int i = 0; i < mult_count; ++i) {
-      if (i == 0) t += obs.write_gamma(int2nat((int64_t)mult_left_[0] - cur));
-      else t += obs.write_gamma((uint64_t)(mult_left_[i] - prev - 1));
-      prev = mult_left_[i];
-      t += obs.write_gamma((uint64_t)(mult_len_[i] - params.min_multiple));
-      if (for_real) stats.multiples_arcs += mult_len_[i];
+      if (i == 0) t += obs.write_gamma(int2nat((int64_t)sc.mult_left[0] - cur));
+      else t += obs.write_gamma((uint64_t)(sc.mult_left[i] - prev - 1));
+      prev = sc.mult_left[i];
+      t += obs.write_gamma((uint64_t)(sc.mult_len[i] - params.min_multiple));
+      if (st) st->multiples_arcs += sc.mult_len[i];
     }
-    if (for_real) stats.bits_multiples += t;
+    if (st) st->bits_multiples += t;
 
-    const int ic = split_intervals(extras_, params.min_interval, left_, len_, residuals_);
+    const int ic = split_intervals(sc.extras, params.min_interval, sc.left, sc.len, sc.residuals);
     t = obs.write_gamma((uint64_t)ic);
     for (int i = 0; i < ic; ++i) {
-      if (i == 0) t += obs.write_gamma(int2nat((int64_t)left_[0] - cur));
-      else t += obs.write_gamma((uint64_t)(left_[i] - prev - 1));
-      prev = (int64_t)left_[i] + len_[i];
-      t += obs.write_gamma((uint64_t)(len_[i] - params.min_interval));
-      if (for_real) stats.intervalised_arcs += len_[i];
+      if (i == 0) t += obs.write_gamma(int2nat((int64_t)sc.left[0] - cur));
+      else t += obs.write_gamma((uint64_t)(sc.left[i] - prev - 1));
+      prev = (int64_t)sc.left[i] + sc.len[i];
+      t += obs.write_gamma((uint64_t)(sc.len[i] - params.min_interval));
+      if (st) st->intervalised_arcs += sc.len[i];
     }
-    if (for_real) stats.bits_intervals += t;
+    if (st) st->bits_intervals += t;
 
-    const int rc = (int)residuals_.size();
+    const int rc = (int)sc.residuals.size();
     if (rc) {
-      t = obs.write_zeta(int2nat((int64_t)residuals_[0] - cur), params.zeta_k);
-      prev = residuals_[0];
+      t = obs.write_zeta(int2nat((int64_t)sc.residuals[0] - cur), params.zeta_k);
+      prev = sc.residuals[0];
       for (int i = 1; i < rc; ++i) {
-        if (residuals_[i] == prev) throw std::runtime_error("repeated residual successor");
-        t += obs.write_zeta((uint64_t)(residuals_[i] - prev - 1), params.zeta_k);
-        prev = residuals_[i];
+        if (sc.residuals[i] == prev) throw std::runtime_error("repeated residual successor");
+        t += obs.write_zeta((uint64_t)(sc.residuals[i] - prev - 1), params.zeta_k);
+        prev = sc.residuals[i];
       }
-      if (for_real) { stats.bits_residuals += t; stats.residual_arcs += rc; }
+      if (st) { st->bits_residuals += t; st->residual_arcs += rc; }
     }
   }
 }
@@ -177,18 +182,154 @@ void GraphEncoder::add_node(const int32_t* succ, int outd) {
       const int cand = (cur - j + cyc) % cyc;
       if (ref_count_[cand] < params.max_ref_count && list_len_[cand] != 0) {
         BitCounter bc;
-        diff_comp(bc, cur, j, list_[cand].data(), list_len_[cand], list_[ci].data(), outd, false);
+        diff_comp(bc, params, scratch_, nullptr, cur, j, list_[cand].data(), list_len_[cand], list_[ci].data(), outd);
         if ((int64_t)bc.nbits < best) { best = (int64_t)bc.nbits; best_idx = cand; }
       }
     }
     ref_count_[ci] = ref_count_[best_idx] + 1;
     const int ref = (cur - best_idx + cyc) % cyc;
-    diff_comp(graph, cur, ref, list_[best_idx].data(), list_len_[best_idx], list_[ci].data(), outd, true);
+    diff_comp(graph, params, scratch_, &stats, cur, ref, list_[best_idx].data(), list_len_[best_idx], list_[ci].data(),
+              outd);
     stats.arcs += outd;
     stats.tot_ref += ref_count_[ci];
     stats.tot_dist += ref;
     stats.max_chain = std::max<int64_t>(stats.max_chain, ref_count_[ci]);
   }
+}
+
+// Runs fn(t, lo, hi) for t < parts over [0, count) split into contiguous ranges.
+template <class Fn>
+static void parallel_ranges(int count, int parts, Fn fn) {
+  parts = std::max(1, std::min(parts, count));
+  std::vector<std::thread> pool;
+  std::vector<std::exception_ptr> errs((size_t)parts);
+  for (int t = 0; t < parts; ++t) {
+    const int lo = (int)((int64_t)count * t / parts), hi = (int)((int64_t)count * (t + 1) / parts);
+    auto run = [&, t, lo, hi] {
+      try {
+        fn(t, lo, hi);
+      } catch (...) {
+        errs[(size_t)t] = std::current_exception();
+      }
+    };
+    if (t + 1 < parts) pool.emplace_back(run);
+    else run();
+  }
+  for (auto& th : pool) th.join();
+  for (auto& e : errs)
+    if (e) std::rethrow_exception(e);
+}
+
+static void add_stats(EncoderStats& a, const EncoderStats& b) {
+  a.copied_arcs += b.copied_arcs;
+  a.intervalised_arcs += b.intervalised_arcs;
+  a.residual_arcs += b.residual_arcs;
+  a.multiples_arcs += b.multiples_arcs;
+  a.bits_outdegrees += b.bits_outdegrees;
+  a.bits_references += b.bits_references;
+  a.bits_blocks += b.bits_blocks;
+  a.bits_residuals += b.bits_residuals;
+  a.bits_intervals += b.bits_intervals;
+  a.bits_multiples += b.bits_multiples;
+}
+
+void GraphEncoder::add_block(const int32_t* const* succ, const int* outd, int count, int threads) {
+  if (count <= 0) return;
+  const int cyc = params.window_size + 1;
+  const int64_t base = cur_node_;
+  // List of node v (in this block, or one of the cyc - 1 before it, kept in the ring).
+  auto list_of = [&](int64_t v, const int32_t** lp) -> int {
+    if (v >= base) {
+      *lp = succ[v - base];
+      return outd[v - base];
+    }
+    const int slot = (int)(v % cyc);
+    *lp = list_[(size_t)slot].data();
+    return list_len_[(size_t)slot];
+  };
+  // 1. Cost of every candidate of every node (-1: not a candidate by content).
+  std::vector<int64_t> cost((size_t)count * cyc, -1);
+  parallel_ranges(count, threads, [&](int, int lo, int hi) {
+    DiffScratch sc;
+    for (int i = lo; i < hi; ++i) {
+      if (outd[i] <= 0) continue;
+      const int64_t v = base + i;
+      for (int j = 0; j < cyc; ++j) {
+        if (v - j < 0) continue;
+        const int32_t* rl = nullptr;
+        const int rlen = j == 0 ? outd[i] : list_of(v - j, &rl);
+        if (rlen == 0) continue;
+        BitCounter bc;
+        diff_comp(bc, params, sc, nullptr, (int)v, j, rl, rlen, succ[i], outd[i]);
+        cost[(size_t)i * cyc + j] = (int64_t)bc.nbits;
+      }
+    }
+  });
+  // 2. Choices in node order: the cheapest candidate whose chain is not full, ties to the nearest.
+  std::vector<int> ref((size_t)count, 0), rc((size_t)count, 0);
+  auto ref_count_of = [&](int64_t v) { return v >= base ? rc[(size_t)(v - base)] : ref_count_[(size_t)(v % cyc)]; };
+  for (int i = 0; i < count; ++i) {
+    ++stats.nodes;
+    if (outd[i] <= 0) {
+      rc[(size_t)i] = ref_count_[(size_t)((base + i) % cyc)];  // unchanged, as add_node leaves it
+      continue;
+    }
+    const int64_t v = base + i;
+    int64_t best = INT32_MAX;
+    int bj = -1;
+    for (int j = 0; j < cyc; ++j) {
+      const int64_t c = cost[(size_t)i * cyc + j];
+      if (c < 0) continue;
+      const int r = j == 0 ? -1 : ref_count_of(v - j);
+      if (r < params.max_ref_count && c < best) {
+        best = c;
+        bj = j;
+      }
+    }
+    rc[(size_t)i] = (bj == 0 ? -1 : ref_count_of(v - bj)) + 1;
+    ref[(size_t)i] = bj;
+    stats.arcs += outd[i];
+    stats.tot_ref += rc[(size_t)i];
+    stats.tot_dist += bj;
+    stats.max_chain = std::max<int64_t>(stats.max_chain, rc[(size_t)i]);
+  }
+  // 3. Records written in parallel, each range into its own stream.
+  const int parts = std::max(1, std::min(threads, count));
+  std::vector<BitWriter> outs((size_t)parts);
+  std::vector<std::vector<uint64_t>> starts((size_t)parts);
+  std::vector<EncoderStats> st((size_t)parts);
+  parallel_ranges(count, parts, [&](int t, int lo, int hi) {
+    DiffScratch sc;
+    BitWriter& o = outs[(size_t)t];
+    for (int i = lo; i < hi; ++i) {
+      starts[(size_t)t].push_back(o.nbits);
+      st[(size_t)t].bits_outdegrees += o.write_gamma((uint64_t)outd[i]);
+      if (outd[i] > 0) {
+        const int32_t* rl = nullptr;
+        const int rlen = ref[(size_t)i] == 0 ? outd[i] : list_of(base + i - ref[(size_t)i], &rl);
+        diff_comp(o, params, sc, &st[(size_t)t], (int)(base + i), ref[(size_t)i], rl, rlen, succ[i], outd[i]);
+      }
+    }
+  });
+  // 4. Join in order; offsets of every record.
+  for (int t = 0; t < parts; ++t) {
+    const uint64_t at = graph.nbits;
+    for (uint64_t s0 : starts[(size_t)t]) {
+      offsets.write_gamma(at + s0 - last_bit_);
+      node_bit_offsets.push_back(at + s0);
+      last_bit_ = at + s0;
+    }
+    graph.append(outs[(size_t)t]);
+    add_stats(stats, st[(size_t)t]);
+  }
+  // 5. The ring holds the last cyc nodes for the next block, as add_node leaves it.
+  for (int i = std::max(0, count - cyc); i < count; ++i) {
+    const size_t slot = (size_t)((base + i) % cyc);
+    list_[slot].assign(succ[i], succ[i] + outd[i]);
+    list_len_[slot] = outd[i];
+    if (outd[i] > 0) ref_count_[slot] = rc[(size_t)i];
+  }
+  cur_node_ += count;
 }
 
 void GraphEncoder::finish() {
@@ -209,6 +350,29 @@ void TimestampEncoder::add_node(const int64_t* ts, int count) {
   for (int i = 0; i < count; ++i) {
     out.write_zeta(int2nat(ts[i] - prev), zeta_k);
     prev = ts[i];
+  }
+}
+
+void TimestampEncoder::add_block(const int64_t* const* ts, const int* count, int nodes, int threads) {
+  if (nodes <= 0) return;
+  const int parts = std::max(1, std::min(threads, nodes));
+  std::vector<BitWriter> outs((size_t)parts);
+  std::vector<std::vector<uint64_t>> starts((size_t)parts);
+  parallel_ranges(nodes, parts, [&](int t, int lo, int hi) {
+    BitWriter& o = outs[(size_t)t];
+    for (int i = lo; i < hi; ++i) {
+      starts[(size_t)t].push_back(o.nbits);
+      int64_t prev = min_timestamp;
+      for (int k = 0; k < count[i]; ++k) {
+        o.write_zeta(int2nat(ts[i][k] - prev), zeta_k);
+        prev = ts[i][k];
+      }
+    }
+  });
+  for (int t = 0; t < parts; ++t) {
+    const uint64_t at = out.nbits;
+    for (uint64_t s0 : starts[(size_t)t]) node_bit_offsets.push_back(at + s0);
+    out.append(outs[(size_t)t]);
   }
 }
 

@@ -42,12 +42,23 @@ struct EncoderStats {
   int64_t max_chain = 0;
 };
 
+// Scratch of one diff_comp evaluation (one per thread of the block encoder).
+struct DiffScratch {
+  std::vector<int32_t> mult_left, mult_len, singles, extras, blocks, left, len, residuals;
+};
+
 // Streaming successor-list encoder.  Nodes must be added in id order 0..n-1, each with
 // its successor list sorted by value (duplicates = parallel temporal edges).
 class GraphEncoder {
  public:
   explicit GraphEncoder(EncoderParams p = {});
   void add_node(const int32_t* succ, int outd);
+  // The next `count` nodes at once, on `threads` threads, with the same bytes, offsets and
+  // statistics as `count` calls of add_node.  A node's reference choice depends on earlier choices
+  // (the chain-depth limit), but the costs it compares do not: the costs of every candidate of
+  // every node are computed in parallel, the choices are made in node order, and the records are
+  // written in parallel into separate streams that are then joined bit by bit.
+  void add_block(const int32_t* const* succ, const int* outd, int count, int threads);
   void finish();  // writes the last offset delta
   BitWriter graph, offsets;
   std::vector<uint64_t> node_bit_offsets;  // n+1 entries
@@ -55,15 +66,11 @@ class GraphEncoder {
   EncoderParams params;
 
  private:
-  template <class Out>
-  void diff_comp(Out& obs, int cur, int ref, const int32_t* ref_list, int ref_len, const int32_t* cur_list,
-                 int cur_len, bool for_real);
   int cur_node_ = 0;
   uint64_t last_bit_ = 0;
   std::vector<std::vector<int32_t>> list_;
   std::vector<int> list_len_, ref_count_;
-  // scratch
-  std::vector<int32_t> mult_left_, mult_len_, singles_, extras_, blocks_, left_, len_, residuals_;
+  DiffScratch scratch_;
 };
 
 // Streaming timestamp writer (one call per node, in node order).
@@ -71,6 +78,8 @@ class TimestampEncoder {
  public:
   TimestampEncoder(int64_t min_timestamp, int zeta_k = 2);
   void add_node(const int64_t* ts, int count);
+  // The next `nodes` nodes at once on `threads` threads (same bytes and offsets as add_node).
+  void add_block(const int64_t* const* ts, const int* count, int nodes, int threads);
   void finish();
   BitWriter out;
   std::vector<uint64_t> node_bit_offsets;  // n+1 entries (first = 64)

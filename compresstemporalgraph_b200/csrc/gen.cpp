@@ -5,9 +5,11 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <numeric>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "format.hpp"
@@ -79,6 +81,32 @@ GenSummary generate_dataset(const GenParams& p, const std::string& dir, const st
   TimestampEncoder te(p.min_timestamp, ep.ts_zeta_k);
   FILE* raw = raw_path.empty() ? nullptr : std::fopen(raw_path.c_str(), "w");
   if (!raw_path.empty() && !raw) throw std::runtime_error("cannot write " + raw_path);
+
+  // Encoding threads: $TGA_ENCODE_THREADS, else the hardware's (at most 32); 0 encodes node by node
+  // (GraphEncoder::add_node).  The files are the same either way.
+  int threads = (int)std::min(32u, std::max(1u, std::thread::hardware_concurrency()));
+  if (const char* e = std::getenv("TGA_ENCODE_THREADS")) threads = std::max(0, std::atoi(e));
+  constexpr int64_t kBlockNodes = 1 << 16;
+  std::vector<int32_t> bsucc;     // the block's successor lists, back to back
+  std::vector<int64_t> bts;       // and their timestamps
+  std::vector<int64_t> boff{0};   // list i of the block: [boff[i], boff[i+1])
+  auto flush = [&]() {
+    const int nb = (int)boff.size() - 1;
+    if (nb == 0) return;
+    std::vector<const int32_t*> sp((size_t)nb);
+    std::vector<const int64_t*> tp((size_t)nb);
+    std::vector<int> len((size_t)nb);
+    for (int i = 0; i < nb; ++i) {
+      sp[(size_t)i] = bsucc.data() + boff[(size_t)i];
+      tp[(size_t)i] = bts.data() + boff[(size_t)i];
+      len[(size_t)i] = (int)(boff[(size_t)i + 1] - boff[(size_t)i]);
+    }
+    ge.add_block(sp.data(), len.data(), nb, threads);
+    te.add_block(tp.data(), len.data(), nb, threads);
+    bsucc.clear();
+    bts.clear();
+    boff.assign(1, 0);
+  };
 
   const int W = 7;
   std::vector<std::vector<int32_t>> ring(W + 1);  // distinct successors of the last vertices
@@ -164,13 +192,21 @@ GenSummary generate_dataset(const GenParams& p, const std::string& dir, const st
       std::sort(tsbuf.begin(), tsbuf.end());
       for (int64_t t : tsbuf) { succ.push_back(pr.first); ts.push_back(t); }
     }
-    ge.add_node(succ.data(), (int)succ.size());
-    te.add_node(ts.data(), (int)ts.size());
+    if (threads == 0) {
+      ge.add_node(succ.data(), (int)succ.size());
+      te.add_node(ts.data(), (int)ts.size());
+    } else {
+      bsucc.insert(bsucc.end(), succ.begin(), succ.end());
+      bts.insert(bts.end(), ts.begin(), ts.end());
+      boff.push_back((int64_t)bsucc.size());
+      if ((int64_t)boff.size() - 1 == kBlockNodes) flush();
+    }
     if (raw)
       for (size_t i = 0; i < succ.size(); ++i) std::fprintf(raw, "%lld\t%d\t1\t%lld\n", (long long)v, succ[i], (long long)ts[i]);
     sum.m += (int64_t)succ.size();
     sum.max_degree = std::max<int64_t>(sum.max_degree, (int64_t)succ.size());
   }
+  flush();
   ge.finish();
   te.finish();
   if (raw) std::fclose(raw);
