@@ -7,6 +7,7 @@
 #include <cerrno>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <exception>
 #include <map>
@@ -580,14 +581,42 @@ WrittenDataset write_dataset(const std::string& dir, const std::string& base, co
   return w;
 }
 
+int encode_threads() {
+  int threads = (int)std::min(32u, std::max(1u, std::thread::hardware_concurrency()));
+  if (const char* e = std::getenv("TGA_ENCODE_THREADS")) threads = std::max(0, std::atoi(e));
+  return threads;
+}
+
 WrittenDataset encode_and_write(const RawGraph& g, const std::string& dir, const std::string& base,
                                 int64_t max_label, const EncoderParams& p) {
   GraphEncoder ge(p);
   TimestampEncoder te(g.min_ts, p.ts_zeta_k);
-  for (int64_t v = 0; v < g.n; ++v) {
-    const int64_t b = g.src_begin[v], e = g.src_begin[v + 1];
-    ge.add_node(g.dst.data() + b, (int)(e - b));
-    te.add_node(g.ts.data() + b, (int)(e - b));
+  const int threads = encode_threads();
+  if (threads == 0) {
+    for (int64_t v = 0; v < g.n; ++v) {
+      const int64_t b = g.src_begin[v], e = g.src_begin[v + 1];
+      ge.add_node(g.dst.data() + b, (int)(e - b));
+      te.add_node(g.ts.data() + b, (int)(e - b));
+    }
+  } else {
+    constexpr int64_t kBlockNodes = 1 << 16;
+    std::vector<const int32_t*> sp;
+    std::vector<const int64_t*> tp;
+    std::vector<int> len;
+    for (int64_t v0 = 0; v0 < g.n; v0 += kBlockNodes) {
+      const int nb = (int)std::min<int64_t>(kBlockNodes, g.n - v0);
+      sp.resize((size_t)nb);
+      tp.resize((size_t)nb);
+      len.resize((size_t)nb);
+      for (int i = 0; i < nb; ++i) {
+        const int64_t b = g.src_begin[v0 + i], e = g.src_begin[v0 + i + 1];
+        sp[(size_t)i] = g.dst.data() + b;
+        tp[(size_t)i] = g.ts.data() + b;
+        len[(size_t)i] = (int)(e - b);
+      }
+      ge.add_block(sp.data(), len.data(), nb, threads);
+      te.add_block(tp.data(), len.data(), nb, threads);
+    }
   }
   ge.finish();
   te.finish();

@@ -73,6 +73,10 @@ class GraphEncoder {
   DiffScratch scratch_;
 };
 
+// Threads of the block encoders: $TGA_ENCODE_THREADS, else the hardware's (at most 32); 0 means
+// node by node (add_node).  The encoded files are the same for every value.
+int encode_threads();
+
 // Streaming timestamp writer (one call per node, in node order).
 class TimestampEncoder {
  public:

@@ -5,11 +5,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
-#include <cstdlib>
 #include <numeric>
 #include <stdexcept>
 #include <string>
-#include <thread>
 #include <vector>
 
 #include "format.hpp"
@@ -82,10 +80,7 @@ GenSummary generate_dataset(const GenParams& p, const std::string& dir, const st
   FILE* raw = raw_path.empty() ? nullptr : std::fopen(raw_path.c_str(), "w");
   if (!raw_path.empty() && !raw) throw std::runtime_error("cannot write " + raw_path);
 
-  // Encoding threads: $TGA_ENCODE_THREADS, else the hardware's (at most 32); 0 encodes node by node
-  // (GraphEncoder::add_node).  The files are the same either way.
-  int threads = (int)std::min(32u, std::max(1u, std::thread::hardware_concurrency()));
-  if (const char* e = std::getenv("TGA_ENCODE_THREADS")) threads = std::max(0, std::atoi(e));
+  const int threads = encode_threads();  // 0: node by node; the files are the same either way
   constexpr int64_t kBlockNodes = 1 << 16;
   std::vector<int32_t> bsucc;     // the block's successor lists, back to back
   std::vector<int64_t> bts;       // and their timestamps

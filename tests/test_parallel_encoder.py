@@ -48,3 +48,24 @@ def test_block_encoder_across_block_boundaries(tmp_path):
     for f in FILES:
         name = f.format(b="g")
         assert (tmp_path / "par" / name).read_bytes() == (tmp_path / "seq" / name).read_bytes(), name
+
+
+@pytest.mark.parametrize("shape", ["chains", "intervals"])
+def test_raw_encoder_block_equals_node(datasets, tmp_path, shape):
+    """tga_encode_raw through the block encoders writes the node-by-node bytes."""
+    d = datasets[shape]
+    outs = {}
+    for threads in (0, 3):
+        old = os.environ.get("TGA_ENCODE_THREADS")
+        os.environ["TGA_ENCODE_THREADS"] = str(threads)
+        try:
+            outs[threads] = tga.encode_raw(d["raw"], tmp_path / f"t{threads}", "r")
+        finally:
+            if old is None:
+                del os.environ["TGA_ENCODE_THREADS"]
+            else:
+                os.environ["TGA_ENCODE_THREADS"] = old
+    assert outs[0] == outs[3]
+    for f in FILES:
+        name = f.format(b="r")
+        assert (tmp_path / "t3" / name).read_bytes() == (tmp_path / "t0" / name).read_bytes(), name
