@@ -86,7 +86,7 @@ def build(verbose: bool = False, force: bool = False) -> Path:
     for name, src in TOOLS.items():
         s = CSRC / src
         exe = BIN / name
-        if s.exists() and (force or _stale(exe, [s, LIB] + headers)):
+        if force or _stale(exe, [s, LIB] + headers):
             _run(["g++", *CXX_FLAGS, f"-I{INCLUDE}", str(s), "-o", str(exe), f"-L{PKG}", "-ltga",
                   f"-Wl,-rpath,$ORIGIN/..", "-lpthread"], verbose)
         if exe.exists():
