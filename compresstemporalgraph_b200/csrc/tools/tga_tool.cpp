@@ -30,6 +30,7 @@
 #include <chrono>
 #include <cinttypes>
 #include <climits>
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -407,6 +408,14 @@ std::string json_str(const std::string& s) {
   return r + "\"";
 }
 
+// A JSON number, or null when the value is not finite (JSON has no NaN or infinity).
+std::string num(double x, const char* fmt = "%.9g") {
+  if (!std::isfinite(x)) return "null";
+  char b[64];
+  std::snprintf(b, sizeof b, fmt, x);
+  return b;
+}
+
 std::string hex64(uint64_t h) {
   char b[24];
   std::snprintf(b, sizeof b, "\"%016" PRIx64 "\"", h);
@@ -455,8 +464,7 @@ std::string summary(const Options& o, const Outputs& r) {
       double hs = 0, as = 0;
       for (float x : r.f32a) hs += (double)x * x;
       for (float x : r.f32b) as += (double)x * x;
-      std::snprintf(b, sizeof b, "\"hub_l2sq\": %.9g, \"auth_l2sq\": %.9g", hs, as);
-      s = b;
+      s = "\"hub_l2sq\": " + num(hs) + ", \"auth_l2sq\": " + num(as);
       break;
     }
     case Alg::NA: {
@@ -476,8 +484,8 @@ std::string summary(const Options& o, const Outputs& r) {
         sum += r.f32a[v];
         if (r.f32a[v] > r.f32a[top]) top = v;
       }
-      std::snprintf(b, sizeof b, "\"rank_sum\": %.9g, \"top_vertex\": %zu", sum, top);
-      s = b;
+      std::snprintf(b, sizeof b, ", \"top_vertex\": %zu", top);
+      s = "\"rank_sum\": " + num(sum) + b;
       break;
     }
     case Alg::NONE:
@@ -565,12 +573,13 @@ int main(int argc, char** argv) {
     char b[768];
     std::snprintf(b, sizeof b,
                   ", \"n\": %d, \"max_label\": %d, \"max_vertex\": %d, \"window\": [%" PRId64 ", %" PRId64
-                  "], \"repeat\": %d, \"device_ms\": %.6f, \"decode_ms\": %.6f, \"wall_ms\": %.6f, \"edges_decoded\": %" PRId64
-                  ", \"gteps\": %.6f, \"iterations\": %d, \"launches\": %" PRId64 ", \"compressed_bytes\": %" PRIu64
-                  ", \"device_bytes\": %" PRIu64,
-                  info.n, info.max_label, info.max_vertex, o.t_lo, o.t_hi, o.repeat, t.total_ms, t.decode_ms, wall_ms,
-                  t.edges_decoded, gteps, t.iterations, t.launches, t.compressed_bytes, info.device_bytes);
+                  "], \"repeat\": %d, \"edges_decoded\": %" PRId64 ", \"iterations\": %d, \"launches\": %" PRId64
+                  ", \"compressed_bytes\": %" PRIu64 ", \"device_bytes\": %" PRIu64,
+                  info.n, info.max_label, info.max_vertex, o.t_lo, o.t_hi, o.repeat, t.edges_decoded, t.iterations,
+                  t.launches, t.compressed_bytes, info.device_bytes);
     line += b;
+    line += ", \"device_ms\": " + num(t.total_ms, "%.6f") + ", \"decode_ms\": " + num(t.decode_ms, "%.6f") +
+            ", \"wall_ms\": " + num(wall_ms, "%.6f") + ", \"gteps\": " + num(gteps, "%.6f");
     if (o.autotune) {
       std::snprintf(b, sizeof b, ", \"tuned\": {\"slice_edges\": %d, \"item_edges\": %d, \"dense_div\": %d}",
                     tune.slice_edges, tune.item_edges, tune.dense_div);
