@@ -118,6 +118,7 @@ def _load() -> C.CDLL:
         "tga_degree": (C.c_int, [P, C.c_int64, C.c_int64, P, P]),
         "tga_color": (C.c_int, [P, C.c_int32, P, C.c_int32, P, P, C.POINTER(C.c_int32)]),
         "tga_bfs_batch": (C.c_int, [P, C.c_int32, P, P, P, P]),
+        "tga_fastest": (C.c_int, [P, C.c_int32, C.c_int64, C.c_int64, P, P]),
         "tga_cc_batch": (C.c_int, [P, C.c_int32, P, P, C.c_int32, P, P]),
         "tga_is_neighbor": (C.c_int, [P, C.c_int32, P, P, P, P, P]),
         "tga_pagerank_batch_iters": (C.c_int, [P, C.c_int32, P, C.c_float, C.c_float, P, P, P]),
@@ -360,6 +361,14 @@ class Graph:
         out = np.zeros((len(src), self.max_vertex), np.int32)
         _check(_lib.tga_bfs_batch(self._h, len(src), _ptr(src), _ptr(lo), _ptr(hi), _ptr(out)))
         return out
+
+    def fastest(self, src: int, t_lo: int = 0, t_hi: int = T_MAX):
+        """Fastest temporal paths from src (tga_fastest): (duration, departure) per vertex, -1 where
+        unreachable; the source has duration 0 and departure -1."""
+        dur = np.zeros(self.max_vertex, np.int64)
+        dep = np.zeros(self.max_vertex, np.int64)
+        _check(_lib.tga_fastest(self._h, src, t_lo, t_hi, _ptr(dur), _ptr(dep)))
+        return dur, dep
 
     def is_neighbor(self, node, neighbor, t_from=None, t_to=None):
         """Windowed point queries (tga_is_neighbor): True where some edge node->neighbor has a

@@ -1,0 +1,90 @@
+// Temporal path queries composed from the batched traversal (host code only: every kernel it runs
+// is the multi-source BFS of batch.cu).
+#include <algorithm>
+#include <climits>
+#include <vector>
+
+#include "engine.hpp"
+
+using namespace tga;
+
+namespace {
+
+void add_timing(tga_timing& sum, const tga_timing& t) {
+  sum.total_ms += t.total_ms;
+  sum.decode_ms += t.decode_ms;
+  sum.decode_launches += t.decode_launches;
+  sum.edges_decoded += t.edges_decoded;
+  sum.compressed_bytes += t.compressed_bytes;
+  sum.iterations += t.iterations;
+  sum.launches += t.launches;
+}
+
+}  // namespace
+
+// Fastest paths (temporal_ligra apps/temporal/Fastest-Compute.C:1-174 asks for the least elapsed
+// time from a source within [start, end]; there edges have a start and an end time, here an edge
+// happens at one instant).  A path's duration is the time of its last edge minus the time of its
+// first edge, its first edge leaving src at one of the distinct in-window timestamps d of src's
+// out-edges.  The earliest arrival from src over the window [d, t_hi) (tga_bfs) bounds the
+// duration of every path that departs at d or later, and the bound is met by a path departing at
+// exactly d when d minimises it, so
+//     duration(v) = min over d of (arrival_d(v) - d),
+// with paths following tga_bfs's edge rule.  The departures run as rows of the multi-source
+// traversal, up to 256 per launch and fewer when max_vertex is large (host rows are bounded to
+// about 256 MiB).  Host work is O(departures x max_vertex) for the minimum.
+extern "C" int tga_fastest(tga_graph* gp, int32_t src, int64_t t_lo, int64_t t_hi, int64_t* duration_out,
+                           int64_t* departure_out) {
+  if (!gp) return fail(TGA_E_ARG, "null graph");
+  GraphHandle& h = *gp;
+  const int32_t nv = h.view.max_vertex;
+  if (src < 0 || src >= nv) return fail(TGA_E_ARG, "source out of range");
+  if (t_lo < 0 || t_lo >= t_hi) return fail(TGA_E_ARG, "empty time window");
+
+  tga_timing sum{};
+  std::vector<int64_t> dep;
+  if (src < h.view.n) {
+    int32_t cnt = 0;
+    TGA_TRY(tga_neighbors(gp, src, nullptr, nullptr, 0, &cnt));
+    add_timing(sum, h.timing);
+    std::vector<int32_t> dst((size_t)std::max(cnt, 1));
+    std::vector<int64_t> ts((size_t)std::max(cnt, 1));
+    TGA_TRY(tga_neighbors(gp, src, dst.data(), ts.data(), cnt, &cnt));
+    add_timing(sum, h.timing);
+    for (int32_t i = 0; i < cnt; ++i)
+      if (ts[(size_t)i] >= t_lo && ts[(size_t)i] < t_hi) dep.push_back(ts[(size_t)i]);
+    std::sort(dep.begin(), dep.end());
+    dep.erase(std::unique(dep.begin(), dep.end()), dep.end());
+  }
+
+  std::vector<int64_t> best((size_t)nv, -1), when((size_t)nv, -1);
+  best[(size_t)src] = 0;
+  const int64_t row_cap = std::max<int64_t>(1, (int64_t(256) << 20) / (4 * (int64_t)nv));
+  const int32_t per = (int32_t)std::min<int64_t>(256, row_cap);
+  std::vector<int32_t> rows;
+  std::vector<int32_t> srcs((size_t)per, src);
+  std::vector<int64_t> his((size_t)per, t_hi);
+  for (size_t b = 0; b < dep.size(); b += (size_t)per) {
+    const int32_t k = (int32_t)std::min<size_t>((size_t)per, dep.size() - b);
+    rows.resize((size_t)k * (size_t)nv);
+    TGA_TRY(tga_bfs_batch(gp, k, srcs.data(), dep.data() + b, his.data(), rows.data()));
+    add_timing(sum, h.timing);
+    // Rows ascend in departure time, so a strict improvement keeps the earliest departure.
+    for (int32_t i = 0; i < k; ++i) {
+      const int64_t d = dep[b + (size_t)i];
+      const int32_t* arr = rows.data() + (size_t)i * (size_t)nv;
+      for (int32_t v = 0; v < nv; ++v) {
+        if (arr[v] == INT32_MAX || v == src) continue;
+        const int64_t dur = (int64_t)arr[v] - d;
+        if (best[(size_t)v] < 0 || dur < best[(size_t)v]) {
+          best[(size_t)v] = dur;
+          when[(size_t)v] = d;
+        }
+      }
+    }
+  }
+  if (duration_out) std::copy(best.begin(), best.end(), duration_out);
+  if (departure_out) std::copy(when.begin(), when.end(), departure_out);
+  h.timing = sum;
+  return TGA_OK;
+}

@@ -226,6 +226,18 @@ int tga_color(tga_graph* g, int32_t prio_mode, const uint32_t* prio_in, int32_t 
 int tga_bfs_batch(tga_graph* g, int32_t nsrc, const int32_t* src, const int64_t* t_lo, const int64_t* t_hi,
                   int32_t* arrival_out);
 
+/* Fastest temporal paths from one source (temporal_ligra apps/temporal/Fastest-Compute.C, whose
+ * edges have a start and an end time; here an edge happens at one instant, and paths follow
+ * tga_bfs's edge rule).  A path's duration is the time of its last edge minus the time of its
+ * first.  duration_out[v] = least duration of a path src -> v over edges with t in [t_lo, t_hi)
+ * (0 for src, -1 when unreachable); departure_out[v] = the earliest first-edge time achieving it
+ * (-1 for src and unreachable vertices).  Computed as the minimum over the distinct in-window
+ * timestamps d of src's out-edges of (earliest arrival over [d, t_hi)) - d, the departures running
+ * as rows of tga_bfs_batch's traversal.  Either output may be NULL.  The earliest-arrival query of
+ * the same project (EarliestArrival-Compute.C) is tga_bfs's arrival_out. */
+int tga_fastest(tga_graph* g, int32_t src, int64_t t_lo, int64_t t_hi, int64_t* duration_out,
+                int64_t* departure_out);
+
 /* Many connected-components queries (one per window [t_lo[i], t_hi[i])) in one launch: up to 32
  * windows share the 256 source slots of each speculative seed batch, every window keeping its own
  * candidates, validation, early exits and labels; larger counts run as several launches.

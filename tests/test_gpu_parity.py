@@ -498,3 +498,69 @@ def test_work_decomposition_does_not_change_results(pairs, shape, slice_edges, i
         assert float(np.abs(auth.astype(np.float64) - oauth).max()) <= 1e-5
     finally:
         g.set_work_params(default["slice_edges"], default["item_edges"])
+
+
+# ---- fastest temporal paths --------------------------------------------------------------------
+
+def _fastest_oracle(p, src, lo, hi):
+    """min over the distinct in-window departure times d of src of (oracle arrival over [d, hi)) - d,
+    the earliest d kept on ties."""
+    dur = np.full(p.mv, -1, np.int64)
+    dep = np.full(p.mv, -1, np.int64)
+    dur[src] = 0
+    if src < p.n:
+        _, ts = p.o.neighbors(src)
+        for d in np.unique(ts[(ts >= lo) & (ts < hi)]):
+            arr, _ = p.o.bfs(p.ml, p.mv, p.act, src, int(d), hi)
+            reach = arr != np.iinfo(np.int32).max
+            reach[src] = False
+            cand = arr.astype(np.int64) - int(d)
+            better = reach & ((dur < 0) | (cand < dur))
+            dur[better] = cand[better]
+            dep[better] = int(d)
+    return dur, dep
+
+
+def _path_sources(p, lo, hi, count=3, most=40):
+    off, _, ts = p.o.csr()
+    out = []
+    for v in np.random.default_rng(5).permutation(min(p.n, p.ml)):
+        t = ts[off[v]:off[v + 1]]
+        if 2 <= len(np.unique(t[(t >= lo) & (t < hi)])) <= most:
+            out.append(int(v))
+            if len(out) == count:
+                break
+    return out
+
+
+# widespan is left out: arrivals are 32-bit times, so the path queries need timestamps below 2^31.
+@pytest.mark.parametrize("shape", ["small", "chains", "hubs", "intervals", "sparse", "small_view"])
+def test_fastest_paths(pairs, shape):
+    p = pairs[shape]
+    for lo, hi in _windows(p)[:2]:
+        lo = max(lo, 0)
+        for src in _path_sources(p, lo, hi):
+            dur, dep = p.g.fastest(src, lo, hi)
+            odur, odep = _fastest_oracle(p, src, lo, hi)
+            assert np.array_equal(dur, odur), (src, lo, hi)
+            assert np.array_equal(dep, odep), (src, lo, hi)
+            assert (dur >= -1).all() and dur[src] == 0
+            # A fastest path departs no earlier than the window and takes no longer than arriving early.
+            arr, _ = p.g.bfs(src, lo, hi)
+            r = dur > 0
+            assert (dep[r] >= lo).all()
+            assert (dur[r] <= arr[r].astype(np.int64) - lo).all()
+
+
+def test_fastest_paths_edge_cases(pairs):
+    p = pairs["small_view"]  # max_vertex exceeds the vertices in the files
+    dur, dep = p.g.fastest(p.mv - 1)
+    assert dur[p.mv - 1] == 0 and (np.delete(dur, p.mv - 1) == -1).all() and (dep == -1).all()
+    off, _, _ = p.o.csr()
+    for sink in np.flatnonzero(np.diff(off) == 0)[:1]:  # a vertex without out-edges, if there is one
+        dur, dep = p.g.fastest(int(sink))
+        assert dur[sink] == 0 and (np.delete(dur, sink) == -1).all() and (dep == -1).all()
+    with pytest.raises(tga.TgaError):
+        p.g.fastest(0, 10, 10)
+    with pytest.raises(tga.TgaError):
+        p.g.fastest(p.mv)
