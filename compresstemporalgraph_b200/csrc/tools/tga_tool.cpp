@@ -100,7 +100,7 @@ struct Options {
   int32_t hits_mode = TGA_HITS_GPU;
   int32_t prio_mode = 0;
   bool java_isolated = false;
-  bool json = false, rank_summary = false, autotune = false;
+  bool json = false, rank_summary = false, autotune = false, show_config = false;
   std::string out;
   int repeat = 1;
 };
@@ -146,6 +146,7 @@ void usage(FILE* f, const char* prog) {
                "                        (also when TGA_DUMP_RANK_SUMMARY is set to a non-zero value)\n"
                "  --repeat N            run the workload N times on one load (one elapsed line each)\n"
                "  --autotune            time the work decompositions first and keep the fastest\n"
+               "  --show-config         print the resolved dataset settings as JSON and exit\n"
                "exit status: 0 ok, 1 missing file / CUDA / decode / format error, 2 bad arguments\n",
                prog);
 }
@@ -248,6 +249,7 @@ Options parse(int argc, char** argv) {
     else if (a == "--rank-summary") o.rank_summary = true;
     else if (a == "--repeat") o.repeat = (int)need_i64(o, "--repeat", val(), 1, 1000000);
     else if (a == "--autotune") o.autotune = true;
+    else if (a == "--show-config") o.show_config = true;
     else bad_args(o, "unknown option: " + a);
   }
   if (o.dir.empty() != o.base.empty()) bad_args(o, "--dir and --base go together");
@@ -502,6 +504,17 @@ int main(int argc, char** argv) {
   const std::string storage = o.storage.empty() ? o.dataset : o.storage;
   cfg.name = o.dataset.c_str();
   cfg.storage_name = storage.c_str();
+  if (o.show_config) {
+    const std::string mts = cfg.min_timestamp == TGA_UNSET_TS ? "null" : std::to_string(cfg.min_timestamp);
+    std::printf("{\"DATASET_NAME\": %s, \"DATASET_STORAGE_NAME\": %s, \"MAX_LABEL\": %d, \"MAX_Vertex\": %d, "
+                "\"minTimestamp\": %s, \"MIN_GRAPH_VERTEX\": %d, \"ACTIVE_VERTEX_BEGIN\": %d, \"BFS_START_VERTEX\": %d, "
+                "\"CONNECTED_COMPONENTS_VERTEX_BEGIN\": %d, \"MULTIPLE_INITIAL_VALUE\": %d, \"PAGERANK_ITERATIONS\": %d, "
+                "\"HITS_ITERATIONS\": %d}\n",
+                json_str(o.dataset).c_str(), json_str(storage).c_str(), cfg.max_label, cfg.max_vertex, mts.c_str(),
+                cfg.min_graph_vertex, cfg.active_vertex_begin, cfg.bfs_start_vertex, cfg.cc_vertex_begin,
+                cfg.multiple_initial_value, cfg.pr_iters, cfg.hits_iters);
+    return 0;
+  }
 
   tga_graph* g = nullptr;
   const int orc = o.dir.empty() ? tga_open(o.root.empty() ? nullptr : o.root.c_str(), &cfg, &g)

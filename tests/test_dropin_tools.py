@@ -8,6 +8,7 @@ the same result.
 """
 import json
 import os
+import re
 import subprocess
 from pathlib import Path
 
@@ -101,6 +102,41 @@ def test_tool_name_as_first_argument():
     assert r.returncode == 2 and "unknown algorithm: nosuch" in r.stderr
     r = run("tga_tool", "connected_components", "--help")
     assert r.returncode == 0 and r.stdout.startswith("usage: tga_tool connected_components ")
+
+
+REF_GPU = Path("/root/reference/gpu_cuda")  # read when the reference tree is present
+
+
+def _macros(path: Path) -> dict:
+    out = {}
+    for m in re.finditer(r'^\s*#define\s+(\w+)\s+("[^"]*"|-?\d+)', path.read_text(), flags=re.M):
+        out.setdefault(m.group(1), m.group(2).strip('"') if m.group(2).startswith('"') else int(m.group(2)))
+    return out
+
+
+@pytest.mark.skipif(not REF_GPU.exists(), reason="reference tree not present")
+@pytest.mark.parametrize("ds", ["Comm", "MyD", "Flickr", "Wiki", "Yahoo", "Yahoo-sub"])
+def test_presets_equal_the_reference_dataset_configs(ds):
+    """Each preset resolves to the reference's macros: gpu_cuda/<DS>/dataset_config.cuh over the
+    #ifndef defaults of shared/dataset_config_base.cuh."""
+    base = _macros(REF_GPU / "shared" / "dataset_config_base.cuh")
+    want = {**base, **_macros(REF_GPU / ds / "dataset_config.cuh")}
+    want.setdefault("DATASET_STORAGE_NAME", want["DATASET_NAME"])
+    r = run("bfs", "--dataset", ds, "--show-config")
+    assert r.returncode == 0, r.stderr
+    got = json.loads(r.stdout)
+    for k, v in got.items():
+        assert want[k] == v, (ds, k)
+
+
+def test_show_config_for_other_datasets():
+    r = run("hits", "--dataset", "x", "--max-label", 5, "--hits-iters", 3, "--show-config")
+    got = json.loads(r.stdout)
+    assert got["MAX_Vertex"] == 6 and got["HITS_ITERATIONS"] == 3 and got["minTimestamp"] is None
+    # Options after a preset override it.
+    r = run("bfs", "--dataset", "Wiki", "--pr-iters", 7, "--bfs-start", 3, "--show-config")
+    got = json.loads(r.stdout)
+    assert got["PAGERANK_ITERATIONS"] == 7 and got["BFS_START_VERTEX"] == 3 and got["HITS_ITERATIONS"] == 100
 
 
 @pytest.mark.skipif(has_gpu(), reason="checks the failure without a GPU")
