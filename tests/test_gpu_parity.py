@@ -12,6 +12,7 @@ import pytest
 import compresstemporalgraph_b200 as tga
 import pyoracle
 from conftest import SHAPES
+from test_temporal_paths import fastest_by_departures
 
 pytestmark = pytest.mark.gpu
 
@@ -503,22 +504,7 @@ def test_work_decomposition_does_not_change_results(pairs, shape, slice_edges, i
 # ---- fastest temporal paths --------------------------------------------------------------------
 
 def _fastest_oracle(p, src, lo, hi):
-    """min over the distinct in-window departure times d of src of (oracle arrival over [d, hi)) - d,
-    the earliest d kept on ties."""
-    dur = np.full(p.mv, -1, np.int64)
-    dep = np.full(p.mv, -1, np.int64)
-    dur[src] = 0
-    if src < p.n:
-        _, ts = p.o.neighbors(src)
-        for d in np.unique(ts[(ts >= lo) & (ts < hi)]):
-            arr, _ = p.o.bfs(p.ml, p.mv, p.act, src, int(d), hi)
-            reach = arr != np.iinfo(np.int32).max
-            reach[src] = False
-            cand = arr.astype(np.int64) - int(d)
-            better = reach & ((dur < 0) | (cand < dur))
-            dur[better] = cand[better]
-            dep[better] = int(d)
-    return dur, dep
+    return fastest_by_departures(p.o, p.n, p.ml, p.mv, p.act, src, lo, hi)
 
 
 def _path_sources(p, lo, hi, count=3, most=40):
