@@ -119,6 +119,8 @@ def _load() -> C.CDLL:
         "tga_color": (C.c_int, [P, C.c_int32, P, C.c_int32, P, P, C.POINTER(C.c_int32)]),
         "tga_bfs_batch": (C.c_int, [P, C.c_int32, P, P, P, P]),
         "tga_fastest": (C.c_int, [P, C.c_int32, C.c_int64, C.c_int64, P, P]),
+        "tga_reverse": (C.c_int, [P, C.c_int64, C.c_char_p, C.c_char_p, C.POINTER(C.c_int64)]),
+        "tga_latest_departure": (C.c_int, [P, C.c_int64, C.c_int32, C.c_int64, C.c_int64, P]),
         "tga_cc_batch": (C.c_int, [P, C.c_int32, P, P, C.c_int32, P, P]),
         "tga_is_neighbor": (C.c_int, [P, C.c_int32, P, P, P, P, P]),
         "tga_pagerank_batch_iters": (C.c_int, [P, C.c_int32, P, C.c_float, C.c_float, P, P, P]),
@@ -139,6 +141,8 @@ def _load() -> C.CDLL:
                                    C.POINTER(_GenSummary)]),
         "tga_encode_raw": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int64, C.POINTER(_GenSummary)]),
         "tga_build_index": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int64]),
+        "tga_write_reversed": (C.c_int, [P, P, P, C.c_int64, C.c_int64, C.c_char_p, C.c_char_p,
+                                          C.POINTER(_GenSummary)]),
         "tga_autotune": (C.c_int, [P, P]),
         "tga_barrier_selftest": (C.c_int, [C.c_double, P]),
         "tga_decode_table": (C.c_int, [C.c_int32, P]),
@@ -370,6 +374,20 @@ class Graph:
         _check(_lib.tga_fastest(self._h, src, t_lo, t_hi, _ptr(dur), _ptr(dep)))
         return dur, dep
 
+    def reverse(self, directory: str | os.PathLike, basename: str, pivot: int = -1) -> int:
+        """Writes the time-reversed copy (edge x->y at t becomes y->x at pivot - t) to
+        <directory>/<basename>.* (tga_reverse); returns the pivot (the largest timestamp when -1)."""
+        out = C.c_int64()
+        _check(_lib.tga_reverse(self._h, pivot, str(directory).encode(), basename.encode(), C.byref(out)))
+        return out.value
+
+    def latest_departure(self, pivot: int, target: int, t_lo: int = 0, t_hi: int = T_MAX) -> np.ndarray:
+        """On a reversed copy: the latest time each vertex can leave on a path to target inside
+        [t_lo, t_hi), -1 when none (tga_latest_departure)."""
+        out = np.zeros(self.max_vertex, np.int64)
+        _check(_lib.tga_latest_departure(self._h, pivot, target, t_lo, t_hi, _ptr(out)))
+        return out
+
     def is_neighbor(self, node, neighbor, t_from=None, t_to=None):
         """Windowed point queries (tga_is_neighbor): True where some edge node->neighbor has a
         timestamp in [t_from, t_to] (inclusive); no bounds when t_from/t_to are None."""
@@ -568,6 +586,17 @@ def encode_raw(raw_path: str | os.PathLike, directory: str | os.PathLike, basena
     s = _GenSummary()
     _check(_lib.tga_encode_raw(str(raw_path).encode(), str(directory).encode(), basename.encode(), max_label,
                                C.byref(s)))
+    return {k: getattr(s, k) for k, _ in _GenSummary._fields_}
+
+
+def write_reversed(offsets, dst, ts, pivot: int, directory: str | os.PathLike, basename: str) -> dict:
+    """Writes the time-reversed graph of a CSR as a dataset (tga_write_reversed, host only)."""
+    off = np.ascontiguousarray(offsets, np.int64)
+    d = np.ascontiguousarray(dst, np.int32)
+    t = np.ascontiguousarray(ts, np.int64)
+    s = _GenSummary()
+    _check(_lib.tga_write_reversed(_ptr(off), _ptr(d), _ptr(t), len(off) - 1, pivot, str(directory).encode(),
+                                   basename.encode(), C.byref(s)))
     return {k: getattr(s, k) for k, _ in _GenSummary._fields_}
 
 

@@ -1,4 +1,6 @@
 // Host-only C entry points of the format layer (no GPU needed).
+#include <algorithm>
+#include <climits>
 #include <cstdlib>
 #include <cstring>
 #include <stdexcept>
@@ -99,6 +101,57 @@ int tga_build_index(const char* dir, const char* base, int64_t max_label) {
       return fail(TGA_E_IO, "cannot write the index files into " + d);
   } catch (const std::exception& e) {
     return fail(TGA_E_FORMAT, std::string("rebuilding the index from .offsets: ") + e.what());
+  }
+  return TGA_OK;
+}
+
+int tga_write_reversed(const int64_t* offsets, const int32_t* dst, const int64_t* ts, int64_t n, int64_t pivot,
+                       const char* dir, const char* base, tga_gen_summary* out) {
+  if (!offsets || !dir || !base || n < 1 || n > INT32_MAX || pivot < 0) return fail(TGA_E_ARG, "bad argument");
+  if (offsets[0] != 0) return fail(TGA_E_ARG, "offsets must start at 0");
+  for (int64_t v = 0; v < n; ++v)
+    if (offsets[v + 1] < offsets[v]) return fail(TGA_E_ARG, "offsets must not decrease");
+  const int64_t m = offsets[n];
+  if (m > 0 && (!dst || !ts)) return fail(TGA_E_ARG, "null edge arrays");
+  // Counting sort by the new source (the old successor); old sources ascend, so every new list comes
+  // out ordered by successor, and a stable sort by reversed time orders each run of repeats.
+  RawGraph r;
+  r.n = n;
+  r.src_begin.assign((size_t)n + 1, 0);
+  for (int64_t e = 0; e < m; ++e) {
+    if (dst[e] < 0 || dst[e] >= n) return fail(TGA_E_ARG, "successor out of range");
+    if (ts[e] < 0 || ts[e] > pivot) return fail(TGA_E_ARG, "timestamp outside [0, pivot]");
+    ++r.src_begin[(size_t)dst[e] + 1];
+  }
+  for (int64_t v = 0; v < n; ++v) r.src_begin[(size_t)v + 1] += r.src_begin[(size_t)v];
+  r.dst.resize((size_t)m);
+  r.ts.resize((size_t)m);
+  std::vector<int64_t> fill(r.src_begin.begin(), r.src_begin.end() - 1);
+  r.min_ts = m ? INT64_MAX : 0;
+  for (int64_t x = 0; x < n; ++x)
+    for (int64_t e = offsets[x]; e < offsets[x + 1]; ++e) {
+      const int64_t at = fill[(size_t)dst[e]]++;
+      r.dst[(size_t)at] = (int32_t)x;
+      r.ts[(size_t)at] = pivot - ts[e];
+      r.min_ts = std::min(r.min_ts, pivot - ts[e]);
+    }
+  for (int64_t y = 0; y < n; ++y) {
+    int64_t a = r.src_begin[(size_t)y];
+    const int64_t end = r.src_begin[(size_t)y + 1];
+    while (a < end) {
+      int64_t b = a + 1;
+      while (b < end && r.dst[(size_t)b] == r.dst[(size_t)a]) ++b;
+      std::sort(r.ts.begin() + a, r.ts.begin() + b);
+      a = b;
+    }
+  }
+  try {
+    const WrittenDataset w = encode_and_write(r, dir, base, n - 1, EncoderParams{});
+    int64_t maxdeg = 0;
+    for (int64_t v = 0; v < n; ++v) maxdeg = std::max<int64_t>(maxdeg, r.src_begin[(size_t)v + 1] - r.src_begin[(size_t)v]);
+    fill_summary(out, w.n, w.m, maxdeg, w.graph_bytes, w.ts_bytes, w.index_bytes, w.stats);
+  } catch (const std::exception& e) {
+    return fail(TGA_E_FORMAT, e.what());
   }
   return TGA_OK;
 }

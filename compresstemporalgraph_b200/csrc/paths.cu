@@ -88,3 +88,48 @@ extern "C" int tga_fastest(tga_graph* gp, int32_t src, int64_t t_lo, int64_t t_h
   h.timing = sum;
   return TGA_OK;
 }
+
+// Time-reversed copy of a graph, for latest-departure queries (temporal_ligra
+// apps/temporal/LatestDeparture-Compute.C:1-149 transposes the graph and walks it from the target).
+// The lists are decoded on the device (tga_decode_all) and written on the host (tga_write_reversed):
+// edge (x -> y, t) becomes (y -> x, pivot - t).
+extern "C" int tga_reverse(tga_graph* gp, int64_t pivot, const char* dir, const char* base, int64_t* pivot_out) {
+  if (!gp || !dir || !base) return fail(TGA_E_ARG, "null argument");
+  GraphHandle& h = *gp;
+  const int64_t n = h.view.n;
+  std::vector<int64_t> off((size_t)n + 1);
+  TGA_TRY(tga_decode_all(gp, off.data(), nullptr, nullptr, 0));
+  const int64_t m = off[(size_t)n];
+  std::vector<int32_t> dst((size_t)std::max<int64_t>(m, 1));
+  std::vector<int64_t> ts((size_t)std::max<int64_t>(m, 1));
+  TGA_TRY(tga_decode_all(gp, off.data(), dst.data(), ts.data(), m));
+  if (pivot < 0) pivot = m ? *std::max_element(ts.begin(), ts.begin() + m) : 0;
+  TGA_TRY(tga_write_reversed(off.data(), dst.data(), ts.data(), n, pivot, dir, base, nullptr));
+  if (pivot_out) *pivot_out = pivot;
+  return TGA_OK;
+}
+
+// Latest departures towards one target: out[v] = the latest time a path v -> target can leave v,
+// using edges with t in [t_lo, t_hi).  On the reversed copy a forward path v -> target leaving at d
+// is a path target -> v arriving at pivot - d, and the window maps to (pivot - t_hi, pivot - t_lo],
+// so one earliest-arrival traversal from the target gives every vertex's latest departure.
+extern "C" int tga_latest_departure(tga_graph* rev, int64_t pivot, int32_t target, int64_t t_lo, int64_t t_hi,
+                                    int64_t* out) {
+  if (!rev) return fail(TGA_E_ARG, "null graph");
+  GraphHandle& h = *rev;
+  const int32_t nv = h.view.max_vertex;
+  if (target < 0 || target >= nv) return fail(TGA_E_ARG, "target out of range");
+  if (t_lo < 0 || t_lo >= t_hi || pivot < 0) return fail(TGA_E_ARG, "empty time window");
+  std::vector<int32_t> arr((size_t)nv);
+  if (t_lo > pivot) {  // every edge is earlier than the window
+    if (out) std::fill(out, out + nv, int64_t(-1));
+    if (out) out[target] = std::min(t_hi - 1, pivot);
+    return TGA_OK;
+  }
+  const int64_t lo = t_hi > pivot ? 0 : pivot - t_hi + 1;
+  const int64_t hi = pivot - t_lo + 1;
+  TGA_TRY(tga_bfs(rev, target, lo, hi, arr.data(), nullptr));
+  if (out)
+    for (int32_t v = 0; v < nv; ++v) out[v] = arr[(size_t)v] == INT32_MAX ? -1 : pivot - arr[(size_t)v];
+  return TGA_OK;
+}

@@ -238,6 +238,19 @@ int tga_bfs_batch(tga_graph* g, int32_t nsrc, const int32_t* src, const int64_t*
 int tga_fastest(tga_graph* g, int32_t src, int64_t t_lo, int64_t t_hi, int64_t* duration_out,
                 int64_t* departure_out);
 
+/* Latest departures towards one target (temporal_ligra apps/temporal/LatestDeparture-Compute.C,
+ * "reverse foremost", which transposes the graph).  tga_reverse writes a time-reversed copy of g to
+ * <dir>/<base>.* with its index files: edge (x -> y, t) becomes (y -> x, pivot - t); pivot < 0 ->
+ * the largest timestamp of g, returned in *pivot_out.  Open the copy with g's configuration.
+ * tga_latest_departure(copy, pivot, target, ...) then gives out[v] = the latest first-edge time of
+ * a path v -> target over edges with t in [t_lo, t_hi) (paths follow tga_bfs's edge rule on the
+ * copy), -1 when there is none; out[target] = min(t_hi - 1, pivot).  One traversal from the target
+ * on the copy over the window [pivot - t_hi + 1, pivot - t_lo + 1); pivot minus the timestamps must
+ * stay below 2^31, as tga_bfs's arrivals are 32-bit. */
+int tga_reverse(tga_graph* g, int64_t pivot, const char* dir, const char* base, int64_t* pivot_out);
+int tga_latest_departure(tga_graph* reversed, int64_t pivot, int32_t target, int64_t t_lo, int64_t t_hi,
+                         int64_t* out);
+
 /* Many connected-components queries (one per window [t_lo[i], t_hi[i])) in one launch: up to 32
  * windows share the 256 source slots of each speculative seed batch, every window keeping its own
  * candidates, validation, early exits and labels; larger counts run as several launches.
@@ -358,6 +371,12 @@ int tga_generate(const tga_gen_params* p, const char* dir, const char* base, con
  * EvolvingMultiGraph.store does (EvolvingMultiGraph.java:147-275), plus the 4 EF index files.
  * max_label < 0 -> n-1. */
 int tga_encode_raw(const char* raw_path, const char* dir, const char* base, int64_t max_label, tga_gen_summary* out);
+
+/* Host-only writer behind tga_reverse: writes the time-reversed graph of a CSR (offsets[n+1],
+ * dst[m], ts[m], every ts in [0, pivot]) as a dataset <dir>/<base>.* with its index files.  Each
+ * new list is ordered by successor, and repeated successors by reversed time. */
+int tga_write_reversed(const int64_t* offsets, const int32_t* dst, const int64_t* ts, int64_t n, int64_t pivot,
+                       const char* dir, const char* base, tga_gen_summary* out);
 
 /* Producer of the four GPU index files (graph_{lower,upper}_bits.bin, timestamp_{lower,upper}_bits.bin,
  * the layout read by sh/bfs.cu:543-565,1785-1789, for which the reference ships no producer) for a

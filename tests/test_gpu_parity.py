@@ -12,7 +12,7 @@ import pytest
 import compresstemporalgraph_b200 as tga
 import pyoracle
 from conftest import SHAPES
-from test_temporal_paths import fastest_by_departures
+from test_temporal_paths import fastest_by_departures, latest_by_reversal
 
 pytestmark = pytest.mark.gpu
 
@@ -550,3 +550,28 @@ def test_fastest_paths_edge_cases(pairs):
         p.g.fastest(0, 10, 10)
     with pytest.raises(tga.TgaError):
         p.g.fastest(p.mv)
+
+
+# ---- latest departure on the time-reversed copy -----------------------------------------------
+
+@pytest.mark.parametrize("shape", ["small", "chains", "hubs", "intervals", "sparse"])
+def test_latest_departure(pairs, shape, tmp_path):
+    p = pairs[shape]
+    off, dst, ts = p.o.csr()
+    pivot = p.g.reverse(tmp_path / "dev", "rev")
+    assert pivot == int(ts.max())
+    # The copy written from the device decode equals the one written from the oracle's lists.
+    tga.write_reversed(off, dst, ts, pivot, tmp_path / "cpu", "rev")
+    for f in sorted((tmp_path / "cpu").iterdir()):
+        assert (tmp_path / "dev" / f.name).read_bytes() == f.read_bytes(), f.name
+    orev = pyoracle.Oracle(tmp_path / "cpu", "rev", p.n)
+    with tga.Graph.open_dir(tmp_path / "dev", "rev", p.cfg) as grev:
+        targets = [int(np.argmax(np.bincount(dst, minlength=p.n))), 1, p.n // 2]
+        lo0, span = p.d["params"].min_timestamp, p.d["params"].ts_span
+        for target in targets:
+            for lo, hi in [(0, T_MAX), (lo0 + span // 4, lo0 + 3 * span // 4), (pivot + 1, T_MAX)]:
+                got = grev.latest_departure(pivot, target, lo, hi)
+                want = latest_by_reversal(orev, p.n, p.ml, p.mv, p.act, pivot, target, lo, hi)
+                assert np.array_equal(got, want), (target, lo, hi)
+        with pytest.raises(tga.TgaError):
+            grev.latest_departure(pivot, 0, 5, 5)

@@ -129,3 +129,87 @@ def test_hand_made_case(tmp_path):
     dur, dep = fastest_by_departures(o, 4, 3, 4, 0, 0, 2, 9)
     assert dur.tolist() == [0, 0, 1, 1]
     assert dep.tolist() == [-1, 5, 5, 5]
+
+
+# ---- latest departure through the time-reversed copy -------------------------------------------
+
+def latest_by_reversal(orev, n, ml, mv, act, pivot, target, lo, hi):
+    """tga_latest_departure's mapping, with the oracle's BFS on the reversed copy."""
+    out = np.full(mv, -1, np.int64)
+    if lo > pivot:
+        out[target] = min(hi - 1, pivot)
+        return out
+    rlo = 0 if hi > pivot else pivot - hi + 1
+    arr, _ = orev.bfs(ml, mv, act, target, rlo, pivot - lo + 1)
+    reach = arr != INF32
+    out[reach] = pivot - arr[reach].astype(np.int64)
+    return out
+
+
+def latest_by_definition(out, n, mv, pivot, target, lo, hi):
+    """Latest first-edge time of a time-respecting path v -> target inside [lo, hi), trying each
+    vertex's out-edges from the latest (plain view: every vertex's edges are followed)."""
+    res = np.full(mv, -1, np.int64)
+    res[target] = min(hi - 1, pivot)
+
+    def reaches(y, d):
+        arr = {y: d}
+        heap = [(d, y)]
+        while heap:
+            a, x = heapq.heappop(heap)
+            if x == target:
+                return True
+            if a != arr[x]:
+                continue
+            for z, t in out[x]:
+                if a <= t < hi and t < arr.get(z, INF32):
+                    arr[z] = t
+                    heapq.heappush(heap, (t, z))
+        return False
+
+    for v in range(n):
+        if v == target:
+            continue
+        for y, d in sorted(out[v], key=lambda e: -e[1]):
+            if lo <= d < hi and (y == target or reaches(y, d)):
+                res[v] = d
+                break
+    return res
+
+
+def test_reversed_copy_is_the_transposition(tmp_path, datasets):
+    d = datasets["chains"]  # reference chains, intervals and repeated successors
+    n = d["summary"]["n"]
+    off, dst, ts = pyoracle.Oracle(d["dir"], d["base"], n).csr()
+    pivot = int(ts.max()) + 3
+    tga.write_reversed(off, dst, ts, pivot, tmp_path, "rev")
+    roff, rdst, rts = pyoracle.Oracle(tmp_path, "rev", n).csr()
+    src = np.repeat(np.arange(n), np.diff(off))
+    order = np.lexsort((pivot - ts, src, dst))  # by new source, then successor, then reversed time
+    assert np.array_equal(roff, np.concatenate([[0], np.cumsum(np.bincount(dst, minlength=n))]))
+    assert np.array_equal(rdst, src[order])
+    assert np.array_equal(rts, (pivot - ts)[order])
+
+
+def test_write_reversed_rejects_bad_input(tmp_path):
+    off = np.array([0, 1, 2])
+    with pytest.raises(tga.TgaError):
+        tga.write_reversed(off, np.array([1, 0]), np.array([5, 9]), 8, tmp_path, "x")  # 9 > pivot
+    with pytest.raises(tga.TgaError):
+        tga.write_reversed(off, np.array([1, 2]), np.array([5, 6]), 8, tmp_path, "x")  # successor 2 >= n
+    with pytest.raises(tga.TgaError):
+        tga.write_reversed(np.array([0, 2, 1]), np.array([1, 0]), np.array([5, 6]), 8, tmp_path, "x")
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_latest_departure_by_reversal_equals_definition(tmp_path, seed):
+    o, out, n = _graph(tmp_path, seed, 40, 220, 30)
+    off, dst, ts = o.csr()
+    pivot = int(ts.max())
+    tga.write_reversed(off, dst, ts, pivot, tmp_path, f"r{seed}")
+    orev = pyoracle.Oracle(tmp_path, f"r{seed}", n)
+    for lo, hi in [(0, tga.T_MAX), (8, 22), (0, 15), (pivot + 1, pivot + 5)]:
+        for target in range(n):
+            got = latest_by_reversal(orev, n, n - 1, n, 0, pivot, target, lo, hi)
+            want = latest_by_definition(out, n, n, pivot, target, lo, hi)
+            assert np.array_equal(got, want), (target, lo, hi)
