@@ -2,6 +2,7 @@
 // is the multi-source BFS of batch.cu).
 #include <algorithm>
 #include <climits>
+#include <thread>
 #include <vector>
 
 #include "engine.hpp"
@@ -32,7 +33,7 @@ void add_timing(tga_timing& sum, const tga_timing& t) {
 //     duration(v) = min over d of (arrival_d(v) - d),
 // with paths following tga_bfs's edge rule.  The departures run as rows of the multi-source
 // traversal, up to 256 per launch and fewer when max_vertex is large (host rows are bounded to
-// about 256 MiB).  Host work is O(departures x max_vertex) for the minimum.
+// about 256 MiB).  Host work is O(departures x max_vertex) for the minimum, on up to 32 threads.
 extern "C" int tga_fastest(tga_graph* gp, int32_t src, int64_t t_lo, int64_t t_hi, int64_t* duration_out,
                            int64_t* departure_out) {
   if (!gp) return fail(TGA_E_ARG, "null graph");
@@ -69,18 +70,37 @@ extern "C" int tga_fastest(tga_graph* gp, int32_t src, int64_t t_lo, int64_t t_h
     rows.resize((size_t)k * (size_t)nv);
     TGA_TRY(tga_bfs_batch(gp, k, srcs.data(), dep.data() + b, his.data(), rows.data()));
     add_timing(sum, h.timing);
-    // Rows ascend in departure time, so a strict improvement keeps the earliest departure.
-    for (int32_t i = 0; i < k; ++i) {
-      const int64_t d = dep[b + (size_t)i];
-      const int32_t* arr = rows.data() + (size_t)i * (size_t)nv;
-      for (int32_t v = 0; v < nv; ++v) {
-        if (arr[v] == INT32_MAX || v == src) continue;
-        const int64_t dur = (int64_t)arr[v] - d;
-        if (best[(size_t)v] < 0 || dur < best[(size_t)v]) {
-          best[(size_t)v] = dur;
-          when[(size_t)v] = d;
+    // Rows ascend in departure time, so a strict improvement keeps the earliest departure.  Each
+    // vertex's minimum is independent: large batches are split by vertex range over host threads.
+    auto fold = [&](int32_t v0, int32_t v1) {
+      for (int32_t i = 0; i < k; ++i) {
+        const int64_t d = dep[b + (size_t)i];
+        const int32_t* arr = rows.data() + (size_t)i * (size_t)nv;
+        for (int32_t v = v0; v < v1; ++v) {
+          if (arr[v] == INT32_MAX || v == src) continue;
+          const int64_t dur = (int64_t)arr[v] - d;
+          if (best[(size_t)v] < 0 || dur < best[(size_t)v]) {
+            best[(size_t)v] = dur;
+            when[(size_t)v] = d;
+          }
         }
       }
+    };
+    const int64_t work = (int64_t)k * nv;
+    const int threads = work < (int64_t(1) << 18)
+                            ? 1
+                            : (int)std::min<unsigned>(32, std::max(1u, std::thread::hardware_concurrency()));
+    if (threads == 1) {
+      fold(0, nv);
+    } else {
+      std::vector<std::thread> pool;
+      const int32_t chunk = (int32_t)((nv + threads - 1) / threads);
+      for (int t = 0; t < threads; ++t) {
+        const int32_t v0 = (int32_t)std::min<int64_t>((int64_t)t * chunk, nv);
+        const int32_t v1 = (int32_t)std::min<int64_t>((int64_t)v0 + chunk, nv);
+        if (v0 < v1) pool.emplace_back(fold, v0, v1);
+      }
+      for (auto& th : pool) th.join();
     }
   }
   if (duration_out) std::copy(best.begin(), best.end(), duration_out);

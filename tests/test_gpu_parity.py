@@ -538,6 +538,22 @@ def test_fastest_paths(pairs, shape):
             assert (dur[r] <= arr[r].astype(np.int64) - lo).all()
 
 
+def test_fastest_paths_from_a_hub(pairs):
+    """400 departures of the largest hub: two traversal batches (256 + 144 rows of 2,000 vertices),
+    each large enough for the minimum to be taken on several host threads."""
+    p = pairs["hubs"]
+    off, _, _ = p.o.csr()
+    hub = int(np.argmax(np.diff(off)))
+    _, ts = p.o.neighbors(hub)
+    uts = np.unique(ts)
+    assert len(uts) > 500
+    lo, hi = int(uts[len(uts) // 4]), int(uts[len(uts) // 4 + 400])
+    dur, dep = p.g.fastest(hub, lo, hi)
+    odur, odep = _fastest_oracle(p, hub, lo, hi)
+    assert np.array_equal(dur, odur)
+    assert np.array_equal(dep, odep)
+
+
 def test_fastest_paths_edge_cases(pairs):
     p = pairs["small_view"]  # max_vertex exceeds the vertices in the files
     dur, dep = p.g.fastest(p.mv - 1)
