@@ -83,6 +83,12 @@ class _GenParams(C.Structure):
                 ("ts_span", C.c_int64), ("min_timestamp", C.c_int64), ("seed", C.c_uint64), ("ref_safe", C.c_int32)]
 
 
+class _RefDepths(C.Structure):
+    _fields_ = [("nodes", C.c_int64), ("referenced_nodes", C.c_int64), ("truncated_nodes", C.c_int64),
+                ("maximum_depth", C.c_int32), ("configured_max_ref_count", C.c_int32),
+                ("depth_counts", C.c_int64 * 16)]
+
+
 class _GenSummary(C.Structure):
     _fields_ = [("n", C.c_int64), ("m", C.c_int64), ("max_degree", C.c_int64), ("graph_bytes", C.c_uint64),
                 ("timestamp_bytes", C.c_uint64), ("index_bytes", C.c_uint64), ("copied_arcs", C.c_int64),
@@ -143,6 +149,7 @@ def _load() -> C.CDLL:
         "tga_build_index": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int64]),
         "tga_write_reversed": (C.c_int, [P, P, P, C.c_int64, C.c_int64, C.c_char_p, C.c_char_p,
                                           C.POINTER(_GenSummary)]),
+        "tga_reference_depths": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(_RefDepths), P]),
         "tga_autotune": (C.c_int, [P, P]),
         "tga_barrier_selftest": (C.c_int, [C.c_double, P]),
         "tga_decode_table": (C.c_int, [C.c_int32, P]),
@@ -598,6 +605,19 @@ def write_reversed(offsets, dst, ts, pivot: int, directory: str | os.PathLike, b
     _check(_lib.tga_write_reversed(_ptr(off), _ptr(d), _ptr(t), len(off) - 1, pivot, str(directory).encode(),
                                    basename.encode(), C.byref(s)))
     return {k: getattr(s, k) for k, _ in _GenSummary._fields_}
+
+
+def reference_depths(directory: str | os.PathLike, basename: str):
+    """Realised reference-chain depth of every list (tga_reference_depths, host only): returns the
+    summary (nodes, referenced_nodes, truncated_nodes, maximum_depth, configured_max_ref_count,
+    depth_counts) and the per-list depths."""
+    r = _RefDepths()
+    _check(_lib.tga_reference_depths(str(directory).encode(), basename.encode(), C.byref(r), None))
+    depth = np.zeros(r.nodes, np.int32)
+    _check(_lib.tga_reference_depths(str(directory).encode(), basename.encode(), C.byref(r), _ptr(depth)))
+    summary = {k: getattr(r, k) for k, _ in _RefDepths._fields_ if k != "depth_counts"}
+    summary["depth_counts"] = list(r.depth_counts)
+    return summary, depth
 
 
 def build_index(directory: str | os.PathLike, basename: str, max_label: int) -> None:

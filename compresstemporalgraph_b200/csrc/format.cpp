@@ -436,6 +436,26 @@ void index_from_offsets(const std::vector<uint8_t>& graph, const std::vector<uin
   *ts_ef = ef_build(toff, ef_low_bits(timestamps.size(), max_label));
 }
 
+std::vector<int32_t> reference_depths(const std::vector<uint8_t>& graph, const std::vector<uint8_t>& offsets,
+                                      int64_t n, int window_size) {
+  if (n <= 0) throw std::runtime_error("vertex count needed (the nodes property)");
+  std::vector<int32_t> depth((size_t)n, 0);
+  FastBitReader ob(offsets), gb(graph);
+  uint64_t at = 0;
+  for (int64_t v = 0; v < n; ++v) {
+    at += ob.gamma();
+    if (at >= (uint64_t)graph.size() * 8 + 1) throw std::runtime_error("offsets point past the end of the graph stream");
+    gb.seek(at);
+    const uint64_t deg = gb.gamma();
+    if (deg == 0 || window_size <= 0) continue;
+    const uint64_t ref = gb.unary();
+    if (ref == 0) continue;
+    if (ref > (uint64_t)v) throw std::runtime_error("reference before the first list at node " + std::to_string(v));
+    depth[(size_t)v] = depth[(size_t)(v - (int64_t)ref)] + 1;
+  }
+  return depth;
+}
+
 uint64_t ef_get_host(const EFIndex& ef, uint64_t i) {
   uint64_t low = 0;
   for (int b = 0; b < ef.l; ++b) {

@@ -139,6 +139,14 @@ void index_from_offsets(const std::vector<uint8_t>& graph, const std::vector<uin
                         EFIndex* graph_ef, EFIndex* ts_ef);
 
 std::map<std::string, std::string> read_properties(const std::string& path);
+
+// Realised reference-chain depth of every list (ReferenceDepthScanner.java:24-87): a list that
+// copies from the list `ref` positions back has depth one more than that list, others depth 0.
+// Reads each record's outdegree and reference only, entering it at its offset from <base>.offsets
+// (gamma-coded bit-position deltas, n+1 of them).  window_size 0 means records carry no
+// reference.  Throws std::runtime_error on malformed input.
+std::vector<int32_t> reference_depths(const std::vector<uint8_t>& graph, const std::vector<uint8_t>& offsets,
+                                      int64_t n, int window_size);
 bool write_file(const std::string& path, const void* data, size_t n);
 bool read_file(const std::string& path, std::vector<uint8_t>& out);
 

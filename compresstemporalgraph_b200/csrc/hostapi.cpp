@@ -156,6 +156,38 @@ int tga_write_reversed(const int64_t* offsets, const int32_t* dst, const int64_t
   return TGA_OK;
 }
 
+int tga_reference_depths(const char* dir, const char* base, tga_ref_depths* out, int32_t* depth_out) {
+  if (!dir || !base || !out) return fail(TGA_E_ARG, "null argument");
+  const std::string bp = std::string(dir) + "/" + base;
+  std::vector<uint8_t> graph, offsets;
+  if (!read_file(bp + ".graph", graph)) return fail(TGA_E_IO, "Cannot open required file: " + bp + ".graph");
+  if (!read_file(bp + ".offsets", offsets)) return fail(TGA_E_IO, "Cannot open required file: " + bp + ".offsets");
+  const auto pr = read_properties(bp + ".properties");
+  auto prop = [&](const char* k, int64_t dflt) {
+    const auto it = pr.find(k);
+    return it == pr.end() ? dflt : (int64_t)std::atoll(it->second.c_str());
+  };
+  const int64_t n = prop("nodes", -1);
+  if (n <= 0) return fail(TGA_E_FORMAT, "the nodes property of " + bp + ".properties is needed");
+  std::memset(out, 0, sizeof *out);
+  try {
+    const std::vector<int32_t> depth = reference_depths(graph, offsets, n, (int)prop("windowsize", 7));
+    out->nodes = n;
+    out->configured_max_ref_count = (int32_t)prop("maxrefcount", 3);
+    for (int64_t v = 0; v < n; ++v) {
+      const int32_t d = depth[(size_t)v];
+      out->referenced_nodes += d > 0;
+      out->maximum_depth = std::max(out->maximum_depth, d);
+      if (d < 16) ++out->depth_counts[d];
+      else ++out->truncated_nodes;
+    }
+    if (depth_out) std::copy(depth.begin(), depth.end(), depth_out);
+  } catch (const std::exception& e) {
+    return fail(TGA_E_FORMAT, e.what());
+  }
+  return TGA_OK;
+}
+
 int tga_decode_table(int32_t kind, int32_t* out) {
   if (!out || (kind != 0 && kind != 3)) return fail(TGA_E_ARG, "kind must be 0 (gamma) or 3 (zeta_3)");
   const std::vector<int32_t> t = table16(kind);

@@ -108,6 +108,7 @@ struct Options {
 void usage(FILE* f, const char* prog) {
   std::fprintf(f,
                "usage: %s [options]            (or: tga_tool <algorithm> [options])\n"
+               "       tga_tool reference_depths <graph-basename>   (ReferenceDepthScanner's report)\n"
                "algorithms: bfs connected_components degree_centrality graph_coloring hits\n"
                "            neighbor_access pagerank\n"
                "dataset (the reference's per-dataset macros; Comm, MyD, Flickr, Wiki, Yahoo and\n"
@@ -498,7 +499,32 @@ std::string summary(const Options& o, const Outputs& r) {
 
 }  // namespace
 
+// `tga_tool reference_depths <graph-basename>`: cpu_java ReferenceDepthScanner.java:89-110, same
+// argument and RESULT line (host only, no GPU).
+int reference_depths_main(int argc, char** argv) {
+  if (argc != 3 || argv[2][0] == '-') {
+    std::fprintf(stderr, "Usage: tga_tool reference_depths <graph-basename>\n");
+    return 2;
+  }
+  const std::string bn = argv[2];
+  const size_t slash = bn.find_last_of('/');
+  const std::string dir = slash == std::string::npos ? "." : bn.substr(0, slash);
+  const std::string base = slash == std::string::npos ? bn : bn.substr(slash + 1);
+  tga_ref_depths r{};
+  const int rc = tga_reference_depths(dir.c_str(), base.c_str(), &r, nullptr);
+  if (rc) {
+    std::fprintf(stderr, "%s\n", tga_last_error());
+    return rc == TGA_E_ARG ? 2 : 1;
+  }
+  std::printf("RESULT basename=%s maximum_depth=%d configured_max_ref_count=%d referenced_nodes=%" PRId64
+              " truncated_nodes=%" PRId64 " depth_counts=0:%" PRId64 ",1:%" PRId64 ",2:%" PRId64 ",3:%" PRId64 "\n",
+              bn.c_str(), r.maximum_depth, r.configured_max_ref_count, r.referenced_nodes, r.truncated_nodes,
+              r.depth_counts[0], r.depth_counts[1], r.depth_counts[2], r.depth_counts[3]);
+  return 0;
+}
+
 int main(int argc, char** argv) {
+  if (argc >= 2 && !std::strcmp(argv[1], "reference_depths")) return reference_depths_main(argc, argv);
   const Options o = parse(argc, argv);
   tga_dataset_cfg cfg = o.cfg;
   const std::string storage = o.storage.empty() ? o.dataset : o.storage;

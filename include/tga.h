@@ -378,6 +378,18 @@ int tga_encode_raw(const char* raw_path, const char* dir, const char* base, int6
 int tga_write_reversed(const int64_t* offsets, const int32_t* dst, const int64_t* ts, int64_t n, int64_t pivot,
                        const char* dir, const char* base, tga_gen_summary* out);
 
+/* Realised backward-reference chain depth (cpu_java ReferenceDepthScanner.java:18-110), host only:
+ * reads <dir>/<base>.graph, .offsets and .properties; a list that copies from the list `ref`
+ * positions back has depth one more than that list, other lists depth 0.  depth_out (n entries,
+ * may be NULL) gets every list's depth; depth_counts[d] counts lists of depth d < 16, deeper ones
+ * are truncated_nodes, as the reference counts them. */
+typedef struct {
+  int64_t nodes, referenced_nodes, truncated_nodes;
+  int32_t maximum_depth, configured_max_ref_count;
+  int64_t depth_counts[16];
+} tga_ref_depths;
+int tga_reference_depths(const char* dir, const char* base, tga_ref_depths* out, int32_t* depth_out);
+
 /* Producer of the four GPU index files (graph_{lower,upper}_bits.bin, timestamp_{lower,upper}_bits.bin,
  * the layout read by sh/bfs.cu:543-565,1785-1789, for which the reference ships no producer) for a
  * directory the Java encoder wrote: graph offsets from <base>.offsets (gamma deltas,
