@@ -57,12 +57,15 @@ def _load() -> C.CDLL:
 
 
 _lib = None
+_max_threads = 1
 
 
 def lib() -> C.CDLL:
-    global _lib
+    global _lib, _max_threads
     if _lib is None:
         _lib = _load()
+        # Read before any call sets a thread count: OpenMP keeps the last one set.
+        _max_threads = _lib.orc_max_threads()
     return _lib
 
 
@@ -189,4 +192,6 @@ def ef_values(lower: bytes, upper: bytes, l: int, count: int) -> np.ndarray:
 
 
 def max_threads() -> int:
-    return lib().orc_max_threads()
+    """Threads the oracle's parallel passes use by default (OpenMP's count when the library loaded)."""
+    lib()
+    return _max_threads
