@@ -80,7 +80,7 @@ def build(verbose: bool = False, force: bool = False) -> Path:
     if force or _stale(LIB, objs):
         tmp = LIB.with_suffix(".so.tmp")
         _run([nvcc, *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lcudart_static", "-lrt", "-lpthread",
-              "-ldl"], verbose)
+              "-ldl", "-lz"], verbose)
         os.replace(tmp, LIB)
     BIN.mkdir(exist_ok=True)
     for name, src in TOOLS.items():

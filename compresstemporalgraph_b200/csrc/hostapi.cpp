@@ -11,6 +11,8 @@
 #include "format.hpp"
 #include "gen.hpp"
 
+#include <zlib.h>
+
 namespace tga {
 int fail(int code, const std::string& msg);
 }
@@ -65,10 +67,26 @@ int tga_generate(const tga_gen_params* p, const char* dir, const char* base, con
   return TGA_OK;
 }
 
+// Whole file, gunzipped when its name ends in ".gz" (the reference keeps its raw inputs as
+// data/raw/<DS>.raw.txt.gz).  False when it cannot be opened or is not valid gzip.
+static bool read_raw_input(const std::string& path, std::vector<uint8_t>& out) {
+  if (path.size() < 3 || path.compare(path.size() - 3, 3, ".gz") != 0) return read_file(path, out);
+  gzFile f = gzopen(path.c_str(), "rb");
+  if (!f) return false;
+  out.clear();
+  std::vector<uint8_t> buf(1 << 20);
+  int got;
+  while ((got = gzread(f, buf.data(), (unsigned)buf.size())) > 0) out.insert(out.end(), buf.begin(), buf.begin() + got);
+  int err = Z_OK;
+  gzerror(f, &err);
+  gzclose(f);
+  return got == 0 && (err == Z_OK || err == Z_STREAM_END);
+}
+
 int tga_encode_raw(const char* raw_path, const char* dir, const char* base, int64_t max_label, tga_gen_summary* out) {
   if (!raw_path || !dir || !base) return fail(TGA_E_ARG, "null argument");
   std::vector<uint8_t> raw;
-  if (!read_file(raw_path, raw)) return fail(TGA_E_IO, std::string("Cannot open required file: ") + raw_path);
+  if (!read_raw_input(raw_path, raw)) return fail(TGA_E_IO, std::string("Cannot open required file: ") + raw_path);
   try {
     const RawGraph g = parse_raw_text(std::string(raw.begin(), raw.end()));
     const WrittenDataset w = encode_and_write(g, dir, base, max_label, EncoderParams{});

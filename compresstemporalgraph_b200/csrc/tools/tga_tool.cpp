@@ -108,6 +108,7 @@ struct Options {
 void usage(FILE* f, const char* prog) {
   std::fprintf(f,
                "usage: %s [options]            (or: tga_tool <algorithm> [options])\n"
+               "       tga_tool prepare <raw-input[.gz]> <output-basename> [max-label]\n"
                "       tga_tool reference_depths <graph-basename>   (ReferenceDepthScanner's report)\n"
                "algorithms: bfs connected_components degree_centrality graph_coloring hits\n"
                "            neighbor_access pagerank\n"
@@ -523,8 +524,38 @@ int reference_depths_main(int argc, char** argv) {
   return 0;
 }
 
+// `tga_tool prepare <raw-input> <output-basename> [max-label]`: the dataset preparation of the
+// reference (BaselineRunner.java:243-259 and its --prepare-only line, 657-666: a raw edge list,
+// gzipped or not, through EvolvingMultiGraph.store), plus the four GPU index files (host only).
+int prepare_main(int argc, char** argv) {
+  if (argc < 4 || argc > 5 || argv[2][0] == '-') {
+    std::fprintf(stderr, "Usage: tga_tool prepare <raw-input> <output-basename> [max-label]\n");
+    return 2;
+  }
+  int64_t max_label = -1;
+  if (argc == 5 && (!parse_i64(argv[4], &max_label) || max_label < 0)) {
+    std::fprintf(stderr, "tga_tool prepare: bad max-label: %s\n", argv[4]);
+    return 2;
+  }
+  const std::string bn = argv[3];
+  const size_t slash = bn.find_last_of('/');
+  const std::string dir = slash == std::string::npos ? "." : bn.substr(0, slash);
+  const std::string base = slash == std::string::npos ? bn : bn.substr(slash + 1);
+  tga_gen_summary s{};
+  const int rc = tga_encode_raw(argv[2], dir.c_str(), base.c_str(), max_label, &s);
+  if (rc) {
+    std::fprintf(stderr, "%s\n", tga_last_error());
+    return rc == TGA_E_ARG ? 2 : 1;
+  }
+  std::printf("PREPARED basename=%s nodes=%" PRId64 " arcs=%" PRId64 " graph_bytes=%" PRIu64 " timestamp_bytes=%" PRIu64
+              " index_bytes=%" PRIu64 "\n",
+              bn.c_str(), s.n, s.m, s.graph_bytes, s.timestamp_bytes, s.index_bytes);
+  return 0;
+}
+
 int main(int argc, char** argv) {
   if (argc >= 2 && !std::strcmp(argv[1], "reference_depths")) return reference_depths_main(argc, argv);
+  if (argc >= 2 && !std::strcmp(argv[1], "prepare")) return prepare_main(argc, argv);
   const Options o = parse(argc, argv);
   tga_dataset_cfg cfg = o.cfg;
   const std::string storage = o.storage.empty() ? o.dataset : o.storage;

@@ -369,6 +369,7 @@ int tga_generate(const tga_gen_params* p, const char* dir, const char* base, con
 
 /* Compresses a 4-column raw text edge list ("src dst w ts", sources sorted) the way
  * EvolvingMultiGraph.store does (EvolvingMultiGraph.java:147-275), plus the 4 EF index files.
+ * A path ending in ".gz" is read through gzip, as the reference's data/raw/<DS>.raw.txt.gz.
  * max_label < 0 -> n-1. */
 int tga_encode_raw(const char* raw_path, const char* dir, const char* base, int64_t max_label, tga_gen_summary* out);
 

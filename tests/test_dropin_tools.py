@@ -303,3 +303,47 @@ def test_pagerank_tool_and_rank_summary(small):
     pairs = [p.split(":") for p in top.split(",")]
     assert [int(i) for i, _ in pairs] == order.tolist()
     np.testing.assert_allclose([float(v) for _, v in pairs], got[order], rtol=1e-9)
+
+
+# ---- dataset preparation ------------------------------------------------------------------------
+
+def test_prepare_plain_and_gzipped_inputs_give_the_same_files(datasets, tmp_path):
+    import gzip
+
+    raw = Path(datasets["chains"]["raw"])
+    gz = tmp_path / "chains.raw.txt.gz"
+    gz.write_bytes(gzip.compress(raw.read_bytes()))
+    outs = {}
+    for name, src in (("plain", raw), ("gz", gz)):
+        bn = tmp_path / name / "chains"
+        r = run("tga_tool", "prepare", src, bn)
+        assert r.returncode == 0, r.stderr
+        assert r.stdout.startswith(f"PREPARED basename={bn} nodes={datasets['chains']['summary']['n']} ")
+        outs[name] = {f.name: f.read_bytes() for f in (tmp_path / name).iterdir()}
+    assert outs["plain"] == outs["gz"]
+    # The generator's own files for the same edges.
+    gen = {f.name: f.read_bytes() for f in Path(datasets["chains"]["dir"]).iterdir() if f.name.startswith("chains.")}
+    for k in ("chains.graph", "chains.timestamps", "chains.offsets"):
+        assert outs["gz"][k] == gen[k], k
+    for k in ("graph_lower_bits.bin", "graph_upper_bits.bin", "timestamp_lower_bits.bin", "timestamp_upper_bits.bin"):
+        assert k in outs["gz"]
+
+
+def test_prepare_errors(tmp_path, datasets):
+    import gzip
+
+    # A truncated gzip stream is refused; a file named .gz that is not gzip at all is read as text
+    # (zlib's transparent mode) and fails as text.
+    whole = gzip.compress(Path(datasets["sparse"]["raw"]).read_bytes())
+    cut = tmp_path / "cut.txt.gz"
+    cut.write_bytes(whole[: len(whole) // 2])
+    r = run("tga_tool", "prepare", cut, tmp_path / "o" / "x")
+    assert r.returncode == 1 and "Cannot open required file" in r.stderr
+    bad = tmp_path / "bad.txt.gz"
+    bad.write_bytes(b"not gzip at all")
+    r = run("tga_tool", "prepare", bad, tmp_path / "o" / "x")
+    assert r.returncode == 1 and "invalid number at line 1" in r.stderr
+    r = run("tga_tool", "prepare", tmp_path / "missing.txt", tmp_path / "o" / "x")
+    assert r.returncode == 1
+    r = run("tga_tool", "prepare", tmp_path / "missing.txt")
+    assert r.returncode == 2 and "Usage: tga_tool prepare" in r.stderr
