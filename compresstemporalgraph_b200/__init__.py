@@ -182,6 +182,20 @@ def _ptr(a: np.ndarray | None):
     return None if a is None else C.c_void_p(a.ctypes.data)
 
 
+# The per-dataset macros of gpu_cuda/<DS>/dataset_config.cuh; other fields keep the defaults of
+# gpu_cuda/shared/dataset_config_base.cuh.
+PRESETS = {
+    "Comm": dict(max_label=9999, max_vertex=10000, min_timestamp=0),
+    "MyD": dict(max_label=999967, max_vertex=1000001, min_timestamp=0),
+    "Flickr": dict(max_label=2585568, max_vertex=2585570, min_timestamp=0),
+    "Wiki": dict(max_label=42640545, max_vertex=42640546, min_timestamp=979675713, min_graph_vertex=1,
+                 multiple_initial_value=0, pagerank_iterations=100, hits_iterations=100),
+    "Yahoo": dict(max_label=102867214, max_vertex=102867263, min_timestamp=1206214540),
+    "Yahoo-sub": dict(max_label=102867214, max_vertex=102867263, min_timestamp=1206214540, storage_name="Yahoo",
+                      active_vertex_begin=2000, bfs_start_vertex=2001, connected_components_vertex_begin=2000),
+}
+
+
 @dataclass
 class DatasetConfig:
     """Runtime form of gpu_cuda/shared/dataset_config_base.cuh (same names and defaults)."""
@@ -199,6 +213,16 @@ class DatasetConfig:
     pagerank_iterations: int = 10
     hits_iterations: int = 10
     _keep: list = field(default_factory=list, repr=False)
+
+    @classmethod
+    def preset(cls, name: str, **overrides) -> "DatasetConfig":
+        """One of the six datasets the reference ships (gpu_cuda/<DS>/dataset_config.cuh), with
+        keyword overrides: Comm, MyD, Flickr, Wiki, Yahoo, Yahoo-sub."""
+        if name not in PRESETS:
+            raise KeyError(f"no preset {name!r}; presets: {', '.join(PRESETS)}")
+        kw = dict(PRESETS[name])
+        kw.update(overrides)
+        return cls(name=name, **kw)
 
     def to_c(self) -> _Cfg:
         c = _Cfg()

@@ -129,6 +129,19 @@ def test_presets_equal_the_reference_dataset_configs(ds):
         assert want[k] == v, (ds, k)
 
 
+@pytest.mark.parametrize("ds", list(tga.PRESETS))
+def test_python_presets_equal_the_tool_presets(ds):
+    got = json.loads(run("bfs", "--dataset", ds, "--show-config").stdout)
+    c = tga.DatasetConfig.preset(ds).to_c()
+    assert got["DATASET_STORAGE_NAME"] == c.storage_name.decode() and got["MAX_LABEL"] == c.max_label
+    assert got["MAX_Vertex"] == c.max_vertex and got["minTimestamp"] == c.min_timestamp
+    assert got["MIN_GRAPH_VERTEX"] == c.min_graph_vertex and got["ACTIVE_VERTEX_BEGIN"] == c.active_vertex_begin
+    assert got["BFS_START_VERTEX"] == c.bfs_start_vertex and got["CONNECTED_COMPONENTS_VERTEX_BEGIN"] == c.cc_vertex_begin
+    assert got["MULTIPLE_INITIAL_VALUE"] == c.multiple_initial_value
+    assert got["PAGERANK_ITERATIONS"] == c.pr_iters and got["HITS_ITERATIONS"] == c.hits_iters
+    assert tga.DatasetConfig.preset(ds, pagerank_iterations=3).pagerank_iterations == 3
+
+
 def test_show_config_for_other_datasets():
     r = run("hits", "--dataset", "x", "--max-label", 5, "--hits-iters", 3, "--show-config")
     got = json.loads(r.stdout)
