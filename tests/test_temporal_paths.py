@@ -213,3 +213,16 @@ def test_latest_departure_by_reversal_equals_definition(tmp_path, seed):
             got = latest_by_reversal(orev, n, n - 1, n, 0, pivot, target, lo, hi)
             want = latest_by_definition(out, n, n, pivot, target, lo, hi)
             assert np.array_equal(got, want), (target, lo, hi)
+
+
+def test_reversal_edge_cases(tmp_path):
+    # No edges at all: an empty copy that still opens in the oracle.
+    tga.write_reversed(np.array([0, 0, 0]), np.array([], np.int32), np.array([], np.int64), 0, tmp_path, "e")
+    off, dst, ts = pyoracle.Oracle(tmp_path, "e", 2).csr()
+    assert off.tolist() == [0, 0, 0] and len(dst) == 0 and len(ts) == 0
+    summary, depth = tga.reference_depths(tmp_path, "e")
+    assert summary["depth_counts"][0] == 2 and depth.tolist() == [0, 0]
+    # One edge 0 -> 1 at 5, reflected about pivot 5: 1 -> 0 at 0.
+    tga.write_reversed(np.array([0, 1, 1]), np.array([1], np.int32), np.array([5], np.int64), 5, tmp_path, "o")
+    off, dst, ts = pyoracle.Oracle(tmp_path, "o", 2).csr()
+    assert off.tolist() == [0, 0, 1] and dst.tolist() == [0] and ts.tolist() == [0]
