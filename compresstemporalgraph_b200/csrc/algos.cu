@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "sweep.cuh"
+#include "trace.cuh"
 
 namespace tga {
 
@@ -591,6 +592,7 @@ using namespace tga;
 extern "C" {
 
 int tga_neighbor_access(tga_graph* gp, uint8_t* small_out, uint64_t* checksum_out, int32_t* degree_out) {
+  TGA_TRACE("tga_neighbor_access");
   if (!gp) return fail(TGA_E_ARG, "null graph");
   GraphHandle& h = *gp;
   const int32_t nv = h.view.max_vertex;
@@ -619,6 +621,7 @@ int tga_neighbor_access(tga_graph* gp, uint8_t* small_out, uint64_t* checksum_ou
 }
 
 int tga_neighbors(tga_graph* gp, int32_t v, int32_t* dst, int64_t* ts, int32_t cap, int32_t* count) {
+  TGA_TRACE("tga_neighbors");
   if (!gp || !count) return fail(TGA_E_ARG, "null argument");
   GraphHandle& h = *gp;
   if (v < 0 || v >= h.view.n) return fail(TGA_E_ARG, "vertex out of range");
@@ -642,6 +645,7 @@ int tga_neighbors(tga_graph* gp, int32_t v, int32_t* dst, int64_t* ts, int32_t c
 
 int tga_is_neighbor(tga_graph* gp, int32_t nq, const int32_t* node, const int32_t* neighbor, const int64_t* t_from,
                     const int64_t* t_to, uint8_t* out) {
+  TGA_TRACE("tga_is_neighbor");
   if (!gp || nq < 0 || (nq && (!node || !neighbor || !out))) return fail(TGA_E_ARG, "bad argument");
   GraphHandle& h = *gp;
   if (nq == 0) return TGA_OK;
@@ -666,6 +670,7 @@ int tga_is_neighbor(tga_graph* gp, int32_t nq, const int32_t* node, const int32_
 }
 
 int tga_decode_all(tga_graph* gp, int64_t* offsets, int32_t* dst, int64_t* ts, int64_t cap) {
+  TGA_TRACE("tga_decode_all");
   if (!gp || !offsets) return fail(TGA_E_ARG, "null argument");
   GraphHandle& h = *gp;
   const int32_t n = h.view.n;
@@ -689,6 +694,7 @@ int tga_decode_all(tga_graph* gp, int64_t* offsets, int32_t* dst, int64_t* ts, i
 }
 
 int tga_pagerank(tga_graph* gp, int32_t iters, float damping, float alpha, int64_t t_lo, int64_t t_hi, float* rank_out) {
+  TGA_TRACE("tga_pagerank");
   if (!gp) return fail(TGA_E_ARG, "null graph");
   GraphHandle& h = *gp;
   if (iters <= 0) iters = h.cfg.pr_iters;
@@ -748,6 +754,7 @@ int tga_pagerank(tga_graph* gp, int32_t iters, float damping, float alpha, int64
 }
 
 int tga_hits(tga_graph* gp, int32_t iters, int32_t mode, int64_t t_lo, int64_t t_hi, float* hub_out, float* auth_out) {
+  TGA_TRACE("tga_hits");
   if (!gp) return fail(TGA_E_ARG, "null graph");
   GraphHandle& h = *gp;
   if (iters <= 0) iters = h.cfg.hits_iters;
@@ -812,6 +819,7 @@ int tga_hits(tga_graph* gp, int32_t iters, int32_t mode, int64_t t_lo, int64_t t
 }
 
 int tga_degree(tga_graph* gp, int64_t t_start, int64_t t_end, int32_t* degree_out, int64_t* avg_out) {
+  TGA_TRACE("tga_degree");
   if (!gp) return fail(TGA_E_ARG, "null graph");
   GraphHandle& h = *gp;
   const int32_t nv = h.view.max_vertex;
@@ -861,6 +869,7 @@ static void java_random_prio(uint32_t* out, int32_t n, int64_t seed) {
 
 int tga_color(tga_graph* gp, int32_t prio_mode, const uint32_t* prio_in, int32_t flags, uint32_t* color_out,
               uint32_t* prio_out, int32_t* rounds_out) {
+  TGA_TRACE("tga_color");
   if (!gp) return fail(TGA_E_ARG, "null graph");
   GraphHandle& h = *gp;
   const int32_t nv = h.view.max_vertex;

@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "gridsync.cuh"
+#include "trace.cuh"
 
 namespace tga {
 
@@ -1534,6 +1535,7 @@ int tga_cc_job_add(tga_cc_job* j, int64_t t_lo, int64_t t_hi, int32_t* slot) {
 }
 
 int tga_cc_job_step(tga_cc_job* j, double budget_ms, uint32_t* finished) {
+  TGA_TRACE("tga_cc_job_step");
   if (!j) return fail(TGA_E_ARG, "null job");
   return cc_job_step(j, budget_ms, finished);
 }
@@ -1552,6 +1554,7 @@ int tga_cc_job_destroy(tga_cc_job* j) {
 
 int tga_cc_batch(tga_graph* g, int32_t nq, const int64_t* t_lo, const int64_t* t_hi, int32_t flags,
                  int32_t* label_out, int32_t* components_out) {
+  TGA_TRACE("tga_cc_batch");
   if (!g || nq < 0 || (nq && (!t_lo || !t_hi))) return fail(TGA_E_ARG, "bad argument");
   if (flags & ~TGA_CC_EARLY_EXIT) return fail(TGA_E_ARG, "tga_cc_batch: only TGA_CC_EARLY_EXIT applies");
   GraphHandle& h = *g;
@@ -1577,6 +1580,7 @@ int tga_cc_batch(tga_graph* g, int32_t nq, const int64_t* t_lo, const int64_t* t
 
 int tga_bfs_batch(tga_graph* g, int32_t nsrc, const int32_t* src, const int64_t* t_lo, const int64_t* t_hi,
                   int32_t* arrival_out) {
+  TGA_TRACE("tga_bfs_batch");
   if (!g || nsrc < 0 || (nsrc && (!src || !t_lo || !t_hi))) return fail(TGA_E_ARG, "bad argument");
   GraphHandle& h = *g;
   const size_t nv = (size_t)h.view.max_vertex;
@@ -1628,6 +1632,7 @@ static int pagerank_batch_all(tga_graph* g, int32_t nq, const int32_t* iters, fl
 
 int tga_pagerank_batch(tga_graph* g, int32_t nq, int32_t iters, float damping, float alpha, const int64_t* t_lo,
                        const int64_t* t_hi, float* rank_out) {
+  TGA_TRACE("tga_pagerank_batch");
   if (!g || nq < 0 || (nq && (!t_lo || !t_hi))) return fail(TGA_E_ARG, "bad argument");
   std::vector<int32_t> it((size_t)nq, iters);
   return pagerank_batch_all(g, nq, it.data(), damping, alpha, t_lo, t_hi, rank_out);
@@ -1635,6 +1640,7 @@ int tga_pagerank_batch(tga_graph* g, int32_t nq, int32_t iters, float damping, f
 
 int tga_pagerank_batch_iters(tga_graph* g, int32_t nq, const int32_t* iters, float damping, float alpha,
                              const int64_t* t_lo, const int64_t* t_hi, float* rank_out) {
+  TGA_TRACE("tga_pagerank_batch_iters");
   if (!g || nq < 0 || (nq && (!iters || !t_lo || !t_hi))) return fail(TGA_E_ARG, "bad argument");
   return pagerank_batch_all(g, nq, iters, damping, alpha, t_lo, t_hi, rank_out);
 }

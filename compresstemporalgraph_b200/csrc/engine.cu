@@ -13,6 +13,7 @@
 #include "decoder.cuh"
 #include "engine.hpp"
 #include "format.hpp"
+#include "trace.cuh"
 
 namespace tga {
 
@@ -631,6 +632,7 @@ static int open_common(const std::string& dir, const std::string& base, const tg
 }
 
 int tga_open(const char* root, const tga_dataset_cfg* cfg, tga_graph** out) {
+  TGA_TRACE("tga_open");
   if (!cfg) return fail(TGA_E_ARG, "null configuration");
   std::string r = root ? root : "";
   if (r.empty()) {
@@ -645,6 +647,7 @@ int tga_open(const char* root, const tga_dataset_cfg* cfg, tga_graph** out) {
 }
 
 int tga_open_dir(const char* dir, const char* basename, const tga_dataset_cfg* cfg, tga_graph** out) {
+  TGA_TRACE("tga_open_dir");
   if (!dir || !basename) return fail(TGA_E_ARG, "null path");
   return open_common(dir, basename, cfg, out);
 }
@@ -686,6 +689,7 @@ int tga_set_work_params(tga_graph* g, int32_t slice_edges, int32_t item_edges) {
 // total.  Slice length and item size are tried as a grid, then the dense-level divisor at the
 // best of those.
 int tga_autotune(tga_graph* g, tga_tune_result* out) {
+  TGA_TRACE("tga_autotune");
   if (!g) return fail(TGA_E_ARG, "null graph");
   GraphHandle& h = *g;
   const int64_t span = h.max_ts - h.view.min_ts;

@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "engine.hpp"
+#include "trace.cuh"
 
 using namespace tga;
 
@@ -36,6 +37,7 @@ void add_timing(tga_timing& sum, const tga_timing& t) {
 // about 256 MiB).  Host work is O(departures x max_vertex) for the minimum, on up to 32 threads.
 extern "C" int tga_fastest(tga_graph* gp, int32_t src, int64_t t_lo, int64_t t_hi, int64_t* duration_out,
                            int64_t* departure_out) {
+  TGA_TRACE("tga_fastest");
   if (!gp) return fail(TGA_E_ARG, "null graph");
   GraphHandle& h = *gp;
   const int32_t nv = h.view.max_vertex;
@@ -114,6 +116,7 @@ extern "C" int tga_fastest(tga_graph* gp, int32_t src, int64_t t_lo, int64_t t_h
 // The lists are decoded on the device (tga_decode_all) and written on the host (tga_write_reversed):
 // edge (x -> y, t) becomes (y -> x, pivot - t).
 extern "C" int tga_reverse(tga_graph* gp, int64_t pivot, const char* dir, const char* base, int64_t* pivot_out) {
+  TGA_TRACE("tga_reverse");
   if (!gp || !dir || !base) return fail(TGA_E_ARG, "null argument");
   GraphHandle& h = *gp;
   const int64_t n = h.view.n;
@@ -135,6 +138,7 @@ extern "C" int tga_reverse(tga_graph* gp, int64_t pivot, const char* dir, const 
 // so one earliest-arrival traversal from the target gives every vertex's latest departure.
 extern "C" int tga_latest_departure(tga_graph* rev, int64_t pivot, int32_t target, int64_t t_lo, int64_t t_hi,
                                     int64_t* out) {
+  TGA_TRACE("tga_latest_departure");
   if (!rev) return fail(TGA_E_ARG, "null graph");
   GraphHandle& h = *rev;
   const int32_t nv = h.view.max_vertex;

@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "gridsync.cuh"
+#include "trace.cuh"
 
 namespace tga {
 
@@ -410,6 +411,7 @@ int tga_barrier_selftest(double limit_ms, int32_t* status_out) {
 }
 
 int tga_bfs(tga_graph* gp, int32_t src, int64_t t_lo, int64_t t_hi, int32_t* arrival_out, int32_t* hops_out) {
+  TGA_TRACE("tga_bfs");
   if (!gp) return fail(TGA_E_ARG, "null graph");
   GraphHandle& h = *gp;
   if (src < 0) src = h.cfg.bfs_start_vertex;
@@ -439,6 +441,7 @@ int tga_bfs(tga_graph* gp, int32_t src, int64_t t_lo, int64_t t_hi, int32_t* arr
 }
 
 int tga_cc(tga_graph* gp, int64_t t_lo, int64_t t_hi, int32_t flags, int32_t* label_out, int32_t* components_out) {
+  TGA_TRACE("tga_cc");
   if (!gp) return fail(TGA_E_ARG, "null graph");
   GraphHandle& h = *gp;
   if (t_lo >= t_hi) return fail(TGA_E_ARG, "empty time window");
