@@ -2,6 +2,8 @@
 // is the multi-source BFS of batch.cu).
 #include <algorithm>
 #include <climits>
+#include <new>
+#include <system_error>
 #include <thread>
 #include <vector>
 
@@ -35,8 +37,8 @@ void add_timing(tga_timing& sum, const tga_timing& t) {
 // with paths following tga_bfs's edge rule.  The departures run as rows of the multi-source
 // traversal, up to 256 per launch and fewer when max_vertex is large (host rows are bounded to
 // about 256 MiB).  Host work is O(departures x max_vertex) for the minimum, on up to 32 threads.
-extern "C" int tga_fastest(tga_graph* gp, int32_t src, int64_t t_lo, int64_t t_hi, int64_t* duration_out,
-                           int64_t* departure_out) {
+static int tga_fastest_impl(tga_graph* gp, int32_t src, int64_t t_lo, int64_t t_hi, int64_t* duration_out,
+                            int64_t* departure_out) {
   TGA_TRACE("tga_fastest");
   if (!gp) return fail(TGA_E_ARG, "null graph");
   GraphHandle& h = *gp;
@@ -92,18 +94,25 @@ extern "C" int tga_fastest(tga_graph* gp, int32_t src, int64_t t_lo, int64_t t_h
     const int threads = work < (int64_t(1) << 18)
                             ? 1
                             : (int)std::min<unsigned>(32, std::max(1u, std::thread::hardware_concurrency()));
-    if (threads == 1) {
-      fold(0, nv);
-    } else {
-      std::vector<std::thread> pool;
+    // Vertices [0, covered) go to threads; whatever no thread could be started for runs here.
+    int32_t covered = 0;
+    std::vector<std::thread> pool;
+    if (threads > 1) {
       const int32_t chunk = (int32_t)((nv + threads - 1) / threads);
-      for (int t = 0; t < threads; ++t) {
-        const int32_t v0 = (int32_t)std::min<int64_t>((int64_t)t * chunk, nv);
-        const int32_t v1 = (int32_t)std::min<int64_t>((int64_t)v0 + chunk, nv);
-        if (v0 < v1) pool.emplace_back(fold, v0, v1);
+      try {
+        for (int t = 0; t < threads; ++t) {
+          const int32_t v0 = (int32_t)std::min<int64_t>((int64_t)t * chunk, nv);
+          const int32_t v1 = (int32_t)std::min<int64_t>((int64_t)v0 + chunk, nv);
+          if (v0 < v1) {
+            pool.emplace_back(fold, v0, v1);
+            covered = v1;
+          }
+        }
+      } catch (const std::system_error&) {
       }
-      for (auto& th : pool) th.join();
     }
+    for (auto& th : pool) th.join();
+    if (covered < nv) fold(covered, nv);
   }
   if (duration_out) std::copy(best.begin(), best.end(), duration_out);
   if (departure_out) std::copy(when.begin(), when.end(), departure_out);
@@ -115,7 +124,7 @@ extern "C" int tga_fastest(tga_graph* gp, int32_t src, int64_t t_lo, int64_t t_h
 // apps/temporal/LatestDeparture-Compute.C:1-149 transposes the graph and walks it from the target).
 // The lists are decoded on the device (tga_decode_all) and written on the host (tga_write_reversed):
 // edge (x -> y, t) becomes (y -> x, pivot - t).
-extern "C" int tga_reverse(tga_graph* gp, int64_t pivot, const char* dir, const char* base, int64_t* pivot_out) {
+static int tga_reverse_impl(tga_graph* gp, int64_t pivot, const char* dir, const char* base, int64_t* pivot_out) {
   TGA_TRACE("tga_reverse");
   if (!gp || !dir || !base) return fail(TGA_E_ARG, "null argument");
   GraphHandle& h = *gp;
@@ -136,8 +145,8 @@ extern "C" int tga_reverse(tga_graph* gp, int64_t pivot, const char* dir, const 
 // using edges with t in [t_lo, t_hi).  On the reversed copy a forward path v -> target leaving at d
 // is a path target -> v arriving at pivot - d, and the window maps to (pivot - t_hi, pivot - t_lo],
 // so one earliest-arrival traversal from the target gives every vertex's latest departure.
-extern "C" int tga_latest_departure(tga_graph* rev, int64_t pivot, int32_t target, int64_t t_lo, int64_t t_hi,
-                                    int64_t* out) {
+static int tga_latest_departure_impl(tga_graph* rev, int64_t pivot, int32_t target, int64_t t_lo,
+                                     int64_t t_hi, int64_t* out) {
   TGA_TRACE("tga_latest_departure");
   if (!rev) return fail(TGA_E_ARG, "null graph");
   GraphHandle& h = *rev;
@@ -156,4 +165,31 @@ extern "C" int tga_latest_departure(tga_graph* rev, int64_t pivot, int32_t targe
   if (out)
     for (int32_t v = 0; v < nv; ++v) out[v] = arr[(size_t)v] == INT32_MAX ? -1 : pivot - arr[(size_t)v];
   return TGA_OK;
+}
+
+// C entry points: host allocation failures come back as TGA_E_OOM instead of unwinding into C.
+extern "C" int tga_fastest(tga_graph* g, int32_t src, int64_t t_lo, int64_t t_hi, int64_t* duration_out,
+                           int64_t* departure_out) {
+  try {
+    return tga_fastest_impl(g, src, t_lo, t_hi, duration_out, departure_out);
+  } catch (const std::bad_alloc&) {
+    return fail(TGA_E_OOM, "host allocation failed");
+  }
+}
+
+extern "C" int tga_reverse(tga_graph* g, int64_t pivot, const char* dir, const char* base, int64_t* pivot_out) {
+  try {
+    return tga_reverse_impl(g, pivot, dir, base, pivot_out);
+  } catch (const std::bad_alloc&) {
+    return fail(TGA_E_OOM, "host allocation failed");
+  }
+}
+
+extern "C" int tga_latest_departure(tga_graph* rev, int64_t pivot, int32_t target, int64_t t_lo, int64_t t_hi,
+                                    int64_t* out) {
+  try {
+    return tga_latest_departure_impl(rev, pivot, target, t_lo, t_hi, out);
+  } catch (const std::bad_alloc&) {
+    return fail(TGA_E_OOM, "host allocation failed");
+  }
 }
