@@ -3,6 +3,7 @@
 #include <climits>
 #include <cstdlib>
 #include <cstring>
+#include <new>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -34,6 +35,89 @@ static void fill_summary(tga_gen_summary* out, int64_t n, int64_t m, int64_t max
   out->residual_arcs = s.residual_arcs;
   out->multiples_arcs = s.multiples_arcs;
   out->max_chain = s.max_chain;
+}
+
+static int write_reversed_impl(const int64_t* offsets, const int32_t* dst, const int64_t* ts, int64_t n, int64_t pivot,
+                               const char* dir, const char* base, tga_gen_summary* out) {
+  if (!offsets || !dir || !base || n < 1 || n > INT32_MAX || pivot < 0) return fail(TGA_E_ARG, "bad argument");
+  if (offsets[0] != 0) return fail(TGA_E_ARG, "offsets must start at 0");
+  for (int64_t v = 0; v < n; ++v)
+    if (offsets[v + 1] < offsets[v]) return fail(TGA_E_ARG, "offsets must not decrease");
+  const int64_t m = offsets[n];
+  if (m > 0 && (!dst || !ts)) return fail(TGA_E_ARG, "null edge arrays");
+  // Counting sort by the new source (the old successor); old sources ascend, so every new list comes
+  // out ordered by successor, and a stable sort by reversed time orders each run of repeats.
+  RawGraph r;
+  r.n = n;
+  r.src_begin.assign((size_t)n + 1, 0);
+  for (int64_t e = 0; e < m; ++e) {
+    if (dst[e] < 0 || dst[e] >= n) return fail(TGA_E_ARG, "successor out of range");
+    if (ts[e] < 0 || ts[e] > pivot) return fail(TGA_E_ARG, "timestamp outside [0, pivot]");
+    ++r.src_begin[(size_t)dst[e] + 1];
+  }
+  for (int64_t v = 0; v < n; ++v) r.src_begin[(size_t)v + 1] += r.src_begin[(size_t)v];
+  r.dst.resize((size_t)m);
+  r.ts.resize((size_t)m);
+  std::vector<int64_t> fill(r.src_begin.begin(), r.src_begin.end() - 1);
+  r.min_ts = m ? INT64_MAX : 0;
+  for (int64_t x = 0; x < n; ++x)
+    for (int64_t e = offsets[x]; e < offsets[x + 1]; ++e) {
+      const int64_t at = fill[(size_t)dst[e]]++;
+      r.dst[(size_t)at] = (int32_t)x;
+      r.ts[(size_t)at] = pivot - ts[e];
+      r.min_ts = std::min(r.min_ts, pivot - ts[e]);
+    }
+  for (int64_t y = 0; y < n; ++y) {
+    int64_t a = r.src_begin[(size_t)y];
+    const int64_t end = r.src_begin[(size_t)y + 1];
+    while (a < end) {
+      int64_t b = a + 1;
+      while (b < end && r.dst[(size_t)b] == r.dst[(size_t)a]) ++b;
+      std::sort(r.ts.begin() + a, r.ts.begin() + b);
+      a = b;
+    }
+  }
+  try {
+    const WrittenDataset w = encode_and_write(r, dir, base, n - 1, EncoderParams{});
+    int64_t maxdeg = 0;
+    for (int64_t v = 0; v < n; ++v) maxdeg = std::max<int64_t>(maxdeg, r.src_begin[(size_t)v + 1] - r.src_begin[(size_t)v]);
+    fill_summary(out, w.n, w.m, maxdeg, w.graph_bytes, w.ts_bytes, w.index_bytes, w.stats);
+  } catch (const std::exception& e) {
+    return fail(TGA_E_FORMAT, e.what());
+  }
+  return TGA_OK;
+}
+
+static int reference_depths_impl(const char* dir, const char* base, tga_ref_depths* out, int32_t* depth_out) {
+  if (!dir || !base || !out) return fail(TGA_E_ARG, "null argument");
+  const std::string bp = std::string(dir) + "/" + base;
+  std::vector<uint8_t> graph, offsets;
+  if (!read_file(bp + ".graph", graph)) return fail(TGA_E_IO, "Cannot open required file: " + bp + ".graph");
+  if (!read_file(bp + ".offsets", offsets)) return fail(TGA_E_IO, "Cannot open required file: " + bp + ".offsets");
+  const auto pr = read_properties(bp + ".properties");
+  auto prop = [&](const char* k, int64_t dflt) {
+    const auto it = pr.find(k);
+    return it == pr.end() ? dflt : (int64_t)std::atoll(it->second.c_str());
+  };
+  const int64_t n = prop("nodes", -1);
+  if (n <= 0) return fail(TGA_E_FORMAT, "the nodes property of " + bp + ".properties is needed");
+  std::memset(out, 0, sizeof *out);
+  try {
+    const std::vector<int32_t> depth = reference_depths(graph, offsets, n, (int)prop("windowsize", 7));
+    out->nodes = n;
+    out->configured_max_ref_count = (int32_t)prop("maxrefcount", 3);
+    for (int64_t v = 0; v < n; ++v) {
+      const int32_t d = depth[(size_t)v];
+      out->referenced_nodes += d > 0;
+      out->maximum_depth = std::max(out->maximum_depth, d);
+      if (d < 16) ++out->depth_counts[d];
+      else ++out->truncated_nodes;
+    }
+    if (depth_out) std::copy(depth.begin(), depth.end(), depth_out);
+  } catch (const std::exception& e) {
+    return fail(TGA_E_FORMAT, e.what());
+  }
+  return TGA_OK;
 }
 
 extern "C" {
@@ -123,88 +207,7 @@ int tga_build_index(const char* dir, const char* base, int64_t max_label) {
   return TGA_OK;
 }
 
-int tga_write_reversed(const int64_t* offsets, const int32_t* dst, const int64_t* ts, int64_t n, int64_t pivot,
-                       const char* dir, const char* base, tga_gen_summary* out) {
-  if (!offsets || !dir || !base || n < 1 || n > INT32_MAX || pivot < 0) return fail(TGA_E_ARG, "bad argument");
-  if (offsets[0] != 0) return fail(TGA_E_ARG, "offsets must start at 0");
-  for (int64_t v = 0; v < n; ++v)
-    if (offsets[v + 1] < offsets[v]) return fail(TGA_E_ARG, "offsets must not decrease");
-  const int64_t m = offsets[n];
-  if (m > 0 && (!dst || !ts)) return fail(TGA_E_ARG, "null edge arrays");
-  // Counting sort by the new source (the old successor); old sources ascend, so every new list comes
-  // out ordered by successor, and a stable sort by reversed time orders each run of repeats.
-  RawGraph r;
-  r.n = n;
-  r.src_begin.assign((size_t)n + 1, 0);
-  for (int64_t e = 0; e < m; ++e) {
-    if (dst[e] < 0 || dst[e] >= n) return fail(TGA_E_ARG, "successor out of range");
-    if (ts[e] < 0 || ts[e] > pivot) return fail(TGA_E_ARG, "timestamp outside [0, pivot]");
-    ++r.src_begin[(size_t)dst[e] + 1];
-  }
-  for (int64_t v = 0; v < n; ++v) r.src_begin[(size_t)v + 1] += r.src_begin[(size_t)v];
-  r.dst.resize((size_t)m);
-  r.ts.resize((size_t)m);
-  std::vector<int64_t> fill(r.src_begin.begin(), r.src_begin.end() - 1);
-  r.min_ts = m ? INT64_MAX : 0;
-  for (int64_t x = 0; x < n; ++x)
-    for (int64_t e = offsets[x]; e < offsets[x + 1]; ++e) {
-      const int64_t at = fill[(size_t)dst[e]]++;
-      r.dst[(size_t)at] = (int32_t)x;
-      r.ts[(size_t)at] = pivot - ts[e];
-      r.min_ts = std::min(r.min_ts, pivot - ts[e]);
-    }
-  for (int64_t y = 0; y < n; ++y) {
-    int64_t a = r.src_begin[(size_t)y];
-    const int64_t end = r.src_begin[(size_t)y + 1];
-    while (a < end) {
-      int64_t b = a + 1;
-      while (b < end && r.dst[(size_t)b] == r.dst[(size_t)a]) ++b;
-      std::sort(r.ts.begin() + a, r.ts.begin() + b);
-      a = b;
-    }
-  }
-  try {
-    const WrittenDataset w = encode_and_write(r, dir, base, n - 1, EncoderParams{});
-    int64_t maxdeg = 0;
-    for (int64_t v = 0; v < n; ++v) maxdeg = std::max<int64_t>(maxdeg, r.src_begin[(size_t)v + 1] - r.src_begin[(size_t)v]);
-    fill_summary(out, w.n, w.m, maxdeg, w.graph_bytes, w.ts_bytes, w.index_bytes, w.stats);
-  } catch (const std::exception& e) {
-    return fail(TGA_E_FORMAT, e.what());
-  }
-  return TGA_OK;
-}
 
-int tga_reference_depths(const char* dir, const char* base, tga_ref_depths* out, int32_t* depth_out) {
-  if (!dir || !base || !out) return fail(TGA_E_ARG, "null argument");
-  const std::string bp = std::string(dir) + "/" + base;
-  std::vector<uint8_t> graph, offsets;
-  if (!read_file(bp + ".graph", graph)) return fail(TGA_E_IO, "Cannot open required file: " + bp + ".graph");
-  if (!read_file(bp + ".offsets", offsets)) return fail(TGA_E_IO, "Cannot open required file: " + bp + ".offsets");
-  const auto pr = read_properties(bp + ".properties");
-  auto prop = [&](const char* k, int64_t dflt) {
-    const auto it = pr.find(k);
-    return it == pr.end() ? dflt : (int64_t)std::atoll(it->second.c_str());
-  };
-  const int64_t n = prop("nodes", -1);
-  if (n <= 0) return fail(TGA_E_FORMAT, "the nodes property of " + bp + ".properties is needed");
-  std::memset(out, 0, sizeof *out);
-  try {
-    const std::vector<int32_t> depth = reference_depths(graph, offsets, n, (int)prop("windowsize", 7));
-    out->nodes = n;
-    out->configured_max_ref_count = (int32_t)prop("maxrefcount", 3);
-    for (int64_t v = 0; v < n; ++v) {
-      const int32_t d = depth[(size_t)v];
-      out->referenced_nodes += d > 0;
-      out->maximum_depth = std::max(out->maximum_depth, d);
-      if (d < 16) ++out->depth_counts[d];
-      else ++out->truncated_nodes;
-    }
-    if (depth_out) std::copy(depth.begin(), depth.end(), depth_out);
-  } catch (const std::exception& e) {
-    return fail(TGA_E_FORMAT, e.what());
-  }
-  return TGA_OK;
-}
 
 int tga_decode_table(int32_t kind, int32_t* out) {
   if (!out || (kind != 0 && kind != 3)) return fail(TGA_E_ARG, "kind must be 0 (gamma) or 3 (zeta_3)");
@@ -250,6 +253,23 @@ int tga_ef_encode(const uint64_t* values, int64_t n, int32_t l, uint8_t* lower, 
   std::memcpy(lower, ef.lower.data(), ef.lower.size());
   std::memcpy(upper, ef.upper.data(), ef.upper.size());
   return TGA_OK;
+}
+
+int tga_write_reversed(const int64_t* offsets, const int32_t* dst, const int64_t* ts, int64_t n, int64_t pivot,
+                       const char* dir, const char* base, tga_gen_summary* out) {
+  try {
+    return write_reversed_impl(offsets, dst, ts, n, pivot, dir, base, out);
+  } catch (const std::bad_alloc&) {
+    return fail(TGA_E_OOM, "host allocation failed");
+  }
+}
+
+int tga_reference_depths(const char* dir, const char* base, tga_ref_depths* out, int32_t* depth_out) {
+  try {
+    return reference_depths_impl(dir, base, out, depth_out);
+  } catch (const std::bad_alloc&) {
+    return fail(TGA_E_OOM, "host allocation failed");
+  }
 }
 
 }  // extern "C"
