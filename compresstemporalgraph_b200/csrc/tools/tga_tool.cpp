@@ -255,6 +255,7 @@ Options parse(int argc, char** argv) {
     else bad_args(o, "unknown option: " + a);
   }
   if (o.dir.empty() != o.base.empty()) bad_args(o, "--dir and --base go together");
+  if (!o.dir.empty() && !o.root.empty()) bad_args(o, "--root and --dir exclude each other");
   if (o.dataset.empty() && o.base.empty()) bad_args(o, "--dataset (or --dir with --base) is required");
   if (o.dataset.empty()) o.dataset = o.base;
   for (const auto& p : kPresets)

@@ -83,6 +83,7 @@ def test_dir_and_base_missing_file(tmp_path):
     (["--dataset", "Comm", "--src", "-4"], "bad value for --src"),
     (["--dataset", "Comm", "--max-label", "10", "--max-vertex", "10"], "--max-vertex must exceed --max-label"),
     (["--dir", "/tmp"], "--dir and --base go together"),
+    (["--dir", "/tmp", "--base", "g", "--root", "/tmp", "--max-label", "9"], "--root and --dir exclude each other"),
     (["--dataset", "Comm", "--repeat"], "missing value for --repeat"),
 ])
 def test_bad_arguments_exit_2(args, msg):
