@@ -49,3 +49,11 @@ def test_cfg_defaults_match_reference_macros():
     # shared/dataset_config_base.cuh:11-37 defaults
     assert c.active_vertex_begin == 0 and c.min_graph_vertex == 0 and c.bfs_start_vertex == 1
     assert c.cc_vertex_begin == 1 and c.multiple_initial_value == -1 and c.pr_iters == 10 and c.hits_iters == 10
+
+
+def test_python_mirror_declares_every_entry_point():
+    """Every function of include/tga.h has a ctypes signature in the Python mirror."""
+    src = (ROOT / "compresstemporalgraph_b200" / "__init__.py").read_text()
+    mirrored = set(re.findall(r'"(tga_[a-z0-9_]+)":\s*\(', src))
+    missing = [n for n in declared() if n not in mirrored]
+    assert not missing, missing
