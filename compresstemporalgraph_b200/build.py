@@ -10,6 +10,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
@@ -65,18 +66,23 @@ def build(verbose: bool = False, force: bool = False) -> Path:
     OUT.mkdir(exist_ok=True)
     headers = _headers()
     objs: list[Path] = []
+    steps: list[list[str]] = []
     for src in CU_SOURCES:
         s = CSRC / src
         o = OUT / (s.stem + ".cu.o")
         if force or _stale(o, [s] + headers):
-            _run([nvcc, *ARCH, *NVCC_FLAGS, f"-I{INCLUDE}", "-c", str(s), "-o", str(o)], verbose)
+            steps.append([nvcc, *ARCH, *NVCC_FLAGS, f"-I{INCLUDE}", "-c", str(s), "-o", str(o)])
         objs.append(o)
     for src in CPP_SOURCES:
         s = CSRC / src
         o = OUT / (s.stem + ".cpp.o")
         if force or _stale(o, [s] + headers):
-            _run(["g++", *CXX_FLAGS, f"-I{INCLUDE}", "-c", str(s), "-o", str(o)], verbose)
+            steps.append(["g++", *CXX_FLAGS, f"-I{INCLUDE}", "-c", str(s), "-o", str(o)])
         objs.append(o)
+    # The translation units are independent: compile them side by side.
+    with ThreadPoolExecutor(max_workers=max(1, min(len(steps), os.cpu_count() or 1))) as pool:
+        for f in [pool.submit(_run, cmd, verbose) for cmd in steps]:
+            f.result()
     if force or _stale(LIB, objs):
         tmp = LIB.with_suffix(".so.tmp")
         _run([nvcc, *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lcudart_static", "-lrt", "-lpthread",

@@ -942,6 +942,7 @@ int tga_color(tga_graph* gp, int32_t prio_mode, const uint32_t* prio_in, int32_t
 // timers).  The scratch is shared by every handle on a device, so overlapping calls race.
 int tga_pagerank_noalloc(tga_graph* gp, int32_t iters, float damping, float alpha, int64_t t_lo, int64_t t_hi,
                          float* rank_out_dev) {
+  TGA_TRACE("tga_pagerank_noalloc");
   if (!gp) return fail(TGA_E_ARG, "null graph");
   GraphHandle& h = *gp;
   if (iters <= 0) iters = h.cfg.pr_iters;
@@ -956,7 +957,9 @@ int tga_pagerank_noalloc(tga_graph* gp, int32_t iters, float damping, float alph
                                std::to_string(kPrNoAllocMaxIters) + "; use tga_pagerank");
   cudaPointerAttributes pa{};
   TGA_CUDA_TRY(cudaPointerGetAttributes(&pa, rank_out_dev));
-  if ((pa.type != cudaMemoryTypeDevice && pa.type != cudaMemoryTypeManaged) || pa.device != h.device)
+  // Plain device memory only: for managed memory pa.device names the allocating device, not where
+  // the pages are.
+  if (pa.type != cudaMemoryTypeDevice || pa.device != h.device)
     return fail(TGA_E_ARG, "tga_pagerank_noalloc: rank_out_dev must be device memory of the graph's device");
   unsigned char* s = nullptr;
   TGA_TRY(pr_noalloc_scratch(h.device, &s));

@@ -2,7 +2,13 @@
 // needs no cudaMalloc.  It sits in its own translation unit (its own CUDA module): under the
 // runtime's default lazy module loading the ~20 MiB are reserved on a device only once the
 // no-allocation entry point has looked the array up there, so the other entry points do not
-// carry it.
+// carry it.  Under eager module loading (CUDA_MODULE_LOADING=EAGER) every module is loaded when
+// the context is created, so the array is reserved then, for every user of the library.
+//
+// The address looked up per device is cached for the life of the process.  It belongs to the
+// device's primary context: after cudaDeviceReset (or anything else that destroys and recreates
+// the primary context) the module is loaded again at a new address, so the cache is checked on
+// every call and refreshed when the runtime no longer knows the cached pointer.
 #include <mutex>
 #include <string>
 
@@ -18,6 +24,15 @@ int pr_noalloc_scratch(int device, unsigned char** out) {
   static unsigned char* addr[kMaxDevices] = {};
   if (device < 0 || device >= kMaxDevices) return fail(TGA_E_ARG, "device ordinal out of range");
   std::lock_guard<std::mutex> lock(mu);
+  if (addr[device]) {
+    // A pointer of a destroyed context is unknown to the runtime (or no longer device memory).
+    cudaPointerAttributes pa{};
+    const cudaError_t e = cudaPointerGetAttributes(&pa, addr[device]);
+    if (e != cudaSuccess || pa.type != cudaMemoryTypeDevice || pa.device != device) {
+      cudaGetLastError();
+      addr[device] = nullptr;
+    }
+  }
   if (!addr[device]) {
     int cur = -1;
     TGA_CUDA_TRY(cudaGetDevice(&cur));

@@ -185,6 +185,10 @@ int tga_pagerank(tga_graph* g, int32_t iters, float damping, float alpha, int64_
  *   requests fail with TGA_E_ARG and a message naming the limit (use tga_pagerank).
  *   First call on a device: looks the array up with cudaGetSymbolAddress (this loads the module
  *   holding it); make one call before capturing a stream or starting latency-critical work.
+ *   Under eager module loading (CUDA_MODULE_LOADING=EAGER) the array is reserved when the
+ *   context is created instead, whether or not this entry point is ever called.  The address
+ *   belongs to the primary context; it is looked up again after a cudaDeviceReset.
+ *   rank_out_dev must be plain device memory (cudaMalloc), not managed memory.
  *   Concurrency: the array is shared by all handles on a device; overlapping calls race, so
  *   serialise them (one call at a time per device).
  *   Timing: only total_ms, iterations and edges_decoded are recorded (no per-kernel timers). */

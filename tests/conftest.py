@@ -2,6 +2,10 @@
 
 Marker ``gpu``: the test needs a CUDA GPU (run with ``-m gpu`` on a B200); everything else runs
 on CPU only.
+
+``TGA_REFERENCE_ROOT``: a checkout of the reference project (Yukun-Cui/CompressTemporalGraph).  The
+few tests that read its files in place (decode tables, dataset configs, the ChronoGraph format
+fixture) run only when it is set; every other test uses the committed fixtures under golden/.
 """
 from __future__ import annotations
 
@@ -12,6 +16,7 @@ from pathlib import Path
 import pytest
 
 ROOT = Path(__file__).resolve().parents[1]
+REFERENCE_ROOT = Path(os.environ["TGA_REFERENCE_ROOT"]) if os.environ.get("TGA_REFERENCE_ROOT") else None
 sys.path.insert(0, str(ROOT))
 sys.path.insert(0, str(ROOT / "oracle"))
 

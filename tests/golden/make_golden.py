@@ -1,6 +1,8 @@
 """Generates tests/golden/golden.json from the reference checkout (run once in a container that
 has it; the fixture is committed so the tests never read the reference at run time).
 
+  python tests/golden/make_golden.py <reference checkout>     (or set TGA_REFERENCE_ROOT)
+
 Contents:
   * decode_tables: for gpu_cuda/decode_tables/gammaInA.txt and zetaInA.txt (65,536 entries of
     (code length << 16) | value) the sha256 of the int32 array, the number of non-zero entries and
@@ -16,7 +18,11 @@ from pathlib import Path
 
 import numpy as np
 
-REF = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+import os
+
+if len(sys.argv) < 2 and not os.environ.get("TGA_REFERENCE_ROOT"):
+    sys.exit("usage: make_golden.py <reference checkout>  (or set TGA_REFERENCE_ROOT)")
+REF = Path(sys.argv[1] if len(sys.argv) > 1 else os.environ["TGA_REFERENCE_ROOT"])
 OUT = Path(__file__).resolve().parent / "golden.json"
 
 

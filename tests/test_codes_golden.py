@@ -11,9 +11,10 @@ import pytest
 
 import compresstemporalgraph_b200 as tga
 import pyoracle
+from conftest import REFERENCE_ROOT
 
 GOLD = json.loads((Path(__file__).parent / "golden" / "golden.json").read_text())
-REF_TABLES = Path("/root/reference/gpu_cuda/decode_tables")
+REF_TABLES = (REFERENCE_ROOT / "gpu_cuda" / "decode_tables") if REFERENCE_ROOT else Path("/nonexistent")
 
 
 @pytest.mark.parametrize("kind,key", [(0, "gamma"), (3, "zeta3")])

@@ -15,7 +15,7 @@ from pathlib import Path
 import numpy as np
 import pytest
 
-from conftest import has_gpu
+from conftest import REFERENCE_ROOT, has_gpu
 
 import compresstemporalgraph_b200 as tga
 
@@ -105,7 +105,7 @@ def test_tool_name_as_first_argument():
     assert r.returncode == 0 and r.stdout.startswith("usage: tga_tool connected_components ")
 
 
-REF_GPU = Path("/root/reference/gpu_cuda")  # read when the reference tree is present
+REF_GPU = (REFERENCE_ROOT / "gpu_cuda") if REFERENCE_ROOT else Path("/nonexistent")  # read when given
 
 
 def _macros(path: Path) -> dict:

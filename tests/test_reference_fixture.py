@@ -13,8 +13,10 @@ import pytest
 
 import compresstemporalgraph_b200 as tga
 import pyoracle
+from conftest import REFERENCE_ROOT
 
-FIXTURE = Path("/root/reference/third_party/ChronoGraph/src/test/resources/cbtComm-sample.txt")
+FIXTURE = ((REFERENCE_ROOT / "third_party/ChronoGraph/src/test/resources/cbtComm-sample.txt") if REFERENCE_ROOT
+           else Path("/nonexistent"))
 INDEX = ("graph_lower_bits.bin", "graph_upper_bits.bin", "timestamp_lower_bits.bin", "timestamp_upper_bits.bin")
 
 pytestmark = pytest.mark.skipif(not FIXTURE.exists(), reason="reference tree not present")

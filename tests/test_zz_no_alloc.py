@@ -38,6 +38,14 @@ def _noalloc(g, iters, lo, hi, out_ptr) -> int:
     return tga.lib().tga_pagerank_noalloc(g.handle, iters, C.c_float(0.85), C.c_float(0.1), lo, hi, out_ptr)
 
 
+def _has_cudart() -> bool:
+    try:
+        C.CDLL("libcudart.so.12")
+        return True
+    except OSError:
+        return False
+
+
 def _err() -> str:
     return (tga.lib().tga_last_error() or b"").decode()
 
@@ -62,6 +70,22 @@ def test_noalloc_matches_pagerank_on_two_calls(data, window):
             assert np.allclose(r, ref, rtol=1e-4, atol=1e-9), call
             t = g.timing()
             assert t["iterations"] == iters and t["total_ms"] > 0
+
+
+def test_noalloc_two_handles_in_turn(data):
+    """Two handles on one device share the fixed scratch: calls made one after the other (the
+    documented safe use) each give their own window's tga_pagerank result."""
+    windows = [(0, tga.T_MAX), (1_000, 6_000)]
+    with _open(data) as g1, _open(data) as g2:
+        graphs = [g1, g2]
+        refs = [g.pagerank(15, 0.85, 0.1, lo, hi) for g, (lo, hi) in zip(graphs, windows)]
+        outs = [torch.full((g.max_vertex,), -1.0, dtype=torch.float32, device="cuda:0") for g in graphs]
+        torch.cuda.synchronize()
+        for _ in range(2):
+            for g, (lo, hi), out, ref in zip(graphs, windows, outs, refs):
+                assert _noalloc(g, 15, lo, hi, C.c_void_p(out.data_ptr())) == tga.TGA_OK, _err()
+                r = out.cpu().numpy()
+                assert float(np.abs(r.astype(np.float64) - ref).sum()) <= 1e-5
 
 
 def test_noalloc_leaves_free_memory_unchanged(data):
@@ -90,6 +114,15 @@ def test_noalloc_rejects_beyond_limits(data):
         assert _noalloc(g, 5, 0, tga.T_MAX, host.ctypes.data_as(C.c_void_p)) == tga.TGA_E_ARG
         assert "device memory" in _err()
         assert _noalloc(g, 5, 0, tga.T_MAX, None) == tga.TGA_E_ARG
+        # Managed memory is refused: its device attribute does not say where the pages are.
+        managed = C.c_void_p()
+        cudart = C.CDLL("libcudart.so.12") if _has_cudart() else None
+        if cudart is not None and cudart.cudaMallocManaged(C.byref(managed), C.c_size_t(nv * 4), 1) == 0:
+            try:
+                assert _noalloc(g, 5, 0, tga.T_MAX, managed) == tga.TGA_E_ARG
+                assert "device memory" in _err()
+            finally:
+                cudart.cudaFree(managed)
     with _open(data, max_vertex=MAX_VERTICES + 1) as g:
         out = torch.empty(MAX_VERTICES + 1, dtype=torch.float32, device="cuda:0")
         assert _noalloc(g, 5, 0, tga.T_MAX, C.c_void_p(out.data_ptr())) == tga.TGA_E_ARG
