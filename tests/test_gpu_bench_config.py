@@ -1,0 +1,124 @@
+"""Parity at the benchmarked size: the seven workloads exactly as bench.py runs them on the
+2M-vertex / 40M-edge "all7" graph, and on a hub-stress graph whose largest list holds more than a
+million edges, against the CPU oracle.
+
+Integer results (checksums, arrivals, hop counts, components, degrees, means, colours) must be
+bit-exact; PageRank and HITS (FP32 on the GPU, FP64 in the oracle) carry the tolerances stated
+next to their assertions.  The datasets are generated once per module (seeded, a few seconds
+each) and decoded by the oracle once.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import compresstemporalgraph_b200 as tga
+import pyoracle
+
+pytestmark = pytest.mark.gpu
+
+# One list of 1,195,288 edges over 3,000 vertices: slices by the tens of thousands, runs of equal
+# successors that slices cut (hundreds of repeats per successor), reference chains of depth 3 and
+# bursty timestamps (10% of the edges in 1% of the span).
+HUB1M = tga.GenParams(n=3000, m=5_000_000, deg_exponent=1.5, max_degree=4_000_000, repeat_frac=0.3, local_frac=0.7,
+                      local_radius=64, pref_frac=0.5, copy_frac=0.3, ts_kind=2, ts_span=100_000_000, seed=31)
+SHAPES = {"all7": tga.CONFIGS["all7"], "hub1m": HUB1M}
+
+
+class Big:
+    def __init__(self, directory, name, summary):
+        n = int(summary["n"])
+        self.n = n
+        self.summary = summary
+        self.cfg = tga.DatasetConfig(name=name, max_label=n - 1, max_vertex=n)
+        self.g = tga.Graph.open_dir(directory, name, self.cfg)
+        self.o = pyoracle.Oracle(directory, name, n)
+        off, _, _ = self.o.csr()
+        self.deg = np.diff(off)
+        # bench.py's BFS source: the vertex with the largest out-list.
+        self.src = int(self.deg.argmax())
+        self.ml, self.mv, self.act = self.cfg.max_label, self.cfg.max_vertex, self.cfg.active_vertex_begin
+        self.span = SHAPES[name].ts_span
+
+    def close(self):
+        self.g.close()
+        self.o.close()
+
+
+@pytest.fixture(scope="module", params=list(SHAPES))
+def big(request, tmp_path_factory):
+    name = request.param
+    d = tmp_path_factory.mktemp(f"bench_{name}")
+    s = tga.generate(SHAPES[name], d, name)
+    b = Big(d, name, s)
+    yield b
+    b.close()
+
+
+def test_shape_is_what_it_claims(big):
+    if big.cfg.name == "all7":
+        assert big.summary["m"] == 40_000_000 and big.n == 2_000_000
+    else:
+        assert big.deg.max() >= 1_000_000
+    assert big.summary["max_chain"] == 3
+
+
+def test_neighbor_access(big):
+    small, csum, deg = big.g.neighbor_access()
+    osmall, ocs = big.o.checksums(big.act, big.ml, big.mv)
+    assert np.array_equal(csum[: big.ml], ocs[: big.ml])
+    assert np.array_equal(small[: big.ml], osmall[: big.ml])
+    assert np.array_equal(deg[: big.n], big.deg.astype(deg.dtype))
+
+
+def test_bfs_from_the_largest_list(big):
+    for lo, hi in [(0, tga.T_MAX), (big.span // 4, big.span // 2)]:
+        arr, hops = big.g.bfs(big.src, lo, hi)
+        oarr, ohops = big.o.bfs(big.ml, big.mv, big.act, big.src, lo, hi)
+        assert np.array_equal(arr, oarr), (lo, hi)
+        assert np.array_equal(hops, ohops), (lo, hi)
+
+
+def test_connected_components(big):
+    lab, k = big.g.connected_components()  # full window, early exits on: as bench.py runs it
+    olab, ok = big.o.cc(big.ml, big.mv, big.act, big.cfg.connected_components_vertex_begin, 0, tga.T_MAX, True)
+    assert k == ok
+    assert np.array_equal(lab, olab)
+
+
+def test_pagerank_30_fp32_vs_fp64(big):
+    r = big.g.pagerank(30)
+    o = big.o.pagerank(big.ml, big.mv, big.act, 30)
+    # Stated tolerance, as on the small shapes: L1 distance to the FP64 oracle <= 1e-5 of the
+    # total rank mass (1.0), every entry within 1e-4 relative + 1e-9 absolute.
+    l1 = float(np.abs(r.astype(np.float64) - o).sum())
+    assert l1 <= 1e-5, l1
+    assert np.allclose(r, o, rtol=1e-4, atol=1e-9)
+
+
+def test_hits_30_fp32_vs_fp64(big):
+    hub, auth = big.g.hits(30)
+    ohub, oauth = big.o.hits(big.ml, big.mv, big.act, 30)
+    # Stated tolerance: unit-L2 vectors; every entry within 1e-5 absolute of FP64, and the L1
+    # distance within 1e-4 per 10,000 vertices (the L1 norm of a unit vector grows with sqrt(n),
+    # and FP32 rounding grows each entry's error with its magnitude).
+    l1_tol = 1e-4 * max(1.0, big.n / 10_000)
+    for a, b in ((hub, ohub), (auth, oauth)):
+        err = np.abs(a.astype(np.float64) - b)
+        assert float(err.max()) <= 1e-5
+        assert float(err.sum()) <= l1_tol, float(err.sum())
+
+
+def test_degree_centrality(big):
+    for s, e in [(0, 0), (big.span // 3, 2 * big.span // 3)]:
+        deg, avg = big.g.degree_centrality(s, e)
+        odeg, oavg = big.o.degree(big.ml, big.mv, big.act, s, e)
+        assert np.array_equal(deg, odeg), (s, e)
+        assert np.array_equal(avg, oavg), (s, e)
+
+
+def test_coloring_curand_priorities(big):
+    col, prio, rounds = big.g.color(0)
+    ocol, orounds = big.o.color(big.ml, big.mv, big.act, prio)
+    assert rounds == orounds
+    assert np.array_equal(col, ocol)
