@@ -282,6 +282,7 @@ int64_t orc_min_ts(orc* o) { return o->min_ts; }
 int64_t orc_graph_offset(orc* o, int64_t v) { return (int64_t)o->goff[v]; }
 int64_t orc_ts_offset(orc* o, int64_t v) { return (int64_t)o->toff[v]; }
 int32_t orc_outdegree(orc* o, int64_t v) { return o->deg[v]; }
+void orc_outdegrees(orc* o, int32_t* out) { memcpy(out, o->deg, (size_t)o->n * 4); }
 
 /* Decodes v's list and timestamps into dst/ts (capacity cap); returns the outdegree. */
 int64_t orc_neighbors(orc* o, int64_t v, int32_t* dst, int64_t* ts, int64_t cap) {
@@ -402,9 +403,62 @@ static hent hpop(heap* h) {
   return top;
 }
 
+/* Source of a vertex's list for the workloads below: the materialised CSR (s == NULL), or the
+ * compressed streams decoded at each visit (streaming mode, used by the timed CPU baseline; s
+ * counts the edges decoded).  succ_only: timestamps are not decoded (left at 0). */
+typedef struct {
+  ivec L;
+  int64_t* ts;
+  int64_t cap;
+  int64_t edges;
+  int succ_only;
+} sctx;
+
+static int64_t stream_list(orc* o, int64_t x, ivec* L, int64_t** tsbuf, int64_t* tscap);
+
+static int64_t view_list(orc* o, int64_t x, sctx* s, const int32_t** dst, const int64_t** ts) {
+  if (!s) {
+    *dst = o->dst + o->off[x];
+    *ts = o->ts + o->off[x];
+    return o->off[x + 1] - o->off[x];
+  }
+  int64_t k;
+  if (s->succ_only) {
+    decode_list(o, x, &s->L, 0);
+    k = s->L.n;
+    if (k > s->cap) { s->cap = 2 * k; s->ts = (int64_t*)realloc(s->ts, (size_t)s->cap * 8); }
+    if (k) memset(s->ts, 0, (size_t)k * 8);
+  } else {
+    k = stream_list(o, x, &s->L, &s->ts, &s->cap);
+  }
+  s->edges += k;
+  *dst = s->L.v;
+  *ts = s->ts;
+  return k;
+}
+
+static void sctx_free(sctx* s) { free(s->L.v); free(s->ts); }
+
+/* FOR_DEDUP_EDGES over a list source. */
+#define FOR_DEDUP_VIEW(o, s, x, lo, hi, Y, T, BODY)                        \
+  do {                                                                     \
+    const int32_t* vd_;                                                    \
+    const int64_t* vt_;                                                    \
+    const int64_t vk_ = view_list((o), (x), (s), &vd_, &vt_);              \
+    int32_t prev_y_ = -1;                                                  \
+    for (int64_t e_ = 0; e_ < vk_; ++e_) {                                 \
+      const int64_t T = vt_[e_];                                           \
+      if (T < (lo) || T >= (hi)) continue;                                 \
+      const int32_t Y = vd_[e_];                                           \
+      if (Y == prev_y_) continue;                                          \
+      prev_y_ = Y;                                                         \
+      BODY                                                                 \
+    }                                                                      \
+  } while (0)
+
 /* Earliest arrival by Dijkstra on arrival times (the relaxation fixpoint is unique); returns the
  * number of vertices other than src that were reached.  key[] holds arrival << 32. */
-static int64_t bfs_core(orc* o, const orc_cfg* c, int32_t src, int64_t lo, int64_t hi, uint64_t* key) {
+static int64_t bfs_core(orc* o, const orc_cfg* c, int32_t src, int64_t lo, int64_t hi, uint64_t* key, sctx* sc) {
   heap h = {0};
   const uint64_t start = (uint64_t)(lo > 0 ? lo : 0) << 32;
   key[src] = start;
@@ -416,7 +470,7 @@ static int64_t bfs_core(orc* o, const orc_cfg* c, int32_t src, int64_t lo, int64
     if (top.key != key[x]) continue;
     if (x < c->active || x > c->max_label || x >= o->n) continue;
     const uint64_t ax = top.key >> 32;
-    FOR_DEDUP_EDGES(o, x, lo, hi, y, t, {
+    FOR_DEDUP_VIEW(o, sc, x, lo, hi, y, t, {
       if (y < c->active || y >= c->max_vertex) continue;
       if ((int64_t)ax > t || t >= 0xFFFFFFFFll) continue;
       const uint64_t nv = (uint64_t)t << 32;
@@ -433,7 +487,7 @@ static int64_t bfs_core(orc* o, const orc_cfg* c, int32_t src, int64_t lo, int64
 
 /* Hop counts: breadth-first over tight edges (arrival(x) <= t == arrival(y)) from src. */
 static void bfs_hops(orc* o, const orc_cfg* c, int32_t src, int64_t lo, int64_t hi, const uint64_t* key,
-                     int32_t* hops) {
+                     int32_t* hops, sctx* sc) {
   int32_t* q = (int32_t*)malloc((size_t)c->max_vertex * 4 + 4);
   int64_t qh = 0, qt = 0;
   hops[src] = 0;
@@ -442,7 +496,7 @@ static void bfs_hops(orc* o, const orc_cfg* c, int32_t src, int64_t lo, int64_t 
     const int32_t x = q[qh++];
     if (x < c->active || x > c->max_label || x >= o->n) continue;
     const int64_t ax = (int64_t)(key[x] >> 32);
-    FOR_DEDUP_EDGES(o, x, lo, hi, y, t, {
+    FOR_DEDUP_VIEW(o, sc, x, lo, hi, y, t, {
       if (y < c->active || y >= c->max_vertex) continue;
       if (ax > t || t >= 0xFFFFFFFFll) continue;
       if ((int64_t)(key[y] >> 32) != t || hops[y] != ORC_INF32) continue;
@@ -458,8 +512,8 @@ void orc_bfs(orc* o, int32_t max_label, int32_t max_vertex, int32_t active, int3
   orc_cfg c = {max_label, max_vertex, active};
   uint64_t* key = (uint64_t*)malloc((size_t)max_vertex * 8);
   for (int32_t i = 0; i < max_vertex; ++i) { key[i] = ~0ull; hops[i] = ORC_INF32; }
-  bfs_core(o, &c, src, lo, hi, key);
-  bfs_hops(o, &c, src, lo, hi, key, hops);
+  bfs_core(o, &c, src, lo, hi, key, NULL);
+  bfs_hops(o, &c, src, lo, hi, key, hops, NULL);
   for (int32_t i = 0; i < max_vertex; ++i) {
     const int inf = (key[i] >> 32) == 0xFFFFFFFFull;
     arr[i] = inf ? ORC_INF32 : (int32_t)(key[i] >> 32);
@@ -468,8 +522,8 @@ void orc_bfs(orc* o, int32_t max_label, int32_t max_vertex, int32_t active, int3
   free(key);
 }
 
-int32_t orc_cc(orc* o, int32_t max_label, int32_t max_vertex, int32_t active, int32_t begin, int64_t lo, int64_t hi,
-               int32_t early_exit, int32_t* label) {
+static int32_t cc_core(orc* o, int32_t max_label, int32_t max_vertex, int32_t active, int32_t begin, int64_t lo,
+                       int64_t hi, int32_t early_exit, int32_t* label, sctx* sc) {
   orc_cfg c = {max_label, max_vertex, active};
   uint64_t* key = (uint64_t*)malloc((size_t)max_vertex * 8);
   uint8_t* reached = (uint8_t*)calloc((size_t)max_vertex, 1);
@@ -482,7 +536,7 @@ int32_t orc_cc(orc* o, int32_t max_label, int32_t max_vertex, int32_t active, in
   for (int32_t v = begin < 0 ? 0 : begin; v < end; ++v) {
     if (early_exit && total > limit) break;
     if (reached[v] || v >= o->n || o->deg[v] <= 9) continue;
-    const int64_t t = bfs_core(o, &c, v, lo, hi, key);
+    const int64_t t = bfs_core(o, &c, v, lo, hi, key, sc);
     for (int32_t y = 0; y < max_vertex; ++y)
       if (key[y] != ~0ull) { label[y] = comp; reached[y] = 1; key[y] = ~0ull; }
     ++comp;
@@ -493,6 +547,11 @@ int32_t orc_cc(orc* o, int32_t max_label, int32_t max_vertex, int32_t active, in
   free(key);
   free(reached);
   return comp;
+}
+
+int32_t orc_cc(orc* o, int32_t max_label, int32_t max_vertex, int32_t active, int32_t begin, int64_t lo, int64_t hi,
+               int32_t early_exit, int32_t* label) {
+  return cc_core(o, max_label, max_vertex, active, begin, lo, hi, early_exit, label, NULL);
 }
 
 /* PageRank with the engine's contract (reference pagerank.cu semantics, reset before scatter). */
@@ -531,104 +590,169 @@ void orc_pagerank(orc* o, int32_t max_label, int32_t max_vertex, int32_t active,
   free(invdeg);
 }
 
-/* HITS; java=0 reference GPU semantics (no reset), java=1 BaselineRunner semantics. */
-void orc_hits(orc* o, int32_t max_label, int32_t max_vertex, int32_t active, int32_t iters, int32_t java, int64_t lo,
-              int64_t hi, double* hub, double* auth) {
+/* HITS; java=0 reference GPU semantics (no reset), java=1 BaselineRunner semantics.  stream:
+ * lists decoded at each visit (successors only when the window holds every timestamp, as the
+ * engine does); returns the edges decoded in streaming mode. */
+static int64_t hits_core(orc* o, int32_t max_label, int32_t max_vertex, int32_t active, int32_t iters, int32_t java,
+                         int64_t lo, int64_t hi, double* hub, double* auth, int stream) {
+  const int succ_only = lo <= o->min_ts && hi == INT64_MAX;  /* every timestamp is >= the header */
+  int64_t edges = 0;
   for (int32_t u = 0; u < max_vertex; ++u) hub[u] = auth[u] = 1.0;
   for (int it = 0; it < iters; ++it) {
     if (java) for (int32_t u = 0; u < max_vertex; ++u) hub[u] = 0.0;
-#pragma omp parallel for schedule(dynamic, 1024)
-    for (int32_t x = active; x < max_label; ++x) {
-      if (x >= o->n) continue;
-      double acc = 0;
-      FOR_DEDUP_EDGES(o, x, lo, hi, y, t, {
-        (void)t;
-        if (y < active || y >= max_vertex) continue;
-        acc += auth[y];
-      });
-      hub[x] += acc;
+#pragma omp parallel reduction(+ : edges)
+    {
+      sctx tsc = {0};
+      tsc.succ_only = succ_only;
+      sctx* sc = stream ? &tsc : NULL;
+#pragma omp for schedule(dynamic, 1024)
+      for (int32_t x = active; x < max_label; ++x) {
+        if (x >= o->n) continue;
+        double acc = 0;
+        FOR_DEDUP_VIEW(o, sc, x, lo, hi, y, t, {
+          (void)t;
+          if (y < active || y >= max_vertex) continue;
+          acc += auth[y];
+        });
+        hub[x] += acc;
+      }
+      edges += tsc.edges;
+      sctx_free(&tsc);
     }
     double s = 0;
     for (int32_t u = 0; u < max_vertex; ++u) s += hub[u] * hub[u];
     s = sqrt(s);
     if (s > 0) for (int32_t u = 0; u < max_vertex; ++u) hub[u] /= s;
     if (java) for (int32_t u = 0; u < max_vertex; ++u) auth[u] = 0.0;
-#pragma omp parallel for schedule(dynamic, 1024)
-    for (int32_t x = active; x < max_label; ++x) {
-      if (x >= o->n) continue;
-      const double hx = hub[x];
-      FOR_DEDUP_EDGES(o, x, lo, hi, y, t, {
-        (void)t;
-        if (y < active || y >= max_vertex) continue;
-        atomic_add_f64(&auth[y], hx);
-      });
+#pragma omp parallel reduction(+ : edges)
+    {
+      sctx tsc = {0};
+      tsc.succ_only = succ_only;
+      sctx* sc = stream ? &tsc : NULL;
+#pragma omp for schedule(dynamic, 1024)
+      for (int32_t x = active; x < max_label; ++x) {
+        if (x >= o->n) continue;
+        const double hx = hub[x];
+        FOR_DEDUP_VIEW(o, sc, x, lo, hi, y, t, {
+          (void)t;
+          if (y < active || y >= max_vertex) continue;
+          atomic_add_f64(&auth[y], hx);
+        });
+      }
+      edges += tsc.edges;
+      sctx_free(&tsc);
     }
     s = 0;
     for (int32_t u = 0; u < max_vertex; ++u) s += auth[u] * auth[u];
     s = sqrt(s);
     if (s > 0) for (int32_t u = 0; u < max_vertex; ++u) auth[u] /= s;
   }
+  return edges;
+}
+
+void orc_hits(orc* o, int32_t max_label, int32_t max_vertex, int32_t active, int32_t iters, int32_t java, int64_t lo,
+              int64_t hi, double* hub, double* auth) {
+  hits_core(o, max_label, max_vertex, active, iters, java, lo, hi, hub, auth, 0);
 }
 
 /* Degree centrality, Java semantics (BaselineRunner.java:316-346). */
-void orc_degree(orc* o, int32_t max_label, int32_t max_vertex, int32_t active, int64_t s, int64_t e, int32_t* deg,
-                int64_t* avg) {
+static int64_t degree_core(orc* o, int32_t max_label, int32_t max_vertex, int32_t active, int64_t s, int64_t e,
+                           int32_t* deg, int64_t* avg, int stream) {
   const int32_t lim = max_label + 1 < max_vertex ? max_label + 1 : max_vertex;
-  for (int32_t x = 0; x < max_vertex; ++x) {
-    int32_t d = 0;
-    int64_t mean = 0;
-    if (x >= active && x <= max_label && x < o->n) {
-      for (int64_t k = o->off[x]; k < o->off[x + 1]; ++k) {
-        const int32_t y = o->dst[k];
-        const int64_t t = o->ts[k];
-        if (y < active || y >= lim) continue;
-        if ((s == 0 && e == 0) || (s <= t && e >= t)) {
-          ++d;
-          mean += (t - mean) / d;
+  int64_t edges = 0;
+#pragma omp parallel reduction(+ : edges)
+  {
+    sctx tsc = {0};
+    sctx* sc = stream ? &tsc : NULL;
+#pragma omp for schedule(dynamic, 1024)
+    for (int32_t x = 0; x < max_vertex; ++x) {
+      int32_t d = 0;
+      int64_t mean = 0;
+      if (x >= active && x <= max_label && x < o->n) {
+        const int32_t* vd;
+        const int64_t* vt;
+        const int64_t k = view_list(o, x, sc, &vd, &vt);
+        for (int64_t i = 0; i < k; ++i) {
+          const int32_t y = vd[i];
+          const int64_t t = vt[i];
+          if (y < active || y >= lim) continue;
+          if ((s == 0 && e == 0) || (s <= t && e >= t)) {
+            ++d;
+            mean += (t - mean) / d;
+          }
         }
+        if (s != e) d = (int32_t)(0.85 * d + 0.15 * d * (double)(mean - s) / (double)(e - s) + 1);
       }
-      if (s != e) d = (int32_t)(0.85 * d + 0.15 * d * (double)(mean - s) / (double)(e - s) + 1);
+      deg[x] = d;
+      avg[x] = mean;
     }
-    deg[x] = d;
-    avg[x] = mean;
+    edges += tsc.edges;
+    sctx_free(&tsc);
   }
+  return edges;
 }
 
-/* Jones-Plassmann rounds with given priorities; returns rounds executed. */
-int32_t orc_color(orc* o, int32_t max_label, int32_t max_vertex, int32_t active, const uint32_t* prio,
-                  int32_t java_isolated, uint32_t* color) {
+void orc_degree(orc* o, int32_t max_label, int32_t max_vertex, int32_t active, int64_t s, int64_t e, int32_t* deg,
+                int64_t* avg) {
+  degree_core(o, max_label, max_vertex, active, s, e, deg, avg, 0);
+}
+
+/* Jones-Plassmann rounds with given priorities; returns rounds executed.  A round decides every
+ * vertex of the worklist from the colours at its start (snap), so the vertices of a round are
+ * independent and run in parallel; the worklist keeps its order. */
+static int32_t color_core(orc* o, int32_t max_label, int32_t max_vertex, int32_t active, const uint32_t* prio,
+                          int32_t java_isolated, uint32_t* color, int stream, int64_t* edges_out) {
   int32_t* wl = (int32_t*)malloc((size_t)max_vertex * 4);
   int32_t* nwl = (int32_t*)malloc((size_t)max_vertex * 4);
+  uint8_t* keep = (uint8_t*)malloc((size_t)max_vertex + 1);
   uint32_t* snap = (uint32_t*)malloc((size_t)max_vertex * 4);
-  int64_t wn = max_vertex;
+  int64_t wn = max_vertex, edges = 0;
   for (int32_t i = 0; i < max_vertex; ++i) { wl[i] = i; color[i] = 0xFFFFFFFFu; }
   int32_t round = 0;
   while (wn && round < 512) {
     memcpy(snap, color, (size_t)max_vertex * 4);
-    int64_t nn = 0;
-    for (int64_t i = 0; i < wn; ++i) {
-      const int32_t x = wl[i];
-      if (x < active || snap[x] != 0xFFFFFFFFu || x > max_label) continue;
-      if (x >= o->n || o->deg[x] == 0) {
-        if (java_isolated) color[x] = (uint32_t)round;
-        continue;
+#pragma omp parallel reduction(+ : edges)
+    {
+      sctx tsc = {0};
+      tsc.succ_only = 1;
+      sctx* sc = stream ? &tsc : NULL;
+#pragma omp for schedule(dynamic, 256)
+      for (int64_t i = 0; i < wn; ++i) {
+        const int32_t x = wl[i];
+        keep[i] = 0;
+        if (x < active || snap[x] != 0xFFFFFFFFu || x > max_label) continue;
+        if (x >= o->n || o->deg[x] == 0) {
+          if (java_isolated) color[x] = (uint32_t)round;
+          continue;
+        }
+        int larger = 0;
+        FOR_DEDUP_VIEW(o, sc, x, INT64_MIN, INT64_MAX, y, t, {
+          (void)t;
+          if (larger) break;
+          if (y < active || y >= max_vertex) continue;
+          if ((prio[y] > prio[x] || (prio[y] == prio[x] && y < x)) && snap[y] >= (uint32_t)round) larger = 1;
+        });
+        if (larger) keep[i] = 1;
+        else color[x] = (uint32_t)round;
       }
-      int larger = 0;
-      FOR_DEDUP_EDGES(o, x, INT64_MIN, INT64_MAX, y, t, {
-        (void)t;
-        if (larger) break;
-        if (y < active || y >= max_vertex) continue;
-        if ((prio[y] > prio[x] || (prio[y] == prio[x] && y < x)) && snap[y] >= (uint32_t)round) larger = 1;
-      });
-      if (larger) nwl[nn++] = x;
-      else color[x] = (uint32_t)round;
+      edges += tsc.edges;
+      sctx_free(&tsc);
     }
+    int64_t nn = 0;
+    for (int64_t i = 0; i < wn; ++i)
+      if (keep[i]) nwl[nn++] = wl[i];
     int32_t* tmp = wl; wl = nwl; nwl = tmp;
     wn = nn;
     ++round;
   }
-  free(wl); free(nwl); free(snap);
+  free(wl); free(nwl); free(keep); free(snap);
+  if (edges_out) *edges_out = edges;
   return round;
+}
+
+int32_t orc_color(orc* o, int32_t max_label, int32_t max_vertex, int32_t active, const uint32_t* prio,
+                  int32_t java_isolated, uint32_t* color) {
+  return color_core(o, max_label, max_vertex, active, prio, java_isolated, color, 0, NULL);
 }
 
 /* java.util.Random(seed).nextInt(256) sequence (documented JDK LCG). */
@@ -725,6 +849,63 @@ int64_t orc_stream_decode(orc* o, int64_t begin, int64_t end, uint64_t* csum, in
     free(L.v);
     free(tsb);
   }
+  return edges;
+}
+
+/* The remaining workloads of the benchmark step, decoded on the fly (streaming mode of the
+ * functions above); each returns the edges it decoded.  threads > 0 sets the OpenMP thread count
+ * (BFS and CC are sequential searches and use one thread). */
+static void set_threads(int32_t threads) {
+#ifdef _OPENMP
+  if (threads > 0) omp_set_num_threads(threads);
+#else
+  (void)threads;
+#endif
+}
+
+int64_t orc_stream_bfs(orc* o, int32_t max_label, int32_t max_vertex, int32_t active, int32_t src, int64_t lo,
+                       int64_t hi, int32_t* arr, int32_t* hops) {
+  orc_cfg c = {max_label, max_vertex, active};
+  sctx sc = {0};
+  uint64_t* key = (uint64_t*)malloc((size_t)max_vertex * 8);
+  for (int32_t i = 0; i < max_vertex; ++i) { key[i] = ~0ull; hops[i] = ORC_INF32; }
+  bfs_core(o, &c, src, lo, hi, key, &sc);
+  bfs_hops(o, &c, src, lo, hi, key, hops, &sc);
+  for (int32_t i = 0; i < max_vertex; ++i) {
+    const int inf = (key[i] >> 32) == 0xFFFFFFFFull;
+    arr[i] = inf ? ORC_INF32 : (int32_t)(key[i] >> 32);
+    if (inf) hops[i] = ORC_INF32;
+  }
+  free(key);
+  sctx_free(&sc);
+  return sc.edges;
+}
+
+int64_t orc_stream_cc(orc* o, int32_t max_label, int32_t max_vertex, int32_t active, int32_t begin, int64_t lo,
+                      int64_t hi, int32_t early_exit, int32_t* label, int32_t* comps) {
+  sctx sc = {0};
+  *comps = cc_core(o, max_label, max_vertex, active, begin, lo, hi, early_exit, label, &sc);
+  sctx_free(&sc);
+  return sc.edges;
+}
+
+int64_t orc_stream_hits(orc* o, int32_t max_label, int32_t max_vertex, int32_t active, int32_t iters, int32_t java,
+                        double* hub, double* auth, int32_t threads) {
+  set_threads(threads);
+  return hits_core(o, max_label, max_vertex, active, iters, java, 0, INT64_MAX, hub, auth, 1);
+}
+
+int64_t orc_stream_degree(orc* o, int32_t max_label, int32_t max_vertex, int32_t active, int64_t s, int64_t e,
+                          int32_t* deg, int64_t* avg, int32_t threads) {
+  set_threads(threads);
+  return degree_core(o, max_label, max_vertex, active, s, e, deg, avg, 1);
+}
+
+int64_t orc_stream_color(orc* o, int32_t max_label, int32_t max_vertex, int32_t active, const uint32_t* prio,
+                         int32_t java_isolated, uint32_t* color, int32_t* rounds, int32_t threads) {
+  set_threads(threads);
+  int64_t edges = 0;
+  *rounds = color_core(o, max_label, max_vertex, active, prio, java_isolated, color, 1, &edges);
   return edges;
 }
 

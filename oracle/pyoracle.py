@@ -32,6 +32,7 @@ def _load() -> C.CDLL:
         "orc_graph_offset": (i64, [P, i64]),
         "orc_ts_offset": (i64, [P, i64]),
         "orc_outdegree": (i32, [P, i64]),
+        "orc_outdegrees": (None, [P, P]),
         "orc_neighbors": (i64, [P, i64, P, P, i64]),
         "orc_materialize": (i64, [P]),
         "orc_csr": (None, [P, P, P, P]),
@@ -45,6 +46,11 @@ def _load() -> C.CDLL:
         "orc_java_random256": (None, [i64, i32, P]),
         "orc_stream_pagerank": (i64, [P, i32, i32, i32, i32, f64, f64, P, i32]),
         "orc_stream_decode": (i64, [P, i64, i64, P, i32]),
+        "orc_stream_bfs": (i64, [P, i32, i32, i32, i32, i64, i64, P, P]),
+        "orc_stream_cc": (i64, [P, i32, i32, i32, i32, i64, i64, i32, P, P]),
+        "orc_stream_hits": (i64, [P, i32, i32, i32, i32, i32, P, P, i32]),
+        "orc_stream_degree": (i64, [P, i32, i32, i32, i64, i64, P, P, i32]),
+        "orc_stream_color": (i64, [P, i32, i32, i32, P, i32, P, P, i32]),
         "orc_max_threads": (i32, []),
         "orc_read_codes": (i64, [P, i64, i32, i32, P, i64]),
         "orc_ef_get": (C.c_uint64, [P, P, i64, i32, i64]),
@@ -100,6 +106,11 @@ class Oracle:
     @property
     def min_ts(self) -> int:
         return self.L.orc_min_ts(self.h)
+
+    def outdegrees(self) -> np.ndarray:
+        out = np.zeros(self.n, np.int32)
+        self.L.orc_outdegrees(self.h, _p(out))
+        return out
 
     def graph_offsets(self) -> np.ndarray:
         return np.array([self.L.orc_graph_offset(self.h, v) for v in range(self.n + 1)], np.int64)
@@ -170,6 +181,42 @@ class Oracle:
         cs = np.zeros(max_vertex or self.n, np.uint64)
         e = self.L.orc_stream_decode(self.h, begin, end, _p(cs), threads)
         return cs, e
+
+    # Streaming forms of the remaining workloads (lists decoded at every visit); each returns its
+    # result and the number of edges it decoded.
+
+    def stream_bfs(self, max_label, max_vertex, active, src, lo=0, hi=INT64_MAX):
+        arr = np.zeros(max_vertex, np.int32)
+        hops = np.zeros(max_vertex, np.int32)
+        e = self.L.orc_stream_bfs(self.h, max_label, max_vertex, active, src, lo, hi, _p(arr), _p(hops))
+        return (arr, hops), e
+
+    def stream_cc(self, max_label, max_vertex, active, begin, lo=0, hi=INT64_MAX, early_exit=True):
+        lab = np.zeros(max_vertex, np.int32)
+        k = C.c_int32()
+        e = self.L.orc_stream_cc(self.h, max_label, max_vertex, active, begin, lo, hi, int(early_exit), _p(lab),
+                                 C.byref(k))
+        return (lab, k.value), e
+
+    def stream_hits(self, max_label, max_vertex, active, iters, java=False, threads=0):
+        hub = np.zeros(max_vertex, np.float64)
+        auth = np.zeros(max_vertex, np.float64)
+        e = self.L.orc_stream_hits(self.h, max_label, max_vertex, active, iters, int(java), _p(hub), _p(auth), threads)
+        return (hub, auth), e
+
+    def stream_degree(self, max_label, max_vertex, active, s=0, e=0, threads=0):
+        deg = np.zeros(max_vertex, np.int32)
+        avg = np.zeros(max_vertex, np.int64)
+        n = self.L.orc_stream_degree(self.h, max_label, max_vertex, active, s, e, _p(deg), _p(avg), threads)
+        return (deg, avg), n
+
+    def stream_color(self, max_label, max_vertex, active, prio, java_isolated=False, threads=0):
+        col = np.zeros(max_vertex, np.uint32)
+        p = np.ascontiguousarray(prio, np.uint32)
+        r = C.c_int32()
+        e = self.L.orc_stream_color(self.h, max_label, max_vertex, active, _p(p), int(java_isolated), _p(col),
+                                    C.byref(r), threads)
+        return (col, r.value), e
 
 
 def java_random256(seed: int, n: int) -> np.ndarray:
