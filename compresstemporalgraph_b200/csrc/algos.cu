@@ -18,6 +18,7 @@
 #include <cstring>
 #include <vector>
 
+#include "lean.cuh"
 #include "sweep.cuh"
 #include "trace.cuh"
 
@@ -26,12 +27,12 @@ namespace tga {
 // ---------------------------------------------------------------------------------------------
 // Neighbour access and raw decode
 
-__global__ void TGA_SWEEP_BOUNDS k_neighbor_access(GraphView g, Work w, int32_t begin, int32_t end,
-                                                    unsigned long long* csum, unsigned long long* edges) {
+__global__ void TGA_LEAN_BOUNDS k_neighbor_access(GraphView g, LeanWork lw, int32_t begin, int32_t end,
+                                                         unsigned long long* csum, unsigned long long* edges) {
   uint64_t h = 0;
   uint32_t k = 0;
-  const unsigned long long mine = run_order<false>(
-      g, w, [&](int v) { return v >= begin && v < end; },
+  const unsigned long long mine = run_lean(
+      g, lw.e, lw.count, lw.slices, lw.run_first, [&](int v) { return v >= begin && v < end; },
       [&](int, int first, int) {
         h = 0;
         k = (uint32_t)first;
@@ -70,11 +71,11 @@ __global__ void k_small_flags(const int32_t* deg, uint8_t* small, int32_t begin,
   if (v < end) small[v] = deg[v] < 4;
 }
 
-__global__ void TGA_SWEEP_BOUNDS k_decode_csr(GraphView g, Work w, const int64_t* off, int32_t* dst, int64_t* ts,
+__global__ void TGA_SWEEP_BOUNDS k_decode_csr(GraphView g, LeanWork lw, const int64_t* off, int32_t* dst, int64_t* ts,
                                                int64_t cap) {
   int64_t o = 0;
-  run_order<false>(
-      g, w, [&](int) { return true; },
+  run_lean(
+      g, lw.e, lw.count, lw.slices, lw.run_first, [&](int) { return true; },
       [&](int v, int first, int) {
         o = off[v] + first;
         return true;
@@ -189,14 +190,15 @@ __device__ __forceinline__ float temporal_weight(float alpha, int64_t t) {
   return a > 18.0f ? 1.0f : 1.0f - expf(-a);
 }
 
-__global__ void TGA_SWEEP_BOUNDS k_pr_iter(GraphView g, Work w, PrArgs a) {
+// k_pr_iter over the lean schedule.
+__global__ void TGA_LEAN_BOUNDS k_pr_iter(GraphView g, LeanWork lw, PrArgs a) {
   for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < g.max_vertex; x += gridDim.x * blockDim.x) a.reset[x] = a.base;
   const double s = a.k == 0 ? 1.0 : 1.0 / a.sums[a.k - 1];
   float local = 0.0f, c0 = 0.0f;
   double total = 0.0;
   int prev_y = -1;
-  const unsigned long long mine = run_order<false, false, true>(
-      g, w,
+  const unsigned long long mine = run_lean<true>(
+      g, lw.e, lw.count, lw.slices, lw.run_first,
       [&](int v) {
         if (v < g.active_begin || v >= g.max_label) return false;
         return a.invdeg ? a.invdeg[v] > 0.0f : a.deg[v] > 0;
@@ -231,11 +233,11 @@ __global__ void k_pr_final(const float* buf, const double* sums, int k, float* o
 }
 
 // In-window outdegree of each source, counted over items, then inverted.
-__global__ void TGA_SWEEP_BOUNDS k_window_count(GraphView g, Work w, int64_t lo, int64_t hi, int32_t* cnt,
+__global__ void TGA_SWEEP_BOUNDS k_window_count(GraphView g, LeanWork lw, int64_t lo, int64_t hi, int32_t* cnt,
                                                  unsigned long long* edges) {
   int k = 0;
-  const unsigned long long mine = run_order<false>(
-      g, w, [&](int v) { return v >= g.active_begin && v < g.max_label; },
+  const unsigned long long mine = run_lean(
+      g, lw.e, lw.count, lw.slices, lw.run_first, [&](int v) { return v >= g.active_begin && v < g.max_label; },
       [&](int, int, int) {
         k = 0;
         return true;
@@ -269,13 +271,13 @@ __global__ void k_hits_base(float* hub, const float* auth_in, float* auth_next, 
 }
 
 template <bool kTimes>
-__global__ void TGA_SWEEP_BOUNDS k_hits_hub(GraphView g, Work w, float* hub, const float* auth_in, const double* aprev,
+__global__ void TGA_SWEEP_BOUNDS k_hits_hub(GraphView g, LeanWork lw, float* hub, const float* auth_in, const double* aprev,
                                              int64_t lo, int64_t hi, unsigned long long* edges) {
   const float sa = (aprev && *aprev > 0) ? (float)(1.0 / sqrt(*aprev)) : 1.0f;
   float acc = 0.0f;
   int prev_y = -1;
-  const unsigned long long mine = run_order<false, false, true, kTimes>(
-      g, w, [&](int v) { return v >= g.active_begin && v < g.max_label; },
+  const unsigned long long mine = run_lean<true, kTimes>(
+      g, lw.e, lw.count, lw.slices, lw.run_first, [&](int v) { return v >= g.active_begin && v < g.max_label; },
       [&](int, int, int) {
         acc = 0.0f;
         prev_y = -1;
@@ -292,13 +294,13 @@ __global__ void TGA_SWEEP_BOUNDS k_hits_hub(GraphView g, Work w, float* hub, con
 }
 
 template <bool kTimes>
-__global__ void TGA_SWEEP_BOUNDS k_hits_auth(GraphView g, Work w, const float* hub, const double* hsum,
+__global__ void TGA_SWEEP_BOUNDS k_hits_auth(GraphView g, LeanWork lw, const float* hub, const double* hsum,
                                               float* auth_next, int64_t lo, int64_t hi, unsigned long long* edges) {
   const float sh = *hsum > 0 ? (float)(1.0 / sqrt(*hsum)) : 1.0f;
   float hn = 0.0f;
   int prev_y = -1;
-  const unsigned long long mine = run_order<false, false, true, kTimes>(
-      g, w, [&](int v) { return v >= g.active_begin && v < g.max_label && hub[v] != 0.0f; },
+  const unsigned long long mine = run_lean<true, kTimes>(
+      g, lw.e, lw.count, lw.slices, lw.run_first, [&](int v) { return v >= g.active_begin && v < g.max_label && hub[v] != 0.0f; },
       [&](int v, int, int) {
         hn = hub[v] * sh;
         prev_y = -1;
@@ -329,14 +331,14 @@ __global__ void k_scale(const float* v, const double* sumsq, float* out, int32_t
 // ---------------------------------------------------------------------------------------------
 // Degree centrality (Java semantics).  Short lists: one thread per list.
 
-__global__ void TGA_TRAVERSE_BOUNDS k_degree(GraphView g, Work w, int64_t s, int64_t e, int32_t* deg, int64_t* avg,
+__global__ void TGA_TRAVERSE_BOUNDS k_degree(GraphView g, LeanWork lw, int64_t s, int64_t e, int32_t* deg, int64_t* avg,
                                            unsigned long long* edges) {
   const bool all = (s == 0 && e == 0);
   const int lim = min(g.max_label + 1, g.max_vertex);
   int32_t d = 0;
   int64_t mean = 0;
-  const unsigned long long mine = run_order<true>(
-      g, w,
+  const unsigned long long mine = run_lean(
+      g, lw.e, lw.count, lw.slices, lw.run_first,
       [&](int v) { return v >= g.active_begin && v <= g.max_label && g.slice_first[v] == g.slice_first[v + 1]; },
       [&](int, int, int) {
         d = 0;
@@ -582,6 +584,11 @@ int compute_max_timestamp(GraphHandle& h) {
   return TGA_OK;
 }
 
+static LeanWork lean_work(const GraphHandle& h) {
+  return LeanWork{h.d_lean.as<LeanEntry>(), h.nlean, h.d_slices.as<SliceState>(), h.d_run_first.as<int32_t>()};
+}
+static unsigned lean_grid(const GraphHandle& h) { return std::max(1u, grid_for(h.nlean, kBlock)); }
+
 }  // namespace tga
 
 using namespace tga;
@@ -605,9 +612,8 @@ int tga_neighbor_access(tga_graph* gp, uint8_t* small_out, uint64_t* checksum_ou
   cudaMemsetAsync(h.s_b.p, 0, (size_t)nv * 8, h.stream);
   const int32_t b = h.view.active_begin, e = std::min(h.view.max_label, h.view.n);
   if (e > b) {
-    const Work w = work_of(h);
     cudaEvent_t* ev = h.kernel_begin();
-    KL(k_neighbor_access, sweep_grid(h))(h.view, w, b, e, h.s_b.as<unsigned long long>(), edges);
+    KL(k_neighbor_access, lean_grid(h))(h.view, lean_work(h), b, e, h.s_b.as<unsigned long long>(), edges);
     h.kernel_end(ev);
     KL(k_small_flags, grid_for(e - b, kBlock))(h.d_deg.as<int32_t>(), h.s_a.as<uint8_t>(), b, e);
   }
@@ -685,8 +691,7 @@ int tga_decode_all(tga_graph* gp, int64_t* offsets, int32_t* dst, int64_t* ts, i
   TGA_TRY(h.s_g.ensure((size_t)std::max<int64_t>(m, 1) * 8));
   TGA_CUDA_TRY(cudaMemcpy(h.s_e.p, offsets, (size_t)(n + 1) * 8, cudaMemcpyHostToDevice));
   TGA_TRY(h.begin_call());
-  const Work w = work_of(h);
-  KL(k_decode_csr, sweep_grid(h))(h.view, w, h.s_e.as<int64_t>(), h.s_f.as<int32_t>(),
+    KL(k_decode_csr, lean_grid(h))(h.view, lean_work(h), h.s_e.as<int64_t>(), h.s_f.as<int32_t>(),
                                                 h.s_g.as<int64_t>(), m);
   cudaMemcpyAsync(dst, h.s_f.p, (size_t)m * 4, cudaMemcpyDeviceToHost, h.stream);
   cudaMemcpyAsync(ts, h.s_g.p, (size_t)m * 8, cudaMemcpyDeviceToHost, h.stream);
@@ -721,9 +726,8 @@ int tga_pagerank(tga_graph* gp, int32_t iters, float damping, float alpha, int64
     int32_t* cnt = h.s_e.as<int32_t>();
     invdeg = h.s_d.as<float>();
     cudaMemsetAsync(cnt, 0, (size_t)nv * 4, h.stream);
-    const Work w = work_of(h);
-    cudaEvent_t* ev = h.kernel_begin();
-    KL(k_window_count, sweep_grid(h))(h.view, w, t_lo, t_hi, cnt, edges);
+        cudaEvent_t* ev = h.kernel_begin();
+    KL(k_window_count, lean_grid(h))(h.view, lean_work(h), t_lo, t_hi, cnt, edges);
     h.kernel_end(ev);
     KL(k_invert, grid_for(nv, kBlock))(cnt, invdeg, nv);
   }
@@ -734,11 +738,10 @@ int tga_pagerank(tga_graph* gp, int32_t iters, float damping, float alpha, int64
                                      bits_of(damping), bits_of(alpha), (uint64_t)t_lo, (uint64_t)t_hi};
   TGA_TRY(run_loop(h, h.pr_loop, key, (size_t)iters, [&]() -> int {
     for (int k = 0; k < iters; ++k) {
-      const Work w = work_of(h);
       PrArgs a{invdeg, h.d_deg.as<int32_t>(), bufs[k % 3], bufs[(k + 1) % 3], bufs[(k + 2) % 3], sums, k,
                damping, alpha, base, t_lo, t_hi, edges};
       cudaEvent_t* ev = h.kernel_begin();
-      KL(k_pr_iter, grid)(h.view, w, a);
+      KL(k_pr_iter, lean_grid(h))(h.view, lean_work(h), a);
       h.kernel_end(ev);
     }
     return TGA_OK;
@@ -789,18 +792,16 @@ int tga_hits(tga_graph* gp, int32_t iters, int32_t mode, int64_t t_lo, int64_t t
       float* ain = auth[k & 1];
       float* anext = auth[(k + 1) & 1];
       KL(k_hits_base, grid_for(nv, kBlock))(hub, ain, anext, aprev, java, nv);
-      Work w = work_of(h);
       cudaEvent_t* ev = h.kernel_begin();
       // (without decoded timestamps every edge reports t = 0, so the window check is opened fully)
-      if (all_times) KL(k_hits_hub<false>, sweep_grid(h))(h.view, w, hub, ain, aprev, INT64_MIN, INT64_MAX, edges);
-      else KL(k_hits_hub<true>, sweep_grid(h))(h.view, w, hub, ain, aprev, t_lo, t_hi, edges);
+      if (all_times) KL(k_hits_hub<false>, lean_grid(h))(h.view, lean_work(h), hub, ain, aprev, INT64_MIN, INT64_MAX, edges);
+      else KL(k_hits_hub<true>, lean_grid(h))(h.view, lean_work(h), hub, ain, aprev, t_lo, t_hi, edges);
       h.kernel_end(ev);
       KL(k_sumsq, grid_for(nv, kBlock))(hub, nv, sums + 2 * k);
-      w = work_of(h);
       ev = h.kernel_begin();
       if (all_times)
-        KL(k_hits_auth<false>, sweep_grid(h))(h.view, w, hub, sums + 2 * k, anext, INT64_MIN, INT64_MAX, edges);
-      else KL(k_hits_auth<true>, sweep_grid(h))(h.view, w, hub, sums + 2 * k, anext, t_lo, t_hi, edges);
+        KL(k_hits_auth<false>, lean_grid(h))(h.view, lean_work(h), hub, sums + 2 * k, anext, INT64_MIN, INT64_MAX, edges);
+      else KL(k_hits_auth<true>, lean_grid(h))(h.view, lean_work(h), hub, sums + 2 * k, anext, t_lo, t_hi, edges);
       h.kernel_end(ev);
       KL(k_scale, grid_for(nv, kBlock))(hub, sums + 2 * k, hub, nv);
       KL(k_sumsq, grid_for(nv, kBlock))(anext, nv, sums + 2 * k + 1);
@@ -830,9 +831,8 @@ int tga_degree(tga_graph* gp, int64_t t_start, int64_t t_end, int32_t* degree_ou
   unsigned long long* edges = edge_counter(h);
   cudaMemsetAsync(h.s_a.p, 0, (size_t)nv * 4, h.stream);
   cudaMemsetAsync(h.s_b.p, 0, (size_t)nv * 8, h.stream);
-  const Work w = work_of(h);
   cudaEvent_t* ev = h.kernel_begin();
-  KL(k_degree, sweep_grid(h))(h.view, w, t_start, t_end, h.s_a.as<int32_t>(), h.s_b.as<int64_t>(), edges);
+  KL(k_degree, lean_grid(h))(h.view, lean_work(h), t_start, t_end, h.s_a.as<int32_t>(), h.s_b.as<int64_t>(), edges);
   h.kernel_end(ev);
   if (h.nlong > 0) {
     cudaEvent_t* ev2 = h.kernel_begin();
@@ -990,14 +990,14 @@ int tga_pagerank_noalloc(tga_graph* gp, int32_t iters, float damping, float alph
     invdeg = invdeg_buf;
     // The in-window outdegrees are accumulated with atomics and start at zero.
     TGA_CUDA_TRY(cudaMemsetAsync(cnt, 0, (size_t)nv * 4, h.stream));
-    KL(k_window_count, sweep_grid(h))(h.view, w, t_lo, t_hi, cnt, edges);
+    KL(k_window_count, lean_grid(h))(h.view, lean_work(h), t_lo, t_hi, cnt, edges);
     KL(k_invert, grid_for(nv, kBlock))(cnt, invdeg, nv);
   }
   const unsigned grid = sweep_grid(h);
   for (int k = 0; k < iters; ++k) {
     PrArgs a{invdeg, h.d_deg.as<int32_t>(), bufs[k % 3], bufs[(k + 1) % 3], bufs[(k + 2) % 3], sums, k,
              damping, alpha, base, t_lo, t_hi, edges};
-    KL(k_pr_iter, grid)(h.view, w, a);
+    KL(k_pr_iter, lean_grid(h))(h.view, lean_work(h), a);
   }
   KL(k_pr_final, grid_for(nv, kBlock))(bufs[iters % 3], sums, iters - 1, rank_out_dev, nv);
   h.timing.iterations = iters;

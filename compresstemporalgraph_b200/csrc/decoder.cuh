@@ -28,7 +28,8 @@ struct ListState {
   int ileft, iend;           // intervals still to read, end (exclusive) of the current one
   int rleft;                 // residuals left including the head
   int x;                     // vertex whose list this is
-  int emitted;               // values returned so far (maintained below level 0)
+  int emitted;               // below level 0: values returned so far; at level 0: copied values
+                             // consumed (the index of hc in the list's resolved copies)
 };
 
 // Copy mask of one level over the next level's list.
@@ -362,7 +363,10 @@ static __device__ __noinline__ OpenRef deep_open_ref(const GraphView& g, DeepSta
 __device__ __forceinline__ int top_next(const GraphView& g, ListState& st, DeepState* deep) {
   const int v = min(min(st.hm, st.hi), min(st.hr, st.hc));
   if (v == kInf) return kInf;
-  if (merge_advance(g, st, v)) st.hc = deep_copy_next(*g.self, *deep);
+  if (merge_advance(g, st, v)) {
+    st.hc = deep_copy_next(*g.self, *deep);
+    ++st.emitted;
+  }
   return v;
 }
 

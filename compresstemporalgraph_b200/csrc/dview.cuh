@@ -64,6 +64,11 @@ struct GraphView {
   const struct GraphView* self;
   int64_t min_ts;        // header of the .timestamps stream
   uint32_t* err;         // device error word
+  // Copied values resolved at load: the values that the copy mask of list x selects from its
+  // referenced list, in order, are copies[copy_base[x] .. copy_base[x+1]) (empty for a list without
+  // a reference).  Read by the lean sweep decoder (lean.cuh) instead of walking the chain.
+  const int32_t* copies;
+  const uint32_t* copy_base;
 };
 
 __device__ __forceinline__ void set_err(const GraphView& g, uint32_t bit) { atomicOr(g.err, bit); }

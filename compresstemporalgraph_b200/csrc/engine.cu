@@ -13,6 +13,7 @@
 #include "decoder.cuh"
 #include "engine.hpp"
 #include "format.hpp"
+#include "lean.cuh"
 #include "trace.cuh"
 
 namespace tga {
@@ -49,7 +50,7 @@ void DevBuf::release() {
 GraphHandle::~GraphHandle() {
   if (stream) cudaStreamSynchronize(stream);
   for (DevBuf* b : {&d_graph, &d_ts, &d_gl, &d_gu, &d_gs, &d_tl, &d_tu, &d_ts_samples, &d_err, &d_deg, &d_slices,
-                    &d_items, &d_slice_first, &d_slice_deep, &d_order, &d_runs, &d_run_pairs, &d_run_first, &d_long, &d_slice_ebase,
+                    &d_items, &d_slice_first, &d_slice_deep, &d_order, &d_lean, &d_copies, &d_copy_base, &d_runs, &d_run_pairs, &d_run_first, &d_long, &d_slice_ebase,
                     &d_view, &s_edges, &s_a, &s_b, &s_c, &s_d, &s_e, &s_f, &s_g, &s_q0, &s_q1, &s_cnt, &s_sum,
                     &m_state, &m_mask, &m_dirty, &m_stamp, &m_touched, &m_dq, &d_divtab})
     b->release();
@@ -191,6 +192,55 @@ __global__ void k_outdegrees(GraphView g, int32_t* deg, uint8_t* chain, int32_t 
   const int d = (int)read_gamma(g, g.g, pos);
   deg[x] = d;
   chain[x] = d > 0 && read_unary(g, g.g, pos) > 0;
+}
+
+// Resolves the copy mask of every list with a reference into GraphView::copies (two passes of
+// k_resolve_copies: counts, then values at their prefix-sum bases).
+static int resolve_copies(GraphHandle& h) {
+  // The chain walk reads the device-global copy of the view (max_list has been set since it was
+  // last published).
+  TGA_TRY(publish_view(h));
+  std::vector<int32_t> ids;
+  for (size_t x = 0; x < h.chain_host.size(); ++x)
+    if (h.chain_host[x]) ids.push_back((int32_t)x);
+  const size_t nb = h.degrees.size() + 1;
+  std::vector<uint32_t> base(nb, 0);
+  int rc;
+  DevBuf d_ids, d_cnt;
+  std::vector<uint32_t> cnt(ids.size(), 0);
+  if (!ids.empty()) {
+    if ((rc = d_ids.ensure(ids.size() * 4)) || (rc = d_cnt.ensure(ids.size() * 4))) return rc;
+    TGA_CUDA_TRY(cudaMemcpy(d_ids.p, ids.data(), ids.size() * 4, cudaMemcpyHostToDevice));
+    k_resolve_copies<<<grid_for((int64_t)ids.size(), 128), 128, 0, h.stream>>>(h.view, d_ids.as<int32_t>(),
+                                                                              (int32_t)ids.size(), d_cnt.as<uint32_t>(),
+                                                                              nullptr, nullptr);
+    TGA_CUDA_TRY(cudaGetLastError());
+    TGA_CUDA_TRY(cudaMemcpyAsync(cnt.data(), d_cnt.p, ids.size() * 4, cudaMemcpyDeviceToHost, h.stream));
+    if ((rc = h.check_device_error())) return rc;
+  }
+  uint64_t total = 0;
+  {
+    size_t k = 0;
+    for (size_t x = 0; x + 1 < nb; ++x) {
+      base[x] = (uint32_t)total;
+      if (k < ids.size() && (size_t)ids[k] == x) total += cnt[k++];
+      if (total >= (1ull << 32)) return fail(TGA_E_FORMAT, "more than 2^32 copied values");
+    }
+    base[nb - 1] = (uint32_t)total;
+  }
+  if ((rc = h.d_copy_base.ensure(nb * 4)) || (rc = h.d_copies.ensure(std::max<uint64_t>(total, 1) * 4))) return rc;
+  TGA_CUDA_TRY(cudaMemcpy(h.d_copy_base.p, base.data(), nb * 4, cudaMemcpyHostToDevice));
+  h.info.device_bytes += nb * 4 + std::max<uint64_t>(total, 1) * 4;
+  if (!ids.empty()) {
+    k_resolve_copies<<<grid_for((int64_t)ids.size(), 128), 128, 0, h.stream>>>(
+        h.view, d_ids.as<int32_t>(), (int32_t)ids.size(), nullptr, h.d_copy_base.as<uint32_t>(), h.d_copies.as<int32_t>());
+    TGA_CUDA_TRY(cudaGetLastError());
+    TGA_CUDA_TRY(cudaStreamSynchronize(h.stream));
+    if ((rc = h.check_device_error())) return rc;
+  }
+  h.view.copies = h.d_copies.as<int32_t>();
+  h.view.copy_base = h.d_copy_base.as<uint32_t>();
+  return publish_view(h);
 }
 
 int load_graph(GraphHandle& h, const std::string& dir, const std::string& base, const tga_dataset_cfg& cfg) {
@@ -350,6 +400,7 @@ int load_graph(GraphHandle& h, const std::string& dir, const std::string& base, 
   }
   h.info_edges = m;
   h.degrees = std::move(deg);
+  if ((rc = resolve_copies(h))) return rc;
   const char* env_slice = std::getenv("TGA_SLICE_EDGES");
   const char* env_item = std::getenv("TGA_ITEM_EDGES");
   if (int rc = build_work(h, env_slice ? std::atoi(env_slice) : kDefaultSliceEdges, env_item ? std::atoi(env_item) : 256))
@@ -537,6 +588,39 @@ int build_work(GraphHandle& h, int32_t slice_len, int32_t item_edges) {
       for (int b = (int)bins.size() - 2 + c; b >= 0; b -= 2) order.insert(order.end(), bins[(size_t)b].begin(), bins[(size_t)b].end());
   }
   h.norder = (int32_t)order.size();
+  // Lean schedule: the order above, with a short copying list (a single slice from edge 0) as a
+  // whole-list entry (the lean decoder opens it from its record and the resolved copies).
+  {
+    std::vector<int32_t> ids;
+    ids.reserve(order.size());
+    for (int32_t e : order) {
+      if (e < 0) {
+        const SliceState& sl = packed[(size_t)(-e - 1)];
+        if (sl.chain && sl.first == 0 && sl.count == h.degrees[(size_t)sl.v]) {
+          ids.push_back(sl.v);
+          continue;
+        }
+      }
+      ids.push_back(e);
+    }
+    h.nlean = (int32_t)ids.size();
+    if (h.info.graph_bytes * 8 >= (1ull << 48) || h.info.timestamp_bytes * 8 >= (1ull << 48))
+      return fail(TGA_E_FORMAT, "stream longer than 2^48 bits");
+    DevBuf tmp_ids;
+    int rc;
+    if ((rc = tmp_ids.ensure(std::max<size_t>(1, ids.size()) * 4)) ||
+        (rc = h.d_lean.ensure(std::max<size_t>(1, ids.size()) * sizeof(LeanEntry))))
+      return rc;
+    if (!ids.empty()) {
+      TGA_CUDA_TRY(cudaMemcpy(tmp_ids.p, ids.data(), ids.size() * 4, cudaMemcpyHostToDevice));
+      k_lean_entries<<<grid_for((int64_t)ids.size(), 256), 256, 0, h.stream>>>(v, tmp_ids.as<int32_t>(), (int32_t)ids.size(),
+                                                                          h.d_lean.as<LeanEntry>());
+      TGA_CUDA_TRY(cudaGetLastError());
+      TGA_CUDA_TRY(cudaStreamSynchronize(h.stream));
+      if ((rc = h.check_device_error())) return rc;
+    }
+    tmp_ids.release();
+  }
   // A traversal level sweeps all lists instead of its queue once the queue holds at least
   // 1/TGA_DENSE_DIV (default 16) of the schedule's entries.
   const char* env_dense = std::getenv("TGA_DENSE_DIV");
@@ -583,6 +667,7 @@ int build_work(GraphHandle& h, int32_t slice_len, int32_t item_edges) {
   v.slice_first = h.d_slice_first.as<int32_t>();
   v.deg = h.d_deg.as<int32_t>();
   h.work_bytes = h.d_slices.bytes + h.d_slice_deep.bytes + h.d_slice_first.bytes + h.d_items.bytes + h.d_order.bytes +
+                 h.d_lean.bytes +
                  h.d_runs.bytes + h.d_run_pairs.bytes + h.d_run_first.bytes + h.d_long.bytes + h.d_slice_ebase.bytes;
   v.seek_min = std::max(16, slice_len / 2);
   return publish_view(h);

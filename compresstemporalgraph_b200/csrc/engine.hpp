@@ -71,6 +71,12 @@ struct GraphHandle {
   uint64_t work_bytes = 0;           // device bytes of the work decomposition (slices, schedule, runs)
   // decode order of the sweeps (vertex ids >= 0 and -(slice+1)), grouped by work class
   DevBuf d_order;
+  // lean sweep schedule (lean.cuh): LeanEntry[nlean], the sweep order with short lists (copying
+  // ones included) as whole-list entries
+  DevBuf d_lean;
+  int32_t nlean = 0;
+  // copied values of every list resolved at load (GraphView::copies / copy_base)
+  DevBuf d_copies, d_copy_base;
   // runs of equal successors cut by slices: RunInfo[nruns], (run, slice) pairs of the per-call
   // pre-pass, and the per-call list index of each run's first in-window edge
   DevBuf d_runs, d_run_pairs, d_run_first;
