@@ -261,22 +261,28 @@ __global__ void k_invert(const int32_t* cnt, float* inv, int32_t n) {
 // HITS.  Per iteration: hub base (vector), hub gather (items), sum hub^2, authority scatter
 // (items), normalise hub, sum auth^2.  Authorities are kept unnormalised between iterations
 // and scaled by 1/||auth|| when read.
+//
+// Per-edge arithmetic is FP32; the hub and authority accumulators are FP64.  With preferential
+// in-degrees one authority receives about a million contributions per half step, each some 10^5
+// times smaller than the running sum: in an FP32 accumulator every addition loses up to half an
+// ulp of the sum, which biased that authority by 0.3% after one iteration on the 2M/40M graph.
 
-__global__ void k_hits_base(float* hub, const float* auth_in, float* auth_next, const double* aprev, int java, int32_t n) {
+__global__ void k_hits_base(double* hub, const double* auth_in, double* auth_next, const double* aprev, int java,
+                            int32_t n) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= n) return;
-  const float sa = (aprev && *aprev > 0) ? (float)(1.0 / sqrt(*aprev)) : 1.0f;
-  if (java) hub[x] = 0.0f;
-  auth_next[x] = java ? 0.0f : auth_in[x] * sa;
+  const double sa = (aprev && *aprev > 0) ? 1.0 / sqrt(*aprev) : 1.0;
+  if (java) hub[x] = 0.0;
+  auth_next[x] = java ? 0.0 : auth_in[x] * sa;
 }
 
 template <bool kTimes>
-__global__ void TGA_SWEEP_BOUNDS k_hits_hub(GraphView g, LeanWork lw, float* hub, const float* auth_in, const double* aprev,
-                                             int64_t lo, int64_t hi, unsigned long long* edges) {
+__global__ void TGA_LEAN_BOUNDS k_hits_hub(GraphView g, LeanWork lw, double* hub, const double* auth_in,
+                                           const double* aprev, int64_t lo, int64_t hi, unsigned long long* edges) {
   const float sa = (aprev && *aprev > 0) ? (float)(1.0 / sqrt(*aprev)) : 1.0f;
   float acc = 0.0f;
   int prev_y = -1;
-  const unsigned long long mine = run_lean<true, kTimes>(
+  const unsigned long long mine = run_lean<true, kTimes, false, !kTimes>(
       g, lw.e, lw.count, lw.slices, lw.run_first, [&](int v) { return v >= g.active_begin && v < g.max_label; },
       [&](int, int, int) {
         acc = 0.0f;
@@ -284,48 +290,51 @@ __global__ void TGA_SWEEP_BOUNDS k_hits_hub(GraphView g, LeanWork lw, float* hub
         return true;
       },
       [&](int, int y, int64_t t) {
-        if (keep_edge(g, lo, hi, y, t, prev_y)) acc += auth_in[y];
+        if (keep_edge(g, lo, hi, y, t, prev_y)) acc += (float)auth_in[y];
         return true;
       },
       [&](int v) {
-        if (acc != 0.0f) atomicAdd(&hub[v], acc * sa);
+        if (acc != 0.0f) atomicAdd(&hub[v], (double)(acc * sa));
       });
   add_edges(edges, mine);
 }
 
 template <bool kTimes>
-__global__ void TGA_SWEEP_BOUNDS k_hits_auth(GraphView g, LeanWork lw, const float* hub, const double* hsum,
-                                              float* auth_next, int64_t lo, int64_t hi, unsigned long long* edges) {
-  const float sh = *hsum > 0 ? (float)(1.0 / sqrt(*hsum)) : 1.0f;
+__global__ void TGA_LEAN_BOUNDS k_hits_auth(GraphView g, LeanWork lw, const double* hub, const double* hsum,
+                                            double* auth_next, int64_t lo, int64_t hi, unsigned long long* edges) {
+  const double sh = *hsum > 0 ? 1.0 / sqrt(*hsum) : 1.0;
   float hn = 0.0f;
   int prev_y = -1;
-  const unsigned long long mine = run_lean<true, kTimes>(
-      g, lw.e, lw.count, lw.slices, lw.run_first, [&](int v) { return v >= g.active_begin && v < g.max_label && hub[v] != 0.0f; },
+  const unsigned long long mine = run_lean<true, kTimes, false, !kTimes>(
+      g, lw.e, lw.count, lw.slices, lw.run_first,
+      [&](int v) { return v >= g.active_begin && v < g.max_label && hub[v] != 0.0; },
       [&](int v, int, int) {
-        hn = hub[v] * sh;
+        hn = (float)(hub[v] * sh);
         prev_y = -1;
         return true;
       },
       [&](int, int y, int64_t t) {
-        if (keep_edge(g, lo, hi, y, t, prev_y)) atomicAdd(&auth_next[y], hn);
+        if (keep_edge(g, lo, hi, y, t, prev_y)) atomicAdd(&auth_next[y], (double)hn);
         return true;
       },
       [&](int) {});
   add_edges(edges, mine);
 }
 
-__global__ void k_sumsq(const float* v, int32_t n, double* out) {
+__global__ void k_sumsq(const double* v, int32_t n, double* out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const double x = i < n ? (double)v[i] : 0.0;
+  const double x = i < n ? v[i] : 0.0;
   const double bs = block_sum(x * x);
   if (threadIdx.x == 0 && bs != 0.0) atomicAdd(out, bs);
 }
 
-__global__ void k_scale(const float* v, const double* sumsq, float* out, int32_t n) {
+// out = v / ||v|| (out may be v).
+template <class Out>
+__global__ void k_scale(const double* v, const double* sumsq, Out* out, int32_t n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double s = *sumsq > 0 ? 1.0 / sqrt(*sumsq) : 1.0;
-  out[i] = (float)((double)v[i] * s);
+  out[i] = (Out)(v[i] * s);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -764,9 +773,10 @@ int tga_hits(tga_graph* gp, int32_t iters, int32_t mode, int64_t t_lo, int64_t t
   if (mode != TGA_HITS_GPU && mode != TGA_HITS_JAVA) return fail(TGA_E_ARG, "unknown HITS mode");
   if (t_lo >= t_hi) return fail(TGA_E_ARG, "empty time window");
   const int32_t nv = h.view.max_vertex;
-  TGA_TRY(h.s_a.ensure((size_t)nv * 4));
-  TGA_TRY(h.s_b.ensure((size_t)nv * 4));
-  TGA_TRY(h.s_c.ensure((size_t)nv * 4));
+  TGA_TRY(h.s_a.ensure((size_t)nv * 8));
+  TGA_TRY(h.s_b.ensure((size_t)nv * 8));
+  TGA_TRY(h.s_c.ensure((size_t)nv * 8));
+  TGA_TRY(h.s_d.ensure((size_t)nv * 8));
   TGA_TRY(h.s_g.ensure((size_t)(2 * iters + 2) * 8));
   TGA_TRY(h.begin_call());
   // With a window that holds every timestamp, HITS depends only on the successor order: the
@@ -774,12 +784,12 @@ int tga_hits(tga_graph* gp, int32_t iters, int32_t mode, int64_t t_lo, int64_t t
   const bool all_times = window_covers_all(h, t_lo, t_hi);
   prepare_runs(h, t_lo, t_hi);
   unsigned long long* edges = edge_counter(h);
-  float* hub = h.s_a.as<float>();
-  float* auth[2] = {h.s_b.as<float>(), h.s_c.as<float>()};
+  double* hub = h.s_a.as<double>();
+  double* auth[2] = {h.s_b.as<double>(), h.s_c.as<double>()};
   double* sums = h.s_g.as<double>();
   const int java = mode == TGA_HITS_JAVA;
-  KL(k_fill_f32, grid_for(nv, kBlock))(hub, 1.0f, nv);
-  KL(k_fill_f32, grid_for(nv, kBlock))(auth[0], 1.0f, nv);
+  KL(k_fill_f64, grid_for(nv, kBlock))(hub, 1.0, nv);
+  KL(k_fill_f64, grid_for(nv, kBlock))(auth[0], 1.0, nv);
   cudaMemsetAsync(sums, 0, (size_t)(2 * iters + 2) * 8, h.stream);
   // sums[2k] = sum hub^2 of iteration k, sums[2k+1] = sum auth^2 of iteration k.  The iterations
   // run as one CUDA graph, replayed by later calls with the same parameters.
@@ -789,8 +799,8 @@ int tga_hits(tga_graph* gp, int32_t iters, int32_t mode, int64_t t_lo, int64_t t
   TGA_TRY(run_loop(h, h.hits_loop, key, (size_t)(2 * iters), [&]() -> int {
     for (int k = 0; k < iters; ++k) {
       const double* aprev = k == 0 ? nullptr : sums + 2 * k - 1;
-      float* ain = auth[k & 1];
-      float* anext = auth[(k + 1) & 1];
+      double* ain = auth[k & 1];
+      double* anext = auth[(k + 1) & 1];
       KL(k_hits_base, grid_for(nv, kBlock))(hub, ain, anext, aprev, java, nv);
       cudaEvent_t* ev = h.kernel_begin();
       // (without decoded timestamps every edge reports t = 0, so the window check is opened fully)
@@ -803,16 +813,18 @@ int tga_hits(tga_graph* gp, int32_t iters, int32_t mode, int64_t t_lo, int64_t t
         KL(k_hits_auth<false>, lean_grid(h))(h.view, lean_work(h), hub, sums + 2 * k, anext, INT64_MIN, INT64_MAX, edges);
       else KL(k_hits_auth<true>, lean_grid(h))(h.view, lean_work(h), hub, sums + 2 * k, anext, t_lo, t_hi, edges);
       h.kernel_end(ev);
-      KL(k_scale, grid_for(nv, kBlock))(hub, sums + 2 * k, hub, nv);
+      KL(k_scale<double>, grid_for(nv, kBlock))(hub, sums + 2 * k, hub, nv);
       KL(k_sumsq, grid_for(nv, kBlock))(anext, nv, sums + 2 * k + 1);
     }
     return TGA_OK;
   }));
-  float* auth_fin = auth[iters & 1];
-  float* out_auth = auth[(iters + 1) & 1];
-  KL(k_scale, grid_for(nv, kBlock))(auth_fin, sums + 2 * iters - 1, out_auth, nv);
-  if (hub_out) cudaMemcpyAsync(hub_out, hub, (size_t)nv * 4, cudaMemcpyDeviceToHost, h.stream);
-  if (auth_out) cudaMemcpyAsync(auth_out, out_auth, (size_t)nv * 4, cudaMemcpyDeviceToHost, h.stream);
+  // FP32 results: the hub as it stands (normalised), the authorities scaled by their last norm.
+  float* hub32 = reinterpret_cast<float*>(auth[(iters + 1) & 1]);
+  float* auth32 = h.s_d.as<float>();
+  KL(k_to_f32, grid_for(nv, kBlock))(hub, hub32, nv);
+  KL(k_scale<float>, grid_for(nv, kBlock))(auth[iters & 1], sums + 2 * iters - 1, auth32, nv);
+  if (hub_out) cudaMemcpyAsync(hub_out, hub32, (size_t)nv * 4, cudaMemcpyDeviceToHost, h.stream);
+  if (auth_out) cudaMemcpyAsync(auth_out, auth32, (size_t)nv * 4, cudaMemcpyDeviceToHost, h.stream);
   h.timing.iterations = iters;
   const int rc = finish(h, edges);
   h.timing.compressed_bytes = (uint64_t)(2 * iters) * pass_bytes(h);

@@ -43,60 +43,70 @@ __host__ __device__ inline LeanEntry lean_entry(int32_t v, uint64_t gbit, uint64
   return e;
 }
 
-// Sequential reader over a big-endian word stream: the next 64 bits at any point are one funnel
-// shift of two registers; consuming past a word loads one more word (clamped to the stream's
-// allocation, whose two trailing words are zero padding).
+// Sequential reader over a big-endian word stream (the graph stream, or the timestamps with
+// kTs): the next 64 bits at any point are one funnel shift of two registers, and a third register
+// holds the word after them, so the load that refills the window is issued a whole word (a code
+// or two) before its bits are needed.  Loads are clamped to the stream's allocation, whose two
+// trailing words are zero padding.
+template <bool kTs>
 struct BitWin {
-  const uint64_t* p;    // next word to load
-  const uint64_t* end;  // one past the last word of the allocation
-  uint64_t a, b;        // current and next word
-  int sh;               // bits of a already consumed (0..63)
+  const uint64_t* p;  // next word to load
+  uint64_t a, b, c;   // current word and the two after it
+  int sh;             // bits of a already consumed (0..63)
 
-  __device__ __forceinline__ void init(const Stream& s, uint64_t pos) {
+  __device__ __forceinline__ static const Stream& st(const GraphView& g) { return kTs ? g.t : g.g; }
+  __device__ __forceinline__ static uint64_t load(const GraphView& g, const uint64_t* q) {
+    const Stream& s = st(g);
+    return q < s.w + s.nwords ? __ldg(q) : 0ull;
+  }
+  __device__ __forceinline__ void init(const GraphView& g, uint64_t pos) {
+    const Stream& s = st(g);
     uint64_t i = pos >> 6;
     const uint64_t last = s.nwords - 2;
     if (i > last) i = last;
-    a = __ldg(s.w + i);
-    b = __ldg(s.w + i + 1);
-    p = s.w + i + 2;
-    end = s.w + s.nwords;
+    const uint64_t* q = s.w + i;
+    a = __ldg(q);
+    b = __ldg(q + 1);
+    c = load(g, q + 2);
+    p = q + 3;
     sh = (int)(pos & 63);
   }
   __device__ __forceinline__ uint64_t window() const {
     // (b >> 1) >> (63 - sh) is b >> (64 - sh) for sh > 0 and 0 for sh == 0, with no branch.
     return (a << sh) | ((b >> 1) >> (63 - sh));
   }
-  __device__ __forceinline__ void skip(int n) {  // n <= 64
+  __device__ __forceinline__ void skip(const GraphView& g, int n) {  // n <= 64
     sh += n;
     if (sh >= 64) {
       sh -= 64;
       a = b;
-      b = p < end ? __ldg(p) : 0ull;
+      b = c;
+      c = load(g, p);
       ++p;
     }
   }
-  // Absolute bit position of the next unread bit (s: the stream the window was opened on).
-  __device__ __forceinline__ uint64_t pos(const Stream& s) const {
-    return ((uint64_t)(p - s.w) - 2) * 64 + (uint64_t)sh;
+  // Absolute bit position of the next unread bit.
+  __device__ __forceinline__ uint64_t pos(const GraphView& g) const {
+    return ((uint64_t)(p - st(g).w) - 3) * 64 + (uint64_t)sh;
   }
   __device__ __forceinline__ uint64_t gamma(const GraphView& g) {
     int len = 0;
     bool bad = false;
     const uint64_t v = win_gamma(window(), &len, &bad);
     if (bad) set_err(g, kErrCode);
-    skip(len);
+    skip(g, len);
     return v;
   }
   __device__ __forceinline__ uint64_t unary(const GraphView& g) {
     const uint64_t w = window();
     if (w == 0) {
       set_err(g, kErrCode);
-      skip(64);
+      skip(g, 64);
       return 0;
     }
     int len = 0;
     const uint64_t v = win_unary(w, &len);
-    skip(len);
+    skip(g, len);
     return v;
   }
   template <int K>
@@ -105,7 +115,7 @@ struct BitWin {
     bool bad = false;
     const uint64_t v = win_zeta<K>(window(), &len, &bad);
     if (bad) set_err(g, kErrCode);
-    skip(len);
+    skip(g, len);
     return v;
   }
 };
@@ -120,8 +130,8 @@ struct LeanCursor {
   int hc;              // copied-values head
   uint32_t cnext, cend;// next copied value to load, end of the list's copied values
   uint64_t mpos, ipos; // next multiples / intervals codes
-  BitWin rr;           // residual gaps
-  BitWin tr;           // timestamp deltas
+  BitWin<false> rr;    // residual gaps
+  BitWin<true> tr;     // timestamp deltas
   int64_t prev;
   int remaining;
 
@@ -129,7 +139,7 @@ struct LeanCursor {
   __device__ __forceinline__ int open(const GraphView& g, int x, uint64_t gbit, uint64_t tbit) {
     hm = hi = hr = hc = kInf;
     remaining = 0;
-    rr.init(g.g, gbit);
+    rr.init(g, gbit);
     const int d = (int)rr.gamma(g);
     if (d <= 0) return 0;
     if (d > g.max_list) {
@@ -163,7 +173,7 @@ struct LeanCursor {
         mrem = (int)rr.gamma(g) + 2;
         mleft = mc - 1;
         extra -= mrem;
-        mpos = rr.pos(g.g);
+        mpos = rr.pos(g);
 #pragma unroll 1
         for (int i = 1; i < mc; ++i) {
           rr.gamma(g);
@@ -183,7 +193,7 @@ struct LeanCursor {
         iend = hi + len;
         ileft = ic - 1;
         extra -= len;
-        ipos = rr.pos(g.g);
+        ipos = rr.pos(g);
 #pragma unroll 1
         for (int i = 1; i < ic; ++i) {
           rr.gamma(g);
@@ -195,7 +205,7 @@ struct LeanCursor {
       rleft = extra;
       hr = x + (int)d_nat2int(rr.template zeta<3>(g));
     }
-    tr.init(g.t, tbit);
+    tr.init(g, tbit);
     prev = g.min_ts;
     remaining = d;
     return d;
@@ -220,8 +230,8 @@ struct LeanCursor {
       cnext = __ldg(g.copy_base + s.v) + (uint32_t)t.emitted + 1;
       cend = __ldg(g.copy_base + s.v + 1);
     }
-    if (hr != kInf) rr.init(g.g, t.rpos);
-    tr.init(g.t, s.tpos);
+    if (hr != kInf) rr.init(g, t.rpos);
+    tr.init(g, s.tpos);
     prev = s.prev;
     remaining = s.count;
     return s.count;
@@ -256,6 +266,26 @@ struct LeanCursor {
     return v;
   }
 
+  // After next() returned y: when the edges that follow repeat y from its multiples run (and no
+  // copied value equals y), consumes them (at most the entry's remaining edges) and returns how
+  // many.  For sweeps that read no timestamps and keep one edge per run of equal successors.
+  __device__ __forceinline__ int skip_repeats(const GraphView& g, int y) {
+    if (hm != y || hc == y) return 0;
+    const int k = min(mrem, remaining);
+    remaining -= k;
+    mrem -= k;
+    if (mrem == 0) {
+      if (mleft > 0) {
+        hm += (int)read_gamma(g, g.g, mpos) + 1;
+        mrem = (int)read_gamma(g, g.g, mpos) + 2;
+        --mleft;
+      } else {
+        hm = kInf;
+      }
+    }
+    return k;
+  }
+
   // Next (successor, timestamp); false once the entry is exhausted (or on a decode error).
   template <bool kTimes>
   __device__ __forceinline__ bool next(const GraphView& g, int& y, int64_t& t) {
@@ -287,8 +317,11 @@ struct LeanWork {
 
 // Sweep driver over a lean schedule: thread i decodes entry i (the schedule groups entries of equal
 // length, so the lanes of a warp finish together).  Hooks and kRuns / kTimes / kRunArg as in
-// run_order (sweep.cuh).
-template <bool kRuns = false, bool kTimes = true, bool kRunArg = false, class Want, class Begin, class Edge, class End>
+// run_order (sweep.cuh).  kSkipRepeats (with kTimes = false, for hooks that keep one edge of each
+// run of equal successors): the repeats of a multiples run after its first edge are consumed
+// without decoding or calling edge(); they still count as decoded edges.
+template <bool kRuns = false, bool kTimes = true, bool kRunArg = false, bool kSkipRepeats = false, class Want,
+          class Begin, class Edge, class End>
 __device__ __forceinline__ unsigned long long run_lean(const GraphView& g, const LeanEntry* entries, int count,
                                                        const SliceState* slices, const int32_t* run_first, Want want,
                                                        Begin begin, Edge edge, End end) {
@@ -321,10 +354,19 @@ __device__ __forceinline__ unsigned long long run_lean(const GraphView& g, const
   if (kRuns) rf.start(lead, first);
   int y;
   int64_t t;
+  static_assert(!(kSkipRepeats && kTimes), "repeats carry their own timestamps");
   while (c.template next<kTimes>(g, y, t)) {
     ++edges;
-    if (kRuns && !rf.pass(y)) continue;
-    if (!edge(x, y, t)) break;
+    const bool pass = !kRuns || rf.pass(y);
+    if (pass && !edge(x, y, t)) break;
+    if constexpr (kSkipRepeats) {
+      // (a slice inside a run whose first kept edge is still ahead keeps decoding edge by edge)
+      if (!kRuns || rf.lead == kNoRunFilter || rf.lead < rf.idx) {
+        const int k = c.skip_repeats(g, y);
+        edges += (unsigned)k;
+        if (kRuns) rf.idx += k;
+      }
+    }
   }
   end(x);
   return edges;

@@ -99,13 +99,13 @@ def test_pagerank_30_fp32_vs_fp64(big):
 def test_hits_30_fp32_vs_fp64(big):
     hub, auth = big.g.hits(30)
     ohub, oauth = big.o.hits(big.ml, big.mv, big.act, 30)
-    # Stated tolerance for FP32 sums over lists and in-lists of up to ~10^5-10^6 terms: unit-L2
-    # vectors; every entry within 1e-3 of the vector's largest entry, and the L1 distance within
-    # 1e-4 of the vector's L1 norm.  (On the small shapes the absolute bound 1e-5 holds.)
+    # Stated tolerance, as on the small shapes: unit-L2 vectors; L1 distance to FP64 <= 1e-4 and
+    # max error <= 1e-5 (the accumulators are FP64; FP32 ones missed this at 2M vertices, where one
+    # authority sums about a million contributions).
     for a, b in ((hub, ohub), (auth, oauth)):
         err = np.abs(a.astype(np.float64) - b)
-        assert float(err.max()) <= 1e-3 * float(np.abs(b).max()), (float(err.max()), float(np.abs(b).max()))
-        assert float(err.sum()) <= 1e-4 * float(np.abs(b).sum()), (float(err.sum()), float(np.abs(b).sum()))
+        assert float(err.sum()) <= 1e-4, float(err.sum())
+        assert float(err.max()) <= 1e-5, float(err.max())
 
 
 def test_degree_centrality(big):
