@@ -291,7 +291,7 @@ __global__ void TGA_LEAN_BOUNDS k_hits_hub(GraphView g, LeanWork lw, double* hub
       },
       [&](int, int y, int64_t t) {
         if (keep_edge(g, lo, hi, y, t, prev_y)) acc += (float)auth_in[y];
-        return true;
+        return 2;  // repeats of y add nothing
       },
       [&](int v) {
         if (acc != 0.0f) atomicAdd(&hub[v], (double)(acc * sa));
@@ -315,7 +315,7 @@ __global__ void TGA_LEAN_BOUNDS k_hits_auth(GraphView g, LeanWork lw, const doub
       },
       [&](int, int y, int64_t t) {
         if (keep_edge(g, lo, hi, y, t, prev_y)) atomicAdd(&auth_next[y], (double)hn);
-        return true;
+        return 2;  // repeats of y add nothing
       },
       [&](int) {});
   add_edges(edges, mine);

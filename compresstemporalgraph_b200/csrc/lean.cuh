@@ -237,18 +237,20 @@ struct LeanCursor {
     return s.count;
   }
 
+  __device__ __forceinline__ void next_multiples_run(const GraphView& g) {
+    if (mleft > 0) {
+      hm += (int)read_gamma(g, g.g, mpos) + 1;
+      mrem = (int)read_gamma(g, g.g, mpos) + 2;
+      --mleft;
+    } else {
+      hm = kInf;
+    }
+  }
+
   __device__ __forceinline__ int next_successor(const GraphView& g) {
     const int v = min(min(hm, hi), min(hr, hc));
     if (v == kInf) return kInf;
-    if (hm == v && --mrem == 0) {
-      if (mleft > 0) {
-        hm += (int)read_gamma(g, g.g, mpos) + 1;
-        mrem = (int)read_gamma(g, g.g, mpos) + 2;
-        --mleft;
-      } else {
-        hm = kInf;
-      }
-    }
+    if (hm == v && --mrem == 0) next_multiples_run(g);
     if (hi == v && ++hi == iend) {
       if (ileft > 0) {
         hi = iend + (int)read_gamma(g, g.g, ipos) + 1;
@@ -266,23 +268,16 @@ struct LeanCursor {
     return v;
   }
 
-  // After next() returned y: when the edges that follow repeat y from its multiples run (and no
-  // copied value equals y), consumes them (at most the entry's remaining edges) and returns how
-  // many.  For sweeps that read no timestamps and keep one edge per run of equal successors.
+  // After next() returned y: when the edges that follow repeat y from its multiples run (hm == y
+  // with mrem copies left; intervals and residuals are strictly increasing, so only a copied value
+  // equal to y could interleave), consumes them (at most the entry's remaining edges) and returns
+  // how many.  For sweeps that read no timestamps.
   __device__ __forceinline__ int skip_repeats(const GraphView& g, int y) {
     if (hm != y || hc == y) return 0;
     const int k = min(mrem, remaining);
     remaining -= k;
     mrem -= k;
-    if (mrem == 0) {
-      if (mleft > 0) {
-        hm += (int)read_gamma(g, g.g, mpos) + 1;
-        mrem = (int)read_gamma(g, g.g, mpos) + 2;
-        --mleft;
-      } else {
-        hm = kInf;
-      }
-    }
+    if (mrem == 0) next_multiples_run(g);
     return k;
   }
 
@@ -316,15 +311,21 @@ struct LeanWork {
 };
 
 // Sweep driver over a lean schedule: thread i decodes entry i (the schedule groups entries of equal
-// length, so the lanes of a warp finish together).  Hooks and kRuns / kTimes / kRunArg as in
-// run_order (sweep.cuh).  kSkipRepeats (with kTimes = false, for hooks that keep one edge of each
-// run of equal successors): the repeats of a multiples run after its first edge are consumed
-// without decoding or calling edge(); they still count as decoded edges.
-template <bool kRuns = false, bool kTimes = true, bool kRunArg = false, bool kSkipRepeats = false, class Want,
-          class Begin, class Edge, class End>
+// length, so the lanes of a warp finish together).  (Measured against a grid of one to two waves in
+// which each thread walks the schedule with the grid's stride and prefetches its next entry: that
+// hid more load latency but its lanes fell out of step, and the PageRank pass took 1.26-1.41 ms
+// against 1.17 ms.)
+// Hooks and kRuns / kTimes / kRunArg as in run_order (sweep.cuh).  kSkip (with kTimes = false):
+// edge() returns an int -- 0 stop the list, 1 go on, 2 go on and the edges that repeat this
+// successor right after it do not matter to the hook: they are consumed without a merge step or a
+// hook call, and count as decoded edges.  (With timestamps the repeats' deltas still have to be
+// decoded one by one, and a per-lane skip loop only makes the warp diverge.)
+template <bool kRuns = false, bool kTimes = true, bool kRunArg = false, bool kSkip = false, class Want, class Begin,
+          class Edge, class End>
 __device__ __forceinline__ unsigned long long run_lean(const GraphView& g, const LeanEntry* entries, int count,
                                                        const SliceState* slices, const int32_t* run_first, Want want,
                                                        Begin begin, Edge edge, End end) {
+  static_assert(!(kSkip && kTimes), "repeats carry their own timestamps");
   unsigned long long edges = 0;
   const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x);
   if (i >= count) return 0;
@@ -354,18 +355,21 @@ __device__ __forceinline__ unsigned long long run_lean(const GraphView& g, const
   if (kRuns) rf.start(lead, first);
   int y;
   int64_t t;
-  static_assert(!(kSkipRepeats && kTimes), "repeats carry their own timestamps");
   while (c.template next<kTimes>(g, y, t)) {
     ++edges;
     const bool pass = !kRuns || rf.pass(y);
-    if (pass && !edge(x, y, t)) break;
-    if constexpr (kSkipRepeats) {
-      // (a slice inside a run whose first kept edge is still ahead keeps decoding edge by edge)
-      if (!kRuns || rf.lead == kNoRunFilter || rf.lead < rf.idx) {
+    if constexpr (kSkip) {
+      if (!pass) continue;
+      const int r = edge(x, y, t);
+      if (r == 0) break;
+      // (a slice inside a run whose kept edge is still ahead goes on edge by edge)
+      if (r == 2 && (!kRuns || rf.lead == kNoRunFilter || rf.lead < rf.idx)) {
         const int k = c.skip_repeats(g, y);
         edges += (unsigned)k;
         if (kRuns) rf.idx += k;
       }
+    } else {
+      if (pass && !edge(x, y, t)) break;
     }
   }
   end(x);

@@ -1,0 +1,84 @@
+// Harness main of the reference GPU programs (see harness_pre.h).  TEST INFRASTRUCTURE ONLY.
+//
+// Runs the reference program's main unchanged, then writes every device buffer it allocated to
+// the file named by $TGA_REF_DUMP: buffers it freed as they were just before cudaFree, buffers it
+// kept as they are after its main returned.  Record layout (little-endian): int32 source line of
+// the allocation, uint64 size in bytes, uint8 1 if freed by the program, uint64 bytes that follow,
+// then those bytes.  Buffers larger than 256 MiB are recorded without their bytes.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
+
+int tga_ref_main();
+
+namespace {
+constexpr size_t kSnapMax = 256u << 20;
+struct Rec {
+  int line;
+  size_t n;
+  void* p;
+  bool live;
+  std::vector<unsigned char> bytes;
+};
+std::vector<Rec>& recs() {
+  static std::vector<Rec> r;
+  return r;
+}
+void snap(Rec& r) {
+  if (r.n > kSnapMax) return;
+  r.bytes.resize(r.n);
+  if (cudaMemcpy(r.bytes.data(), r.p, r.n, cudaMemcpyDeviceToHost) != cudaSuccess) r.bytes.clear();
+}
+}  // namespace
+
+cudaError_t tga_ref_malloc(void** p, size_t n, int line) {
+  const cudaError_t e = cudaMalloc(p, n);
+  if (e == cudaSuccess) recs().push_back(Rec{line, n, *p, true, {}});
+  return e;
+}
+
+cudaError_t tga_ref_free(void* p, int line) {
+  (void)line;
+  for (auto it = recs().rbegin(); it != recs().rend(); ++it) {
+    if (it->live && it->p == p) {
+      cudaDeviceSynchronize();
+      snap(*it);
+      it->live = false;
+      break;
+    }
+  }
+  return cudaFree(p);
+}
+
+int main() {
+  const char* out = std::getenv("TGA_REF_DUMP");
+  if (!out) {
+    std::fprintf(stderr, "TGA_REF_DUMP is not set\n");
+    return 2;
+  }
+  const int rc = tga_ref_main();
+  const cudaError_t sync = cudaDeviceSynchronize();
+  if (sync != cudaSuccess) {
+    std::fprintf(stderr, "reference program ended with a CUDA error: %s\n", cudaGetErrorString(sync));
+    return 3;
+  }
+  FILE* f = std::fopen(out, "wb");
+  if (!f) return 4;
+  for (Rec& r : recs()) {
+    if (r.live) snap(r);
+    const int32_t line = r.line;
+    const uint64_t n = r.n;
+    const uint8_t freed = r.live ? 0 : 1;
+    const uint64_t have = r.bytes.size();
+    std::fwrite(&line, 4, 1, f);
+    std::fwrite(&n, 8, 1, f);
+    std::fwrite(&freed, 1, 1, f);
+    std::fwrite(&have, 8, 1, f);
+    if (have) std::fwrite(r.bytes.data(), 1, have, f);
+  }
+  std::fclose(f);
+  return rc;
+}
