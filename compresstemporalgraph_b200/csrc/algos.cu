@@ -92,9 +92,8 @@ __global__ void TGA_SWEEP_BOUNDS k_decode_csr(GraphView g, LeanWork lw, const in
 }
 
 __global__ void k_neighbors(GraphView g, int32_t v, int32_t* dst, int64_t* ts, int32_t cap, int32_t* count) {
-  DeepState deep;
-  EdgeCursor c(&deep);
-  const int d = c.open(g, v);
+  LeanCursor c;
+  const int d = c.open_vertex(g, v);
   int i = 0, y;
   int64_t t;
   while (c.next(g, y, t)) {
@@ -121,8 +120,7 @@ __global__ void TGA_DECODE_BOUNDS k_is_neighbor(GraphView g, int32_t nq, const i
   const int64_t lo = t_from[i], hi = t_to[i];
   uint8_t found = 0;
   if (x >= 0 && x < g.n && want >= 0) {
-    DeepState deep;
-    EdgeCursor c(&deep);
+    LeanCursor c;
     const int s0 = __ldg(g.slice_first + x), s1 = __ldg(g.slice_first + x + 1);
     int y;
     int64_t t;
@@ -131,14 +129,14 @@ __global__ void TGA_DECODE_BOUNDS k_is_neighbor(GraphView g, int32_t nq, const i
 #pragma unroll 1
       while (a < b) {
         const int mid = (a + b + 1) >> 1;
-        cursor_restore(g, c, g.slices[mid]);
+        c.restore(g, g.slices[mid]);
         if (c.next<false>(g, y, t) && y < want) a = mid;
         else b = mid - 1;
       }
       bool stop = false;
 #pragma unroll 1
       for (int k = a; k < s1 && !stop && !found; ++k) {
-        cursor_restore(g, c, g.slices[k]);
+        c.restore(g, g.slices[k]);
         while (c.next(g, y, t)) {
           if (y < want) continue;
           if (y > want) {
@@ -152,8 +150,8 @@ __global__ void TGA_DECODE_BOUNDS k_is_neighbor(GraphView g, int32_t nq, const i
         }
       }
     } else {
-      c.open(g, x);
-      while (c.next(g, y, t)) {
+      c.open_vertex(g, x);
+      while (c.next<true>(g, y, t)) {
         if (y < want) continue;
         if (y > want) break;
         if (t >= lo && t <= hi) {
@@ -385,9 +383,8 @@ __global__ void TGA_TRAVERSE_BOUNDS k_degree_slices(GraphView g, const SliceStat
   if (j < nslices) {
     const SliceState& sl = slices[j];
     if (sl.v >= g.active_begin && sl.v <= g.max_label) {
-      DeepState deep;
-      EdgeCursor c(&deep);
-      cursor_restore(g, c, sl);
+      LeanCursor c;
+      c.restore(g, sl);
       int64_t* out = buf + ebase[j];
       int y;
       int64_t t;

@@ -178,8 +178,7 @@ __device__ unsigned long long multi_relax_wide(const GraphView& g, MultiArgs& a,
   const uint64_t* Fc = a.F[L & 1];
   uint64_t* Fn = a.F[(L + 1) & 1];
   const int lane = threadIdx.x & 31;
-  DeepState deep;
-  EdgeCursor c(&deep);
+  LeanCursor c;
   unsigned long long edges = 0;
   for (;;) {
     int i = 0;
@@ -428,9 +427,8 @@ __global__ void TGA_DECODE_BOUNDS k_run_first_multi(GraphView g, const SliceStat
   const int2 pr = pairs[p];
   const RunInfo r = runs[pr.x];
   const SliceState& s = slices[pr.y];
-  DeepState deep;
-  EdgeCursor c(&deep);
-  cursor_restore(g, c, s);
+  LeanCursor c;
+  c.restore(g, s);
   uint64_t found[kWords] = {};
   int idx = s.first, y_run = -1, y;
   int64_t t;

@@ -184,6 +184,7 @@ void GraphEncoder::add_node(const int32_t* succ, int outd) {
       if (ref_count_[cand] < params.max_ref_count && list_len_[cand] != 0) {
         BitCounter bc;
         diff_comp(bc, params, scratch_, nullptr, cur, j, list_[cand].data(), list_len_[cand], list_[ci].data(), outd);
+        if (params.no_empty_first_copy && j != 0 && !scratch_.blocks.empty() && scratch_.blocks[0] == 0) continue;
         if ((int64_t)bc.nbits < best) { best = (int64_t)bc.nbits; best_idx = cand; }
       }
     }
@@ -262,6 +263,7 @@ void GraphEncoder::add_block(const int32_t* const* succ, const int* outd, int co
         if (rlen == 0) continue;
         BitCounter bc;
         diff_comp(bc, params, sc, nullptr, (int)v, j, rl, rlen, succ[i], outd[i]);
+        if (params.no_empty_first_copy && j != 0 && !sc.blocks.empty() && sc.blocks[0] == 0) continue;
         cost[(size_t)i * cyc + j] = (int64_t)bc.nbits;
       }
     }

@@ -32,6 +32,10 @@ struct EncoderParams {
   int min_multiple = 2;      // BVMultiGraph.DEFAULT_MIN_MULTIPLE_LENGTH
   int zeta_k = 3;            // BVMultiGraph.DEFAULT_ZETA_K (residuals)
   int ts_zeta_k = 2;         // BaselineRunner.ZETA_K (timestamps)
+  // Never reference a list when the copy mask would start with an empty copy block (a valid
+  // record, but one that the reference's GPU decoder reads differently): for datasets that its
+  // GPU programs must decode as the format defines.
+  bool no_empty_first_copy = false;
 };
 
 struct EncoderStats {

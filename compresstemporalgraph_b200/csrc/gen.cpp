@@ -75,6 +75,9 @@ GenSummary generate_dataset(const GenParams& p, const std::string& dir, const st
   const int32_t hi_id = p.ref_safe ? (int32_t)(n - 2) : (int32_t)(n - 1);
 
   EncoderParams ep;
+  // The reference-safe layout also keeps the reference GPU decoder away from copy masks that start
+  // with an empty copy block.
+  ep.no_empty_first_copy = p.ref_safe;
   GraphEncoder ge(ep);
   TimestampEncoder te(p.min_timestamp, ep.ts_zeta_k);
   FILE* raw = raw_path.empty() ? nullptr : std::fopen(raw_path.c_str(), "w");

@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "engine.hpp"
+#include "leancursor.cuh"
 
 namespace tga {
 
@@ -83,17 +84,17 @@ struct Work {
 
 // Opens queue entry e: a whole list (e >= 0) or one slice.  Returns the vertex; `lead` is the
 // leading-run filter of the entry (see RunFilter).
-__device__ __forceinline__ int open_entry(const GraphView& g, const Work& w, int e, EdgeCursor& c, int& first,
+__device__ __forceinline__ int open_entry(const GraphView& g, const Work& w, int e, LeanCursor& c, int& first,
                                           int& count, int& lead, int& run) {
   lead = kNoRunFilter;
   run = -1;
   if (e >= 0) {
     first = 0;
-    count = c.open(g, e);
+    count = c.open_vertex(g, e);
     return e;
   }
   const SliceState& s = w.slices[-e - 1];
-  cursor_restore(g, c, s);
+  c.restore(g, s);
   first = s.first;
   count = s.count;
   if (s.run >= 0 && w.run_first) lead = __ldg(w.run_first + s.run);
@@ -172,23 +173,22 @@ __device__ __forceinline__ unsigned long long run_order(const GraphView& g, cons
   const int start = kSpread ? spread_warp_rank() * 32 + (int)(threadIdx.x & 31) : (int)(blockIdx.x * blockDim.x + threadIdx.x);
   for (int i = start; i < w.norder; i += gridDim.x * blockDim.x) {
     const int e = w.order[i];
-    DeepState deep;
-    EdgeCursor c(&deep);
+    LeanCursor c;
     RunFilter rf;
     int x, first = 0, count, lead = kNoRunFilter, run = -1;
     if (e >= 0) {
       x = e;
       if (!want(x)) continue;
-      count = c.open(g, x);
+      count = c.open_vertex(g, x);
     } else {
       const SliceState& s = w.slices[-e - 1];
       x = s.v;
       if (!want(x)) continue;
       if (kWhole) {
         if (s.first != 0) continue;
-        count = c.open(g, x);
+        count = c.open_vertex(g, x);
       } else {
-        cursor_restore(g, c, s);
+        c.restore(g, s);
         first = s.first;
         count = s.count;
         if (kRuns && s.run >= 0) lead = __ldg(w.run_first + s.run);
@@ -218,8 +218,7 @@ __device__ __forceinline__ unsigned long long run_order(const GraphView& g, cons
 template <bool kRuns = false, bool kTimes = true, bool kRunArg = false, class Begin, class Edge, class End>
 __device__ __forceinline__ unsigned long long drive_queue(const GraphView& g, const Work& w, const int32_t* q, int qn,
                                                           Begin begin, Edge edge, End end) {
-  DeepState deep;
-  EdgeCursor c(&deep);
+  LeanCursor c;
   RunFilter rf;
   rf.start(kNoRunFilter, 0);
   c.remaining = 0;
@@ -287,9 +286,8 @@ static __global__ void TGA_DECODE_BOUNDS k_run_first(GraphView g, const SliceSta
   const int2 pr = pairs[p];
   const RunInfo r = runs[pr.x];
   const SliceState& s = slices[pr.y];
-  DeepState deep;
-  EdgeCursor c(&deep);
-  cursor_restore(g, c, s);
+  LeanCursor c;
+  c.restore(g, s);
   int idx = s.first, y_run = -1, y;
   int64_t t;
   while (c.next(g, y, t)) {
