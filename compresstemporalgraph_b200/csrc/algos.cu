@@ -397,11 +397,51 @@ __global__ void TGA_TRAVERSE_BOUNDS k_degree_slices(GraphView g, const SliceStat
   add_edges(edges, mine);
 }
 
+// Compaction of each long list's segment to its counted timestamps (one block per list, chunks of
+// the block's size in order: every thread reads its element, a block scan of the counted flags
+// gives the write positions, then the block writes, so writes never pass unread elements); the
+// count goes to cnt[i].  The running mean below then reads its k-th input and the divisor entry of
+// k + 1 at addresses known in advance.
+__global__ void k_degree_compact(const LongList* longs, int32_t nlong, const int32_t* outdeg, int64_t* buf,
+                                 int32_t active, int32_t max_label, int32_t* cnt) {
+  const int i = blockIdx.x;
+  if (i >= nlong) return;
+  const int v = longs[i].v;
+  if (v < active || v > max_label) return;
+  int64_t* p = buf + longs[i].base;
+  const int n = outdeg[v];
+  __shared__ int warp_tot[kBlock / 32];
+  __shared__ int base_s;
+  if (threadIdx.x == 0) base_s = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int c0 = 0; c0 < n; c0 += blockDim.x) {
+    const int k = c0 + (int)threadIdx.x;
+    const int64_t t = k < n ? p[k] : kDcSkip;
+    const int f = t != kDcSkip;
+    const unsigned bal = __ballot_sync(0xffffffffu, f);
+    const int before = __popc(bal & ((1u << lane) - 1u));
+    if (lane == 31) warp_tot[wid] = before + f;
+    __syncthreads();
+    int off = base_s;
+    for (int w = 0; w < wid; ++w) off += warp_tot[w];
+    int total = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) total += warp_tot[w];
+    __syncthreads();  // every thread has read p[k] and the totals
+    if (f) p[off + before] = t;
+    if (threadIdx.x == 0) base_s += total;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) cnt[i] = base_s;
+}
+
 // kNarrow: every timestamp t of the graph satisfies 0 <= t - base < 2^31 (base = the smallest),
 // so the mean is carried as mean - base in 32 bits; t - mean and every intermediate are the same
 // integers as in 64 bits, and the recurrence's critical path is single-word arithmetic.
+// One thread per long list runs the sequential truncating mean over its compacted counted
+// timestamps (the Java mean truncates at every step, so it cannot be split).
 template <bool kNarrow>
-__global__ void k_degree_long(const LongList* longs, int32_t nlong, const int32_t* outdeg, const int64_t* buf,
+__global__ void k_degree_long(const LongList* longs, int32_t nlong, const int32_t* cnt, const int64_t* buf,
                               const uint2* divtab, int64_t base, int32_t active, int32_t max_label, int64_t s,
                               int64_t e, int32_t* deg, int64_t* avg) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -409,26 +449,15 @@ __global__ void k_degree_long(const LongList* longs, int32_t nlong, const int32_
   const int v = longs[i].v;
   if (v < active || v > max_label) return;
   const int64_t* p = buf + longs[i].base;
-  const int n = outdeg[v];
-  int32_t d = 0;
+  const int n = cnt[i];
   int64_t mean = 0;     // 64-bit form
   int32_t mean32 = 0;   // narrow form: mean - base
-  bool first = true;
-  // One step of the truncating mean, mean += (t - mean) / d (Java long division, towards zero);
-  // when |t - mean| < 2^32 the quotient is a multiply-high and two shifts with d's entry ml of the
-  // division table, off the divide sequence on the recurrence's critical path.
-  auto step = [&](int64_t t, uint2 ml) {
-    if (t == kDcSkip) return;
-    ++d;
+  // Step d (the d-th counted timestamp t, d >= 2): mean += (t - mean) / d (Java long division,
+  // towards zero); when |t - mean| < 2^32 the quotient is a multiply-high and two shifts with d's
+  // entry ml of the division table.
+  auto step = [&](int64_t t, uint2 ml, int d) {
     if constexpr (kNarrow) {
-      // The first step sets mean = t (d = 1); afterwards both are within [0, 2^31) of base.
-      const int32_t t32 = (int32_t)(t - base);
-      if (first) {
-        mean32 = t32;
-        first = false;
-        return;
-      }
-      const int32_t a = t32 - mean32;
+      const int32_t a = (int32_t)(t - base) - mean32;
       const uint32_t x = (uint32_t)(a < 0 ? -a : a);
       const uint32_t th = __umulhi(ml.x, x);
       const int32_t q = (int32_t)((th + ((x - th) >> 1)) >> (ml.y - 1));
@@ -438,58 +467,58 @@ __global__ void k_degree_long(const LongList* longs, int32_t nlong, const int32_
       const uint64_t na = (uint64_t)(a < 0 ? -a : a);
       if (na <= 0xFFFFFFFFull) {
         const uint32_t x = (uint32_t)na;
-        uint32_t q = x;
-        if (d > 1) {
-          const uint32_t th = __umulhi(ml.x, x);
-          q = (th + ((x - th) >> 1)) >> (ml.y - 1);
-        }
+        const uint32_t th = __umulhi(ml.x, x);
+        const uint32_t q = (th + ((x - th) >> 1)) >> (ml.y - 1);
         mean += a < 0 ? -(int64_t)q : (int64_t)q;
       } else {
         mean += a / d;
       }
     }
   };
-  // The recurrence is sequential; its inputs are not, so they are loaded a batch ahead: the next
-  // batch's timestamps and the table entries of the counts it reaches are in flight while the
-  // current batch is folded in.
-  constexpr int kBatch = 16;
-  int64_t cur[kBatch], nxt[kBatch];
-  uint2 mcur[kBatch], mnxt[kBatch];
-  auto table_for = [&](const int64_t* tb, int d0, uint2* mt) {
-    int dd = d0;
+  if (n > 0) {
+    // d = 1 sets the mean to the first timestamp.
+    if constexpr (kNarrow) mean32 = (int32_t)(p[0] - base);
+    else mean = p[0];
+  }
+  // Inputs and divisor entries in flight two batches ahead of the recurrence.
+  constexpr int kBatch = 8;
+  int64_t b0[kBatch], b1[kBatch];
+  uint2 m0[kBatch], m1[kBatch];
+  int k = 1;
+  auto load = [&](int at, int64_t* tb, uint2* mb) {
 #pragma unroll
     for (int j = 0; j < kBatch; ++j) {
-      dd += tb[j] != kDcSkip;
-      mt[j] = __ldg(divtab + dd);
+      tb[j] = __ldcs(p + at + j);
+      mb[j] = __ldg(divtab + at + j + 1);
     }
-    return dd;
   };
-  int k = 0;
-  if (n >= kBatch) {
+  if (n - 1 >= 2 * kBatch) {
+    load(1, b0, m0);
+    load(1 + kBatch, b1, m1);
+    for (; k + 3 * kBatch <= n; k += kBatch) {
+      int64_t tb[kBatch];
+      uint2 mb[kBatch];
+      load(k + 2 * kBatch, tb, mb);
 #pragma unroll
-    for (int j = 0; j < kBatch; ++j) cur[j] = __ldcs(p + j);
-    int dnext = table_for(cur, 0, mcur);
-    for (k = kBatch; k + kBatch <= n; k += kBatch) {
-#pragma unroll
-      for (int j = 0; j < kBatch; ++j) nxt[j] = __ldcs(p + k + j);
-      const int dafter = table_for(nxt, dnext, mnxt);
-#pragma unroll
-      for (int j = 0; j < kBatch; ++j) step(cur[j], mcur[j]);
+      for (int j = 0; j < kBatch; ++j) step(b0[j], m0[j], k + j + 1);
 #pragma unroll
       for (int j = 0; j < kBatch; ++j) {
-        cur[j] = nxt[j];
-        mcur[j] = mnxt[j];
+        b0[j] = b1[j];
+        m0[j] = m1[j];
+        b1[j] = tb[j];
+        m1[j] = mb[j];
       }
-      dnext = dafter;
     }
 #pragma unroll
-    for (int j = 0; j < kBatch; ++j) step(cur[j], mcur[j]);
+    for (int j = 0; j < kBatch; ++j) step(b0[j], m0[j], k + j + 1);
+    k += kBatch;
+#pragma unroll
+    for (int j = 0; j < kBatch; ++j) step(b1[j], m1[j], k + j + 1);
+    k += kBatch;
   }
-  for (; k < n; ++k) {
-    const int64_t t = p[k];
-    step(t, __ldg(divtab + d + (t != kDcSkip)));
-  }
-  if constexpr (kNarrow) mean = d > 0 ? base + (int64_t)mean32 : 0;
+  for (; k < n; ++k) step(p[k], __ldg(divtab + k + 1), k + 1);
+  if constexpr (kNarrow) mean = n > 0 ? base + (int64_t)mean32 : 0;
+  int32_t d = n;
   if (s != e) d = (int32_t)(0.85 * d + 0.15 * d * (double)(mean - s) / (double)(e - s) + 1);
   deg[v] = d;
   avg[v] = mean;
@@ -835,7 +864,10 @@ int tga_degree(tga_graph* gp, int64_t t_start, int64_t t_end, int32_t* degree_ou
   const int32_t nv = h.view.max_vertex;
   TGA_TRY(h.s_a.ensure((size_t)nv * 4));
   TGA_TRY(h.s_b.ensure((size_t)nv * 8));
-  if (h.nlong > 0) TGA_TRY(h.s_edges.ensure((size_t)h.long_edges * 8));
+  if (h.nlong > 0) {
+    TGA_TRY(h.s_edges.ensure((size_t)h.long_edges * 8));
+    TGA_TRY(h.s_c.ensure((size_t)h.nlong * 4));
+  }
   TGA_TRY(h.begin_call());
   unsigned long long* edges = edge_counter(h);
   cudaMemsetAsync(h.s_a.p, 0, (size_t)nv * 4, h.stream);
@@ -850,8 +882,11 @@ int tga_degree(tga_graph* gp, int64_t t_start, int64_t t_end, int32_t* degree_ou
     h.kernel_end(ev2);
     // Narrow form when the graph's whole timestamp span fits 31 bits (max_ts found at load).
     const bool narrow = h.max_ts != INT64_MAX && h.min_ts_data >= 0 && h.max_ts - h.min_ts_data < INT32_MAX;
+    int32_t* cnt = h.s_c.as<int32_t>();
+    KL(k_degree_compact, h.nlong)(h.d_long.as<LongList>(), h.nlong, h.d_deg.as<int32_t>(), h.s_edges.as<int64_t>(),
+                                  h.view.active_begin, h.view.max_label, cnt);
     auto long_kernel = narrow ? k_degree_long<true> : k_degree_long<false>;
-    KL(long_kernel, grid_for(h.nlong, kBlock))(h.d_long.as<LongList>(), h.nlong, h.d_deg.as<int32_t>(),
+    KL(long_kernel, grid_for(h.nlong, kBlock))(h.d_long.as<LongList>(), h.nlong, cnt,
                                                h.s_edges.as<int64_t>(), h.d_divtab.as<uint2>(), h.min_ts_data,
                                                h.view.active_begin, h.view.max_label, t_start, t_end,
                                                h.s_a.as<int32_t>(), h.s_b.as<int64_t>());

@@ -5,7 +5,9 @@ programs under oracle/_ref/ are built for exactly this seeded synthetic graph: 6
 120,000 temporal edges, reference chains of depth 3, generated in the reference-safe layout
 (vertex 0 and the largest id receive no edge, the smallest timestamp is 0), which keeps clear of
 the reference decoder's hazards with a first residual equal to 0, a successor equal to MAX_LABEL
-and a timestamp base other than the minTimestamp macro.
+and a timestamp base other than the minTimestamp macro; in that layout the encoder also never
+writes a copy mask whose first copy block is empty (the reference's GPU decoder reads those lists
+differently).
 """
 
 NAME = "refgpu"

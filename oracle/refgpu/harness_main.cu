@@ -80,5 +80,8 @@ int main() {
     if (have) std::fwrite(r.bytes.data(), 1, have, f);
   }
   std::fclose(f);
-  return rc;
+  // The reference's neighbour-access main ends with `return;` in an int function, so its value is
+  // indeterminate; its failures exit(1) from inside (CHECK), so reaching here means it completed.
+  std::printf("harness: reference main returned %d\n", rc);
+  return 0;
 }

@@ -3,19 +3,32 @@ by oracle/refgpu/build_ref.py into oracle/_ref/) run on the same seeded graph as
 their results are compared with the engine's.
 
 The programs' sizes are compile-time macros, so they are built for one dataset (oracle/refgpu/
-config.py: 6,000 vertices, 120,000 temporal edges, reference chains of depth 3, reference-safe
-layout).  Each program reads the reference's file layout under $TGA_COMPRESS_ROOT: the dataset
-files written by the engine's encoder, and the decode tables gammaInA.txt / zetaInA.txt written
-from the engine's regenerated tables (equal to the reference's files, test_codes_golden.py).  The
-harness copies every device buffer back (oracle/refgpu/harness_main.cu); the compared buffers are
-found by the source line of their allocation (oracle/_ref/manifest.json).
+config.py: 6,000 vertices, 120,000 temporal edges, reference chains of depth 3, 5,432 copied arcs,
+generated in the reference-safe layout).  Each program reads the reference's file layout under
+$TGA_COMPRESS_ROOT: the dataset files written by the engine's encoder, and the decode tables
+gammaInA.txt / zetaInA.txt written from the engine's regenerated tables (equal to the reference's
+files, test_codes_golden.py).  The harness copies every device buffer back (oracle/refgpu/
+harness_main.cu); the compared buffers are found by the source line of their allocation
+(oracle/_ref/manifest.json).
 
-Compared: BFS arrival times (bit-exact), connected-component labels (bit-exact), colouring
-priorities and colours (bit-exact), neighbour access's small-list flags (bit-exact), PageRank
-and HITS (FP64 in the reference, FP32 in the engine; tolerances stated below).  Degree centrality
-is not compared: the reference program calls it with the window (0, 0), for which its kernel
-evaluates `(s == e) == 0` as false and counts only edges with timestamp 0, and its centrality step
-then divides by e - s = 0 (gpu_cuda/shared/degree_centrality.cu:1444,1630).
+Compared, bit-exact: BFS arrival times, neighbour access's small-list flags, colouring priorities
+(cuRAND) and colours, connected-component labels of every vertex the engine reaches.  PageRank and
+HITS (FP64 in the reference, FP32 per edge in the engine) within the tolerances stated below.
+
+Where the reference differs by construction, and what the comparison does about it:
+  * connected components: only the first label is initialised (`cudaMemset(component, 0,
+    sizeof(int))`, connected_components.cu), so a vertex no seed reaches reads as component 0 there
+    (memory a fresh allocation leaves zero) and as -1 in the engine;
+  * PageRank: getNewRank returns before resetting newRank[u] for u >= MAX_LABEL
+    (pagerank.cu:1618-1621), so vertex MAX_LABEL keeps a stale value that enters every
+    normalisation; it is left out and both vectors renormalised over [0, MAX_LABEL);
+  * degree centrality is not compared: the program calls it with the window (0, 0), for which its
+    kernel evaluates `(s == e) == 0` as false and counts only edges with timestamp 0, and its
+    centrality step divides by e - s = 0 (degree_centrality.cu:1444,1630);
+  * the reference-safe layout also keeps the encoder from copy masks whose first copy block is
+    empty: the reference's GPU decoder reads those lists differently from the format (measured on
+    a dataset that has them: shifted timestamps after the copied part, and its exhausted-list value
+    MAX_LABEL emitted as a successor).
 
 Skipped when oracle/_ref/ holds no built programs (the reference checkout was absent at build).
 """
@@ -130,8 +143,12 @@ def test_connected_components_equal_the_reference(setup):
     root, g = setup
     b = run_program(root, "connected_components")
     comp = np.frombuffer(b["component"], np.int32)
-    lab, _ = g.connected_components()
-    assert np.array_equal(comp, lab)
+    lab, k = g.connected_components()
+    reached = lab >= 0
+    assert k >= 1 and int(reached.sum()) > N // 2
+    assert np.array_equal(comp[reached], lab[reached])
+    # Vertices no seed reaches: never written by the reference (its fresh allocation reads 0).
+    assert np.all(comp[~reached] == 0)
 
 
 def test_coloring_equals_the_reference(setup):
@@ -149,11 +166,14 @@ def test_pagerank_close_to_the_reference(setup):
     root, g = setup
     b = run_program(root, "pagerank")
     ref = np.frombuffer(b["Rank"], np.float64)
-    r = g.pagerank(refcfg.PR_ITERS)
-    # Stated tolerance: the reference sums in FP64 and its iteration resets the next vector while
-    # other blocks may still scatter into it (pagerank.cu:1590,1621), the engine sums in FP32; L1
-    # distance <= 1e-4 of the rank mass.
-    l1 = float(np.abs(r.astype(np.float64) - ref).sum())
+    r = g.pagerank(refcfg.PR_ITERS).astype(np.float64)
+    # Vertex MAX_LABEL (= N - 1) is stale in the reference; both vectors renormalised without it.
+    a, c = r[: N - 1] / r[: N - 1].sum(), ref[: N - 1] / ref[: N - 1].sum()
+    # Stated tolerance: L1 <= 1e-4 of the rank mass.  The reference sums in FP64 but resets each
+    # vertex's next rank in the same kernel that other blocks scatter into (pagerank.cu:1621 against
+    # :1590), so a contribution that lands before its target's reset is lost; the engine resets
+    # before the scatter and sums in FP32.  (Measured: 2.5e-5.)
+    l1 = float(np.abs(a - c).sum())
     assert l1 <= 1e-4, l1
 
 
@@ -163,7 +183,8 @@ def test_hits_close_to_the_reference(setup):
     hub = np.frombuffer(b["hub"], np.float64)
     auth = np.frombuffer(b["authority"], np.float64)
     h, a = g.hits(refcfg.HITS_ITERS, tga.HITS_GPU)
-    # Stated tolerance: unit-L2 vectors, L1 distance <= 1e-4 each.
+    # Stated tolerance: unit-L2 vectors, L1 distance <= 1e-4 each (the engine's FP32 arithmetic per
+    # edge; the FP64 oracle equals the reference to 2e-14).
     for x, y in ((h, hub), (a, auth)):
         l1 = float(np.abs(x.astype(np.float64) - y).sum())
         assert l1 <= 1e-4, l1
