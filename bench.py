@@ -10,9 +10,11 @@ per launch / its average launch time against the measured HBM copy bandwidth.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
   python bench.py --batched-graph batched      # batched form alone on the 20M/500M graph
+  python bench.py --skew-graph skew            # HITS x30 + colouring on the 100M/2B skew graph
 
-The line also carries the batched form (256 windowed BFS + 32 windowed PageRanks against one query
-per call), the served form (open-loop queries through the server against plain calls), a second
+The line also carries the batched form at its own size (256 windowed BFS + 32 windowed PageRanks
+against one query per call on the 20M-vertex / 500M-edge graph, generated on the machine on first
+use), the served form (open-loop queries through the server against plain calls), a second
 GTEPS figure over the workloads that read the timestamp stream, and the FP32 PageRank/HITS error
 against the FP64 oracle at this configuration (computed after the timed regions).
 
@@ -402,6 +404,36 @@ def served_section(tga, graphs, spans, load, count):
                                              for k, name in kinds.items()}}}
 
 
+def batched_at_size(tga, g_tune, name: str) -> dict:
+    """The batched form on its named configuration (20M vertices / 500M temporal edges by default),
+    generated on this machine if absent: the project autotuner runs on the benchmark graph g_tune
+    (the 2M/40M one; tuning the 20M graph itself would take minutes) and its slice length and item
+    size are applied to the large graph, whose batched section then runs with plain calls timed on
+    a sample (16 BFS, 4 PageRanks) and scaled."""
+    p = tga.CONFIGS[name]
+    ddir = Path(tempfile.gettempdir()) / f"tga_bench_{name}"
+    t0 = time.perf_counter()
+    if not (ddir / f"{name}.graph").exists():
+        tga.generate(p, ddir, name)
+    gen_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    tune = g_tune.autotune()
+    tune["wall_s"] = time.perf_counter() - t0
+    n = int(p.n)
+    t0 = time.perf_counter()
+    big = tga.Graph.open_dir(ddir, name, tga.DatasetConfig(name=name, max_label=n - 1, max_vertex=n))
+    load_s = time.perf_counter() - t0
+    try:
+        big.set_work_params(tune["slice_edges"], tune["item_edges"])
+        sec = batched_section(tga, big, n, int(p.ts_span), tune=False, plain_bfs=16, plain_pr=4)
+    finally:
+        big.close()
+    sec["autotune"] = dict(tune, applied="slice length and item size, tuned on the benchmark graph")
+    sec["config"] = {"workload": name, "vertices": n, "temporal_edges": int(p.m)}
+    sec["generate_s"], sec["load_s"] = gen_s, load_s
+    return sec
+
+
 def run_batched_scale(args):
     """Batched form alone on a named configuration (the 20M/500M one by default): generated here,
     loaded, one batched section with plain calls timed on a sample.  Prints one JSON line."""
@@ -471,6 +503,53 @@ def reference_step(o, n: int, deg, src: int, prio, threads: int) -> dict:
     timed("DC", lambda: o.stream_degree(ml, mv, act, 0, 0, threads=threads)[1])
     timed("GC", lambda: o.stream_color(ml, mv, act, prio, threads=threads)[1])
     return out
+
+
+def run_skew(args):
+    """Skew stress on its named configuration (100M vertices / 2B temporal edges, Zipf 1.6, 16 hubs of
+    5M out-edges, bursty timestamps): generated on this machine if absent, loaded, then HITS x30 and
+    Jones-Plassmann colouring (cuRAND priorities) timed as the benchmark times its steps (device
+    time, W warm-up and K timed runs).  Prints one JSON line.  Parity at this shape, scaled down 100x,
+    is tests/test_gpu_bench_config.py's skew1m case."""
+    import compresstemporalgraph_b200 as tga
+
+    name = args.skew_graph
+    p = tga.CONFIGS[name]
+    ddir = Path(tempfile.gettempdir()) / f"tga_bench_{name}"
+    t0 = time.perf_counter()
+    summary = None
+    if not (ddir / f"{name}.graph").exists():
+        summary = tga.generate(p, ddir, name)
+    gen_s = time.perf_counter() - t0
+    n = int(p.n)
+    t0 = time.perf_counter()
+    g = tga.Graph.open_dir(ddir, name, tga.DatasetConfig(name=name, max_label=n - 1, max_vertex=n))
+    load_s = time.perf_counter() - t0
+    info = g.info
+    out = {}
+    for wl, fn in (("HITS", lambda: g.hits(30, outputs=False)), ("GC", lambda: g.color(0, outputs=False))):
+        for _ in range(args.warmup):
+            fn()
+        ms = edges = 0.0
+        for _ in range(args.steps):
+            fn()
+            t = g.timing()
+            ms += t["total_ms"]
+            edges += t["edges_decoded"]
+        out[wl] = {"ms": ms / args.steps, "edges": int(edges / args.steps), "gteps": edges / (ms / 1e3) / 1e9}
+    _, _, deg = g.neighbor_access()
+    g.close()
+    tot_edges = sum(v["edges"] for v in out.values())
+    tot_ms = sum(v["ms"] for v in out.values())
+    line = {"metric": "GTEPS on compressed graph (skew stress: HITS x30 + JP colouring)", "value": tot_edges / tot_ms / 1e6,
+            "unit": "GTEPS", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "data": "synthetic", "config": {"workload": name, "vertices": n, "temporal_edges": int(p.m),
+                                            "hubs": int(p.hub_count), "hub_degree": int(p.hub_degree),
+                                            "largest_list": int(deg.max()), "compressed_bytes": info["graph_bytes"] +
+                                            info["timestamp_bytes"] + info["index_bytes"]},
+            "workloads": out, "generate_s": gen_s, "load_s": load_s, "summary": summary, "info": info}
+    print(json.dumps(line), flush=True)
+    return 0
 
 
 def run_reference(args):
@@ -545,8 +624,12 @@ def main():
     ap.add_argument("--served-count", type=int, default=300)
     ap.add_argument("--served-graphs", default="small,served1m",
                     help="resident graphs of the served section besides the benchmark graph (configuration names)")
+    ap.add_argument("--batched-config", default="batched",
+                    help="configuration of the line's batched section (default: batched, 20M/500M; '' skips it)")
     ap.add_argument("--batched-graph", default=None,
                     help="run only the batched section on this generated configuration (e.g. batched: 20M/500M)")
+    ap.add_argument("--skew-graph", default=None,
+                    help="run only the skew-stress section on this generated configuration (e.g. skew: 100M/2B)")
     ap.add_argument("--only", choices=["RA", "BFS", "CC", "PR", "HITS", "DC", "GC"],
                     help="run one workload per step (for profiling; the line is not the benchmark)")
     args = ap.parse_args()
@@ -556,6 +639,8 @@ def main():
         return run_reference(args)
     if args.batched_graph:
         return run_batched_scale(args)
+    if args.skew_graph:
+        return run_skew(args)
 
     import torch
 
@@ -660,7 +745,6 @@ def main():
     }
     if rank == 0 and not args.no_forms and not ONLY:
         try:
-            line["batched"] = batched_section(tga, g, n, int(tga.CONFIGS[CONFIG_NAME].ts_span))
             extra = []
             names = [nm for nm in args.served_graphs.split(",") if nm and nm != CONFIG_NAME]
             for name in names:
@@ -675,6 +759,11 @@ def main():
                 gg.close()
         except Exception as e:  # reported, not fatal
             line["served_error"] = str(e)
+        if args.batched_config:
+            try:
+                line["batched"] = batched_at_size(tga, g, args.batched_config)
+            except Exception as e:  # reported, not fatal
+                line["batched_error"] = str(e)
     if rank == 0 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(ddir, summary, 0)

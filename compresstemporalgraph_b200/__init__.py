@@ -80,7 +80,8 @@ class _GenParams(C.Structure):
     _fields_ = [("n", C.c_int64), ("m", C.c_int64), ("deg_exponent", C.c_double), ("max_degree", C.c_int64),
                 ("repeat_frac", C.c_double), ("local_frac", C.c_double), ("local_radius", C.c_int32),
                 ("pref_frac", C.c_double), ("copy_frac", C.c_double), ("ts_kind", C.c_int32),
-                ("ts_span", C.c_int64), ("min_timestamp", C.c_int64), ("seed", C.c_uint64), ("ref_safe", C.c_int32)]
+                ("ts_span", C.c_int64), ("min_timestamp", C.c_int64), ("seed", C.c_uint64), ("ref_safe", C.c_int32),
+                ("hub_count", C.c_int32), ("hub_degree", C.c_int64)]
 
 
 class _RefDepths(C.Structure):
@@ -576,6 +577,8 @@ class GenParams:
     min_timestamp: int = 0
     seed: int = 1
     ref_safe: bool = False
+    hub_count: int = 0       # this many vertices get exactly hub_degree out-edges each
+    hub_degree: int = 0
 
 
 # Synthetic stand-ins for the benchmark configurations (the real datasets are absent).
@@ -596,9 +599,11 @@ CONFIGS = {
     "served10m": GenParams(n=10_000_000, m=200_000_000, deg_exponent=2.0, max_degree=200_000, repeat_frac=0.30,
                            local_frac=0.70, local_radius=64, pref_frac=0.5, copy_frac=0.20, ts_kind=1,
                            ts_span=100_000_000, seed=4),
+    # Skew stress: Zipf 1.6 out-degrees plus 16 hubs of 5M out-edges each (block-scale lists), bursty
+    # timestamps (10% of the edges in 1% of the span).
     "skew": GenParams(n=100_000_000, m=2_000_000_000, deg_exponent=1.6, max_degree=5_000_000, repeat_frac=0.30,
                       local_frac=0.70, local_radius=64, pref_frac=0.5, copy_frac=0.20, ts_kind=2,
-                      ts_span=100_000_000, seed=5),
+                      ts_span=100_000_000, seed=5, hub_count=16, hub_degree=5_000_000),
 }
 
 

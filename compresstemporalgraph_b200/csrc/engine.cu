@@ -432,7 +432,7 @@ int build_work(GraphHandle& h, int32_t slice_len, int32_t item_edges) {
   if (int rc = publish_view(h)) return rc;
   const int32_t nd = (int32_t)h.degrees.size();
   std::vector<int32_t> big_v;
-  std::vector<int64_t> slot_base{0};
+  std::vector<int64_t> slot_base{0}, deep_base{0};
   for (int32_t x = 0; x < nd; ++x) {
     const int32_t d = h.degrees[(size_t)x];
     // Long lists are sliced; so is every list that copies from a reference chain, whatever its
@@ -441,7 +441,10 @@ int build_work(GraphHandle& h, int32_t slice_len, int32_t item_edges) {
     // opening is kept as a checkpoint (a single slice when the list is short).
     if (d > slice_len || (d > 0 && h.chain_host[(size_t)x])) {
       big_v.push_back(x);
-      slot_base.push_back(slot_base.back() + (d + slice_len - 1) / slice_len);
+      const int64_t nslot = (d + slice_len - 1) / slice_len;
+      slot_base.push_back(slot_base.back() + nslot);
+      // Chain levels only for the slices of lists that copy from a chain.
+      deep_base.push_back(deep_base.back() + (h.chain_host[(size_t)x] ? nslot : 0));
     }
   }
   const int32_t nbig = (int32_t)big_v.size();
@@ -449,26 +452,27 @@ int build_work(GraphHandle& h, int32_t slice_len, int32_t item_edges) {
   std::vector<SliceState> slices;
   std::vector<DeepState> slice_deep_tmp;
   if (nbig) {
-    DevBuf bv, sb, ns, tmp, tmpd;
+    DevBuf bv, sb, db, ns, tmp, tmpd;
     int rc;
-    if ((rc = bv.ensure((size_t)nbig * 4)) || (rc = sb.ensure(slot_base.size() * 8)) || (rc = ns.ensure((size_t)nbig * 4)) ||
-        (rc = tmp.ensure((size_t)slot_base.back() * sizeof(SliceState))) ||
-        (rc = tmpd.ensure((size_t)slot_base.back() * sizeof(DeepState))))
+    if ((rc = bv.ensure((size_t)nbig * 4)) || (rc = sb.ensure(slot_base.size() * 8)) || (rc = db.ensure(deep_base.size() * 8)) ||
+        (rc = ns.ensure((size_t)nbig * 4)) || (rc = tmp.ensure((size_t)slot_base.back() * sizeof(SliceState))) ||
+        (rc = tmpd.ensure((size_t)std::max<int64_t>(1, deep_base.back()) * sizeof(DeepState))))
       return rc;
+    TGA_CUDA_TRY(cudaMemcpyAsync(db.p, deep_base.data(), deep_base.size() * 8, cudaMemcpyHostToDevice, h.stream));
     TGA_CUDA_TRY(cudaMemcpyAsync(bv.p, big_v.data(), (size_t)nbig * 4, cudaMemcpyHostToDevice, h.stream));
     TGA_CUDA_TRY(cudaMemcpyAsync(sb.p, slot_base.data(), slot_base.size() * 8, cudaMemcpyHostToDevice, h.stream));
-    k_build_slices<<<grid_for(nbig, 64), 64, 0, h.stream>>>(v, bv.as<int32_t>(), sb.as<int64_t>(), nbig, slice_len,
+    k_build_slices<<<grid_for(nbig, 64), 64, 0, h.stream>>>(v, bv.as<int32_t>(), sb.as<int64_t>(), db.as<int64_t>(), nbig, slice_len,
                                                            tmp.as<SliceState>(), tmpd.as<DeepState>(), ns.as<int32_t>());
     TGA_CUDA_TRY(cudaGetLastError());
     slices.resize((size_t)slot_base.back());
     TGA_CUDA_TRY(cudaMemcpyAsync(nsl.data(), ns.p, (size_t)nbig * 4, cudaMemcpyDeviceToHost, h.stream));
     TGA_CUDA_TRY(cudaMemcpyAsync(slices.data(), tmp.p, slices.size() * sizeof(SliceState), cudaMemcpyDeviceToHost,
                                  h.stream));
-    slice_deep_tmp.resize((size_t)slot_base.back());
+    slice_deep_tmp.resize((size_t)deep_base.back());
     TGA_CUDA_TRY(cudaMemcpyAsync(slice_deep_tmp.data(), tmpd.p, slice_deep_tmp.size() * sizeof(DeepState),
                                  cudaMemcpyDeviceToHost, h.stream));
     if ((rc = h.check_device_error())) return rc;
-    bv.release(); sb.release(); ns.release(); tmp.release(); tmpd.release();
+    bv.release(); sb.release(); db.release(); ns.release(); tmp.release(); tmpd.release();
   }
   // Compact the slices, build slice_first and the work items (slices first, then short lists).
   std::vector<SliceState> packed;
@@ -483,10 +487,11 @@ int build_work(GraphHandle& h, int32_t slice_len, int32_t item_edges) {
         for (int32_t j = 0; j < nsl[(size_t)b]; ++j) {
           items.push_back(WorkItem{x, x + 1, (int32_t)packed.size()});
           const size_t slot = (size_t)(slot_base[(size_t)b] + j);
+          const size_t dslot = (size_t)(deep_base[(size_t)b] + j);
           SliceState sl = slices[slot];
           if (sl.chain) {
             sl.deep = (int32_t)packed_deep.size();
-            packed_deep.push_back(slice_deep_tmp[slot]);
+            packed_deep.push_back(slice_deep_tmp[dslot]);
           }
           packed.push_back(sl);
         }

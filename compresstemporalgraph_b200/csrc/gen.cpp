@@ -43,8 +43,14 @@ GenSummary generate_dataset(const GenParams& p, const std::string& dir, const st
   if (p.n < 4 || p.m < 1) throw std::runtime_error("generator needs n >= 4 and m >= 1");
   const int64_t n = p.n;
   Rng rng(p.seed);
-  // Out-degrees: Pareto weights with tail exponent (zipf-1), capped, scaled to exactly m.
+  // Out-degrees: Pareto weights with tail exponent (zipf-1), capped, scaled to exactly m; with hubs,
+  // hub_count vertices spread over the id range take hub_degree edges each and the others share the
+  // rest.
   std::vector<int64_t> deg((size_t)n, 0);
+  const int64_t nhub = p.hub_degree > 0 ? std::max<int64_t>(0, std::min<int64_t>(p.hub_count, n - 2)) : 0;
+  if (nhub * p.hub_degree >= p.m) throw std::runtime_error("hubs hold more edges than m");
+  auto hub_vertex = [&](int64_t k) { return (int64_t)(((2 * k + 1) * (n - 1)) / (2 * nhub)); };
+  const int64_t m_rest = p.m - nhub * p.hub_degree;
   {
     std::vector<double> w((size_t)n);
     const double a = std::max(0.05, p.deg_exponent - 1.0);
@@ -54,16 +60,18 @@ GenSummary generate_dataset(const GenParams& p, const std::string& dir, const st
       double u = rng.uniform();
       if (u < 1e-300) u = 1e-300;
       w[(size_t)v] = std::min(cap, std::pow(u, -1.0 / a));
-      tot += w[(size_t)v];
     }
+    for (int64_t k = 0; k < nhub; ++k) w[(size_t)hub_vertex(k)] = 0.0;
+    for (int64_t v = 0; v < n; ++v) tot += w[(size_t)v];
     long double cum = 0;
     int64_t prev = 0;
     for (int64_t v = 0; v < n; ++v) {
       cum += w[(size_t)v];
-      const int64_t c = (int64_t)std::llround((long double)p.m * cum / tot);
+      const int64_t c = (int64_t)std::llround((long double)m_rest * cum / tot);
       deg[(size_t)v] = c - prev;
       prev = c;
     }
+    for (int64_t k = 0; k < nhub; ++k) deg[(size_t)hub_vertex(k)] = p.hub_degree;
     // Make the largest id a source so that n = max id + 1 holds even with no in-edges to it.
     if (deg[(size_t)n - 1] == 0) {
       const auto it = std::max_element(deg.begin(), deg.end());

@@ -22,6 +22,8 @@ struct GenParams {
   int64_t min_timestamp = 0;    // forced to occur once
   uint64_t seed = 1;
   bool ref_safe = false;        // no in-edges to vertex 0 and to vertex n-1
+  int32_t hub_count = 0;        // this many vertices, spread over the id range, get exactly
+  int64_t hub_degree = 0;       // hub_degree out-edges each; the others share the remaining edges
 };
 
 struct GenSummary {

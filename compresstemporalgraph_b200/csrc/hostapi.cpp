@@ -139,6 +139,8 @@ int tga_generate(const tga_gen_params* p, const char* dir, const char* base, con
   g.min_timestamp = p->min_timestamp;
   g.seed = p->seed;
   g.ref_safe = p->ref_safe != 0;
+  g.hub_count = p->hub_count;
+  g.hub_degree = p->hub_degree;
   if (g.n > INT32_MAX || g.ts_span <= 0 || g.min_timestamp < 0 || g.ts_span > (INT64_C(1) << 62) ||
       g.min_timestamp > (INT64_C(1) << 62))
     return fail(TGA_E_ARG, "vertex ids must fit in [0, 2^31) and timestamps in [0, 2^63)");

@@ -50,13 +50,16 @@ __device__ __forceinline__ void cursor_save(const EdgeCursor& c, SliceState& s, 
 // One thread per long list: walks the list once and records a slice every `len` edges.  A slice
 // that starts inside a run of equal successors gets run = the list index where that run starts
 // (the host turns it into a run index).  cap[b] slots are reserved per list.
-static __global__ void k_build_slices(GraphView g, const int32_t* big_v, const int64_t* slot_base, int32_t nbig, int32_t len,
-                               SliceState* out, DeepState* deep_out, int32_t* nslices) {
+// Chain levels go to deep_out + deep_base[b] (deep_base[b + 1] - deep_base[b] is the list's slot count when it
+// copies from a chain, 0 otherwise: cursor_save writes them only for such lists).
+static __global__ void k_build_slices(GraphView g, const int32_t* big_v, const int64_t* slot_base,
+                                      const int64_t* deep_base, int32_t nbig, int32_t len, SliceState* out,
+                                      DeepState* deep_out, int32_t* nslices) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= nbig) return;
   const int v = big_v[b];
   SliceState* dst = out + slot_base[b];
-  DeepState* ddst = deep_out + slot_base[b];
+  DeepState* ddst = deep_out + deep_base[b];
   const int cap = (int)(slot_base[b + 1] - slot_base[b]);
   DeepState deep, saved_deep;
   EdgeCursor c(&deep);

@@ -358,6 +358,8 @@ typedef struct {
   int64_t ts_span, min_timestamp;
   uint64_t seed;
   int32_t ref_safe;               /* no in-edges to vertex 0 and n-1 */
+  int32_t hub_count;              /* hubs: this many vertices, spread over the id range, get */
+  int64_t hub_degree;             /* exactly hub_degree out-edges each (0: none) */
 } tga_gen_params;
 
 typedef struct {

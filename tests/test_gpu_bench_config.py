@@ -1,6 +1,6 @@
 """Parity at the benchmarked size: the seven workloads exactly as bench.py runs them on the
-2M-vertex / 40M-edge "all7" graph, and on a hub-stress graph whose largest list holds more than a
-million edges, against the CPU oracle.
+2M-vertex / 40M-edge "all7" graph, on a hub-stress graph whose largest list holds more than a
+million edges, and on the skew-stress configuration scaled down 100x, against the CPU oracle.
 
 Integer results (checksums, arrivals, hop counts, components, degrees, means, colours) must be
 bit-exact; PageRank and HITS (FP32 on the GPU, FP64 in the oracle) carry the tolerances stated
@@ -22,7 +22,12 @@ pytestmark = pytest.mark.gpu
 # bursty timestamps (10% of the edges in 1% of the span).
 HUB1M = tga.GenParams(n=3000, m=5_000_000, deg_exponent=1.5, max_degree=4_000_000, repeat_frac=0.3, local_frac=0.7,
                       local_radius=64, pref_frac=0.5, copy_frac=0.3, ts_kind=2, ts_span=100_000_000, seed=31)
-SHAPES = {"all7": tga.CONFIGS["all7"], "hub1m": HUB1M}
+# The skew-stress configuration scaled down 100x: 1M vertices, 20M temporal edges, Zipf 1.6 out-degrees,
+# two hubs of 500,000 out-edges, bursty timestamps.
+SKEW1M = tga.GenParams(n=1_000_000, m=20_000_000, deg_exponent=1.6, max_degree=100_000, repeat_frac=0.3, local_frac=0.7,
+                       local_radius=64, pref_frac=0.5, copy_frac=0.2, ts_kind=2, ts_span=100_000_000, seed=5,
+                       hub_count=2, hub_degree=500_000)
+SHAPES = {"all7": tga.CONFIGS["all7"], "hub1m": HUB1M, "skew1m": SKEW1M}
 
 
 class Big:
@@ -58,8 +63,10 @@ def big(request, tmp_path_factory):
 def test_shape_is_what_it_claims(big):
     if big.cfg.name == "all7":
         assert big.summary["m"] == 40_000_000 and big.n == 2_000_000
-    else:
+    elif big.cfg.name == "hub1m":
         assert big.deg.max() >= 1_000_000
+    else:
+        assert big.n == 1_000_000 and int((big.deg == 500_000).sum()) == 2
     assert big.summary["max_chain"] == 3
 
 
