@@ -120,6 +120,7 @@ def _load() -> C.CDLL:
         "tga_bfs": (C.c_int, [P, C.c_int32, C.c_int64, C.c_int64, P, P]),
         "tga_cc": (C.c_int, [P, C.c_int64, C.c_int64, C.c_int32, P, C.POINTER(C.c_int32)]),
         "tga_pagerank": (C.c_int, [P, C.c_int32, C.c_float, C.c_float, C.c_int64, C.c_int64, P]),
+        "tga_shortest": (C.c_int, [P, C.c_int32, C.c_int64, C.c_int64, P, P]),
         "tga_pagerank_noalloc": (C.c_int, [P, C.c_int32, C.c_float, C.c_float, C.c_int64, C.c_int64, P]),
         "tga_hits": (C.c_int, [P, C.c_int32, C.c_int32, C.c_int64, C.c_int64, P, P]),
         "tga_degree": (C.c_int, [P, C.c_int64, C.c_int64, P, P]),
@@ -397,6 +398,13 @@ class Graph:
         out = np.zeros((len(src), self.max_vertex), np.int32)
         _check(_lib.tga_bfs_batch(self._h, len(src), _ptr(src), _ptr(lo), _ptr(hi), _ptr(out)))
         return out
+
+    def shortest(self, src: int, t_lo: int = 0, t_hi: int = T_MAX):
+        """Fewest-hop temporal paths from src (tga_shortest): (hops, earliest arrival)."""
+        hops = np.zeros(self.max_vertex, np.int32)
+        arr = np.zeros(self.max_vertex, np.int32)
+        _check(_lib.tga_shortest(self._h, src, t_lo, t_hi, _ptr(hops), _ptr(arr)))
+        return hops, arr
 
     def fastest(self, src: int, t_lo: int = 0, t_hi: int = T_MAX):
         """Fastest temporal paths from src (tga_fastest): (duration, departure) per vertex, -1 where

@@ -193,3 +193,148 @@ extern "C" int tga_latest_departure(tga_graph* rev, int64_t pivot, int32_t targe
     return fail(TGA_E_OOM, "host allocation failed");
   }
 }
+
+// ---------------------------------------------------------------------------------------------
+// Fewest-hop temporal paths (temporal_ligra apps/temporal/Shortest-Compute.C asks for the shortest
+// time-respecting paths from a source within [start, end]; its update keeps a label only when it is
+// both earlier and shorter, which depends on the visiting order).  Here the value is exact: hops[v]
+// = the fewest edges on a time-respecting path from src to v within [t_lo, t_hi), with tga_bfs's
+// edge rule (edge (x->y, t) usable when arrival(x) <= t, first in-window occurrence of equal
+// consecutive successors).  Level-synchronous relaxation:
+//     A_k[v] = min(A_{k-1}[v], min over usable edges (x->v, t) with A_{k-1}[x] <= t of t),
+// where only the vertices whose A dropped at level k-1 are expanded, reading A_{k-1} (prev) while
+// writing A_k (next) with RED.MIN, so every level is deterministic; hops[v] is the first k with
+// A_k[v] finite, and the last A is the earliest arrival (tga_bfs's).
+#include "sweep.cuh"
+
+namespace tga {
+
+namespace {
+
+constexpr uint32_t kSpInf = 0xFFFFFFFFu;
+
+struct SpArgs {
+  const uint32_t* prev;
+  uint32_t* next;
+  uint32_t* dirty;
+  int64_t lo, hi;
+  unsigned long long* edges;
+};
+
+__global__ void TGA_TRAVERSE_BOUNDS k_sp_relax(GraphView g, Work w, SpArgs a, const int32_t* q, int32_t qn) {
+  uint32_t ax = kSpInf;
+  int prev_y = -1;
+  const unsigned long long mine = drive_queue<true>(
+      g, w, q, qn,
+      [&](int x, int, int) {
+        if (x < g.active_begin || x > g.max_label) return false;
+        ax = __ldcg(a.prev + x);
+        prev_y = -1;
+        return ax != kSpInf;
+      },
+      [&](int, int y, int64_t t) {
+        if (!keep_edge(g, a.lo, a.hi, y, t, prev_y)) return true;
+        if ((int64_t)ax > t || t >= (int64_t)kSpInf) return true;
+        if (atomicMin(a.next + y, (uint32_t)t) > (uint32_t)t) atomicOr(a.dirty + (y >> 5), 1u << (y & 31));
+        return true;
+      },
+      [](int) {});
+  add_edges(a.edges, mine);
+}
+
+// After level `level`: every vertex whose arrival dropped takes it, gets its hop count if it was
+// unreached, and joins the next queue (itself, or all its slices).
+__global__ void k_sp_scan(Work w, uint32_t* prev, const uint32_t* next, uint32_t* dirty, int32_t* hops, int32_t nwords,
+                          int32_t level, int32_t* q, int32_t* qcnt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nwords) return;
+  uint32_t bits = dirty[i];
+  if (!bits) return;
+  dirty[i] = 0;
+  while (bits) {
+    const int b = __ffs(bits) - 1;
+    bits &= bits - 1;
+    const int y = i * 32 + b;
+    if (prev[y] == kSpInf) hops[y] = level;
+    prev[y] = next[y];
+    enqueue(w, y, q, qcnt);
+  }
+}
+
+__global__ void k_sp_unpack(const uint32_t* prev, int32_t* arr, int32_t n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) arr[i] = prev[i] == kSpInf ? INT32_MAX : (int32_t)prev[i];
+}
+
+}  // namespace
+
+static int tga_shortest_impl(tga_graph* gp, int32_t src, int64_t t_lo, int64_t t_hi, int32_t* hops_out,
+                             int32_t* arrival_out) {
+  TGA_TRACE("tga_shortest");
+  if (!gp) return fail(TGA_E_ARG, "null graph");
+  GraphHandle& h = *gp;
+  const int32_t nv = h.view.max_vertex;
+  if (src < 0 || src >= nv) return fail(TGA_E_ARG, "source out of range");
+  if (t_lo >= t_hi) return fail(TGA_E_ARG, "empty time window");
+  const int32_t nwords = (nv + 31) / 32;
+  const size_t qcap = (size_t)nv + (size_t)h.nslices + 1;
+  TGA_TRY(h.s_a.ensure((size_t)nv * 4));
+  TGA_TRY(h.s_b.ensure((size_t)nv * 4));
+  TGA_TRY(h.s_c.ensure((size_t)nv * 4));
+  TGA_TRY(h.s_d.ensure((size_t)nwords * 4));
+  TGA_TRY(h.s_q0.ensure(qcap * 4));
+  TGA_TRY(h.s_q1.ensure(qcap * 4));
+  TGA_TRY(h.s_cnt.ensure(64));
+  TGA_TRY(h.begin_call());
+  prepare_runs(h, t_lo, t_hi);
+  unsigned long long* edges = edge_counter(h);
+  uint32_t* prev = h.s_a.as<uint32_t>();
+  uint32_t* next = h.s_b.as<uint32_t>();
+  int32_t* hops = h.s_c.as<int32_t>();
+  uint32_t* dirty = h.s_d.as<uint32_t>();
+  int32_t* q[2] = {h.s_q0.as<int32_t>(), h.s_q1.as<int32_t>()};
+  int32_t* qcnt = h.s_cnt.as<int32_t>();
+  cudaMemsetAsync(prev, 0xFF, (size_t)nv * 4, h.stream);
+  cudaMemsetAsync(next, 0xFF, (size_t)nv * 4, h.stream);
+  KL(k_fill_i32, grid_for(nv, kBlock))(hops, INT32_MAX, nv);
+  cudaMemsetAsync(dirty, 0, (size_t)nwords * 4, h.stream);
+  const uint32_t start = (uint32_t)(t_lo > 0 ? std::min<int64_t>(t_lo, (int64_t)kSpInf - 1) : 0);
+  const int32_t zero = 0;
+  TGA_CUDA_TRY(cudaMemcpyAsync(prev + src, &start, 4, cudaMemcpyHostToDevice, h.stream));
+  TGA_CUDA_TRY(cudaMemcpyAsync(next + src, &start, 4, cudaMemcpyHostToDevice, h.stream));
+  TGA_CUDA_TRY(cudaMemcpyAsync(hops + src, &zero, 4, cudaMemcpyHostToDevice, h.stream));
+  std::vector<int32_t> first;
+  int32_t qn = src < h.view.n ? seed_entries(h, src, first) : 0;
+  if (qn) TGA_CUDA_TRY(cudaMemcpyAsync(q[0], first.data(), (size_t)qn * 4, cudaMemcpyHostToDevice, h.stream));
+  const SpArgs a{prev, next, dirty, t_lo, t_hi, edges};
+  int32_t level = 0;
+  for (; qn > 0; ++level) {
+    if (level >= nv) return fail(TGA_E_TIMEOUT, "tga_shortest: more levels than vertices");
+    const Work w = work_of(h);
+    TGA_CUDA_TRY(cudaMemsetAsync(qcnt, 0, 4, h.stream));
+    cudaEvent_t* ev = h.kernel_begin();
+    KL(k_sp_relax, decode_grid(h, qn))(h.view, w, a, q[level & 1], qn);
+    h.kernel_end(ev);
+    KL(k_sp_scan, grid_for(nwords, kBlock))(w, prev, next, dirty, hops, nwords, level + 1, q[(level + 1) & 1], qcnt);
+    TGA_CUDA_TRY(cudaMemcpyAsync(&h.h_pinned[20], qcnt, 4, cudaMemcpyDeviceToHost, h.stream));
+    TGA_CUDA_TRY(cudaStreamSynchronize(h.stream));
+    qn = (int32_t)h.h_pinned[20];
+  }
+  int32_t* arr = reinterpret_cast<int32_t*>(next);  // next is no longer needed
+  KL(k_sp_unpack, grid_for(nv, kBlock))(prev, arr, nv);
+  if (hops_out) cudaMemcpyAsync(hops_out, hops, (size_t)nv * 4, cudaMemcpyDeviceToHost, h.stream);
+  if (arrival_out) cudaMemcpyAsync(arrival_out, arr, (size_t)nv * 4, cudaMemcpyDeviceToHost, h.stream);
+  h.timing.iterations = level;
+  return finish(h, edges);
+}
+
+}  // namespace tga
+
+extern "C" int tga_shortest(tga_graph* g, int32_t src, int64_t t_lo, int64_t t_hi, int32_t* hops_out,
+                            int32_t* arrival_out) {
+  try {
+    return tga::tga_shortest_impl(g, src, t_lo, t_hi, hops_out, arrival_out);
+  } catch (const std::bad_alloc&) {
+    return fail(TGA_E_OOM, "host allocation failed in tga_shortest");
+  }
+}

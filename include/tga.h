@@ -242,6 +242,15 @@ int tga_bfs_batch(tga_graph* g, int32_t nsrc, const int32_t* src, const int64_t*
 int tga_fastest(tga_graph* g, int32_t src, int64_t t_lo, int64_t t_hi, int64_t* duration_out,
                 int64_t* departure_out);
 
+/* Fewest-hop temporal paths (temporal_ligra apps/temporal/Shortest-Compute.C, whose update keeps a
+ * label only when it is both earlier and shorter and so depends on the visiting order; here the
+ * value is exact): hops_out[v] = the fewest edges on a time-respecting path from src to v within
+ * [t_lo, t_hi) under tga_bfs's edge rule (INT32_MAX when unreached), arrival_out[v] = the earliest
+ * arrival (equal to tga_bfs's).  Computed by level-synchronous relaxation: level k expands only the
+ * vertices whose earliest arrival over at most k-1 edges dropped at level k-1.  Either output may
+ * be NULL. */
+int tga_shortest(tga_graph* g, int32_t src, int64_t t_lo, int64_t t_hi, int32_t* hops_out, int32_t* arrival_out);
+
 /* Latest departures towards one target (temporal_ligra apps/temporal/LatestDeparture-Compute.C,
  * "reverse foremost", which transposes the graph).  tga_reverse writes a time-reversed copy of g to
  * <dir>/<base>.* with its index files: edge (x -> y, t) becomes (y -> x, pivot - t); pivot < 0 ->

@@ -755,6 +755,54 @@ int32_t orc_color(orc* o, int32_t max_label, int32_t max_vertex, int32_t active,
   return color_core(o, max_label, max_vertex, active, prio, java_isolated, color, 0, NULL);
 }
 
+/* Fewest-hop temporal paths: hops[v] = the fewest edges on a time-respecting path from src to v
+ * within [lo, hi) (edge (x->y, t) usable when arr(x) <= t, BFS's edge rule), arr[v] = the earliest
+ * arrival.  Level-synchronous relaxation: A_k[v] = min(A_{k-1}[v], min over usable edges (x->v, t)
+ * with A_{k-1}[x] <= t of t), expanding only the vertices whose A dropped at level k-1; hops[v] is the
+ * first k with A_k[v] finite. */
+void orc_shortest(orc* o, int32_t max_label, int32_t max_vertex, int32_t active, int32_t src, int64_t lo, int64_t hi,
+                  int32_t* arr, int32_t* hops) {
+  orc_cfg c = {max_label, max_vertex, active};
+  (void)c;
+  int64_t* prev = (int64_t*)malloc((size_t)max_vertex * 8);
+  int64_t* next = (int64_t*)malloc((size_t)max_vertex * 8);
+  int32_t* fr = (int32_t*)malloc((size_t)max_vertex * 4);
+  int32_t* nf = (int32_t*)malloc((size_t)max_vertex * 4);
+  uint8_t* mark = (uint8_t*)calloc((size_t)max_vertex, 1);
+  const int64_t INF = INT64_MAX;
+  for (int32_t i = 0; i < max_vertex; ++i) { prev[i] = next[i] = INF; hops[i] = ORC_INF32; }
+  prev[src] = next[src] = lo > 0 ? lo : 0;
+  hops[src] = 0;
+  int64_t fn = 0;
+  fr[fn++] = src;
+  for (int32_t level = 1; fn > 0 && level <= max_vertex; ++level) {
+    int64_t nn = 0;
+    for (int64_t i = 0; i < fn; ++i) {
+      const int32_t x = fr[i];
+      if (x < active || x > max_label || x >= o->n) continue;
+      const int64_t ax = prev[x];
+      FOR_DEDUP_EDGES(o, x, lo, hi, y, t, {
+        if (y < active || y >= max_vertex) continue;
+        if (ax > t || t >= 0xFFFFFFFFll) continue;
+        if (t < next[y]) {
+          next[y] = t;
+          if (!mark[y]) { mark[y] = 1; nf[nn++] = y; }
+        }
+      });
+    }
+    for (int64_t i = 0; i < nn; ++i) {
+      const int32_t y = nf[i];
+      mark[y] = 0;
+      if (prev[y] == INF) hops[y] = level;
+      prev[y] = next[y];
+    }
+    int32_t* tmp = fr; fr = nf; nf = tmp;
+    fn = nn;
+  }
+  for (int32_t i = 0; i < max_vertex; ++i) arr[i] = prev[i] == INF ? ORC_INF32 : (int32_t)prev[i];
+  free(prev); free(next); free(fr); free(nf); free(mark);
+}
+
 /* java.util.Random(seed).nextInt(256) sequence (documented JDK LCG). */
 void orc_java_random256(int64_t seed, int32_t n, uint32_t* out) {
   uint64_t s = ((uint64_t)seed ^ 0x5DEECE66Dull) & ((1ull << 48) - 1);

@@ -51,6 +51,7 @@ def _load() -> C.CDLL:
         "orc_stream_hits": (i64, [P, i32, i32, i32, i32, i32, P, P, i32]),
         "orc_stream_degree": (i64, [P, i32, i32, i32, i64, i64, P, P, i32]),
         "orc_stream_color": (i64, [P, i32, i32, i32, P, i32, P, P, i32]),
+        "orc_shortest": (None, [P, i32, i32, i32, i32, i64, i64, P, P]),
         "orc_max_threads": (i32, []),
         "orc_read_codes": (i64, [P, i64, i32, i32, P, i64]),
         "orc_ef_get": (C.c_uint64, [P, P, i64, i32, i64]),
@@ -143,6 +144,13 @@ class Oracle:
         hops = np.zeros(max_vertex, np.int32)
         self.L.orc_bfs(self.h, max_label, max_vertex, active, src, lo, hi, _p(arr), _p(hops))
         return arr, hops
+
+    def shortest(self, max_label, max_vertex, active, src, lo=0, hi=INT64_MAX):
+        """Fewest-hop temporal paths from src: (hops, earliest arrival)."""
+        arr = np.zeros(max_vertex, np.int32)
+        hops = np.zeros(max_vertex, np.int32)
+        self.L.orc_shortest(self.h, max_label, max_vertex, active, src, lo, hi, _p(arr), _p(hops))
+        return hops, arr
 
     def cc(self, max_label, max_vertex, active, begin, lo=0, hi=INT64_MAX, early_exit=True):
         lab = np.zeros(max_vertex, np.int32)

@@ -591,3 +591,33 @@ def test_latest_departure(pairs, shape, tmp_path):
                 assert np.array_equal(got, want), (target, lo, hi)
         with pytest.raises(tga.TgaError):
             grev.latest_departure(pivot, 0, 5, 5)
+
+
+# ---- fewest-hop temporal paths --------------------------------------------------------------
+
+# widespan is left out: arrivals are 32-bit times, as in tga_bfs.
+@pytest.mark.parametrize("shape", ["small", "chains", "hubs", "intervals", "sparse", "refsafe", "small_view"])
+def test_shortest_paths(pairs, shape):
+    p = pairs[shape]
+    off, _, _ = p.o.csr()
+    degs = np.diff(off)
+    srcs = [int(np.argmax(degs)), max(p.act, 1), p.act + 7]
+    for src in srcs:
+        for lo, hi in _windows(p):
+            hops, arr = p.g.shortest(src, lo, hi)
+            ohops, oarr = p.o.shortest(p.ml, p.mv, p.act, src, lo, hi)
+            assert np.array_equal(hops, ohops), (src, lo, hi)
+            assert np.array_equal(arr, oarr), (src, lo, hi)
+            # The earliest arrival is tga_bfs's, and no path is longer than the one along earliest arrivals.
+            barr, bhops = p.g.bfs(src, lo, hi)
+            assert np.array_equal(arr, barr)
+            r = hops != np.iinfo(np.int32).max
+            assert (hops[r] <= bhops[r]).all()
+
+
+def test_shortest_paths_rejects_bad_input(pairs):
+    p = pairs["small"]
+    with pytest.raises(tga.TgaError):
+        p.g.shortest(0, 10, 10)
+    with pytest.raises(tga.TgaError):
+        p.g.shortest(p.mv)
