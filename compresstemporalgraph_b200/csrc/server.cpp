@@ -1,15 +1,18 @@
 // Served form: several resident graphs answer a stream of (algorithm, source, window) queries.
 //
-// One worker thread per graph repeatedly takes the queries that arrived since its last round,
-// admits them while the device working memory they need fits the server's budget (shared by all
-// graphs), and runs them together: the BFS queries as one batched traversal (tga_bfs_batch), the
-// PageRank queries as one strided vector (tga_pagerank_batch_iters, each with its own iteration
-// count).  CC
-// queries join the graph's resumable CC job (tga_cc_job_*, up to 32 windows in flight): each round
-// advances it by one time slice, so a long CC never holds back the short queries that arrive
-// meanwhile, and every window is published the moment it finishes.  Each graph's work runs on that
-// graph's own stream, so rounds of different graphs overlap on the device.  Latency is measured
-// from tga_submit to the moment the result is in the caller's buffer.
+// One worker thread per graph takes turns on the device with the others: the graph holding the
+// oldest outstanding query goes first, so across graphs the queries are served in arrival order.
+// A graph's turn serves the kind of its oldest waiting query together with every other waiting
+// query of that kind, admitted while the device working memory they need fits the server's budget
+// (shared by all graphs): BFS queries as one batched traversal (tga_bfs_batch), PageRank queries as
+// one strided vector (tga_pagerank_batch_iters, each with its own iteration count), CC windows as
+// one multi-window seed loop (the CC job, up to 32 windows, run to completion), point queries as one
+// launch.  A query therefore never waits behind work that arrived after it, except for the
+// same-kind queries that join its batch, which cost little (a batched traversal decodes each list
+// once per level for all its sources).  Turns run one at a time: the traversal kernels are
+// cooperative launches that occupy every SM, so rounds of different graphs could not overlap on the
+// device anyway.  Latency is measured from tga_submit to the moment the result is in the caller's
+// buffer.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -51,22 +54,12 @@ struct GraphSlot {
   std::deque<Pending> pending;
   std::thread worker;
   tga_cc_job* cc = nullptr;                 // created at the first CC query
-  std::vector<Pending> cc_slot;             // query in each job slot (ticket 0: free)
-  std::deque<Pending> cc_waiting;           // admitted CC queries waiting for a free job slot
   bool wants_device = false;                // has a round to run (guarded by the server mutex)
   Clock::time_point oldest{};               // submit time of its oldest outstanding query
 };
 
+// CC windows per round (the job's capacity).
 constexpr int32_t kCcJobWindows = 32;
-// Windows in flight per graph.  Windows sharing a job split its source slots, so each finishes
-// later while the throughput stays about the same; a short first-come queue keeps the tail low.
-constexpr int32_t kCcInFlight = 2;
-// Device time of a CC job step, by age: the step lasts until the oldest non-CC query waiting for
-// the next round would be as old as the oldest CC window (at least kCcSliceMs), or kCcIdleMs when
-// nothing else waits.  Across kinds that is first come first served, while BFS and PageRank still
-// batch within their kind.
-constexpr double kCcSliceMs = 15.0;
-constexpr double kCcIdleMs = 100.0;
 
 // Device working bytes of one query (per vertex of its graph): BFS arrival + last-enqueued arrival
 // + result; PageRank three rank vectors + inverse degree + result; CC the single traversal's arrays.
@@ -95,8 +88,7 @@ struct tga_server {
 
   void worker(GraphSlot* slot);
   void run_round(GraphSlot* slot, std::vector<Pending>& round);
-  void step_cc(GraphSlot* slot, double budget_ms);
-  double cc_budget_ms(GraphSlot* slot);
+  void run_cc(GraphSlot* slot, std::vector<Pending>& round);
   void publish(const std::vector<const Pending*>& done, const std::vector<int>& status);
 };
 
@@ -184,132 +176,71 @@ void tga_server::run_round(GraphSlot* slot, std::vector<Pending>& round) {
       publish(done, std::vector<int>(done.size(), rc));
     }
   }
-  for (const Pending& p : round)
-    if (p.q.kind == TGA_Q_CC) slot->cc_waiting.push_back(p);
+  run_cc(slot, round);
 }
 
-// Moves waiting CC windows into free job slots, advances the job by one slice and publishes the
-// windows that finished.  A job error fails every window in flight and drops the job.
-void tga_server::step_cc(GraphSlot* slot, double budget_ms) {
-  std::vector<const Pending*> done;
-  std::vector<int> status;
-  std::vector<Pending> failed_now;
+// CC windows of the round: added to the graph's CC job and run to completion in one step; each
+// window's labels go straight to its query's buffer.  A job error fails these windows and drops the
+// job (the next CC round makes a new one).
+void tga_server::run_cc(GraphSlot* slot, std::vector<Pending>& round) {
+  std::vector<const Pending*> cc;
+  for (const Pending& p : round)
+    if (p.q.kind == TGA_Q_CC) cc.push_back(&p);
+  if (cc.empty()) return;
   int rc = TGA_OK;
-  if (!slot->cc && !slot->cc_waiting.empty()) {
-    rc = tga_cc_job_create(slot->g, kCcJobWindows, TGA_CC_EARLY_EXIT, &slot->cc);
-    if (rc == TGA_OK) slot->cc_slot.assign(kCcJobWindows, Pending{});
-  }
-  int32_t inflight_now = 0;
-  for (const Pending& p : slot->cc_slot) inflight_now += p.ticket != 0;
-  while (rc == TGA_OK && !slot->cc_waiting.empty() && inflight_now < kCcInFlight) {
-    int32_t s = -1;
-    const Pending& p = slot->cc_waiting.front();
-    const int arc = tga_cc_job_add(slot->cc, p.q.t_lo, p.q.t_hi, &s);
-    if (arc == TGA_E_AGAIN) break;  // job full: wait for a slot
-    if (arc != TGA_OK) {
-      rc = arc;
-      break;
-    }
-    slot->cc_slot[(size_t)s] = p;
-    slot->cc_waiting.pop_front();
-    ++inflight_now;
-  }
-  bool inflight = false;
-  for (const Pending& p : slot->cc_slot) inflight |= p.ticket != 0;
+  if (!slot->cc) rc = tga_cc_job_create(slot->g, kCcJobWindows, TGA_CC_EARLY_EXIT, &slot->cc);
+  std::vector<int32_t> slot_of(cc.size(), -1);
+  for (size_t k = 0; k < cc.size() && rc == TGA_OK; ++k) rc = tga_cc_job_add(slot->cc, cc[k]->q.t_lo, cc[k]->q.t_hi, &slot_of[k]);
   uint32_t finished = 0;
-  if (rc == TGA_OK && inflight) rc = tga_cc_job_step(slot->cc, budget_ms, &finished);
-  std::vector<Pending> out_list;
+  if (rc == TGA_OK) rc = tga_cc_job_step(slot->cc, 0.0, &finished);  // budget 0: to completion
+  std::vector<int> status(cc.size(), rc);
   if (rc == TGA_OK) {
-    for (int32_t s = 0; s < kCcJobWindows; ++s)
-      if (finished & (1u << s)) {
-        Pending& p = slot->cc_slot[(size_t)s];
-        const int trc = tga_cc_job_take(slot->cc, s, static_cast<int32_t*>(p.q.out), nullptr);
-        out_list.push_back(p);
-        status.push_back(trc);
-        p = Pending{};
-      }
+    for (size_t k = 0; k < cc.size(); ++k)
+      status[k] = (finished >> slot_of[k]) & 1u
+                      ? tga_cc_job_take(slot->cc, slot_of[k], static_cast<int32_t*>(cc[k]->q.out), nullptr)
+                      : TGA_E_CUDA;
   } else {
-    for (Pending& p : slot->cc_slot)
-      if (p.ticket != 0) {
-        out_list.push_back(p);
-        status.push_back(rc);
-        p = Pending{};
-      }
-    while (!slot->cc_waiting.empty()) {
-      out_list.push_back(slot->cc_waiting.front());
-      status.push_back(rc);
-      slot->cc_waiting.pop_front();
-    }
     if (slot->cc) tga_cc_job_destroy(slot->cc);
     slot->cc = nullptr;
   }
-  for (const Pending& p : out_list) done.push_back(&p);
-  if (!done.empty()) publish(done, status);
-}
-
-static bool cc_busy(const GraphSlot* slot) {
-  if (!slot->cc_waiting.empty()) return true;
-  for (const Pending& p : slot->cc_slot)
-    if (p.ticket != 0) return true;
-  return false;
-}
-
-double tga_server::cc_budget_ms(GraphSlot* slot) {
-  bool have_cc = false;
-  Clock::time_point cc_oldest{};
-  for (const Pending& p : slot->cc_slot)
-    if (p.ticket != 0 && (!have_cc || p.submitted < cc_oldest)) {
-      cc_oldest = p.submitted;
-      have_cc = true;
-    }
-  if (!slot->cc_waiting.empty() && (!have_cc || slot->cc_waiting.front().submitted < cc_oldest)) {
-    cc_oldest = slot->cc_waiting.front().submitted;
-    have_cc = true;
-  }
-  if (!have_cc) return kCcSliceMs;
-  std::lock_guard<std::mutex> lk(mu);
-  bool have_other = false;
-  Clock::time_point other{};
-  for (const auto& o : graphs)
-    for (const Pending& p : o->pending)  // arrival order: the first non-CC one is the oldest
-      if (p.q.kind != TGA_Q_CC) {
-        if (!have_other || p.submitted < other) other = p.submitted;
-        have_other = true;
-        break;
-      }
-  if (!have_other) return kCcIdleMs;
-  return std::max(kCcSliceMs, std::chrono::duration<double, std::milli>(other - cc_oldest).count());
+  publish(cc, status);
 }
 
 void tga_server::worker(GraphSlot* slot) {
   std::unique_lock<std::mutex> lk(mu);
   for (;;) {
-    // CC windows in flight keep the worker going without waiting for new queries.
-    work_cv.wait(lk, [&] { return stopping || !slot->pending.empty() || cc_busy(slot); });
-    if (slot->pending.empty() && !cc_busy(slot)) {
+    work_cv.wait(lk, [&] { return stopping || !slot->pending.empty(); });
+    if (slot->pending.empty()) {
       if (stopping) break;
       continue;
     }
-    // Admit queued queries while they fit the budget (at least one when nothing else runs).
+    // The kind of the oldest waiting query, with every other waiting query of that kind, admitted
+    // while they fit the budget (at least one when nothing else runs); CC at most a job's windows.
+    const int32_t kind = slot->pending.front().q.kind;
     std::vector<Pending> round;
+    std::deque<Pending> rest;
+    bool full = false;
     while (!slot->pending.empty()) {
-      const Pending& p = slot->pending.front();
-      if (in_use + p.bytes > budget && !(round.empty() && in_use == 0)) break;
+      Pending p = slot->pending.front();
+      slot->pending.pop_front();
+      if (full || p.q.kind != kind || (kind == TGA_Q_CC && (int32_t)round.size() >= kCcJobWindows) ||
+          (in_use + p.bytes > budget && !(round.empty() && in_use == 0))) {
+        if (p.q.kind == kind && !round.empty()) full = full || in_use + p.bytes > budget;
+        rest.push_back(p);
+        continue;
+      }
       in_use += p.bytes;
       round.push_back(p);
-      slot->pending.pop_front();
     }
-    if (round.empty() && !cc_busy(slot)) {  // the budget is held by other graphs: wait until some is released
+    slot->pending.swap(rest);
+    if (round.empty()) {  // the budget is held by other graphs: wait until some is released
       work_cv.wait(lk);
       continue;
     }
-    // Device turn: rounds of different graphs run one at a time, the graph holding the oldest
-    // outstanding query first, so a query is not overtaken by newer work on another graph.
+    // Device turn: the graph holding the oldest outstanding query first.
     Clock::time_point oldest = Clock::time_point::max();
     for (const Pending& p : round) oldest = std::min(oldest, p.submitted);
-    for (const Pending& p : slot->cc_waiting) oldest = std::min(oldest, p.submitted);
-    for (const Pending& p : slot->cc_slot)
-      if (p.ticket != 0) oldest = std::min(oldest, p.submitted);
+    for (const Pending& p : slot->pending) oldest = std::min(oldest, p.submitted);
     slot->oldest = oldest;
     slot->wants_device = true;
     turn_cv.wait(lk, [&] {
@@ -324,7 +255,6 @@ void tga_server::worker(GraphSlot* slot) {
     running += (int64_t)round.size();
     lk.unlock();
     run_round(slot, round);
-    step_cc(slot, cc_budget_ms(slot));
     lk.lock();
     device_busy = false;
     turn_cv.notify_all();

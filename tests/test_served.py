@@ -105,3 +105,33 @@ def test_served_rejects_queries_beyond_budget(datasets):
             assert e.value.code == tga.TGA_E_OOM
     finally:
         g.close()
+
+
+def test_served_live_arrivals_equal_plain(datasets):
+    """Queries keep arriving while earlier rounds run on the device (a CC window first, then batches
+    of BFS and PageRank joined by queries submitted while they are in flight): every result equals
+    the plain single-query call, and the server ran many rounds rather than one batch."""
+    import time
+
+    rng = np.random.default_rng(31)
+    graphs = [_open(datasets["chains"]), _open(datasets["hubs"])]
+    try:
+        with tga.Server(budget_bytes=1 << 30) as srv:
+            gids = [srv.add_graph(g) for g in graphs]
+            queries = [dict(kind=tga.Q_CC, graph=gids[1], t_lo=0, t_hi=T_MAX)]
+            queries += _mix(rng, gids[0], datasets["chains"], 40) + _mix(rng, gids[1], datasets["hubs"], 40)
+            tickets = []
+            for k, q in enumerate(queries):
+                tickets.append(srv.submit(**q))
+                if k % 5 == 4:
+                    time.sleep(0.003)  # the next queries arrive while the last round runs
+            srv.drain()
+            results = [srv.poll(t)[0] for t in tickets]
+            st = srv.stats()
+            assert st["completed"] == len(queries) and st["failed"] == 0
+            assert st["rounds"] >= 8, st["rounds"]
+        for q, r in zip(queries, results):
+            assert _same(q, _plain(graphs[q["graph"]], q), r), q
+    finally:
+        for g in graphs:
+            g.close()
