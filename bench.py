@@ -15,8 +15,9 @@ per launch / its average launch time against the measured HBM copy bandwidth.
 The line also carries the batched form at its own size (256 windowed BFS + 32 windowed PageRanks
 against one query per call on the 20M-vertex / 500M-edge graph, generated on the machine on first
 use), the served form (open-loop queries through the server against plain calls), a second
-GTEPS figure over the workloads that read the timestamp stream, and the FP32 PageRank/HITS error
-against the FP64 oracle at this configuration (computed after the timed regions).
+GTEPS figure over the workloads that read the timestamp stream, the FP32 PageRank/HITS error
+against the FP64 oracle at this configuration (computed after the timed regions), and the
+reference's own GPU programs timed beside the engine on the small graph they are built for.
 
 --impl reference is the CPU arm: the same graph (generated in a child process, so the engine's
 library is never loaded there) and the same seven-workload step, run by the C port of the
@@ -242,6 +243,78 @@ def fp64_check(ddir: Path, summary: dict, pr, hub, auth, bfs_src: int) -> dict:
     return {"pagerank_x30": err(pr, opr), "hits_x30_hub": err(hub, ohub), "hits_x30_auth": err(auth, oauth),
             "tolerance": "PageRank L1 <= 1e-5 of the rank mass; HITS max <= 1e-5 per entry (tests)",
             "oracle_s": round(time.time() - t, 1)}
+
+
+REF_GPU_PROGRAMS = {  # reference program -> the engine's call for the same workload on the same graph
+    "neighbor_access": ("RA", lambda g, c: g.neighbor_access(outputs=False)),
+    "bfs": ("BFS", lambda g, c: g.bfs(c.BFS_SOURCE, outputs=False)),
+    "connected_components": ("CC", lambda g, c: g.connected_components(outputs=False)),
+    "pagerank": ("PR", lambda g, c: g.pagerank(c.PR_ITERS, outputs=False)),
+    "hits": ("HITS", lambda g, c: g.hits(c.HITS_ITERS, outputs=False)),
+    "graph_coloring": ("GC", lambda g, c: g.color(0, outputs=False)),
+}
+
+
+def ref_gpu_section(tga) -> dict:
+    """The reference's own GPU programs beside the engine, on one GPU and one graph (a baseline leg,
+    like cpu_baseline; their results are compared with the engine's in tests/test_reference_gpu.py).
+
+    The programs (gpu_cuda/shared/<algorithm>.cu, built unchanged into oracle/_ref/ with sizes
+    compiled in) run on the 6,000-vertex / 120,000-edge dataset they were built for; their harness
+    brackets every kernel launch with events and reports the device time per kernel.  The engine's
+    figure is the device time of the same workload through its public call, best of 5 after a
+    warm-up.  Skipped when oracle/_ref/ holds no programs."""
+    ref = ROOT / "oracle" / "_ref"
+    if not (ref / "manifest.json").exists():
+        return {"skipped": "reference GPU programs not built (oracle/_ref/manifest.json absent)"}
+    sys.path.insert(0, str(ROOT / "oracle" / "refgpu"))
+    import config as refcfg
+
+    root = Path(tempfile.mkdtemp(prefix="tga_refgpu_"))
+    ddir = root / "data" / "compressed" / refcfg.NAME
+    tga.generate(tga.GenParams(**refcfg.PARAMS), ddir, refcfg.NAME)
+    tables = root / "gpu_cuda" / "decode_tables"
+    tables.mkdir(parents=True)
+    for kind, fname in ((0, "gammaInA.txt"), (3, "zetaInA.txt")):
+        (tables / fname).write_text(",".join(str(int(v)) for v in tga.decode_table(kind)) + ",")
+    n = refcfg.N
+    cfg = tga.DatasetConfig(name=refcfg.NAME, max_label=n - 1, max_vertex=n, bfs_start_vertex=refcfg.BFS_SOURCE,
+                            connected_components_vertex_begin=refcfg.CC_BEGIN)
+    g = tga.Graph.open_dir(ddir, refcfg.NAME, cfg)
+    out = {"workload": f"reference GPU programs vs the engine on the {n:,}-vertex / "
+                       f"{refcfg.PARAMS['m']:,}-edge graph they are built for (PR and HITS x{refcfg.PR_ITERS})",
+           "programs": {}}
+    try:
+        for prog, (name, call) in REF_GPU_PROGRAMS.items():
+            exe = ref / prog
+            if not exe.exists():
+                continue
+            times = root / f"{prog}.times"
+            env = dict(os.environ, TGA_COMPRESS_ROOT=str(root), TGA_REF_DUMP=str(root / f"{prog}.dump"),
+                       TGA_REF_TIMES=str(times))
+            r = subprocess.run([str(exe)], cwd=root, env=env, capture_output=True, text=True, timeout=600)
+            if r.returncode != 0 or not times.exists():
+                out["programs"][prog] = {"error": f"exit {r.returncode}: {(r.stderr or r.stdout)[-200:]}"}
+                continue
+            kernels = {}
+            for line in times.read_text().splitlines():
+                cnt, ms, kname = line.split(" ", 2)
+                kernels[kname] = {"launches": int(cnt), "ms": float(ms)}
+            ref_ms = sum(k["ms"] for k in kernels.values())
+            call(g, refcfg)  # warm-up
+            eng = []
+            for _ in range(5):
+                call(g, refcfg)
+                eng.append(g.timing()["total_ms"])
+            top = max(kernels.items(), key=lambda kv: kv[1]["ms"]) if kernels else ("", {"ms": 0.0})
+            out["programs"][prog] = {
+                "engine_workload": name, "ref_kernel_ms": round(ref_ms, 4),
+                "ref_launches": sum(k["launches"] for k in kernels.values()),
+                "ref_top_kernel": {"name": top[0], "ms": round(top[1]["ms"], 4)},
+                "engine_ms": round(min(eng), 4), "speedup": round(ref_ms / min(eng), 2) if min(eng) > 0 else None}
+    finally:
+        g.close()
+    return out
 
 
 def random_windows(rng, k, span, lo_frac=0.05, hi_frac=0.5):
@@ -774,6 +847,10 @@ def main():
                 line["batched"] = batched_at_size(tga, g, args.batched_config)
             except Exception as e:  # reported, not fatal
                 line["batched_error"] = str(e)
+        try:
+            line["ref_gpu"] = ref_gpu_section(tga)
+        except Exception as e:  # reported, not fatal
+            line["ref_gpu"] = {"error": str(e)}
     if rank == 0 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(ddir, summary, 0)

@@ -18,6 +18,7 @@
 #include <cstring>
 #include <vector>
 
+#include "hot.cuh"
 #include "lean.cuh"
 #include "sweep.cuh"
 #include "trace.cuh"
@@ -190,20 +191,30 @@ __device__ __forceinline__ float temporal_weight(float alpha, int64_t t) {
 
 // k_pr_iter over the lean schedule.
 __global__ void TGA_LEAN_BOUNDS k_pr_iter(GraphView g, LeanWork lw, PrArgs a) {
+  TGA_HOT_SHARED(float, hot)
+  hot.init(g);
   for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < g.max_vertex; x += gridDim.x * blockDim.x) a.reset[x] = a.base;
   const double s = a.k == 0 ? 1.0 : 1.0 / a.sums[a.k - 1];
   float local = 0.0f, c0 = 0.0f;
   double total = 0.0;
   int prev_y = -1;
+  // The source's rank and degree are loaded when the entry is taken and used once the list is open,
+  // so their latency overlaps the open instead of preceding it.
+  float in_v = 0.0f, inv_v = 0.0f;
+  int deg_v = 0;
   const unsigned long long mine = run_lean<true>(
       g, lw.e, lw.count, lw.slices, lw.run_first,
       [&](int v) {
         if (v < g.active_begin || v >= g.max_label) return false;
-        return a.invdeg ? a.invdeg[v] > 0.0f : a.deg[v] > 0;
+        in_v = __ldg(a.in + v);
+        if (a.invdeg) inv_v = __ldg(a.invdeg + v);
+        else deg_v = __ldg(a.deg + v);
+        return true;
       },
       [&](int v, int, int) {
-        const float inv = a.invdeg ? a.invdeg[v] : 1.0f / (float)a.deg[v];
-        c0 = a.damping * (float)((double)a.in[v] * s) * inv;
+        const float inv = a.invdeg ? inv_v : (deg_v > 0 ? 1.0f / (float)deg_v : 0.0f);
+        if (inv == 0.0f) return false;  // no (in-window) out-edges: nothing to scatter
+        c0 = a.damping * (float)((double)in_v * s) * inv;
         prev_y = -1;
         local = 0.0f;
         return true;
@@ -211,11 +222,12 @@ __global__ void TGA_LEAN_BOUNDS k_pr_iter(GraphView g, LeanWork lw, PrArgs a) {
       [&](int, int y, int64_t t) {
         if (!keep_edge(g, a.lo, a.hi, y, t, prev_y)) return true;
         const float contrib = c0 * temporal_weight(a.alpha, t);
-        atomicAdd(&a.out[y], contrib);
+        if (!hot.add(y, contrib)) atomicAdd(&a.out[y], contrib);
         local += contrib;
         return true;
       },
       [&](int) { total += (double)local; });
+  hot.flush(a.out);
   add_edges(a.edges, mine);
   warp_add(&a.sums[a.k], total);
 }
@@ -300,22 +312,33 @@ __global__ void TGA_LEAN_BOUNDS k_hits_hub(GraphView g, LeanWork lw, double* hub
 template <bool kTimes>
 __global__ void TGA_LEAN_BOUNDS k_hits_auth(GraphView g, LeanWork lw, const double* hub, const double* hsum,
                                             double* auth_next, int64_t lo, int64_t hi, unsigned long long* edges) {
+  // Hot authorities take block-local FP32 partials (a few hundred contributions per block),
+  // added to the FP64 accumulators once per block.
+  TGA_HOT_SHARED(float, hot)
+  hot.init(g);
   const double sh = *hsum > 0 ? 1.0 / sqrt(*hsum) : 1.0;
   float hn = 0.0f;
+  double hub_v = 0.0;
   int prev_y = -1;
   const unsigned long long mine = run_lean<true, kTimes, false, !kTimes>(
       g, lw.e, lw.count, lw.slices, lw.run_first,
-      [&](int v) { return v >= g.active_begin && v < g.max_label && hub[v] != 0.0; },
-      [&](int v, int, int) {
-        hn = (float)(hub[v] * sh);
+      [&](int v) {
+        if (v < g.active_begin || v >= g.max_label) return false;
+        hub_v = __ldg(hub + v);  // used once the list is open (see k_pr_iter)
+        return true;
+      },
+      [&](int, int, int) {
+        if (hub_v == 0.0) return false;
+        hn = (float)(hub_v * sh);
         prev_y = -1;
         return true;
       },
       [&](int, int y, int64_t t) {
-        if (keep_edge(g, lo, hi, y, t, prev_y)) atomicAdd(&auth_next[y], (double)hn);
+        if (keep_edge(g, lo, hi, y, t, prev_y) && !hot.add(y, hn)) atomicAdd(&auth_next[y], (double)hn);
         return 2;  // repeats of y add nothing
       },
       [&](int) {});
+  hot.flush(auth_next);
   add_edges(edges, mine);
 }
 
@@ -623,6 +646,50 @@ static LeanWork lean_work(const GraphHandle& h) {
   return LeanWork{h.d_lean.as<LeanEntry>(), h.nlean, h.d_slices.as<SliceState>(), h.d_run_first.as<int32_t>()};
 }
 static unsigned lean_grid(const GraphHandle& h) { return std::max(1u, grid_for(h.nlean, kBlock)); }
+
+// Hot scatter targets (hot.cuh): in-degrees counted on the device, the largest kept on the host.
+// TGA_HOT=0 leaves the table out (every target on the global path).
+int build_hot(GraphHandle& h) {
+  h.view.hot = nullptr;
+  h.nhot = 0;
+  const char* env = std::getenv("TGA_HOT");
+  const int64_t n = (int64_t)h.degrees.size();
+  if ((env && std::atoi(env) == 0) || n == 0 || h.nlean == 0) return publish_view(h);
+  DevBuf d_in;
+  if (int rc = d_in.ensure((size_t)n * 4)) return rc;
+  TGA_CUDA_TRY(cudaMemsetAsync(d_in.p, 0, (size_t)n * 4, h.stream));
+  k_in_degree<<<lean_grid(h), kBlock, 0, h.stream>>>(h.view, lean_work(h), d_in.as<int32_t>());
+  TGA_CUDA_TRY(cudaGetLastError());
+  std::vector<int32_t> indeg((size_t)n);
+  TGA_CUDA_TRY(cudaMemcpyAsync(indeg.data(), d_in.p, (size_t)n * 4, cudaMemcpyDeviceToHost, h.stream));
+  TGA_CUDA_TRY(cudaStreamSynchronize(h.stream));
+  if (int rc = h.check_device_error()) return rc;
+  std::vector<int32_t> ids((size_t)n);
+  for (int64_t i = 0; i < n; ++i) ids[(size_t)i] = (int32_t)i;
+  const size_t k = std::min<size_t>((size_t)kHotMax, ids.size());
+  std::partial_sort(ids.begin(), ids.begin() + (ptrdiff_t)k, ids.end(), [&](int32_t a, int32_t b) {
+    return indeg[(size_t)a] != indeg[(size_t)b] ? indeg[(size_t)a] > indeg[(size_t)b] : a < b;
+  });
+  const int64_t min_in = std::max<int64_t>(2, (int64_t)(h.info_edges / kHotMinShare));
+  std::vector<int32_t> table(kHotSlots, -1);
+  int placed = 0;
+  for (size_t i = 0; i < k; ++i) {
+    const int32_t y = ids[i];
+    if (indeg[(size_t)y] < min_in) break;
+    int32_t& slot = table[(size_t)hot_slot(y)];
+    if (slot < 0) {
+      slot = y;
+      ++placed;
+    }
+  }
+  if (placed > 0) {
+    if (int rc = h.d_hot.ensure(kHotSlots * 4)) return rc;
+    TGA_CUDA_TRY(cudaMemcpy(h.d_hot.p, table.data(), kHotSlots * 4, cudaMemcpyHostToDevice));
+    h.view.hot = h.d_hot.as<int32_t>();
+    h.nhot = placed;
+  }
+  return publish_view(h);
+}
 
 }  // namespace tga
 

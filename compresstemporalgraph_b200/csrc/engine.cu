@@ -50,7 +50,7 @@ void DevBuf::release() {
 GraphHandle::~GraphHandle() {
   if (stream) cudaStreamSynchronize(stream);
   for (DevBuf* b : {&d_graph, &d_ts, &d_gl, &d_gu, &d_gs, &d_tl, &d_tu, &d_ts_samples, &d_err, &d_deg, &d_slices,
-                    &d_items, &d_slice_first, &d_slice_deep, &d_order, &d_lean, &d_copies, &d_copy_base, &d_runs, &d_run_pairs, &d_run_first, &d_long, &d_slice_ebase,
+                    &d_items, &d_slice_first, &d_slice_deep, &d_order, &d_lean, &d_copies, &d_copy_base, &d_hot, &d_runs, &d_run_pairs, &d_run_first, &d_long, &d_slice_ebase,
                     &d_view, &s_edges, &s_a, &s_b, &s_c, &s_d, &s_e, &s_f, &s_g, &s_q0, &s_q1, &s_cnt, &s_sum,
                     &m_state, &m_mask, &m_dirty, &m_stamp, &m_touched, &m_dq, &d_divtab})
     b->release();
@@ -405,6 +405,7 @@ int load_graph(GraphHandle& h, const std::string& dir, const std::string& base, 
   const char* env_item = std::getenv("TGA_ITEM_EDGES");
   if (int rc = build_work(h, env_slice ? std::atoi(env_slice) : kDefaultSliceEdges, env_item ? std::atoi(env_item) : 256))
     return rc;
+  if (int rc = build_hot(h)) return rc;
   return compute_max_timestamp(h);
 }
 

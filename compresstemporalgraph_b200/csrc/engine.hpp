@@ -77,6 +77,8 @@ struct GraphHandle {
   int32_t nlean = 0;
   // copied values of every list resolved at load (GraphView::copies / copy_base)
   DevBuf d_copies, d_copy_base;
+  DevBuf d_hot;  // hot scatter targets (GraphView::hot)
+  int32_t nhot = 0;
   // runs of equal successors cut by slices: RunInfo[nruns], (run, slice) pairs of the per-call
   // pre-pass, and the per-call list index of each run's first in-window edge
   DevBuf d_runs, d_run_pairs, d_run_first;
@@ -146,6 +148,7 @@ int publish_view(GraphHandle& h);
 
 // Computes h.max_ts with one timestamp-only pass (after the work decomposition exists).
 int compute_max_timestamp(GraphHandle& h);
+int build_hot(GraphHandle& h);
 // True when [lo, hi) contains every timestamp of the graph.
 inline bool window_covers_all(const GraphHandle& h, int64_t lo, int64_t hi) {
   return lo <= h.view.min_ts && hi > h.max_ts;

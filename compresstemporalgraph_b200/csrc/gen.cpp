@@ -71,13 +71,14 @@ GenSummary generate_dataset(const GenParams& p, const std::string& dir, const st
       deg[(size_t)v] = c - prev;
       prev = c;
     }
-    for (int64_t k = 0; k < nhub; ++k) deg[(size_t)hub_vertex(k)] = p.hub_degree;
-    // Make the largest id a source so that n = max id + 1 holds even with no in-edges to it.
+    // Make the largest id a source so that n = max id + 1 holds even with no in-edges to it (the
+    // edge is taken from the largest list that is not a hub, so hubs keep exactly hub_degree).
     if (deg[(size_t)n - 1] == 0) {
       const auto it = std::max_element(deg.begin(), deg.end());
       --*it;
       deg[(size_t)n - 1] = 1;
     }
+    for (int64_t k = 0; k < nhub; ++k) deg[(size_t)hub_vertex(k)] = p.hub_degree;
   }
   const int32_t lo_id = p.ref_safe ? 1 : 0;
   const int32_t hi_id = p.ref_safe ? (int32_t)(n - 2) : (int32_t)(n - 1);

@@ -3,7 +3,8 @@
 For each program of config.PROGRAMS it writes a translation unit that defines the dataset macros of
 config.py (as a gpu_cuda/<DS>/dataset_config.cuh does) and includes the reference's
 gpu_cuda/shared/dataset_config_base.cuh and gpu_cuda/shared/<program>.cu from the checkout, unchanged;
-nvcc compiles it for sm_100a with harness_pre.h force-included and links harness_main.cu.  Outputs go
+nvcc compiles it for sm_100a with harness_pre.h force-included and links harness_main.cu against the
+shared CUDA runtime (the harness brackets each kernel launch with events, harness_main.cu).  Outputs go
 only to oracle/_ref/: the executables and manifest.json (for each compared buffer, the source line of
 its allocation).
 
@@ -68,11 +69,12 @@ def main() -> int:
         exe = OUT / prog
         manifest["programs"][prog] = {b: alloc_line(src, b) for b in bufs}
         stale = not exe.exists() or any(p.stat().st_mtime > exe.stat().st_mtime
-                                        for p in (src, HERE / "harness_pre.h", HERE / "harness_main.cu", HERE / "config.py"))
+                                        for p in (src, HERE / "harness_pre.h", HERE / "harness_main.cu", HERE / "config.py",
+                                                  HERE / "build_ref.py"))
         if stale:
             obj = OUT / f"{prog}_tu.o"
             jobs.append([[*arch, "-w", "-Xcompiler", "-fpermissive", "-include", str(HERE / "harness_pre.h"), "-c", str(tu), "-o", str(obj)],
-                         [*arch, str(obj), str(harness), "-o", str(exe)]])
+                         [*arch, "-cudart", "shared", str(obj), str(harness), "-o", str(exe), "-ldl"]])
 
     def run(steps):
         for cmd in steps:
