@@ -671,20 +671,22 @@ int build_hot(GraphHandle& h) {
     return indeg[(size_t)a] != indeg[(size_t)b] ? indeg[(size_t)a] > indeg[(size_t)b] : a < b;
   });
   const int64_t min_in = std::max<int64_t>(2, (int64_t)(h.info_edges / kHotMinShare));
-  std::vector<int32_t> table(kHotSlots, -1);
+  std::vector<int32_t> table(2 * kHotSlots, -1);  // ids, then compact indexes
   int placed = 0;
   for (size_t i = 0; i < k; ++i) {
     const int32_t y = ids[i];
     if (indeg[(size_t)y] < min_in) break;
-    int32_t& slot = table[(size_t)hot_slot(y)];
-    if (slot < 0) {
-      slot = y;
-      ++placed;
+    const size_t s = (size_t)hot_slot(y);
+    if (table[s] < 0) {
+      table[s] = y;
+      table[kHotSlots + s] = placed++;
     }
   }
+  for (size_t s = 0; s < (size_t)kHotSlots; ++s)
+    if (table[s] < 0) table[kHotSlots + s] = 0;
   if (placed > 0) {
-    if (int rc = h.d_hot.ensure(kHotSlots * 4)) return rc;
-    TGA_CUDA_TRY(cudaMemcpy(h.d_hot.p, table.data(), kHotSlots * 4, cudaMemcpyHostToDevice));
+    if (int rc = h.d_hot.ensure(2 * kHotSlots * 4)) return rc;
+    TGA_CUDA_TRY(cudaMemcpy(h.d_hot.p, table.data(), 2 * kHotSlots * 4, cudaMemcpyHostToDevice));
     h.view.hot = h.d_hot.as<int32_t>();
     h.nhot = placed;
   }

@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "gridsync.cuh"
+#include "hot.cuh"
 #include "trace.cuh"
 
 namespace tga {
@@ -79,7 +80,7 @@ constexpr int kSparseSlots = kWarpSources - 1;
 __device__ __forceinline__ unsigned long long multi_relax_sparse(const GraphView& g, MultiArgs& a, const Work& w,
                                                                  const int64_t* slo, const int64_t* shi,
                                                                  const int32_t* scol, const int32_t* q, int qn, int L,
-                                                                 bool dense) {
+                                                                 bool dense, const int32_t* hids) {
   const uint64_t* Fc = a.F[L & 1];
   uint64_t* Fn = a.F[(L + 1) & 1];
   int src[kSparseSlots];     // source of slot i (-1: empty)
@@ -132,6 +133,7 @@ __device__ __forceinline__ unsigned long long multi_relax_sparse(const GraphView
       yprev = y;
     }
     const bool usable = y >= g.active_begin && y < g.max_vertex && t >= 0 && t < 0xFFFFFFFFll;
+    const bool hot = usable && hot_is(hids, y);
     uint64_t add0 = 0, add1 = 0, add2 = 0, add3 = 0;
 #pragma unroll
     for (int i = 0; i < kSparseSlots; ++i) {
@@ -140,6 +142,7 @@ __device__ __forceinline__ unsigned long long multi_relax_sparse(const GraphView
       if (t < slo[s] || t >= shi[s]) continue;
       seen |= 1u << i;
       if (!usable || (int64_t)ax[i] > t) continue;
+      if (hot && __ldcg(a.arr + arr_at(a, y, s)) <= (uint32_t)t) continue;  // nothing to lower
       atomicMin(a.arr + arr_at(a, y, s), (uint32_t)t);
       const uint64_t bit = 1ull << (s & 63);
       const int wd = s >> 6;
@@ -150,11 +153,17 @@ __device__ __forceinline__ unsigned long long multi_relax_sparse(const GraphView
     }
     if (add0 | add1 | add2 | add3) {
       unsigned long long* f = (unsigned long long*)(Fn + (size_t)y * kWords);
+      if (hot) {  // bits another relaxation of this level has set already need no atomic
+        if (add0 && (__ldcg(f + 0) & add0) == add0) add0 = 0;
+        if (add1 && (__ldcg(f + 1) & add1) == add1) add1 = 0;
+        if (add2 && (__ldcg(f + 2) & add2) == add2) add2 = 0;
+        if (add3 && (__ldcg(f + 3) & add3) == add3) add3 = 0;
+      }
       if (add0) atomicOr(f + 0, (unsigned long long)add0);
       if (add1) atomicOr(f + 1, (unsigned long long)add1);
       if (add2) atomicOr(f + 2, (unsigned long long)add2);
       if (add3) atomicOr(f + 3, (unsigned long long)add3);
-      atomicOr(&a.dirty[y >> 5], 1u << (y & 31));
+      if (!hot || !((__ldcg(&a.dirty[y >> 5]) >> (y & 31)) & 1u)) atomicOr(&a.dirty[y >> 5], 1u << (y & 31));
     }
     return true;
   };
@@ -173,7 +182,7 @@ __device__ __forceinline__ unsigned long long multi_relax_sparse(const GraphView
 // Wide part of a level: one warp per entry of the wide queue (entries taken from *counter).
 __device__ unsigned long long multi_relax_wide(const GraphView& g, MultiArgs& a, const int64_t* slo,
                                                const int64_t* shi, const int32_t* scol, const int32_t* dq, int dn,
-                                               int32_t* counter, int L) {
+                                               int32_t* counter, int L, const int32_t* hids) {
   constexpr unsigned kFull = 0xffffffffu;
   const uint64_t* Fc = a.F[L & 1];
   uint64_t* Fn = a.F[(L + 1) & 1];
@@ -207,20 +216,23 @@ __device__ unsigned long long multi_relax_wide(const GraphView& g, MultiArgs& a,
         if (run >= 0 && __ldg(a.run_first + (size_t)run * a.run_stride + scol[s]) < first) seen |= 1u << k;
       }
     }
+    // Every lane decodes the entry (the same words, loaded once for the warp, and the same code
+    // path, so the warp does not diverge): no lane waits on a shuffle from a decoding lane, and the
+    // next edge is decoded while the current one is relaxed.
     int count = 0;
-    if (lane == 0) {
+    {
       int f, lead, r;
       open_entry(g, a.w, e, c, f, count, lead, r);
     }
-    if (__shfl_sync(kFull, count, 0) <= 0) continue;
+    if (count <= 0) continue;
     int yprev = run >= 0 ? kKeepSeen : -1;
-    for (;;) {
-      int y = 0, more = 0;
-      int64_t t = 0;
-      if (lane == 0) more = c.next(g, y, t);
-      if (!__shfl_sync(kFull, more, 0)) break;
-      y = __shfl_sync(kFull, y, 0);
-      t = __shfl_sync(kFull, t, 0);
+    int yn = 0;
+    int64_t tn = 0;
+    bool more = c.next(g, yn, tn);
+    while (more) {
+      const int y = yn;
+      const int64_t t = tn;
+      more = c.next(g, yn, tn);
       edges += lane == 0;
       if (yprev == kKeepSeen) {
         yprev = y;
@@ -229,6 +241,7 @@ __device__ unsigned long long multi_relax_wide(const GraphView& g, MultiArgs& a,
         yprev = y;
       }
       const bool usable = y >= g.active_begin && y < g.max_vertex && t >= 0 && t < 0xFFFFFFFFll;
+      const bool hot = usable && hot_is(hids, y);
       uint32_t add = 0;
 #pragma unroll
       for (int k = 0; k < kSlots; ++k) {
@@ -237,6 +250,7 @@ __device__ unsigned long long multi_relax_wide(const GraphView& g, MultiArgs& a,
         if (t < slo[s] || t >= shi[s]) continue;
         seen |= 1u << k;
         if (!usable || (int64_t)ax[k] > t) continue;
+        if (hot && __ldcg(a.arr + arr_at(a, y, s)) <= (uint32_t)t) continue;  // nothing to lower
         atomicMin(a.arr + arr_at(a, y, s), (uint32_t)t);
         add |= 1u << k;
       }
@@ -246,9 +260,11 @@ __device__ unsigned long long multi_relax_wide(const GraphView& g, MultiArgs& a,
           const uint32_t lo = __ballot_sync(kFull, (add >> (2 * wd)) & 1);
           const uint32_t hi = __ballot_sync(kFull, (add >> (2 * wd + 1)) & 1);
           const uint64_t bits = (uint64_t)lo | ((uint64_t)hi << 32);
-          if (lane == 0 && bits) atomicOr((unsigned long long*)(Fn + (size_t)y * kWords + wd), (unsigned long long)bits);
+          unsigned long long* f = (unsigned long long*)(Fn + (size_t)y * kWords + wd);
+          if (lane == 0 && bits && !(hot && (__ldcg(f) & bits) == bits)) atomicOr(f, (unsigned long long)bits);
         }
-        if (lane == 0) atomicOr(&a.dirty[y >> 5], 1u << (y & 31));
+        if (lane == 0 && (!hot || !((__ldcg(&a.dirty[y >> 5]) >> (y & 31)) & 1u)))
+          atomicOr(&a.dirty[y >> 5], 1u << (y & 31));
       }
     }
   }
@@ -278,58 +294,40 @@ __device__ __forceinline__ void multi_scan(MultiArgs& a, const int32_t* cq, int 
       bits = __ldcg(a.dirty + i);
       if (bits) a.dirty[i] = 0;
     }
-    uint32_t keep_bits = 0, wide_bits = 0;
-    int n = 0, nw = 0;
-    for (uint32_t b = bits; b; b &= b - 1) {
-      const int v = i * 32 + __ffs(b) - 1;
+    deal_dirty(bits, base, [&](int v) {
       int nkept = 0;
+      if (v >= 0) {
 #pragma unroll
-      for (int k = 0; k < kWords; ++k) {
-        const uint64_t m = __ldcg(Fn + (size_t)v * kWords + k);
-        uint64_t kept = 0;
-        for (uint64_t c = m; c; c &= c - 1) {
-          const int bb = __ffsll((long long)c) - 1;
-          const size_t at = arr_at(a, v, k * 64 + bb);
-          const uint32_t now = __ldcg(a.arr + at), before = __ldcg(a.prev + at);
-          if (now < before) {
-            a.prev[at] = now;
-            kept |= 1ull << bb;
+        for (int k = 0; k < kWords; ++k) {
+          const uint64_t m = __ldcg(Fn + (size_t)v * kWords + k);
+          uint64_t kept = 0;
+          for (uint64_t c = m; c; c &= c - 1) {
+            const int bb = __ffsll((long long)c) - 1;
+            const size_t at = arr_at(a, v, k * 64 + bb);
+            const uint32_t now = __ldcg(a.arr + at), before = __ldcg(a.prev + at);
+            if (now < before) {
+              a.prev[at] = now;
+              kept |= 1ull << bb;
+            }
           }
+          if (kept != m) Fn[(size_t)v * kWords + k] = kept;
+          nkept += __popcll(kept);
         }
-        if (kept != m) Fn[(size_t)v * kWords + k] = kept;
-        nkept += __popcll(kept);
       }
-      if (nkept >= kWarpSources) {
-        wide_bits |= b & (~b + 1);
-        nw += entry_count(a.w, v);
-      } else if (nkept > 0) {
-        keep_bits |= b & (~b + 1);
-        n += entry_count(a.w, v);
+      const bool wide = nkept >= kWarpSources, sparse = nkept > 0 && !wide;
+      const int ec = (wide || sparse) ? entry_count(a.w, v) : 0;
+      const int at = warp_reserve(ncnt, sparse ? ec : 0);
+      if (sparse) write_entries(a.w, v, nq, at);
+      const int atw = warp_reserve(ndcnt, wide ? ec : 0);
+      if (wide) write_entries(a.w, v, ndq, atw);
+      // kept vertices this traversal has not touched before
+      const bool fresh = (wide || sparse) && __ldcg(&a.stamp[v]) != a.epoch;
+      const int tat = warp_reserve(a.ntouched, fresh ? 1 : 0);
+      if (fresh) {
+        a.stamp[v] = a.epoch;
+        a.touched[tat] = v;
       }
-    }
-    int at = warp_reserve(ncnt, n);
-    for (uint32_t b = keep_bits; b; b &= b - 1) {
-      const int v = i * 32 + __ffs(b) - 1;
-      write_entries(a.w, v, nq, at);
-      at += entry_count(a.w, v);
-    }
-    at = warp_reserve(ndcnt, nw);
-    for (uint32_t b = wide_bits; b; b &= b - 1) {
-      const int v = i * 32 + __ffs(b) - 1;
-      write_entries(a.w, v, ndq, at);
-      at += entry_count(a.w, v);
-    }
-    uint32_t fresh = 0;  // kept vertices this traversal has not touched before
-    for (uint32_t b = keep_bits | wide_bits; b; b &= b - 1) {
-      const int v = i * 32 + __ffs(b) - 1;
-      if (__ldcg(&a.stamp[v]) != a.epoch) fresh |= b & (~b + 1);
-    }
-    int tat = warp_reserve(a.ntouched, __popc(fresh));
-    for (uint32_t b = fresh; b; b &= b - 1) {
-      const int v = i * 32 + __ffs(b) - 1;
-      a.stamp[v] = a.epoch;
-      a.touched[tat++] = v;
-    }
+    });
   }
 }
 
@@ -337,7 +335,7 @@ __device__ __forceinline__ void multi_scan(MultiArgs& a, const int32_t* cq, int 
 // and the dirty bits); the control block's queue and work counters must be zero.  All blocks of
 // the cooperative launch call it together; false if the launch has failed (return at once).
 __device__ bool multi_levels(const GraphView& g, MultiArgs& a, const int64_t* slo, const int64_t* shi,
-                             const int32_t* scol, unsigned long long& mine, int& levels) {
+                             const int32_t* scol, unsigned long long& mine, int& levels, const int32_t* hids) {
   const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
   TravCtl* ctl = a.ctl;
   // The sources were seeded as level 0's relaxations: the scan turns them into level 1's queues.
@@ -360,11 +358,11 @@ __device__ bool multi_levels(const GraphView& g, MultiArgs& a, const int64_t* sl
       ctl->dcnt[(L + 2) % 3] = 0;
       ctl->dnext[(L + 1) % 3] = 0;
     }
-    if (dn > 0) mine += multi_relax_wide(g, a, slo, shi, scol, a.dq[L & 1], dn, &ctl->dnext[L % 3], L);
+    if (dn > 0) mine += multi_relax_wide(g, a, slo, shi, scol, a.dq[L & 1], dn, &ctl->dnext[L % 3], L, hids);
     if (qn > 0) {
       Work w = a.w;
       w.next = &ctl->next[L % 3];
-      mine += multi_relax_sparse(g, a, w, slo, shi, scol, a.q[L & 1], qn, L, qn >= a.dense_min);
+      mine += multi_relax_sparse(g, a, w, slo, shi, scol, a.q[L & 1], qn, L, qn >= a.dense_min, hids);
     }
     if (!grid_sync(ctl, g)) return false;
     multi_scan(a, a.q[L & 1], qn, a.dq[L & 1], dn, a.q[(L + 1) & 1], &ctl->cnt[(L + 1) % 3], a.dq[(L + 1) & 1],
@@ -404,10 +402,12 @@ __device__ __forceinline__ void load_windows(const MultiArgs& a, int64_t* slo, i
 __global__ void TGA_DECODE_BOUNDS k_bfs_multi(GraphView g, MultiArgs a) {
   __shared__ int64_t slo[kMaxSources], shi[kMaxSources];
   __shared__ int32_t scol[kMaxSources];
+  __shared__ int32_t hids[kHotSlots];
+  hot_load(g, hids);
   load_windows(a, slo, shi, scol);
   unsigned long long mine = 0;
   int levels = 0;
-  if (!multi_levels(g, a, slo, shi, scol, mine, levels)) return;
+  if (!multi_levels(g, a, slo, shi, scol, mine, levels, hids)) return;
   add_edges(a.edges, mine);
   if (blockIdx.x == 0 && threadIdx.x == 0) a.ctl->levels = levels;
 }
@@ -897,9 +897,12 @@ __device__ void cc_label_reset(const MultiArgs& a, const CcArgs& c, const CcSlot
       bool r = false;
       if (j < nslots) {
         const size_t at = arr_at(a, u, j);
-        r = __ldcg(a.arr + at) != kNoArrival && __ldcg(c.comp_of + j) >= 0;
-        a.arr[at] = kNoArrival;
-        a.prev[at] = kNoArrival;
+        // prev is only ever set to an arrival, so an unset arrival has an unset prev as well
+        if (__ldcg(a.arr + at) != kNoArrival) {
+          r = __ldcg(c.comp_of + j) >= 0;
+          a.arr[at] = kNoArrival;
+          a.prev[at] = kNoArrival;
+        }
       }
       realw[k] = __ballot_sync(kFull, r);
     }
@@ -924,7 +927,7 @@ __device__ void cc_label_reset(const MultiArgs& a, const CcArgs& c, const CcSlot
   }
 }
 
-__global__ void TGA_TRAVERSE_BOUNDS k_cc_batches(GraphView g, MultiArgs a, CcArgs c) {
+__global__ void TGA_DECODE_BOUNDS k_cc_batches(GraphView g, MultiArgs a, CcArgs c) {
   __shared__ int64_t slo[kMaxSources], shi[kMaxSources];
   __shared__ int32_t scol[kMaxSources];
   __shared__ uint32_t reaches[kMaxSources][kMaxSources / 32];
@@ -932,6 +935,8 @@ __global__ void TGA_TRAVERSE_BOUNDS k_cc_batches(GraphView g, MultiArgs a, CcArg
   __shared__ int32_t s_cand[kMaxSources];
   __shared__ int32_t s_wsum[kBlock / 32], s_count;
   __shared__ CcSlots sl;
+  __shared__ int32_t hids[kHotSlots];
+  hot_load(g, hids);  // (the first cc_allot synchronises the block)
   const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
   const uint32_t epoch0 = a.epoch;
   const uint64_t t_start = global_ns();
@@ -994,7 +999,7 @@ __global__ void TGA_TRAVERSE_BOUNDS k_cc_batches(GraphView g, MultiArgs a, CcArg
     }
     if (!grid_sync(a.ctl, g)) return;
     int lv = 0;
-    if (!multi_levels(g, a, slo, shi, scol, mine, lv)) return;
+    if (!multi_levels(g, a, slo, shi, scol, mine, lv, hids)) return;
     levels += lv;
     cc_count(a, c, sl, scol, s_cnt);
     if (!grid_sync(a.ctl, g)) return;
@@ -1242,25 +1247,33 @@ __device__ __forceinline__ float temporal_weight_multi(float alpha, int64_t t) {
   return a > 18.0f ? 1.0f : 1.0f - expf(-a);
 }
 
-__global__ void TGA_DECODE_BOUNDS k_pr_multi_iter(GraphView g, Work w, PrMultiArgs a) {
+// One iteration of the batch over the lean schedule (one entry per thread).  Contributions to the
+// hot targets (hot.cuh) are summed per block and query in shared memory and added once per block:
+// the queries' entries of one vertex share a cache line, so without that every query's adds to a
+// hot vertex would queue at the same L2 slice.
+__global__ void TGA_DECODE_BOUNDS k_pr_multi_iter(GraphView g, LeanWork lw, PrMultiArgs a) {
   __shared__ int64_t slo[kMaxRankQueries], shi[kMaxRankQueries];
   __shared__ float sinv[kMaxRankQueries];
+  __shared__ int32_t hids[kHotSlots], hidx[kHotSlots];
+  __shared__ float hacc[kHotMax * kMaxRankQueries];
+  hot_load(g, hids, hidx);
+  for (int i = threadIdx.x; i < kHotMax * kMaxRankQueries; i += blockDim.x) hacc[i] = 0.0f;
   for (int q = threadIdx.x; q < kMaxRankQueries; q += blockDim.x) {
     slo[q] = q < a.nq ? a.lo[q] : 0;
     shi[q] = q < a.nq ? a.hi[q] : 0;
     sinv[q] = (q < a.nq && a.sums_prev) ? (float)(1.0 / a.sums_prev[q]) : 1.0f;
   }
   __syncthreads();
-  const size_t S = (size_t)a.S;
-  const int64_t total = (int64_t)a.nv * a.S;
+  const int S = a.S;
+  const int64_t total = (int64_t)a.nv * S;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x)
     a.reset[i] = a.base;
   float c0[kMaxRankQueries];
   uint32_t act = 0, seen = 0;
   int yprev = -1;
   constexpr int kKeepSeen = -3;
-  const unsigned long long mine = run_order<false, false, false, true, true>(
-      g, w, [&](int v) { return v >= g.active_begin && v < g.max_label; },
+  const unsigned long long mine = run_lean<false, true, true>(
+      g, lw.e, lw.count, lw.slices, lw.run_first, [&](int v) { return v >= g.active_begin && v < g.max_label; },
       [&](int x, int first, int, int run) {
         act = 0;
         const float inv_all = a.deg[x] > 0 ? 1.0f / (float)a.deg[x] : 0.0f;
@@ -1294,6 +1307,7 @@ __global__ void TGA_DECODE_BOUNDS k_pr_multi_iter(GraphView g, Work w, PrMultiAr
           yprev = y;
         }
         const bool usable = y >= g.active_begin && y < g.max_vertex;
+        const int hk = usable ? hot_index(hids, hidx, y) : -1;
         float wgt = 0.0f;
         bool have_w = false;
         for (uint32_t c = act & ~seen; c; c &= c - 1) {
@@ -1305,11 +1319,19 @@ __global__ void TGA_DECODE_BOUNDS k_pr_multi_iter(GraphView g, Work w, PrMultiAr
             wgt = temporal_weight_multi(a.alpha, t);
             have_w = true;
           }
-          atomicAdd(&a.out[(size_t)y * S + q], c0[q] * wgt);
+          if (hk >= 0) atomicAdd(&hacc[hk * S + q], c0[q] * wgt);
+          else atomicAdd(&a.out[(size_t)y * S + q], c0[q] * wgt);
         }
         return true;
       },
       [](int) {});
+  __syncthreads();
+  for (int i = threadIdx.x; i < kHotSlots * S; i += blockDim.x) {
+    const int sl = i / S, q = i % S;
+    if (hids[sl] < 0) continue;
+    const float v = hacc[hidx[sl] * S + q];
+    if (v != 0.0f) atomicAdd(&a.out[(size_t)hids[sl] * S + q], v);
+  }
   add_edges(a.edges, mine);
 }
 
@@ -1434,8 +1456,8 @@ static int pagerank_multi_batch(GraphHandle& h, int32_t nq, const int32_t* iters
                                (uint64_t)windowed, bits_of(damping), bits_of(alpha), ptr_key(dlo)};
   for (int q = 0; q < nq; ++q) key.push_back((uint64_t)iters[q]);
   TGA_TRY(run_loop(h, h.prm_loop, key, (size_t)maxit, [&]() -> int {
+    const LeanWork lw{h.d_lean.as<LeanEntry>(), h.nlean, h.d_slices.as<SliceState>(), h.d_run_first.as<int32_t>()};
     for (int k = 0; k < maxit; ++k) {
-      Work w = work_of(h);
       PrMultiArgs a{};
       a.invdeg = invdeg;
       a.deg = h.d_deg.as<int32_t>();
@@ -1461,7 +1483,7 @@ static int pagerank_multi_batch(GraphHandle& h, int32_t nq, const int32_t* iters
       a.base = base;
       a.edges = edges;
       cudaEvent_t* ev = h.kernel_begin();
-      KL(k_pr_multi_iter, sweep_grid(h))(h.view, w, a);
+      KL(k_pr_multi_iter, std::max(1u, grid_for(h.nlean, kBlock)))(h.view, lw, a);
       h.kernel_end(ev);
       k_sums_multi_part<<<dim3(kSumParts, nq), kBlock, 0, h.stream>>>(a.out, (int32_t)nv, S, part);
       k_sums_multi_fin<<<1, kMaxRankQueries, 0, h.stream>>>(part, nq, sums + (size_t)k * kMaxRankQueries);

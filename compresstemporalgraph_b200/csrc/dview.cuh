@@ -69,8 +69,8 @@ struct GraphView {
   // a reference).  Read by the lean sweep decoder (lean.cuh) instead of walking the chain.
   const int32_t* copies;
   const uint32_t* copy_base;
-  // Hot scatter targets (hot.cuh): a direct-mapped table of kHotSlots vertex ids (-1 empty), or
-  // null when no vertex qualifies.
+  // Hot scatter targets (hot.cuh): a direct-mapped table of kHotSlots vertex ids (-1 empty) and
+  // their kHotSlots compact indexes, or null when no vertex qualifies.
   const int32_t* hot;
 };
 

@@ -94,6 +94,46 @@ __device__ __forceinline__ int warp_reserve(int32_t* cnt, int n) {
 }
 
 // Entries of vertex v in a queue: v itself or all its slices.
+// Deals the vertices marked in 32 words of a dirty bitmap (lane l holds word base + l, already
+// loaded into `bits`) one per lane, in rounds of 32, so that a word with many marked vertices does
+// not leave one lane to process them all while the others wait: fn(v) is called by every lane of
+// the warp in every round (all 32 lanes must call deal_dirty together), with v = -1 for a lane
+// that has no vertex in that round.  Marked vertex idx (in word order) belongs to the first lane
+// whose inclusive count exceeds idx, at rank idx - (that lane's exclusive count) among its bits.
+template <class Fn>
+__device__ __forceinline__ void deal_dirty(uint32_t bits, int base, Fn fn) {
+  constexpr unsigned kFull = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int cnt = __popc(bits);
+  int incl = cnt;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int u = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += u;
+  }
+  const int total = __shfl_sync(kFull, incl, 31);
+  for (int j0 = 0; j0 < total; j0 += 32) {
+    const int idx = j0 + lane;
+    int owner = 0;  // lanes whose inclusive count is <= idx
+    for (int step = 16; step; step >>= 1) {
+      const int probe = __shfl_sync(kFull, incl, owner + step - 1);
+      if (probe <= idx) owner += step;
+    }
+    owner = min(owner, 31);
+    uint32_t w = __shfl_sync(kFull, bits, owner);
+    int r = idx - (__shfl_sync(kFull, incl, owner) - __shfl_sync(kFull, cnt, owner));
+    int pos = 0;  // the r-th (0-based) set bit of w
+    for (int width = 16; width; width >>= 1) {
+      const int c = __popc(w & ((1u << width) - 1));
+      if (r >= c) {
+        r -= c;
+        w >>= width;
+        pos += width;
+      }
+    }
+    fn(idx < total ? (base + owner) * 32 + pos : -1);
+  }
+}
+
 __device__ __forceinline__ int entry_count(const Work& w, int v) {
   const int n = __ldg(w.slice_first + v + 1) - __ldg(w.slice_first + v);
   return n ? n : 1;

@@ -2,14 +2,17 @@
 //
 // One worker thread per graph takes turns on the device with the others: the graph holding the
 // oldest outstanding query goes first, so across graphs the queries are served in arrival order.
-// A graph's turn serves the kind of its oldest waiting query together with every other waiting
-// query of that kind, admitted while the device working memory they need fits the server's budget
-// (shared by all graphs): BFS queries as one batched traversal (tga_bfs_batch), PageRank queries as
-// one strided vector (tga_pagerank_batch_iters, each with its own iteration count), CC windows as
-// one multi-window seed loop (the CC job, up to 32 windows, run to completion), point queries as one
-// launch.  A query therefore never waits behind work that arrived after it, except for the
-// same-kind queries that join its batch, which cost little (a batched traversal decodes each list
-// once per level for all its sources).  Turns run one at a time: the traversal kernels are
+// A graph's turn serves the kind of its oldest waiting query together with the other waiting
+// queries of that kind that can share its launch, admitted while the device working memory they
+// need fits the server's budget (shared by all graphs): BFS queries as one batched traversal
+// (tga_bfs_batch), PageRank queries as one strided vector (tga_pagerank_batch_iters, each with its
+// own iteration count; fewer than kPrBatchMin of them one call each), CC windows as one
+// multi-window seed loop (the CC job, up to 32 windows, run to completion), point queries as one
+// launch.  Queries of a kind whose batch costs less than its single calls join the round from
+// anywhere in the queue (a batched traversal decodes each list once per level for all its sources);
+// the others only from the head of the queue, so they never overtake an earlier query.  A query
+// therefore never waits behind work that arrived after it, except for the same-kind queries that
+// join its batch, which cost little.  Turns run one at a time: the traversal kernels are
 // cooperative launches that occupy every SM, so rounds of different graphs could not overlap on the
 // device anyway.  Latency is measured from tga_submit to the moment the result is in the caller's
 // buffer.
@@ -60,6 +63,11 @@ struct GraphSlot {
 
 // CC windows per round (the job's capacity).
 constexpr int32_t kCcJobWindows = 32;
+// PageRank rounds smaller than this run their queries one call each: the strided batch decodes
+// each list once for all its queries but scatters per query, and below four queries one plain
+// call per query costs less device time (2M/40M graph, 20 iterations: 1 query 16.5 ms plain
+// against 37.9 ms batched, 2 queries 33 against 43.5 ms, 4 queries 65 against 61 ms).
+constexpr size_t kPrBatchMin = 4;
 
 // Device working bytes of one query (per vertex of its graph): BFS arrival + last-enqueued arrival
 // + result; PageRank three rank vectors + inverse degree + result; CC the single traversal's arrays.
@@ -147,7 +155,12 @@ void tga_server::run_round(GraphSlot* slot, std::vector<Pending>& round) {
         lo.push_back(p.q.t_lo);
         hi.push_back(p.q.t_hi);
       }
-    if (!done.empty()) {
+    if (!done.empty() && done.size() < kPrBatchMin) {
+      for (size_t k = 0; k < done.size(); ++k) {
+        const int rc = tga_pagerank(slot->g, iters[k], 0.85f, 0.1f, lo[k], hi[k], static_cast<float*>(done[k]->q.out));
+        publish({done[k]}, {rc});
+      }
+    } else if (!done.empty()) {
       std::vector<float*> rows(done.size());
       for (size_t k = 0; k < done.size(); ++k) rows[k] = static_cast<float*>(done[k]->q.out);
       const int rc = tga::pagerank_batch_rows(slot->g, (int32_t)done.size(), iters.data(), 0.85f, 0.1f, lo.data(),
@@ -214,16 +227,25 @@ void tga_server::worker(GraphSlot* slot) {
       if (stopping) break;
       continue;
     }
-    // The kind of the oldest waiting query, with every other waiting query of that kind, admitted
-    // while they fit the budget (at least one when nothing else runs); CC at most a job's windows.
+    // The kind of the oldest waiting query.  Where one launch for several queries of that kind
+    // costs less device time than their single calls (BFS, point queries, PageRank from
+    // kPrBatchMin queries on), every waiting query of the kind joins the round, though some arrived
+    // after queries of other kinds; otherwise (CC windows, which gain nothing from sharing a launch,
+    // and fewer PageRank queries) only the queries of the kind at the head of the queue, so none
+    // overtakes an earlier query.  Admitted while they fit the budget (at least one when nothing
+    // else runs); CC at most a job's windows.
     const int32_t kind = slot->pending.front().q.kind;
+    size_t waiting = 0;
+    for (const Pending& p : slot->pending) waiting += p.q.kind == kind;
+    const bool gather = kind == TGA_Q_BFS || kind == TGA_Q_NEIGHBOR || (kind == TGA_Q_PAGERANK && waiting >= kPrBatchMin);
     std::vector<Pending> round;
     std::deque<Pending> rest;
-    bool full = false;
+    bool full = false, head = true;
     while (!slot->pending.empty()) {
       Pending p = slot->pending.front();
       slot->pending.pop_front();
-      if (full || p.q.kind != kind || (kind == TGA_Q_CC && (int32_t)round.size() >= kCcJobWindows) ||
+      head = head && p.q.kind == kind;
+      if (full || p.q.kind != kind || (!gather && !head) || (kind == TGA_Q_CC && (int32_t)round.size() >= kCcJobWindows) ||
           (in_use + p.bytes > budget && !(round.empty() && in_use == 0))) {
         if (p.q.kind == kind && !round.empty()) full = full || in_use + p.bytes > budget;
         rest.push_back(p);

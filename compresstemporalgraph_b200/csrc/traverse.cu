@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "gridsync.cuh"
+#include "hot.cuh"
 #include "trace.cuh"
 
 namespace tga {
@@ -64,8 +65,8 @@ __device__ __forceinline__ void seed_queue(const Work& w, TravArgs& a, int L, in
   a.ctl->cnt[L % 3] = k;
 }
 
-// Scan over the dirty bitmap after a level: keep(v) decides (once per marked vertex, by the one
-// thread that owns its word) whether v joins the next frontier; its entries are appended to nq,
+// Scan over the dirty bitmap after a level: keep(v) decides (once per marked vertex, the marked
+// vertices of a warp's words dealt over its lanes) whether v joins the next frontier; its entries are appended to nq,
 // its frontier mark set, and touched(v) -> bool adds it to the touched list (CC).  Clears the
 // bitmap.
 template <class Keep, class Touched>
@@ -80,26 +81,17 @@ __device__ __forceinline__ void scan_dirty(TravArgs& a, int32_t* nq, int32_t* nc
       bits = __ldcg(a.dirty + i);
       if (bits) a.dirty[i] = 0;
     }
-    uint32_t keep_bits = 0, touch_bits = 0;
-    int n = 0;
-    for (uint32_t b = bits; b; b &= b - 1) {
-      const int v = i * 32 + __ffs(b) - 1;
+    deal_dirty(bits, base, [&](int v) {
       bool t = false;
-      if (keep(v, t)) {
-        keep_bits |= b & (~b + 1);
-        n += entry_count(a.w, v);
-        if (t) touch_bits |= b & (~b + 1);
+      const bool k = v >= 0 && keep(v, t);
+      const int at = warp_reserve(ncnt, k ? entry_count(a.w, v) : 0);
+      const int tat = touched(0) ? warp_reserve(&a.ctl->tcnt, (k && t) ? 1 : 0) : 0;
+      if (k) {
+        write_entries(a.w, v, nq, at);
+        mark[v] = wave;
+        if (t) a.touched[tat] = v;
       }
-    }
-    int at = warp_reserve(ncnt, n);
-    int tat = touched(0) ? warp_reserve(&a.ctl->tcnt, __popc(touch_bits)) : 0;
-    for (uint32_t b = keep_bits; b; b &= b - 1) {
-      const int v = i * 32 + __ffs(b) - 1;
-      write_entries(a.w, v, nq, at);
-      at += entry_count(a.w, v);
-      mark[v] = wave;
-      if (touch_bits & (b & (~b + 1))) a.touched[tat++] = v;
-    }
+    });
   }
 }
 
@@ -135,7 +127,8 @@ __device__ __forceinline__ bool level_loop(const GraphView& g, TravArgs& a, int&
 // Phase 1 level: tp[v] holds arrival << 32 and only decreases (RED.MIN); the scan enqueues every
 // relaxed vertex whose arrival dropped below the one it was last enqueued with.
 __device__ __forceinline__ unsigned long long relax_level(const GraphView& g, TravArgs& a, const Work& w,
-                                                          const int32_t* q, int qn, int L, bool dense) {
+                                                          const int32_t* q, int qn, int L, bool dense,
+                                                          const int32_t* hids) {
   const uint32_t wcur = a.wave0 + (uint32_t)L;
   const uint32_t* mcur = a.mark[L & 1];
   uint32_t ax = 0;
@@ -149,8 +142,11 @@ __device__ __forceinline__ unsigned long long relax_level(const GraphView& g, Tr
   auto edge = [&](int, int y, int64_t t) {
     if (!keep_edge(g, a.lo, a.hi, y, t, prev_y)) return true;
     if ((int64_t)ax > t || t >= 0xFFFFFFFFll) return true;
+    const bool hot = hot_is(hids, y);
+    // (a hot successor's arrival has usually dropped to t or below already: no atomic then)
+    if (hot && (int64_t)(__ldcg(&a.tp[y]) >> 32) <= t) return true;
     atomicMin((unsigned long long*)&a.tp[y], (unsigned long long)t << 32);
-    atomicOr(&a.dirty[y >> 5], 1u << (y & 31));
+    if (!hot || !((__ldcg(&a.dirty[y >> 5]) >> (y & 31)) & 1u)) atomicOr(&a.dirty[y >> 5], 1u << (y & 31));
     return true;
   };
   if (dense) return run_order<false, true, true>(g, w, [&](int x) { return __ldcg(&mcur[x]) == wcur; }, begin, edge, [](int) {});
@@ -175,7 +171,8 @@ __device__ __forceinline__ void relax_scan(TravArgs& a, int32_t* nq, int32_t* nc
 // arrival(x) <= t == arrival(y); RED.MIN(hops[y], h + 1) claims y, and the scan enqueues the
 // vertices whose hop level became h + 1 (earlier claims keep their smaller level).
 __device__ __forceinline__ unsigned long long hop_level(const GraphView& g, TravArgs& a, const Work& w,
-                                                        const int32_t* q, int qn, uint32_t h, bool dense) {
+                                                        const int32_t* q, int qn, uint32_t h, bool dense,
+                                                        const int32_t* hids) {
   uint32_t ax = 0;
   int prev_y = -1;
   auto begin = [&](int x, int, int) {
@@ -188,8 +185,10 @@ __device__ __forceinline__ unsigned long long hop_level(const GraphView& g, Trav
     if (!keep_edge(g, a.lo, a.hi, y, t, prev_y)) return true;
     if ((int64_t)ax > t || t >= 0xFFFFFFFFll) return true;
     if ((int64_t)(__ldcg(&a.tp[y]) >> 32) != t) return true;
+    const bool hot = hot_is(hids, y);
+    if (hot && __ldcg(&a.hops[y]) <= h + 1) return true;  // claimed already
     atomicMin(&a.hops[y], h + 1);
-    atomicOr(&a.dirty[y >> 5], 1u << (y & 31));
+    if (!hot || !((__ldcg(&a.dirty[y >> 5]) >> (y & 31)) & 1u)) atomicOr(&a.dirty[y >> 5], 1u << (y & 31));
     return true;
   };
   if (dense) return run_order<false, true, true>(g, w, [&](int x) { return __ldcg(&a.hops[x]) == h; }, begin, edge, [](int) {});
@@ -204,6 +203,8 @@ __global__ void k_barrier_selftest(TravCtl* ctl, uint32_t* err, uint64_t limit_n
 }
 
 __global__ void TGA_TRAVERSE_BOUNDS k_bfs(GraphView g, TravArgs a) {
+  __shared__ int32_t hids[kHotSlots];
+  hot_load(g, hids);  // (the first grid barrier synchronises the block)
   int L = 0;
   unsigned long long mine = 0;
   const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
@@ -216,7 +217,7 @@ __global__ void TGA_TRAVERSE_BOUNDS k_bfs(GraphView g, TravArgs a) {
   if (!grid_sync(a.ctl, g)) return;
   const bool ok1 = level_loop(
       g, a, L,
-      [&](const Work& w, const int32_t* q, int qn, int lv, bool dense) { mine += relax_level(g, a, w, q, qn, lv, dense); },
+      [&](const Work& w, const int32_t* q, int qn, int lv, bool dense) { mine += relax_level(g, a, w, q, qn, lv, dense, hids); },
       [&](int32_t* nq, int32_t* ncnt, int lv) { relax_scan<false>(a, nq, ncnt, lv); });
   if (!ok1) return;
   // Phase 2 from the source again; its levels continue the level numbering of the queues.  The
@@ -229,7 +230,7 @@ __global__ void TGA_TRAVERSE_BOUNDS k_bfs(GraphView g, TravArgs a) {
   const bool ok2 = level_loop(
       g, a, L,
       [&](const Work& w, const int32_t* q, int qn, int lv, bool dense) {
-        mine += hop_level(g, a, w, q, qn, (uint32_t)(lv - L2), dense);
+        mine += hop_level(g, a, w, q, qn, (uint32_t)(lv - L2), dense, hids);
       },
       [&](int32_t* nq, int32_t* ncnt, int lv) {
         const uint32_t claim = (uint32_t)(lv - L2) + 1;
@@ -245,6 +246,9 @@ __global__ void TGA_TRAVERSE_BOUNDS k_bfs(GraphView g, TravArgs a) {
 // Seeds ascend from cc_begin below cc_end: the smallest unreached vertex with outdegree > 9
 // starts a phase-1 traversal; every vertex it reaches gets its component number (last seed wins).
 __global__ void TGA_TRAVERSE_BOUNDS k_cc(GraphView g, TravArgs a) {
+  __shared__ int32_t hids[kHotSlots];
+  hot_load(g, hids);
+  __syncthreads();
   const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
   int L = 0, comp = 0, small_run = 0;
@@ -273,7 +277,7 @@ __global__ void TGA_TRAVERSE_BOUNDS k_cc(GraphView g, TravArgs a) {
     if (!grid_sync(a.ctl, g)) return;
     const bool ok = level_loop(
         g, a, L,
-        [&](const Work& w, const int32_t* q, int qn, int lv, bool dense) { mine += relax_level(g, a, w, q, qn, lv, dense); },
+        [&](const Work& w, const int32_t* q, int qn, int lv, bool dense) { mine += relax_level(g, a, w, q, qn, lv, dense, hids); },
         [&](int32_t* nq, int32_t* ncnt, int lv) { relax_scan<true>(a, nq, ncnt, lv); });
     if (!ok) return;
     const int reach = __ldcg(&a.ctl->tcnt);
