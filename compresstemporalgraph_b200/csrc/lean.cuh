@@ -49,13 +49,11 @@ struct LeanWork {
 // decoded one by one, and a per-lane skip loop only makes the warp diverge.)
 template <bool kRuns = false, bool kTimes = true, bool kRunArg = false, bool kSkip = false, class Want, class Begin,
           class Edge, class End>
-__device__ __forceinline__ unsigned long long run_lean(const GraphView& g, const LeanEntry* entries, int count,
-                                                       const SliceState* slices, const int32_t* run_first, Want want,
-                                                       Begin begin, Edge edge, End end) {
+__device__ __forceinline__ unsigned long long lean_one(const GraphView& g, const LeanEntry* entries, int i,
+                                                       const SliceState* slices, const int32_t* run_first, Want& want,
+                                                       Begin& begin, Edge& edge, End& end) {
   static_assert(!(kSkip && kTimes), "repeats carry their own timestamps");
   unsigned long long edges = 0;
-  const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x);
-  if (i >= count) return 0;
   const LeanEntry e = entries[i];
   LeanCursor c;
   RunFilter rf;
@@ -100,6 +98,30 @@ __device__ __forceinline__ unsigned long long run_lean(const GraphView& g, const
     }
   }
   end(x);
+  return edges;
+}
+
+template <bool kRuns = false, bool kTimes = true, bool kRunArg = false, bool kSkip = false, class Want, class Begin,
+          class Edge, class End>
+__device__ __forceinline__ unsigned long long run_lean(const GraphView& g, const LeanEntry* entries, int count,
+                                                       const SliceState* slices, const int32_t* run_first, Want want,
+                                                       Begin begin, Edge edge, End end) {
+  const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (i >= count) return 0;
+  return lean_one<kRuns, kTimes, kRunArg, kSkip>(g, entries, i, slices, run_first, want, begin, edge, end);
+}
+
+// The same over a fixed grid (a cooperative launch, for the dense levels of the traversals, which
+// sweep the whole schedule with a frontier test in want): chunks of 32 entries are dealt by
+// spread_warp_rank(), so that the slices of one long list, which sit together in the schedule,
+// land on different SMs.
+template <bool kRuns = false, bool kTimes = true, bool kRunArg = false, class Want, class Begin, class Edge, class End>
+__device__ __forceinline__ unsigned long long run_lean_grid(const GraphView& g, const LeanWork& lw, Want want, Begin begin,
+                                                            Edge edge, End end) {
+  unsigned long long edges = 0;
+  const int nthreads = (int)(gridDim.x * blockDim.x);
+  for (int i = spread_warp_rank() * 32 + (int)(threadIdx.x & 31); i < lw.count; i += nthreads)
+    edges += lean_one<kRuns, kTimes, kRunArg, false>(g, lw.e, i, lw.slices, lw.run_first, want, begin, edge, end);
   return edges;
 }
 

@@ -269,6 +269,44 @@ struct LeanCursor {
     return k;
   }
 
+  // Successor-only state (no timestamp window) for a later resume_successors(): the heads and
+  // stream positions in t, the copied-values cursor in cn / ce.
+  __device__ __forceinline__ void save_successors(const GraphView& g, ListState& t, uint32_t& cn, uint32_t& ce) const {
+    t.mpos = mpos;
+    t.ipos = ipos;
+    t.rpos = hr != kInf ? rr.pos(g) : 0;
+    t.hm = hm;
+    t.hi = hi;
+    t.hr = hr;
+    t.hc = hc;
+    t.mleft = mleft;
+    t.mrem = mrem;
+    t.ileft = ileft;
+    t.iend = iend;
+    t.rleft = rleft;
+    cn = cnext;
+    ce = cend;
+  }
+  __device__ __forceinline__ void resume_successors(const GraphView& g, const ListState& t, uint32_t cn, uint32_t ce,
+                                                    int count) {
+    hm = t.hm;
+    mrem = t.mrem;
+    mleft = t.mleft;
+    mpos = t.mpos;
+    hi = t.hi;
+    iend = t.iend;
+    ileft = t.ileft;
+    ipos = t.ipos;
+    hr = t.hr;
+    rleft = t.rleft;
+    hc = t.hc;
+    cnext = cn;
+    cend = ce;
+    if (hr != kInf) rr.init(g, t.rpos);
+    prev = 0;
+    remaining = count;
+  }
+
   // Next (successor, timestamp); false once the entry is exhausted (or on a decode error).
   template <bool kTimes = true>
   __device__ __forceinline__ bool next(const GraphView& g, int& y, int64_t& t) {

@@ -64,10 +64,11 @@ struct GraphSlot {
 // CC windows per round (the job's capacity).
 constexpr int32_t kCcJobWindows = 32;
 // PageRank rounds smaller than this run their queries one call each: the strided batch decodes
-// each list once for all its queries but scatters per query, and below four queries one plain
-// call per query costs less device time (2M/40M graph, 20 iterations: 1 query 16.5 ms plain
-// against 37.9 ms batched, 2 queries 33 against 43.5 ms, 4 queries 65 against 61 ms).
-constexpr size_t kPrBatchMin = 4;
+// each list once for all its queries but scatters per query, and below three queries one plain
+// call per query costs less device time (2M/40M graph, windowed, 20 iterations: 1 query 16.6 ms
+// plain against 32.9 ms batched, 2 queries 33.2 against 37.2 ms, 4 queries 66 against 46 ms,
+// 8 queries 133 against 73 ms).
+constexpr size_t kPrBatchMin = 3;
 
 // Device working bytes of one query (per vertex of its graph): BFS arrival + last-enqueued arrival
 // + result; PageRank three rank vectors + inverse degree + result; CC the single traversal's arrays.

@@ -31,6 +31,7 @@ namespace tga {
 
 struct TravArgs {
   Work w;
+  LeanWork lw;           // lean schedule for the dense levels (run_first: the call's run table)
   TravCtl* ctl;
   int32_t* q[2];
   uint64_t* tp;          // arrival << 32 per vertex (all ones = unreached)
@@ -149,7 +150,7 @@ __device__ __forceinline__ unsigned long long relax_level(const GraphView& g, Tr
     if (!hot || !((__ldcg(&a.dirty[y >> 5]) >> (y & 31)) & 1u)) atomicOr(&a.dirty[y >> 5], 1u << (y & 31));
     return true;
   };
-  if (dense) return run_order<false, true, true>(g, w, [&](int x) { return __ldcg(&mcur[x]) == wcur; }, begin, edge, [](int) {});
+  if (dense) return run_lean_grid<true>(g, a.lw, [&](int x) { return __ldcg(&mcur[x]) == wcur; }, begin, edge, [](int) {});
   return drive_queue<true>(g, w, q, qn, begin, edge, [](int) {});
 }
 
@@ -191,7 +192,7 @@ __device__ __forceinline__ unsigned long long hop_level(const GraphView& g, Trav
     if (!hot || !((__ldcg(&a.dirty[y >> 5]) >> (y & 31)) & 1u)) atomicOr(&a.dirty[y >> 5], 1u << (y & 31));
     return true;
   };
-  if (dense) return run_order<false, true, true>(g, w, [&](int x) { return __ldcg(&a.hops[x]) == h; }, begin, edge, [](int) {});
+  if (dense) return run_lean_grid<true>(g, a.lw, [&](int x) { return __ldcg(&a.hops[x]) == h; }, begin, edge, [](int) {});
   return drive_queue<true>(g, w, q, qn, begin, edge, [](int) {});
 }
 
@@ -339,6 +340,7 @@ static TravArgs trav_args(GraphHandle& h, int64_t t_lo, int64_t t_hi, unsigned l
   TravArgs a{};
   a.w = Work{h.d_items.as<WorkItem>(), h.d_slices.as<SliceState>(), h.d_slice_first.as<int32_t>(), nullptr, h.nitems,
              h.d_order.as<int32_t>(), h.norder, h.d_run_first.as<int32_t>()};
+  a.lw = LeanWork{h.d_lean.as<LeanEntry>(), h.nlean, h.d_slices.as<SliceState>(), h.d_run_first.as<int32_t>()};
   prepare_runs(h, t_lo, t_hi);
   a.ctl = h.s_cnt.as<TravCtl>();
   a.q[0] = h.s_q0.as<int32_t>();
