@@ -149,6 +149,7 @@ def _load() -> C.CDLL:
                                    C.POINTER(_GenSummary)]),
         "tga_encode_raw": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int64, C.POINTER(_GenSummary)]),
         "tga_build_index": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int64]),
+        "tga_build_index_device": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int64]),
         "tga_write_reversed": (C.c_int, [P, P, P, C.c_int64, C.c_int64, C.c_char_p, C.c_char_p,
                                           C.POINTER(_GenSummary)]),
         "tga_reference_depths": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(_RefDepths), P]),
@@ -657,9 +658,11 @@ def reference_depths(directory: str | os.PathLike, basename: str):
     return summary, depth
 
 
-def build_index(directory: str | os.PathLike, basename: str, max_label: int) -> None:
-    """Writes the four GPU index files of a directory that has <base>.offsets (tga_build_index)."""
-    _check(_lib.tga_build_index(str(directory).encode(), basename.encode(), max_label))
+def build_index(directory: str | os.PathLike, basename: str, max_label: int, device: bool = False) -> None:
+    """Writes the four GPU index files of a directory that has <base>.offsets (tga_build_index;
+    with device=True the walks run on the GPU, tga_build_index_device)."""
+    fn = _lib.tga_build_index_device if device else _lib.tga_build_index
+    _check(fn(str(directory).encode(), basename.encode(), max_label))
 
 
 def barrier_selftest(limit_ms: float = 200.0) -> bool:

@@ -25,7 +25,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-r
               "-Xptxas", "-warn-spills"]
 CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-Wall", "-Wno-unused-function"]
 
-CU_SOURCES = ["engine.cu", "algos.cu", "traverse.cu", "batch.cu", "noalloc.cu", "paths.cu"]
+CU_SOURCES = ["engine.cu", "algos.cu", "traverse.cu", "batch.cu", "noalloc.cu", "paths.cu", "indexbuild.cu"]
 CPP_SOURCES = ["format.cpp", "gen.cpp", "hostapi.cpp", "server.cpp"]
 TOOLS = {"tga_tool": "tools/tga_tool.cpp"}
 DROPIN_NAMES = ["bfs", "connected_components", "degree_centrality", "graph_coloring", "hits",

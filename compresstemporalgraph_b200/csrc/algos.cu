@@ -476,22 +476,19 @@ __global__ void k_degree_long(const LongList* longs, int32_t nlong, const int32_
   int64_t mean = 0;     // 64-bit form
   int32_t mean32 = 0;   // narrow form: mean - base
   // Step d (the d-th counted timestamp t, d >= 2): mean += (t - mean) / d (Java long division,
-  // towards zero); when |t - mean| < 2^32 the quotient is a multiply-high and two shifts with d's
-  // entry ml of the division table.
+  // towards zero); when |t - mean| < 2^31 the quotient is one multiply-high and one shift with d's
+  // entry ml of the division table (ml.x = M, ml.y = l - 1).
   auto step = [&](int64_t t, uint2 ml, int d) {
     if constexpr (kNarrow) {
       const int32_t a = (int32_t)(t - base) - mean32;
       const uint32_t x = (uint32_t)(a < 0 ? -a : a);
-      const uint32_t th = __umulhi(ml.x, x);
-      const int32_t q = (int32_t)((th + ((x - th) >> 1)) >> (ml.y - 1));
+      const int32_t q = (int32_t)(__umulhi(ml.x, x) >> ml.y);
       mean32 += a < 0 ? -q : q;
     } else {
       const int64_t a = t - mean;
       const uint64_t na = (uint64_t)(a < 0 ? -a : a);
-      if (na <= 0xFFFFFFFFull) {
-        const uint32_t x = (uint32_t)na;
-        const uint32_t th = __umulhi(ml.x, x);
-        const uint32_t q = (th + ((x - th) >> 1)) >> (ml.y - 1);
+      if (na < 0x80000000ull) {
+        const uint32_t q = __umulhi(ml.x, (uint32_t)na) >> ml.y;
         mean += a < 0 ? -(int64_t)q : (int64_t)q;
       } else {
         mean += a / d;

@@ -170,14 +170,20 @@ __device__ __forceinline__ int nth_set_bit64(uint64_t w, int r) {
   return pos + (r >= (int)(x & 1u));
 }
 
-// Position of the i-th one (0-based) of the upper bits.
+// Position of the i-th one (0-based) of the upper bits.  The scan from the sample is bounded by
+// the bitmap's end, not by a fixed word count: after a hub's record (5M edges, 190M bits of
+// timestamps) the next one lies thousands of words further on.
 __device__ __forceinline__ uint64_t ef_select(const GraphView& g, const EFView& e, uint64_t i) {
   uint64_t p = __ldg(e.samples + (i >> 6));
   int r = (int)(i & 63);
   uint64_t wi = p >> 6;
+  if (wi >= e.upper_words) {
+    set_err(g, kErrIndex);
+    return 0;
+  }
   uint64_t w = __ldg(e.upper + wi) & (~0ull << (p & 63));
 #pragma unroll 1
-  for (int guard = 0; guard < 4096; ++guard) {
+  for (;;) {
     const int c = __popcll(w);
     if (r < c) return wi * 64 + (uint64_t)nth_set_bit64(w, r);
     r -= c;

@@ -263,7 +263,8 @@ int load_graph(GraphHandle& h, const std::string& dir, const std::string& base, 
   if (ts.size() < 8) return fail(TGA_E_FORMAT, "timestamps file shorter than its 64-bit header");
   if (!missing.empty()) {
     // No GPU index files (a directory written by the Java encoder): rebuild their content from
-    // <base>.offsets and the streams (index_from_offsets).
+    // <base>.offsets and the streams, walked on the GPU (offsets_on_device; the host walk
+    // index_from_offsets only if its speculative chunks did not fall into step).
     std::vector<uint8_t> offsets;
     if (!read_file(bp + ".offsets", offsets))
       return fail(TGA_E_IO, "Cannot open required file: " + missing + " (nor " + bp +
@@ -273,7 +274,17 @@ int load_graph(GraphHandle& h, const std::string& dir, const std::string& base, 
     if (it == pr.end()) return fail(TGA_E_FORMAT, "rebuilding the index needs the nodes property of " + bp + ".properties");
     try {
       EFIndex ge, te;
-      index_from_offsets(graph, offsets, ts, std::atoll(it->second.c_str()), 2, cfg.max_label, &ge, &te);
+      const int64_t nodes = std::atoll(it->second.c_str());
+      std::vector<uint64_t> goff, toff;
+      const int drc = offsets_on_device(graph, offsets, ts, nodes, goff, toff);
+      if (drc == TGA_OK) {
+        ge = ef_build(goff, ef_low_bits(graph.size(), cfg.max_label));
+        te = ef_build(toff, ef_low_bits(ts.size(), cfg.max_label));
+      } else if (drc == TGA_E_TIMEOUT) {
+        index_from_offsets(graph, offsets, ts, nodes, 2, cfg.max_label, &ge, &te);
+      } else {
+        return drc;
+      }
       gl = std::move(ge.lower);
       gu = std::move(ge.upper);
       tl = std::move(te.lower);
@@ -385,16 +396,17 @@ int load_graph(GraphHandle& h, const std::string& dir, const std::string& base, 
   // The largest outdegree caps every header-driven loop of the decoder on damaged streams.
   v.max_list = (int32_t)std::min<int64_t>(INT32_MAX / 4, std::max<int64_t>(maxd, 1));
   {
-    // Per count d: l = ceil(log2 d) and m = floor(2^32 (2^l - d) / d) + 1, so that for any 32-bit
-    // n, n / d = (t + ((n - t) >> 1)) >> (l - 1) with t = mulhi(m, n) (Granlund and Montgomery,
-    // "Division by Invariant Integers using Multiplication", PLDI 1994, Fig. 4.1); d = 1 divides
-    // trivially.  Entry 0 is unused.
+    // Per count d >= 2: l = ceil(log2 d) and M = ceil(2^(31 + l) / d), which is below 2^32, so that
+    // for every n < 2^31, n / d = mulhi(M, n) >> (l - 1) (Granlund and Montgomery, "Division by
+    // Invariant Integers using Multiplication", PLDI 1994: with M d - 2^(31+l) = e < d <= 2^l,
+    // n e < 2^(31+l) keeps the rounding error below one step).  Stored as (M, l - 1); d = 1
+    // divides trivially and entry 0 is unused.
     std::vector<uint32_t> tab(2 * ((size_t)v.max_list + 2), 0);
     for (uint64_t d = 2; d < (uint64_t)v.max_list + 2; ++d) {
       int l = 0;
       while ((1ull << l) < d) ++l;
-      tab[2 * d] = (uint32_t)(((1ull << 32) * ((1ull << l) - d)) / d + 1);
-      tab[2 * d + 1] = (uint32_t)l;
+      tab[2 * d] = (uint32_t)(((1ull << (31 + l)) + d - 1) / d);
+      tab[2 * d + 1] = (uint32_t)(l - 1);
     }
     if ((rc = upload(h, h.d_divtab, tab))) return rc;
   }

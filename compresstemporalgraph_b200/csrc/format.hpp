@@ -142,6 +142,14 @@ void index_from_offsets(const std::vector<uint8_t>& graph, const std::vector<uin
                         const std::vector<uint8_t>& timestamps, int64_t n, int ts_zeta_k, int64_t max_label,
                         EFIndex* graph_ef, EFIndex* ts_ef);
 
+// The same offsets walked on the GPU (indexbuild.cu: speculative chunked decoding of the offsets
+// and timestamp streams): graph record offsets goff[0..n] and timestamp offsets toff[0..n], which
+// ef_build packs as index_from_offsets does.  Returns a TGA_E_* code (TGA_E_TIMEOUT when the
+// speculative chunks did not fall into step, for which the host walk is the answer).
+int offsets_on_device(const std::vector<uint8_t>& graph, const std::vector<uint8_t>& offsets,
+                      const std::vector<uint8_t>& timestamps, int64_t n, std::vector<uint64_t>& goff,
+                      std::vector<uint64_t>& toff);
+
 std::map<std::string, std::string> read_properties(const std::string& path);
 
 // Realised reference-chain depth of every list (ReferenceDepthScanner.java:24-87): a list that

@@ -185,6 +185,34 @@ int tga_encode_raw(const char* raw_path, const char* dir, const char* base, int6
   return TGA_OK;
 }
 
+static int write_index(const std::string& d, const EFIndex& ge, const EFIndex& te) {
+  if (!write_file(d + "/graph_lower_bits.bin", ge.lower.data(), ge.lower.size()) ||
+      !write_file(d + "/graph_upper_bits.bin", ge.upper.data(), ge.upper.size()) ||
+      !write_file(d + "/timestamp_lower_bits.bin", te.lower.data(), te.lower.size()) ||
+      !write_file(d + "/timestamp_upper_bits.bin", te.upper.data(), te.upper.size()))
+    return fail(TGA_E_IO, "cannot write the index files into " + d);
+  return TGA_OK;
+}
+
+int tga_build_index_device(const char* dir, const char* base, int64_t max_label) {
+  if (!dir || !base || max_label < 0) return fail(TGA_E_ARG, "bad argument");
+  const std::string d(dir), bp = d + "/" + base;
+  std::vector<uint8_t> graph, offsets, ts;
+  if (!read_file(bp + ".graph", graph)) return fail(TGA_E_IO, "Cannot open required file: " + bp + ".graph");
+  if (!read_file(bp + ".timestamps", ts)) return fail(TGA_E_IO, "Cannot open required file: " + bp + ".timestamps");
+  if (!read_file(bp + ".offsets", offsets)) return fail(TGA_E_IO, "Cannot open required file: " + bp + ".offsets");
+  const auto pr = read_properties(bp + ".properties");
+  const auto it = pr.find("nodes");
+  if (it == pr.end()) return fail(TGA_E_FORMAT, "the nodes property of " + bp + ".properties is needed");
+  std::vector<uint64_t> goff, toff;
+  if (int rc = offsets_on_device(graph, offsets, ts, std::atoll(it->second.c_str()), goff, toff)) return rc;
+  try {
+    return write_index(d, ef_build(goff, ef_low_bits(graph.size(), max_label)), ef_build(toff, ef_low_bits(ts.size(), max_label)));
+  } catch (const std::exception& e) {
+    return fail(TGA_E_FORMAT, std::string("packing the index: ") + e.what());
+  }
+}
+
 int tga_build_index(const char* dir, const char* base, int64_t max_label) {
   if (!dir || !base || max_label < 0) return fail(TGA_E_ARG, "bad argument");
   const std::string d(dir), bp = d + "/" + base;
@@ -198,11 +226,7 @@ int tga_build_index(const char* dir, const char* base, int64_t max_label) {
   try {
     EFIndex ge, te;
     index_from_offsets(graph, offsets, ts, std::atoll(it->second.c_str()), 2, max_label, &ge, &te);
-    if (!write_file(d + "/graph_lower_bits.bin", ge.lower.data(), ge.lower.size()) ||
-        !write_file(d + "/graph_upper_bits.bin", ge.upper.data(), ge.upper.size()) ||
-        !write_file(d + "/timestamp_lower_bits.bin", te.lower.data(), te.lower.size()) ||
-        !write_file(d + "/timestamp_upper_bits.bin", te.upper.data(), te.upper.size()))
-      return fail(TGA_E_IO, "cannot write the index files into " + d);
+    return write_index(d, ge, te);
   } catch (const std::exception& e) {
     return fail(TGA_E_FORMAT, std::string("rebuilding the index from .offsets: ") + e.what());
   }

@@ -413,6 +413,11 @@ int tga_reference_depths(const char* dir, const char* base, tga_ref_depths* out,
  * outdegree (EvolvingMultiGraph.java:131-275); needs the nodes property of <base>.properties.
  * tga_open does the same in memory when the index files are missing. */
 int tga_build_index(const char* dir, const char* base, int64_t max_label);
+/* The same files with the two walks run on the GPU: the offsets and timestamp streams decoded
+ * speculatively in 4096-bit chunks, each chunk redecoded from its predecessor's exit until the
+ * chunks fall into step, then every offset written in parallel.  TGA_E_TIMEOUT if the chunks do
+ * not settle in 64 rounds (tga_build_index then gives the files). */
+int tga_build_index_device(const char* dir, const char* base, int64_t max_label);
 
 /* 65536-entry 16-bit look-ahead decode table, (length << 16) | value, 0 if the code does not fit;
  * kind 0 = gamma (gpu_cuda/decode_tables/gammaInA.txt), 3 = zeta_3 (zetaInA.txt). */

@@ -27,7 +27,12 @@ HUB1M = tga.GenParams(n=3000, m=5_000_000, deg_exponent=1.5, max_degree=4_000_00
 SKEW1M = tga.GenParams(n=1_000_000, m=20_000_000, deg_exponent=1.6, max_degree=100_000, repeat_frac=0.3, local_frac=0.7,
                        local_radius=64, pref_frac=0.5, copy_frac=0.2, ts_kind=2, ts_span=100_000_000, seed=5,
                        hub_count=2, hub_degree=500_000)
-SHAPES = {"all7": tga.CONFIGS["all7"], "hub1m": HUB1M, "skew1m": SKEW1M}
+# A 5M-edge hub among 2M short lists: its record spans ~190M bits of timestamps, so the Elias-Fano
+# upper bits after it hold a run of over a million zeros (thousands of words between two ones).
+HUBGAP = tga.GenParams(n=2_000_000, m=8_000_000, deg_exponent=2.0, max_degree=20_000, repeat_frac=0.3, local_frac=0.7,
+                       local_radius=64, pref_frac=0.5, copy_frac=0.2, ts_kind=1, ts_span=100_000_000, seed=9,
+                       hub_count=1, hub_degree=5_000_000)
+SHAPES = {"all7": tga.CONFIGS["all7"], "hub1m": HUB1M, "skew1m": SKEW1M, "hubgap": HUBGAP}
 
 
 class Big:
@@ -65,6 +70,9 @@ def test_shape_is_what_it_claims(big):
         assert big.summary["m"] == 40_000_000 and big.n == 2_000_000
     elif big.cfg.name == "hub1m":
         assert big.deg.max() >= 1_000_000
+    elif big.cfg.name == "hubgap":
+        assert big.n == 2_000_000 and int(big.deg.max()) == 5_000_000
+        return
     else:
         assert big.n == 1_000_000 and int((big.deg == 500_000).sum()) == 2
     assert big.summary["max_chain"] == 3

@@ -1,6 +1,7 @@
 """The GPU index files rebuilt from the webgraph offsets (what a directory written by the Java
-encoder holds instead of them): byte-identical to the files the encoder writes, and a graph opened
-without them decodes the same lists."""
+encoder holds instead of them): byte-identical to the files the encoder writes, whether the walks
+run on the host (tga_build_index) or on the GPU (tga_build_index_device, speculative chunked
+decoding), and a graph opened without them decodes the same lists."""
 from __future__ import annotations
 
 import shutil
@@ -51,3 +52,28 @@ def test_open_without_index_files(datasets, tmp_path, shape):
         for x, y in zip(ca, cb):
             assert np.array_equal(x, y)
         assert np.array_equal(a.bfs(0)[0], b.bfs(0)[0])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape", ["small", "chains", "hubs", "intervals", "sparse"])
+def test_device_rebuilt_index_files_equal_encoder_output(datasets, tmp_path, shape):
+    d = datasets[shape]
+    out = _strip(d, tmp_path, shape)
+    tga.build_index(out, d["base"], d["summary"]["n"] - 1, device=True)
+    for f in INDEX_FILES:
+        assert (out / f).read_bytes() == (d["dir"] / f).read_bytes(), f
+
+
+@pytest.mark.gpu
+def test_device_rebuilt_index_at_bench_size(tmp_path):
+    # 2M vertices / 40M edges: 46K chunks of the timestamp stream, most entered mid-code at first.
+    name = "all7"
+    src = tmp_path / "src"
+    tga.generate(tga.CONFIGS[name], src, name)
+    out = tmp_path / "out"
+    shutil.copytree(src, out)
+    for f in INDEX_FILES:
+        (out / f).unlink()
+    tga.build_index(out, name, tga.CONFIGS[name].n - 1, device=True)
+    for f in INDEX_FILES:
+        assert (out / f).read_bytes() == (src / f).read_bytes(), f
