@@ -614,12 +614,15 @@ def run_skew(args):
         for _ in range(args.warmup):
             fn()
         ms = edges = 0.0
+        iters = 0
         for _ in range(args.steps):
             fn()
             t = g.timing()
             ms += t["total_ms"]
             edges += t["edges_decoded"]
-        out[wl] = {"ms": ms / args.steps, "edges": int(edges / args.steps), "gteps": edges / (ms / 1e3) / 1e9}
+            iters = t["iterations"]
+        out[wl] = {"ms": ms / args.steps, "edges": int(edges / args.steps), "gteps": edges / (ms / 1e3) / 1e9,
+                   "iterations": iters}
     _, _, deg = g.neighbor_access()
     g.close()
     tot_edges = sum(v["edges"] for v in out.values())

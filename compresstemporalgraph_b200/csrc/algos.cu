@@ -189,7 +189,9 @@ __device__ __forceinline__ float temporal_weight(float alpha, int64_t t) {
   return a > 18.0f ? 1.0f : 1.0f - expf(-a);
 }
 
-// k_pr_iter over the lean schedule.
+// k_pr_iter over the lean schedule (kAll: the window holds every timestamp of the graph, so no
+// edge is tested against it).
+template <bool kAll>
 __global__ void TGA_LEAN_BOUNDS k_pr_iter(GraphView g, LeanWork lw, PrArgs a) {
   TGA_HOT_SHARED(float, hot)
   hot.init(g);
@@ -220,7 +222,7 @@ __global__ void TGA_LEAN_BOUNDS k_pr_iter(GraphView g, LeanWork lw, PrArgs a) {
         return true;
       },
       [&](int, int y, int64_t t) {
-        if (!keep_edge(g, a.lo, a.hi, y, t, prev_y)) return true;
+        if (!(kAll ? keep_edge_all(g, y, prev_y) : keep_edge(g, a.lo, a.hi, y, t, prev_y))) return true;
         const float contrib = c0 * temporal_weight(a.alpha, t);
         if (!hot.add(y, contrib)) atomicAdd(&a.out[y], contrib);
         local += contrib;
@@ -300,7 +302,7 @@ __global__ void TGA_LEAN_BOUNDS k_hits_hub(GraphView g, LeanWork lw, double* hub
         return true;
       },
       [&](int, int y, int64_t t) {
-        if (keep_edge(g, lo, hi, y, t, prev_y)) acc += (float)auth_in[y];
+        if (kTimes ? keep_edge(g, lo, hi, y, t, prev_y) : keep_edge_all(g, y, prev_y)) acc += (float)auth_in[y];
         return 2;  // repeats of y add nothing
       },
       [&](int v) {
@@ -334,7 +336,8 @@ __global__ void TGA_LEAN_BOUNDS k_hits_auth(GraphView g, LeanWork lw, const doub
         return true;
       },
       [&](int, int y, int64_t t) {
-        if (keep_edge(g, lo, hi, y, t, prev_y) && !hot.add(y, hn)) atomicAdd(&auth_next[y], (double)hn);
+        if ((kTimes ? keep_edge(g, lo, hi, y, t, prev_y) : keep_edge_all(g, y, prev_y)) && !hot.add(y, hn))
+          atomicAdd(&auth_next[y], (double)hn);
         return 2;  // repeats of y add nothing
       },
       [&](int) {});
@@ -866,6 +869,7 @@ int tga_pagerank(tga_graph* gp, int32_t iters, float damping, float alpha, int64
   if (t_lo >= t_hi) return fail(TGA_E_ARG, "empty time window");
   const int32_t nv = h.view.max_vertex;
   const bool windowed = !(t_lo <= 0 && t_hi == TGA_T_MAX);
+  const bool all_times = window_covers_all(h, t_lo, t_hi);
   TGA_TRY(h.s_a.ensure((size_t)nv * 4));
   TGA_TRY(h.s_b.ensure((size_t)nv * 4));
   TGA_TRY(h.s_c.ensure((size_t)nv * 4));
@@ -901,7 +905,8 @@ int tga_pagerank(tga_graph* gp, int32_t iters, float damping, float alpha, int64
       PrArgs a{invdeg, h.d_deg.as<int32_t>(), bufs[k % 3], bufs[(k + 1) % 3], bufs[(k + 2) % 3], sums, k,
                damping, alpha, base, t_lo, t_hi, edges};
       cudaEvent_t* ev = h.kernel_begin();
-      KL(k_pr_iter, lean_grid(h))(h.view, lean_work(h), a);
+      if (all_times) KL(k_pr_iter<true>, lean_grid(h))(h.view, lean_work(h), a);
+      else KL(k_pr_iter<false>, lean_grid(h))(h.view, lean_work(h), a);
       h.kernel_end(ev);
     }
     return TGA_OK;
@@ -1151,6 +1156,7 @@ int tga_pagerank_noalloc(tga_graph* gp, int32_t iters, float damping, float alph
                h.d_order.as<int32_t>(), h.norder, h.d_run_first.as<int32_t>()};
   prepare_runs(h, t_lo, t_hi);  // fills the handle's run table (allocated at open)
   const bool windowed = !(t_lo <= 0 && t_hi == TGA_T_MAX);
+  const bool all_times = window_covers_all(h, t_lo, t_hi);
   const float base = (1.0f - damping) / (float)h.view.max_label;
   KL(k_fill_f32, grid_for(nv, kBlock))(bufs[0], 1.0f / (float)nv, nv);
   KL(k_fill_f32, grid_for(nv, kBlock))(bufs[1], base, nv);
@@ -1167,7 +1173,8 @@ int tga_pagerank_noalloc(tga_graph* gp, int32_t iters, float damping, float alph
   for (int k = 0; k < iters; ++k) {
     PrArgs a{invdeg, h.d_deg.as<int32_t>(), bufs[k % 3], bufs[(k + 1) % 3], bufs[(k + 2) % 3], sums, k,
              damping, alpha, base, t_lo, t_hi, edges};
-    KL(k_pr_iter, lean_grid(h))(h.view, lean_work(h), a);
+    if (all_times) KL(k_pr_iter<true>, lean_grid(h))(h.view, lean_work(h), a);
+    else KL(k_pr_iter<false>, lean_grid(h))(h.view, lean_work(h), a);
   }
   KL(k_pr_final, grid_for(nv, kBlock))(bufs[iters % 3], sums, iters - 1, rank_out_dev, nv);
   h.timing.iterations = iters;

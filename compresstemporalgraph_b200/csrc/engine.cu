@@ -640,9 +640,12 @@ int build_work(GraphHandle& h, int32_t slice_len, int32_t item_edges) {
     tmp_ids.release();
   }
   // A traversal level sweeps all lists instead of its queue once the queue holds at least
-  // 1/TGA_DENSE_DIV (default 16) of the schedule's entries.
+  // 1/TGA_DENSE_DIV of the schedule's entries.  Default 1 (a sweep only when every entry is in the
+  // frontier): with the lean decoder the queue is the faster form at every level size measured
+  // (2M/40M graph: BFS 11.3 ms with divisor 16, 7.5 with 4, 7.1 with 2 or 1; CC 39.6 / 37.3 /
+  // 35.8 / 35.8 ms).
   const char* env_dense = std::getenv("TGA_DENSE_DIV");
-  const int dense_div = h.dense_div > 0 ? h.dense_div : env_dense ? std::max(1, std::atoi(env_dense)) : 16;
+  const int dense_div = h.dense_div > 0 ? h.dense_div : env_dense ? std::max(1, std::atoi(env_dense)) : 1;
   h.dense_min = std::max<int32_t>(1, h.norder / dense_div);
   h.nslices = (int64_t)packed.size();
   h.slice_len = slice_len;
@@ -817,7 +820,7 @@ int tga_autotune(tga_graph* g, tga_tune_result* out) {
   tga_tune_result r{};
   r.slice_edges = h.slice_len;
   r.item_edges = h.item_edges;
-  r.dense_div = h.dense_div > 0 ? h.dense_div : 16;
+  r.dense_div = h.dense_div > 0 ? h.dense_div : 1;
   TGA_TRY(probe(&r.default_ms));
   r.best_ms = r.default_ms;
   r.candidates = 1;
@@ -835,7 +838,7 @@ int tga_autotune(tga_graph* g, tga_tune_result* out) {
       }
     }
   const int32_t base_div = r.dense_div;
-  for (int32_t dd : {8, 16, 32}) {
+  for (int32_t dd : {1, 2, 4}) {
     if (dd == base_div) continue;
     h.dense_div = dd;
     TGA_TRY(build_work(h, r.slice_edges, r.item_edges));

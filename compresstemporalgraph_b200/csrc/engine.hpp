@@ -91,7 +91,7 @@ struct GraphHandle {
   DevBuf d_view;                     // device-global copy of `view` (GraphView::self)
   int32_t norder = 0;
   int32_t dense_min = 1;             // traversal levels with at least this many entries sweep all lists
-  int32_t dense_div = 0;             // dense_min = schedule entries / dense_div (0: $TGA_DENSE_DIV or 16)
+  int32_t dense_div = 0;             // dense_min = schedule entries / dense_div (0: $TGA_DENSE_DIV or 1)
   std::vector<uint8_t> chain_host;   // list copies from a reference chain
   int32_t nitems = 0, nslice_items = 0;
   int64_t nslices = 0;

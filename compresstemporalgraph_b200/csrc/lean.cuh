@@ -81,7 +81,6 @@ __device__ __forceinline__ unsigned long long lean_one(const GraphView& g, const
   int y;
   int64_t t;
   while (c.template next<kTimes>(g, y, t)) {
-    ++edges;
     const bool pass = !kRuns || rf.pass(y);
     if constexpr (kSkip) {
       if (!pass) continue;
@@ -90,7 +89,6 @@ __device__ __forceinline__ unsigned long long lean_one(const GraphView& g, const
       // (a slice inside a run whose kept edge is still ahead goes on edge by edge)
       if (r == 2 && (!kRuns || rf.lead == kNoRunFilter || rf.lead < rf.idx)) {
         const int k = c.skip_repeats(g, y);
-        edges += (unsigned)k;
         if (kRuns) rf.idx += k;
       }
     } else {
@@ -98,6 +96,8 @@ __device__ __forceinline__ unsigned long long lean_one(const GraphView& g, const
     }
   }
   end(x);
+  // decoded edges (repeats consumed by skip_repeats included): what the cursor no longer holds
+  edges = (unsigned long long)(cnt - max(c.remaining, 0));
   return edges;
 }
 

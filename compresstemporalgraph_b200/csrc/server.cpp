@@ -63,12 +63,14 @@ struct GraphSlot {
 
 // CC windows per round (the job's capacity).
 constexpr int32_t kCcJobWindows = 32;
-// PageRank rounds smaller than this run their queries one call each: the strided batch decodes
-// each list once for all its queries but scatters per query, and below three queries one plain
-// call per query costs less device time (2M/40M graph, windowed, 20 iterations: 1 query 16.6 ms
-// plain against 32.9 ms batched, 2 queries 33.2 against 37.2 ms, 4 queries 66 against 46 ms,
-// 8 queries 133 against 73 ms).
-constexpr size_t kPrBatchMin = 3;
+// PageRank rounds smaller than this run their queries one call each.  The strided batch decodes
+// each list once for all its queries but scatters per query, and every query of a batch gets its
+// result when the whole batch ends: measured on the 2M/40M graph (windowed, 20 iterations), one
+// call per query takes 16.6 ms, a batch of 2 37.2 ms, of 4 46 ms, of 8 73 ms.  From three queries
+// the batch costs less device time, but the queries' summed completion times (what latency sees)
+// are lower for one call after the other until about eight (4: 184 against 166 ms; 8: 584 against
+// 598 ms), so the server batches PageRank only from eight waiting queries.
+constexpr size_t kPrBatchMin = 8;
 
 // Device working bytes of one query (per vertex of its graph): BFS arrival + last-enqueued arrival
 // + result; PageRank three rank vectors + inverse degree + result; CC the single traversal's arrays.

@@ -145,6 +145,12 @@ __device__ __forceinline__ bool keep_edge(const GraphView& g, int64_t lo, int64_
   prev_y = y;
   return y >= g.active_begin && y < g.max_vertex;
 }
+// The same for a window that holds every timestamp of the graph (no time test).
+__device__ __forceinline__ bool keep_edge_all(const GraphView& g, int y, int& prev_y) {
+  if (y == prev_y) return false;
+  prev_y = y;
+  return y >= g.active_begin && y < g.max_vertex;
+}
 
 // Rank of the calling warp when warps are dealt round-robin over the blocks (warp k of block b has
 // rank k * gridDim.x + b): consecutive 32-entry chunks then go to different blocks, so a run of

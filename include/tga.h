@@ -106,7 +106,7 @@ int tga_get_work_params(tga_graph* g, int32_t* slice_edges, int32_t* item_edges,
 /* Project autotuner (no reference counterpart): times the workloads whose speed depends on the
  * work decomposition (one PageRank and one HITS iteration, a full-window BFS, a full-window CC and
  * a CC over the middle half of the timestamp span) for slice lengths {16, 24, 32, 48} x item sizes {128, 256, 512}, then the
- * dense-level divisor {8, 16, 32} (a traversal level sweeps every list once its queue holds
+ * dense-level divisor {1, 2, 4} (a traversal level sweeps every list once its queue holds
  * 1/dense_div of the schedule), and leaves the graph configured with the fastest.  Results of
  * every call are independent of the choice.  CC jobs made before it refuse to run afterwards. */
 typedef struct {

@@ -256,7 +256,7 @@ def test_autotune_keeps_results(pairs):
         r = p.g.autotune()
         assert r["slice_edges"] in (16, 24, 32, 48) and r["item_edges"] in (128, 256, 512)
         # the starting configuration is timed once (one fewer grid point when it lies on the grid)
-        assert r["dense_div"] in (8, 16, 32) and r["candidates"] in (14, 15)
+        assert r["dense_div"] in (1, 2, 4) and r["candidates"] in (14, 15)
         assert 0 < r["best_ms"] <= r["default_ms"]
         assert p.g.work_params()["slice_edges"] == r["slice_edges"]
         off, dst, ts = p.g.decode_all()
