@@ -18,6 +18,7 @@
 #include <cstring>
 #include <vector>
 
+#include "gridsync.cuh"
 #include "hot.cuh"
 #include "lean.cuh"
 #include "sweep.cuh"
@@ -230,6 +231,7 @@ __global__ void TGA_LEAN_BOUNDS k_pr_iter(GraphView g, LeanWork lw, PrArgs a) {
       },
       [&](int) { total += (double)local; });
   hot.flush(a.out);
+  // (per warp: per-block sums measured 0.782 against 0.764 ms per launch here)
   add_edges(a.edges, mine);
   warp_add(&a.sums[a.k], total);
 }
@@ -308,7 +310,7 @@ __global__ void TGA_LEAN_BOUNDS k_hits_hub(GraphView g, LeanWork lw, double* hub
       [&](int v) {
         if (acc != 0.0f) atomicAdd(&hub[v], (double)(acc * sa));
       });
-  add_edges(edges, mine);
+  block_add_edges(edges, mine);
 }
 
 template <bool kTimes>
@@ -342,7 +344,7 @@ __global__ void TGA_LEAN_BOUNDS k_hits_auth(GraphView g, LeanWork lw, const doub
       },
       [&](int) {});
   hot.flush(auth_next);
-  add_edges(edges, mine);
+  block_add_edges(edges, mine);
 }
 
 __global__ void k_sumsq(const double* v, int32_t n, double* out) {
@@ -662,23 +664,36 @@ __global__ void TGA_LEAN_BOUNDS k_gc_check(GraphView g, const int32_t* entries, 
 __global__ void k_gc_decide(GraphView g, const int32_t* wl, int32_t wn, const int32_t* deg, uint32_t* color,
                             const uint32_t* found, uint32_t round, int java_isolated, int32_t* out_wl, int32_t* out_n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= wn) return;
-  const int x = wl[i];
-  if (x < g.active_begin || x > g.max_label || color[x] != kColorInf) return;
-  if (x >= g.n || deg[x] == 0) {
-    if (java_isolated) color[x] = round;
-    return;
+  int x = -1;
+  bool keep = false;  // stays uncoloured: joins the next worklist
+  if (i < wn) {
+    x = wl[i];
+    if (x >= g.active_begin && x <= g.max_label && color[x] == kColorInf) {
+      if (x >= g.n || deg[x] == 0) {
+        if (java_isolated) color[x] = round;
+      } else if (found[x] == round + 1) {
+        keep = true;
+      } else {
+        color[x] = round;
+      }
+    }
   }
-  if (found[x] == round + 1) out_wl[atomicAdd(out_n, 1)] = x;
-  else color[x] = round;
+  // places reserved per warp (all lanes of the warp take part)
+  const int at = warp_reserve(out_n, keep ? 1 : 0);
+  if (keep) out_wl[at] = x;
 }
 
-__global__ void k_gc_first(GraphView g, Work w, const int32_t* deg, int32_t n, int32_t* wl, int32_t* wn,
-                           int32_t* entries, int32_t* en) {
+// The first round: every vertex on the worklist (in order), the entries of every list with edges
+// in the queue (places reserved per warp: one atomic per vertex on one counter would queue 2M
+// requests at one L2 slice).
+__global__ void k_gc_first(GraphView g, Work w, const int32_t* deg, int32_t n, int32_t* wl, int32_t* entries,
+                           int32_t* en) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  if (x >= n) return;
-  wl[atomicAdd(wn, 1)] = x;
-  if (x >= g.active_begin && x <= g.max_label && x < g.n && deg[x] > 0) enqueue(w, x, entries, en);
+  const bool in = x < n;
+  if (in) wl[x] = x;
+  const bool listed = in && x >= g.active_begin && x <= g.max_label && x < g.n && deg[x] > 0;
+  const int at = warp_reserve(en, listed ? entry_count(w, x) : 0);
+  if (listed) write_entries(w, x, entries, at);
 }
 
 // Host side: the queue entries of one vertex (itself or its slices).
@@ -1077,7 +1092,7 @@ int tga_color(tga_graph* gp, int32_t prio_mode, const uint32_t* prio_in, int32_t
   cudaMemsetAsync(found, 0, (size_t)nv * 4, h.stream);
   int32_t* cnt = h.s_cnt.as<int32_t>();  // [0] worklist, [1] entries
   cudaMemsetAsync(cnt, 0, 8, h.stream);
-  KL(k_gc_first, grid_for(nv, kBlock))(h.view, w, h.d_deg.as<int32_t>(), nv, h.s_q0.as<int32_t>(), cnt,
+  KL(k_gc_first, grid_for(nv, kBlock))(h.view, w, h.d_deg.as<int32_t>(), nv, h.s_q0.as<int32_t>(),
                                        h.s_d.as<int32_t>(), cnt + 1);
   DevBuf *wl = &h.s_q0, *nwl = &h.s_q1, *en = &h.s_d, *nen = &h.s_e;
   int32_t wn = nv, ne = 0;

@@ -80,7 +80,7 @@ constexpr int kSparseSlots = kWarpSources - 1;
 __device__ __forceinline__ unsigned long long multi_relax_sparse(const GraphView& g, MultiArgs& a, const Work& w,
                                                                  const int64_t* slo, const int64_t* shi,
                                                                  const int32_t* scol, const int32_t* q, int qn, int L,
-                                                                 bool dense, const int32_t* hids) {
+                                                                 bool dense) {
   const uint64_t* Fc = a.F[L & 1];
   uint64_t* Fn = a.F[(L + 1) & 1];
   int src[kSparseSlots];     // source of slot i (-1: empty)
@@ -133,7 +133,6 @@ __device__ __forceinline__ unsigned long long multi_relax_sparse(const GraphView
       yprev = y;
     }
     const bool usable = y >= g.active_begin && y < g.max_vertex && t >= 0 && t < 0xFFFFFFFFll;
-    const bool hot = usable && hot_is(hids, y);
     uint64_t add0 = 0, add1 = 0, add2 = 0, add3 = 0;
 #pragma unroll
     for (int i = 0; i < kSparseSlots; ++i) {
@@ -142,7 +141,9 @@ __device__ __forceinline__ unsigned long long multi_relax_sparse(const GraphView
       if (t < slo[s] || t >= shi[s]) continue;
       seen |= 1u << i;
       if (!usable || (int64_t)ax[i] > t) continue;
-      if (hot && __ldcg(a.arr + arr_at(a, y, s)) <= (uint32_t)t) continue;  // nothing to lower
+      // An arrival already at t or earlier needs no atomic (measured on the CC of 2M/40M: checking
+      // every successor, not only the hot ones, 36.3 -> 34.8 ms).
+      if (__ldcg(a.arr + arr_at(a, y, s)) <= (uint32_t)t) continue;
       atomicMin(a.arr + arr_at(a, y, s), (uint32_t)t);
       const uint64_t bit = 1ull << (s & 63);
       const int wd = s >> 6;
@@ -153,7 +154,7 @@ __device__ __forceinline__ unsigned long long multi_relax_sparse(const GraphView
     }
     if (add0 | add1 | add2 | add3) {
       unsigned long long* f = (unsigned long long*)(Fn + (size_t)y * kWords);
-      if (hot) {  // bits another relaxation of this level has set already need no atomic
+      {  // bits another relaxation of this level has set already need no atomic
         if (add0 && (__ldcg(f + 0) & add0) == add0) add0 = 0;
         if (add1 && (__ldcg(f + 1) & add1) == add1) add1 = 0;
         if (add2 && (__ldcg(f + 2) & add2) == add2) add2 = 0;
@@ -163,7 +164,7 @@ __device__ __forceinline__ unsigned long long multi_relax_sparse(const GraphView
       if (add1) atomicOr(f + 1, (unsigned long long)add1);
       if (add2) atomicOr(f + 2, (unsigned long long)add2);
       if (add3) atomicOr(f + 3, (unsigned long long)add3);
-      if (!hot || !((__ldcg(&a.dirty[y >> 5]) >> (y & 31)) & 1u)) atomicOr(&a.dirty[y >> 5], 1u << (y & 31));
+      if (!((__ldcg(&a.dirty[y >> 5]) >> (y & 31)) & 1u)) atomicOr(&a.dirty[y >> 5], 1u << (y & 31));
     }
     return true;
   };
@@ -364,7 +365,7 @@ __device__ bool multi_levels(const GraphView& g, MultiArgs& a, const int64_t* sl
     if (qn > 0) {
       Work w = a.w;
       w.next = &ctl->next[L % 3];
-      mine += multi_relax_sparse(g, a, w, slo, shi, scol, a.q[L & 1], qn, L, qn >= a.dense_min, hids);
+      mine += multi_relax_sparse(g, a, w, slo, shi, scol, a.q[L & 1], qn, L, qn >= a.dense_min);
     }
     if (!grid_sync(ctl, g)) return false;
     multi_scan(a, a.q[L & 1], qn, a.dq[L & 1], dn, a.q[(L + 1) & 1], &ctl->cnt[(L + 1) % 3], a.dq[(L + 1) & 1],

@@ -63,6 +63,15 @@ __device__ __forceinline__ double block_sum(double v) {
   return s;  // valid in thread 0
 }
 
+// Edge count summed over the block and added once per block (every thread of the block must call
+// it): a sweep of 12,653 blocks would otherwise send 101K atomics to one L2 slice.  The count
+// passes through a double, exact below 2^53.
+__device__ __forceinline__ void block_add_edges(unsigned long long* ctr, unsigned long long mine) {
+  const double s = block_sum((double)mine);
+  if (threadIdx.x == 0 && s != 0.0) atomicAdd(ctr, (unsigned long long)s);
+  __syncthreads();  // (the shared partials are free again)
+}
+
 // Sum of v over the warp, added to *out by lane 0 (no block barrier: warps leave independently).
 __device__ __forceinline__ void warp_add(double* out, double v) {
   for (int o = 16; o; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -221,6 +230,20 @@ __device__ __forceinline__ unsigned long long run_order(const GraphView& g, cons
 // Flat loop over the entries q[0..qn) of a queue (vertices or slices); q may have been written
 // earlier in the same launch by other blocks (it is read through L2).  kRuns, kTimes, kRunArg as
 // in run_order.
+// Next index of a shared work counter for the calling lane: the lanes of the warp that ask at the
+// same time take consecutive indexes with one atomic.  (One atomic per entry sends every request
+// of the level to one L2 slice: on the 2M/40M graph's CC, levels of 1.4M entries spent most of
+// their time queued there.)
+__device__ __forceinline__ int take_next(int32_t* counter) {
+  const unsigned act = __activemask();
+  const int lane = (int)(threadIdx.x & 31);
+  const int leader = __ffs(act) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(counter, __popc(act));
+  base = __shfl_sync(act, base, leader);
+  return base + __popc(act & ((1u << lane) - 1u));
+}
+
 template <bool kRuns = false, bool kTimes = true, bool kRunArg = false, class Begin, class Edge, class End>
 __device__ __forceinline__ unsigned long long drive_queue(const GraphView& g, const Work& w, const int32_t* q, int qn,
                                                           Begin begin, Edge edge, End end) {
@@ -248,7 +271,7 @@ __device__ __forceinline__ unsigned long long drive_queue(const GraphView& g, co
         end(cur);
         cur = -1;
       }
-      if (i < 0) i = nthreads + atomicAdd(w.next, 1);
+      if (i < 0) i = nthreads + take_next(w.next);
       if (i >= qn) break;
       int first, count, lead, run;
       const int x = open_entry(g, w, __ldcg(q + i), c, first, count, lead, run);
