@@ -403,13 +403,14 @@ constexpr int64_t kDcSkip = INT64_MIN;
 
 __global__ void TGA_TRAVERSE_BOUNDS k_degree_slices(GraphView g, const SliceState* slices, const int64_t* ebase,
                                                   int32_t nslices, int64_t s, int64_t e, int64_t* buf,
-                                                  unsigned long long* edges) {
+                                                  int32_t* scnt, unsigned long long* edges) {
   const bool all = (s == 0 && e == 0);
   const int lim = min(g.max_label + 1, g.max_vertex);
   unsigned long long mine = 0;
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j < nslices) {
     const SliceState& sl = slices[j];
+    int counted = 0;
     if (sl.v >= g.active_begin && sl.v <= g.max_label) {
       LeanCursor c;
       c.restore(g, sl);
@@ -417,50 +418,55 @@ __global__ void TGA_TRAVERSE_BOUNDS k_degree_slices(GraphView g, const SliceStat
       int y;
       int64_t t;
       while (c.next(g, y, t)) {
-        *out++ = (y >= g.active_begin && y < lim && (all || (s <= t && e >= t))) ? t : kDcSkip;
+        const bool in = y >= g.active_begin && y < lim && (all || (s <= t && e >= t));
+        *out++ = in ? t : kDcSkip;
+        counted += in;
         ++mine;
       }
     }
+    scnt[j] = counted;
   }
   add_edges(edges, mine);
 }
 
-// Compaction of each long list's segment to its counted timestamps (one block per list, chunks of
-// the block's size in order: every thread reads its element, a block scan of the counted flags
-// gives the write positions, then the block writes, so writes never pass unread elements); the
-// count goes to cnt[i].  The running mean below then reads its k-th input and the divisor entry of
-// k + 1 at addresses known in advance.
-__global__ void k_degree_compact(const LongList* longs, int32_t nlong, const int32_t* outdeg, int64_t* buf,
-                                 int32_t active, int32_t max_label, int32_t* cnt) {
-  const int i = blockIdx.x;
-  if (i >= nlong) return;
+// Where each slice's counted timestamps go in the compacted buffer: one warp per long list scans
+// its slices' counts 32 at a time; cnt[i] = the list's counted total.
+__global__ void k_degree_bases(const LongList* longs, int32_t nlong, const int32_t* slice_first, const int32_t* scnt,
+                               int32_t active, int32_t max_label, int64_t* cbase, int32_t* cnt) {
+  constexpr unsigned kFull = 0xffffffffu;
+  const int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = (int)(threadIdx.x & 31);
+  if (i >= nlong) return;  // (whole warps leave together)
   const int v = longs[i].v;
   if (v < active || v > max_label) return;
-  int64_t* p = buf + longs[i].base;
-  const int n = outdeg[v];
-  __shared__ int warp_tot[kBlock / 32];
-  __shared__ int base_s;
-  if (threadIdx.x == 0) base_s = 0;
-  __syncthreads();
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  for (int c0 = 0; c0 < n; c0 += blockDim.x) {
-    const int k = c0 + (int)threadIdx.x;
-    const int64_t t = k < n ? p[k] : kDcSkip;
-    const int f = t != kDcSkip;
-    const unsigned bal = __ballot_sync(0xffffffffu, f);
-    const int before = __popc(bal & ((1u << lane) - 1u));
-    if (lane == 31) warp_tot[wid] = before + f;
-    __syncthreads();
-    int off = base_s;
-    for (int w = 0; w < wid; ++w) off += warp_tot[w];
-    int total = 0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) total += warp_tot[w];
-    __syncthreads();  // every thread has read p[k] and the totals
-    if (f) p[off + before] = t;
-    if (threadIdx.x == 0) base_s += total;
-    __syncthreads();
+  const int a = slice_first[v], b = slice_first[v + 1];
+  int64_t running = longs[i].base;
+  for (int j0 = a; j0 < b; j0 += 32) {
+    const int j = j0 + lane;
+    const int c = j < b ? scnt[j] : 0;
+    int incl = c;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int u = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += u;
+    }
+    if (j < b) cbase[j] = running + incl - c;
+    running += __shfl_sync(kFull, incl, 31);
   }
-  if (threadIdx.x == 0) cnt[i] = base_s;
+  if (lane == 0) cnt[i] = (int32_t)(running - longs[i].base);
+}
+
+// The counted timestamps of every slice to their place in the compacted buffer (one thread per
+// slice, so the longest list's compaction is spread over all of its slices).
+__global__ void k_degree_gather(const SliceState* slices, int32_t nslices, const int64_t* ebase, const int64_t* cbase,
+                                const int32_t* scnt, const int64_t* buf, int64_t* cbuf) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nslices || scnt[j] == 0) return;
+  const int64_t* in = buf + ebase[j];
+  int64_t* out = cbuf + cbase[j];
+  const int n = slices[j].count;
+  for (int k = 0; k < n; ++k) {
+    const int64_t t = in[k];
+    if (t != kDcSkip) *out++ = t;
+  }
 }
 
 // kNarrow: every timestamp t of the graph satisfies 0 <= t - base < 2^31 (base = the smallest),
@@ -1010,8 +1016,11 @@ int tga_degree(tga_graph* gp, int64_t t_start, int64_t t_end, int32_t* degree_ou
   TGA_TRY(h.s_a.ensure((size_t)nv * 4));
   TGA_TRY(h.s_b.ensure((size_t)nv * 8));
   if (h.nlong > 0) {
-    TGA_TRY(h.s_edges.ensure((size_t)h.long_edges * 8));
-    TGA_TRY(h.s_c.ensure((size_t)h.nlong * 4));
+    TGA_TRY(h.s_edges.ensure((size_t)h.long_edges * 8));  // per-edge timestamps (or skips) of the sliced lists
+    TGA_TRY(h.s_f.ensure((size_t)h.long_edges * 8));      // their counted timestamps, compacted per list
+    TGA_TRY(h.s_c.ensure((size_t)h.nlong * 4));           // counted per list
+    TGA_TRY(h.s_d.ensure((size_t)h.nslices * 4));         // counted per slice
+    TGA_TRY(h.s_e.ensure((size_t)h.nslices * 8));         // compacted base per slice
   }
   TGA_TRY(h.begin_call());
   unsigned long long* edges = edge_counter(h);
@@ -1023,16 +1032,22 @@ int tga_degree(tga_graph* gp, int64_t t_start, int64_t t_end, int32_t* degree_ou
   if (h.nlong > 0) {
     cudaEvent_t* ev2 = h.kernel_begin();
     KL(k_degree_slices, grid_for(h.nslices, kBlock))(h.view, h.d_slices.as<SliceState>(), h.d_slice_ebase.as<int64_t>(),
-                                                     (int32_t)h.nslices, t_start, t_end, h.s_edges.as<int64_t>(), edges);
+                                                     (int32_t)h.nslices, t_start, t_end, h.s_edges.as<int64_t>(),
+                                                     h.s_d.as<int32_t>(), edges);
     h.kernel_end(ev2);
     // Narrow form when the graph's whole timestamp span fits 31 bits (max_ts found at load).
     const bool narrow = h.max_ts != INT64_MAX && h.min_ts_data >= 0 && h.max_ts - h.min_ts_data < INT32_MAX;
     int32_t* cnt = h.s_c.as<int32_t>();
-    KL(k_degree_compact, h.nlong)(h.d_long.as<LongList>(), h.nlong, h.d_deg.as<int32_t>(), h.s_edges.as<int64_t>(),
-                                  h.view.active_begin, h.view.max_label, cnt);
+    KL(k_degree_bases, grid_for((int64_t)h.nlong * 32, kBlock))(h.d_long.as<LongList>(), h.nlong,
+                                                                h.d_slice_first.as<int32_t>(), h.s_d.as<int32_t>(),
+                                                                h.view.active_begin, h.view.max_label,
+                                                                h.s_e.as<int64_t>(), cnt);
+    KL(k_degree_gather, grid_for(h.nslices, kBlock))(h.d_slices.as<SliceState>(), (int32_t)h.nslices,
+                                                     h.d_slice_ebase.as<int64_t>(), h.s_e.as<int64_t>(),
+                                                     h.s_d.as<int32_t>(), h.s_edges.as<int64_t>(), h.s_f.as<int64_t>());
     auto long_kernel = narrow ? k_degree_long<true> : k_degree_long<false>;
     KL(long_kernel, grid_for(h.nlong, kBlock))(h.d_long.as<LongList>(), h.nlong, cnt,
-                                               h.s_edges.as<int64_t>(), h.d_divtab.as<uint2>(), h.min_ts_data,
+                                               h.s_f.as<int64_t>(), h.d_divtab.as<uint2>(), h.min_ts_data,
                                                h.view.active_begin, h.view.max_label, t_start, t_end,
                                                h.s_a.as<int32_t>(), h.s_b.as<int64_t>());
   }

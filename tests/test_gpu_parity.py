@@ -621,3 +621,33 @@ def test_shortest_paths_rejects_bad_input(pairs):
         p.g.shortest(0, 10, 10)
     with pytest.raises(tga.TgaError):
         p.g.shortest(p.mv)
+
+
+@pytest.mark.parametrize("shape", ["hubs", "chains"])
+def test_dense_levels_equal_queue_levels(datasets, shape, monkeypatch):
+    """With the default divisor a level sweeps the whole schedule only when every entry is in its
+    frontier; TGA_DENSE_DIV=64 (read at open) makes every level with 1/64 of the entries a sweep,
+    so the dense paths of BFS (phase 1 and hops), the one-seed and batched CC and the multi-source
+    BFS give the oracle's results as well."""
+    monkeypatch.setenv("TGA_DENSE_DIV", "64")
+    p = Pair(datasets[shape])
+    try:
+        off, _, _ = p.o.csr()
+        src = int(np.argmax(np.diff(off)))
+        for lo, hi in _windows(p)[:2]:
+            arr, hops = p.g.bfs(src, lo, hi)
+            oarr, ohops = p.o.bfs(p.ml, p.mv, p.act, src, lo, hi)
+            assert np.array_equal(arr, oarr) and np.array_equal(hops, ohops), (lo, hi)
+            for one_seed in (False, True):
+                lab, k = p.g.connected_components(lo, hi, early_exit=False, one_seed=one_seed)
+                olab, ok = p.o.cc(p.ml, p.mv, p.act, p.cfg.connected_components_vertex_begin, lo, hi, False)
+                assert k == ok and np.array_equal(lab, olab), (lo, hi, one_seed)
+        srcs = np.arange(0, p.n, max(1, p.n // 40), dtype=np.int32)[:40]
+        lo = np.zeros(len(srcs), np.int64)
+        hi = np.full(len(srcs), T_MAX, np.int64)
+        out = p.g.bfs_batch(srcs, lo, hi)
+        for i in range(0, len(srcs), 5):
+            oarr, _ = p.o.bfs(p.ml, p.mv, p.act, int(srcs[i]), 0, T_MAX)
+            assert np.array_equal(out[i], oarr), i
+    finally:
+        p.g.close()
