@@ -291,7 +291,7 @@ __global__ void k_hits_base(double* hub, const double* auth_in, double* auth_nex
 }
 
 template <bool kTimes>
-__global__ void TGA_LEAN_BOUNDS k_hits_hub(GraphView g, LeanWork lw, double* hub, const double* auth_in,
+__global__ void TGA_LEAN_BOUNDS5 k_hits_hub(GraphView g, LeanWork lw, double* hub, const double* auth_in,
                                            const double* aprev, int64_t lo, int64_t hi, unsigned long long* edges) {
   const float sa = (aprev && *aprev > 0) ? (float)(1.0 / sqrt(*aprev)) : 1.0f;
   float acc = 0.0f;
@@ -314,7 +314,7 @@ __global__ void TGA_LEAN_BOUNDS k_hits_hub(GraphView g, LeanWork lw, double* hub
 }
 
 template <bool kTimes>
-__global__ void TGA_LEAN_BOUNDS k_hits_auth(GraphView g, LeanWork lw, const double* hub, const double* hsum,
+__global__ void TGA_LEAN_BOUNDS5 k_hits_auth(GraphView g, LeanWork lw, const double* hub, const double* hsum,
                                             double* auth_next, int64_t lo, int64_t hi, unsigned long long* edges) {
   // Hot authorities take block-local FP32 partials (a few hundred contributions per block),
   // added to the FP64 accumulators once per block.
@@ -602,7 +602,7 @@ struct GcPoint {
 // One round's check: one queue entry per thread (round 0 opens every entry, later rounds resume
 // the blocked ones from their points).  A blocked entry marks its vertex (found = round + 1),
 // saves its point and joins the next round's queue.
-__global__ void TGA_LEAN_BOUNDS k_gc_check(GraphView g, const int32_t* entries, int32_t en, int32_t nv,
+__global__ void TGA_LEAN_BOUNDS5 k_gc_check(GraphView g, const int32_t* entries, int32_t en, int32_t nv,
                                            const uint32_t* color, const uint32_t* prio, uint32_t round,
                                            uint32_t* found, GcPoint* pts, int32_t* next, int32_t* next_cnt,
                                            unsigned long long* edges) {

@@ -8,8 +8,12 @@
 
 namespace tga {
 
-// Lean sweeps: 4 blocks of 256 per SM (up to 64 registers, no local memory).
+// Lean sweeps: 4 blocks of 256 per SM (up to 64 registers, no local memory).  The HITS sweeps and
+// the colouring check run with 5 (51 registers and a few spilled words): measured on the 2M/40M
+// graph, HITS x30 29.1 -> 27.5 ms and colouring 4.13 -> 3.99 ms, while PageRank and neighbour
+// access were slower that way (23.4 -> 25.8 ms, 0.58 -> 0.62 ms) and keep 4.
 #define TGA_LEAN_BOUNDS __launch_bounds__(kBlock, 4)
+#define TGA_LEAN_BOUNDS5 __launch_bounds__(kBlock, 5)
 
 // Schedule entry of a lean sweep: v >= 0 a whole list whose record starts at bit gbit of the
 // graph stream and whose timestamps start at bit tbit; v < 0 the slice -(v+1) (positions unused).
