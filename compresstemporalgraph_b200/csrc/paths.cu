@@ -205,7 +205,7 @@ extern "C" int tga_latest_departure(tga_graph* rev, int64_t pivot, int32_t targe
 // where only the vertices whose A dropped at level k-1 are expanded, reading A_{k-1} (prev) while
 // writing A_k (next) with RED.MIN, so every level is deterministic; hops[v] is the first k with
 // A_k[v] finite, and the last A is the earliest arrival (tga_bfs's).
-#include "sweep.cuh"
+#include "gridsync.cuh"
 
 namespace tga {
 
@@ -244,21 +244,25 @@ __global__ void TGA_TRAVERSE_BOUNDS k_sp_relax(GraphView g, Work w, SpArgs a, co
 
 // After level `level`: every vertex whose arrival dropped takes it, gets its hop count if it was
 // unreached, and joins the next queue (itself, or all its slices).
+// (the marked vertices of a warp's 32 words dealt over its lanes, queue places reserved per warp)
 __global__ void k_sp_scan(Work w, uint32_t* prev, const uint32_t* next, uint32_t* dirty, int32_t* hops, int32_t nwords,
                           int32_t level, int32_t* q, int32_t* qcnt) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nwords) return;
-  uint32_t bits = dirty[i];
-  if (!bits) return;
-  dirty[i] = 0;
-  while (bits) {
-    const int b = __ffs(bits) - 1;
-    bits &= bits - 1;
-    const int y = i * 32 + b;
-    if (prev[y] == kSpInf) hops[y] = level;
-    prev[y] = next[y];
-    enqueue(w, y, q, qcnt);
+  const int base = i & ~31;
+  if (base >= nwords) return;  // (whole warps leave together)
+  uint32_t bits = 0;
+  if (i < nwords) {
+    bits = dirty[i];
+    if (bits) dirty[i] = 0;
   }
+  deal_dirty(bits, base, [&](int y) {
+    if (y >= 0) {
+      if (prev[y] == kSpInf) hops[y] = level;
+      prev[y] = next[y];
+    }
+    const int at = warp_reserve(qcnt, y >= 0 ? entry_count(w, y) : 0);
+    if (y >= 0) write_entries(w, y, q, at);
+  });
 }
 
 __global__ void k_sp_unpack(const uint32_t* prev, int32_t* arr, int32_t n) {
