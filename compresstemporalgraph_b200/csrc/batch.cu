@@ -402,7 +402,8 @@ __device__ __forceinline__ void load_windows(const MultiArgs& a, int64_t* slo, i
   __syncthreads();
 }
 
-__global__ void TGA_DECODE_BOUNDS k_bfs_multi(GraphView g, MultiArgs a) {
+// 3 blocks per SM (80 registers): 8 sources on the 2M/40M graph 22.0 -> 21.3 ms against 2 blocks.
+__global__ void TGA_TRAVERSE_BOUNDS k_bfs_multi(GraphView g, MultiArgs a) {
   __shared__ int64_t slo[kMaxSources], shi[kMaxSources];
   __shared__ int32_t scol[kMaxSources];
   __shared__ int32_t hids[kHotSlots];
