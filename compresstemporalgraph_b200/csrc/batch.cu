@@ -710,7 +710,11 @@ struct CcSlots {
   int32_t total;                // live slots of the batch
 };
 
-constexpr int kCcMinK = 4;
+// Smallest (and first) number of candidates a batch takes.  Measured on the 2M/40M graph (full
+// window / window over the middle half of the span): 4 -> 34.5 / 38.7 ms, 16 -> 34.3 / 38.1,
+// 64 -> 32.4 / 36.5, 128 -> 31.7 / 37.3, 256 -> 38.7 / 35.9 ms; the seeds before the giant
+// component reach few vertices, so small first batches spend their levels on little work.
+constexpr int kCcMinK = 64;
 constexpr int64_t kCcWasteAllowance = 4096;  // reach a batch may throw away and still grow K
 
 // Every block: slot ranges of this batch from the queries' states (same result in every block).
