@@ -698,6 +698,7 @@ struct CcArgs {
   int32_t nq;
   int32_t end;                  // candidates lie below this vertex
   int32_t early;                // apply the early exits
+  int32_t min_k;                // first and smallest number of candidates a batch takes
   int64_t limit;                // early exit: reach total above this
   int64_t budget_ns;            // stop at a batch boundary once the launch ran this long (0: never)
 };
@@ -710,11 +711,16 @@ struct CcSlots {
   int32_t total;                // live slots of the batch
 };
 
-// Smallest (and first) number of candidates a batch takes.  Measured on the 2M/40M graph (full
-// window / window over the middle half of the span): 4 -> 34.5 / 38.7 ms, 16 -> 34.3 / 38.1,
-// 64 -> 32.4 / 36.5, 128 -> 31.7 / 37.3, 256 -> 38.7 / 35.9 ms; the seeds before the giant
-// component reach few vertices, so small first batches spend their levels on little work.
-constexpr int kCcMinK = 64;
+// Smallest (and first) number of candidates a batch takes, by the number of candidate vertices.
+// Measured on the 2M/40M graph (full window / window over the middle half of the span): 4 -> 34.5
+// / 38.7 ms, 16 -> 34.3 / 38.1, 64 -> 32.4 / 36.5, 128 -> 31.7 / 37.3, 256 -> 38.7 / 35.9 ms; the
+// seeds before the giant component reach few vertices, so small first batches spend their levels
+// on little work.  On the 6,000-vertex / 120,000-edge graph the first seed reaches most of the
+// graph and the early exit stops after a few seeds: 4 -> 1.28 ms, 64 -> 9.8 ms (each extra seed
+// of the first batch is a traversal of the whole graph that is thrown away).
+constexpr int kCcMinKSmall = 4;
+constexpr int kCcMinKLarge = 64;
+constexpr int32_t kCcLargeGraph = 1 << 20;
 constexpr int64_t kCcWasteAllowance = 4096;  // reach a batch may throw away and still grow K
 
 // Every block: slot ranges of this batch from the queries' states (same result in every block).
@@ -877,7 +883,7 @@ __device__ void cc_validate(const CcArgs& c, int q, int base, int n, uint32_t (*
   // Over the limit now: the next real seed would stop the loop before labelling anything.
   if (c.early && total > c.limit) stop = true;
   if (8 * wasted <= useful + kCcWasteAllowance) K = min(2 * K, kMaxSources);
-  else if (wasted > useful + kCcWasteAllowance) K = max(kCcMinK, K / 2);
+  else if (wasted > useful + kCcWasteAllowance) K = max(c.min_k, K / 2);
   st->total = total;
   st->v = v;
   st->comp = comp;
@@ -1090,6 +1096,7 @@ static int cc_job_create(GraphHandle& h, int32_t cap, int32_t flags, tga_cc_job*
   c.cand = nullptr;  // set per step (the handle's source slots)
   c.end = std::min(std::min(h.view.max_label, (int32_t)nv), h.view.n);
   c.early = (flags & TGA_CC_EARLY_EXIT) ? 1 : 0;
+  c.min_k = c.end >= kCcLargeGraph ? kCcMinKLarge : kCcMinKSmall;
   c.limit = (int64_t)(0.8 * h.view.max_label);
   j->used.assign((size_t)cap, 0);
   j->st.assign((size_t)cap, CcBatchState{});
@@ -1117,7 +1124,7 @@ static int cc_job_add(tga_cc_job* j, int64_t t_lo, int64_t t_hi, int32_t* slot) 
   CcArgs& c = j->args;
   CcBatchState s0{};
   s0.v = std::max(h.cfg.cc_vertex_begin, 0);
-  s0.K = kCcMinK;
+  s0.K = c.min_k;
   j->st[(size_t)q] = s0;
   // Pageable sources: each copy is staged before the call returns.
   TGA_CUDA_TRY(cudaMemcpyAsync(c.st + q, &s0, sizeof s0, cudaMemcpyHostToDevice, h.stream));
