@@ -24,7 +24,8 @@ library is never loaded there) and the same seven-workload step, run by the C po
 reference's algorithms on the host cores with every list decoded at each visit; PageRank and HITS
 run a sample of their 30 iterations and the step's time is projected from it.
 Multi-GPU runs are independent replicas (every graph fits one GPU; nothing is exchanged): time is
-the slowest rank's, edges are summed over ranks.
+the slowest rank's, edges are summed over ranks; the forms, the CPU baseline and the FP64 check
+run only at N = 1.
 """
 from __future__ import annotations
 
@@ -829,7 +830,9 @@ def main():
         "workloads": breakdown,
         "timestamp_reading": timestamp_reading,
     }
-    if rank == 0 and not args.no_forms and not ONLY:
+    # The forms, the CPU baseline and the FP64 check describe the one-GPU line; a replica run
+    # (N > 1) reports the replicas' figures only, so its GPUs are held for the timed work alone.
+    if rank == 0 and world == 1 and not args.no_forms and not ONLY:
         try:
             extra = []
             names = [nm for nm in args.served_graphs.split(",") if nm and nm != CONFIG_NAME]
@@ -854,7 +857,7 @@ def main():
             line["ref_gpu"] = ref_gpu_section(tga)
         except Exception as e:  # reported, not fatal
             line["ref_gpu"] = {"error": str(e)}
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(ddir, summary, 0)
         except Exception as e:  # reported, not fatal
