@@ -62,8 +62,8 @@ struct GraphHandle {
   DevBuf d_graph, d_ts, d_gl, d_gu, d_gs, d_tl, d_tu, d_ts_samples, d_err;
   // per-vertex outdegrees (int32, filled once at load by a decode kernel)
   DevBuf d_deg;
-  // division by a running count d in [1, max outdegree] by multiplication: (m, l) per d (algos.cu,
-  // degree centrality); built at load
+  // division by a running count d in [2, max outdegree + 1] by multiplication: (M, l - 1) per d
+  // (k_degree_long in algos.cu, degree centrality); built at load
   DevBuf d_divtab;
   // edge-balanced work decomposition (slices.cuh): slices of long lists, work items, and
   // slice_first[v]..slice_first[v+1] = slices of vertex v (empty for short lists)

@@ -7,7 +7,7 @@
 // read the arrival (and frontier bits) of a hot successor before relaxing it: after its first
 // levels its arrival is rarely lowered, and the atomic that would change nothing is not sent.
 //
-// The set is chosen once at load (build_hot, engine.cu): the kHotMax vertices with the largest
+// The set is chosen once at load (build_hot, algos.cu): the kHotMax vertices with the largest
 // in-degree (counted over all arcs by k_in_degree), those with at least kHotMinShare of the arcs,
 // placed in a direct-mapped table of kHotSlots ids indexed by a multiplicative hash (a vertex whose
 // slot is taken by a hotter one stays on the global path).  The device table holds the ids
