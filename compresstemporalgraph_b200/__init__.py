@@ -608,6 +608,10 @@ CONFIGS = {
     "served10m": GenParams(n=10_000_000, m=200_000_000, deg_exponent=2.0, max_degree=200_000, repeat_frac=0.30,
                            local_frac=0.70, local_radius=64, pref_frac=0.5, copy_frac=0.20, ts_kind=1,
                            ts_span=100_000_000, seed=4),
+    # Served-form resident graph of 50M vertices / 1B temporal edges.
+    "served50m": GenParams(n=50_000_000, m=1_000_000_000, deg_exponent=2.0, max_degree=1_000_000, repeat_frac=0.30,
+                           local_frac=0.70, local_radius=64, pref_frac=0.5, copy_frac=0.20, ts_kind=1,
+                           ts_span=100_000_000, seed=4),
     # Skew stress: Zipf 1.6 out-degrees plus 16 hubs of 5M out-edges each (block-scale lists), bursty
     # timestamps (10% of the edges in 1% of the span).
     "skew": GenParams(n=100_000_000, m=2_000_000_000, deg_exponent=1.6, max_degree=5_000_000, repeat_frac=0.30,
