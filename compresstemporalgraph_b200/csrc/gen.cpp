@@ -5,9 +5,12 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <exception>
 #include <numeric>
 #include <stdexcept>
 #include <string>
+#include <thread>
+#include <utility>
 #include <vector>
 
 #include "format.hpp"
@@ -94,26 +97,58 @@ GenSummary generate_dataset(const GenParams& p, const std::string& dir, const st
 
   const int threads = encode_threads();  // 0: node by node; the files are the same either way
   constexpr int64_t kBlockNodes = 1 << 16;
-  std::vector<int32_t> bsucc;     // the block's successor lists, back to back
-  std::vector<int64_t> bts;       // and their timestamps
-  std::vector<int64_t> boff{0};   // list i of the block: [boff[i], boff[i+1])
-  auto flush = [&]() {
-    const int nb = (int)boff.size() - 1;
-    if (nb == 0) return;
+  struct Block {
+    std::vector<int32_t> succ;    // the block's successor lists, back to back
+    std::vector<int64_t> ts;      // and their timestamps
+    std::vector<int64_t> off{0};  // list i of the block: [off[i], off[i+1])
+    int nodes() const { return (int)off.size() - 1; }
+  };
+  // While one block is generated (one sequential random stream), the block before it is encoded
+  // on its own thread (with the encoders' own worker threads).  Blocks reach the encoders one at a
+  // time and in node order, so the files are the same as with no overlap.
+  Block fill, busy;
+  std::thread encoder;
+  std::exception_ptr encoder_error;
+  auto encode_block = [&](const Block& b) {
+    const int nb = b.nodes();
     std::vector<const int32_t*> sp((size_t)nb);
     std::vector<const int64_t*> tp((size_t)nb);
     std::vector<int> len((size_t)nb);
     for (int i = 0; i < nb; ++i) {
-      sp[(size_t)i] = bsucc.data() + boff[(size_t)i];
-      tp[(size_t)i] = bts.data() + boff[(size_t)i];
-      len[(size_t)i] = (int)(boff[(size_t)i + 1] - boff[(size_t)i]);
+      sp[(size_t)i] = b.succ.data() + b.off[(size_t)i];
+      tp[(size_t)i] = b.ts.data() + b.off[(size_t)i];
+      len[(size_t)i] = (int)(b.off[(size_t)i + 1] - b.off[(size_t)i]);
     }
     ge.add_block(sp.data(), len.data(), nb, threads);
     te.add_block(tp.data(), len.data(), nb, threads);
-    bsucc.clear();
-    bts.clear();
-    boff.assign(1, 0);
   };
+  auto wait_encoder = [&]() {
+    if (encoder.joinable()) encoder.join();
+    if (encoder_error) std::rethrow_exception(std::exchange(encoder_error, nullptr));
+  };
+  auto flush = [&]() {
+    if (fill.nodes() == 0) return;
+    wait_encoder();
+    std::swap(fill, busy);
+    fill.succ.clear();
+    fill.ts.clear();
+    fill.off.assign(1, 0);
+    encoder = std::thread([&] {
+      try {
+        encode_block(busy);
+      } catch (...) {
+        encoder_error = std::current_exception();
+      }
+    });
+  };
+  // Declared after everything the encoder thread uses, so an exception leaving this function
+  // joins the thread before those are destroyed.
+  struct Joiner {
+    std::thread& t;
+    ~Joiner() {
+      if (t.joinable()) t.join();
+    }
+  } joiner{encoder};
 
   const int W = 7;
   std::vector<std::vector<int32_t>> ring(W + 1);  // distinct successors of the last vertices
@@ -203,10 +238,10 @@ GenSummary generate_dataset(const GenParams& p, const std::string& dir, const st
       ge.add_node(succ.data(), (int)succ.size());
       te.add_node(ts.data(), (int)ts.size());
     } else {
-      bsucc.insert(bsucc.end(), succ.begin(), succ.end());
-      bts.insert(bts.end(), ts.begin(), ts.end());
-      boff.push_back((int64_t)bsucc.size());
-      if ((int64_t)boff.size() - 1 == kBlockNodes) flush();
+      fill.succ.insert(fill.succ.end(), succ.begin(), succ.end());
+      fill.ts.insert(fill.ts.end(), ts.begin(), ts.end());
+      fill.off.push_back((int64_t)fill.succ.size());
+      if (fill.nodes() == kBlockNodes) flush();
     }
     if (raw)
       for (size_t i = 0; i < succ.size(); ++i) std::fprintf(raw, "%lld\t%d\t1\t%lld\n", (long long)v, succ[i], (long long)ts[i]);
@@ -214,6 +249,7 @@ GenSummary generate_dataset(const GenParams& p, const std::string& dir, const st
     sum.max_degree = std::max<int64_t>(sum.max_degree, (int64_t)succ.size());
   }
   flush();
+  wait_encoder();
   ge.finish();
   te.finish();
   if (raw) std::fclose(raw);

@@ -1,5 +1,6 @@
 """The block-parallel encoder (reference costs on threads, choices in order, records joined bit by
-bit) writes the same files and statistics as the node-by-node encoder, whatever the thread count."""
+bit) writes the same files and statistics as the node-by-node encoder, whatever the thread count;
+with blocks, the generator encodes each block on its own thread while it generates the next."""
 from __future__ import annotations
 
 import os
