@@ -29,6 +29,8 @@ inline int msb64(uint64_t v) { return v ? 63 - __builtin_clzll(v) : -1; }
 inline uint64_t int2nat(int64_t x) { return x >= 0 ? (uint64_t)x << 1 : ((uint64_t)(-(x + 1)) << 1) | 1u; }
 inline int64_t nat2int(uint64_t n) { return (n & 1) ? -(int64_t)(n >> 1) - 1 : (int64_t)(n >> 1); }
 
+class WordWriter;
+
 class BitWriter {
  public:
   std::vector<uint8_t> bytes;
@@ -77,24 +79,98 @@ class BitWriter {
     return u + write_minimal_binary(v - left, (left << k) - left);
   }
   int write_long(uint64_t x, int len) { write_bits(x, len); return len; }
-  // Appends all bits of o (whose bits past o.nbits are zero, as every BitWriter keeps them).
-  void append(const BitWriter& o) {
-    const uint64_t ob = (o.nbits + 7) / 8;
-    const int used = (int)(nbits & 7);
-    const size_t old = bytes.size();
-    if (used == 0) {
-      bytes.insert(bytes.end(), o.bytes.begin(), o.bytes.begin() + (ptrdiff_t)ob);
-    } else {
-      bytes.resize(old + ob, 0);
-      for (uint64_t i = 0; i < ob; ++i) {
-        bytes[old - 1 + i] |= (uint8_t)(o.bytes[i] >> used);
-        bytes[old + i] |= (uint8_t)(o.bytes[i] << (8 - used));
-      }
-    }
-    nbits += o.nbits;
-    bytes.resize((nbits + 7) / 8);
-  }
+  // Appends all bits of a finished WordWriter.
+  inline void append_words(const WordWriter& o);
 };
+
+// The same codes written a 64-bit word at a time (MSB-first within each word), for the encoders'
+// per-thread streams, which BitWriter::append_words joins into the byte stream; the bits are the
+// ones BitWriter writes for the same calls.  finish() before the words are read.
+class WordWriter {
+ public:
+  std::vector<uint64_t> words;  // complete words (after finish(): every bit written)
+  uint64_t nbits = 0;
+
+  // Appends the low `len` bits of `v`, most significant first (len <= 64).
+  void write_bits(uint64_t v, int len) {
+    if (len <= 0) return;
+    if (len < 64) v &= (1ull << len) - 1;
+    nbits += (uint64_t)len;
+    const int room = 64 - pend_;
+    if (len < room) {
+      acc_ |= v << (room - len);
+      pend_ += len;
+      return;
+    }
+    const int rest = len - room;  // bits of v that do not fit in the current word
+    acc_ |= rest ? v >> rest : v;
+    words.push_back(acc_);
+    acc_ = rest ? v << (64 - rest) : 0;
+    pend_ = rest;
+  }
+  int write_unary(uint64_t x) {
+    uint64_t z = x;
+    while (z >= 32) { write_bits(0, 32); z -= 32; }
+    write_bits(1, (int)z + 1);
+    return (int)x + 1;
+  }
+  int write_gamma(uint64_t x) {
+    const uint64_t v = x + 1;
+    const int m = msb64(v);
+    write_unary((uint64_t)m);
+    if (m) write_bits(v, m);
+    return 2 * m + 1;
+  }
+  int write_minimal_binary(uint64_t x, uint64_t b) {
+    const int lb = msb64(b);
+    const uint64_t m = (lb + 1 >= 64 ? 0ull : (1ull << (lb + 1))) - b;
+    if (x < m) { if (lb) write_bits(x, lb); return lb; }
+    write_bits(x + m, lb + 1);
+    return lb + 1;
+  }
+  int write_zeta(uint64_t x, int k) {
+    const uint64_t v = x + 1;
+    const int h = msb64(v) / k;
+    const int u = write_unary((uint64_t)h);
+    const uint64_t left = 1ull << (h * k);
+    return u + write_minimal_binary(v - left, (left << k) - left);
+  }
+  // Moves the pending bits into words (zero-padded); nothing may be written afterwards.
+  void finish() {
+    if (pend_ > 0) words.push_back(acc_);
+    acc_ = 0;
+    pend_ = 0;
+  }
+
+ private:
+  uint64_t acc_ = 0;  // pending bits, in the top pend_ bits
+  int pend_ = 0;      // < 64
+};
+
+inline void BitWriter::append_words(const WordWriter& o) {
+  if (o.nbits == 0) return;
+  const int used = (int)(nbits & 7);
+  const size_t first = (size_t)(nbits >> 3);  // byte holding bit nbits
+  nbits += o.nbits;
+  bytes.resize((size_t)((nbits + 7) >> 3), 0);
+  uint8_t* d = bytes.data() + first;
+  const size_t avail = bytes.size() - first;  // bytes from d on
+  const size_t nw = (size_t)((o.nbits + 63) >> 6);
+  for (size_t i = 0; i < nw; ++i) {
+    const uint64_t x = o.words[i];
+    const uint64_t hi = x >> used;                                    // bytes 8i .. 8i+7
+    const uint8_t lo = used ? (uint8_t)(x << (8 - used)) : (uint8_t)0;  // top of byte 8i+8
+    const size_t at = 8 * i;
+    if (at + 9 <= avail) {
+      for (int k = 0; k < 8; ++k) d[at + (size_t)k] |= (uint8_t)(hi >> (56 - 8 * k));
+      d[at + 8] |= lo;
+    } else {
+      // The last word: bytes past the end hold only zero padding.
+      for (int k = 0; k < 8 && at + (size_t)k < avail; ++k) d[at + (size_t)k] |= (uint8_t)(hi >> (56 - 8 * k));
+      if (at + 8 < avail) d[at + 8] |= lo;
+    }
+  }
+}
 
 // Counts bits without storing them (the "NullOutputStream" bit counter of diffComp).
 struct BitCounter {

@@ -298,12 +298,12 @@ void GraphEncoder::add_block(const int32_t* const* succ, const int* outd, int co
   }
   // 3. Records written in parallel, each range into its own stream.
   const int parts = std::max(1, std::min(threads, count));
-  std::vector<BitWriter> outs((size_t)parts);
+  std::vector<WordWriter> outs((size_t)parts);
   std::vector<std::vector<uint64_t>> starts((size_t)parts);
   std::vector<EncoderStats> st((size_t)parts);
   parallel_ranges(count, parts, [&](int t, int lo, int hi) {
     DiffScratch sc;
-    BitWriter& o = outs[(size_t)t];
+    WordWriter& o = outs[(size_t)t];
     for (int i = lo; i < hi; ++i) {
       starts[(size_t)t].push_back(o.nbits);
       st[(size_t)t].bits_outdegrees += o.write_gamma((uint64_t)outd[i]);
@@ -313,6 +313,7 @@ void GraphEncoder::add_block(const int32_t* const* succ, const int* outd, int co
         diff_comp(o, params, sc, &st[(size_t)t], (int)(base + i), ref[(size_t)i], rl, rlen, succ[i], outd[i]);
       }
     }
+    o.finish();
   });
   // 4. Join in order; offsets of every record.
   for (int t = 0; t < parts; ++t) {
@@ -322,7 +323,7 @@ void GraphEncoder::add_block(const int32_t* const* succ, const int* outd, int co
       node_bit_offsets.push_back(at + s0);
       last_bit_ = at + s0;
     }
-    graph.append(outs[(size_t)t]);
+    graph.append_words(outs[(size_t)t]);
     add_stats(stats, st[(size_t)t]);
   }
   // 5. The ring holds the last cyc nodes for the next block, as add_node leaves it.
@@ -359,10 +360,10 @@ void TimestampEncoder::add_node(const int64_t* ts, int count) {
 void TimestampEncoder::add_block(const int64_t* const* ts, const int* count, int nodes, int threads) {
   if (nodes <= 0) return;
   const int parts = std::max(1, std::min(threads, nodes));
-  std::vector<BitWriter> outs((size_t)parts);
+  std::vector<WordWriter> outs((size_t)parts);
   std::vector<std::vector<uint64_t>> starts((size_t)parts);
   parallel_ranges(nodes, parts, [&](int t, int lo, int hi) {
-    BitWriter& o = outs[(size_t)t];
+    WordWriter& o = outs[(size_t)t];
     for (int i = lo; i < hi; ++i) {
       starts[(size_t)t].push_back(o.nbits);
       int64_t prev = min_timestamp;
@@ -371,11 +372,12 @@ void TimestampEncoder::add_block(const int64_t* const* ts, const int* count, int
         prev = ts[i][k];
       }
     }
+    o.finish();
   });
   for (int t = 0; t < parts; ++t) {
     const uint64_t at = out.nbits;
     for (uint64_t s0 : starts[(size_t)t]) node_bit_offsets.push_back(at + s0);
-    out.append(outs[(size_t)t]);
+    out.append_words(outs[(size_t)t]);
   }
 }
 
