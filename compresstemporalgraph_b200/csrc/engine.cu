@@ -146,10 +146,17 @@ int GraphHandle::end_call() {
 // ---------------------------------------------------------------------------------------------
 // Loading
 
+#if defined(__BYTE_ORDER__) && __BYTE_ORDER__ != __ORDER_LITTLE_ENDIAN__
+#error "the stream words are built by byte-swapping little-endian host loads"
+#endif
+
+// Byte i of the stream becomes bits 63-8(i%8) .. 56-8(i%8) of word i/8 (the device reads the
+// streams as big-endian 64-bit words); bytes past the end are zero.
 static void to_be_words(const std::vector<uint8_t>& bytes, std::vector<uint64_t>& words, size_t pad_words) {
   const size_t nw = (bytes.size() + 7) / 8;
   words.assign(nw + pad_words, 0);
-  for (size_t i = 0; i < bytes.size(); ++i) words[i >> 3] |= (uint64_t)bytes[i] << (56 - 8 * (i & 7));
+  if (!bytes.empty()) std::memcpy(words.data(), bytes.data(), bytes.size());
+  for (size_t i = 0; i < nw; ++i) words[i] = __builtin_bswap64(words[i]);
 }
 
 static void to_le_words(const std::vector<uint8_t>& bytes, std::vector<uint64_t>& words, size_t pad_words) {

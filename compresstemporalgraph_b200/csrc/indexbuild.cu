@@ -145,9 +145,12 @@ struct DeviceStream {
   DevBuf buf;
   Stream s{};
   int up(const std::vector<uint8_t>& bytes, cudaStream_t st) {
+    // big-endian 64-bit words, as the loader uploads the streams (two words of zero padding;
+    // the host is little-endian, which engine.cu checks)
     const size_t nw = (bytes.size() + 7) / 8 + 2;
     std::vector<uint64_t> w(nw, 0);
-    for (size_t i = 0; i < bytes.size(); ++i) w[i >> 3] |= (uint64_t)bytes[i] << (56 - 8 * (i & 7));
+    if (!bytes.empty()) std::memcpy(w.data(), bytes.data(), bytes.size());
+    for (size_t i = 0; i + 2 < nw; ++i) w[i] = __builtin_bswap64(w[i]);
     if (int rc = buf.ensure(nw * 8)) return rc;
     TGA_CUDA_TRY(cudaMemcpyAsync(buf.p, w.data(), nw * 8, cudaMemcpyHostToDevice, st));
     TGA_CUDA_TRY(cudaStreamSynchronize(st));
